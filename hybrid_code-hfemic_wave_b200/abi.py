@@ -1,0 +1,260 @@
+"""ctypes mirror of include/h1d_gpu.h.
+
+:class:`Run` drives one run through any library exporting the h1d C-ABI (the entry
+points are looked up with a name prefix, ``h1d_`` for the CUDA library).  Errors come back
+as the exceptions the reference raises for the same condition: ``H1D_ERR_MOVED_TOO_FAR``
+is ``std::domain_error`` "particle(s) moved too far" in PartSpecies::update_pos
+(src/hybrid_1d/Core/PartSpecies.cc:215-219) and becomes :class:`MovedTooFar`;
+``H1D_ERR_INVALID_ARG`` (std::invalid_argument) becomes :class:`ValueError`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import configs as _cfg
+
+PAD = 3
+MAX_KINETIC = 8
+MAX_COLD = 4
+ABI_VERSION = 1
+
+OK, ERR_INVALID_ARG, ERR_MOVED_TOO_FAR, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_NAN, ERR_STATE, \
+    ERR_NO_DEVICE = range(9)
+
+
+class H1DError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"h1d error {code}: {msg}")
+        self.code = code
+
+
+class MovedTooFar(H1DError):
+    """std::domain_error("... - particle(s) moved too far") of PartSpecies::update_pos."""
+
+
+class KineticDesc(C.Structure):
+    _fields_ = [("Oc", C.c_double), ("op", C.c_double), ("n_smooth", C.c_int64), ("Nc", C.c_int64),
+                ("shape_order", C.c_int64), ("moment_norm", C.c_double)]
+
+
+class ColdDesc(C.Structure):
+    _fields_ = [("Oc", C.c_double), ("op", C.c_double), ("n_smooth", C.c_int64)]
+
+
+class EFluidDesc(C.Structure):
+    _fields_ = [("Oc", C.c_double), ("op", C.c_double), ("beta", C.c_double), ("gamma", C.c_double)]
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("Nx", C.c_int64), ("Dx", C.c_double), ("xi", C.c_double), ("O0", C.c_double),
+        ("c", C.c_double), ("dt", C.c_double), ("n_subcycles", C.c_int64),
+        ("algorithm", C.c_int32), ("particle_bc", C.c_int32), ("randomize_gyrophase", C.c_int32),
+        ("precision", C.c_int32), ("gyrophase_seed", C.c_uint64),
+        ("phase_retardation_inset", C.c_int64), ("phase_retardation_factor", C.c_double),
+        ("amplitude_damping_inset", C.c_int64), ("amplitude_damping_factor", C.c_double),
+        ("moment_weighting", C.c_double), ("sort_interval", C.c_int32), ("n_kinetic", C.c_int32),
+        ("n_cold", C.c_int32), ("reserved0", C.c_int32), ("efluid", EFluidDesc),
+        ("kinetic", KineticDesc * MAX_KINETIC), ("cold", ColdDesc * MAX_COLD),
+    ]
+
+
+def make_params(cfg: "_cfg.RunConfig") -> Params:
+    cfg.validate()
+    p = Params()
+    p.Nx, p.Dx, p.xi, p.O0, p.c, p.dt = cfg.Nx, cfg.Dx, cfg.xi, cfg.O0, cfg.c, cfg.dt
+    p.n_subcycles = cfg.n_subcycles
+    p.algorithm, p.particle_bc = cfg.algorithm, cfg.particle_bc
+    p.randomize_gyrophase, p.gyrophase_seed = int(cfg.randomize_gyrophase), cfg.gyrophase_seed
+    p.precision = cfg.precision
+    p.phase_retardation_inset, p.phase_retardation_factor = cfg.phase_retardation
+    p.amplitude_damping_inset, p.amplitude_damping_factor = cfg.amplitude_damping
+    p.moment_weighting = 1.0
+    p.sort_interval = cfg.sort_interval
+    p.n_kinetic, p.n_cold = len(cfg.kinetic), len(cfg.cold)
+    if p.n_kinetic > MAX_KINETIC or p.n_cold > MAX_COLD:
+        raise ValueError("too many species")
+    ef = cfg.efluid
+    p.efluid = EFluidDesc(ef.Oc, ef.op, ef.beta, ef.gamma)
+    for i, k in enumerate(cfg.kinetic):
+        p.kinetic[i] = KineticDesc(k.Oc, k.op, k.n_smooth, k.Nc, k.shape_order, cfg.moment_norm(k))
+    for i, c in enumerate(cfg.cold):
+        p.cold[i] = ColdDesc(c.Oc, c.op, c.n_smooth)
+    return p
+
+
+_dp = C.POINTER(C.c_double)
+_lp = C.POINTER(C.c_int64)
+
+
+def _declare(lib, prefix):
+    def f(name, *args, res=C.c_int):
+        fn = getattr(lib, prefix + name)
+        fn.argtypes = list(args)
+        fn.restype = res
+        return fn
+
+    v = C.c_void_p
+    return dict(
+        create=f("create", C.POINTER(Params), C.POINTER(C.c_void_p)),
+        destroy=f("destroy", v),
+        upload_particles=f("upload_particles", v, C.c_int, C.c_int64, _dp, _dp, _dp, _dp, _dp),
+        upload_fields=f("upload_fields", v, _dp, _dp),
+        upload_cold=f("upload_cold", v, C.c_int, _dp, _dp),
+        advance=f("advance", v, C.c_uint32),
+        particle_count=f("particle_count", v, C.c_int, _lp),
+        download_particles=f("download_particles", v, C.c_int, _dp, _dp, _dp, _dp, _dp, _lp),
+        download_fields=f("download_fields", v, _dp, _dp),
+        download_sources=f("download_sources", v, _dp, _dp),
+        download_moments=f("download_moments", v, C.c_int, _dp, _dp, _dp),
+        download_cold=f("download_cold", v, C.c_int, _dp, _dp, _dp, _dp, _dp),
+        energy=f("energy", v, _dp, _dp, _dp, _dp),
+        status_string=f("status_string", v, res=C.c_char_p),
+    )
+
+
+def _ptr(a, ctype=C.c_double):
+    if a is None:
+        return None
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+_LIBS = {}
+
+
+def load_library(path: str, prefix: str):
+    key = (os.path.abspath(path), prefix)
+    if key not in _LIBS:
+        lib = C.CDLL(key[0])
+        _LIBS[key] = (lib, _declare(lib, prefix))
+    return _LIBS[key]
+
+
+class Run:
+    """One run (a Domain) behind the h1d C-ABI of library ``path`` with symbol ``prefix``."""
+
+    def __init__(self, cfg: "_cfg.RunConfig", path: str, prefix: str = "h1d_"):
+        self.cfg = cfg
+        self.lib, self.fn = load_library(path, prefix)
+        self.params = make_params(cfg)
+        self.M = cfg.Nx + 2 * PAD
+        h = C.c_void_p()
+        self._check(self.fn["create"](C.byref(self.params), C.byref(h)), h=None)
+        self.h = h
+
+    # ----- plumbing -----
+    def _check(self, st, h="self"):
+        if st == OK:
+            return
+        hh = self.h if h == "self" else h
+        msg = self.fn["status_string"](hh).decode() if hh else ""
+        if st == ERR_MOVED_TOO_FAR:
+            raise MovedTooFar(st, msg or "particle(s) moved too far")
+        if st == ERR_INVALID_ARG:
+            raise ValueError(msg or "invalid argument")
+        raise H1DError(st, msg)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.fn["destroy"](self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ----- uploads -----
+    def upload_particles(self, s, q1, vx, vy, vz, w):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (q1, vx, vy, vz, w)]
+        n = arrs[0].size
+        self._check(self.fn["upload_particles"](self.h, s, n, *[_ptr(a) for a in arrs]))
+
+    def upload_fields(self, B, E):
+        B = np.ascontiguousarray(B, dtype=np.float64).reshape(-1)
+        E = np.ascontiguousarray(E, dtype=np.float64).reshape(-1)
+        assert B.size == 3 * self.M and E.size == 3 * self.M
+        self._check(self.fn["upload_fields"](self.h, _ptr(B), _ptr(E)))
+
+    def upload_cold(self, i, n_full, nV_full):
+        n = np.ascontiguousarray(n_full, dtype=np.float64).reshape(-1)
+        v = np.ascontiguousarray(nV_full, dtype=np.float64).reshape(-1)
+        self._check(self.fn["upload_cold"](self.h, i, _ptr(n), _ptr(v)))
+
+    def upload_state(self, st):
+        """Upload a state dict as read by tests/golden/state_io.read_state."""
+        for s, p in enumerate(st["particles"]):
+            self.upload_particles(s, p["q1"], p["vx"], p["vy"], p["vz"], p["w"])
+        self.upload_fields(st["B"], st["E"])
+        for i, c in enumerate(st["cold"]):
+            self.upload_cold(i, c["n_full"], c["nV_full"])
+
+    # ----- stepping -----
+    def advance(self, n_steps: int):
+        self._check(self.fn["advance"](self.h, n_steps))
+
+    # ----- downloads -----
+    def particle_count(self, s) -> int:
+        n = C.c_int64()
+        self._check(self.fn["particle_count"](self.h, s, C.byref(n)))
+        return n.value
+
+    def particles(self, s):
+        n = self.particle_count(s)
+        out = {k: np.empty(n) for k in ("q1", "vx", "vy", "vz", "w")}
+        pid = np.empty(n, dtype=np.int64)
+        self._check(self.fn["download_particles"](self.h, s, *[_ptr(out[k]) for k in ("q1", "vx", "vy", "vz", "w")],
+                                                  _ptr(pid, C.c_int64)))
+        out["pid"] = pid
+        return out
+
+    def fields(self):
+        B, E = np.empty((self.M, 3)), np.empty((self.M, 3))
+        self._check(self.fn["download_fields"](self.h, _ptr(B), _ptr(E)))
+        return B, E
+
+    def sources(self):
+        rho, J = np.empty(self.M), np.empty((self.M, 3))
+        self._check(self.fn["download_sources"](self.h, _ptr(rho), _ptr(J)))
+        return rho, J
+
+    def moments(self, s):
+        n, nV, nvv = np.empty(self.M), np.empty((self.M, 3)), np.empty((self.M, 6))
+        self._check(self.fn["download_moments"](self.h, s, _ptr(n), _ptr(nV), _ptr(nvv)))
+        return n, nV, nvv
+
+    def cold(self, i):
+        n, nV, nvv = np.empty(self.M), np.empty((self.M, 3)), np.empty((self.M, 6))
+        nf, nVf = np.empty(self.M), np.empty((self.M, 3))
+        self._check(self.fn["download_cold"](self.h, i, _ptr(n), _ptr(nV), _ptr(nvv), _ptr(nf), _ptr(nVf)))
+        return dict(n=n, nV=nV, nvv=nvv, n_full=nf, nV_full=nVf)
+
+    def energy(self):
+        ns = len(self.cfg.kinetic) + len(self.cfg.cold)
+        b, e = np.empty(3), np.empty(3)
+        lab, pla = np.empty((ns, 3)), np.empty((ns, 3))
+        self._check(self.fn["energy"](self.h, _ptr(b), _ptr(e), _ptr(lab), _ptr(pla)))
+        return dict(dB2O2=b, dE2O2=e, KE_lab=lab, KE_pla=pla)
+
+    def state(self):
+        """Everything, in the layout of tests/golden/state_io.read_state."""
+        B, E = self.fields()
+        rho, J = self.sources()
+        st = dict(B=B, E=E, charge=rho, current=J, particles=[], moments=[], cold=[])
+        for s in range(len(self.cfg.kinetic)):
+            st["particles"].append(self.particles(s))
+            n, nV, nvv = self.moments(s)
+            st["moments"].append(dict(n=n, nV=nV, nvv=nvv))
+        for i in range(len(self.cfg.cold)):
+            st["cold"].append(self.cold(i))
+        return st

@@ -1,0 +1,250 @@
+"""Run descriptions for the hybrid_1d hot path.
+
+The reference fixes every parameter at compile time in ``struct Input``
+(src/hybrid_1d/Include/Inputs.h:13-241).  Here a run is described at runtime by
+:class:`RunConfig`, which maps field-for-field onto that struct and onto the C struct
+``h1d_params`` of include/h1d_gpu.h.
+
+Species are given in physical terms (density fraction ``f``, charge number ``Z``, mass
+number ``A``) and converted with the reference's own normalisation: O0 = 1 (proton
+cyclotron frequency), ``c`` = c/vA, so a species has ``Oc = Z/A`` and
+``op = c*sqrt(f*Z**2/A)``; the electron fluid is ``eFluidDesc({-1836, c*sqrt(1836*ne)}, beta_e,
+closure)`` with ``ne = sum(f*Z)``.  The thermal speed of a bi-Maxwellian is
+``vth1 = sqrt(beta1)*c*|Oc|/op`` (src/LibPIC/PIC/VDF/MaxwellianVDF.cc:209).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from dataclasses import dataclass, field
+from typing import List
+
+ALGO_PC, ALGO_CAMCL = 0, 1
+BC_PERIODIC, BC_REFLECTING, BC_ABSORBING = 0, 1, 2
+PREC_FP64, PREC_MIXED = 0, 1
+ISOTHERMAL, ADIABATIC = 11, 53  # Closure (src/LibPIC/PIC/Predefined.h:35-38)
+
+
+@dataclass
+class Kinetic:
+    """A bi-Maxwellian kinetic species (BiMaxPlasmaDesc, PlasmaDesc.h:207-236)."""
+
+    Oc: float
+    op: float
+    Nc: int  # particles per cell
+    shape_order: int = 2
+    n_smooth: int = 2
+    beta1: float = 0.1  # parallel beta
+    T2_T1: float = 1.0  # perpendicular / parallel temperature
+
+    def vth1(self, c: float) -> float:
+        return math.sqrt(self.beta1) * c * abs(self.Oc) / self.op
+
+
+@dataclass
+class Cold:
+    """A cold fluid species (ColdPlasmaDesc, PlasmaDesc.h:92-114)."""
+
+    Oc: float
+    op: float
+    n_smooth: int = 2
+
+
+@dataclass
+class EFluid:
+    """Charge-neutralising massless electron fluid (eFluidDesc, PlasmaDesc.h:66-88)."""
+
+    Oc: float
+    op: float
+    beta: float = 0.0
+    closure: int = ISOTHERMAL
+
+    @property
+    def gamma(self) -> float:
+        # gamma(closure / 10) with integer division, then gamma /= closure % 10
+        return float(self.closure // 10) / float(self.closure % 10)
+
+
+@dataclass
+class RunConfig:
+    name: str
+    Nx: int
+    Dx: float
+    xi: float
+    c: float
+    dt: float
+    efluid: EFluid
+    kinetic: List[Kinetic] = field(default_factory=list)
+    cold: List[Cold] = field(default_factory=list)
+    O0: float = 1.0
+    n_subcycles: int = 10
+    algorithm: int = ALGO_CAMCL
+    particle_bc: int = BC_PERIODIC
+    randomize_gyrophase: bool = False
+    gyrophase_seed: int = 0
+    phase_retardation: tuple = (0, 0.0)
+    amplitude_damping: tuple = (0, 0.0)
+    precision: int = PREC_FP64
+    sort_interval: int = 0
+    steps: int = 1  # run length the preset is quoted on
+    inner_Nt: int = 10  # Input::inner_Nt
+
+    def replace(self, **kw) -> "RunConfig":
+        return dataclasses.replace(self, **kw)
+
+    @property
+    def n_particles(self) -> int:
+        return sum(k.Nc * self.Nx for k in self.kinetic)
+
+    # ----- extents (ParamSet.cc:20-23) -----
+    @property
+    def q1min(self) -> float:
+        return -0.5 * self.Nx
+
+    @property
+    def q1max(self) -> float:
+        return -0.5 * self.Nx + self.Nx
+
+    @property
+    def homogeneous(self) -> bool:
+        return self.xi < 1e-10  # MirrorGeometry.h:109, :185
+
+    def moment_norm(self, k: Kinetic) -> float:
+        """PartSpecies::Nc = Nx*Nc*Nrefcell_div_Ntotal (PartSpecies.cc:150-154) for a
+        bi-Maxwellian (MaxwellianVDF.cc:213-215, N_of_q1 :229-239)."""
+        if self.Nx * k.Nc == 0:
+            return 1.0
+        return self.Nx * k.Nc * nrefcell_div_ntotal(self, k)
+
+    def validate(self) -> None:
+        """The static checks of InputWrapper.h:132-155 and ParamSet.cc:25-29."""
+        if self.Nx < 6:
+            raise ValueError("Nx must be at least 2*number_of_ghost_cells")
+        if self.n_subcycles < 2:
+            raise ValueError("number of subcyclings should be at least 2")
+        for inset, _ in (self.phase_retardation, self.amplitude_damping):
+            if inset > self.Nx // 2:
+                raise ValueError("masking inset is greater than half the domain length")
+        if self.xi > 0:
+            for q1 in (self.q1min, self.q1max, self.q1min + 0.5, self.q1max + 0.5):
+                if not abs(self.xi * self.Dx * q1) < math.pi / 2:
+                    raise ValueError("invalid domain extent: |xi*D1*q1| >= pi/2")
+
+
+def _n_of_q1(cfg: RunConfig, k: Kinetic, q1: float) -> float:
+    """MaxwellianVDF::N_of_q1 (MaxwellianVDF.cc:229-239)."""
+    T2OT1 = k.T2_T1
+    if cfg.homogeneous:
+        xiD1q1 = cfg.xi * cfg.Dx * q1
+        return q1 * (1 - (xiD1q1 * xiD1q1) * (T2OT1 - 1) / 3)
+    s = math.sqrt(T2OT1)
+    return math.atan(s * math.tan(cfg.xi * cfg.Dx * q1)) / (s * cfg.Dx * cfg.xi)
+
+
+def _q1_of_n(cfg: RunConfig, k: Kinetic, N: float) -> float:
+    """MaxwellianVDF::q1_of_N (MaxwellianVDF.cc:240-250)."""
+    T2OT1 = k.T2_T1
+    if cfg.homogeneous:
+        xiD1N = cfg.xi * cfg.Dx * N
+        return N * (1 + (xiD1N * xiD1N) * (T2OT1 - 1) / 3)
+    s = math.sqrt(T2OT1)
+    return math.atan(math.tan(s * cfg.Dx * cfg.xi * N) / s) / (cfg.xi * cfg.Dx)
+
+
+def nrefcell_div_ntotal(cfg: RunConfig, k: Kinetic) -> float:
+    loc = _n_of_q1(cfg, k, cfg.q1min)
+    length = _n_of_q1(cfg, k, cfg.q1max) - loc
+    return (_n_of_q1(cfg, k, +0.5) - _n_of_q1(cfg, k, -0.5)) / length
+
+
+def plasma(c: float, species, cold_fraction: float, beta_e: float, closure=ISOTHERMAL,
+           cold_smooth: int = 2):
+    """Build (efluid, kinetic, cold) from physical fractions.
+
+    ``species`` is a list of dicts with keys f, Z, A, Nc, shape_order, beta1, T2_T1, n_smooth.
+    """
+    kin = []
+    ne = 0.0
+    for s in species:
+        Z, A, f = s.get("Z", 1.0), s.get("A", 1.0), s["f"]
+        ne += f * Z
+        kin.append(Kinetic(Oc=Z / A, op=c * math.sqrt(f * Z * Z / A), Nc=s["Nc"],
+                           shape_order=s.get("shape_order", 2), n_smooth=s.get("n_smooth", 2),
+                           beta1=s["beta1"], T2_T1=s.get("T2_T1", 1.0)))
+    cold = []
+    if cold_fraction > 0:
+        ne += cold_fraction
+        cold.append(Cold(Oc=1.0, op=c * math.sqrt(cold_fraction), n_smooth=cold_smooth))
+    ef = EFluid(Oc=-1836.0, op=c * math.sqrt(1836.0 * ne), beta=beta_e, closure=closure)
+    return ef, kin, cold
+
+
+# ---------------------------------------------------------------------------------------------
+# presets
+# ---------------------------------------------------------------------------------------------
+
+def config1() -> RunConfig:
+    """Plain FP64, CPU-runnable: uniform B0, periodic, Nx=256, Dx=0.3, dt=0.02, 1000 steps,
+    hot H+ (f=0.1, beta_par=0.1, T_perp/T_par=3, 100 ppc, CIC) + cold H+, beta_e=0.1, c/vA=100."""
+    ef, kin, cold = plasma(100.0, [dict(f=0.1, Nc=100, shape_order=1, beta1=0.1, T2_T1=3.0)],
+                           0.9, 0.1)
+    return RunConfig("config1_cic_periodic_nx256", Nx=256, Dx=0.3, xi=0.0, c=100.0, dt=0.02,
+                     efluid=ef, kinetic=kin, cold=cold, steps=1000)
+
+
+def config2() -> RunConfig:
+    """Plain FP64 GPU drop-in: mirror xi=0.002, Nx=2048, masking over 128 cells each end,
+    hot H+ (beta 0.2, A 4, 10%) + hot He+ (beta 0.05, A 2, 5%), 1000 ppc each, TSC,
+    dt=0.01, 5000 steps.  Particle boundary: reflecting (the reference has no absorbing BC)."""
+    ef, kin, cold = plasma(100.0, [
+        dict(f=0.10, Z=1, A=1, Nc=1000, shape_order=2, beta1=0.2, T2_T1=4.0),
+        dict(f=0.05, Z=1, A=4, Nc=1000, shape_order=2, beta1=0.05, T2_T1=2.0),
+    ], 0.85, 0.1)
+    return RunConfig("config2_tsc_mirror_nx2048", Nx=2048, Dx=0.3, xi=0.002, c=100.0, dt=0.01,
+                     efluid=ef, kinetic=kin, cold=cold, particle_bc=BC_REFLECTING,
+                     phase_retardation=(128, 1.0), amplitude_damping=(128, 0.2), steps=5000)
+
+
+def config3(precision=PREC_MIXED) -> RunConfig:
+    """Config-1 plasma at Nx=4096 with 4000 particles per cell (one kinetic species:
+    16.4M particles), 2000 steps."""
+    ef, kin, cold = plasma(100.0, [dict(f=0.1, Nc=4000, shape_order=1, beta1=0.1, T2_T1=3.0)],
+                           0.9, 0.1)
+    return RunConfig("config3_cic_periodic_nx4096", Nx=4096, Dx=0.3, xi=0.0, c=100.0, dt=0.02,
+                     efluid=ef, kinetic=kin, cold=cold, precision=precision, steps=2000)
+
+
+# small cases the oracle finishes in seconds; each is also built against the reference
+def parity_p1() -> RunConfig:
+    ef, kin, cold = plasma(100.0, [dict(f=0.1, Nc=16, shape_order=1, beta1=0.1, T2_T1=3.0)], 0.9, 0.1)
+    return RunConfig("p1_cic_periodic", Nx=32, Dx=0.3, xi=0.0, c=100.0, dt=0.02, efluid=ef,
+                     kinetic=kin, cold=cold, steps=10)
+
+
+def parity_p2() -> RunConfig:
+    ef, kin, cold = plasma(100.0, [
+        dict(f=0.10, Z=1, A=1, Nc=16, shape_order=2, beta1=0.2, T2_T1=4.0),
+        dict(f=0.05, Z=1, A=4, Nc=12, shape_order=2, beta1=0.05, T2_T1=2.0),
+    ], 0.85, 0.1)
+    return RunConfig("p2_tsc_mirror_reflecting", Nx=64, Dx=0.3, xi=0.05, c=100.0, dt=0.01,
+                     efluid=ef, kinetic=kin, cold=cold, particle_bc=BC_REFLECTING,
+                     phase_retardation=(8, 1.0), amplitude_damping=(8, 0.2), steps=10)
+
+
+def parity_p3() -> RunConfig:
+    ef, kin, cold = plasma(100.0, [dict(f=0.2, Nc=20, shape_order=3, beta1=0.3, T2_T1=2.0,
+                                        n_smooth=1)], 0.8, 0.2, closure=ADIABATIC, cold_smooth=1)
+    return RunConfig("p3_o3_adiabatic_periodic", Nx=48, Dx=0.25, xi=0.0, c=50.0, dt=0.02,
+                     efluid=ef, kinetic=kin, cold=cold, n_subcycles=4, steps=10)
+
+
+def parity_p4() -> RunConfig:
+    ef, kin, cold = plasma(100.0, [dict(f=0.1, Nc=16, shape_order=2, beta1=0.2, T2_T1=3.0)], 0.9, 0.1)
+    return RunConfig("p4_pc_tsc_mirror_reflecting", Nx=64, Dx=0.3, xi=0.03, c=100.0, dt=0.01,
+                     efluid=ef, kinetic=kin, cold=cold, algorithm=ALGO_PC,
+                     particle_bc=BC_REFLECTING, phase_retardation=(6, 1.0),
+                     amplitude_damping=(6, 0.2), steps=10)
+
+
+PARITY = {f().name: f for f in (parity_p1, parity_p2, parity_p3, parity_p4)}
+PRESETS = {f().name: f for f in (config1, config2, config3)}

@@ -1,0 +1,191 @@
+/*
+ * h1d_gpu.h -- C-ABI of the B200 (sm_100a) implementation of the hybrid_1d per-step hot path.
+ *
+ * The hot path is one step of the kinetic-ion / fluid-electron cycle of the 1-D hybrid code
+ * for HFEMIC wave simulations (kyungguk1/hybrid_code-hfemic_wave):
+ *   Boris push of kinetic ions in the mirror field B0(1 + xi^2 x^2) with its curvilinear
+ *   transforms, Shape<1..3> interpolation of E and dB to the particles, deposit of the n and
+ *   nV moments (nvv on demand), particle boundary conditions, and the CAM-CL or
+ *   predictor-corrector B/E/current cycle that consumes the moments.
+ *
+ * Every entry point replaces one piece of the reference's `Domain` interface, so that a
+ * `Domain` subclass can forward `advance_by` here (see INTEGRATION.md for the adapter):
+ *
+ *   h1d_create            <- Domain_CAMCL / Domain_PC constructors
+ *                            (src/hybrid_1d/Core/Domain_CAMCL.cc:11, Core/Domain_PC.cc:11,
+ *                             Core/Domain.cc:42-55) with the compile-time `Input` of
+ *                            src/hybrid_1d/Include/Inputs.h:13-241 passed as a runtime struct
+ *   h1d_upload_particles  <- PartSpecies::bucket after populate/load_ptls
+ *                            (Core/PartSpecies.h:33-34, Core/PartSpecies.cc:180-206)
+ *   h1d_upload_fields     <- Domain::bfield / Domain::efield contents (Core/Domain.h:30-31)
+ *   h1d_upload_cold       <- ColdSpecies::mom0_full / mom1_full (Core/ColdSpecies.h:191-192)
+ *   h1d_advance           <- Domain::advance_by(unsigned) (Core/Domain.h:46,
+ *                            Core/Domain_CAMCL.cc:21-56, Core/Domain_PC.cc:21-78)
+ *   h1d_download_*        <- what the recorders read after advance_by: bfield, efield,
+ *                            charge, current, Species::moment<0..2>() (Core/Species.h:61-75),
+ *                            the particle bucket (Driver.cc:211-220)
+ *   h1d_energy            <- EnergyRecorder::dump (src/hybrid_1d/Recorder/EnergyRecorder.cc:98-140)
+ *
+ * Conventions
+ *   - Every function returns an int status (H1D_OK = 0).  Nonzero codes map to the
+ *     reference's exceptions: H1D_ERR_MOVED_TOO_FAR is the std::domain_error
+ *     "particle(s) moved too far" of PartSpecies::update_pos (Core/PartSpecies.cc:215-219);
+ *     H1D_ERR_INVALID_ARG is std::invalid_argument of the descriptors/ParamSet checks.
+ *     h1d_status_string() gives the detail of the last error of a run.
+ *   - Grid buffers use the reference GridArray layout (LibPIC/PIC/GridArray.h:36-38):
+ *     (Nx + 2*H1D_PAD) elements from dead_begin() to dead_end(), ghost cells included;
+ *     CartVector elements are interleaved {x,y,z} (24 B), CartTensor elements are
+ *     {xx,yy,zz,xy,yz,zx} (48 B, LibPIC/PIC/VT/TensorTemplate.h:25-38).
+ *   - Particle buffers are structure-of-arrays in caller memory.  The library keeps no
+ *     pointer to caller memory after a call returns.  The library owns all device memory.
+ *   - One run is driven by one host thread at a time (the reference Domain is
+ *     single-threaded).  Each run owns one CUDA stream; all work of a run is ordered on it.
+ */
+#ifndef H1D_GPU_H
+#define H1D_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define H1D_ABI_VERSION 1
+
+/* number of ghost cells on each side; Input::number_of_ghost_cells (Include/Inputs.h:22) */
+#define H1D_PAD 3
+#define H1D_MAX_KINETIC 8
+#define H1D_MAX_COLD 4
+
+/* status codes */
+enum {
+    H1D_OK                = 0,
+    H1D_ERR_INVALID_ARG   = 1, /* std::invalid_argument in the reference */
+    H1D_ERR_MOVED_TOO_FAR = 2, /* std::domain_error, PartSpecies.cc:218 */
+    H1D_ERR_OOM           = 3,
+    H1D_ERR_CUDA          = 4,
+    H1D_ERR_TIMEOUT       = 5,
+    H1D_ERR_NAN           = 6,
+    H1D_ERR_STATE         = 7, /* call out of order, e.g. advance before upload */
+    H1D_ERR_NO_DEVICE     = 8
+};
+
+/* Algorithm (LibPIC/PIC/Predefined.h:27-30): same numeric values */
+enum { H1D_ALGO_PC = 0, H1D_ALGO_CAMCL = 1 };
+/* BC (Predefined.h:49-52): same numeric values; ABSORBING is an extension without a
+ * reference counterpart (particles leaving the domain are dropped) */
+enum { H1D_BC_PERIODIC = 0, H1D_BC_REFLECTING = 1, H1D_BC_ABSORBING = 2 };
+/* arithmetic of the particle push/deposit; the field cycle is FP64 in both */
+enum { H1D_PREC_FP64 = 0, H1D_PREC_MIXED = 1 };
+
+/* KineticPlasmaDesc (LibPIC/PIC/PlasmaDesc.h:118-177), full-f only */
+typedef struct h1d_kinetic_desc {
+    double  Oc;          /* PlasmaDesc::Oc, signed cyclotron frequency */
+    double  op;          /* PlasmaDesc::op, plasma frequency */
+    int64_t n_smooth;    /* PlasmaDesc::number_of_source_smoothings */
+    int64_t Nc;          /* KineticPlasmaDesc::Nc, particles per cell (informational) */
+    int64_t shape_order; /* 1 (CIC), 2 (TSC) or 3 */
+    double  moment_norm; /* PartSpecies::Nc (PartSpecies.cc:150-154): Nx*Nc*Nrefcell_div_Ntotal,
+                            the particle count of the reference cell used to normalise moments */
+} h1d_kinetic_desc;
+
+/* ColdPlasmaDesc (PlasmaDesc.h:92-114) */
+typedef struct h1d_cold_desc {
+    double  Oc;
+    double  op;
+    int64_t n_smooth;
+} h1d_cold_desc;
+
+/* eFluidDesc (PlasmaDesc.h:66-88); gamma = closure/10 / (closure%10) */
+typedef struct h1d_efluid_desc {
+    double Oc;
+    double op;
+    double beta;
+    double gamma;
+} h1d_efluid_desc;
+
+/* The runtime form of `struct Input` (Include/Inputs.h:13-241) for one run */
+typedef struct h1d_params {
+    int64_t Nx;          /* Input::Nx, whole domain (one GPU holds the whole field line) */
+    double  Dx;          /* Input::Dx */
+    double  xi;          /* Input::xi */
+    double  O0;          /* Input::O0 */
+    double  c;           /* Input::c */
+    double  dt;          /* Input::dt */
+    int64_t n_subcycles; /* Input::n_subcycles (CAM-CL only), >= 2 */
+    int32_t algorithm;   /* H1D_ALGO_* */
+    int32_t particle_bc; /* H1D_BC_* */
+    int32_t randomize_gyrophase; /* Input::should_randomize_gyrophase_of_reflecting_particles;
+                                    the reference seeds from std::random_device (Delegate.cc:146-156);
+                                    here a counter-based hash of (seed, step, particle) */
+    int32_t precision;   /* H1D_PREC_* */
+    uint64_t gyrophase_seed;
+    int64_t phase_retardation_inset;  /* Input::phase_retardation (MaskingFunction.h:14-39) */
+    double  phase_retardation_factor;
+    int64_t amplitude_damping_inset;  /* Input::amplitude_damping */
+    double  amplitude_damping_factor;
+    double  moment_weighting; /* Species::m_moment_weighting_factor = 1/clones (Species.cc:110-117); 1 */
+    int32_t sort_interval;    /* steps between particle cell sorts; 0 = library default */
+    int32_t n_kinetic;
+    int32_t n_cold;
+    int32_t reserved0;
+    h1d_efluid_desc  efluid;
+    h1d_kinetic_desc kinetic[H1D_MAX_KINETIC];
+    h1d_cold_desc    cold[H1D_MAX_COLD];
+} h1d_params;
+
+typedef struct h1d_run h1d_run;
+
+/* ABI introspection: H1D_ABI_VERSION and sizeof(h1d_params) the library was built with */
+int  h1d_abi_version(void);
+size_t h1d_params_size(void);
+
+/* Validate params (same checks as InputWrapper.h:132-155, ParamSet.cc:25-29 and the
+ * descriptor constructors) and allocate the run on the current CUDA device. */
+int h1d_create(const h1d_params *params, h1d_run **out);
+int h1d_destroy(h1d_run *run);
+
+/* Particles of kinetic species `s` as SoA, positions q1 in [-Nx/2, Nx/2) (ParamSet.cc:22).
+ * Replaces any previous particles of that species. */
+int h1d_upload_particles(h1d_run *run, int s, int64_t n, const double *q1, const double *vx,
+                         const double *vy, const double *vz, const double *w);
+/* B (full grid) and E (half grid), each (Nx+2*H1D_PAD)*3 doubles, GridArray layout */
+int h1d_upload_fields(h1d_run *run, const double *B, const double *E);
+/* cold species `i`: mom0_full (Nx+2*H1D_PAD doubles), mom1_full ((Nx+2*H1D_PAD)*3) */
+int h1d_upload_cold(h1d_run *run, int i, const double *n_full, const double *nV_full);
+
+/* Domain::advance_by(n_steps), then wait and check the device status word. */
+int h1d_advance(h1d_run *run, uint32_t n_steps);
+/* Enqueue advance_by(n_steps) on the run's stream without waiting. */
+int h1d_advance_async(h1d_run *run, uint32_t n_steps);
+/* Wait for the run's stream; report a device-side error (moved too far, NaN) if any. */
+int h1d_synchronize(h1d_run *run);
+/* The run's cudaStream_t, for callers that time or order work around the run. */
+int h1d_get_stream(h1d_run *run, void **stream);
+
+int h1d_particle_count(h1d_run *run, int s, int64_t *n);
+/* Any output pointer may be NULL.  pid[k] is the upload index of the k-th particle (the
+ * library keeps particles cell-sorted, so the order is its own). */
+int h1d_download_particles(h1d_run *run, int s, double *q1, double *vx, double *vy, double *vz,
+                           double *w, int64_t *pid);
+int h1d_download_fields(h1d_run *run, double *B, double *E);
+/* Domain::charge and Domain::current after the last step ((Nx+2*H1D_PAD) and *3 doubles) */
+int h1d_download_sources(h1d_run *run, double *charge, double *current);
+/* Species::moment<0..2>() of kinetic species `s` after the post-process collect_all
+ * (PartSpecies.cc:234-248, 330-349, always CIC) and boundary_gather; any pointer may be NULL */
+int h1d_download_moments(h1d_run *run, int s, double *n, double *nV, double *nvv);
+/* cold species moments after collect_all (ColdSpecies.cc:268-297) and mom0_full/mom1_full */
+int h1d_download_cold(h1d_run *run, int i, double *n, double *nV, double *nvv, double *n_full,
+                      double *nV_full);
+/* EnergyRecorder::dump (EnergyRecorder.cc:98-140): dB2O2[3], dE2O2[3], and for every kinetic
+ * species then every cold species KE_lab[3], KE_pla[3]; computed on the device */
+int h1d_energy(h1d_run *run, double *dB2O2, double *dE2O2, double *KE_lab, double *KE_pla);
+
+const char *h1d_status_string(h1d_run *run);
+const char *h1d_error_name(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* H1D_GPU_H */

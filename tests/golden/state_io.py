@@ -1,0 +1,51 @@
+"""Reader for the raw state files written by oracle/ref/ref_driver.cc (``dump``).
+
+layout (little endian):
+  char[8] "H1DSTATE"; int64 Nx, pad, n_kinetic, n_cold, step; double moment_norm[n_kinetic]
+  per kinetic species: int64 n; double q1[n], vx[n], vy[n], vz[n], w[n]; int64 id[n]
+  B[M*3], E[M*3], charge[M], current[M*3]                       (M = Nx + 2*pad)
+  per kinetic species: n[M], nV[M*3], nvv[M*6]
+  per cold species:    n_full[M], nV_full[M*3], n[M], nV[M*3], nvv[M*6]
+"""
+import numpy as np
+
+
+def read_state(path):
+    with open(path, "rb") as f:
+        buf = f.read()
+    if buf[:8] != b"H1DSTATE":
+        raise ValueError("not a state file")
+    off = 8
+
+    def i64(k=1):
+        nonlocal off
+        a = np.frombuffer(buf, dtype="<i8", count=k, offset=off)
+        off += 8 * k
+        return a
+
+    def f64(k):
+        nonlocal off
+        a = np.frombuffer(buf, dtype="<f8", count=k, offset=off).copy()
+        off += 8 * k
+        return a
+
+    Nx, pad, nk, nc, step = (int(x) for x in i64(5))
+    M = Nx + 2 * pad
+    st = dict(Nx=Nx, pad=pad, step=step, moment_norm=f64(nk), particles=[], moments=[], cold=[])
+    for _ in range(nk):
+        n = int(i64()[0])
+        p = {k: f64(n) for k in ("q1", "vx", "vy", "vz", "w")}
+        p["id"] = i64(n).copy()
+        st["particles"].append(p)
+    st["B"] = f64(3 * M).reshape(M, 3)
+    st["E"] = f64(3 * M).reshape(M, 3)
+    st["charge"] = f64(M)
+    st["current"] = f64(3 * M).reshape(M, 3)
+    for _ in range(nk):
+        st["moments"].append(dict(n=f64(M), nV=f64(3 * M).reshape(M, 3), nvv=f64(6 * M).reshape(M, 6)))
+    for _ in range(nc):
+        st["cold"].append(dict(n_full=f64(M), nV_full=f64(3 * M).reshape(M, 3), n=f64(M),
+                               nV=f64(3 * M).reshape(M, 3), nvv=f64(6 * M).reshape(M, 6)))
+    if off != len(buf):
+        raise ValueError("trailing bytes in state file")
+    return st
