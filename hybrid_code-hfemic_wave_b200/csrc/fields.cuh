@@ -1,0 +1,412 @@
+// Grid phase of the hybrid_1d hot path (FP64): everything of one cycle that is not a particle
+// loop, in one kernel launch.
+//
+// CAM-CL (src/hybrid_1d/Core/Domain_CAMCL.cc:57-193):
+//   per species collect_smooth of n/nV at x^N and x^{N+1} (Domain.hh:155-194): 1/Nc scale,
+//   charge/current conversion factors (Species.h:42-49), ghost fold (SubdomainDelegate.cc:122-181),
+//   3-point smoothing (GridArray.h:134-142); cold fluid push and moments (ColdSpecies.cc:251-285);
+//   averaging; the B subcycle with Ohm's-law E (BField.cc:74-124, EField.cc:245-330);
+//   E*, current advance with Lambda/Gamma (Domain_CAMCL.cc:131-151, Current.cc:181-188); final E;
+//   B on the half grid for the next push (PartSpecies.cc:132-139).
+// Predictor-corrector (src/hybrid_1d/Core/Domain_PC.cc:84-205) uses the same building blocks in
+// three phases around its two particle passes.
+//
+// Layout and parallelisation.  Every grid quantity of the reference, ghost cells included, is
+// the periodic image of the interior after each boundary_pass (ghosts are filled periodically
+// whatever the particle boundary; only the moment fold and the masking depend on position).  So
+// each CTA owns `seg` interior cells and recomputes, redundantly, a halo of `H` cells on each side
+// from the step's inputs; H is larger than the total stencil reach of one cycle, so CTAs never
+// exchange data inside a step and there is no inter-CTA synchronisation.  One thread per local
+// cell; all arrays of the cycle live in shared memory.  Per-cell geometry (cos of the mirror
+// field at full and half grid points, masking factors) is tabulated once on the host.
+//
+// This file is compiled without FMA contraction so that, given the same moments, the field
+// cycle evaluates the reference's expressions operation for operation.
+#pragma once
+
+#include "device_common.cuh"
+
+namespace h1d {
+
+constexpr int MAXK = 8;
+constexpr int MAXC = 4;
+
+// per-cell geometry table, SoA over the Nx interior cells (index = interior cell)
+enum GeoIdx {
+    G_FCOV_X, G_FCOV_Y, G_FCOV_Z, // covariant basis at full-grid points  (CurviBasis.h:52-56)
+    G_FCON_X, G_FCON_Y, G_FCON_Z, // contravariant basis at full-grid points (CurviBasis.h:65-69)
+    G_HCOV_X, G_HCOV_Y, G_HCOV_Z, // same at half-grid points
+    G_HCON_X, G_HCON_Y, G_HCON_Z,
+    G_HBX,                        // Bcart(half point).x = O0/cos^2 (MFABasis.h:262)
+    G_MP1, G_MP2, G_MA1, G_MA2,   // phase-retardation / amplitude-damping factors, in the order
+                                  // the reference applies them (BField.cc:90-98)
+    G_COUNT
+};
+
+struct KinSrc {
+    double const *raw[2][4]; // unscaled deposits at x^N and x^{N+1}: n, nVx, nVy, nVz (cell 0)
+    double       *zero[2][4]; // the deposit set of the next cycle, cleared here
+    double        s1;         // 1/Nc (PartSpecies.cc:327-328)
+    double        cdcf, ccf;  // charge / current density conversion factors
+    double        lamf, gamf; // Lambda / Gamma factors (Charge.cc:75-80, Current.cc:170-175)
+    int           nsm;
+};
+struct ColdSrc {
+    double const *n;    // mom0_full (cell 0)
+    double const *nV_in;
+    double       *nV_out;
+    BorisK        boris;
+    double        cdcf, ccf, lamf, gamf, w;
+    int           nsm;
+};
+
+struct FieldArgs {
+    int           Nx, H, seg, bc;
+    double const *geo; // G_COUNT x Nx
+    double const *B_in, *E_in; // AoS, cell 0
+    double       *B_out, *E_out, *Bh_out, *charge_out, *current_out;
+    int           nk, nc;
+    KinSrc        k[MAXK];
+    ColdSrc       c[MAXC];
+    double        dt, sub_dt, c_light, sqrt_g, O0, inv_D1;
+    int           m; // n_subcycles
+    // electron fluid (EField.cc:267-291)
+    double        mOeOO0oe2, gamma, O02beO2, cO2, cOsqrtg;
+    // predictor-corrector phase selector
+    int           phase;
+    double const *B0_in, *E0_in, *charge_in, *current_in; // PC
+    double       *B1_out, *E1_out;                       // PC averaged fields for the pushes
+};
+
+struct Cell {
+    int    t, L, g, gm;
+    bool   owner;
+    double fcx, fcy, fcz, fnx, fny, fnz, hcx, hcy, hcz, hnx, hny, hnz, hbx, mp1, mp2, ma1, ma2;
+};
+
+// fold of one raw deposit array onto interior cell gm, times 1/Nc and a conversion factor
+__device__ __forceinline__ double fold(double const *r, int gm, int Nx, int bc, double s1, double f)
+{
+    double v = (r[gm] * s1) * f;
+    if (bc == 0) {
+        if (gm < PAD)
+            v = v + (r[Nx + gm] * s1) * f;
+        if (gm >= Nx - PAD)
+            v = v + (r[gm - Nx] * s1) * f;
+    } else {
+        if (gm == 0)
+            v = v + ((r[-1] * s1) * f + ((r[-2] * s1) * f + (r[-3] * s1) * f));
+        if (gm == Nx - 1)
+            v = v + ((r[Nx] * s1) * f + ((r[Nx + 1] * s1) * f + (r[Nx + 2] * s1) * f));
+    }
+    return v;
+}
+
+__device__ __forceinline__ d3 sld3(double const *a, int t) { return { a[3 * t], a[3 * t + 1], a[3 * t + 2] }; }
+__device__ __forceinline__ void sst3(double *a, int t, d3 v) { a[3 * t] = v.x, a[3 * t + 1] = v.y, a[3 * t + 2] = v.z; }
+
+// n smoothings of a scalar and a vector array together (Charge::smooth / Current::smooth,
+// GridArray.h:134-142); ping-pongs between (a, v) and (ta, tv) and returns where the result is
+struct SV {
+    double *a, *v;
+};
+static __device__ SV smooth_n(Cell const &C, int n, double *a, double *v, double *ta, double *tv)
+{
+    int const tl = max(C.t - 1, 0), tr = min(C.t + 1, C.L - 1);
+    for (int it = 0; it < n; ++it) {
+        __syncthreads();
+        ta[C.t] = (a[tl] + 2 * a[C.t] + a[tr]) * .25;
+        for (int k = 0; k < 3; ++k)
+            tv[3 * C.t + k] = (v[3 * tl + k] + 2 * v[3 * C.t + k] + v[3 * tr + k]) * .25;
+        double *x = a;
+        a         = ta;
+        ta        = x;
+        x         = v;
+        v         = tv;
+        tv        = x;
+    }
+    __syncthreads();
+    return { a, v };
+}
+
+__device__ __forceinline__ d3 covar_full(Cell const &C, d3 b) { return { C.fcx * b.x, C.fcy * b.y, C.fcz * b.z }; }
+__device__ __forceinline__ d3 contr_full(Cell const &C, d3 b) { return { C.fnx * b.x, C.fny * b.y, C.fnz * b.z }; }
+__device__ __forceinline__ d3 covar_half(Cell const &C, d3 b) { return { C.hcx * b.x, C.hcy * b.y, C.hcz * b.z }; }
+__device__ __forceinline__ d3 contr_half(Cell const &C, d3 b) { return { C.hnx * b.x, C.hny * b.y, C.hnz * b.z }; }
+__device__ __forceinline__ d3 mask_p(Cell const &C, d3 v) { return (v * C.mp1) * C.mp2; }
+__device__ __forceinline__ d3 mask_a(Cell const &C, d3 v) { return (v * C.ma1) * C.ma2; }
+
+// electron pressure gradient, masked (EField.cc:267-291, 248): needs Pe of the neighbours
+__device__ __forceinline__ double dPe_at(FieldArgs const &a, Cell const &C, double const *Pe)
+{
+    int const tl = max(C.t - 1, 0), tr = min(C.t + 1, C.L - 1);
+    return ((Pe[tr] - Pe[tl]) * a.cO2 * C.mp1) * C.mp2;
+}
+__device__ __forceinline__ double Pe_of(FieldArgs const &a, double rho)
+{
+    return pow(a.mOeOO0oe2 * rho, a.gamma) * a.O02beO2;
+}
+
+// Ohm's law at this cell (EField.cc:292-330) from Bcov/Bcon of the current B (with the
+// neighbour at t+1), contravariant current jc, masked dPe and rho; returns the masked E
+__device__ __forceinline__ d3 E_at(FieldArgs const &a, Cell const &C, double const *Bcov, double const *Bcon, d3 jc,
+                                   double dPe, double rho)
+{
+    int const t = C.t, tr = min(t + 1, C.L - 1);
+    d3 const  B1 = sld3(Bcov, tr), B0 = sld3(Bcov, t);
+    d3        Je = { 0 - jc.x, (-B1.z + B0.z) * a.cOsqrtg - jc.y, (+B1.y - B0.y) * a.cOsqrtg - jc.z };
+    Je           = mask_p(C, Je);
+    d3 const  d1 = sld3(Bcon, tr), d0 = sld3(Bcon, t);
+    d3 const  Bc = { a.inv_D1 * a.O0 + (d1.x + d0.x) * 0.5, 0 * a.O0 + (d1.y + d0.y) * 0.5, 0 * a.O0 + (d1.z + d0.z) * 0.5 };
+    d3 const  lz = cross(Je, Bc) * a.sqrt_g;
+    d3 const  Ec = { (lz.x - dPe) / rho, (lz.y - 0.0) / rho, (lz.z - 0.0) / rho };
+    return mask_a(C, contr_half(C, Ec));
+}
+
+// Faraday at this cell (BField.cc:74-114) from Ecov at t and t-1; returns the new masked B
+__device__ __forceinline__ d3 B_at(FieldArgs const &a, Cell const &C, double const *Ecov, d3 Bprev, double dtp)
+{
+    int const    t = C.t, tl = max(t - 1, 0);
+    double const k = dtp * a.c_light / a.sqrt_g;
+    d3 const     E1 = sld3(Ecov, t), E0 = sld3(Ecov, tl);
+    d3 const     Bc = { 0, (-E1.z + E0.z) * k, (+E1.y - E0.y) * k };
+    d3 const     Bk = covar_full(C, Bc); // contr_to_cart uses the covariant basis
+    d3           B  = { 0 - Bk.x, 0 - Bk.y, 0 - Bk.z };
+    B               = mask_p(C, B);
+    B               = B + Bprev;
+    return mask_a(C, B);
+}
+
+__device__ __forceinline__ void load_cell(FieldArgs const &a, Cell &C)
+{
+    C.t     = threadIdx.x;
+    C.L     = blockDim.x;
+    int const g0 = blockIdx.x * a.seg;
+    C.g     = g0 - a.H + C.t;
+    C.gm    = ((C.g % a.Nx) + a.Nx) % a.Nx;
+    C.owner = C.t >= a.H && C.t < a.H + a.seg && C.g < a.Nx;
+    double const *G = a.geo;
+    long const    N = a.Nx, i = C.gm;
+    C.fcx = G[G_FCOV_X * N + i], C.fcy = G[G_FCOV_Y * N + i], C.fcz = G[G_FCOV_Z * N + i];
+    C.fnx = G[G_FCON_X * N + i], C.fny = G[G_FCON_Y * N + i], C.fnz = G[G_FCON_Z * N + i];
+    C.hcx = G[G_HCOV_X * N + i], C.hcy = G[G_HCOV_Y * N + i], C.hcz = G[G_HCOV_Z * N + i];
+    C.hnx = G[G_HCON_X * N + i], C.hny = G[G_HCON_Y * N + i], C.hnz = G[G_HCON_Z * N + i];
+    C.hbx = G[G_HBX * N + i];
+    C.mp1 = G[G_MP1 * N + i], C.mp2 = G[G_MP2 * N + i], C.ma1 = G[G_MA1 * N + i], C.ma2 = G[G_MA2 * N + i];
+}
+
+// owner writes of an interior value and of its ghost images (periodic fill, Delegate.cc:159-170)
+__device__ __forceinline__ void put3(double *g, Cell const &C, int Nx, d3 v)
+{
+    st3(g, C.gm, v);
+    if (C.gm < PAD)
+        st3(g, Nx + C.gm, v);
+    if (C.gm >= Nx - PAD)
+        st3(g, C.gm - Nx, v);
+}
+__device__ __forceinline__ void put1(double *g, Cell const &C, int Nx, double v)
+{
+    g[C.gm] = v;
+    if (C.gm < PAD)
+        g[Nx + C.gm] = v;
+    if (C.gm >= Nx - PAD)
+        g[C.gm - Nx] = v;
+}
+
+// shared-memory carve-up: 9 scalar and 14 vector arrays of L doubles
+struct Smem {
+    double *rho0, *rho1, *tr, *ts, *Pe, *Pe1, *lam, *t2, *rho_avg;
+    double *J0, *J1, *tJ, *tJs, *B0, *B1, *E, *Bcov, *Bcon, *Ecov, *gam, *Jsum, *Javg, *aux;
+};
+constexpr int SMEM_SCALARS = 9, SMEM_VECTORS = 14;
+__device__ __forceinline__ Smem carve(double *sm, int L)
+{
+    Smem s;
+    double *p = sm;
+    s.rho0 = p, p += L;
+    s.rho1 = p, p += L;
+    s.tr = p, p += L;
+    s.ts = p, p += L;
+    s.Pe = p, p += L;
+    s.Pe1 = p, p += L;
+    s.lam = p, p += L;
+    s.t2 = p, p += L;
+    s.rho_avg = p, p += L;
+    s.J0 = p, p += 3 * L;
+    s.J1 = p, p += 3 * L;
+    s.tJ = p, p += 3 * L;
+    s.tJs = p, p += 3 * L;
+    s.B0 = p, p += 3 * L;
+    s.B1 = p, p += 3 * L;
+    s.E = p, p += 3 * L;
+    s.Bcov = p, p += 3 * L;
+    s.Bcon = p, p += 3 * L;
+    s.Ecov = p, p += 3 * L;
+    s.gam = p, p += 3 * L;
+    s.Jsum = p, p += 3 * L;
+    s.Javg = p, p += 3 * L;
+    s.aux = p, p += 3 * L;
+    return s;
+}
+
+// collect_smooth of one kinetic species' deposit d; ends synchronised
+static __device__ SV collect_kinetic(FieldArgs const &a, Cell const &C, Smem const &S, KinSrc const &K, int d)
+{
+    int const gm = C.gm;
+    S.tr[C.t]    = fold(K.raw[d][0], gm, a.Nx, a.bc, K.s1, K.cdcf);
+    for (int q = 0; q < 3; ++q)
+        S.tJ[3 * C.t + q] = fold(K.raw[d][1 + q], gm, a.Nx, a.bc, K.s1, K.ccf);
+    return smooth_n(C, K.nsm, S.tr, S.tJ, S.ts, S.tJs);
+}
+
+// cold species (ColdSpecies.cc:251-285): push nV with E and the background field, moments x w
+static __device__ d3 cold_push(FieldArgs const &a, Cell const &C, ColdSrc const &K, double const *E_cell0)
+{
+    d3 const     E  = ld3(E_cell0, C.gm);
+    double const n  = K.n[C.gm];
+    d3 const     Bc = { C.hbx, 0 * a.O0, 0 * a.O0 };
+    return boris_push(K.boris, ld3(K.nV_in, C.gm), Bc, E * n);
+}
+
+#ifdef H1D_FIELD_TU
+// ------------------------------------------------------------------------------------------------
+// CAM-CL cycle (Domain_CAMCL.cc:57-193)
+// ------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(512) camcl_field_kernel(FieldArgs a)
+{
+    extern __shared__ double sm[];
+    Cell C;
+    load_cell(a, C);
+    Smem const S = carve(sm, C.L);
+    int const  t = C.t, Nx = a.Nx;
+
+    // 1-2. sources at x^N and x^{N+1}
+    S.rho0[t] = 0, S.rho1[t] = 0;
+    sst3(S.J0, t, { 0, 0, 0 });
+    sst3(S.J1, t, { 0, 0, 0 });
+    for (int s = 0; s < a.nk; ++s) {
+        KinSrc const &K = a.k[s];
+        for (int d = 0; d < 2; ++d) {
+            SV const r   = collect_kinetic(a, C, S, K, d);
+            double  *rho = d ? S.rho1 : S.rho0;
+            double  *J   = d ? S.J1 : S.J0;
+            sst3(J, t, sld3(J, t) + sld3(r.v, t));
+            rho[t] += r.a[t];
+        }
+    }
+    d3 cold_nV[MAXC];
+    for (int ci = 0; ci < a.nc; ++ci) {
+        ColdSrc const &K = a.c[ci];
+        cold_nV[ci]      = cold_push(a, C, K, a.E_in);
+        S.tr[t]          = (K.n[C.gm] * K.w) * K.cdcf;
+        sst3(S.tJ, t, (cold_nV[ci] * K.w) * K.ccf);
+        SV const r = smooth_n(C, K.nsm, S.tr, S.tJ, S.ts, S.tJs);
+        sst3(S.J0, t, sld3(S.J0, t) + sld3(r.v, t));
+        S.rho0[t] += r.a[t];
+        sst3(S.J1, t, sld3(S.J1, t) + sld3(r.v, t));
+        S.rho1[t] += r.a[t];
+    }
+    // 3. averages
+    double const rho_avg = (S.rho0[t] + S.rho1[t]) * .5;
+    d3 const     J_avg   = (sld3(S.J0, t) + sld3(S.J1, t)) * .5;
+    S.rho_avg[t]         = rho_avg;
+    sst3(S.Javg, t, J_avg);
+    S.Pe[t]  = Pe_of(a, rho_avg);
+    S.Pe1[t] = Pe_of(a, S.rho1[t]);
+    // B0 = B1 = B^N; covariant/contravariant components of B0
+    d3 const Bn = ld3(a.B_in, C.gm);
+    sst3(S.B0, t, Bn);
+    sst3(S.B1, t, Bn);
+    sst3(S.Bcov, t, covar_full(C, Bn));
+    sst3(S.Bcon, t, contr_full(C, Bn));
+    __syncthreads();
+    double const dPe  = dPe_at(a, C, S.Pe);
+    double const dPe1 = dPe_at(a, C, S.Pe1);
+    d3 const     jc   = contr_half(C, J_avg);
+
+    // 4. subcycle: X is updated, Y holds the newest B
+    double *X = S.B1, *Y = S.B0; // prologue: E from b0, then b1 = b1 + dt*curl E
+    for (int i = 0; i <= a.m; ++i) {
+        d3 const E = E_at(a, C, S.Bcov, S.Bcon, jc, dPe, rho_avg);
+        sst3(S.Ecov, t, covar_half(C, E));
+        __syncthreads();
+        double const dtp = (i == 0 || i == a.m) ? a.sub_dt : 2.0 * a.sub_dt;
+        if (i == 0) {
+            X = S.B1, Y = S.B0;
+        }
+        d3 const Bnew = B_at(a, C, S.Ecov, sld3(X, t), dtp);
+        sst3(X, t, Bnew);
+        sst3(S.Bcov, t, covar_full(C, Bnew));
+        sst3(S.Bcon, t, contr_full(C, Bnew));
+        __syncthreads();
+        double *tmp = X; // the older array is updated next
+        X           = Y;
+        Y           = tmp;
+    }
+    // after the loop Y is b0 (updated last) and X is b1; average into B
+    d3 const Bavg = (sld3(Y, t) + sld3(X, t)) * .5;
+    __syncthreads();
+    sst3(S.B0, t, Bavg);
+    sst3(S.Bcov, t, covar_full(C, Bavg));
+    sst3(S.Bcon, t, contr_full(C, Bavg));
+    __syncthreads();
+
+    // 5. E* from (B, rho^{N+1}, J^{N+1/2})
+    d3 const Es = E_at(a, C, S.Bcov, S.Bcon, jc, dPe1, S.rho1[t]);
+    sst3(S.E, t, Es);
+    __syncthreads();
+    // current advance (Domain_CAMCL.cc:131-151, Current.cc:181-188)
+    d3 const Bi = { C.hbx + (sld3(S.B0, min(t + 1, C.L - 1)).x + Bavg.x) * 0.5,
+                    0 * a.O0 + (sld3(S.B0, min(t + 1, C.L - 1)).y + Bavg.y) * 0.5,
+                    0 * a.O0 + (sld3(S.B0, min(t + 1, C.L - 1)).z + Bavg.z) * 0.5 };
+    for (int s = 0; s < a.nk + a.nc; ++s) {
+        double lam;
+        d3     gam;
+        int    nsm;
+        if (s < a.nk) {
+            KinSrc const &K = a.k[s];
+            lam             = fold(K.raw[1][0], C.gm, Nx, a.bc, K.s1, K.lamf);
+            gam             = { fold(K.raw[1][1], C.gm, Nx, a.bc, K.s1, K.gamf), fold(K.raw[1][2], C.gm, Nx, a.bc, K.s1, K.gamf),
+                    fold(K.raw[1][3], C.gm, Nx, a.bc, K.s1, K.gamf) };
+            nsm             = K.nsm;
+        } else {
+            ColdSrc const &K = a.c[s - a.nk];
+            lam              = (K.n[C.gm] * K.w) * K.lamf;
+            gam              = (cold_nV[s - a.nk] * K.w) * K.gamf;
+            nsm              = K.nsm;
+        }
+        d3 const Jadv = (Es * lam + cross(gam, Bi)) * (0.5 * a.dt);
+        S.t2[t]       = 0;
+        sst3(S.tJ, t, { 0 + Jadv.x, 0 + Jadv.y, 0 + Jadv.z });
+        SV const r = smooth_n(C, nsm, S.t2, S.tJ, S.ts, S.tJs);
+        sst3(S.J1, t, sld3(S.J1, t) + sld3(r.v, t));
+    }
+    // 6. E from (B, rho^{N+1}, J^+ advanced)
+    d3 const Ef = E_at(a, C, S.Bcov, S.Bcon, contr_half(C, sld3(S.J1, t)), dPe1, S.rho1[t]);
+    sst3(S.E, t, Ef);
+    __syncthreads();
+
+    if (C.owner) {
+        put3(a.B_out, C, Nx, Bavg);
+        put3(a.E_out, C, Nx, Ef);
+        put1(a.charge_out, C, Nx, rho_avg);
+        put3(a.current_out, C, Nx, J_avg);
+        d3 const Bh = (sld3(S.B0, min(t + 1, C.L - 1)) + Bavg) * 0.5;
+        st3(a.Bh_out, C.gm, Bh);
+        if (C.gm < PAD - 1)
+            st3(a.Bh_out, Nx + C.gm, Bh);
+        if (C.gm >= Nx - PAD)
+            st3(a.Bh_out, C.gm - Nx, Bh);
+        for (int ci = 0; ci < a.nc; ++ci)
+            st3(a.c[ci].nV_out, C.gm, cold_nV[ci]);
+        // clear the deposit set of the next cycle (interior + ghost images)
+        for (int s = 0; s < a.nk; ++s)
+            for (int d = 0; d < 2; ++d)
+                for (int q = 0; q < 4; ++q)
+                    put1(a.k[s].zero[d][q], C, Nx, 0.0);
+    }
+}
+
+#endif // H1D_FIELD_TU
+
+} // namespace h1d

@@ -1,0 +1,46 @@
+// Grid kernels of the hybrid_1d hot path.  This translation unit is compiled with
+// --fmad=false: the field cycle is latency-bound, and without contraction it evaluates the
+// reference's expressions operation for operation.
+#define H1D_FIELD_TU
+#include "launchers.h"
+#include "post.cuh"
+
+namespace h1d {
+
+cudaError_t set_field_smem(size_t bytes)
+{
+    return cudaFuncSetAttribute(camcl_field_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+}
+cudaError_t launch_camcl_fields(FieldArgs const &a, int blocks, int threads, size_t smem, cudaStream_t st)
+{
+    camcl_field_kernel<<<blocks, threads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_prep_fields(double *B, double *E, double *Bh, int Nx, cudaStream_t st)
+{
+    prep_fields_kernel<<<(Nx + 2 * PAD + 255) / 256, 256, 0, st>>>(B, E, Bh, Nx);
+    return cudaGetLastError();
+}
+cudaError_t launch_finalize_kinetic(double const *raw, double *out, int Nx, double s1, int reflecting, cudaStream_t st)
+{
+    finalize_kinetic_kernel<<<1, 256, 0, st>>>(raw, out, Nx, s1, reflecting);
+    return cudaGetLastError();
+}
+cudaError_t launch_finalize_cold(double const *n_full, double const *nV_full, double *out, int Nx, double w,
+                                 cudaStream_t st)
+{
+    finalize_cold_kernel<<<1, 256, 0, st>>>(n_full, nV_full, out, Nx, w);
+    return cudaGetLastError();
+}
+cudaError_t launch_energy(EnergyArgs const &a, cudaStream_t st)
+{
+    energy_kernel<<<1, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_iota(int32_t *pid, int64_t n, cudaStream_t st)
+{
+    iota_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(pid, n);
+    return cudaGetLastError();
+}
+
+} // namespace h1d

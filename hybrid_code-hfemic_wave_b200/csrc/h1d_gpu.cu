@@ -1,0 +1,899 @@
+// libh1d_gpu.so: host side and C-ABI of the B200 implementation of the hybrid_1d hot path.
+// The entry points are declared, with the reference interface each one replaces, in
+// include/h1d_gpu.h.
+#include "h1d_gpu.h"
+
+#include "device_common.cuh"
+#include "fields.cuh"
+#include "particles.cuh"
+#include "sort.cuh"
+#include "launchers.h"
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <tuple>
+#include <vector>
+
+using namespace h1d;
+
+namespace {
+
+constexpr int FIELD_BLOCK_MIN = 256;
+
+struct SpeciesState {
+    int64_t  n = 0, cap = 0;
+    double  *buf[2][5] = {}; // [parity][q1, vx, vy, vz, w]
+    int32_t *pid[2]    = {};
+    int      cur       = 0;
+    // sort scratch
+    uint32_t *keys[2] = {}, *idx[2] = {};
+    uint32_t *hist = nullptr, *part = nullptr;
+    int64_t   hist_cap = 0, part_cap = 0;
+    unsigned long long *dead = nullptr;
+    int       since_sort = 1 << 30;
+    // deposits [set][deposit][q] -> M doubles each, contiguous
+    double *dep = nullptr;
+    // collect_all raw sums: 10 x M
+    double *mom_raw = nullptr;
+    // finalized moments (GridArray layout): n (M), nV (3M), nvv (6M)
+    double *mom = nullptr;
+};
+
+struct ColdState {
+    double *n   = nullptr;  // M
+    double *nV[2] = {};     // 3M ping-pong
+    int     cur   = 0;
+    double *mom   = nullptr; // n (M), nV (3M), nvv (6M)
+};
+
+} // namespace
+
+struct h1d_run {
+    h1d_params   p;
+    int          device = 0;
+    cudaStream_t stream = nullptr;
+    long         Nx = 0, M = 0;
+    int          H = 0, seg = 0, L = 0, nblocks_field = 0;
+    size_t       field_smem = 0;
+    double      *geo = nullptr;
+    double      *B[2] = {}, *E[2] = {}, *Bh = nullptr, *charge = nullptr, *current = nullptr;
+    int          fcur = 0; // field parity
+    int          dset = 0; // deposit set parity
+    SpeciesState sp[H1D_MAX_KINETIC];
+    ColdState    cold[H1D_MAX_COLD];
+    unsigned    *d_status = nullptr;
+    unsigned    *h_status = nullptr; // pinned
+    double      *d_energy = nullptr;
+    bool         recurring = false, moments_stale = true, fields_dirty = true;
+    int64_t      step = 0;
+    int          sort_interval = 16;
+    std::string  msg;
+    // profiling: event pairs per phase (0 push, 1 sort, 2 field)
+    bool                                           profiling = false;
+    std::vector<std::pair<int, cudaEvent_t>>       ev_open;
+    std::vector<std::tuple<int, cudaEvent_t, cudaEvent_t>> ev_done;
+    std::vector<cudaEvent_t>                       ev_pool;
+    h1d_profile                                    prof{};
+};
+
+namespace {
+
+std::string fmt(char const *f, ...)
+{
+    char    b[512];
+    va_list ap;
+    va_start(ap, f);
+    std::vsnprintf(b, sizeof b, f, ap);
+    va_end(ap);
+    return b;
+}
+
+int set_err(h1d_run *r, int code, std::string const &m)
+{
+    if (r)
+        r->msg = m;
+    return code;
+}
+
+cudaEvent_t pool_event(h1d_run *r)
+{
+    if (!r->ev_pool.empty()) {
+        cudaEvent_t e = r->ev_pool.back();
+        r->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+void phase_begin(h1d_run *r, int kind)
+{
+    if (!r->profiling)
+        return;
+    cudaEvent_t e = pool_event(r);
+    cudaEventRecord(e, r->stream);
+    r->ev_open.emplace_back(kind, e);
+}
+void phase_end(h1d_run *r, int kernels)
+{
+    if (!r->profiling)
+        return;
+    cudaEvent_t e = pool_event(r);
+    cudaEventRecord(e, r->stream);
+    auto const [kind, b] = r->ev_open.back();
+    r->ev_open.pop_back();
+    r->ev_done.emplace_back(kind, b, e);
+    r->prof.kernel_launches += kernels;
+    if (kind == 0)
+        r->prof.push_launches += 1;
+    else if (kind == 1)
+        r->prof.sort_calls += 1;
+    else
+        r->prof.field_launches += 1;
+}
+
+#define CU(call)                                                                                             \
+    do {                                                                                                     \
+        cudaError_t const e_ = (call);                                                                       \
+        if (e_ != cudaSuccess)                                                                               \
+            return set_err(run, e_ == cudaErrorMemoryAllocation ? H1D_ERR_OOM : H1D_ERR_CUDA,                \
+                           fmt("%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__));        \
+    } while (0)
+
+int validate(h1d_params const *p, std::string &m)
+{
+#define BAD(...) return m = fmt(__VA_ARGS__), H1D_ERR_INVALID_ARG
+    if (!p)
+        BAD("null params");
+    if (p->Nx < 2 * PAD || p->Nx > 65535)
+        BAD("Nx must be in [%d, 65535]", 2 * PAD);
+    if (!(p->Dx > 0) || !(p->c > 0) || !(p->O0 > 0) || !(p->dt > 0) || !(p->xi >= 0))
+        BAD("Dx, c, O0 and dt must be positive and xi non-negative");
+    if (p->n_subcycles < 2 || p->n_subcycles > 256)
+        BAD("n_subcycles should be in [2, 256]");
+    if (p->algorithm != H1D_ALGO_PC && p->algorithm != H1D_ALGO_CAMCL)
+        BAD("unknown algorithm %d", p->algorithm);
+    if (p->particle_bc < 0 || p->particle_bc > 2)
+        BAD("unknown particle boundary condition %d", p->particle_bc);
+    if (p->precision != H1D_PREC_FP64 && p->precision != H1D_PREC_MIXED)
+        BAD("unknown precision %d", p->precision);
+    if (p->n_kinetic < 0 || p->n_kinetic > H1D_MAX_KINETIC || p->n_cold < 0 || p->n_cold > H1D_MAX_COLD)
+        BAD("too many species");
+    if (p->phase_retardation_inset < 0 || p->phase_retardation_inset > p->Nx / 2 || p->amplitude_damping_inset < 0
+        || p->amplitude_damping_inset > p->Nx / 2)
+        BAD("masking inset is greater than half the domain length");
+    if (!(p->phase_retardation_factor >= 0 && p->phase_retardation_factor <= 1)
+        || !(p->amplitude_damping_factor >= 0 && p->amplitude_damping_factor <= 1))
+        BAD("masking factor outside [0, 1]");
+    if (!(p->efluid.Oc < 0) || !(p->efluid.op > 0) || !(p->efluid.beta >= 0))
+        BAD("invalid electron fluid descriptor");
+    for (int s = 0; s < p->n_kinetic; ++s) {
+        h1d_kinetic_desc const &d = p->kinetic[s];
+        if (d.Oc == 0 || !(d.op > 0))
+            BAD("kinetic species %d: Oc should not be zero and op should be positive", s);
+        if (d.shape_order < 1 || d.shape_order > 3)
+            BAD("kinetic species %d: shape order must be 1, 2 or 3", s);
+        if (!(d.moment_norm > 0))
+            BAD("kinetic species %d: moment_norm must be positive", s);
+        if (d.n_smooth < 0 || d.n_smooth > 64)
+            BAD("kinetic species %d: smoothing count outside [0, 64]", s);
+    }
+    for (int s = 0; s < p->n_cold; ++s)
+        if (p->cold[s].Oc == 0 || !(p->cold[s].op > 0) || p->cold[s].n_smooth < 0 || p->cold[s].n_smooth > 64)
+            BAD("cold species %d: invalid descriptor", s);
+    if (p->xi > 0) { // ParamSet.cc:25-29
+        double const xd   = p->xi * p->Dx;
+        double const e[4] = { -0.5 * p->Nx, -0.5 * p->Nx + p->Nx, -0.5 * p->Nx + 0.5, -0.5 * p->Nx + 0.5 + p->Nx };
+        for (double q : e)
+            if (!(std::fabs(xd * q) < M_PI_2))
+                BAD("invalid domain extent: |xi*D1*q1| >= pi/2");
+    }
+    return H1D_OK;
+#undef BAD
+}
+
+double mask_fn(long inset, double factor, double offset)
+{
+    double const a = offset < 0 ? -offset : offset;
+    if (0 == inset || a > static_cast<double>(inset))
+        return 1;
+    double const tmp = factor * (1 - a / static_cast<double>(inset));
+    return (1 - tmp) * (1 + tmp);
+}
+
+// per-cell geometry, computed on the host with libm (CurviBasis.h:42, 52-69; MFABasis.h:262;
+// MaskingFunction.h:28-35 applied as in BField.cc:90-98)
+std::vector<double> geometry_table(h1d_params const &p)
+{
+    long const          N = p.Nx;
+    std::vector<double> g(static_cast<size_t>(G_COUNT) * N);
+    double const        D1 = p.Dx, D2 = 1, D3 = 1, iD1 = 1 / D1, iD2 = 1 / D2, iD3 = 1 / D3;
+    double const        full_min = -0.5 * N, half_min = full_min + 0.5;
+    for (long i = 0; i < N; ++i) {
+        double const cf = std::cos(p.xi * D1 * (static_cast<double>(i) + full_min));
+        double const ch = std::cos(p.xi * D1 * (static_cast<double>(i) + half_min));
+        g[G_FCOV_X * N + i] = D1 / (cf * cf), g[G_FCOV_Y * N + i] = D2 * cf, g[G_FCOV_Z * N + i] = D3 * cf;
+        g[G_FCON_X * N + i] = iD1 * (cf * cf), g[G_FCON_Y * N + i] = iD2 / cf, g[G_FCON_Z * N + i] = iD3 / cf;
+        g[G_HCOV_X * N + i] = D1 / (ch * ch), g[G_HCOV_Y * N + i] = D2 * ch, g[G_HCOV_Z * N + i] = D3 * ch;
+        g[G_HCON_X * N + i] = iD1 * (ch * ch), g[G_HCON_Y * N + i] = iD2 / ch, g[G_HCON_Z * N + i] = iD3 / ch;
+        double const ih     = 1 / ch;
+        g[G_HBX * N + i]    = (ih * ih) * p.O0;
+        long const   a = i < N - 1 - i ? i : N - 1 - i, b = i < N - 1 - i ? N - 1 - i : i;
+        g[G_MP1 * N + i] = mask_fn(p.phase_retardation_inset, p.phase_retardation_factor, 0.0 + a);
+        g[G_MP2 * N + i] = mask_fn(p.phase_retardation_inset, p.phase_retardation_factor, 0.0 + b);
+        g[G_MA1 * N + i] = mask_fn(p.amplitude_damping_inset, p.amplitude_damping_factor, 0.0 + a);
+        g[G_MA2 * N + i] = mask_fn(p.amplitude_damping_inset, p.amplitude_damping_factor, 0.0 + b);
+    }
+    return g;
+}
+
+double cdcf(h1d_params const &p, double Oc, double op) { return ((op * op) * p.O0) / Oc; }
+double ccf(h1d_params const &p, double Oc, double op) { return cdcf(p, Oc, op) / p.c; }
+
+template <class T>
+int dalloc(h1d_run *run, T **ptr, size_t count)
+{
+    CU(cudaMalloc(reinterpret_cast<void **>(ptr), sizeof(T) * (count ? count : 1)));
+    CU(cudaMemsetAsync(*ptr, 0, sizeof(T) * (count ? count : 1), run->stream));
+    return H1D_OK;
+}
+
+#define TRY(x)                                                                                               \
+    do {                                                                                                     \
+        int const st_ = (x);                                                                                 \
+        if (st_ != H1D_OK)                                                                                   \
+            return st_;                                                                                      \
+    } while (0)
+
+double *dep_ptr(h1d_run *run, int s, int set, int d, int q)
+{
+    return run->sp[s].dep + ((static_cast<size_t>(set) * 2 + d) * 4 + q) * run->M + PAD;
+}
+
+int ppt_for(h1d_run const *run, int s)
+{
+    double const ppc = static_cast<double>(run->sp[s].n) / static_cast<double>(run->Nx);
+    int          k   = static_cast<int>(ppc / 128);
+    return k < 1 ? 1 : k > 16 ? 16 : k;
+}
+
+PushArgs push_args(h1d_run *run, int s)
+{
+    h1d_params const       &p = run->p;
+    h1d_kinetic_desc const &d = p.kinetic[s];
+    SpeciesState           &S = run->sp[s];
+    PushArgs                a{};
+    a.q1 = S.buf[S.cur][0], a.vx = S.buf[S.cur][1], a.vy = S.buf[S.cur][2], a.vz = S.buf[S.cur][3];
+    a.w = S.buf[S.cur][4], a.pid = S.pid[S.cur];
+    a.n = S.n, a.ppt = ppt_for(run, s), a.Nx = static_cast<int>(run->Nx);
+    a.E = run->E[run->fcur] + 3 * PAD, a.Bh = run->Bh + 3 * PAD;
+    for (int dd = 0; dd < 2; ++dd)
+        for (int q = 0; q < 4; ++q)
+            a.dep[dd][q] = dep_ptr(run, s, run->dset, dd, q);
+    a.full_min = -0.5 * p.Nx, a.full_len = static_cast<double>(p.Nx), a.full_max = a.full_min + a.full_len;
+    a.half_min = a.full_min + 0.5;
+    a.xi = p.xi, a.xi2 = p.xi * p.xi, a.xiD1 = p.xi * p.Dx, a.D1 = p.Dx, a.inv_D1 = 1 / p.Dx, a.O0 = p.O0;
+    a.Oc = d.Oc, a.dt = p.dt, a.travel_scale = 1.0, a.boris = boris_make(p.dt, p.c, p.O0, d.Oc);
+    a.status = run->d_status, a.seed = p.gyrophase_seed, a.counter = static_cast<uint64_t>(run->step) * 8;
+    a.species = s, a.randomize = p.randomize_gyrophase, a.homogeneous_poly = p.xi < 1e-10;
+    a.move_steps = 1, a.deposit_mask = 3, a.write_back = 1;
+    return a;
+}
+
+template <int O, bool MIRROR>
+void launch_push_bc(PushArgs const &a, int bc, dim3 g, cudaStream_t st)
+{
+    if (bc == H1D_BC_PERIODIC)
+        push_kernel<O, MIRROR, BCK_PERIODIC><<<g, 256, 0, st>>>(a);
+    else if (bc == H1D_BC_REFLECTING)
+        push_kernel<O, MIRROR, BCK_REFLECTING><<<g, 256, 0, st>>>(a);
+    else
+        push_kernel<O, MIRROR, BCK_ABSORBING><<<g, 256, 0, st>>>(a);
+}
+template <int O>
+void launch_push_o(PushArgs const &a, bool mirror, int bc, dim3 g, cudaStream_t st)
+{
+    if (mirror)
+        launch_push_bc<O, true>(a, bc, g, st);
+    else
+        launch_push_bc<O, false>(a, bc, g, st);
+}
+int launch_push(h1d_run *run, int s, PushArgs const &a)
+{
+    if (a.n == 0)
+        return H1D_OK;
+    int64_t const chunks = (a.n + 32LL * a.ppt - 1) / (32LL * a.ppt);
+    dim3 const    g(static_cast<unsigned>((chunks + 7) / 8));
+    bool const    mirror = run->p.xi != 0;
+    switch (run->p.kinetic[s].shape_order) {
+    case 1: launch_push_o<1>(a, mirror, run->p.particle_bc, g, run->stream); break;
+    case 2: launch_push_o<2>(a, mirror, run->p.particle_bc, g, run->stream); break;
+    default: launch_push_o<3>(a, mirror, run->p.particle_bc, g, run->stream); break;
+    }
+    CU(cudaGetLastError());
+    return H1D_OK;
+}
+
+// stable cell sort of species s (sort.cuh)
+int sort_species(h1d_run *run, int s)
+{
+    SpeciesState &S = run->sp[s];
+    S.since_sort    = 0;
+    if (S.n == 0)
+        return H1D_OK;
+    cudaStream_t const st     = run->stream;
+    int const          Nx     = static_cast<int>(run->Nx);
+    int const          passes = Nx < 256 ? 1 : 2; // keys in [0, Nx] (Nx = absorbed)
+    int64_t const      ntiles = (S.n + SORT_TILE - 1) / SORT_TILE;
+    int64_t const      hlen   = 256 * ntiles;
+    int64_t const      nparts = (hlen + SCAN_SEG - 1) / SCAN_SEG;
+    if (hlen > S.hist_cap) {
+        cudaFree(S.hist);
+        S.hist = nullptr;
+        CU(cudaMalloc(&S.hist, sizeof(uint32_t) * hlen));
+        S.hist_cap = hlen;
+    }
+    if (nparts > S.part_cap) {
+        cudaFree(S.part);
+        S.part = nullptr;
+        CU(cudaMalloc(&S.part, sizeof(uint32_t) * nparts));
+        S.part_cap = nparts;
+    }
+    phase_begin(run, 1);
+    CU(cudaMemsetAsync(S.dead, 0, sizeof(unsigned long long), st));
+    unsigned const nb = static_cast<unsigned>((S.n + 255) / 256);
+    keys_kernel<<<nb, 256, 0, st>>>(S.buf[S.cur][0], S.buf[S.cur][4], S.n, -0.5 * Nx, Nx, S.keys[0], S.idx[0], S.dead,
+                                    run->d_status);
+    int src = 0;
+    for (int pass = 0; pass < passes; ++pass) {
+        int const shift = 8 * pass;
+        hist_kernel<<<static_cast<unsigned>(ntiles), SORT_THREADS, 0, st>>>(S.keys[src], S.n, shift,
+                                                                            static_cast<int>(ntiles), S.hist);
+        scan_reduce_kernel<<<static_cast<unsigned>(nparts), SCAN_THREADS, 0, st>>>(S.hist, hlen, S.part);
+        scan_partials_kernel<<<1, 1024, 0, st>>>(S.part, static_cast<int>(nparts));
+        scan_down_kernel<<<static_cast<unsigned>(nparts), SCAN_THREADS, 0, st>>>(S.hist, hlen, S.part);
+        scatter_kernel<<<static_cast<unsigned>(ntiles), SORT_THREADS, 0, st>>>(
+            S.keys[src], S.idx[src], pass == 0, S.n, shift, static_cast<int>(ntiles), S.hist, S.keys[1 - src],
+            S.idx[1 - src]);
+        src = 1 - src;
+    }
+    GatherArgs g{};
+    for (int k = 0; k < 5; ++k)
+        g.src[k] = S.buf[S.cur][k], g.dst[k] = S.buf[1 - S.cur][k];
+    g.pid_src = S.pid[S.cur], g.pid_dst = S.pid[1 - S.cur], g.idx = S.idx[src], g.n = S.n;
+    gather_kernel<<<nb, 256, 0, st>>>(g);
+    CU(cudaGetLastError());
+    phase_end(run, 2 + 5 * passes);
+    S.cur = 1 - S.cur;
+    if (run->p.particle_bc == H1D_BC_ABSORBING) { // trim removed particles (sorted to the end)
+        unsigned long long dead = 0;
+        CU(cudaMemcpyAsync(&dead, S.dead, sizeof dead, cudaMemcpyDeviceToHost, st));
+        CU(cudaStreamSynchronize(st));
+        S.n -= static_cast<int64_t>(dead);
+    }
+    return H1D_OK;
+}
+
+FieldArgs field_args(h1d_run *run)
+{
+    h1d_params const &p = run->p;
+    FieldArgs         a{};
+    a.Nx = static_cast<int>(run->Nx), a.H = run->H, a.seg = run->seg, a.bc = p.particle_bc == H1D_BC_PERIODIC ? 0 : 1;
+    a.geo = run->geo;
+    a.B_in = run->B[run->fcur] + 3 * PAD, a.E_in = run->E[run->fcur] + 3 * PAD;
+    a.B_out = run->B[1 - run->fcur] + 3 * PAD, a.E_out = run->E[1 - run->fcur] + 3 * PAD;
+    a.Bh_out = run->Bh + 3 * PAD, a.charge_out = run->charge + PAD, a.current_out = run->current + 3 * PAD;
+    a.nk = p.n_kinetic, a.nc = p.n_cold;
+    for (int s = 0; s < p.n_kinetic; ++s) {
+        h1d_kinetic_desc const &d = p.kinetic[s];
+        KinSrc                 &K = a.k[s];
+        for (int dd = 0; dd < 2; ++dd)
+            for (int q = 0; q < 4; ++q) {
+                K.raw[dd][q]  = dep_ptr(run, s, run->dset, dd, q);
+                K.zero[dd][q] = dep_ptr(run, s, 1 - run->dset, dd, q);
+            }
+        K.s1 = 1.0 / d.moment_norm, K.cdcf = cdcf(p, d.Oc, d.op), K.ccf = ccf(p, d.Oc, d.op);
+        K.lamf = K.cdcf * d.Oc / p.O0, K.gamf = K.ccf * d.Oc / p.O0, K.nsm = static_cast<int>(d.n_smooth);
+    }
+    for (int c = 0; c < p.n_cold; ++c) {
+        h1d_cold_desc const &d = p.cold[c];
+        ColdSrc             &K = a.c[c];
+        ColdState           &C = run->cold[c];
+        K.n = C.n + PAD, K.nV_in = C.nV[C.cur] + 3 * PAD, K.nV_out = C.nV[1 - C.cur] + 3 * PAD;
+        K.boris = boris_make(p.dt, p.c, p.O0, d.Oc);
+        K.cdcf = cdcf(p, d.Oc, d.op), K.ccf = ccf(p, d.Oc, d.op), K.lamf = K.cdcf * d.Oc / p.O0, K.gamf = K.ccf * d.Oc / p.O0;
+        K.w = p.moment_weighting, K.nsm = static_cast<int>(d.n_smooth);
+    }
+    a.dt = p.dt, a.sub_dt = p.dt / p.n_subcycles, a.c_light = p.c, a.sqrt_g = p.Dx * 1 * 1, a.O0 = p.O0, a.inv_D1 = 1 / p.Dx;
+    a.m = static_cast<int>(p.n_subcycles);
+    h1d_efluid_desc const &ef = p.efluid;
+    a.O02beO2 = (p.O0 * p.O0) * ef.beta * 0.5, a.mOeOO0oe2 = -ef.Oc / (p.O0 * (ef.op * ef.op)), a.gamma = ef.gamma;
+    a.cO2 = p.c / 2, a.cOsqrtg = p.c / a.sqrt_g;
+    return a;
+}
+
+// first advance: fill ghost cells of E and B (Domain_CAMCL.cc:27-35) and B on the half grid
+int prepare_fields(h1d_run *run)
+{
+    CU(launch_prep_fields(run->B[run->fcur] + 3 * PAD, run->E[run->fcur] + 3 * PAD, run->Bh + 3 * PAD,
+                          static_cast<int>(run->Nx), run->stream));
+    run->fields_dirty = false;
+    return H1D_OK;
+}
+
+int camcl_step(h1d_run *run)
+{
+    h1d_params const &p = run->p;
+    for (int s = 0; s < p.n_kinetic; ++s) {
+        if (run->sp[s].since_sort >= run->sort_interval)
+            TRY(sort_species(run, s));
+        phase_begin(run, 0);
+        TRY(launch_push(run, s, push_args(run, s)));
+        phase_end(run, run->sp[s].n > 0 ? 1 : 0);
+        if (run->profiling)
+            run->prof.particles_pushed += run->sp[s].n;
+        run->sp[s].since_sort++;
+    }
+    FieldArgs const a = field_args(run);
+    phase_begin(run, 2);
+    CU(launch_camcl_fields(a, run->nblocks_field, run->L, run->field_smem, run->stream));
+    phase_end(run, 1);
+    run->fcur = 1 - run->fcur;
+    run->dset = 1 - run->dset;
+    for (int c = 0; c < p.n_cold; ++c)
+        run->cold[c].cur = 1 - run->cold[c].cur;
+    run->step++;
+    return H1D_OK;
+}
+
+int check_status(h1d_run *run)
+{
+    CU(cudaStreamSynchronize(run->stream));
+    CU(cudaMemcpy(run->h_status, run->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    unsigned const s = *run->h_status;
+    if (s & ST_MOVED_TOO_FAR)
+        return set_err(run, H1D_ERR_MOVED_TOO_FAR, "PartSpecies::update_pos - particle(s) moved too far");
+    if (s & ST_OUT_OF_RANGE)
+        return set_err(run, H1D_ERR_NAN, "particle(s) outside the padded grid (non-finite or lost particle state)");
+    if (s)
+        return set_err(run, H1D_ERR_CUDA, fmt("device status 0x%x", s));
+    return H1D_OK;
+}
+
+// post-process of advance_by: collect_all + boundary_gather (Domain_CAMCL.cc:45-55), on demand
+int finalize_moments(h1d_run *run)
+{
+    if (!run->moments_stale)
+        return H1D_OK;
+    h1d_params const &p = run->p;
+    for (int s = 0; s < p.n_kinetic; ++s) {
+        SpeciesState &S = run->sp[s];
+        CU(cudaMemsetAsync(S.mom_raw, 0, sizeof(double) * 10 * run->M, run->stream));
+        if (S.n > 0) {
+            MomentArgs a{};
+            a.q1 = S.buf[S.cur][0], a.vx = S.buf[S.cur][1], a.vy = S.buf[S.cur][2], a.vz = S.buf[S.cur][3];
+            a.w = S.buf[S.cur][4], a.n = S.n, a.ppt = ppt_for(run, s), a.Nx = static_cast<int>(run->Nx);
+            a.half_min = -0.5 * p.Nx + 0.5, a.status = run->d_status;
+            for (int q = 0; q < 10; ++q)
+                a.out[q] = S.mom_raw + static_cast<size_t>(q) * run->M + PAD;
+            int64_t const chunks = (S.n + 32LL * a.ppt - 1) / (32LL * a.ppt);
+            moments_kernel<<<static_cast<unsigned>((chunks + 7) / 8), 256, 0, run->stream>>>(a);
+        }
+        CU(launch_finalize_kinetic(S.mom_raw, S.mom, static_cast<int>(run->Nx), 1.0 / p.kinetic[s].moment_norm,
+                                   p.particle_bc == H1D_BC_PERIODIC ? 0 : 1, run->stream));
+    }
+    for (int c = 0; c < p.n_cold; ++c) {
+        ColdState &C = run->cold[c];
+        CU(launch_finalize_cold(C.n, C.nV[C.cur], C.mom, static_cast<int>(run->Nx), p.moment_weighting,
+                                run->stream));
+    }
+    CU(cudaGetLastError());
+    run->moments_stale = false;
+    return H1D_OK;
+}
+
+} // namespace
+
+// ------------------------------------------------------------------------------------------------
+// C-ABI
+// ------------------------------------------------------------------------------------------------
+extern "C" {
+
+int    h1d_abi_version(void) { return H1D_ABI_VERSION; }
+size_t h1d_params_size(void) { return sizeof(h1d_params); }
+
+char const *h1d_error_name(int status)
+{
+    switch (status) {
+    case H1D_OK: return "ok";
+    case H1D_ERR_INVALID_ARG: return "invalid argument";
+    case H1D_ERR_MOVED_TOO_FAR: return "particle(s) moved too far";
+    case H1D_ERR_OOM: return "out of device memory";
+    case H1D_ERR_CUDA: return "CUDA error";
+    case H1D_ERR_TIMEOUT: return "timeout";
+    case H1D_ERR_NAN: return "non-finite state";
+    case H1D_ERR_STATE: return "call out of order";
+    case H1D_ERR_NO_DEVICE: return "no CUDA device";
+    default: return "unknown";
+    }
+}
+
+char const *h1d_status_string(h1d_run *run) { return run ? run->msg.c_str() : "null run"; }
+
+int h1d_create(h1d_params const *params, h1d_run **out)
+{
+    if (!out)
+        return H1D_ERR_INVALID_ARG;
+    *out = nullptr;
+    std::string m;
+    if (int const st = validate(params, m)) {
+        std::fprintf(stderr, "h1d_create: %s\n", m.c_str());
+        return st;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return H1D_ERR_NO_DEVICE;
+    h1d_run *run = new (std::nothrow) h1d_run{};
+    if (!run)
+        return H1D_ERR_OOM;
+    run->p = *params;
+    if (!(run->p.moment_weighting > 0))
+        run->p.moment_weighting = 1;
+    h1d_params const &p = run->p;
+    auto const        fail = [&](int st) {
+        h1d_destroy(run);
+        return st;
+    };
+    if (cudaGetDevice(&run->device) != cudaSuccess || cudaStreamCreateWithFlags(&run->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(H1D_ERR_CUDA);
+    run->Nx            = p.Nx;
+    run->M             = p.Nx + 2 * PAD;
+    run->sort_interval = p.sort_interval > 0 ? p.sort_interval : 16;
+    // halo of the field kernel: reach of one cycle (2 x smoothing + subcycle + E*, advance, E, Bh)
+    int rs = 0;
+    for (int s = 0; s < p.n_kinetic; ++s)
+        rs = std::max(rs, static_cast<int>(p.kinetic[s].n_smooth));
+    for (int c = 0; c < p.n_cold; ++c)
+        rs = std::max(rs, static_cast<int>(p.cold[c].n_smooth));
+    run->H   = 2 * rs + static_cast<int>(p.n_subcycles) + 6;
+    int L    = FIELD_BLOCK_MIN;
+    while (L - 2 * run->H < 64 && L < 512)
+        L += 64;
+    if (L - 2 * run->H < 32)
+        return fail(set_err(run, H1D_ERR_INVALID_ARG, "n_subcycles / smoothing counts too large for one field block"));
+    run->L             = L;
+    run->seg           = static_cast<int>(std::min<long>(L - 2 * run->H, run->Nx));
+    run->nblocks_field = static_cast<int>((run->Nx + run->seg - 1) / run->seg);
+    run->field_smem    = sizeof(double) * static_cast<size_t>(L) * (SMEM_SCALARS + 3 * SMEM_VECTORS);
+    if (set_field_smem(run->field_smem) != cudaSuccess)
+        return fail(H1D_ERR_CUDA);
+
+    long const M = run->M;
+    if (dalloc(run, &run->geo, G_COUNT * run->Nx) || dalloc(run, &run->B[0], 3 * M) || dalloc(run, &run->B[1], 3 * M)
+        || dalloc(run, &run->E[0], 3 * M) || dalloc(run, &run->E[1], 3 * M) || dalloc(run, &run->Bh, 3 * M)
+        || dalloc(run, &run->charge, M) || dalloc(run, &run->current, 3 * M) || dalloc(run, &run->d_status, 1)
+        || dalloc(run, &run->d_energy, 6 + 6 * (H1D_MAX_KINETIC + H1D_MAX_COLD)))
+        return fail(H1D_ERR_OOM);
+    if (cudaMallocHost(&run->h_status, sizeof(unsigned)) != cudaSuccess)
+        return fail(H1D_ERR_OOM);
+    for (int s = 0; s < p.n_kinetic; ++s) {
+        SpeciesState &S = run->sp[s];
+        if (dalloc(run, &S.dep, 16 * M) || dalloc(run, &S.mom_raw, 10 * M) || dalloc(run, &S.mom, 10 * M)
+            || dalloc(run, &S.dead, 1))
+            return fail(H1D_ERR_OOM);
+    }
+    for (int c = 0; c < p.n_cold; ++c) {
+        ColdState &C = run->cold[c];
+        if (dalloc(run, &C.n, M) || dalloc(run, &C.nV[0], 3 * M) || dalloc(run, &C.nV[1], 3 * M) || dalloc(run, &C.mom, 10 * M))
+            return fail(H1D_ERR_OOM);
+    }
+    std::vector<double> const g = geometry_table(p);
+    if (cudaMemcpyAsync(run->geo, g.data(), sizeof(double) * g.size(), cudaMemcpyHostToDevice, run->stream) != cudaSuccess
+        || cudaStreamSynchronize(run->stream) != cudaSuccess)
+        return fail(H1D_ERR_CUDA);
+    // B on the half grid keeps NaN in its last ghost cell (PartSpecies.cc:137)
+    double const nan3[3] = { NAN, NAN, NAN };
+    if (cudaMemcpy(run->Bh + 3 * (M - 1), nan3, sizeof nan3, cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(H1D_ERR_CUDA);
+    *out = run;
+    return H1D_OK;
+}
+
+int h1d_destroy(h1d_run *run)
+{
+    if (!run)
+        return H1D_OK;
+    if (run->stream)
+        cudaStreamSynchronize(run->stream);
+    cudaFree(run->geo);
+    for (int k = 0; k < 2; ++k)
+        cudaFree(run->B[k]), cudaFree(run->E[k]);
+    cudaFree(run->Bh), cudaFree(run->charge), cudaFree(run->current), cudaFree(run->d_status), cudaFree(run->d_energy);
+    if (run->h_status)
+        cudaFreeHost(run->h_status);
+    for (auto &S : run->sp) {
+        for (int k = 0; k < 2; ++k) {
+            for (auto *b : S.buf[k])
+                cudaFree(b);
+            cudaFree(S.pid[k]), cudaFree(S.keys[k]), cudaFree(S.idx[k]);
+        }
+        cudaFree(S.hist), cudaFree(S.part), cudaFree(S.dead), cudaFree(S.dep), cudaFree(S.mom_raw), cudaFree(S.mom);
+    }
+    for (auto &C : run->cold)
+        cudaFree(C.n), cudaFree(C.nV[0]), cudaFree(C.nV[1]), cudaFree(C.mom);
+    for (auto &[k, b, e] : run->ev_done)
+        cudaEventDestroy(b), cudaEventDestroy(e);
+    for (auto e : run->ev_pool)
+        cudaEventDestroy(e);
+    if (run->stream)
+        cudaStreamDestroy(run->stream);
+    delete run;
+    return H1D_OK;
+}
+
+int h1d_upload_particles(h1d_run *run, int s, int64_t n, double const *q1, double const *vx, double const *vy,
+                         double const *vz, double const *w)
+{
+    if (!run || s < 0 || s >= run->p.n_kinetic || n < 0 || n > (int64_t{ 1 } << 31) - 1
+        || (n > 0 && (!q1 || !vx || !vy || !vz || !w)))
+        return set_err(run, H1D_ERR_INVALID_ARG, "h1d_upload_particles: bad arguments");
+    SpeciesState &S = run->sp[s];
+    CU(cudaStreamSynchronize(run->stream));
+    if (n > S.cap) {
+        int64_t const cap = n + 64;
+        for (int k = 0; k < 2; ++k) {
+            for (auto *&b : S.buf[k]) {
+                cudaFree(b);
+                b = nullptr;
+                CU(cudaMalloc(&b, sizeof(double) * cap));
+            }
+            cudaFree(S.pid[k]), cudaFree(S.keys[k]), cudaFree(S.idx[k]);
+            S.pid[k] = nullptr, S.keys[k] = nullptr, S.idx[k] = nullptr;
+            CU(cudaMalloc(&S.pid[k], sizeof(int32_t) * cap));
+            CU(cudaMalloc(&S.keys[k], sizeof(uint32_t) * cap));
+            CU(cudaMalloc(&S.idx[k], sizeof(uint32_t) * cap));
+        }
+        S.cap = cap;
+    }
+    S.cur              = 0;
+    S.n                = n;
+    double const *src[5] = { q1, vx, vy, vz, w };
+    for (int k = 0; k < 5; ++k)
+        if (n)
+            CU(cudaMemcpyAsync(S.buf[0][k], src[k], sizeof(double) * n, cudaMemcpyHostToDevice, run->stream));
+    if (n)
+        CU(launch_iota(S.pid[0], n, run->stream));
+    S.since_sort       = 1 << 30;
+    run->moments_stale = true;
+    CU(cudaStreamSynchronize(run->stream));
+    return H1D_OK;
+}
+
+int h1d_upload_fields(h1d_run *run, double const *B, double const *E)
+{
+    if (!run)
+        return H1D_ERR_INVALID_ARG;
+    size_t const bytes = sizeof(double) * 3 * run->M;
+    if (B)
+        CU(cudaMemcpyAsync(run->B[run->fcur], B, bytes, cudaMemcpyHostToDevice, run->stream));
+    if (E)
+        CU(cudaMemcpyAsync(run->E[run->fcur], E, bytes, cudaMemcpyHostToDevice, run->stream));
+    CU(cudaStreamSynchronize(run->stream));
+    run->fields_dirty = true;
+    return H1D_OK;
+}
+
+int h1d_upload_cold(h1d_run *run, int i, double const *n_full, double const *nV_full)
+{
+    if (!run || i < 0 || i >= run->p.n_cold || !n_full || !nV_full)
+        return set_err(run, H1D_ERR_INVALID_ARG, "h1d_upload_cold: bad arguments");
+    ColdState &C = run->cold[i];
+    CU(cudaMemcpyAsync(C.n, n_full, sizeof(double) * run->M, cudaMemcpyHostToDevice, run->stream));
+    CU(cudaMemcpyAsync(C.nV[C.cur], nV_full, sizeof(double) * 3 * run->M, cudaMemcpyHostToDevice, run->stream));
+    CU(cudaMemcpyAsync(C.nV[1 - C.cur], nV_full, sizeof(double) * 3 * run->M, cudaMemcpyHostToDevice, run->stream));
+    CU(cudaStreamSynchronize(run->stream));
+    run->moments_stale = true;
+    return H1D_OK;
+}
+
+int h1d_advance_async(h1d_run *run, uint32_t n_steps)
+{
+    if (!run)
+        return H1D_ERR_INVALID_ARG;
+    if (run->p.algorithm != H1D_ALGO_CAMCL)
+        return set_err(run, H1D_ERR_INVALID_ARG, "predictor-corrector is not available in this build");
+    if (!run->recurring || run->fields_dirty) {
+        TRY(prepare_fields(run));
+        run->recurring = true;
+    }
+    for (uint32_t i = 0; i < n_steps; ++i)
+        TRY(camcl_step(run));
+    run->moments_stale = true;
+    return H1D_OK;
+}
+
+int h1d_synchronize(h1d_run *run)
+{
+    if (!run)
+        return H1D_ERR_INVALID_ARG;
+    return check_status(run);
+}
+
+int h1d_advance(h1d_run *run, uint32_t n_steps)
+{
+    TRY(h1d_advance_async(run, n_steps));
+    return h1d_synchronize(run);
+}
+
+int h1d_get_stream(h1d_run *run, void **stream)
+{
+    if (!run || !stream)
+        return H1D_ERR_INVALID_ARG;
+    *stream = run->stream;
+    return H1D_OK;
+}
+
+int h1d_profile_enable(h1d_run *run, int on)
+{
+    if (!run)
+        return H1D_ERR_INVALID_ARG;
+    CU(cudaStreamSynchronize(run->stream));
+    for (auto &[k, b, e] : run->ev_done)
+        run->ev_pool.push_back(b), run->ev_pool.push_back(e);
+    run->ev_done.clear();
+    if (on)
+        run->prof = h1d_profile{};
+    run->profiling = on != 0;
+    return H1D_OK;
+}
+
+int h1d_profile_read(h1d_run *run, h1d_profile *out)
+{
+    if (!run || !out)
+        return H1D_ERR_INVALID_ARG;
+    CU(cudaStreamSynchronize(run->stream));
+    for (auto &[k, b, e] : run->ev_done) {
+        float ms = 0;
+        CU(cudaEventElapsedTime(&ms, b, e));
+        (k == 0 ? run->prof.push_ms : k == 1 ? run->prof.sort_ms : run->prof.field_ms) += ms;
+        run->ev_pool.push_back(b), run->ev_pool.push_back(e);
+    }
+    run->ev_done.clear();
+    *out = run->prof;
+    return H1D_OK;
+}
+
+int h1d_particle_count(h1d_run *run, int s, int64_t *n)
+{
+    if (!run || s < 0 || s >= run->p.n_kinetic || !n)
+        return H1D_ERR_INVALID_ARG;
+    *n = run->sp[s].n;
+    return H1D_OK;
+}
+
+int h1d_download_particles(h1d_run *run, int s, double *q1, double *vx, double *vy, double *vz, double *w, int64_t *pid)
+{
+    if (!run || s < 0 || s >= run->p.n_kinetic)
+        return H1D_ERR_INVALID_ARG;
+    SpeciesState &S = run->sp[s];
+    if (run->p.particle_bc == H1D_BC_ABSORBING && S.n > 0)
+        TRY(sort_species(run, s)); // drop absorbed particles
+    double *dst[5] = { q1, vx, vy, vz, w };
+    for (int k = 0; k < 5; ++k)
+        if (dst[k] && S.n)
+            CU(cudaMemcpyAsync(dst[k], S.buf[S.cur][k], sizeof(double) * S.n, cudaMemcpyDeviceToHost, run->stream));
+    if (pid && S.n) {
+        std::vector<int32_t> tmp(S.n);
+        CU(cudaMemcpyAsync(tmp.data(), S.pid[S.cur], sizeof(int32_t) * S.n, cudaMemcpyDeviceToHost, run->stream));
+        CU(cudaStreamSynchronize(run->stream));
+        for (int64_t k = 0; k < S.n; ++k)
+            pid[k] = tmp[k];
+    }
+    CU(cudaStreamSynchronize(run->stream));
+    return H1D_OK;
+}
+
+int h1d_download_fields(h1d_run *run, double *B, double *E)
+{
+    if (!run)
+        return H1D_ERR_INVALID_ARG;
+    if (run->fields_dirty)
+        TRY(prepare_fields(run));
+    size_t const bytes = sizeof(double) * 3 * run->M;
+    if (B)
+        CU(cudaMemcpyAsync(B, run->B[run->fcur], bytes, cudaMemcpyDeviceToHost, run->stream));
+    if (E)
+        CU(cudaMemcpyAsync(E, run->E[run->fcur], bytes, cudaMemcpyDeviceToHost, run->stream));
+    CU(cudaStreamSynchronize(run->stream));
+    return H1D_OK;
+}
+
+int h1d_download_sources(h1d_run *run, double *charge, double *current)
+{
+    if (!run)
+        return H1D_ERR_INVALID_ARG;
+    if (charge)
+        CU(cudaMemcpyAsync(charge, run->charge, sizeof(double) * run->M, cudaMemcpyDeviceToHost, run->stream));
+    if (current)
+        CU(cudaMemcpyAsync(current, run->current, sizeof(double) * 3 * run->M, cudaMemcpyDeviceToHost, run->stream));
+    CU(cudaStreamSynchronize(run->stream));
+    return H1D_OK;
+}
+
+int h1d_download_moments(h1d_run *run, int s, double *n, double *nV, double *nvv)
+{
+    if (!run || s < 0 || s >= run->p.n_kinetic)
+        return H1D_ERR_INVALID_ARG;
+    TRY(finalize_moments(run));
+    double const *m = run->sp[s].mom;
+    if (n)
+        CU(cudaMemcpyAsync(n, m, sizeof(double) * run->M, cudaMemcpyDeviceToHost, run->stream));
+    if (nV)
+        CU(cudaMemcpyAsync(nV, m + run->M, sizeof(double) * 3 * run->M, cudaMemcpyDeviceToHost, run->stream));
+    if (nvv)
+        CU(cudaMemcpyAsync(nvv, m + 4 * run->M, sizeof(double) * 6 * run->M, cudaMemcpyDeviceToHost, run->stream));
+    CU(cudaStreamSynchronize(run->stream));
+    return H1D_OK;
+}
+
+int h1d_download_cold(h1d_run *run, int i, double *n, double *nV, double *nvv, double *n_full, double *nV_full)
+{
+    if (!run || i < 0 || i >= run->p.n_cold)
+        return H1D_ERR_INVALID_ARG;
+    TRY(finalize_moments(run));
+    ColdState const &C = run->cold[i];
+    long const       M = run->M;
+    if (n)
+        CU(cudaMemcpyAsync(n, C.mom, sizeof(double) * M, cudaMemcpyDeviceToHost, run->stream));
+    if (nV)
+        CU(cudaMemcpyAsync(nV, C.mom + M, sizeof(double) * 3 * M, cudaMemcpyDeviceToHost, run->stream));
+    if (nvv)
+        CU(cudaMemcpyAsync(nvv, C.mom + 4 * M, sizeof(double) * 6 * M, cudaMemcpyDeviceToHost, run->stream));
+    if (n_full)
+        CU(cudaMemcpyAsync(n_full, C.n, sizeof(double) * M, cudaMemcpyDeviceToHost, run->stream));
+    if (nV_full)
+        CU(cudaMemcpyAsync(nV_full, C.nV[C.cur], sizeof(double) * 3 * M, cudaMemcpyDeviceToHost, run->stream));
+    CU(cudaStreamSynchronize(run->stream));
+    return H1D_OK;
+}
+
+int h1d_energy(h1d_run *run, double *dB2O2, double *dE2O2, double *KE_lab, double *KE_pla)
+{
+    if (!run || !dB2O2 || !dE2O2 || !KE_lab || !KE_pla)
+        return H1D_ERR_INVALID_ARG;
+    TRY(finalize_moments(run));
+    h1d_params const &p  = run->p;
+    int const         ns = p.n_kinetic + p.n_cold;
+    EnergyArgs        a{};
+    a.B = run->B[run->fcur] + 3 * PAD, a.E = run->E[run->fcur] + 3 * PAD, a.Nx = static_cast<int>(run->Nx);
+    a.ns = ns, a.out = run->d_energy;
+    for (int s = 0; s < ns; ++s) {
+        double Oc, op;
+        double const *m;
+        if (s < p.n_kinetic)
+            Oc = p.kinetic[s].Oc, op = p.kinetic[s].op, m = run->sp[s].mom;
+        else
+            Oc = p.cold[s - p.n_kinetic].Oc, op = p.cold[s - p.n_kinetic].op, m = run->cold[s - p.n_kinetic].mom;
+        double const tmp = p.O0 / Oc * op / p.c; // Species.h:50-54
+        a.n[s]          = m + PAD;
+        a.nV[s]         = m + run->M + 3 * PAD;
+        a.nvv[s]        = m + 4 * run->M + 6 * PAD;
+        a.factor[s]     = tmp * tmp / (2 * static_cast<double>(p.Nx));
+    }
+    CU(launch_energy(a, run->stream));
+    std::vector<double> h(6 + 6 * ns);
+    CU(cudaMemcpyAsync(h.data(), run->d_energy, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, run->stream));
+    CU(cudaStreamSynchronize(run->stream));
+    for (int c = 0; c < 3; ++c)
+        dB2O2[c] = h[c], dE2O2[c] = h[3 + c];
+    for (int s = 0; s < ns; ++s)
+        for (int c = 0; c < 3; ++c)
+            KE_lab[3 * s + c] = h[6 + 6 * s + c], KE_pla[3 * s + c] = h[6 + 6 * s + 3 + c];
+    return H1D_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,28 @@
+// Host-side launchers of the grid kernels, which live in their own translation unit
+// (fields_kernels.cu) because that unit is compiled without FMA contraction.
+#pragma once
+
+#include "fields.cuh"
+
+#include <cuda_runtime.h>
+
+namespace h1d {
+
+struct EnergyArgs {
+    double const *B, *E; // cell 0
+    int           Nx, ns;
+    double const *n[MAXK + MAXC], *nV[MAXK + MAXC], *nvv[MAXK + MAXC];
+    double        factor[MAXK + MAXC];
+    double       *out; // 6 + 6 * ns
+};
+
+cudaError_t set_field_smem(size_t bytes);
+cudaError_t launch_camcl_fields(FieldArgs const &a, int blocks, int threads, size_t smem, cudaStream_t st);
+cudaError_t launch_prep_fields(double *B, double *E, double *Bh, int Nx, cudaStream_t st);
+cudaError_t launch_finalize_kinetic(double const *raw, double *out, int Nx, double s1, int reflecting, cudaStream_t st);
+cudaError_t launch_finalize_cold(double const *n_full, double const *nV_full, double *out, int Nx, double w,
+                                 cudaStream_t st);
+cudaError_t launch_energy(EnergyArgs const &a, cudaStream_t st);
+cudaError_t launch_iota(int32_t *pid, int64_t n, cudaStream_t st);
+
+} // namespace h1d

@@ -1,0 +1,161 @@
+// Small grid kernels: ghost fill on the first advance, the post-process of advance_by
+// (collect_all scaling and boundary_gather, ColdSpecies::collect_all) and the energy reductions
+// of EnergyRecorder::dump.
+#pragma once
+
+#include "device_common.cuh"
+#include "launchers.h"
+
+namespace h1d {
+
+__global__ void iota_kernel(int32_t *pid, int64_t n)
+{
+    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n)
+        pid[i] = static_cast<int32_t>(i);
+}
+
+__device__ __forceinline__ int wrap(int i, int Nx) { return i < 0 ? i + Nx : i >= Nx ? i - Nx : i; }
+
+// boundary_pass of E and B (periodic ghost fill, Delegate.cc:159-170) and B on the half grid
+// (PartSpecies.cc:132-139; its last ghost stays NaN)
+__global__ void prep_fields_kernel(double *B, double *E, double *Bh, int Nx)
+{
+    int const i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x) - PAD;
+    if (i >= Nx + PAD)
+        return;
+    if (i < Nx + PAD - 1) {
+        d3 const b1 = ld3(B, wrap(i + 1, Nx)), b0 = ld3(B, wrap(i, Nx));
+        st3(Bh, i, (b1 + b0) * 0.5);
+    }
+    if (i < 0 || i >= Nx) {
+        st3(B, i, ld3(B, wrap(i, Nx)));
+        st3(E, i, ld3(E, wrap(i, Nx)));
+    }
+}
+
+// collect_all scaling by 1/Nc (PartSpecies.cc:346-348) and boundary_gather of the three moments
+// (SubdomainDelegate.cc:115-181).  raw: 10 arrays of M (n, nV xyz, nvv xx yy zz xy yz zx);
+// out: GridArray layout n[M], nV[3M], nvv[6M].
+__global__ void finalize_kinetic_kernel(double const *raw, double *out, int Nx, double s1, int reflecting)
+{
+    int const M = Nx + 2 * PAD;
+    double   *n = out, *nV = out + M, *nvv = out + 4 * M;
+    for (int i = threadIdx.x; i < M; i += blockDim.x) {
+        n[i] = raw[i] * s1;
+        for (int c = 0; c < 3; ++c)
+            nV[3 * i + c] = raw[(1 + c) * M + i] * s1;
+        for (int c = 0; c < 6; ++c)
+            nvv[6 * i + c] = raw[(4 + c) * M + i] * s1;
+    }
+    __syncthreads();
+    if (threadIdx.x != 0)
+        return;
+    struct G {
+        double *a;
+        int     nc;
+    } const grids[3] = { { n, 1 }, { nV, 3 }, { nvv, 6 } };
+    for (G const &g : grids) {
+        double *a = g.a;
+        int const nc = g.nc;
+        if (reflecting) {
+            for (int i = 0; i < PAD; ++i) // cells -3 -> -2 -> -1 -> 0
+                for (int c = 0; c < nc; ++c) {
+                    a[nc * (i + 1) + c] += a[nc * i + c];
+                    a[nc * i + c] = 0;
+                }
+            for (int i = M - 1; i >= Nx + PAD; --i)
+                for (int c = 0; c < nc; ++c) {
+                    a[nc * (i - 1) + c] += a[nc * i + c];
+                    a[nc * i + c] = 0;
+                }
+        }
+        double left[6 * PAD], right[6 * PAD];
+        for (int k = 0; k < PAD; ++k)
+            for (int c = 0; c < nc; ++c)
+                left[nc * k + c] = a[nc * k + c], right[nc * k + c] = a[nc * (Nx + PAD + k) + c];
+        for (int k = 0; k < PAD; ++k)
+            for (int c = 0; c < nc; ++c)
+                a[nc * (Nx + k) + c] += left[nc * k + c];
+        for (int k = 0; k < PAD; ++k)
+            for (int c = 0; c < nc; ++c)
+                a[nc * (PAD + k) + c] += right[nc * k + c];
+    }
+}
+
+// ColdSpecies::collect_all (ColdSpecies.cc:268-297): moments x weight on the interior,
+// zero ghosts, nvv = (nV/n) nV
+__global__ void finalize_cold_kernel(double const *n_full, double const *nV_full, double *out, int Nx, double w)
+{
+    int const M = Nx + 2 * PAD;
+    double   *n = out, *nV = out + M, *nvv = out + 4 * M;
+    for (int i = threadIdx.x; i < M; i += blockDim.x) {
+        bool const interior = i >= PAD && i < Nx + PAD;
+        double const ni     = interior ? n_full[i] * w : 0.0;
+        d3 const     v      = interior ? ld3(nV_full, i) * w : d3{ 0, 0, 0 };
+        n[i]                = ni;
+        st3(nV, i, v);
+        double t[6] = { 0, 0, 0, 0, 0, 0 };
+        if (interior) {
+            t[0] = t[3] = v.x / ni;
+            t[1] = t[4] = v.y / ni;
+            t[2] = t[5] = v.z / ni;
+            t[0] *= v.x, t[1] *= v.y, t[2] *= v.z;
+            t[3] *= v.y, t[4] *= v.z, t[5] *= v.x;
+        }
+        for (int c = 0; c < 6; ++c)
+            nvv[6 * i + c] = t[c];
+    }
+}
+
+__device__ double block_sum(double v, double *sh)
+{
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0)
+        sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double r = 0;
+    if (threadIdx.x < 32) {
+        r = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+        r = warp_sum(r);
+    }
+    __syncthreads();
+    return r;
+}
+
+// EnergyRecorder::dump (EnergyRecorder.cc:98-140); MFA components equal Cartesian ones here
+__global__ void energy_kernel(EnergyArgs a)
+{
+    __shared__ double sh[32];
+    double const      denom = 2 * static_cast<double>(a.Nx);
+    for (int f = 0; f < 2; ++f) {
+        double const *g = f ? a.E : a.B;
+        for (int c = 0; c < 3; ++c) {
+            double acc = 0;
+            for (int i = threadIdx.x; i < a.Nx; i += blockDim.x)
+                acc += g[3 * i + c] * g[3 * i + c];
+            double const s = block_sum(acc, sh);
+            if (threadIdx.x == 0)
+                a.out[3 * f + c] = s / denom;
+        }
+    }
+    for (int s = 0; s < a.ns; ++s)
+        for (int c = 0; c < 3; ++c) {
+            double lab = 0, pla = 0;
+            for (int i = threadIdx.x; i < a.Nx; i += blockDim.x) {
+                double const n = a.n[s][i];
+                if (n < 1e-15)
+                    continue;
+                double const t = a.nvv[s][6 * i + c], v = a.nV[s][3 * i + c];
+                lab += t;
+                pla += t - v * v / n;
+            }
+            double const L = block_sum(lab, sh), P = block_sum(pla, sh);
+            if (threadIdx.x == 0) {
+                a.out[6 + 6 * s + c]     = L * a.factor[s];
+                a.out[6 + 6 * s + 3 + c] = P * a.factor[s];
+            }
+        }
+}
+
+} // namespace h1d

@@ -182,6 +182,21 @@ int h1d_download_cold(h1d_run *run, int i, double *n, double *nV, double *nvv, d
  * species then every cold species KE_lab[3], KE_pla[3]; computed on the device */
 int h1d_energy(h1d_run *run, double *dB2O2, double *dE2O2, double *KE_lab, double *KE_pla);
 
+/* Phase timing with CUDA events recorded on the run's stream around each kernel group while
+ * profiling is enabled; read() waits for the stream and returns the accumulated figures. */
+typedef struct h1d_profile {
+    double  push_ms;          /* fused push/deposit kernels */
+    double  sort_ms;          /* cell sort (keys, histograms, scans, scatters, gather) */
+    double  field_ms;         /* grid-phase kernel */
+    int64_t push_launches;
+    int64_t sort_calls;
+    int64_t field_launches;
+    int64_t kernel_launches;  /* every kernel this library launched while profiling */
+    int64_t particles_pushed; /* sum over push launches of the particles each processed */
+} h1d_profile;
+int h1d_profile_enable(h1d_run *run, int on); /* on != 0 also resets the counters */
+int h1d_profile_read(h1d_run *run, h1d_profile *out);
+
 const char *h1d_status_string(h1d_run *run);
 const char *h1d_error_name(int status);
 

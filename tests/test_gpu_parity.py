@@ -1,0 +1,132 @@
+"""Parity of the CUDA path (through the C-ABI) with the oracle on identical particles.
+
+The oracle reproduces the reference bit for bit (test_oracle_vs_reference.py).  The GPU path
+differs from it only in floating-point association: deposits are summed in another order
+(cell-sorted particles, warp reductions, atomics) and the particle push uses FMA and CUDA's
+libm.  Tolerances (max-norm relative error against the oracle):
+  - one step from an identical state: 1e-12 for fields, sources, moments and particles, and
+    the full-grid cell index of every particle identical (a mismatch is allowed only for a
+    particle within 1e-12 of a cell boundary, and none is expected);
+  - ten steps: 1e-9 (the difference grows with the plasma's own error amplification).
+"""
+import os
+
+import numpy as np
+import pytest
+from parity_util import by_pid, cell_keys, cell_mismatches, rel_err, state_errors
+from state_io import read_state
+
+import hfemic_b200 as h
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+CAMCL = [n for n in sorted(h.configs.PARITY) if h.configs.PARITY[n]().algorithm == h.configs.ALGO_CAMCL]
+ALL = sorted(h.configs.PARITY)
+TOL1, TOL10 = 1e-12, 1e-9
+
+
+def run_both(cfg, init, steps, gpu_lib, oracle_lib, chunks=1):
+    with h.Run(cfg, gpu_lib, "h1d_") as g, h.Run(cfg, oracle_lib, "orc_") as c:
+        g.upload_state(init)
+        c.upload_state(init)
+        for _ in range(chunks):
+            g.advance(steps)
+            c.advance(steps)
+        return g.state(), c.state(), g.energy(), c.energy()
+
+
+@pytest.mark.parametrize("name", ALL)
+def test_one_step(name, gpu_lib, oracle_lib):
+    cfg = h.configs.PARITY[name]()
+    init = read_state(os.path.join(GOLDEN, f"{name}.init.bin"))
+    g, c, eg, ec = run_both(cfg, init, 1, gpu_lib, oracle_lib)
+    errs = state_errors(g, c, cfg)
+    print(name, "1 step:", {k: f"{v:.2e}" for k, v in errs.items()})
+    bad = {k: v for k, v in errs.items() if not v <= TOL1}
+    assert not bad, bad
+    mism = cell_mismatches(g, c, cfg)
+    assert all(d < 1e-12 for _, _, d in mism), mism
+    for key in ("dB2O2", "dE2O2", "KE_lab", "KE_pla"):
+        assert rel_err(eg[key], ec[key]) <= TOL1, key
+
+
+@pytest.mark.parametrize("name", ALL)
+def test_ten_steps(name, gpu_lib, oracle_lib):
+    cfg = h.configs.PARITY[name]()
+    init = read_state(os.path.join(GOLDEN, f"{name}.init.bin"))
+    g, c, eg, ec = run_both(cfg, init, 5, gpu_lib, oracle_lib, chunks=2)
+    errs = state_errors(g, c, cfg)
+    print(name, "10 steps:", {k: f"{v:.2e}" for k, v in errs.items()})
+    bad = {k: v for k, v in errs.items() if not v <= TOL10}
+    assert not bad, bad
+    assert not [m for m in cell_mismatches(g, c, cfg) if m[2] >= 1e-9]
+
+
+@pytest.mark.parametrize("name", ALL)
+def test_against_reference_fixture(name, gpu_lib):
+    """The GPU path against the reference's own output after ten steps (golden fixture)."""
+    cfg = h.configs.PARITY[name]()
+    init = read_state(os.path.join(GOLDEN, f"{name}.init.bin"))
+    ref = read_state(os.path.join(GOLDEN, f"{name}.step10.bin"))
+    with h.Run(cfg, gpu_lib, "h1d_") as g:
+        g.upload_state(init)
+        g.advance(10)
+        st = g.state()
+    for key in ("B", "E", "charge", "current"):
+        assert rel_err(st[key], ref[key]) <= TOL10, key
+    id0 = init["particles"][0]["id"]
+    ids = ref["particles"][0]["id"]
+    pg = by_pid(st["particles"][0])
+    order = np.argsort(ids)
+    assert rel_err(pg["q1"], ref["particles"][0]["q1"][order]) <= TOL10
+    assert np.array_equal(np.sort(id0[st["particles"][0]["pid"]]), np.sort(ids))
+
+
+def test_sort_order_is_stable_cell_sort(gpu_lib):
+    """With a sort before every step, the device order after one step is exactly the CPU
+    stable sort, by full-grid cell, of the uploaded particles."""
+    cfg = h.configs.parity_p2().replace(sort_interval=1)
+    init = read_state(os.path.join(GOLDEN, f"{cfg.name}.init.bin"))
+    with h.Run(cfg, gpu_lib, "h1d_") as g:
+        g.upload_state(init)
+        g.advance(1)
+        for s in range(len(cfg.kinetic)):
+            pid = g.particles(s)["pid"]
+            keys = cell_keys(init["particles"][s]["q1"], cfg.Nx)
+            np.testing.assert_array_equal(pid, np.argsort(keys, kind="stable"))
+
+
+def test_large_random_state(gpu_lib, oracle_lib):
+    """A synthetic state with more particles than the fixtures (seeded loader)."""
+    from hfemic_b200.loader import initial_state
+
+    cfg = h.configs.parity_p2().replace(Nx=256, phase_retardation=(32, 1.0), amplitude_damping=(32, 0.2))
+    for k in cfg.kinetic:
+        k.Nc = 200
+    init = initial_state(cfg, seed=3)
+    g, c, _, _ = run_both(cfg, init, 2, gpu_lib, oracle_lib)
+    errs = state_errors(g, c, cfg)
+    print("large 2 steps:", {k: f"{v:.2e}" for k, v in errs.items()})
+    assert max(errs.values()) <= 1e-11
+
+
+def test_moved_too_far(gpu_lib):
+    cfg = h.configs.parity_p1()
+    init = read_state(os.path.join(GOLDEN, f"{cfg.name}.init.bin"))
+    init["particles"][0]["vx"][5] = 2.0 * cfg.Dx / cfg.dt
+    with h.Run(cfg, gpu_lib, "h1d_") as g:
+        g.upload_state(init)
+        with pytest.raises(h.MovedTooFar):
+            g.advance(1)
+
+
+def test_invalid_params(gpu_lib):
+    cfg = h.configs.parity_p1()
+    p = h.abi.make_params(cfg)
+    p.kinetic[0].shape_order = 4
+    lib, fn = h.abi.load_library(gpu_lib, "h1d_")
+    import ctypes
+
+    handle = ctypes.c_void_p()
+    assert fn["create"](ctypes.byref(p), ctypes.byref(handle)) == h.abi.ERR_INVALID_ARG
+    assert not handle.value
