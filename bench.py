@@ -269,6 +269,7 @@ def main():
                 "traffic": None, "kernel": "push_kernel (fused push + 2 deposits + move + BC, FP64)",
                 "peak_kind": peak_kind,
                 "bytes_per_launch": bytes_per_launch,
+                "window_miss_rate": prof.window_misses / max(2 * prof.particles_pushed, 1),
                 "phase_ms_per_step": {"push": prof.push_ms / args.steps, "sort": prof.sort_ms / args.steps,
                                       "field": prof.field_ms / args.steps}}
     traffic_path = os.path.join(ROOT, "profiles", "push_kernel_traffic.json")

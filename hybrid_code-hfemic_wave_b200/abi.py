@@ -89,7 +89,8 @@ def make_params(cfg: "_cfg.RunConfig") -> Params:
 class Profile(C.Structure):
     _fields_ = [("push_ms", C.c_double), ("sort_ms", C.c_double), ("field_ms", C.c_double),
                 ("push_launches", C.c_int64), ("sort_calls", C.c_int64), ("field_launches", C.c_int64),
-                ("kernel_launches", C.c_int64), ("particles_pushed", C.c_int64)]
+                ("kernel_launches", C.c_int64), ("particles_pushed", C.c_int64),
+                ("window_misses", C.c_int64)]
 
 
 _dp = C.POINTER(C.c_double)

@@ -21,6 +21,7 @@ enum : unsigned {
     ST_OUT_OF_RANGE  = 1u << 1, // a particle's stencil fell outside the padded grid (non-finite or lost particle)
     ST_NAN           = 1u << 2,
     ST_SORT_OVERFLOW = 1u << 3,
+    ST_TIMEOUT       = 1u << 4, // a bounded wait on a pipeline barrier gave up
 };
 
 struct d3 {

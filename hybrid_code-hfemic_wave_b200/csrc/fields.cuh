@@ -64,7 +64,7 @@ struct FieldArgs {
     int           Nx, H, seg, bc;
     double const *geo; // G_COUNT x Nx
     double const *B_in, *E_in; // AoS, cell 0
-    double       *B_out, *E_out, *Bh_out, *charge_out, *current_out;
+    double       *B_out, *E_out, *EB_out, *charge_out, *current_out; // EB: {E, B on the half grid} per cell
     int           nk, nc;
     KinSrc        k[MAXK];
     ColdSrc       c[MAXC];
@@ -72,10 +72,12 @@ struct FieldArgs {
     int           m; // n_subcycles
     // electron fluid (EField.cc:267-291)
     double        mOeOO0oe2, gamma, O02beO2, cO2, cOsqrtg;
-    // predictor-corrector phase selector
+    // predictor-corrector (Domain_PC.cc:84-205): phase 0 initial sources, 1 predicted fields,
+    // 2 after the predictor deposit, 3 after the corrector deposit
     int           phase;
-    double const *B0_in, *E0_in, *charge_in, *current_in; // PC
-    double       *B1_out, *E1_out;                       // PC averaged fields for the pushes
+    double const *charge_in, *current_in; // sources of the previous corrector (cell 0)
+    double const *E1_in;                  // averaged E of the previous phase (cell 0)
+    double       *E1_out;                 // averaged E for the next particle pass (cell 0)
 };
 
 struct Cell {
@@ -211,6 +213,23 @@ __device__ __forceinline__ void put1(double *g, Cell const &C, int Nx, double v)
         g[Nx + C.gm] = v;
     if (C.gm >= Nx - PAD)
         g[C.gm - Nx] = v;
+}
+
+// owner write of the interleaved push record {E, B averaged onto the half grid} and its ghost
+// images; the half-grid B of the last ghost cell stays NaN (PartSpecies.cc:137)
+__device__ __forceinline__ void put_eb(double *eb, Cell const &C, int Nx, d3 E, d3 Bh)
+{
+    auto put = [&](int i, bool withB) {
+        double *p = eb + 6 * i;
+        p[0] = E.x, p[1] = E.y, p[2] = E.z;
+        if (withB)
+            p[3] = Bh.x, p[4] = Bh.y, p[5] = Bh.z;
+    };
+    put(C.gm, true);
+    if (C.gm < PAD)
+        put(Nx + C.gm, C.gm < PAD - 1);
+    if (C.gm >= Nx - PAD)
+        put(C.gm - Nx, true);
 }
 
 // shared-memory carve-up: 9 scalar and 14 vector arrays of L doubles
@@ -392,11 +411,7 @@ __global__ void __launch_bounds__(512) camcl_field_kernel(FieldArgs a)
         put1(a.charge_out, C, Nx, rho_avg);
         put3(a.current_out, C, Nx, J_avg);
         d3 const Bh = (sld3(S.B0, min(t + 1, C.L - 1)) + Bavg) * 0.5;
-        st3(a.Bh_out, C.gm, Bh);
-        if (C.gm < PAD - 1)
-            st3(a.Bh_out, Nx + C.gm, Bh);
-        if (C.gm >= Nx - PAD)
-            st3(a.Bh_out, C.gm - Nx, Bh);
+        put_eb(a.EB_out, C, Nx, Ef, Bh);
         for (int ci = 0; ci < a.nc; ++ci)
             st3(a.c[ci].nV_out, C.gm, cold_nV[ci]);
         // clear the deposit set of the next cycle (interior + ghost images)
@@ -404,6 +419,102 @@ __global__ void __launch_bounds__(512) camcl_field_kernel(FieldArgs a)
             for (int d = 0; d < 2; ++d)
                 for (int q = 0; q < 4; ++q)
                     put1(a.k[s].zero[d][q], C, Nx, 0.0);
+    }
+}
+
+
+// ------------------------------------------------------------------------------------------------
+// predictor-corrector phases (Domain_PC.cc:21-205)
+// ------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(512) pc_field_kernel(FieldArgs a)
+{
+    extern __shared__ double sm[];
+    Cell C;
+    load_cell(a, C);
+    Smem const S = carve(sm, C.L);
+    int const  t = C.t, Nx = a.Nx, ph = a.phase;
+
+    // sources: kinetic species (deposit at the end position), then cold species
+    double rho = 0;
+    d3     J   = { 0, 0, 0 };
+    if (ph != 1) {
+        for (int s = 0; s < a.nk; ++s) {
+            SV const r = collect_kinetic(a, C, S, a.k[s], 1);
+            rho += r.a[t];
+            J = J + sld3(r.v, t);
+        }
+        for (int ci = 0; ci < a.nc; ++ci) {
+            ColdSrc const &K = a.c[ci];
+            d3             v;
+            if (ph == 0)
+                v = ld3(K.nV_in, C.gm);
+            else if (ph == 2) // predictor copy pushed with the predicted fields (Domain_PC.cc:125-133)
+                v = boris_push(K.boris, ld3(K.nV_in, C.gm), d3{ C.hbx, 0 * a.O0, 0 * a.O0 }, ld3(a.E1_in, C.gm) * K.n[C.gm]);
+            else // corrector: the state pushed in phase 2
+                v = ld3(K.nV_out, C.gm);
+            S.tr[t] = (K.n[C.gm] * K.w) * K.cdcf;
+            sst3(S.tJ, t, (v * K.w) * K.ccf);
+            SV const r = smooth_n(C, K.nsm, S.tr, S.tJ, S.ts, S.tJs);
+            rho += r.a[t];
+            J = J + sld3(r.v, t);
+        }
+    }
+    if (ph == 0) {
+        if (C.owner) {
+            put1(a.charge_out, C, Nx, rho);
+            put3(a.current_out, C, Nx, J);
+            for (int s = 0; s < a.nk; ++s)
+                for (int d = 0; d < 2; ++d)
+                    for (int q = 0; q < 4; ++q)
+                        put1(a.k[s].zero[d][q], C, Nx, 0.0);
+        }
+        return;
+    }
+    double const rho_src = ph == 1 ? a.charge_in[C.gm] : rho;
+    d3 const     J_src   = ph == 1 ? ld3(a.current_in, C.gm) : J;
+    d3 const     E0      = ld3(a.E_in, C.gm);
+    d3 const     B0      = ld3(a.B_in, C.gm);
+    d3 const     Eb      = ph == 1 ? E0 : ld3(a.E1_in, C.gm); // E driving Faraday's law
+    sst3(S.Ecov, t, covar_half(C, Eb));
+    S.Pe[t] = Pe_of(a, rho_src);
+    __syncthreads();
+    d3 const     Bn  = B_at(a, C, S.Ecov, B0, a.dt);
+    double const dPe = dPe_at(a, C, S.Pe);
+    sst3(S.Bcov, t, covar_full(C, Bn));
+    sst3(S.Bcon, t, contr_full(C, Bn));
+    __syncthreads();
+    d3 const En = E_at(a, C, S.Bcov, S.Bcon, contr_half(C, J_src), dPe, rho_src);
+    if (ph == 3) {
+        if (C.owner) {
+            put3(a.B_out, C, Nx, Bn);
+            put3(a.E_out, C, Nx, En);
+            put1(a.charge_out, C, Nx, rho_src);
+            put3(a.current_out, C, Nx, J_src);
+            for (int s = 0; s < a.nk; ++s)
+                for (int d = 0; d < 2; ++d)
+                    for (int q = 0; q < 4; ++q)
+                        put1(a.k[s].zero[d][q], C, Nx, 0.0);
+        }
+        return;
+    }
+    d3 const B1a = (Bn + B0) * .5;
+    d3 const E1a = (En + E0) * .5;
+    sst3(S.B0, t, B1a);
+    __syncthreads();
+    d3 const Bh = (sld3(S.B0, min(t + 1, C.L - 1)) + B1a) * 0.5;
+    if (C.owner) {
+        put3(a.E1_out, C, Nx, E1a);
+        put_eb(a.EB_out, C, Nx, E1a, Bh);
+        if (ph == 2) {
+            for (int ci = 0; ci < a.nc; ++ci) { // corrector push of the cold fluid (Domain_PC.cc:182-188)
+                ColdSrc const &K = a.c[ci];
+                st3(K.nV_out, C.gm, boris_push(K.boris, ld3(K.nV_in, C.gm), d3{ C.hbx, 0 * a.O0, 0 * a.O0 }, E1a * K.n[C.gm]));
+            }
+            for (int s = 0; s < a.nk; ++s)
+                for (int d = 0; d < 2; ++d)
+                    for (int q = 0; q < 4; ++q)
+                        put1(a.k[s].zero[d][q], C, Nx, 0.0);
+        }
     }
 }
 

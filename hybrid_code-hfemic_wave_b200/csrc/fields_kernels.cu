@@ -9,16 +9,24 @@ namespace h1d {
 
 cudaError_t set_field_smem(size_t bytes)
 {
-    return cudaFuncSetAttribute(camcl_field_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    cudaError_t e = cudaFuncSetAttribute(camcl_field_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+    if (e != cudaSuccess)
+        return e;
+    return cudaFuncSetAttribute(pc_field_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+}
+cudaError_t launch_pc_fields(FieldArgs const &a, int blocks, int threads, size_t smem, cudaStream_t st)
+{
+    pc_field_kernel<<<blocks, threads, smem, st>>>(a);
+    return cudaGetLastError();
 }
 cudaError_t launch_camcl_fields(FieldArgs const &a, int blocks, int threads, size_t smem, cudaStream_t st)
 {
     camcl_field_kernel<<<blocks, threads, smem, st>>>(a);
     return cudaGetLastError();
 }
-cudaError_t launch_prep_fields(double *B, double *E, double *Bh, int Nx, cudaStream_t st)
+cudaError_t launch_prep_fields(double *B, double *E, double *EB, int Nx, cudaStream_t st)
 {
-    prep_fields_kernel<<<(Nx + 2 * PAD + 255) / 256, 256, 0, st>>>(B, E, Bh, Nx);
+    prep_fields_kernel<<<(Nx + 2 * PAD + 255) / 256, 256, 0, st>>>(B, E, EB, Nx);
     return cudaGetLastError();
 }
 cudaError_t launch_finalize_kinetic(double const *raw, double *out, int Nx, double s1, int reflecting, cudaStream_t st)

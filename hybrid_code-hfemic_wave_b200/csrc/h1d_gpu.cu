@@ -54,18 +54,20 @@ struct ColdState {
 
 struct h1d_run {
     h1d_params   p;
-    int          device = 0;
+    int          device = 0, num_sms = 148;
     cudaStream_t stream = nullptr;
     long         Nx = 0, M = 0;
     int          H = 0, seg = 0, L = 0, nblocks_field = 0;
     size_t       field_smem = 0;
     double      *geo = nullptr;
-    double      *B[2] = {}, *E[2] = {}, *Bh = nullptr, *charge = nullptr, *current = nullptr;
+    double      *B[2] = {}, *E[2] = {}, *EB = nullptr, *charge = nullptr, *current = nullptr;
+    double      *E1[2] = {}; // predictor-corrector: averaged E of phases 1 and 2
     int          fcur = 0; // field parity
     int          dset = 0; // deposit set parity
     SpeciesState sp[H1D_MAX_KINETIC];
     ColdState    cold[H1D_MAX_COLD];
     unsigned    *d_status = nullptr;
+    unsigned long long *d_fallbacks = nullptr;
     unsigned    *h_status = nullptr; // pinned
     double      *d_energy = nullptr;
     bool         recurring = false, moments_stale = true, fields_dirty = true;
@@ -270,7 +272,7 @@ PushArgs push_args(h1d_run *run, int s)
     a.q1 = S.buf[S.cur][0], a.vx = S.buf[S.cur][1], a.vy = S.buf[S.cur][2], a.vz = S.buf[S.cur][3];
     a.w = S.buf[S.cur][4], a.pid = S.pid[S.cur];
     a.n = S.n, a.ppt = ppt_for(run, s), a.Nx = static_cast<int>(run->Nx);
-    a.E = run->E[run->fcur] + 3 * PAD, a.Bh = run->Bh + 3 * PAD;
+    a.EB = run->EB + 6 * PAD;
     for (int dd = 0; dd < 2; ++dd)
         for (int q = 0; q < 4; ++q)
             a.dep[dd][q] = dep_ptr(run, s, run->dset, dd, q);
@@ -278,21 +280,44 @@ PushArgs push_args(h1d_run *run, int s)
     a.half_min = a.full_min + 0.5;
     a.xi = p.xi, a.xi2 = p.xi * p.xi, a.xiD1 = p.xi * p.Dx, a.D1 = p.Dx, a.inv_D1 = 1 / p.Dx, a.O0 = p.O0;
     a.Oc = d.Oc, a.dt = p.dt, a.travel_scale = 1.0, a.boris = boris_make(p.dt, p.c, p.O0, d.Oc);
-    a.status = run->d_status, a.seed = p.gyrophase_seed, a.counter = static_cast<uint64_t>(run->step) * 8;
+    a.xiO0_Oc = p.xi * p.O0 / d.Oc;
+    a.status = run->d_status, a.fallbacks = run->d_fallbacks, a.seed = p.gyrophase_seed, a.counter = static_cast<uint64_t>(run->step) * 8;
     a.species = s, a.randomize = p.randomize_gyrophase, a.homogeneous_poly = p.xi < 1e-10;
     a.move_steps = 1, a.deposit_mask = 3, a.write_back = 1;
     return a;
+}
+
+template <int O, bool MIRROR, int BC>
+cudaError_t push_attr()
+{
+    return cudaFuncSetAttribute(push_kernel<O, MIRROR, BC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(PIPE_SMEM));
+}
+cudaError_t set_push_smem()
+{
+    cudaError_t e = cudaSuccess;
+    auto        k = [&](cudaError_t x) {
+        if (e == cudaSuccess)
+            e = x;
+    };
+    k(push_attr<1, false, 0>()), k(push_attr<1, false, 1>()), k(push_attr<1, false, 2>());
+    k(push_attr<1, true, 0>()), k(push_attr<1, true, 1>()), k(push_attr<1, true, 2>());
+    k(push_attr<2, false, 0>()), k(push_attr<2, false, 1>()), k(push_attr<2, false, 2>());
+    k(push_attr<2, true, 0>()), k(push_attr<2, true, 1>()), k(push_attr<2, true, 2>());
+    k(push_attr<3, false, 0>()), k(push_attr<3, false, 1>()), k(push_attr<3, false, 2>());
+    k(push_attr<3, true, 0>()), k(push_attr<3, true, 1>()), k(push_attr<3, true, 2>());
+    return e;
 }
 
 template <int O, bool MIRROR>
 void launch_push_bc(PushArgs const &a, int bc, dim3 g, cudaStream_t st)
 {
     if (bc == H1D_BC_PERIODIC)
-        push_kernel<O, MIRROR, BCK_PERIODIC><<<g, 256, 0, st>>>(a);
+        push_kernel<O, MIRROR, BCK_PERIODIC><<<g, PIPE_THREADS, PIPE_SMEM, st>>>(a);
     else if (bc == H1D_BC_REFLECTING)
-        push_kernel<O, MIRROR, BCK_REFLECTING><<<g, 256, 0, st>>>(a);
+        push_kernel<O, MIRROR, BCK_REFLECTING><<<g, PIPE_THREADS, PIPE_SMEM, st>>>(a);
     else
-        push_kernel<O, MIRROR, BCK_ABSORBING><<<g, 256, 0, st>>>(a);
+        push_kernel<O, MIRROR, BCK_ABSORBING><<<g, PIPE_THREADS, PIPE_SMEM, st>>>(a);
 }
 template <int O>
 void launch_push_o(PushArgs const &a, bool mirror, int bc, dim3 g, cudaStream_t st)
@@ -306,8 +331,8 @@ int launch_push(h1d_run *run, int s, PushArgs const &a)
 {
     if (a.n == 0)
         return H1D_OK;
-    int64_t const chunks = (a.n + 32LL * a.ppt - 1) / (32LL * a.ppt);
-    dim3 const    g(static_cast<unsigned>((chunks + 7) / 8));
+    int64_t const chunks = (a.n + PIPE_CHUNK - 1) / PIPE_CHUNK;
+    dim3 const    g(static_cast<unsigned>(std::min<int64_t>(chunks, static_cast<int64_t>(run->num_sms) * 3)));
     bool const    mirror = run->p.xi != 0;
     switch (run->p.kinetic[s].shape_order) {
     case 1: launch_push_o<1>(a, mirror, run->p.particle_bc, g, run->stream); break;
@@ -386,7 +411,7 @@ FieldArgs field_args(h1d_run *run)
     a.geo = run->geo;
     a.B_in = run->B[run->fcur] + 3 * PAD, a.E_in = run->E[run->fcur] + 3 * PAD;
     a.B_out = run->B[1 - run->fcur] + 3 * PAD, a.E_out = run->E[1 - run->fcur] + 3 * PAD;
-    a.Bh_out = run->Bh + 3 * PAD, a.charge_out = run->charge + PAD, a.current_out = run->current + 3 * PAD;
+    a.EB_out = run->EB + 6 * PAD, a.charge_out = run->charge + PAD, a.current_out = run->current + 3 * PAD;
     a.nk = p.n_kinetic, a.nc = p.n_cold;
     for (int s = 0; s < p.n_kinetic; ++s) {
         h1d_kinetic_desc const &d = p.kinetic[s];
@@ -419,7 +444,7 @@ FieldArgs field_args(h1d_run *run)
 // first advance: fill ghost cells of E and B (Domain_CAMCL.cc:27-35) and B on the half grid
 int prepare_fields(h1d_run *run)
 {
-    CU(launch_prep_fields(run->B[run->fcur] + 3 * PAD, run->E[run->fcur] + 3 * PAD, run->Bh + 3 * PAD,
+    CU(launch_prep_fields(run->B[run->fcur] + 3 * PAD, run->E[run->fcur] + 3 * PAD, run->EB + 6 * PAD,
                           static_cast<int>(run->Nx), run->stream));
     run->fields_dirty = false;
     return H1D_OK;
@@ -450,6 +475,92 @@ int camcl_step(h1d_run *run)
     return H1D_OK;
 }
 
+
+// Domain_PC::cycle (Domain_PC.cc:79-205): predicted fields, predictor pass (particles not kept),
+// re-predicted fields, corrector pass, corrected fields.  Deposit set X = dset takes the
+// predictor's deposit, Y = 1 - dset the corrector's; each field phase clears the set the next
+// particle pass uses.
+int pc_launch_fields(h1d_run *run, int phase, int raw_set, int zero_set, double const *E1_in, double *E1_out)
+{
+    FieldArgs a = field_args(run);
+    for (int s = 0; s < run->p.n_kinetic; ++s)
+        for (int d = 0; d < 2; ++d)
+            for (int q = 0; q < 4; ++q) {
+                a.k[s].raw[d][q]  = dep_ptr(run, s, raw_set, d, q);
+                a.k[s].zero[d][q] = dep_ptr(run, s, zero_set, d, q);
+            }
+    a.phase      = phase;
+    a.charge_in  = run->charge + PAD;
+    a.current_in = run->current + 3 * PAD;
+    a.E1_in      = E1_in ? E1_in + 3 * PAD : nullptr;
+    a.E1_out     = E1_out ? E1_out + 3 * PAD : nullptr;
+    phase_begin(run, 2);
+    CU(launch_pc_fields(a, run->nblocks_field, run->L, run->field_smem, run->stream));
+    phase_end(run, 1);
+    return H1D_OK;
+}
+
+int pc_particles(h1d_run *run, int pass, int dep_set) // pass 0 predictor, 1 corrector, 2 initial deposit
+{
+    for (int s = 0; s < run->p.n_kinetic; ++s) {
+        if (pass != 2 && run->sp[s].since_sort >= run->sort_interval)
+            TRY(sort_species(run, s));
+        PushArgs a = push_args(run, s);
+        for (int q = 0; q < 4; ++q)
+            a.dep[0][q] = dep_ptr(run, s, dep_set, 0, q), a.dep[1][q] = dep_ptr(run, s, dep_set, 1, q);
+        a.move_steps   = pass == 2 ? 0 : 2;
+        a.deposit_mask = 2;
+        a.write_back   = pass == 1;
+        a.travel_scale = 1.0 / 0.5;
+        a.counter      = static_cast<uint64_t>(run->step) * 8 + (pass == 1 ? 2 : 0);
+        phase_begin(run, 0);
+        TRY(launch_push(run, s, a));
+        phase_end(run, run->sp[s].n > 0 ? 1 : 0);
+        if (run->profiling)
+            run->prof.particles_pushed += run->sp[s].n;
+        if (pass == 1)
+            run->sp[s].since_sort++;
+    }
+    return H1D_OK;
+}
+
+int pc_initial_sources(h1d_run *run) // Domain_PC.cc:36-56
+{
+    int const X = run->dset, Y = 1 - X;
+    TRY(pc_particles(run, 2, Y));
+    TRY(pc_launch_fields(run, 0, Y, X, nullptr, nullptr));
+    return H1D_OK;
+}
+
+int pc_step(h1d_run *run)
+{
+    int const X = run->dset, Y = 1 - X;
+    TRY(pc_launch_fields(run, 1, X, X, nullptr, run->E1[0])); // B1, E1 predicted and averaged (clears nothing new)
+    TRY(pc_particles(run, 0, X));
+    TRY(pc_launch_fields(run, 2, X, Y, run->E1[0], run->E1[1]));
+    TRY(pc_particles(run, 1, Y));
+    {
+        FieldArgs a = field_args(run);
+        for (int s = 0; s < run->p.n_kinetic; ++s)
+            for (int d = 0; d < 2; ++d)
+                for (int q = 0; q < 4; ++q) {
+                    a.k[s].raw[d][q]  = dep_ptr(run, s, Y, d, q);
+                    a.k[s].zero[d][q] = dep_ptr(run, s, X, d, q);
+                }
+        a.phase  = 3;
+        a.E1_in  = run->E1[1] + 3 * PAD;
+        a.E1_out = nullptr;
+        phase_begin(run, 2);
+        CU(launch_pc_fields(a, run->nblocks_field, run->L, run->field_smem, run->stream));
+        phase_end(run, 1);
+    }
+    run->fcur = 1 - run->fcur;
+    for (int c = 0; c < run->p.n_cold; ++c)
+        run->cold[c].cur = 1 - run->cold[c].cur;
+    run->step++;
+    return H1D_OK;
+}
+
 int check_status(h1d_run *run)
 {
     CU(cudaStreamSynchronize(run->stream));
@@ -457,6 +568,8 @@ int check_status(h1d_run *run)
     unsigned const s = *run->h_status;
     if (s & ST_MOVED_TOO_FAR)
         return set_err(run, H1D_ERR_MOVED_TOO_FAR, "PartSpecies::update_pos - particle(s) moved too far");
+    if (s & ST_TIMEOUT)
+        return set_err(run, H1D_ERR_TIMEOUT, "a particle-pipeline barrier wait timed out");
     if (s & ST_OUT_OF_RANGE)
         return set_err(run, H1D_ERR_NAN, "particle(s) outside the padded grid (non-finite or lost particle state)");
     if (s)
@@ -569,13 +682,15 @@ int h1d_create(h1d_params const *params, h1d_run **out)
     run->seg           = static_cast<int>(std::min<long>(L - 2 * run->H, run->Nx));
     run->nblocks_field = static_cast<int>((run->Nx + run->seg - 1) / run->seg);
     run->field_smem    = sizeof(double) * static_cast<size_t>(L) * (SMEM_SCALARS + 3 * SMEM_VECTORS);
-    if (set_field_smem(run->field_smem) != cudaSuccess)
+    if (set_field_smem(run->field_smem) != cudaSuccess || set_push_smem() != cudaSuccess)
         return fail(H1D_ERR_CUDA);
+    cudaDeviceGetAttribute(&run->num_sms, cudaDevAttrMultiProcessorCount, run->device);
 
     long const M = run->M;
     if (dalloc(run, &run->geo, G_COUNT * run->Nx) || dalloc(run, &run->B[0], 3 * M) || dalloc(run, &run->B[1], 3 * M)
-        || dalloc(run, &run->E[0], 3 * M) || dalloc(run, &run->E[1], 3 * M) || dalloc(run, &run->Bh, 3 * M)
+        || dalloc(run, &run->E[0], 3 * M) || dalloc(run, &run->E[1], 3 * M) || dalloc(run, &run->EB, 6 * M)
         || dalloc(run, &run->charge, M) || dalloc(run, &run->current, 3 * M) || dalloc(run, &run->d_status, 1)
+        || dalloc(run, &run->E1[0], 3 * M) || dalloc(run, &run->E1[1], 3 * M) || dalloc(run, &run->d_fallbacks, 1)
         || dalloc(run, &run->d_energy, 6 + 6 * (H1D_MAX_KINETIC + H1D_MAX_COLD)))
         return fail(H1D_ERR_OOM);
     if (cudaMallocHost(&run->h_status, sizeof(unsigned)) != cudaSuccess)
@@ -595,10 +710,6 @@ int h1d_create(h1d_params const *params, h1d_run **out)
     if (cudaMemcpyAsync(run->geo, g.data(), sizeof(double) * g.size(), cudaMemcpyHostToDevice, run->stream) != cudaSuccess
         || cudaStreamSynchronize(run->stream) != cudaSuccess)
         return fail(H1D_ERR_CUDA);
-    // B on the half grid keeps NaN in its last ghost cell (PartSpecies.cc:137)
-    double const nan3[3] = { NAN, NAN, NAN };
-    if (cudaMemcpy(run->Bh + 3 * (M - 1), nan3, sizeof nan3, cudaMemcpyHostToDevice) != cudaSuccess)
-        return fail(H1D_ERR_CUDA);
     *out = run;
     return H1D_OK;
 }
@@ -611,8 +722,9 @@ int h1d_destroy(h1d_run *run)
         cudaStreamSynchronize(run->stream);
     cudaFree(run->geo);
     for (int k = 0; k < 2; ++k)
-        cudaFree(run->B[k]), cudaFree(run->E[k]);
-    cudaFree(run->Bh), cudaFree(run->charge), cudaFree(run->current), cudaFree(run->d_status), cudaFree(run->d_energy);
+        cudaFree(run->B[k]), cudaFree(run->E[k]), cudaFree(run->E1[k]);
+    cudaFree(run->d_fallbacks);
+    cudaFree(run->EB), cudaFree(run->charge), cudaFree(run->current), cudaFree(run->d_status), cudaFree(run->d_energy);
     if (run->h_status)
         cudaFreeHost(run->h_status);
     for (auto &S : run->sp) {
@@ -704,14 +816,14 @@ int h1d_advance_async(h1d_run *run, uint32_t n_steps)
 {
     if (!run)
         return H1D_ERR_INVALID_ARG;
-    if (run->p.algorithm != H1D_ALGO_CAMCL)
-        return set_err(run, H1D_ERR_INVALID_ARG, "predictor-corrector is not available in this build");
-    if (!run->recurring || run->fields_dirty) {
+    bool const first = !run->recurring;
+    if (first || run->fields_dirty)
         TRY(prepare_fields(run));
-        run->recurring = true;
-    }
+    if (first && run->p.algorithm == H1D_ALGO_PC)
+        TRY(pc_initial_sources(run));
+    run->recurring = true;
     for (uint32_t i = 0; i < n_steps; ++i)
-        TRY(camcl_step(run));
+        TRY(run->p.algorithm == H1D_ALGO_CAMCL ? camcl_step(run) : pc_step(run));
     run->moments_stale = true;
     return H1D_OK;
 }
@@ -745,8 +857,10 @@ int h1d_profile_enable(h1d_run *run, int on)
     for (auto &[k, b, e] : run->ev_done)
         run->ev_pool.push_back(b), run->ev_pool.push_back(e);
     run->ev_done.clear();
-    if (on)
+    if (on) {
         run->prof = h1d_profile{};
+        CU(cudaMemsetAsync(run->d_fallbacks, 0, sizeof(unsigned long long), run->stream));
+    }
     run->profiling = on != 0;
     return H1D_OK;
 }
@@ -763,6 +877,9 @@ int h1d_profile_read(h1d_run *run, h1d_profile *out)
         run->ev_pool.push_back(b), run->ev_pool.push_back(e);
     }
     run->ev_done.clear();
+    unsigned long long miss = 0;
+    CU(cudaMemcpy(&miss, run->d_fallbacks, sizeof miss, cudaMemcpyDeviceToHost));
+    run->prof.window_misses = static_cast<int64_t>(miss);
     *out = run->prof;
     return H1D_OK;
 }

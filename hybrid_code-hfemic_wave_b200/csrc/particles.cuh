@@ -17,6 +17,7 @@
 #pragma once
 
 #include "device_common.cuh"
+#include "tma.cuh"
 
 namespace h1d {
 
@@ -29,16 +30,17 @@ struct PushArgs {
     int64_t        n;
     int            ppt; // particles per lane per warp-chunk
     int            Nx;
-    double const  *E;  // AoS double3, pointer at interior cell 0 (ghost cells at negative index)
-    double const  *Bh; // B averaged onto the half grid (PartSpecies.cc:132-139), same layout
+    double const  *EB; // per cell {Ex, Ey, Ez, dBx, dBy, dBz}: E and B averaged onto the half grid
+                       // (PartSpecies.cc:132-139), pointer at interior cell 0
     double        *dep[2][4]; // [deposit at x^N | x^{N+1}][n, nVx, nVy, nVz], at cell 0
     double         half_min, full_min, full_max, full_len;
-    double         xi, xi2, xiD1, D1, inv_D1, O0, Oc, dt, travel_scale;
+    double         xi, xi2, xiD1, D1, inv_D1, O0, Oc, dt, travel_scale, xiO0_Oc;
     BorisK         boris;
     unsigned      *status;
+    unsigned long long *fallbacks; // deposits that missed the register window (diagnostic)
     uint64_t       seed, counter;
     int            species, randomize, homogeneous_poly;
-    int            move_steps; // 1: CAM-CL full step; 2: PC half step, push, half step
+    int            move_steps; // 1: CAM-CL full step; 2: PC half step, push, half step; 0: deposit only
     int            deposit_mask; // bit0: deposit at x^N, bit1: deposit at the end position
     int            write_back;   // 0 for the PC predictor (particles are not kept)
 };
@@ -59,24 +61,33 @@ __device__ __forceinline__ void acc_zero(Acc<O, S> &a)
 }
 
 // deposit one particle: register window if its stencil fits, else direct atomics
+template <int O, int S, int R>
+__device__ __forceinline__ void deposit_at(Acc<O, S> &acc, Shape<O> const &sh, double const (&vw)[4])
+{
+#pragma unroll
+    for (int j = 0; j <= O; ++j)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            acc.v[q][R + j] = fma(vw[q], sh.w[j], acc.v[q][R + j]);
+}
 template <int O, int S, int D>
 __device__ __forceinline__ void deposit(Acc<O, S> &acc, int base, Shape<O> const &sh, double w, d3 v,
                                         PushArgs const &a)
 {
-    double const vw[4] = { w, v.x * w, v.y * w, v.z * w };
-    int const    r     = sh.i0 - base;
-    if (r >= 0 && r <= S - O - 1) {
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            double ws = 0;
-#pragma unroll
-            for (int j = 0; j <= O; ++j)
-                ws = (s - r == j) ? sh.w[j] : ws;
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                acc.v[q][s] = fma(vw[q], ws, acc.v[q][s]);
-        }
-    } else {
+    constexpr int RW     = S - O - 1; // window offsets 0..RW
+    double const  vw[4] = { w, v.x * w, v.y * w, v.z * w };
+    int const     r     = sh.i0 - base;
+    static_assert(RW >= 1 && RW <= 3, "window offsets 0..RW with RW in {1, 2, 3}");
+    if (r == 0)
+        deposit_at<O, S, 0>(acc, sh, vw);
+    else if (r == 1)
+        deposit_at<O, S, 1>(acc, sh, vw);
+    else if (RW >= 2 && r == 2)
+        deposit_at<O, S, (RW >= 2 ? 2 : 0)>(acc, sh, vw);
+    else if (RW >= 3 && r == 3)
+        deposit_at<O, S, (RW >= 3 ? 3 : 0)>(acc, sh, vw);
+    else {
+        atomicAdd(a.fallbacks, 1ull);
 #pragma unroll
         for (int j = 0; j <= O; ++j)
 #pragma unroll
@@ -161,136 +172,299 @@ __device__ __forceinline__ bool boundary(PushArgs const &a, double &q1, d3 &v, i
     }
 }
 
-// background mirror field at the particle with its gyro-radius offset
-// (PartSpecies.cc:274-279; MFABasis.h:287-290; MirrorGeometry.cc:199-212)
+// background mirror field at the particle with its gyro-radius offset (PartSpecies.cc:274-279;
+// MFABasis.h:287-290; MirrorGeometry.cc:199-212).  With c = cos(xi D1 q1), s = sin(xi D1 q1):
+// B/B0 = 1/c^2, x = tan/xi, rL = (-vz, vy) c^2/Oc, so the transverse components
+// -xi^2 x rL O0 reduce to (xi O0/Oc) s c (vz, -vy).  Also returns c^2 for the move.
 template <bool MIRROR>
-__device__ __forceinline__ d3 background_B(PushArgs const &a, double q1, d3 v)
+__device__ __forceinline__ d3 background_B(PushArgs const &a, double q1, d3 v, double &c2)
 {
     if constexpr (MIRROR) {
         double s, c;
         sincos(a.xiD1 * q1, &s, &c);
-        double const ic  = 1 / c;
-        double const Ocl = a.Oc * (ic * ic);
-        double const rLy = -v.z / Ocl;
-        double const rLz = +v.y / Ocl;
-        double       x;
-        if (a.homogeneous_poly) {
-            double const D1q1 = q1 * a.D1;
-            x                 = D1q1 * (1 + a.xi * a.xi * D1q1 * D1q1 / 3);
-        } else {
-            x = (s * ic) / a.xi;
-        }
-        return { (1 + a.xi2 * (x * x)) * a.O0, -a.xi2 * x * rLy * a.O0, -a.xi2 * x * rLz * a.O0 };
+        c2               = c * c;
+        double const ksc = a.xiO0_Oc * (s * c);
+        return { a.O0 / c2, ksc * v.z, -ksc * v.y };
     } else {
+        c2 = 1;
         return { a.O0, 0, 0 };
     }
 }
 
+// E and dB interpolated at the particle (GridArray.h:110-119) from the interleaved cell records
 template <int O>
-__device__ __forceinline__ d3 interp(double const *g, Shape<O> const &sh)
+__device__ __forceinline__ void interp_EB(double const *eb, Shape<O> const &sh, d3 &E, d3 &B)
 {
-    d3 y = { 0, 0, 0 };
+    E = { 0, 0, 0 };
+    B = { 0, 0, 0 };
 #pragma unroll
     for (int j = 0; j <= O; ++j) {
-        d3 const f = ld3(g, sh.i0 + j);
-        y.x += f.x * sh.w[j];
-        y.y += f.y * sh.w[j];
-        y.z += f.z * sh.w[j];
+        double2 const *p = reinterpret_cast<double2 const *>(eb + 6 * (sh.i0 + j));
+        double2 const  x = __ldg(p), y = __ldg(p + 1), z = __ldg(p + 2);
+        double const   w = sh.w[j];
+        E.x += x.x * w, E.y += x.y * w, E.z += y.x * w;
+        B.x += y.y * w, B.y += z.x * w, B.z += z.y * w;
     }
-    return y;
 }
 
+// ------------------------------------------------------------------------------------------------
+// The particle pass.  Warp-specialised pipeline per CTA: one producer warp streams chunks of
+// PIPE_CHUNK particles global -> shared with 1-D TMA bulk copies completing on mbarriers
+// (PIPE_STAGES deep) and bulk-stores the updated particles back; PIPE_CONSUMER_WARPS warps
+// compute.  A consumer warp owns 32 x PIPE_PPT consecutive (cell-sorted) particles of a chunk and
+// makes two passes over them in shared memory: (1) push at x^N, deposit at x^N, move, boundary,
+// results written in place; (2) deposit at the new position.  Splitting the two deposits halves
+// the register windows.
+//
 // One pass of a species: CAM-CL (move_steps == 1): push at x^N, deposit, move, BC, deposit.
-// Predictor-corrector (move_steps == 2, Domain_PC.cc:110-124, 169-181): half move, BC,
-// push at the half-step position, half move, BC, deposit.
-template <int O, bool MIRROR, int BC>
-__global__ void __launch_bounds__(256) push_kernel(PushArgs a)
+// Predictor-corrector (move_steps == 2, Domain_PC.cc:110-124, 169-181): half move, BC, push at
+// the half-step position, half move, BC, deposit.  move_steps == 0: deposit only
+// (Domain_PC.cc:36-44).
+// ------------------------------------------------------------------------------------------------
+constexpr int PIPE_CONSUMER_WARPS = 4;
+constexpr int PIPE_THREADS        = 32 * (PIPE_CONSUMER_WARPS + 1);
+constexpr int PIPE_PPT            = 4;
+constexpr int PIPE_CHUNK          = 32 * PIPE_CONSUMER_WARPS * PIPE_PPT;
+constexpr int PIPE_STAGES         = 3;
+
+struct PipeStage {
+    double  q1[PIPE_CHUNK], vx[PIPE_CHUNK], vy[PIPE_CHUNK], vz[PIPE_CHUNK], w[PIPE_CHUNK];
+    int32_t pid[PIPE_CHUNK];
+};
+constexpr size_t PIPE_SMEM = sizeof(PipeStage) * PIPE_STAGES + 2 * PIPE_STAGES * sizeof(uint64_t);
+
+__device__ __forceinline__ uint32_t round16(uint32_t b) { return (b + 15u) & ~15u; }
+
+// warp reduce-scatter by recursive halving of V (16 or 32) values: after log2(V) exchange rounds
+// (V/2 + V/4 + ... shuffles) and a butterfly over the remaining lane bits, lane l holds the warp
+// total of value (l >> (5 - log2 V))
+template <int V>
+__device__ __forceinline__ double reduce_scatter(double (&x)[V], int lane)
 {
-    constexpr int R = 2;
+    static_assert(V == 16 || V == 32, "V must be 16 or 32");
+#pragma unroll
+    for (int h = V / 2, m = 16; h >= 1; h >>= 1, m >>= 1) {
+        bool const up = (lane & m) != 0;
+#pragma unroll
+        for (int j = 0; j < h; ++j) {
+            double const send = up ? x[j] : x[j + h];
+            double const keep = up ? x[j + h] : x[j];
+            x[j]              = keep + __shfl_xor_sync(0xffffffffu, send, m);
+        }
+    }
+    double v = x[0];
+    if constexpr (V == 16)
+        v += __shfl_xor_sync(0xffffffffu, v, 1);
+    return v;
+}
+
+template <int O, int S, int D>
+__device__ __forceinline__ void flush_rs(Acc<O, S> const &acc, int base, int lane, PushArgs const &a)
+{
+    constexpr int V  = 4 * S <= 16 ? 16 : 32;
+    constexpr int SH = V == 16 ? 1 : 0;
+    static_assert(4 * S <= 32, "window too wide for one reduce-scatter");
+    double x[V];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+            x[q * S + s] = acc.v[q][s];
+#pragma unroll
+    for (int k = 4 * S; k < V; ++k)
+        x[k] = 0;
+    double const v  = reduce_scatter<V>(x, lane);
+    int const    vi = lane >> SH;
+    if ((lane & SH) == 0 && vi < 4 * S && v != 0.0) {
+        int const q = vi / S, cell = base + vi % S;
+        if (cell >= -PAD && cell < a.Nx + PAD)
+            atomicAdd(a.dep[D][q] + cell, v);
+        else
+            atomicOr(a.status, ST_OUT_OF_RANGE);
+    }
+}
+
+// warp-uniform window base: the smallest stencil base index among the warp's particles
+template <int O>
+__device__ __forceinline__ int window_base(double const *q1s, int w0, int lane, int cnt, double half_min)
+{
+    int m = 0x7fffffff;
+#pragma unroll
+    for (int k = 0; k < PIPE_PPT; ++k) {
+        int const idx = w0 + k * 32 + lane;
+        if (idx < cnt) {
+            double const x = q1s[idx] - half_min;
+            if (x == x) {
+                int const i0 = make_shape<O>(x).i0;
+                m            = i0 < m ? i0 : m;
+            }
+        }
+    }
+    return __reduce_min_sync(0xffffffffu, m);
+}
+
+template <int O, bool MIRROR, int BC>
+__global__ void __launch_bounds__(PIPE_THREADS, 3) push_kernel(PushArgs a)
+{
+    constexpr int R = 3; // window of four stencil base cells: i0 in [base, base + 3]
     constexpr int S = O + 1 + R;
-    int const     lane   = threadIdx.x & 31;
-    int64_t const warp   = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    int64_t const chunk0 = warp * 32 * a.ppt;
-    if (chunk0 >= a.n)
+    extern __shared__ __align__(128) unsigned char smraw[];
+    PipeStage    *stage = reinterpret_cast<PipeStage *>(smraw);
+    uint64_t     *full  = reinterpret_cast<uint64_t *>(smraw + sizeof(PipeStage) * PIPE_STAGES);
+    uint64_t     *empty = full + PIPE_STAGES;
+    int const     warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int64_t const nchunks = (a.n + PIPE_CHUNK - 1) / PIPE_CHUNK;
+    int64_t const mine    = blockIdx.x < nchunks ? (nchunks - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    bool const    load_pid = a.randomize != 0;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < PIPE_STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], PIPE_CONSUMER_WARPS);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    if (warp == PIPE_CONSUMER_WARPS) { // ---------------- producer ----------------
+        if (lane == 0) {
+            for (int64_t i = 0; i < mine + PIPE_STAGES; ++i) {
+                int const s = static_cast<int>(i % PIPE_STAGES);
+                if (i >= PIPE_STAGES && i - PIPE_STAGES < mine) { // retire the chunk held by stage s
+                    int64_t const j = i - PIPE_STAGES;
+                    if (!mbar_wait(&empty[s], static_cast<uint32_t>((j / PIPE_STAGES) & 1))) {
+                        atomicOr(a.status, ST_TIMEOUT);
+                        break;
+                    }
+                    if (a.write_back) {
+                        int64_t const  start = (blockIdx.x + j * gridDim.x) * PIPE_CHUNK;
+                        uint32_t const cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
+                        uint32_t const b8    = round16(cnt * 8);
+                        bulk_store(a.q1 + start, stage[s].q1, b8);
+                        bulk_store(a.vx + start, stage[s].vx, b8);
+                        bulk_store(a.vy + start, stage[s].vy, b8);
+                        bulk_store(a.vz + start, stage[s].vz, b8);
+                        if (BC == BCK_ABSORBING)
+                            bulk_store(a.w + start, stage[s].w, b8);
+                        bulk_commit();
+                    }
+                    bulk_wait_read_all();
+                }
+                if (i < mine) {
+                    int64_t const  start = (blockIdx.x + i * gridDim.x) * PIPE_CHUNK;
+                    uint32_t const cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
+                    uint32_t const b8 = round16(cnt * 8), b4 = round16(cnt * 4);
+                    mbar_arrive_expect_tx(&full[s], 5 * b8 + (load_pid ? b4 : 0));
+                    bulk_load(stage[s].q1, a.q1 + start, b8, &full[s]);
+                    bulk_load(stage[s].vx, a.vx + start, b8, &full[s]);
+                    bulk_load(stage[s].vy, a.vy + start, b8, &full[s]);
+                    bulk_load(stage[s].vz, a.vz + start, b8, &full[s]);
+                    bulk_load(stage[s].w, a.w + start, b8, &full[s]);
+                    if (load_pid)
+                        bulk_load(stage[s].pid, a.pid + start, b4, &full[s]);
+                }
+            }
+            bulk_wait_all();
+        }
         return;
-
-    // warp-uniform window base from the first particle of every lane
-    int first = 0x7fffffff;
-    if (chunk0 + lane < a.n) {
-        Shape<O> const sh = make_shape<O>(a.q1[chunk0 + lane] - a.half_min);
-        first             = sh.i0;
     }
-    int const base = __reduce_min_sync(0xffffffffu, first) - 1;
 
-    Acc<O, S> acc0, acc1;
-    acc_zero(acc0);
-    acc_zero(acc1);
+    // ---------------- consumers ----------------
     unsigned bad = 0;
-
-    for (int k = 0; k < a.ppt; ++k) {
-        int64_t const idx = chunk0 + static_cast<int64_t>(k) * 32 + lane;
-        if (idx >= a.n)
+    for (int64_t i = 0; i < mine; ++i) {
+        int const s = static_cast<int>(i % PIPE_STAGES);
+        if (!mbar_wait(&full[s], static_cast<uint32_t>((i / PIPE_STAGES) & 1))) {
+            bad |= ST_TIMEOUT;
             break;
-        double   q1 = a.q1[idx];
-        d3       v  = { a.vx[idx], a.vy[idx], a.vz[idx] };
-        double   w  = a.w[idx];
-        int32_t  pid = a.pid[idx];
-        bool     alive = true;
+        }
+        int64_t const start = (blockIdx.x + i * gridDim.x) * PIPE_CHUNK;
+        int const     cnt   = static_cast<int>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
+        PipeStage    &P     = stage[s];
+        int const     w0    = warp * 32 * PIPE_PPT;
 
-        if (a.move_steps == 2) { // PC: first half step
-            double const moved = move<MIRROR>(a, q1, v.x, 0.5 * a.dt);
-            if (static_cast<long long>(moved) != 0)
-                bad |= ST_MOVED_TOO_FAR;
-            alive = boundary<BC>(a, q1, v, pid, a.counter);
-            if (!alive) { // absorbed: park the particle with zero weight; the next sort drops it
-                w  = 0;
-                q1 = a.full_min + 0.5;
-                v  = { 0, 0, 0 };
+        // pass 1: push, deposit at x^N, move, boundary
+        {
+            int const  base = window_base<O>(P.q1, w0, lane, cnt, a.half_min);
+            Acc<O, S>  acc;
+            acc_zero(acc);
+#pragma unroll 1
+            for (int k = 0; k < PIPE_PPT; ++k) {
+                int const idx = w0 + k * 32 + lane;
+                if (idx >= cnt)
+                    break;
+                double  q1    = P.q1[idx];
+                d3      v     = { P.vx[idx], P.vy[idx], P.vz[idx] };
+                double  w     = P.w[idx];
+                int32_t pid   = load_pid ? P.pid[idx] : 0;
+                bool    alive = true;
+                if (a.move_steps == 2) {
+                    double const moved = move<MIRROR>(a, q1, v.x, 0.5 * a.dt);
+                    if (static_cast<long long>(moved) != 0)
+                        bad |= ST_MOVED_TOO_FAR;
+                    alive = boundary<BC>(a, q1, v, pid, a.counter);
+                    if (!alive)
+                        w = 0, q1 = a.full_min + 0.5, v = { 0, 0, 0 };
+                }
+                Shape<O> const sh = make_shape<O>(q1 - a.half_min);
+                if (!stencil_ok(sh, a.Nx) || !(q1 == q1)) {
+                    bad |= ST_OUT_OF_RANGE;
+                    continue;
+                }
+                double c2 = 1;
+                if (alive && a.move_steps != 0) {
+                    d3 E, dB;
+                    interp_EB<O>(a.EB, sh, E, dB);
+                    d3 const B = background_B<MIRROR>(a, q1, v, c2) + dB;
+                    v          = boris_push(a.boris, v, B, E);
+                }
+                if (a.deposit_mask & 1)
+                    deposit<O, S, 0>(acc, base, sh, alive ? w : 0.0, v, a);
+                if (alive && a.move_steps != 0) {
+                    // contravariant q1-velocity v_x cos^2 / D1 at the position of the push (CurviBasis.h:65-69)
+                    double moved = (a.inv_D1 * c2) * v.x * (a.move_steps == 2 ? 0.5 * a.dt : a.dt);
+                    q1 += moved;
+                    moved *= a.travel_scale;
+                    if (static_cast<long long>(moved) != 0)
+                        bad |= ST_MOVED_TOO_FAR;
+                    alive = boundary<BC>(a, q1, v, pid, a.counter + (a.move_steps == 2 ? 1 : 0));
+                    if (!alive)
+                        w = 0, q1 = a.full_min + 0.5, v = { 0, 0, 0 };
+                }
+                P.q1[idx] = q1;
+                P.vx[idx] = v.x;
+                P.vy[idx] = v.y;
+                P.vz[idx] = v.z;
+                if (BC == BCK_ABSORBING)
+                    P.w[idx] = w;
             }
+            if (a.deposit_mask & 1)
+                flush_rs<O, S, 0>(acc, base, lane, a);
         }
-        Shape<O> const sh = make_shape<O>(q1 - a.half_min);
-        if (!stencil_ok(sh, a.Nx) || !(q1 == q1)) {
-            bad |= ST_OUT_OF_RANGE;
-            continue;
-        }
-        if (alive) {
-            d3 const B = background_B<MIRROR>(a, q1, v) + interp<O>(a.Bh, sh);
-            d3 const E = interp<O>(a.E, sh);
-            v          = boris_push(a.boris, v, B, E);
-        }
-        if (a.deposit_mask & 1)
-            deposit<O, S, 0>(acc0, base, sh, alive ? w : 0.0, v, a);
-        if (alive) {
-            double const moved = move<MIRROR>(a, q1, v.x, a.move_steps == 2 ? 0.5 * a.dt : a.dt);
-            if (static_cast<long long>(moved) != 0)
-                bad |= ST_MOVED_TOO_FAR;
-            alive = boundary<BC>(a, q1, v, pid, a.counter + (a.move_steps == 2 ? 1 : 0));
-            if (!alive) {
-                w  = 0;
-                q1 = a.full_min + 0.5;
-                v  = { 0, 0, 0 };
-            }
-        }
+        // pass 2: deposit at the end position
         if (a.deposit_mask & 2) {
-            Shape<O> const sh2 = make_shape<O>(q1 - a.half_min);
-            if (!stencil_ok(sh2, a.Nx) || !(q1 == q1))
-                bad |= ST_OUT_OF_RANGE;
-            else
-                deposit<O, S, 1>(acc1, base, sh2, w, v, a);
+            int const base = window_base<O>(P.q1, w0, lane, cnt, a.half_min);
+            Acc<O, S> acc;
+            acc_zero(acc);
+#pragma unroll 2
+            for (int k = 0; k < PIPE_PPT; ++k) {
+                int const idx = w0 + k * 32 + lane;
+                if (idx >= cnt)
+                    break;
+                double const   q1 = P.q1[idx];
+                Shape<O> const sh = make_shape<O>(q1 - a.half_min);
+                if (!stencil_ok(sh, a.Nx) || !(q1 == q1)) {
+                    bad |= ST_OUT_OF_RANGE;
+                    continue;
+                }
+                deposit<O, S, 1>(acc, base, sh, P.w[idx], d3{ P.vx[idx], P.vy[idx], P.vz[idx] }, a);
+            }
+            flush_rs<O, S, 1>(acc, base, lane, a);
         }
-        if (a.write_back) {
-            a.q1[idx] = q1;
-            a.vx[idx] = v.x;
-            a.vy[idx] = v.y;
-            a.vz[idx] = v.z;
-            if (BC == BCK_ABSORBING)
-                a.w[idx] = w;
-        }
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0)
+            mbar_arrive(&empty[s]);
     }
-    if (a.deposit_mask & 1)
-        flush<O, S, 0>(acc0, base, lane, a);
-    if (a.deposit_mask & 2)
-        flush<O, S, 1>(acc1, base, lane, a);
     bad = __reduce_or_sync(0xffffffffu, bad);
     if (bad && lane == 0)
         atomicOr(a.status, bad);

@@ -17,20 +17,26 @@ __global__ void iota_kernel(int32_t *pid, int64_t n)
 
 __device__ __forceinline__ int wrap(int i, int Nx) { return i < 0 ? i + Nx : i >= Nx ? i - Nx : i; }
 
-// boundary_pass of E and B (periodic ghost fill, Delegate.cc:159-170) and B on the half grid
-// (PartSpecies.cc:132-139; its last ghost stays NaN)
-__global__ void prep_fields_kernel(double *B, double *E, double *Bh, int Nx)
+// boundary_pass of E and B (periodic ghost fill, Delegate.cc:159-170) and the push record
+// {E, B on the half grid} (PartSpecies.cc:132-139; the last ghost's half-grid B stays NaN)
+__global__ void prep_fields_kernel(double *B, double *E, double *EB, int Nx)
 {
     int const i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x) - PAD;
     if (i >= Nx + PAD)
         return;
+    d3 const e = ld3(E, wrap(i, Nx));
+    double  *p = EB + 6 * i;
+    p[0] = e.x, p[1] = e.y, p[2] = e.z;
     if (i < Nx + PAD - 1) {
         d3 const b1 = ld3(B, wrap(i + 1, Nx)), b0 = ld3(B, wrap(i, Nx));
-        st3(Bh, i, (b1 + b0) * 0.5);
+        d3 const bh = (b1 + b0) * 0.5;
+        p[3] = bh.x, p[4] = bh.y, p[5] = bh.z;
+    } else {
+        p[3] = p[4] = p[5] = __longlong_as_double(0x7ff8000000000000LL);
     }
     if (i < 0 || i >= Nx) {
         st3(B, i, ld3(B, wrap(i, Nx)));
-        st3(E, i, ld3(E, wrap(i, Nx)));
+        st3(E, i, e);
     }
 }
 

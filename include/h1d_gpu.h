@@ -193,6 +193,7 @@ typedef struct h1d_profile {
     int64_t field_launches;
     int64_t kernel_launches;  /* every kernel this library launched while profiling */
     int64_t particles_pushed; /* sum over push launches of the particles each processed */
+    int64_t window_misses;    /* particle deposits that missed the register window of their warp */
 } h1d_profile;
 int h1d_profile_enable(h1d_run *run, int on); /* on != 0 also resets the counters */
 int h1d_profile_read(h1d_run *run, h1d_profile *out);

@@ -100,7 +100,7 @@ def test_large_random_state(gpu_lib, oracle_lib):
     """A synthetic state with more particles than the fixtures (seeded loader)."""
     from hfemic_b200.loader import initial_state
 
-    cfg = h.configs.parity_p2().replace(Nx=256, phase_retardation=(32, 1.0), amplitude_damping=(32, 0.2))
+    cfg = h.configs.parity_p2().replace(Nx=256, xi=0.01, phase_retardation=(32, 1.0), amplitude_damping=(32, 0.2))
     for k in cfg.kinetic:
         k.Nc = 200
     init = initial_state(cfg, seed=3)
