@@ -38,6 +38,78 @@ __device__ __forceinline__ d3 cross(d3 A, d3 B)
 __device__ __forceinline__ d3 ld3(double const *g, long i) { return { g[3 * i], g[3 * i + 1], g[3 * i + 2] }; }
 __device__ __forceinline__ void st3(double *g, long i, d3 v) { g[3 * i] = v.x, g[3 * i + 1] = v.y, g[3 * i + 2] = v.z; }
 
+// Exact floor / round-half-away-from-zero / ceil of |x| < 2^30 with their integer value, on the
+// FP64 pipe instead of the conversion unit: t = x + 1.5*2^52 holds x rounded to the nearest
+// integer (ties to even) in its low mantissa word, and t - 1.5*2^52 is that integer as a double;
+// one comparison then corrects the rounding direction.
+struct IntReal {
+    int    i;
+    double d;
+};
+__device__ __forceinline__ IntReal rint_magic(double x)
+{
+    double const M = 6755399441055744.0;
+    double const t = __dadd_rn(x, M);
+    return { __double2loint(t), __dsub_rn(t, M) };
+}
+__device__ __forceinline__ IntReal floor_ir(double x)
+{
+    IntReal r = rint_magic(x);
+    if (r.d > x)
+        r.i -= 1, r.d -= 1.0;
+    return r;
+}
+__device__ __forceinline__ IntReal ceil_ir(double x)
+{
+    IntReal r = rint_magic(x);
+    if (r.d < x)
+        r.i += 1, r.d += 1.0;
+    return r;
+}
+__device__ __forceinline__ IntReal round_ir(double x) // std::round: halves away from zero
+{
+    IntReal      r = rint_magic(x);
+    double const f = x - r.d; // exact
+    if (f == 0.5 && x > 0)
+        r.i += 1, r.d += 1.0;
+    else if (f == -0.5 && x < 0)
+        r.i -= 1, r.d -= 1.0;
+    return r;
+}
+
+// sin and cos of |x| <= pi/2 from their Taylor series through x^23 and x^24 (truncation error
+// below 1e-20), Horner in x^2; no range reduction is needed because |xi D1 q1| < pi/2 holds on the
+// whole domain (ParamSet.cc:25-29)
+__device__ __forceinline__ void sincos_taylor(double x, double &s, double &c)
+{
+    double const x2 = x * x;
+    double       ps = -3.868170170630684e-23;
+    ps              = fma(ps, x2, 1.9572941063391263e-20);
+    ps              = fma(ps, x2, -8.22063524662433e-18);
+    ps              = fma(ps, x2, 2.8114572543455206e-15);
+    ps              = fma(ps, x2, -7.647163731819816e-13);
+    ps              = fma(ps, x2, 1.6059043836821613e-10);
+    ps              = fma(ps, x2, -2.505210838544172e-08);
+    ps              = fma(ps, x2, 2.7557319223985893e-06);
+    ps              = fma(ps, x2, -0.0001984126984126984);
+    ps              = fma(ps, x2, 0.008333333333333333);
+    ps              = fma(ps, x2, -0.16666666666666666);
+    s               = fma(ps * x2, x, x);
+    double pc       = 1.6117375710961184e-24;
+    pc              = fma(pc, x2, -8.896791392450574e-22);
+    pc              = fma(pc, x2, 4.110317623312165e-19);
+    pc              = fma(pc, x2, -1.5619206968586225e-16);
+    pc              = fma(pc, x2, 4.779477332387385e-14);
+    pc              = fma(pc, x2, -1.1470745597729725e-11);
+    pc              = fma(pc, x2, 2.08767569878681e-09);
+    pc              = fma(pc, x2, -2.755731922398589e-07);
+    pc              = fma(pc, x2, 2.48015873015873e-05);
+    pc              = fma(pc, x2, -0.001388888888888889);
+    pc              = fma(pc, x2, 0.041666666666666664);
+    pc              = fma(pc, x2, -0.5);
+    c               = fma(pc, x2, 1.0);
+}
+
 // Shape<Order>: base index i0 and weights w[0..Order]
 template <int O>
 struct Shape {
@@ -49,22 +121,22 @@ __device__ __forceinline__ Shape<O> make_shape(double x)
 {
     Shape<O> s;
     if constexpr (O == 1) {
-        double const f = floor(x);
-        s.i0           = static_cast<int>(f);
-        s.w[1]         = x - f;
-        s.w[0]         = 1 - s.w[1];
+        IntReal const f = floor_ir(x);
+        s.i0            = f.i;
+        s.w[1]          = x - f.d;
+        s.w[0]          = 1 - s.w[1];
     } else if constexpr (O == 2) {
-        double const r = round(x); // half away from zero, as std::round
-        s.i0           = static_cast<int>(r) - 1;
-        double t       = r - x;
-        s.w[1]         = 0.75 - t * t;
+        IntReal const r = round_ir(x);
+        s.i0            = r.i - 1;
+        double t        = r.d - x;
+        s.w[1]          = 0.75 - t * t;
         t += 0.5;
         s.w[0] = 0.5 * (t * t);
         s.w[2] = 1 - (s.w[0] + s.w[1]);
     } else {
-        double const c = ceil(x);
-        s.i0           = static_cast<int>(c) - 2;
-        double const i0 = c - 2;
+        IntReal const c = ceil_ir(x);
+        s.i0            = c.i - 2;
+        double const i0 = c.d - 2;
         double       t  = 2 + (i0 - x);
         s.w[0]          = (1. / 6) * (t * t * t);
         t               = 2 - ((i0 + 3) - x);
@@ -75,6 +147,8 @@ __device__ __forceinline__ Shape<O> make_shape(double x)
     }
     return s;
 }
+// positions further than this from the grid are lost particles (NaN and Inf included)
+__device__ __forceinline__ bool finite_pos(double x) { return x > -1073741824.0 && x < 1073741824.0; }
 
 // Boris push constants (BorisPush.h:25-30)
 struct BorisK {

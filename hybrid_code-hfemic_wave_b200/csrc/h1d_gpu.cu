@@ -332,7 +332,7 @@ int launch_push(h1d_run *run, int s, PushArgs const &a)
     if (a.n == 0)
         return H1D_OK;
     int64_t const chunks = (a.n + PIPE_CHUNK - 1) / PIPE_CHUNK;
-    dim3 const    g(static_cast<unsigned>(std::min<int64_t>(chunks, static_cast<int64_t>(run->num_sms) * 3)));
+    dim3 const    g(static_cast<unsigned>(std::min<int64_t>(chunks, static_cast<int64_t>(run->num_sms) * PIPE_CTAS_PER_SM)));
     bool const    mirror = run->p.xi != 0;
     switch (run->p.kinetic[s].shape_order) {
     case 1: launch_push_o<1>(a, mirror, run->p.particle_bc, g, run->stream); break;
@@ -609,6 +609,23 @@ int finalize_moments(h1d_run *run)
     return H1D_OK;
 }
 
+__global__ void math_check_kernel(double const *x, int64_t n, double *out)
+{
+    int64_t const k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= n)
+        return;
+    double const v = x[k];
+    out[5 * k + 0] = floor_ir(v).d + 0.0 * floor_ir(v).i;
+    out[5 * k + 1] = static_cast<double>(round_ir(v).i);
+    out[5 * k + 2] = static_cast<double>(ceil_ir(v).i);
+    double s, c;
+    sincos_taylor(v, s, c);
+    out[5 * k + 3] = s;
+    out[5 * k + 4] = c;
+    if (floor_ir(v).d != static_cast<double>(floor_ir(v).i)) // integer and real parts must agree
+        out[5 * k + 0] = __longlong_as_double(0x7ff8000000000000LL);
+}
+
 } // namespace
 
 // ------------------------------------------------------------------------------------------------
@@ -636,6 +653,31 @@ char const *h1d_error_name(int status)
 }
 
 char const *h1d_status_string(h1d_run *run) { return run ? run->msg.c_str() : "null run"; }
+
+int h1d_math_check(double const *x, int64_t n, double *out)
+{
+    if (n < 0 || (n > 0 && (!x || !out)))
+        return H1D_ERR_INVALID_ARG;
+    if (n == 0)
+        return H1D_OK;
+    double *dx = nullptr, *dout = nullptr;
+    if (cudaMalloc(&dx, sizeof(double) * n) != cudaSuccess || cudaMalloc(&dout, sizeof(double) * 5 * n) != cudaSuccess) {
+        cudaFree(dx);
+        return H1D_ERR_OOM;
+    }
+    int st = H1D_OK;
+    if (cudaMemcpy(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+        st = H1D_ERR_CUDA;
+    if (st == H1D_OK) {
+        math_check_kernel<<<static_cast<unsigned>((n + 255) / 256), 256>>>(dx, n, dout);
+        if (cudaGetLastError() != cudaSuccess
+            || cudaMemcpy(out, dout, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+            st = H1D_ERR_CUDA;
+    }
+    cudaFree(dx);
+    cudaFree(dout);
+    return st;
+}
 
 int h1d_create(h1d_params const *params, h1d_run **out)
 {

@@ -126,7 +126,8 @@ template <bool MIRROR>
 __device__ __forceinline__ double contr_vx(PushArgs const &a, double q1, double vx)
 {
     if constexpr (MIRROR) {
-        double const c = cos(a.xiD1 * q1);
+        double s, c;
+        sincos_taylor(a.xiD1 * q1, s, c);
         return (a.inv_D1 * (c * c)) * vx;
     } else {
         return a.inv_D1 * vx;
@@ -181,7 +182,7 @@ __device__ __forceinline__ d3 background_B(PushArgs const &a, double q1, d3 v, d
 {
     if constexpr (MIRROR) {
         double s, c;
-        sincos(a.xiD1 * q1, &s, &c);
+        sincos_taylor(a.xiD1 * q1, s, c);
         c2               = c * c;
         double const ksc = a.xiO0_Oc * (s * c);
         return { a.O0 / c2, ksc * v.z, -ksc * v.y };
@@ -226,9 +227,11 @@ constexpr int PIPE_THREADS        = 32 * (PIPE_CONSUMER_WARPS + 1);
 constexpr int PIPE_PPT            = 4;
 constexpr int PIPE_CHUNK          = 32 * PIPE_CONSUMER_WARPS * PIPE_PPT;
 constexpr int PIPE_STAGES         = 3;
+constexpr int PIPE_CTAS_PER_SM    = 2;
 
 struct PipeStage {
     double  q1[PIPE_CHUNK], vx[PIPE_CHUNK], vy[PIPE_CHUNK], vz[PIPE_CHUNK], w[PIPE_CHUNK];
+    double  q1n[PIPE_CHUNK], wn[PIPE_CHUNK]; // position and weight after the move
     int32_t pid[PIPE_CHUNK];
 };
 constexpr size_t PIPE_SMEM = sizeof(PipeStage) * PIPE_STAGES + 2 * PIPE_STAGES * sizeof(uint64_t);
@@ -258,6 +261,7 @@ __device__ __forceinline__ double reduce_scatter(double (&x)[V], int lane)
     return v;
 }
 
+// add a warp's register window to the global moments: one atomic per (cell, quantity) and warp
 template <int O, int S, int D>
 __device__ __forceinline__ void flush_rs(Acc<O, S> const &acc, int base, int lane, PushArgs const &a)
 {
@@ -284,37 +288,71 @@ __device__ __forceinline__ void flush_rs(Acc<O, S> const &acc, int base, int lan
     }
 }
 
-// warp-uniform window base: the smallest stencil base index among the warp's particles
-template <int O>
-__device__ __forceinline__ int window_base(double const *q1s, int w0, int lane, int cnt, double half_min)
-{
-    int m = 0x7fffffff;
-#pragma unroll
-    for (int k = 0; k < PIPE_PPT; ++k) {
-        int const idx = w0 + k * 32 + lane;
-        if (idx < cnt) {
-            double const x = q1s[idx] - half_min;
-            if (x == x) {
-                int const i0 = make_shape<O>(x).i0;
-                m            = i0 < m ? i0 : m;
-            }
+// A warp's deposit window: register accumulators over cells [base, base + S), S = O + 1 + R,
+// kept across batches and chunks.  When a batch of 32 particles reaches past the window the warp
+// flushes it and re-bases it at the batch minimum; particles below the window (drift since the
+// last sort) deposit with direct atomics.
+template <int O, int R, int D>
+struct Window {
+    static constexpr int S    = O + 1 + R;
+    static constexpr int NONE = -0x40000000;
+    Acc<O, S> acc;
+    int       base;
+
+    __device__ __forceinline__ void init()
+    {
+        acc_zero(acc);
+        base = NONE;
+    }
+    // batch step: i0 is this lane's stencil base (valid lanes only)
+    __device__ __forceinline__ void prepare(bool valid, int i0, int lane, PushArgs const &a)
+    {
+        bool const above = valid && i0 > base + R;
+        if (__any_sync(0xffffffffu, above)) {
+            if (base != NONE)
+                flush_rs<O, S, D>(acc, base, lane, a);
+            acc_zero(acc);
+            base = __reduce_min_sync(0xffffffffu, valid ? i0 : 0x7fffffff);
         }
     }
-    return __reduce_min_sync(0xffffffffu, m);
-}
+    __device__ __forceinline__ void add(Shape<O> const &sh, double w, d3 v, PushArgs const &a)
+    {
+        deposit<O, S, D>(acc, base, sh, w, v, a);
+    }
+    __device__ __forceinline__ void finish(int lane, PushArgs const &a)
+    {
+        if (base != NONE)
+            flush_rs<O, S, D>(acc, base, lane, a);
+    }
+};
 
+// ------------------------------------------------------------------------------------------------
+// The particle pass.  Warp-specialised pipeline per CTA: one producer warp streams the CTA's
+// contiguous run of chunks (PIPE_CHUNK particles each) global -> shared with 1-D TMA bulk copies
+// completing on mbarriers (PIPE_STAGES deep) and bulk-stores the updated particles back;
+// PIPE_CONSUMER_WARPS warps compute.  A consumer warp owns 32 x PIPE_PPT consecutive
+// (cell-sorted) particles of each chunk and makes two passes over them in shared memory:
+// (1) push at x^N, deposit at x^N, move, boundary, results written in place; (2) deposit at the
+// new position.  Its two deposit windows persist across the chunks of the run.
+//
+// CAM-CL (move_steps == 1): push at x^N, deposit, move, BC, deposit.
+// Predictor-corrector (move_steps == 2, Domain_PC.cc:110-124, 169-181): half move, BC, push at
+// the half-step position, half move, BC, deposit.  move_steps == 0: deposit only
+// (Domain_PC.cc:36-44).
+// ------------------------------------------------------------------------------------------------
 template <int O, bool MIRROR, int BC>
-__global__ void __launch_bounds__(PIPE_THREADS, 3) push_kernel(PushArgs a)
+__global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(PushArgs a)
 {
-    constexpr int R = 3; // window of four stencil base cells: i0 in [base, base + 3]
-    constexpr int S = O + 1 + R;
+    constexpr int R = 2;
     extern __shared__ __align__(128) unsigned char smraw[];
     PipeStage    *stage = reinterpret_cast<PipeStage *>(smraw);
     uint64_t     *full  = reinterpret_cast<uint64_t *>(smraw + sizeof(PipeStage) * PIPE_STAGES);
     uint64_t     *empty = full + PIPE_STAGES;
     int const     warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int64_t const nchunks = (a.n + PIPE_CHUNK - 1) / PIPE_CHUNK;
-    int64_t const mine    = blockIdx.x < nchunks ? (nchunks - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    int64_t const per     = (nchunks + gridDim.x - 1) / gridDim.x;
+    int64_t const c0      = static_cast<int64_t>(blockIdx.x) * per;
+    int64_t const mine    = c0 < nchunks ? min(per, nchunks - c0) : 0;
     bool const    load_pid = a.randomize != 0;
 
     if (threadIdx.x == 0) {
@@ -337,21 +375,21 @@ __global__ void __launch_bounds__(PIPE_THREADS, 3) push_kernel(PushArgs a)
                         break;
                     }
                     if (a.write_back) {
-                        int64_t const  start = (blockIdx.x + j * gridDim.x) * PIPE_CHUNK;
+                        int64_t const  start = (c0 + j) * PIPE_CHUNK;
                         uint32_t const cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
                         uint32_t const b8    = round16(cnt * 8);
-                        bulk_store(a.q1 + start, stage[s].q1, b8);
+                        bulk_store(a.q1 + start, stage[s].q1n, b8);
                         bulk_store(a.vx + start, stage[s].vx, b8);
                         bulk_store(a.vy + start, stage[s].vy, b8);
                         bulk_store(a.vz + start, stage[s].vz, b8);
                         if (BC == BCK_ABSORBING)
-                            bulk_store(a.w + start, stage[s].w, b8);
+                            bulk_store(a.w + start, stage[s].wn, b8);
                         bulk_commit();
                     }
                     bulk_wait_read_all();
                 }
                 if (i < mine) {
-                    int64_t const  start = (blockIdx.x + i * gridDim.x) * PIPE_CHUNK;
+                    int64_t const  start = (c0 + i) * PIPE_CHUNK;
                     uint32_t const cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
                     uint32_t const b8 = round16(cnt * 8), b4 = round16(cnt * 4);
                     mbar_arrive_expect_tx(&full[s], 5 * b8 + (load_pid ? b4 : 0));
@@ -370,101 +408,120 @@ __global__ void __launch_bounds__(PIPE_THREADS, 3) push_kernel(PushArgs a)
     }
 
     // ---------------- consumers ----------------
-    unsigned bad = 0;
+    unsigned        bad = 0;
+    Window<O, R, 0> win0;
+    Window<O, R, 1> win1;
+    win0.init();
+    win1.init();
     for (int64_t i = 0; i < mine; ++i) {
         int const s = static_cast<int>(i % PIPE_STAGES);
         if (!mbar_wait(&full[s], static_cast<uint32_t>((i / PIPE_STAGES) & 1))) {
             bad |= ST_TIMEOUT;
             break;
         }
-        int64_t const start = (blockIdx.x + i * gridDim.x) * PIPE_CHUNK;
+        int64_t const start = (c0 + i) * PIPE_CHUNK;
         int const     cnt   = static_cast<int>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
         PipeStage    &P     = stage[s];
         int const     w0    = warp * 32 * PIPE_PPT;
 
-        // pass 1: push, deposit at x^N, move, boundary
-        {
-            int const  base = window_base<O>(P.q1, w0, lane, cnt, a.half_min);
-            Acc<O, S>  acc;
-            acc_zero(acc);
-#pragma unroll 1
-            for (int k = 0; k < PIPE_PPT; ++k) {
-                int const idx = w0 + k * 32 + lane;
-                if (idx >= cnt)
-                    break;
-                double  q1    = P.q1[idx];
-                d3      v     = { P.vx[idx], P.vy[idx], P.vz[idx] };
-                double  w     = P.w[idx];
-                int32_t pid   = load_pid ? P.pid[idx] : 0;
-                bool    alive = true;
-                if (a.move_steps == 2) {
-                    double const moved = move<MIRROR>(a, q1, v.x, 0.5 * a.dt);
-                    if (static_cast<long long>(moved) != 0)
-                        bad |= ST_MOVED_TOO_FAR;
-                    alive = boundary<BC>(a, q1, v, pid, a.counter);
-                    if (!alive)
-                        w = 0, q1 = a.full_min + 0.5, v = { 0, 0, 0 };
-                }
-                Shape<O> const sh = make_shape<O>(q1 - a.half_min);
-                if (!stencil_ok(sh, a.Nx) || !(q1 == q1)) {
-                    bad |= ST_OUT_OF_RANGE;
-                    continue;
-                }
-                double c2 = 1;
+        // pass A: push at x^N (half steps around it for PC), move, boundary; no warp collectives,
+        // so the compiler interleaves the independent particles of a lane.  Slots past `cnt` hold
+        // stale finite data and are processed but never deposited or stored.
+#pragma unroll 2
+        for (int k = 0; k < PIPE_PPT; ++k) {
+            int const idx   = w0 + k * 32 + lane;
+            double    q1    = P.q1[idx];
+            d3        v     = { P.vx[idx], P.vy[idx], P.vz[idx] };
+            double    w     = P.w[idx];
+            int32_t   pid   = load_pid ? P.pid[idx] : 0;
+            bool      alive = true;
+            if (a.move_steps == 2) {
+                double const moved = move<MIRROR>(a, q1, v.x, 0.5 * a.dt);
+                if (idx < cnt && !(fabs(moved) < 1.0)) // long(moved * scale) != 0 (PartSpecies.cc:261)
+                    bad |= ST_MOVED_TOO_FAR;
+                alive = boundary<BC>(a, q1, v, pid, a.counter);
+                if (!alive)
+                    w = 0, q1 = a.full_min + 0.5, v = { 0, 0, 0 };
+                P.q1[idx] = q1; // PC deposits nothing at the push position
+            }
+            Shape<O> const sh = make_shape<O>(q1 - a.half_min);
+            if (finite_pos(q1) && stencil_ok(sh, a.Nx)) {
                 if (alive && a.move_steps != 0) {
                     d3 E, dB;
                     interp_EB<O>(a.EB, sh, E, dB);
+                    double   c2;
                     d3 const B = background_B<MIRROR>(a, q1, v, c2) + dB;
                     v          = boris_push(a.boris, v, B, E);
-                }
-                if (a.deposit_mask & 1)
-                    deposit<O, S, 0>(acc, base, sh, alive ? w : 0.0, v, a);
-                if (alive && a.move_steps != 0) {
                     // contravariant q1-velocity v_x cos^2 / D1 at the position of the push (CurviBasis.h:65-69)
                     double moved = (a.inv_D1 * c2) * v.x * (a.move_steps == 2 ? 0.5 * a.dt : a.dt);
                     q1 += moved;
                     moved *= a.travel_scale;
-                    if (static_cast<long long>(moved) != 0)
+                    if (idx < cnt && !(fabs(moved) < 1.0))
                         bad |= ST_MOVED_TOO_FAR;
+                    d3 const v_push = v;
                     alive = boundary<BC>(a, q1, v, pid, a.counter + (a.move_steps == 2 ? 1 : 0));
                     if (!alive)
                         w = 0, q1 = a.full_min + 0.5, v = { 0, 0, 0 };
+                    // the deposit at x^N uses the velocity before the boundary pass: a particle the
+                    // boundary reflected or removed deposits it here and is skipped by pass B
+                    if ((a.deposit_mask & 1) && (v.x != v_push.x || v.y != v_push.y || v.z != v_push.z)) {
+                        if (idx < cnt) {
+                            double const vw[4] = { P.w[idx], v_push.x * P.w[idx], v_push.y * P.w[idx], v_push.z * P.w[idx] };
+#pragma unroll
+                            for (int j = 0; j <= O; ++j)
+#pragma unroll
+                                for (int q = 0; q < 4; ++q)
+                                    atomicAdd(a.dep[0][q] + sh.i0 + j, vw[q] * sh.w[j]);
+                        }
+                        P.q1[idx] = __longlong_as_double(0x7ff8000000000000LL);
+                    }
                 }
-                P.q1[idx] = q1;
-                P.vx[idx] = v.x;
-                P.vy[idx] = v.y;
-                P.vz[idx] = v.z;
-                if (BC == BCK_ABSORBING)
-                    P.w[idx] = w;
+            } else if (idx < cnt) {
+                bad |= ST_OUT_OF_RANGE;
             }
-            if (a.deposit_mask & 1)
-                flush_rs<O, S, 0>(acc, base, lane, a);
+            P.q1n[idx] = q1;
+            P.vx[idx]  = v.x;
+            P.vy[idx]  = v.y;
+            P.vz[idx]  = v.z;
+            if (BC == BCK_ABSORBING)
+                P.wn[idx] = w;
         }
-        // pass 2: deposit at the end position
-        if (a.deposit_mask & 2) {
-            int const base = window_base<O>(P.q1, w0, lane, cnt, a.half_min);
-            Acc<O, S> acc;
-            acc_zero(acc);
-#pragma unroll 2
+        __syncwarp();
+        // pass B: deposit at x^N with v^{N+1/2} (CAM-CL)
+        if (a.deposit_mask & 1) {
+#pragma unroll 1
             for (int k = 0; k < PIPE_PPT; ++k) {
-                int const idx = w0 + k * 32 + lane;
-                if (idx >= cnt)
-                    break;
-                double const   q1 = P.q1[idx];
-                Shape<O> const sh = make_shape<O>(q1 - a.half_min);
-                if (!stencil_ok(sh, a.Nx) || !(q1 == q1)) {
-                    bad |= ST_OUT_OF_RANGE;
-                    continue;
-                }
-                deposit<O, S, 1>(acc, base, sh, P.w[idx], d3{ P.vx[idx], P.vy[idx], P.vz[idx] }, a);
+                int const      idx   = w0 + k * 32 + lane;
+                double const   q1    = P.q1[idx];
+                Shape<O> const sh    = make_shape<O>(q1 - a.half_min);
+                bool const     valid = idx < cnt && finite_pos(q1) && stencil_ok(sh, a.Nx);
+                win0.prepare(valid, sh.i0, lane, a);
+                if (valid)
+                    win0.add(sh, P.w[idx], d3{ P.vx[idx], P.vy[idx], P.vz[idx] }, a);
             }
-            flush_rs<O, S, 1>(acc, base, lane, a);
+        }
+        // pass C: deposit at the end position
+        if (a.deposit_mask & 2) {
+#pragma unroll 1
+            for (int k = 0; k < PIPE_PPT; ++k) {
+                int const      idx   = w0 + k * 32 + lane;
+                double const   q1    = P.q1n[idx];
+                Shape<O> const sh    = make_shape<O>(q1 - a.half_min);
+                bool const     valid = idx < cnt && finite_pos(q1) && stencil_ok(sh, a.Nx);
+                win1.prepare(valid, sh.i0, lane, a);
+                if (valid)
+                    win1.add(sh, BC == BCK_ABSORBING ? P.wn[idx] : P.w[idx], d3{ P.vx[idx], P.vy[idx], P.vz[idx] }, a);
+            }
         }
         fence_proxy_async_smem();
         __syncwarp();
         if (lane == 0)
             mbar_arrive(&empty[s]);
     }
+    if (a.deposit_mask & 1)
+        win0.finish(lane, a);
+    if (a.deposit_mask & 2)
+        win1.finish(lane, a);
     bad = __reduce_or_sync(0xffffffffu, bad);
     if (bad && lane == 0)
         atomicOr(a.status, bad);
@@ -505,7 +562,7 @@ __global__ void __launch_bounds__(256) moments_kernel(MomentArgs a)
             break;
         double const   q1 = a.q1[idx], vx = a.vx[idx], vy = a.vy[idx], vz = a.vz[idx], w = a.w[idx];
         Shape<1> const sh = make_shape<1>(q1 - a.half_min);
-        if (!stencil_ok(sh, a.Nx) || !(q1 == q1)) {
+        if (!finite_pos(q1) || !stencil_ok(sh, a.Nx)) {
             bad |= ST_OUT_OF_RANGE;
             continue;
         }

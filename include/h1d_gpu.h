@@ -198,6 +198,12 @@ typedef struct h1d_profile {
 int h1d_profile_enable(h1d_run *run, int on); /* on != 0 also resets the counters */
 int h1d_profile_read(h1d_run *run, h1d_profile *out);
 
+/* Evaluate the device arithmetic primitives of the particle kernels on the current device, for
+ * self-checks against the host C library: for each x[k] (|x| < 2^30) writes
+ * out[5k .. 5k+4] = floor(x), round(x) (halves away from zero), ceil(x), and for |x| <= pi/2
+ * sin(x), cos(x) as computed by the kernels. */
+int h1d_math_check(const double *x, int64_t n, double *out);
+
 const char *h1d_status_string(h1d_run *run);
 const char *h1d_error_name(int status);
 

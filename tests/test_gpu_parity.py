@@ -130,3 +130,36 @@ def test_invalid_params(gpu_lib):
     handle = ctypes.c_void_p()
     assert fn["create"](ctypes.byref(p), ctypes.byref(handle)) == h.abi.ERR_INVALID_ARG
     assert not handle.value
+
+
+def test_device_rounding_and_trig(gpu_lib):
+    """The kernels' exact floor / round / ceil (no conversion unit) equal the C library's on
+    random, half-integer, integer and near-integer arguments; their Taylor sin/cos on
+    [-pi/2, pi/2] are within 4e-16 (absolute) of the C library's."""
+    import ctypes
+
+    rng = np.random.default_rng(7)
+    x = np.concatenate([
+        rng.uniform(-5000, 5000, 200000),
+        np.arange(-4000, 4000) + 0.5,
+        np.arange(-4000, 4000, dtype=float),
+        np.nextafter(np.arange(-100, 100, dtype=float), np.inf),
+        np.nextafter(np.arange(-100, 100, dtype=float), -np.inf),
+        np.nextafter(np.arange(-100, 100, dtype=float) + 0.5, np.inf),
+        np.nextafter(np.arange(-100, 100, dtype=float) + 0.5, -np.inf),
+        [0.0, -0.0, 0.49999999999999994, -0.49999999999999994],
+    ])
+    lib = ctypes.CDLL(gpu_lib)
+    dp = ctypes.POINTER(ctypes.c_double)
+    lib.h1d_math_check.argtypes = [dp, ctypes.c_int64, dp]
+    out = np.empty((x.size, 5))
+    assert lib.h1d_math_check(x.ctypes.data_as(dp), x.size, out.ctypes.data_as(dp)) == 0
+    np.testing.assert_array_equal(out[:, 0], np.floor(x))
+    away = np.where(np.abs(x - np.trunc(x)) == 0.5, np.trunc(x) + np.sign(x), np.round(x))  # std::round
+    np.testing.assert_array_equal(out[:, 1], away)
+    np.testing.assert_array_equal(out[:, 2], np.ceil(x))
+    t = np.concatenate([rng.uniform(-np.pi / 2, np.pi / 2, 100000), [0.0, np.pi / 2, -np.pi / 2, 1e-300]])
+    out = np.empty((t.size, 5))
+    assert lib.h1d_math_check(t.ctypes.data_as(dp), t.size, out.ctypes.data_as(dp)) == 0
+    assert np.max(np.abs(out[:, 3] - np.sin(t))) <= 4e-16
+    assert np.max(np.abs(out[:, 4] - np.cos(t))) <= 4e-16
