@@ -10,6 +10,7 @@
 #include "launchers.h"
 
 #include <cmath>
+#include <mutex>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -626,6 +627,34 @@ __global__ void math_check_kernel(double const *x, int64_t n, double *out)
         out[5 * k + 0] = __longlong_as_double(0x7ff8000000000000LL);
 }
 
+// Fixed scratch of h1d_collect_moments_noalloc: raw sums (10 x M), finalized moments (10 x M) and a
+// status word.  Host code must not use the symbol as a pointer; it looks up the device address
+// with cudaGetSymbolAddress, once per device.
+constexpr int64_t NOALLOC_M = H1D_NOALLOC_MAX_NX + 2 * PAD;
+static __device__ __align__(256) double noalloc_scratch[20 * NOALLOC_M + 2];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex    noalloc_mutex;
+double       *noalloc_addr[NOALLOC_MAX_DEVICES] = {};
+
+int noalloc_scratch_address(double **out)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return H1D_ERR_NO_DEVICE;
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES)
+        return H1D_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(noalloc_mutex);
+    if (!noalloc_addr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, noalloc_scratch) != cudaSuccess || !p)
+            return H1D_ERR_CUDA;
+        noalloc_addr[dev] = static_cast<double *>(p);
+    }
+    *out = noalloc_addr[dev];
+    return H1D_OK;
+}
+
 } // namespace
 
 // ------------------------------------------------------------------------------------------------
@@ -677,6 +706,59 @@ int h1d_math_check(double const *x, int64_t n, double *out)
     cudaFree(dx);
     cudaFree(dout);
     return st;
+}
+
+int h1d_collect_moments_noalloc(int64_t Nx, double moment_norm, int particle_bc, double const *q1, double const *vx,
+                                double const *vy, double const *vz, double const *w, int64_t n, double *n_out,
+                                double *nV_out, double *nvv_out, void *stream)
+{
+    if (Nx < 2 * PAD || Nx > H1D_NOALLOC_MAX_NX) {
+        std::fprintf(stderr, "h1d_collect_moments_noalloc: Nx = %lld is outside [%d, %d], the size of its fixed scratch\n",
+                     static_cast<long long>(Nx), 2 * PAD, H1D_NOALLOC_MAX_NX);
+        return H1D_ERR_INVALID_ARG;
+    }
+    if (!(moment_norm > 0) || n < 0 || n > (int64_t{ 1 } << 31) - 1 || particle_bc < 0 || particle_bc > 2
+        || (n > 0 && (!q1 || !vx || !vy || !vz || !w)) || !n_out || !nV_out || !nvv_out)
+        return H1D_ERR_INVALID_ARG;
+    double *scratch = nullptr;
+    if (int const st = noalloc_scratch_address(&scratch))
+        return st;
+    cudaStream_t const st     = static_cast<cudaStream_t>(stream);
+    int64_t const      M      = Nx + 2 * PAD;
+    double            *raw    = scratch;
+    double            *fin    = scratch + 10 * M;
+    unsigned          *status = reinterpret_cast<unsigned *>(scratch + 20 * NOALLOC_M);
+    // the raw sums are accumulated with atomics and must start at zero, as must the status word
+    if (cudaMemsetAsync(raw, 0, sizeof(double) * 10 * M, st) != cudaSuccess
+        || cudaMemsetAsync(status, 0, sizeof(unsigned), st) != cudaSuccess)
+        return H1D_ERR_CUDA;
+    if (n > 0) {
+        MomentArgs a{};
+        a.q1 = q1, a.vx = vx, a.vy = vy, a.vz = vz, a.w = w, a.n = n, a.Nx = static_cast<int>(Nx);
+        double const ppc = static_cast<double>(n) / static_cast<double>(Nx);
+        a.ppt            = ppc < 128 ? 1 : ppc >= 16 * 128 ? 16 : static_cast<int>(ppc / 128);
+        a.half_min       = -0.5 * static_cast<double>(Nx) + 0.5;
+        a.status         = status;
+        for (int q = 0; q < 10; ++q)
+            a.out[q] = raw + static_cast<int64_t>(q) * M + PAD;
+        int64_t const chunks = (n + 32LL * a.ppt - 1) / (32LL * a.ppt);
+        moments_kernel<<<static_cast<unsigned>((chunks + 7) / 8), 256, 0, st>>>(a);
+        if (cudaGetLastError() != cudaSuccess)
+            return H1D_ERR_CUDA;
+    }
+    if (launch_finalize_kinetic(raw, fin, static_cast<int>(Nx), 1.0 / moment_norm, particle_bc == H1D_BC_PERIODIC ? 0 : 1, st)
+            != cudaSuccess
+        || cudaMemcpyAsync(n_out, fin, sizeof(double) * M, cudaMemcpyDeviceToDevice, st) != cudaSuccess
+        || cudaMemcpyAsync(nV_out, fin + M, sizeof(double) * 3 * M, cudaMemcpyDeviceToDevice, st) != cudaSuccess
+        || cudaMemcpyAsync(nvv_out, fin + 4 * M, sizeof(double) * 6 * M, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        return H1D_ERR_CUDA;
+    unsigned hstatus = 0;
+    if (cudaMemcpyAsync(&hstatus, status, sizeof hstatus, cudaMemcpyDeviceToHost, st) != cudaSuccess
+        || cudaStreamSynchronize(st) != cudaSuccess)
+        return H1D_ERR_CUDA;
+    if (hstatus & ST_OUT_OF_RANGE)
+        return H1D_ERR_NAN;
+    return hstatus ? H1D_ERR_CUDA : H1D_OK;
 }
 
 int h1d_create(h1d_params const *params, h1d_run **out)

@@ -204,6 +204,31 @@ int h1d_profile_read(h1d_run *run, h1d_profile *out);
  * sin(x), cos(x) as computed by the kernels. */
 int h1d_math_check(const double *x, int64_t n, double *out);
 
+/* Allocation-free moment collection.  No counterpart in the reference: it is an addition for
+ * callers that cannot call cudaMalloc -- for example code running inside an application whose
+ * own pool allocator has reserved the device memory (an allocation outside the pool fails or
+ * defeats its accounting), or a latency-critical loop where an allocation, which may
+ * synchronise the device, is not acceptable.
+ *
+ * Computes what h1d_download_moments returns -- n, nV, nvv with the CIC shape, scaled by
+ * 1/moment_norm and ghost-folded for the given particle boundary (PartSpecies::collect_all +
+ * boundary_gather) -- from particles the caller holds in device memory, into device buffers the
+ * caller provides (GridArray layout: n[Nx+6], nV[(Nx+6)*3], nvv[(Nx+6)*6]).  Work is enqueued on
+ * `stream` (a cudaStream_t; NULL for the legacy default stream) and the call returns after that
+ * stream has finished it.
+ *
+ * Scratch space is a fixed array compiled into this library (a static __device__ array of
+ * 20 * (H1D_NOALLOC_MAX_NX + 6) doubles plus a status word, about 0.65 MB, held on every GPU that
+ * loads the library until the process exits).  Nx above H1D_NOALLOC_MAX_NX is rejected with
+ * H1D_ERR_INVALID_ARG.  The first call on a device looks up that array's device address (once per
+ * device, with the device current); make that first call before any stream capture.  All calls
+ * share the one array: calls that overlap on the GPU (concurrent streams or threads) race and
+ * must be serialised by the caller. */
+#define H1D_NOALLOC_MAX_NX 4096
+int h1d_collect_moments_noalloc(int64_t Nx, double moment_norm, int particle_bc, const double *q1, const double *vx,
+                                const double *vy, const double *vz, const double *w, int64_t n, double *n_out,
+                                double *nV_out, double *nvv_out, void *stream);
+
 const char *h1d_status_string(h1d_run *run);
 const char *h1d_error_name(int status);
 
