@@ -1,19 +1,25 @@
-"""Benchmark of the hybrid_1d hot path on B200: particle-steps/s of the plain FP64 GPU drop-in.
+"""Benchmark of the hybrid_1d hot path on B200: particle-steps/s, mixed precision against plain FP64.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config NAME]
+                    [--precision auto|fp64|mixed]
 
-Workload (default): the FP64 drop-in configuration -- mirror field xi=0.002, Nx=2048, masking
-over 128 cells at each end, reflecting particles, hot H+ and hot He+ with 1000 particles per
-cell each (TSC, 4.1M particles), dt=0.01, CAM-CL with 10 B subcycles.  One bench step is one
-CAM-CL cycle of every particle (push, two deposits, move, boundary, field cycle), cell sorts
-included.  Synthetic seeded bi-Maxwellian particles; 197 MB of particle state per GPU, larger
-than L2, so no flush is needed between steps.
+Workload (default): the config-1 plasma at Nx=4096 with 4000 particles per cell -- uniform B0,
+periodic, one kinetic H+ species (beta_par 0.1, T_perp/T_par 3, CIC; 16.4M particles) plus a
+cold H+ background, isothermal electrons, dt=0.02, CAM-CL with 10 B subcycles -- run with the
+mixed-precision particle pass (int32 cell + FP32 offset, FP32 velocity / interpolation / push,
+FP32 warp deposits summed into FP64 cells; FP64 field cycle).  One bench step is one CAM-CL
+cycle of every particle (push, two deposits, move, boundary, field cycle), cell sorts included.
+Beside it the same workload in plain FP64 (`fp64`), the mixed run's error against FP64 after
+100 steps from the same state (`error_vs_fp64`, wave energy, particle energy and moments), and
+the FP64 drop-in configuration (mirror field, Nx=2048, two TSC species, 4.1M particles,
+`drop_in_fp64`).  Synthetic seeded bi-Maxwellian particles; the particle state (459 MB mixed,
+722 MB FP64) is larger than L2, so no flush is needed between steps.
 
 Multi-GPU: every rank runs an independent replica of the workload (the path does not shard;
 no collective is used); value = particle-steps of all ranks / max-over-ranks device time.
 
 --impl reference times the reference's own CPU implementation of the same workload
-(oracle/_ref, compiled from the reference sources) with one process per host core, each
+(oracle/_ref, compiled from the reference sources, FP64) with one process per host core, each
 holding 1/P of the particles (PartSpecies::populate(color, divisor)); rank 0 only.
 """
 from __future__ import annotations
@@ -44,7 +50,14 @@ def _package():
 
 
 METRIC = "particle-steps/s"
-BYTES_PER_PARTICLE_STEP = 72  # FP64: read q1, vx, vy, vz, w (40 B), write q1, vx, vy, vz (32 B)
+# algorithmic HBM bytes per particle-step of the particle pass
+BYTES_PER_PARTICLE_STEP = {
+    "fp64": 72,   # read q1, vx, vy, vz, w (40 B), write q1, vx, vy, vz (32 B)
+    "mixed": 44,  # read cell, offset, vx, vy, vz, w (24 B), write cell, offset, vx, vy, vz (20 B)
+}
+STATE_BYTES = {"fp64": 44, "mixed": 28}  # stored bytes per particle, id included
+KERNEL = {"fp64": "push_kernel (fused push + 2 deposits + move + BC, FP64)",
+          "mixed": "push_kernel_mixed (fused push + 2 deposits + move + BC, FP32 with int32 cell)"}
 
 
 def measured_peak():
@@ -116,21 +129,24 @@ def workload(h, name):
 
 
 def cpu_baseline_reference(cfg, budget_s=20.0):
-    """The reference binary (oracle/_ref) on one core for a bounded number of steps."""
+    """The reference binary (oracle/_ref) on one core for a bounded number of steps, holding
+    1/divisor of the particles (PartSpecies::populate(0, divisor)) so that loading stays short."""
     drv = os.path.join(ROOT, "oracle", "_ref", cfg.name, "ref_driver")
     if not os.path.exists(drv):
         return None
+    div = max(1, cfg.n_particles // 1_000_000)
+    args = [] if div == 1 else ["0", str(div)]
     steps = 2
-    out = subprocess.run([drv, "bench", str(steps)], capture_output=True, text=True, timeout=600)
+    out = subprocess.run([drv, "bench", str(steps), *args], capture_output=True, text=True, timeout=600)
     r = json.loads(out.stdout.strip().splitlines()[-1])
     per_step = r["advance_s"] / steps
-    steps = max(2, min(60, int(budget_s / max(per_step, 1e-6))))
+    steps = max(2, min(200, int(budget_s / max(per_step, 1e-6))))
     if steps > 2:
-        out = subprocess.run([drv, "bench", str(steps)], capture_output=True, text=True, timeout=600)
+        out = subprocess.run([drv, "bench", str(steps), *args], capture_output=True, text=True, timeout=600)
         r = json.loads(out.stdout.strip().splitlines()[-1])
     return {"value": r["particle_steps_per_s"], "unit": METRIC, "cores": 1, "kind": "reference",
-            "sample": f"{cfg.name}: {r['particles']} particles x {r['steps']} steps of Domain_CAMCL::advance_by "
-                      f"({r['advance_s']:.1f} s, loader excluded), one core"}
+            "sample": f"{cfg.name} with 1/{div} of the particles: {r['particles']} particles x {r['steps']} steps of "
+                      f"Domain_CAMCL::advance_by ({r['advance_s']:.1f} s, loader excluded), one core, FP64"}
 
 
 def cpu_baseline_port(h, cfg, budget_s=15.0):
@@ -185,15 +201,199 @@ def run_reference_arm(args, h, rank):
     print(json.dumps(line))
 
 
+def precision_name(cfg, h):
+    return "mixed" if cfg.precision == h.configs.PREC_MIXED else "fp64"
+
+
+class TimedRun:
+    """A run behind the C-ABI with its stream, for device-timed advances."""
+
+    def __init__(self, h, cfg, st):
+        import ctypes
+
+        import torch
+
+        self.h, self.cfg = h, cfg
+        self.run = h.open_run(cfg)
+        lib = self.lib = self.run.lib
+        lib.h1d_advance_async.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
+        lib.h1d_synchronize.argtypes = [ctypes.c_void_p]
+        lib.h1d_get_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+        lib.h1d_profile_enable.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        lib.h1d_profile_read.argtypes = [ctypes.c_void_p, ctypes.POINTER(h.abi.Profile)]
+        self.run.upload_state(st)
+        sp = ctypes.c_void_p()
+        self.run._check(lib.h1d_get_stream(self.run.h, ctypes.byref(sp)))
+        self.stream = torch.cuda.ExternalStream(sp.value)
+        self.n_particles = sum(p["q1"].size for p in st["particles"])
+
+    def advance(self, n):
+        self.run._check(self.lib.h1d_advance_async(self.run.h, n))
+        self.run._check(self.lib.h1d_synchronize(self.run.h))
+
+    def timed(self, steps, world=1, clocks_index=None):
+        """Device time (ms) of `steps` steps, max over ranks, with the library's phase profile."""
+        import ctypes
+
+        import torch
+        import torch.distributed as dist
+
+        r, lib = self.run, self.lib
+        r._check(lib.h1d_profile_enable(r.h, 1))
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clk = ClockSampler(clocks_index) if clocks_index is not None else None
+        if clk:
+            clk.__enter__()
+        try:
+            start.record(self.stream)
+            r._check(lib.h1d_advance_async(r.h, steps))
+            end.record(self.stream)
+            r._check(lib.h1d_synchronize(r.h))
+            torch.cuda.synchronize()
+        finally:
+            if clk:
+                clk.__exit__(None, None, None)
+        ms = start.elapsed_time(end)
+        prof = self.h.abi.Profile()
+        r._check(lib.h1d_profile_read(r.h, ctypes.byref(prof)))
+        r._check(lib.h1d_profile_enable(r.h, 0))
+        if world > 1:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            dist.barrier()
+        return ms, prof, (clk.summary() if clk else None)
+
+    def close(self):
+        self.run.close()
+
+
+def roofline_of(prof, precision, steps, traffic_table):
+    """Roofline of the dominant kernel (the particle pass): algorithmic bytes per launch over its
+    average launch time (CUDA events on the run's stream around every launch)."""
+    peak, peak_kind = measured_peak()
+    B = BYTES_PER_PARTICLE_STEP[precision]
+    push_avg_ms = prof.push_ms / max(prof.push_launches, 1)
+    bytes_per_launch = B * prof.particles_pushed / max(prof.push_launches, 1)
+    achieved = bytes_per_launch / (push_avg_ms / 1e3) / 1e9
+    traffic = None
+    tr = traffic_table.get(precision)
+    if tr:
+        traffic = tr["bytes_per_particle"] * bytes_per_launch / B
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "kernel": KERNEL[precision], "peak_kind": peak_kind,
+            "bytes_per_particle_step": B, "bytes_per_launch": bytes_per_launch, "launch_ms": push_avg_ms,
+            "window_miss_rate": prof.window_misses / max(2 * prof.particles_pushed, 1),
+            "phase_ms_per_step": {"push": prof.push_ms / steps, "sort": prof.sort_ms / steps,
+                                  "field": prof.field_ms / steps}}
+
+
+def load_traffic():
+    path = os.path.join(ROOT, "profiles", "push_kernel_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def error_vs_fp64(h, cfg, st, steps=100):
+    """Max-norm relative error of the mixed run against the FP64 run after `steps` steps from the
+    same state: wave energy (dB^2/2, dE^2/2 per component), particle energies and the moments."""
+    import numpy as np
+
+    out = {}
+    for prec in (h.configs.PREC_FP64, h.configs.PREC_MIXED):
+        with h.open_run(cfg.replace(precision=prec)) as r:
+            r.upload_state(st)
+            r.advance(steps)
+            e = r.energy()
+            mom = [r.moments(s) for s in range(len(cfg.kinetic))]
+            out[prec] = (e, mom)
+    (e0, m0), (e1, m1) = out[h.configs.PREC_FP64], out[h.configs.PREC_MIXED]
+
+    def rel(a, b):
+        a, b = np.asarray(a), np.asarray(b)
+        sc = np.max(np.abs(b))
+        return float(np.max(np.abs(a - b)) / sc) if sc else float(np.max(np.abs(a - b)))
+
+    errs = {"dB2O2": rel(e1["dB2O2"], e0["dB2O2"]), "dE2O2": rel(e1["dE2O2"], e0["dE2O2"]),
+            "KE_lab": rel(e1["KE_lab"], e0["KE_lab"]), "KE_pla": rel(e1["KE_pla"], e0["KE_pla"])}
+    for s in range(len(cfg.kinetic)):
+        for k, key in enumerate(("n", "nV", "nvv")):
+            errs[f"moments[{s}].{key}"] = rel(m1[s][k], m0[s][k])
+    return {"steps": steps, "max": max(errs.values()), "tolerance": 1e-4,
+            "within_tolerance": max(errs.values()) <= 1e-4, "errors": errs}
+
+
+def e2e_measure(h, cfg, st, K, world):
+    """The same metric through the C-ABI with host buffers: upload from pinned memory, K steps as
+    advance_by(inner_Nt) chunks with the recorder downloads (fields, sources, moments) after each,
+    particles back at the end; wall clock, max over ranks."""
+    import torch
+    import torch.distributed as dist
+
+    n_particles = sum(p["q1"].size for p in st["particles"])
+    pinned = []
+    for p in st["particles"]:
+        d = {}
+        for key in ("q1", "vx", "vy", "vz", "w"):
+            t = torch.empty(p[key].size, dtype=torch.float64, pin_memory=True)
+            t.numpy()[:] = p[key]
+            d[key] = t.numpy()
+        pinned.append(d)
+    inner = cfg.inner_Nt
+    with h.open_run(cfg) as r2:
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for s, d in enumerate(pinned):
+            r2.upload_particles(s, d["q1"], d["vx"], d["vy"], d["vz"], d["w"])
+        r2.upload_fields(st["B"], st["E"])
+        for i, c in enumerate(st["cold"]):
+            r2.upload_cold(i, c["n_full"], c["nV_full"])
+        done = 0
+        d2h = 0
+        while done < K:
+            k = min(inner, K - done)
+            r2.advance(k)
+            done += k
+            run_B, run_E = r2.fields()
+            rho, J = r2.sources()
+            d2h += run_B.nbytes + run_E.nbytes + rho.nbytes + J.nbytes
+            for s in range(len(cfg.kinetic)):
+                d2h += sum(a.nbytes for a in r2.moments(s))
+        for s in range(len(cfg.kinetic)):
+            p = r2.particles(s)
+            d2h += sum(p[k].nbytes for k in ("q1", "vx", "vy", "vz", "w"))
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = sum(p["q1"].nbytes * 5 for p in st["particles"]) + st["B"].nbytes + st["E"].nbytes
+    return {"value": n_particles * K * world / e2e_s, "unit": METRIC, "h2d_bytes_per_step": h2d / K,
+            "d2h_bytes_per_step": d2h / K,
+            "note": f"FP64 host buffers; upload, {K} steps as advance_by({inner}) chunks with field/source/moment "
+                    "downloads after each chunk, particle download at the end"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=300)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="config2_tsc_mirror_nx2048")
+    ap.add_argument("--config", default="config3_cic_periodic_nx4096")
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the fp64 / error / drop-in side measurements")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference", "at least 3 warm-up steps"
 
@@ -205,9 +405,6 @@ def main():
         run_reference_arm(args, h, rank)
         return
 
-    import ctypes
-
-    import numpy as np
     import torch
     import torch.distributed as dist
 
@@ -216,148 +413,76 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     cfg = workload(h, args.config)
+    if args.precision != "auto":
+        cfg = cfg.replace(precision=h.configs.PREC_MIXED if args.precision == "mixed" else h.configs.PREC_FP64)
+    prec = precision_name(cfg, h)
     from hfemic_b200.loader import initial_state
 
     st = initial_state(cfg, seed=1000 + rank)
-    n_particles = sum(p["q1"].size for p in st["particles"])
+    traffic = load_traffic()
 
-    run = h.open_run(cfg)
-    lib = run.lib
-    lib.h1d_advance_async.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
-    lib.h1d_synchronize.argtypes = [ctypes.c_void_p]
-    lib.h1d_get_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
-    lib.h1d_profile_enable.argtypes = [ctypes.c_void_p, ctypes.c_int]
-    lib.h1d_profile_read.argtypes = [ctypes.c_void_p, ctypes.POINTER(h.abi.Profile)]
-    run.upload_state(st)
-    sp = ctypes.c_void_p()
-    run._check(lib.h1d_get_stream(run.h, ctypes.byref(sp)))
-    stream = torch.cuda.ExternalStream(sp.value)
-
-    # warm-up
-    run._check(lib.h1d_advance_async(run.h, args.warmup))
-    run._check(lib.h1d_synchronize(run.h))
-
-    # timed region: K steps, events on the run's stream, profiling events around each kernel group
-    run._check(lib.h1d_profile_enable(run.h, 1))
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        start.record(stream)
-        run._check(lib.h1d_advance_async(run.h, args.steps))
-        end.record(stream)
-        run._check(lib.h1d_synchronize(run.h))
-        torch.cuda.synchronize()
-    ms = start.elapsed_time(end)
-    prof = h.abi.Profile()
-    run._check(lib.h1d_profile_read(run.h, ctypes.byref(prof)))
-    run._check(lib.h1d_profile_enable(run.h, 0))
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
+    tr = TimedRun(h, cfg, st)
+    tr.advance(args.warmup)
+    ms, prof, clocks = tr.timed(args.steps, world, clocks_index=local)
+    n_particles = tr.n_particles
+    tr.close()
     value = n_particles * args.steps * world / (ms / 1e3)
+    roofline = roofline_of(prof, prec, args.steps, traffic)
 
-    # roofline of the dominant kernel (fused push/deposit): algorithmic bytes per launch / avg launch time
-    peak, peak_kind = measured_peak()
-    push_avg_ms = prof.push_ms / max(prof.push_launches, 1)
-    bytes_per_launch = BYTES_PER_PARTICLE_STEP * prof.particles_pushed / max(prof.push_launches, 1)
-    achieved = bytes_per_launch / (push_avg_ms / 1e3) / 1e9
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": "push_kernel (fused push + 2 deposits + move + BC, FP64)",
-                "peak_kind": peak_kind,
-                "bytes_per_launch": bytes_per_launch,
-                "window_miss_rate": prof.window_misses / max(2 * prof.particles_pushed, 1),
-                "phase_ms_per_step": {"push": prof.push_ms / args.steps, "sort": prof.sort_ms / args.steps,
-                                      "field": prof.field_ms / args.steps}}
-    traffic_path = os.path.join(ROOT, "profiles", "push_kernel_traffic.json")
-    if os.path.exists(traffic_path):
-        try:
-            with open(traffic_path) as f:
-                tr = json.load(f)
-            roofline["traffic"] = tr["bytes_per_particle"] * bytes_per_launch / BYTES_PER_PARTICLE_STEP
-        except Exception:
-            pass
+    # side measurements on the same state: the plain FP64 pass, the mixed pass's error against it,
+    # and the FP64 drop-in configuration
+    extras = {}
+    if not args.no_extras:
+        if prec == "mixed":
+            t64 = TimedRun(h, cfg.replace(precision=h.configs.PREC_FP64), st)
+            t64.advance(args.warmup)
+            ms64, prof64, _ = t64.timed(args.steps, world)
+            t64.close()
+            v64 = n_particles * args.steps * world / (ms64 / 1e3)
+            extras["fp64"] = {"value": v64, "unit": METRIC, "ms_per_step": ms64 / args.steps,
+                              "roofline": roofline_of(prof64, "fp64", args.steps, traffic)}
+            extras["mixed_over_fp64"] = value / v64
+            extras["error_vs_fp64"] = error_vs_fp64(h, cfg, st)
+        if cfg.name != "config2_tsc_mirror_nx2048":
+            c2 = h.configs.config2()
+            st2 = initial_state(c2, seed=2000 + rank)
+            t2 = TimedRun(h, c2, st2)
+            t2.advance(args.warmup)
+            k2 = max(args.steps, 100)
+            ms2, prof2, _ = t2.timed(k2, world)
+            v2 = t2.n_particles * k2 * world / (ms2 / 1e3)
+            t2.close()
+            extras["drop_in_fp64"] = {"workload": c2.name, "particles_per_gpu": t2.n_particles, "value": v2,
+                                      "unit": METRIC, "ms_per_step": ms2 / k2,
+                                      "roofline": roofline_of(prof2, "fp64", k2, traffic)}
+            del st2
 
-    # e2e through the C-ABI with host buffers: upload from pinned memory, inner_Nt-step chunks
-    # with the recorder downloads (fields, sources, moments) after each, particles back at the end
-    e2e = None
-    if not args.no_e2e:
-        K = args.steps
-        inner = cfg.inner_Nt
-        pinned = []
-        for p in st["particles"]:
-            d = {}
-            for key in ("q1", "vx", "vy", "vz", "w"):
-                t = torch.empty(p[key].size, dtype=torch.float64, pin_memory=True)
-                t.numpy()[:] = p[key]
-                d[key] = t.numpy()
-            pinned.append(d)
-        M = cfg.Nx + 6
-        bufB = torch.empty((M, 3), dtype=torch.float64, pin_memory=True).numpy()
-        bufE = torch.empty((M, 3), dtype=torch.float64, pin_memory=True).numpy()
-        outs = [{k: torch.empty(p["q1"].size, dtype=torch.float64, pin_memory=True).numpy()
-                 for k in ("q1", "vx", "vy", "vz", "w")} for p in st["particles"]]
-        with h.open_run(cfg) as r2:
-            if world > 1:
-                dist.barrier()
-            torch.cuda.synchronize()
-            t0 = time.perf_counter()
-            for s, d in enumerate(pinned):
-                r2.upload_particles(s, d["q1"], d["vx"], d["vy"], d["vz"], d["w"])
-            r2.upload_fields(st["B"], st["E"])
-            for i, c in enumerate(st["cold"]):
-                r2.upload_cold(i, c["n_full"], c["nV_full"])
-            done = 0
-            d2h = 0
-            while done < K:
-                k = min(inner, K - done)
-                r2.advance(k)
-                done += k
-                run_B, run_E = r2.fields()
-                rho, J = r2.sources()
-                d2h += (run_B.nbytes + run_E.nbytes + rho.nbytes + J.nbytes)
-                for s in range(len(cfg.kinetic)):
-                    m = r2.moments(s)
-                    d2h += sum(a.nbytes for a in m)
-            for s in range(len(cfg.kinetic)):
-                p = r2.particles(s)
-                d2h += sum(p[k].nbytes for k in ("q1", "vx", "vy", "vz", "w"))
-            torch.cuda.synchronize()
-            e2e_s = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([e2e_s], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        h2d = sum(p["q1"].nbytes * 5 for p in st["particles"]) + st["B"].nbytes + st["E"].nbytes
-        e2e = {"value": n_particles * K * world / e2e_s, "unit": METRIC, "h2d_bytes_per_step": h2d / K,
-               "d2h_bytes_per_step": d2h / K,
-               "note": f"upload, {K} steps as advance_by({inner}) chunks with field/source/moment downloads "
-                       "after each chunk, particle download at the end"}
+    e2e = None if args.no_e2e else e2e_measure(h, cfg, st, args.steps, world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_reference(cfg) or cpu_baseline_port(h, cfg)
 
-    run.close()
     if world > 1:
         dist.destroy_process_group()
     if rank != 0:
         return
+    state_mb = n_particles * STATE_BYTES[prec] / 1e6
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded bi-Maxwellian loader)",
+        "vs_baseline": None, "dtype": "f32+i32 particles, f64 fields" if prec == "mixed" else "f64",
+        "data": "synthetic (seeded bi-Maxwellian loader)",
         "config": {"workload": cfg.name, "Nx": cfg.Nx, "particles_per_gpu": n_particles,
                    "species": len(cfg.kinetic), "ppc": [k.Nc for k in cfg.kinetic],
                    "shape_order": [k.shape_order for k in cfg.kinetic], "xi": cfg.xi,
-                   "algorithm": "CAM-CL", "n_subcycles": cfg.n_subcycles, "precision": "fp64",
-                   "l2": "particle state (197 MB per GPU) larger than L2; no flush",
+                   "algorithm": "CAM-CL" if cfg.algorithm == h.configs.ALGO_CAMCL else "PC",
+                   "n_subcycles": cfg.n_subcycles, "precision": prec,
+                   "l2": f"particle state ({state_mb:.0f} MB per GPU, one buffer set) larger than L2; no flush",
                    "parallelism": f"replicas x{world}"},
-        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+        "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": int(prof.kernel_launches),
+        **extras,
     }
     print(json.dumps(line))
 

@@ -65,6 +65,7 @@ struct FieldArgs {
     double const *geo; // G_COUNT x Nx
     double const *B_in, *E_in; // AoS, cell 0
     double       *B_out, *E_out, *EB_out, *charge_out, *current_out; // EB: {E, B on the half grid} per cell
+    float        *EBf_out; // FP32 copy of EB for the mixed-precision particle pass, or null
     int           nk, nc;
     KinSrc        k[MAXK];
     ColdSrc       c[MAXC];
@@ -217,13 +218,19 @@ __device__ __forceinline__ void put1(double *g, Cell const &C, int Nx, double v)
 
 // owner write of the interleaved push record {E, B averaged onto the half grid} and its ghost
 // images; the half-grid B of the last ghost cell stays NaN (PartSpecies.cc:137)
-__device__ __forceinline__ void put_eb(double *eb, Cell const &C, int Nx, d3 E, d3 Bh)
+__device__ __forceinline__ void put_eb(double *eb, float *ebf, Cell const &C, int Nx, d3 E, d3 Bh)
 {
     auto put = [&](int i, bool withB) {
         double *p = eb + 6 * i;
         p[0] = E.x, p[1] = E.y, p[2] = E.z;
         if (withB)
             p[3] = Bh.x, p[4] = Bh.y, p[5] = Bh.z;
+        if (ebf) {
+            float *f = ebf + 6 * i;
+            f[0] = static_cast<float>(E.x), f[1] = static_cast<float>(E.y), f[2] = static_cast<float>(E.z);
+            if (withB)
+                f[3] = static_cast<float>(Bh.x), f[4] = static_cast<float>(Bh.y), f[5] = static_cast<float>(Bh.z);
+        }
     };
     put(C.gm, true);
     if (C.gm < PAD)
@@ -411,7 +418,7 @@ __global__ void __launch_bounds__(512) camcl_field_kernel(FieldArgs a)
         put1(a.charge_out, C, Nx, rho_avg);
         put3(a.current_out, C, Nx, J_avg);
         d3 const Bh = (sld3(S.B0, min(t + 1, C.L - 1)) + Bavg) * 0.5;
-        put_eb(a.EB_out, C, Nx, Ef, Bh);
+        put_eb(a.EB_out, a.EBf_out, C, Nx, Ef, Bh);
         for (int ci = 0; ci < a.nc; ++ci)
             st3(a.c[ci].nV_out, C.gm, cold_nV[ci]);
         // clear the deposit set of the next cycle (interior + ghost images)
@@ -504,7 +511,7 @@ __global__ void __launch_bounds__(512) pc_field_kernel(FieldArgs a)
     d3 const Bh = (sld3(S.B0, min(t + 1, C.L - 1)) + B1a) * 0.5;
     if (C.owner) {
         put3(a.E1_out, C, Nx, E1a);
-        put_eb(a.EB_out, C, Nx, E1a, Bh);
+        put_eb(a.EB_out, a.EBf_out, C, Nx, E1a, Bh);
         if (ph == 2) {
             for (int ci = 0; ci < a.nc; ++ci) { // corrector push of the cold fluid (Domain_PC.cc:182-188)
                 ColdSrc const &K = a.c[ci];

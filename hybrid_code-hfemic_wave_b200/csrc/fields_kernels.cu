@@ -24,9 +24,9 @@ cudaError_t launch_camcl_fields(FieldArgs const &a, int blocks, int threads, siz
     camcl_field_kernel<<<blocks, threads, smem, st>>>(a);
     return cudaGetLastError();
 }
-cudaError_t launch_prep_fields(double *B, double *E, double *EB, int Nx, cudaStream_t st)
+cudaError_t launch_prep_fields(double *B, double *E, double *EB, float *EBf, int Nx, cudaStream_t st)
 {
-    prep_fields_kernel<<<(Nx + 2 * PAD + 255) / 256, 256, 0, st>>>(B, E, EB, Nx);
+    prep_fields_kernel<<<(Nx + 2 * PAD + 255) / 256, 256, 0, st>>>(B, E, EB, EBf, Nx);
     return cudaGetLastError();
 }
 cudaError_t launch_finalize_kinetic(double const *raw, double *out, int Nx, double s1, int reflecting, cudaStream_t st)

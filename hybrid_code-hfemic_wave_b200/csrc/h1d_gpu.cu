@@ -6,6 +6,7 @@
 #include "device_common.cuh"
 #include "fields.cuh"
 #include "particles.cuh"
+#include "particles_mixed.cuh"
 #include "sort.cuh"
 #include "launchers.h"
 
@@ -27,7 +28,9 @@ constexpr int FIELD_BLOCK_MIN = 256;
 
 struct SpeciesState {
     int64_t  n = 0, cap = 0;
-    double  *buf[2][5] = {}; // [parity][q1, vx, vy, vz, w]
+    double  *buf[2][5] = {}; // FP64: [parity][q1, vx, vy, vz, w]
+    int32_t *cell[2]   = {}; // mixed precision: [parity] full-grid cell
+    float   *fbuf[2][5] = {}; // mixed precision: [parity][offset in the cell, vx, vy, vz, w]
     int32_t *pid[2]    = {};
     int      cur       = 0;
     // sort scratch
@@ -62,6 +65,8 @@ struct h1d_run {
     size_t       field_smem = 0;
     double      *geo = nullptr;
     double      *B[2] = {}, *E[2] = {}, *EB = nullptr, *charge = nullptr, *current = nullptr;
+    float       *EBf = nullptr; // FP32 push record of the mixed-precision particle pass
+    bool         mixed = false;
     double      *E1[2] = {}; // predictor-corrector: averaged E of phases 1 and 2
     int          fcur = 0; // field parity
     int          dset = 0; // deposit set parity
@@ -328,10 +333,82 @@ void launch_push_o(PushArgs const &a, bool mirror, int bc, dim3 g, cudaStream_t 
     else
         launch_push_bc<O, false>(a, bc, g, st);
 }
+template <int O, bool MIRROR, int BC>
+cudaError_t push_attr_mixed()
+{
+    return cudaFuncSetAttribute(push_kernel_mixed<O, MIRROR, BC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(PIPE_SMEM_MIXED));
+}
+cudaError_t set_push_smem_mixed()
+{
+    cudaError_t e = cudaSuccess;
+    auto        k = [&](cudaError_t x) {
+        if (e == cudaSuccess)
+            e = x;
+    };
+    k(push_attr_mixed<1, false, 0>()), k(push_attr_mixed<1, false, 1>()), k(push_attr_mixed<1, false, 2>());
+    k(push_attr_mixed<1, true, 0>()), k(push_attr_mixed<1, true, 1>()), k(push_attr_mixed<1, true, 2>());
+    k(push_attr_mixed<2, false, 0>()), k(push_attr_mixed<2, false, 1>()), k(push_attr_mixed<2, false, 2>());
+    k(push_attr_mixed<2, true, 0>()), k(push_attr_mixed<2, true, 1>()), k(push_attr_mixed<2, true, 2>());
+    k(push_attr_mixed<3, false, 0>()), k(push_attr_mixed<3, false, 1>()), k(push_attr_mixed<3, false, 2>());
+    k(push_attr_mixed<3, true, 0>()), k(push_attr_mixed<3, true, 1>()), k(push_attr_mixed<3, true, 2>());
+    return e;
+}
+template <int O, bool MIRROR>
+void launch_push_mixed_bc(PushArgsMixed const &a, int bc, dim3 g, cudaStream_t st)
+{
+    if (bc == H1D_BC_PERIODIC)
+        push_kernel_mixed<O, MIRROR, BCK_PERIODIC><<<g, PIPE_THREADS, PIPE_SMEM_MIXED, st>>>(a);
+    else if (bc == H1D_BC_REFLECTING)
+        push_kernel_mixed<O, MIRROR, BCK_REFLECTING><<<g, PIPE_THREADS, PIPE_SMEM_MIXED, st>>>(a);
+    else
+        push_kernel_mixed<O, MIRROR, BCK_ABSORBING><<<g, PIPE_THREADS, PIPE_SMEM_MIXED, st>>>(a);
+}
+template <int O>
+void launch_push_mixed_o(PushArgsMixed const &a, bool mirror, int bc, dim3 g, cudaStream_t st)
+{
+    if (mirror)
+        launch_push_mixed_bc<O, true>(a, bc, g, st);
+    else
+        launch_push_mixed_bc<O, false>(a, bc, g, st);
+}
+// the mixed-precision pass of species s with the pass settings of `a` (constants rounded to FP32)
+int launch_push_mixed(h1d_run *run, int s, PushArgs const &a)
+{
+    SpeciesState &S = run->sp[s];
+    PushArgsMixed m{};
+    m.cell = S.cell[S.cur], m.off = S.fbuf[S.cur][0], m.vx = S.fbuf[S.cur][1], m.vy = S.fbuf[S.cur][2];
+    m.vz = S.fbuf[S.cur][3], m.w = S.fbuf[S.cur][4], m.pid = S.pid[S.cur], m.n = a.n, m.Nx = a.Nx;
+    m.EB = run->EBf + 6 * PAD;
+    for (int d = 0; d < 2; ++d)
+        for (int q = 0; q < 4; ++q)
+            m.dep[d][q] = a.dep[d][q];
+    m.full_min = static_cast<float>(a.full_min), m.xiD1 = static_cast<float>(a.xiD1);
+    m.inv_D1 = static_cast<float>(a.inv_D1), m.O0 = static_cast<float>(a.O0), m.dt = static_cast<float>(a.dt);
+    m.travel_scale = static_cast<float>(a.travel_scale), m.xiO0_Oc = static_cast<float>(a.xiO0_Oc);
+    m.dtOc_2O0 = static_cast<float>(a.boris.dtOc_2O0), m.cDtOc_2O0 = static_cast<float>(a.boris.cDtOc_2O0);
+    m.status = a.status, m.fallbacks = a.fallbacks, m.seed = a.seed, m.counter = a.counter;
+    m.species = a.species, m.randomize = a.randomize;
+    m.move_steps = a.move_steps, m.deposit_mask = a.deposit_mask, m.write_back = a.write_back;
+    int64_t const chunks = (a.n + PIPE_CHUNK - 1) / PIPE_CHUNK;
+    dim3 const    g(static_cast<unsigned>(
+        std::min<int64_t>(chunks, static_cast<int64_t>(run->num_sms) * PIPE_CTAS_PER_SM_MIXED)));
+    bool const mirror = run->p.xi != 0;
+    switch (run->p.kinetic[s].shape_order) {
+    case 1: launch_push_mixed_o<1>(m, mirror, run->p.particle_bc, g, run->stream); break;
+    case 2: launch_push_mixed_o<2>(m, mirror, run->p.particle_bc, g, run->stream); break;
+    default: launch_push_mixed_o<3>(m, mirror, run->p.particle_bc, g, run->stream); break;
+    }
+    CU(cudaGetLastError());
+    return H1D_OK;
+}
+
 int launch_push(h1d_run *run, int s, PushArgs const &a)
 {
     if (a.n == 0)
         return H1D_OK;
+    if (run->mixed)
+        return launch_push_mixed(run, s, a);
     int64_t const chunks = (a.n + PIPE_CHUNK - 1) / PIPE_CHUNK;
     dim3 const    g(static_cast<unsigned>(std::min<int64_t>(chunks, static_cast<int64_t>(run->num_sms) * PIPE_CTAS_PER_SM)));
     bool const    mirror = run->p.xi != 0;
@@ -372,8 +449,12 @@ int sort_species(h1d_run *run, int s)
     phase_begin(run, 1);
     CU(cudaMemsetAsync(S.dead, 0, sizeof(unsigned long long), st));
     unsigned const nb = static_cast<unsigned>((S.n + 255) / 256);
-    keys_kernel<<<nb, 256, 0, st>>>(S.buf[S.cur][0], S.buf[S.cur][4], S.n, -0.5 * Nx, Nx, S.keys[0], S.idx[0], S.dead,
-                                    run->d_status);
+    if (run->mixed)
+        keys_kernel_mixed<<<nb, 256, 0, st>>>(S.cell[S.cur], S.fbuf[S.cur][4], S.n, Nx, S.keys[0], S.idx[0], S.dead,
+                                              run->d_status);
+    else
+        keys_kernel<<<nb, 256, 0, st>>>(S.buf[S.cur][0], S.buf[S.cur][4], S.n, -0.5 * Nx, Nx, S.keys[0], S.idx[0],
+                                        S.dead, run->d_status);
     int src = 0;
     for (int pass = 0; pass < passes; ++pass) {
         int const shift = 8 * pass;
@@ -387,11 +468,20 @@ int sort_species(h1d_run *run, int s)
             S.idx[1 - src]);
         src = 1 - src;
     }
-    GatherArgs g{};
-    for (int k = 0; k < 5; ++k)
-        g.src[k] = S.buf[S.cur][k], g.dst[k] = S.buf[1 - S.cur][k];
-    g.pid_src = S.pid[S.cur], g.pid_dst = S.pid[1 - S.cur], g.idx = S.idx[src], g.n = S.n;
-    gather_kernel<<<nb, 256, 0, st>>>(g);
+    if (run->mixed) {
+        GatherArgsMixed g{};
+        for (int k = 0; k < 5; ++k)
+            g.src[k] = S.fbuf[S.cur][k], g.dst[k] = S.fbuf[1 - S.cur][k];
+        g.cell_src = S.cell[S.cur], g.cell_dst = S.cell[1 - S.cur];
+        g.pid_src = S.pid[S.cur], g.pid_dst = S.pid[1 - S.cur], g.idx = S.idx[src], g.n = S.n;
+        gather_kernel_mixed<<<nb, 256, 0, st>>>(g);
+    } else {
+        GatherArgs g{};
+        for (int k = 0; k < 5; ++k)
+            g.src[k] = S.buf[S.cur][k], g.dst[k] = S.buf[1 - S.cur][k];
+        g.pid_src = S.pid[S.cur], g.pid_dst = S.pid[1 - S.cur], g.idx = S.idx[src], g.n = S.n;
+        gather_kernel<<<nb, 256, 0, st>>>(g);
+    }
     CU(cudaGetLastError());
     phase_end(run, 2 + 5 * passes);
     S.cur = 1 - S.cur;
@@ -412,7 +502,7 @@ FieldArgs field_args(h1d_run *run)
     a.geo = run->geo;
     a.B_in = run->B[run->fcur] + 3 * PAD, a.E_in = run->E[run->fcur] + 3 * PAD;
     a.B_out = run->B[1 - run->fcur] + 3 * PAD, a.E_out = run->E[1 - run->fcur] + 3 * PAD;
-    a.EB_out = run->EB + 6 * PAD, a.charge_out = run->charge + PAD, a.current_out = run->current + 3 * PAD;
+    a.EB_out = run->EB + 6 * PAD, a.EBf_out = run->EBf ? run->EBf + 6 * PAD : nullptr, a.charge_out = run->charge + PAD, a.current_out = run->current + 3 * PAD;
     a.nk = p.n_kinetic, a.nc = p.n_cold;
     for (int s = 0; s < p.n_kinetic; ++s) {
         h1d_kinetic_desc const &d = p.kinetic[s];
@@ -446,7 +536,7 @@ FieldArgs field_args(h1d_run *run)
 int prepare_fields(h1d_run *run)
 {
     CU(launch_prep_fields(run->B[run->fcur] + 3 * PAD, run->E[run->fcur] + 3 * PAD, run->EB + 6 * PAD,
-                          static_cast<int>(run->Nx), run->stream));
+                          run->EBf ? run->EBf + 6 * PAD : nullptr, static_cast<int>(run->Nx), run->stream));
     run->fields_dirty = false;
     return H1D_OK;
 }
@@ -587,7 +677,16 @@ int finalize_moments(h1d_run *run)
     for (int s = 0; s < p.n_kinetic; ++s) {
         SpeciesState &S = run->sp[s];
         CU(cudaMemsetAsync(S.mom_raw, 0, sizeof(double) * 10 * run->M, run->stream));
-        if (S.n > 0) {
+        if (S.n > 0 && run->mixed) {
+            MomentArgsMixed a{};
+            a.cell = S.cell[S.cur], a.off = S.fbuf[S.cur][0], a.vx = S.fbuf[S.cur][1], a.vy = S.fbuf[S.cur][2];
+            a.vz = S.fbuf[S.cur][3], a.w = S.fbuf[S.cur][4], a.n = S.n, a.ppt = ppt_for(run, s);
+            a.Nx = static_cast<int>(run->Nx), a.status = run->d_status;
+            for (int q = 0; q < 10; ++q)
+                a.out[q] = S.mom_raw + static_cast<size_t>(q) * run->M + PAD;
+            int64_t const chunks = (S.n + 32LL * a.ppt - 1) / (32LL * a.ppt);
+            moments_kernel_mixed<<<static_cast<unsigned>((chunks + 7) / 8), 256, 0, run->stream>>>(a);
+        } else if (S.n > 0) {
             MomentArgs a{};
             a.q1 = S.buf[S.cur][0], a.vx = S.buf[S.cur][1], a.vy = S.buf[S.cur][2], a.vz = S.buf[S.cur][3];
             a.w = S.buf[S.cur][4], a.n = S.n, a.ppt = ppt_for(run, s), a.Nx = static_cast<int>(run->Nx);
@@ -806,7 +905,9 @@ int h1d_create(h1d_params const *params, h1d_run **out)
     run->seg           = static_cast<int>(std::min<long>(L - 2 * run->H, run->Nx));
     run->nblocks_field = static_cast<int>((run->Nx + run->seg - 1) / run->seg);
     run->field_smem    = sizeof(double) * static_cast<size_t>(L) * (SMEM_SCALARS + 3 * SMEM_VECTORS);
-    if (set_field_smem(run->field_smem) != cudaSuccess || set_push_smem() != cudaSuccess)
+    run->mixed = p.precision == H1D_PREC_MIXED;
+    if (set_field_smem(run->field_smem) != cudaSuccess || set_push_smem() != cudaSuccess
+        || (run->mixed && set_push_smem_mixed() != cudaSuccess))
         return fail(H1D_ERR_CUDA);
     cudaDeviceGetAttribute(&run->num_sms, cudaDevAttrMultiProcessorCount, run->device);
 
@@ -815,7 +916,8 @@ int h1d_create(h1d_params const *params, h1d_run **out)
         || dalloc(run, &run->E[0], 3 * M) || dalloc(run, &run->E[1], 3 * M) || dalloc(run, &run->EB, 6 * M)
         || dalloc(run, &run->charge, M) || dalloc(run, &run->current, 3 * M) || dalloc(run, &run->d_status, 1)
         || dalloc(run, &run->E1[0], 3 * M) || dalloc(run, &run->E1[1], 3 * M) || dalloc(run, &run->d_fallbacks, 1)
-        || dalloc(run, &run->d_energy, 6 + 6 * (H1D_MAX_KINETIC + H1D_MAX_COLD)))
+        || dalloc(run, &run->d_energy, 6 + 6 * (H1D_MAX_KINETIC + H1D_MAX_COLD))
+        || (run->mixed && dalloc(run, &run->EBf, 6 * M)))
         return fail(H1D_ERR_OOM);
     if (cudaMallocHost(&run->h_status, sizeof(unsigned)) != cudaSuccess)
         return fail(H1D_ERR_OOM);
@@ -848,13 +950,16 @@ int h1d_destroy(h1d_run *run)
     for (int k = 0; k < 2; ++k)
         cudaFree(run->B[k]), cudaFree(run->E[k]), cudaFree(run->E1[k]);
     cudaFree(run->d_fallbacks);
-    cudaFree(run->EB), cudaFree(run->charge), cudaFree(run->current), cudaFree(run->d_status), cudaFree(run->d_energy);
+    cudaFree(run->EB), cudaFree(run->EBf), cudaFree(run->charge), cudaFree(run->current), cudaFree(run->d_status), cudaFree(run->d_energy);
     if (run->h_status)
         cudaFreeHost(run->h_status);
     for (auto &S : run->sp) {
         for (int k = 0; k < 2; ++k) {
             for (auto *b : S.buf[k])
                 cudaFree(b);
+            for (auto *b : S.fbuf[k])
+                cudaFree(b);
+            cudaFree(S.cell[k]);
             cudaFree(S.pid[k]), cudaFree(S.keys[k]), cudaFree(S.idx[k]);
         }
         cudaFree(S.hist), cudaFree(S.part), cudaFree(S.dead), cudaFree(S.dep), cudaFree(S.mom_raw), cudaFree(S.mom);
@@ -880,12 +985,23 @@ int h1d_upload_particles(h1d_run *run, int s, int64_t n, double const *q1, doubl
     SpeciesState &S = run->sp[s];
     CU(cudaStreamSynchronize(run->stream));
     if (n > S.cap) {
-        int64_t const cap = n + 64;
+        int64_t const cap = n + 64; // slack for the 16-byte rounding of the last bulk copy of a pass
         for (int k = 0; k < 2; ++k) {
-            for (auto *&b : S.buf[k]) {
-                cudaFree(b);
-                b = nullptr;
-                CU(cudaMalloc(&b, sizeof(double) * cap));
+            if (run->mixed) {
+                for (auto *&b : S.fbuf[k]) {
+                    cudaFree(b);
+                    b = nullptr;
+                    CU(cudaMalloc(&b, sizeof(float) * cap));
+                }
+                cudaFree(S.cell[k]);
+                S.cell[k] = nullptr;
+                CU(cudaMalloc(&S.cell[k], sizeof(int32_t) * cap));
+            } else {
+                for (auto *&b : S.buf[k]) {
+                    cudaFree(b);
+                    b = nullptr;
+                    CU(cudaMalloc(&b, sizeof(double) * cap));
+                }
             }
             cudaFree(S.pid[k]), cudaFree(S.keys[k]), cudaFree(S.idx[k]);
             S.pid[k] = nullptr, S.keys[k] = nullptr, S.idx[k] = nullptr;
@@ -898,7 +1014,26 @@ int h1d_upload_particles(h1d_run *run, int s, int64_t n, double const *q1, doubl
     S.cur              = 0;
     S.n                = n;
     double const *src[5] = { q1, vx, vy, vz, w };
-    for (int k = 0; k < 5; ++k)
+    if (run->mixed && n) { // stage each FP64 component on the device and convert it
+        double *tmp = nullptr;
+        CU(cudaMalloc(&tmp, sizeof(double) * n));
+        unsigned const nb = static_cast<unsigned>((n + 255) / 256);
+        int            st = H1D_OK;
+        for (int k = 0; k < 5 && st == H1D_OK; ++k) {
+            if (cudaMemcpyAsync(tmp, src[k], sizeof(double) * n, cudaMemcpyHostToDevice, run->stream) != cudaSuccess)
+                st = set_err(run, H1D_ERR_CUDA, "h1d_upload_particles: copy failed");
+            else if (k == 0)
+                q1_to_mixed_kernel<<<nb, 256, 0, run->stream>>>(tmp, n, -0.5 * run->Nx, S.cell[0], S.fbuf[0][0]);
+            else
+                to_f32_kernel<<<nb, 256, 0, run->stream>>>(tmp, n, S.fbuf[0][k]);
+            if (st == H1D_OK && cudaGetLastError() != cudaSuccess)
+                st = set_err(run, H1D_ERR_CUDA, "h1d_upload_particles: conversion failed");
+        }
+        cudaStreamSynchronize(run->stream);
+        cudaFree(tmp);
+        TRY(st);
+    }
+    for (int k = 0; k < 5 && !run->mixed; ++k)
         if (n)
             CU(cudaMemcpyAsync(S.buf[0][k], src[k], sizeof(double) * n, cudaMemcpyHostToDevice, run->stream));
     if (n)
@@ -1012,6 +1147,8 @@ int h1d_particle_count(h1d_run *run, int s, int64_t *n)
 {
     if (!run || s < 0 || s >= run->p.n_kinetic || !n)
         return H1D_ERR_INVALID_ARG;
+    if (run->p.particle_bc == H1D_BC_ABSORBING && run->sp[s].n > 0 && run->sp[s].since_sort > 0)
+        TRY(sort_species(run, s)); // drop absorbed particles, so that the count is exact
     *n = run->sp[s].n;
     return H1D_OK;
 }
@@ -1021,10 +1158,28 @@ int h1d_download_particles(h1d_run *run, int s, double *q1, double *vx, double *
     if (!run || s < 0 || s >= run->p.n_kinetic)
         return H1D_ERR_INVALID_ARG;
     SpeciesState &S = run->sp[s];
-    if (run->p.particle_bc == H1D_BC_ABSORBING && S.n > 0)
+    if (run->p.particle_bc == H1D_BC_ABSORBING && S.n > 0 && S.since_sort > 0)
         TRY(sort_species(run, s)); // drop absorbed particles
     double *dst[5] = { q1, vx, vy, vz, w };
-    for (int k = 0; k < 5; ++k)
+    if (run->mixed && S.n) { // convert each component to FP64 in a device staging buffer
+        double *tmp = nullptr;
+        CU(cudaMalloc(&tmp, sizeof(double) * S.n));
+        unsigned const nb = static_cast<unsigned>((S.n + 255) / 256);
+        int            st = H1D_OK;
+        for (int k = 0; k < 5 && st == H1D_OK; ++k) {
+            if (!dst[k])
+                continue;
+            from_mixed_kernel<<<nb, 256, 0, run->stream>>>(k == 0 ? S.cell[S.cur] : nullptr, S.fbuf[S.cur][k], S.n,
+                                                           -0.5 * run->Nx, tmp);
+            if (cudaGetLastError() != cudaSuccess
+                || cudaMemcpyAsync(dst[k], tmp, sizeof(double) * S.n, cudaMemcpyDeviceToHost, run->stream) != cudaSuccess
+                || cudaStreamSynchronize(run->stream) != cudaSuccess)
+                st = set_err(run, H1D_ERR_CUDA, "h1d_download_particles: conversion failed");
+        }
+        cudaFree(tmp);
+        TRY(st);
+    }
+    for (int k = 0; k < 5 && !run->mixed; ++k)
         if (dst[k] && S.n)
             CU(cudaMemcpyAsync(dst[k], S.buf[S.cur][k], sizeof(double) * S.n, cudaMemcpyDeviceToHost, run->stream));
     if (pid && S.n) {

@@ -19,7 +19,7 @@ __device__ __forceinline__ int wrap(int i, int Nx) { return i < 0 ? i + Nx : i >
 
 // boundary_pass of E and B (periodic ghost fill, Delegate.cc:159-170) and the push record
 // {E, B on the half grid} (PartSpecies.cc:132-139; the last ghost's half-grid B stays NaN)
-__global__ void prep_fields_kernel(double *B, double *E, double *EB, int Nx)
+__global__ void prep_fields_kernel(double *B, double *E, double *EB, float *EBf, int Nx)
 {
     int const i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x) - PAD;
     if (i >= Nx + PAD)
@@ -34,6 +34,9 @@ __global__ void prep_fields_kernel(double *B, double *E, double *EB, int Nx)
     } else {
         p[3] = p[4] = p[5] = __longlong_as_double(0x7ff8000000000000LL);
     }
+    if (EBf)
+        for (int c = 0; c < 6; ++c)
+            EBf[6 * i + c] = static_cast<float>(p[c]);
     if (i < 0 || i >= Nx) {
         st3(B, i, ld3(B, wrap(i, Nx)));
         st3(E, i, e);

@@ -110,6 +110,25 @@ def test_large_random_state(gpu_lib, oracle_lib):
     assert max(errs.values()) <= 1e-11
 
 
+def test_absorbing_boundary(gpu_lib, oracle_lib):
+    """Absorbing walls (an extension: the reference has periodic and reflecting particles only):
+    the GPU path removes exactly the particles the oracle removes, and the rest agree."""
+    from hfemic_b200.loader import initial_state
+
+    cfg = h.configs.parity_p2().replace(particle_bc=h.configs.BC_ABSORBING, Nx=128, xi=0.02)
+    for k in cfg.kinetic:
+        k.Nc = 64
+    init = initial_state(cfg, seed=9)
+    g, c, eg, ec = run_both(cfg, init, 10, gpu_lib, oracle_lib)
+    for s in range(len(cfg.kinetic)):
+        pg, pc = by_pid(g["particles"][s]), by_pid(c["particles"][s])
+        assert pg["q1"].size < init["particles"][s]["q1"].size  # the case does absorb particles
+        np.testing.assert_array_equal(pg["pid"], pc["pid"])
+    errs = state_errors(g, c, cfg)
+    bad = {k: v for k, v in errs.items() if not v <= TOL10}
+    assert not bad, bad
+
+
 def test_moved_too_far(gpu_lib):
     cfg = h.configs.parity_p1()
     init = read_state(os.path.join(GOLDEN, f"{cfg.name}.init.bin"))
