@@ -265,3 +265,117 @@ class Run:
         for i in range(len(self.cfg.cold)):
             st["cold"].append(self.cold(i))
         return st
+
+
+# ---------------------------------------------------------------------------------------------
+# ensembles and tuning (CUDA library only; no counterpart in the reference or the oracle)
+# ---------------------------------------------------------------------------------------------
+
+class BatchStats(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("kernel_launches", C.c_int64), ("graph_launches", C.c_int64),
+                ("graphs_built", C.c_int64)]
+
+
+def _declare_batch(lib):
+    v, u = C.c_void_p, C.POINTER(C.c_uint32)
+    ip = C.POINTER(C.c_int)
+    spec = {
+        "h1d_batch_create": ([C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+        "h1d_batch_destroy": ([v], C.c_int),
+        "h1d_batch_advance": ([v, C.c_uint32], C.c_int),
+        "h1d_batch_advance_async": ([v, C.c_uint32], C.c_int),
+        "h1d_batch_synchronize": ([v], C.c_int),
+        "h1d_batch_get_stream": ([v, C.POINTER(C.c_void_p)], C.c_int),
+        "h1d_batch_configure": ([v, C.c_int, C.c_int, C.c_int], C.c_int),
+        "h1d_batch_autotune": ([v, u, ip, ip], C.c_int),
+        "h1d_batch_stats_read": ([v, C.POINTER(BatchStats)], C.c_int),
+        "h1d_batch_status_string": ([v], C.c_char_p),
+        "h1d_configure": ([v, C.c_int, C.c_int], C.c_int),
+        "h1d_autotune": ([v, u, ip, ip], C.c_int),
+    }
+    for name, (args, res) in spec.items():
+        fn = getattr(lib, name)
+        fn.argtypes, fn.restype = args, res
+    return lib
+
+
+def configure(run: Run, sort_interval: int = 0, push_ctas_per_sm: int = 0):
+    """Sort interval and CTAs per SM of the particle pass of one run (h1d_configure)."""
+    lib = _declare_batch(run.lib)
+    run._check(lib.h1d_configure(run.h, sort_interval, push_ctas_per_sm))
+
+
+def autotune(run: Run):
+    """h1d_autotune: advances the run by real steps while choosing its sort interval and CTA count.
+    Returns (steps_taken, sort_interval, ctas_per_sm)."""
+    lib = _declare_batch(run.lib)
+    n, k, c = C.c_uint32(), C.c_int(), C.c_int()
+    run._check(lib.h1d_autotune(run.h, C.byref(n), C.byref(k), C.byref(c)))
+    return n.value, k.value, c.value
+
+
+class Batch:
+    """Many CAM-CL runs advanced together (h1d_batch_*); the runs stay owned by the caller."""
+
+    def __init__(self, runs):
+        self.runs = list(runs)
+        self.lib = _declare_batch(self.runs[0].lib)
+        arr = (C.c_void_p * len(self.runs))(*[r.h.value for r in self.runs])
+        h = C.c_void_p()
+        st = self.lib.h1d_batch_create(arr, len(self.runs), C.byref(h))
+        if st != OK:
+            raise H1DError(st, "h1d_batch_create failed")
+        self.h = h
+
+    def _check(self, st):
+        if st == OK:
+            return
+        msg = self.lib.h1d_batch_status_string(self.h).decode()
+        if st == ERR_MOVED_TOO_FAR or "moved too far" in msg:
+            raise MovedTooFar(st, msg)
+        raise H1DError(st, msg)
+
+    def configure(self, sort_interval=0, push_ctas_per_sm=0, use_graphs=True):
+        self._check(self.lib.h1d_batch_configure(self.h, sort_interval, push_ctas_per_sm, int(use_graphs)))
+
+    def advance(self, n_steps: int):
+        self._check(self.lib.h1d_batch_advance(self.h, n_steps))
+
+    def advance_async(self, n_steps: int):
+        self._check(self.lib.h1d_batch_advance_async(self.h, n_steps))
+
+    def synchronize(self):
+        self._check(self.lib.h1d_batch_synchronize(self.h))
+
+    def stream(self):
+        s = C.c_void_p()
+        self._check(self.lib.h1d_batch_get_stream(self.h, C.byref(s)))
+        return s.value
+
+    def autotune(self):
+        n, k, c = C.c_uint32(), C.c_int(), C.c_int()
+        self._check(self.lib.h1d_batch_autotune(self.h, C.byref(n), C.byref(k), C.byref(c)))
+        return n.value, k.value, c.value
+
+    def stats(self):
+        s = BatchStats()
+        self._check(self.lib.h1d_batch_stats_read(self.h, C.byref(s)))
+        return dict(steps=s.steps, kernel_launches=s.kernel_launches, graph_launches=s.graph_launches,
+                    graphs_built=s.graphs_built)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.h1d_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

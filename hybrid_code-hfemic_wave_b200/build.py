@@ -7,6 +7,7 @@ kernels use FMA.  The CUDA runtime is linked statically, so the library needs on
 """
 from __future__ import annotations
 
+import concurrent.futures
 import glob
 import os
 import subprocess
@@ -23,6 +24,8 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path
           "--expt-relaxed-constexpr"]
 UNITS = {
     "h1d_gpu.cu": [],
+    "push_fp64.cu": [],
+    "push_mixed.cu": [],
     "fields_kernels.cu": ["--fmad=false"],
 }
 
@@ -43,7 +46,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
     os.makedirs(BUILD, exist_ok=True)
     headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + [
         os.path.join(ROOT, "include", "h1d_gpu.h")]
-    objs = []
+    objs, cmds = [], []
     for unit, extra in UNITS.items():
         src = os.path.join(CSRC, unit)
         obj = os.path.join(BUILD, unit.replace(".cu", ".o"))
@@ -52,9 +55,14 @@ def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = Fals
             cmd = [nvcc(), *ARCH, *COMMON, *extra, "-c", src, "-o", obj]
             if ptxas_verbose:
                 cmd += ["-Xptxas", "-v"]
+            cmds.append(cmd)
+    # the translation units compile in parallel
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for cmd in cmds:
             if verbose:
                 print(" ".join(cmd))
-            subprocess.check_call(cmd)
+        for f in [ex.submit(subprocess.check_call, cmd) for cmd in cmds]:
+            f.result()
     if force or _stale(LIB, objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-cudart", "static"]
         if verbose:

@@ -248,3 +248,37 @@ def parity_p4() -> RunConfig:
 
 PARITY = {f().name: f for f in (parity_p1, parity_p2, parity_p3, parity_p4)}
 PRESETS = {f().name: f for f in (config1, config2, config3)}
+
+
+# ---------------------------------------------------------------------------------------------
+# ensemble members: seeded draws of the ensemble distribution
+# ---------------------------------------------------------------------------------------------
+
+ENSEMBLE_NX = (256, 512, 1024, 2048, 4096)
+
+
+def ensemble_member(seed: int, precision=PREC_MIXED, steps: int = 500, ppc_scale: float = 1.0) -> RunConfig:
+    """One member of the ensemble workload, drawn from a generator seeded with ``seed``: Nx uniform
+    over ENSEMBLE_NX, particles per cell log-uniform in [100, 2000], T_perp/T_par uniform in
+    [1.5, 5], beta_par log-uniform in [0.01, 0.5], xi uniform in [0, 0.004] (redrawn until
+    |xi*Dx*q1| < pi/2 holds on the grid), TSC.  The plasma is that of config1 (one hot H+ species
+    at 10 % density, cold H+ background, isothermal electrons with beta_e 0.1, c/vA = 100) with
+    Dx = 0.3, dt = 0.01, reflecting particles and masking over Nx/16 cells at each end.
+    ``ppc_scale`` shrinks the particle count for tests."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    Nx = int(rng.choice(ENSEMBLE_NX))
+    Nc = max(1, int(round(math.exp(rng.uniform(math.log(100), math.log(2000))) * ppc_scale)))
+    T2_T1 = float(rng.uniform(1.5, 5.0))
+    beta1 = float(math.exp(rng.uniform(math.log(0.01), math.log(0.5))))
+    Dx = 0.3
+    while True:
+        xi = float(rng.uniform(0.0, 0.004))
+        if abs(xi * Dx * (0.5 * Nx + 0.5)) < math.pi / 2 * 0.999:
+            break
+    ef, kin, cold = plasma(100.0, [dict(f=0.1, Nc=Nc, shape_order=2, beta1=beta1, T2_T1=T2_T1)], 0.9, 0.1)
+    inset = Nx // 16
+    return RunConfig(f"ensemble_{seed}", Nx=Nx, Dx=Dx, xi=xi, c=100.0, dt=0.01, efluid=ef, kinetic=kin, cold=cold,
+                     particle_bc=BC_REFLECTING, phase_retardation=(inset, 1.0), amplitude_damping=(inset, 0.2),
+                     precision=precision, steps=steps)

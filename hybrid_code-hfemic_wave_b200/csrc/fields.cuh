@@ -81,6 +81,11 @@ struct FieldArgs {
     double       *E1_out;                 // averaged E for the next particle pass (cell 0)
 };
 
+// block -> (run, segment) of a batched field launch
+struct FieldBlock {
+    int run, seg;
+};
+
 struct Cell {
     int    t, L, g, gm;
     bool   owner;
@@ -180,11 +185,11 @@ __device__ __forceinline__ d3 B_at(FieldArgs const &a, Cell const &C, double con
     return mask_a(C, B);
 }
 
-__device__ __forceinline__ void load_cell(FieldArgs const &a, Cell &C)
+__device__ __forceinline__ void load_cell(FieldArgs const &a, Cell &C, int blk)
 {
     C.t     = threadIdx.x;
     C.L     = blockDim.x;
-    int const g0 = blockIdx.x * a.seg;
+    int const g0 = blk * a.seg;
     C.g     = g0 - a.H + C.t;
     C.gm    = ((C.g % a.Nx) + a.Nx) % a.Nx;
     C.owner = C.t >= a.H && C.t < a.H + a.seg && C.g < a.Nx;
@@ -298,11 +303,11 @@ static __device__ d3 cold_push(FieldArgs const &a, Cell const &C, ColdSrc const 
 // ------------------------------------------------------------------------------------------------
 // CAM-CL cycle (Domain_CAMCL.cc:57-193)
 // ------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) camcl_field_kernel(FieldArgs a)
+__device__ __forceinline__ void camcl_field_body(FieldArgs const &a, int blk)
 {
     extern __shared__ double sm[];
     Cell C;
-    load_cell(a, C);
+    load_cell(a, C, blk);
     Smem const S = carve(sm, C.L);
     int const  t = C.t, Nx = a.Nx;
 
@@ -433,11 +438,11 @@ __global__ void __launch_bounds__(512) camcl_field_kernel(FieldArgs a)
 // ------------------------------------------------------------------------------------------------
 // predictor-corrector phases (Domain_PC.cc:21-205)
 // ------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(512) pc_field_kernel(FieldArgs a)
+__device__ __forceinline__ void pc_field_body(FieldArgs const &a, int blk)
 {
     extern __shared__ double sm[];
     Cell C;
-    load_cell(a, C);
+    load_cell(a, C, blk);
     Smem const S = carve(sm, C.L);
     int const  t = C.t, Nx = a.Nx, ph = a.phase;
 
@@ -523,6 +528,36 @@ __global__ void __launch_bounds__(512) pc_field_kernel(FieldArgs a)
                         put1(a.k[s].zero[d][q], C, Nx, 0.0);
         }
     }
+}
+
+// one run: the arguments are kernel constants, block b covers segment b
+__global__ void __launch_bounds__(512) camcl_field_kernel(FieldArgs a) { camcl_field_body(a, blockIdx.x); }
+__global__ void __launch_bounds__(512) pc_field_kernel(FieldArgs a) { pc_field_body(a, blockIdx.x); }
+
+// an ensemble: block b covers segment map[b].seg of run map[b].run, whose arguments it copies
+// from the device table into shared memory
+__device__ __forceinline__ void load_args(FieldArgs &dst, FieldArgs const *src)
+{
+    static_assert(sizeof(FieldArgs) % 8 == 0, "FieldArgs is copied in 8-byte words");
+    auto const *s = reinterpret_cast<unsigned long long const *>(src);
+    auto       *d = reinterpret_cast<unsigned long long *>(&dst);
+    for (int i = threadIdx.x; i < static_cast<int>(sizeof(FieldArgs) / 8); i += blockDim.x)
+        d[i] = s[i];
+    __syncthreads();
+}
+__global__ void __launch_bounds__(512) camcl_field_batch_kernel(FieldArgs const *table, FieldBlock const *map)
+{
+    __shared__ FieldArgs a;
+    FieldBlock const     b = map[blockIdx.x];
+    load_args(a, table + b.run);
+    camcl_field_body(a, b.seg);
+}
+__global__ void __launch_bounds__(512) pc_field_batch_kernel(FieldArgs const *table, FieldBlock const *map)
+{
+    __shared__ FieldArgs a;
+    FieldBlock const     b = map[blockIdx.x];
+    load_args(a, table + b.run);
+    pc_field_body(a, b.seg);
 }
 
 #endif // H1D_FIELD_TU

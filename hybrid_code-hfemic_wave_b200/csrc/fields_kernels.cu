@@ -24,6 +24,26 @@ cudaError_t launch_camcl_fields(FieldArgs const &a, int blocks, int threads, siz
     camcl_field_kernel<<<blocks, threads, smem, st>>>(a);
     return cudaGetLastError();
 }
+cudaError_t set_field_batch_smem(size_t bytes)
+{
+    cudaError_t e = cudaFuncSetAttribute(camcl_field_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(bytes));
+    if (e != cudaSuccess)
+        return e;
+    return cudaFuncSetAttribute(pc_field_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes));
+}
+cudaError_t launch_camcl_fields_batch(FieldArgs const *table, FieldBlock const *map, int blocks, int threads,
+                                      size_t smem, cudaStream_t st)
+{
+    camcl_field_batch_kernel<<<blocks, threads, smem, st>>>(table, map);
+    return cudaGetLastError();
+}
+cudaError_t launch_pc_fields_batch(FieldArgs const *table, FieldBlock const *map, int blocks, int threads,
+                                   size_t smem, cudaStream_t st)
+{
+    pc_field_batch_kernel<<<blocks, threads, smem, st>>>(table, map);
+    return cudaGetLastError();
+}
 cudaError_t launch_prep_fields(double *B, double *E, double *EB, float *EBf, int Nx, cudaStream_t st)
 {
     prep_fields_kernel<<<(Nx + 2 * PAD + 255) / 256, 256, 0, st>>>(B, E, EB, EBf, Nx);

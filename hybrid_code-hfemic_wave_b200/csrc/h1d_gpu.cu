@@ -5,8 +5,8 @@
 
 #include "device_common.cuh"
 #include "fields.cuh"
-#include "particles.cuh"
-#include "particles_mixed.cuh"
+#include "particle_io.cuh"
+#include "push_launch.h"
 #include "sort.cuh"
 #include "launchers.h"
 
@@ -79,6 +79,9 @@ struct h1d_run {
     bool         recurring = false, moments_stale = true, fields_dirty = true;
     int64_t      step = 0;
     int          sort_interval = 16;
+    int          ctas_per_sm   = 0; // CTAs per SM of the particle pass; 0: the kernel's default
+    uint64_t     gen           = 0; // bumped by every upload and particle-count change
+    int          batch_count   = 0; // batches this run is a member of (at most one)
     std::string  msg;
     // profiling: event pairs per phase (0 push, 1 sort, 2 field)
     bool                                           profiling = false;
@@ -293,87 +296,8 @@ PushArgs push_args(h1d_run *run, int s)
     return a;
 }
 
-template <int O, bool MIRROR, int BC>
-cudaError_t push_attr()
-{
-    return cudaFuncSetAttribute(push_kernel<O, MIRROR, BC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(PIPE_SMEM));
-}
-cudaError_t set_push_smem()
-{
-    cudaError_t e = cudaSuccess;
-    auto        k = [&](cudaError_t x) {
-        if (e == cudaSuccess)
-            e = x;
-    };
-    k(push_attr<1, false, 0>()), k(push_attr<1, false, 1>()), k(push_attr<1, false, 2>());
-    k(push_attr<1, true, 0>()), k(push_attr<1, true, 1>()), k(push_attr<1, true, 2>());
-    k(push_attr<2, false, 0>()), k(push_attr<2, false, 1>()), k(push_attr<2, false, 2>());
-    k(push_attr<2, true, 0>()), k(push_attr<2, true, 1>()), k(push_attr<2, true, 2>());
-    k(push_attr<3, false, 0>()), k(push_attr<3, false, 1>()), k(push_attr<3, false, 2>());
-    k(push_attr<3, true, 0>()), k(push_attr<3, true, 1>()), k(push_attr<3, true, 2>());
-    return e;
-}
-
-template <int O, bool MIRROR>
-void launch_push_bc(PushArgs const &a, int bc, dim3 g, cudaStream_t st)
-{
-    if (bc == H1D_BC_PERIODIC)
-        push_kernel<O, MIRROR, BCK_PERIODIC><<<g, PIPE_THREADS, PIPE_SMEM, st>>>(a);
-    else if (bc == H1D_BC_REFLECTING)
-        push_kernel<O, MIRROR, BCK_REFLECTING><<<g, PIPE_THREADS, PIPE_SMEM, st>>>(a);
-    else
-        push_kernel<O, MIRROR, BCK_ABSORBING><<<g, PIPE_THREADS, PIPE_SMEM, st>>>(a);
-}
-template <int O>
-void launch_push_o(PushArgs const &a, bool mirror, int bc, dim3 g, cudaStream_t st)
-{
-    if (mirror)
-        launch_push_bc<O, true>(a, bc, g, st);
-    else
-        launch_push_bc<O, false>(a, bc, g, st);
-}
-template <int O, bool MIRROR, int BC>
-cudaError_t push_attr_mixed()
-{
-    return cudaFuncSetAttribute(push_kernel_mixed<O, MIRROR, BC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(PIPE_SMEM_MIXED));
-}
-cudaError_t set_push_smem_mixed()
-{
-    cudaError_t e = cudaSuccess;
-    auto        k = [&](cudaError_t x) {
-        if (e == cudaSuccess)
-            e = x;
-    };
-    k(push_attr_mixed<1, false, 0>()), k(push_attr_mixed<1, false, 1>()), k(push_attr_mixed<1, false, 2>());
-    k(push_attr_mixed<1, true, 0>()), k(push_attr_mixed<1, true, 1>()), k(push_attr_mixed<1, true, 2>());
-    k(push_attr_mixed<2, false, 0>()), k(push_attr_mixed<2, false, 1>()), k(push_attr_mixed<2, false, 2>());
-    k(push_attr_mixed<2, true, 0>()), k(push_attr_mixed<2, true, 1>()), k(push_attr_mixed<2, true, 2>());
-    k(push_attr_mixed<3, false, 0>()), k(push_attr_mixed<3, false, 1>()), k(push_attr_mixed<3, false, 2>());
-    k(push_attr_mixed<3, true, 0>()), k(push_attr_mixed<3, true, 1>()), k(push_attr_mixed<3, true, 2>());
-    return e;
-}
-template <int O, bool MIRROR>
-void launch_push_mixed_bc(PushArgsMixed const &a, int bc, dim3 g, cudaStream_t st)
-{
-    if (bc == H1D_BC_PERIODIC)
-        push_kernel_mixed<O, MIRROR, BCK_PERIODIC><<<g, PIPE_THREADS, PIPE_SMEM_MIXED, st>>>(a);
-    else if (bc == H1D_BC_REFLECTING)
-        push_kernel_mixed<O, MIRROR, BCK_REFLECTING><<<g, PIPE_THREADS, PIPE_SMEM_MIXED, st>>>(a);
-    else
-        push_kernel_mixed<O, MIRROR, BCK_ABSORBING><<<g, PIPE_THREADS, PIPE_SMEM_MIXED, st>>>(a);
-}
-template <int O>
-void launch_push_mixed_o(PushArgsMixed const &a, bool mirror, int bc, dim3 g, cudaStream_t st)
-{
-    if (mirror)
-        launch_push_mixed_bc<O, true>(a, bc, g, st);
-    else
-        launch_push_mixed_bc<O, false>(a, bc, g, st);
-}
-// the mixed-precision pass of species s with the pass settings of `a` (constants rounded to FP32)
-int launch_push_mixed(h1d_run *run, int s, PushArgs const &a)
+// the mixed-precision arguments of species s with the pass settings of `a` (constants in FP32)
+PushArgsMixed mixed_args(h1d_run *run, int s, PushArgs const &a)
 {
     SpeciesState &S = run->sp[s];
     PushArgsMixed m{};
@@ -390,34 +314,24 @@ int launch_push_mixed(h1d_run *run, int s, PushArgs const &a)
     m.status = a.status, m.fallbacks = a.fallbacks, m.seed = a.seed, m.counter = a.counter;
     m.species = a.species, m.randomize = a.randomize;
     m.move_steps = a.move_steps, m.deposit_mask = a.deposit_mask, m.write_back = a.write_back;
-    int64_t const chunks = (a.n + PIPE_CHUNK - 1) / PIPE_CHUNK;
-    dim3 const    g(static_cast<unsigned>(
-        std::min<int64_t>(chunks, static_cast<int64_t>(run->num_sms) * PIPE_CTAS_PER_SM_MIXED)));
-    bool const mirror = run->p.xi != 0;
-    switch (run->p.kinetic[s].shape_order) {
-    case 1: launch_push_mixed_o<1>(m, mirror, run->p.particle_bc, g, run->stream); break;
-    case 2: launch_push_mixed_o<2>(m, mirror, run->p.particle_bc, g, run->stream); break;
-    default: launch_push_mixed_o<3>(m, mirror, run->p.particle_bc, g, run->stream); break;
-    }
-    CU(cudaGetLastError());
-    return H1D_OK;
+    return m;
 }
 
 int launch_push(h1d_run *run, int s, PushArgs const &a)
 {
     if (a.n == 0)
         return H1D_OK;
-    if (run->mixed)
-        return launch_push_mixed(run, s, a);
-    int64_t const chunks = (a.n + PIPE_CHUNK - 1) / PIPE_CHUNK;
-    dim3 const    g(static_cast<unsigned>(std::min<int64_t>(chunks, static_cast<int64_t>(run->num_sms) * PIPE_CTAS_PER_SM)));
-    bool const    mirror = run->p.xi != 0;
-    switch (run->p.kinetic[s].shape_order) {
-    case 1: launch_push_o<1>(a, mirror, run->p.particle_bc, g, run->stream); break;
-    case 2: launch_push_o<2>(a, mirror, run->p.particle_bc, g, run->stream); break;
-    default: launch_push_o<3>(a, mirror, run->p.particle_bc, g, run->stream); break;
+    int const  order  = run->p.kinetic[s].shape_order;
+    bool const mirror = run->p.xi != 0;
+    if (run->mixed) {
+        PushArgsMixed const m = mixed_args(run, s, a);
+        CU(launch_push_groups(&m, 1, order, mirror, run->p.particle_bc,
+                              run->num_sms * (run->ctas_per_sm ? run->ctas_per_sm : PIPE_CTAS_PER_SM_MIXED), run->stream));
+    } else {
+        CU(launch_push_groups(&a, 1, order, mirror, run->p.particle_bc,
+                              run->num_sms * (run->ctas_per_sm ? std::min(run->ctas_per_sm, PIPE_CTAS_PER_SM) : PIPE_CTAS_PER_SM),
+                              run->stream));
     }
-    CU(cudaGetLastError());
     return H1D_OK;
 }
 
@@ -490,6 +404,8 @@ int sort_species(h1d_run *run, int s)
         CU(cudaMemcpyAsync(&dead, S.dead, sizeof dead, cudaMemcpyDeviceToHost, st));
         CU(cudaStreamSynchronize(st));
         S.n -= static_cast<int64_t>(dead);
+        if (dead)
+            run->gen++;
     }
     return H1D_OK;
 }
@@ -754,6 +670,336 @@ int noalloc_scratch_address(double **out)
     return H1D_OK;
 }
 
+
+// ------------------------------------------------------------------------------------------------
+// Ensembles (h1d_batch_*): many CAM-CL runs advanced together on one stream.  A step is one
+// launch of the particle pass per kind of group (shape order, geometry, boundary, precision) over
+// every species of every member, then one launch of the field cycle over every member's grid.
+// Steps come in blocks of sort_interval steps; every group is cell-sorted at the start of a block.
+// Two blocks restore every ping-pong parity, so a pair of blocks is captured once as a CUDA graph
+// and replayed while the members' state signature is unchanged.
+// ------------------------------------------------------------------------------------------------
+} // namespace
+
+struct h1d_batch {
+    std::vector<h1d_run *>     runs;
+    std::vector<cudaStream_t>  saved;
+    cudaStream_t               stream = nullptr;
+    int                        device = 0, num_sms = 148;
+    int                        k = 16;          // sort interval = steps per block
+    int                        ctas = 0;        // CTAs per SM of the particle pass (0: defaults)
+    bool                       use_graphs = true;
+    int                        since_block = 1 << 30;
+    int                        L = 0, nblocks = 0;
+    size_t                     smem = 0;
+    FieldArgs                 *d_table = nullptr; // [2][runs]: state parity 0 and 1
+    FieldBlock                *d_map = nullptr;
+    int                        parity = 0;
+    cudaGraph_t                graph = nullptr;
+    cudaGraphExec_t            exec = nullptr;
+    std::vector<int64_t>       graph_sig;
+    int64_t                    graph_kernels = 0;
+    bool                       capturing = false, graphs_warm = false;
+    h1d_batch_stats            stats{};
+    std::string                msg;
+};
+
+namespace {
+
+int bset_err(h1d_batch *b, int code, std::string const &m)
+{
+    if (b)
+        b->msg = m;
+    return code;
+}
+#define BCU(call)                                                                                            \
+    do {                                                                                                     \
+        cudaError_t const e_ = (call);                                                                       \
+        if (e_ != cudaSuccess)                                                                               \
+            return bset_err(b, e_ == cudaErrorMemoryAllocation ? H1D_ERR_OOM : H1D_ERR_CUDA,                 \
+                            fmt("%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__));       \
+    } while (0)
+#define BTRY(r, x)                                                                                           \
+    do {                                                                                                     \
+        int const st_ = (x);                                                                                 \
+        if (st_ != H1D_OK)                                                                                   \
+            return bset_err(b, st_, (r)->msg);                                                               \
+    } while (0)
+
+bool graph_eligible(h1d_batch const *b)
+{
+    if (!b->use_graphs)
+        return false;
+    for (h1d_run const *r : b->runs)
+        if (r->p.particle_bc == H1D_BC_ABSORBING || r->p.randomize_gyrophase)
+            return false;
+    return true;
+}
+
+// everything a captured pair of blocks depends on
+std::vector<int64_t> batch_signature(h1d_batch const *b)
+{
+    std::vector<int64_t> sig{ b->k, b->ctas, b->parity, static_cast<int64_t>(b->runs.size()) };
+    for (h1d_run const *r : b->runs) {
+        sig.push_back(static_cast<int64_t>(r->gen));
+        sig.push_back(r->fcur), sig.push_back(r->dset);
+        for (int c = 0; c < r->p.n_cold; ++c)
+            sig.push_back(r->cold[c].cur);
+        for (int s = 0; s < r->p.n_kinetic; ++s)
+            sig.push_back(r->sp[s].cur), sig.push_back(r->sp[s].n);
+    }
+    return sig;
+}
+
+void drop_graph(h1d_batch *b)
+{
+    if (b->exec)
+        cudaGraphExecDestroy(b->exec);
+    if (b->graph)
+        cudaGraphDestroy(b->graph);
+    b->exec = nullptr, b->graph = nullptr;
+    b->graph_sig.clear();
+}
+
+// field launch geometry shared by the members (one block size) and the per-parity argument tables
+int build_field_tables(h1d_batch *b)
+{
+    int L = FIELD_BLOCK_MIN;
+    for (h1d_run const *r : b->runs)
+        L = std::max(L, r->L);
+    std::vector<FieldArgs>  tab(2 * b->runs.size());
+    std::vector<FieldBlock> map;
+    for (size_t i = 0; i < b->runs.size(); ++i) {
+        h1d_run *r   = b->runs[i];
+        int const seg = static_cast<int>(std::min<long>(L - 2 * r->H, r->Nx));
+        int const nb  = static_cast<int>((r->Nx + seg - 1) / seg);
+        for (int blk = 0; blk < nb; ++blk)
+            map.push_back({ static_cast<int>(i), blk });
+        for (int par = 0; par < 2; ++par) {
+            if (par) { // the state after one step
+                r->fcur ^= 1, r->dset ^= 1;
+                for (int c = 0; c < r->p.n_cold; ++c)
+                    r->cold[c].cur ^= 1;
+            }
+            FieldArgs a = field_args(r);
+            a.seg       = seg;
+            tab[par * b->runs.size() + i] = a;
+            if (par) {
+                r->fcur ^= 1, r->dset ^= 1;
+                for (int c = 0; c < r->p.n_cold; ++c)
+                    r->cold[c].cur ^= 1;
+            }
+        }
+    }
+    size_t const smem = sizeof(double) * static_cast<size_t>(L) * (SMEM_SCALARS + 3 * SMEM_VECTORS);
+    if (L != b->L || static_cast<int>(map.size()) != b->nblocks || !b->d_table) {
+        cudaFree(b->d_table), cudaFree(b->d_map);
+        b->d_table = nullptr, b->d_map = nullptr;
+        BCU(cudaMalloc(&b->d_table, sizeof(FieldArgs) * tab.size()));
+        BCU(cudaMalloc(&b->d_map, sizeof(FieldBlock) * map.size()));
+        BCU(set_field_batch_smem(smem));
+        drop_graph(b);
+    }
+    b->L = L, b->nblocks = static_cast<int>(map.size()), b->smem = smem, b->parity = 0;
+    BCU(cudaMemcpyAsync(b->d_table, tab.data(), sizeof(FieldArgs) * tab.size(), cudaMemcpyHostToDevice, b->stream));
+    BCU(cudaMemcpyAsync(b->d_map, map.data(), sizeof(FieldBlock) * map.size(), cudaMemcpyHostToDevice, b->stream));
+    BCU(cudaStreamSynchronize(b->stream));
+    return H1D_OK;
+}
+
+// one CAM-CL step of every member (sorting all groups first at a block start)
+int batch_step(h1d_batch *b)
+{
+    if (b->since_block >= b->k) {
+        for (h1d_run *r : b->runs)
+            for (int s = 0; s < r->p.n_kinetic; ++s) {
+                int const passes = r->Nx < 256 ? 1 : 2;
+                BTRY(r, sort_species(r, s));
+                b->stats.kernel_launches += r->sp[s].n > 0 ? 2 + 5 * passes : 0;
+            }
+        b->since_block = 0;
+    }
+    // particle pass: one launch per kind of group
+    struct Kind {
+        int  order, bc;
+        bool mirror, mixed;
+        bool operator==(Kind const &o) const
+        {
+            return order == o.order && bc == o.bc && mirror == o.mirror && mixed == o.mixed;
+        }
+    };
+    std::vector<Kind>                       kinds;
+    std::vector<std::vector<PushArgs>>      fp;
+    std::vector<std::vector<PushArgsMixed>> mx;
+    for (h1d_run *r : b->runs)
+        for (int s = 0; s < r->p.n_kinetic; ++s) {
+            if (r->sp[s].n == 0)
+                continue;
+            Kind const kd{ static_cast<int>(r->p.kinetic[s].shape_order), r->p.particle_bc, r->p.xi != 0, r->mixed };
+            size_t     ki = 0;
+            while (ki < kinds.size() && !(kinds[ki] == kd))
+                ++ki;
+            if (ki == kinds.size())
+                kinds.push_back(kd), fp.emplace_back(), mx.emplace_back();
+            PushArgs const a = push_args(r, s);
+            if (kd.mixed)
+                mx[ki].push_back(mixed_args(r, s, a));
+            else
+                fp[ki].push_back(a);
+        }
+    for (size_t ki = 0; ki < kinds.size(); ++ki) {
+        Kind const &kd = kinds[ki];
+        if (kd.mixed)
+            BCU(launch_push_groups(mx[ki].data(), static_cast<int>(mx[ki].size()), kd.order, kd.mirror, kd.bc,
+                                   b->num_sms * (b->ctas ? b->ctas : PIPE_CTAS_PER_SM_MIXED), b->stream));
+        else
+            BCU(launch_push_groups(fp[ki].data(), static_cast<int>(fp[ki].size()), kd.order, kd.mirror, kd.bc,
+                                   b->num_sms * (b->ctas ? std::min(b->ctas, PIPE_CTAS_PER_SM) : PIPE_CTAS_PER_SM),
+                                   b->stream));
+        size_t const groups = kd.mixed ? mx[ki].size() : fp[ki].size();
+        b->stats.kernel_launches += static_cast<int64_t>((groups + BATCH_GROUPS - 1) / BATCH_GROUPS);
+    }
+    // field cycle of every member
+    BCU(launch_camcl_fields_batch(b->d_table + b->parity * b->runs.size(), b->d_map, b->nblocks, b->L, b->smem,
+                                  b->stream));
+    b->stats.kernel_launches += 1;
+    for (h1d_run *r : b->runs) {
+        r->fcur ^= 1, r->dset ^= 1;
+        for (int c = 0; c < r->p.n_cold; ++c)
+            r->cold[c].cur ^= 1;
+        for (int s = 0; s < r->p.n_kinetic; ++s)
+            r->sp[s].since_sort++;
+        r->step++;
+        r->moments_stale = true;
+    }
+    b->parity ^= 1;
+    b->since_block++;
+    b->stats.steps++;
+    return H1D_OK;
+}
+
+// the members' first advance: ghost cells of E and B and the push record
+int batch_prepare(h1d_batch *b)
+{
+    for (h1d_run *r : b->runs) {
+        if (!r->recurring || r->fields_dirty) {
+            BTRY(r, prepare_fields(r));
+            b->stats.kernel_launches += 1;
+        }
+        r->recurring = true;
+    }
+    return H1D_OK;
+}
+
+int batch_advance(h1d_batch *b, uint32_t n_steps)
+{
+    if (n_steps == 0)
+        return H1D_OK;
+    for (h1d_run *r : b->runs)
+        r->profiling = false; // phase events are not recorded inside a batch
+    if (int const st = batch_prepare(b))
+        return st;
+    if (int const st = build_field_tables(b))
+        return st;
+    uint32_t left = n_steps;
+    // finish the current block eagerly
+    for (; left > 0 && b->since_block < b->k; --left)
+        if (int const st = batch_step(b))
+            return st;
+    uint32_t const pair = 2u * static_cast<uint32_t>(b->k);
+    if (graph_eligible(b)) {
+        while (left >= pair) {
+            std::vector<int64_t> const sig = batch_signature(b);
+            if (b->exec && sig == b->graph_sig) {
+                BCU(cudaGraphLaunch(b->exec, b->stream));
+                for (h1d_run *r : b->runs) { // the host side of the replayed steps
+                    r->step += pair;
+                    for (int s = 0; s < r->p.n_kinetic; ++s)
+                        r->sp[s].since_sort = b->k;
+                    r->moments_stale = true;
+                }
+                b->stats.graph_launches++;
+                b->stats.kernel_launches += b->graph_kernels;
+                b->stats.steps += pair;
+                left -= pair;
+                continue;
+            }
+            if (b->exec) { // the members changed: the next capture follows an eager pair again
+                drop_graph(b);
+                b->graphs_warm = false;
+            }
+            if (!b->graphs_warm) { // a first eager pair sizes every scratch buffer
+                for (uint32_t i = 0; i < pair; ++i)
+                    if (int const st = batch_step(b))
+                        return st;
+                b->graphs_warm = true;
+                left -= pair;
+                continue;
+            }
+            int64_t const k0 = b->stats.kernel_launches, s0 = b->stats.steps;
+            BCU(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            b->capturing = true;
+            int st       = H1D_OK;
+            for (uint32_t i = 0; i < pair && st == H1D_OK; ++i)
+                st = batch_step(b);
+            cudaGraph_t       g  = nullptr;
+            cudaError_t const ec = cudaStreamEndCapture(b->stream, &g);
+            b->capturing         = false;
+            if (st != H1D_OK) {
+                if (g)
+                    cudaGraphDestroy(g);
+                return st;
+            }
+            BCU(ec);
+            b->graph = g;
+            BCU(cudaGraphInstantiate(&b->exec, g, 0));
+            b->graph_kernels = b->stats.kernel_launches - k0;
+            b->stats.kernel_launches = k0, b->stats.steps = s0;
+            // the capture advanced the host state by a pair; the signature is that of its start
+            b->graph_sig = sig;
+            b->stats.graphs_built++;
+            BCU(cudaGraphLaunch(b->exec, b->stream));
+            b->stats.graph_launches++;
+            b->stats.kernel_launches += b->graph_kernels;
+            b->stats.steps += pair;
+            left -= pair;
+        }
+    }
+    for (; left > 0; --left)
+        if (int const st = batch_step(b))
+            return st;
+    return H1D_OK;
+}
+
+int batch_check(h1d_batch *b)
+{
+    BCU(cudaStreamSynchronize(b->stream));
+    for (h1d_run *r : b->runs)
+        if (int const st = check_status(r))
+            return bset_err(b, st, fmt("member run %p: %s", static_cast<void *>(r), r->msg.c_str()));
+    return H1D_OK;
+}
+
+// time `steps` batch steps (eager, whole blocks) in milliseconds
+int batch_time(h1d_batch *b, uint32_t steps, float *ms)
+{
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    BCU(cudaEventCreate(&e0));
+    BCU(cudaEventCreate(&e1));
+    int st = H1D_OK;
+    if (cudaEventRecord(e0, b->stream) != cudaSuccess)
+        st = bset_err(b, H1D_ERR_CUDA, "event record failed");
+    for (uint32_t i = 0; i < steps && st == H1D_OK; ++i)
+        st = batch_step(b);
+    if (st == H1D_OK && (cudaEventRecord(e1, b->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess
+                         || cudaEventElapsedTime(ms, e0, e1) != cudaSuccess))
+        st = bset_err(b, H1D_ERR_CUDA, "event timing failed");
+    cudaEventDestroy(e0), cudaEventDestroy(e1);
+    if (st == H1D_OK)
+        st = batch_check(b);
+    return st;
+}
+
 } // namespace
 
 // ------------------------------------------------------------------------------------------------
@@ -906,8 +1152,8 @@ int h1d_create(h1d_params const *params, h1d_run **out)
     run->nblocks_field = static_cast<int>((run->Nx + run->seg - 1) / run->seg);
     run->field_smem    = sizeof(double) * static_cast<size_t>(L) * (SMEM_SCALARS + 3 * SMEM_VECTORS);
     run->mixed = p.precision == H1D_PREC_MIXED;
-    if (set_field_smem(run->field_smem) != cudaSuccess || set_push_smem() != cudaSuccess
-        || (run->mixed && set_push_smem_mixed() != cudaSuccess))
+    if (set_field_smem(run->field_smem) != cudaSuccess || set_push_smem_fp64() != cudaSuccess
+        || set_push_smem_mixed() != cudaSuccess)
         return fail(H1D_ERR_CUDA);
     cudaDeviceGetAttribute(&run->num_sms, cudaDevAttrMultiProcessorCount, run->device);
 
@@ -1040,6 +1286,7 @@ int h1d_upload_particles(h1d_run *run, int s, int64_t n, double const *q1, doubl
         CU(launch_iota(S.pid[0], n, run->stream));
     S.since_sort       = 1 << 30;
     run->moments_stale = true;
+    run->gen++;
     CU(cudaStreamSynchronize(run->stream));
     return H1D_OK;
 }
@@ -1055,6 +1302,7 @@ int h1d_upload_fields(h1d_run *run, double const *B, double const *E)
         CU(cudaMemcpyAsync(run->E[run->fcur], E, bytes, cudaMemcpyHostToDevice, run->stream));
     CU(cudaStreamSynchronize(run->stream));
     run->fields_dirty = true;
+    run->gen++;
     return H1D_OK;
 }
 
@@ -1068,6 +1316,7 @@ int h1d_upload_cold(h1d_run *run, int i, double const *n_full, double const *nV_
     CU(cudaMemcpyAsync(C.nV[1 - C.cur], nV_full, sizeof(double) * 3 * run->M, cudaMemcpyHostToDevice, run->stream));
     CU(cudaStreamSynchronize(run->stream));
     run->moments_stale = true;
+    run->gen++;
     return H1D_OK;
 }
 
@@ -1255,6 +1504,207 @@ int h1d_download_cold(h1d_run *run, int i, double *n, double *nV, double *nvv, d
         CU(cudaMemcpyAsync(nV_full, C.nV[C.cur], sizeof(double) * 3 * M, cudaMemcpyDeviceToHost, run->stream));
     CU(cudaStreamSynchronize(run->stream));
     return H1D_OK;
+}
+
+
+// ---- ensembles -----------------------------------------------------------------------------------
+
+int h1d_batch_create(h1d_run *const *runs, int n_runs, h1d_batch **out)
+{
+    if (!out)
+        return H1D_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (!runs || n_runs <= 0) {
+        std::fprintf(stderr, "h1d_batch_create: no runs\n");
+        return H1D_ERR_INVALID_ARG;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return H1D_ERR_NO_DEVICE;
+    for (int i = 0; i < n_runs; ++i) {
+        h1d_run *r = runs[i];
+        char const *why = !r ? "null run"
+                          : r->p.algorithm != H1D_ALGO_CAMCL ? "batches advance CAM-CL runs only"
+                          : r->device != dev                ? "run lives on another device"
+                          : r->batch_count                  ? "run is already a member of a batch"
+                                                            : nullptr;
+        for (int j = 0; j < i && !why; ++j)
+            if (runs[j] == r)
+                why = "run listed twice";
+        if (why) {
+            std::fprintf(stderr, "h1d_batch_create: member %d: %s\n", i, why);
+            return H1D_ERR_INVALID_ARG;
+        }
+    }
+    h1d_batch *b = new (std::nothrow) h1d_batch{};
+    if (!b)
+        return H1D_ERR_OOM;
+    b->device = dev;
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete b;
+        return H1D_ERR_CUDA;
+    }
+    cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, dev);
+    b->k = runs[0]->sort_interval;
+    for (int i = 0; i < n_runs; ++i) {
+        h1d_run *r = runs[i];
+        cudaStreamSynchronize(r->stream);
+        b->runs.push_back(r);
+        b->saved.push_back(r->stream);
+        r->stream      = b->stream;
+        r->batch_count = 1;
+    }
+    *out = b;
+    return H1D_OK;
+}
+
+int h1d_batch_destroy(h1d_batch *b)
+{
+    if (!b)
+        return H1D_OK;
+    cudaStreamSynchronize(b->stream);
+    for (size_t i = 0; i < b->runs.size(); ++i) {
+        b->runs[i]->stream      = b->saved[i];
+        b->runs[i]->batch_count = 0;
+        for (int s = 0; s < b->runs[i]->p.n_kinetic; ++s) // the run resumes its own sort schedule
+            b->runs[i]->sp[s].since_sort = std::min(b->runs[i]->sp[s].since_sort, b->since_block);
+    }
+    drop_graph(b);
+    cudaFree(b->d_table), cudaFree(b->d_map);
+    cudaStreamDestroy(b->stream);
+    delete b;
+    return H1D_OK;
+}
+
+int h1d_batch_advance_async(h1d_batch *b, uint32_t n_steps)
+{
+    if (!b)
+        return H1D_ERR_INVALID_ARG;
+    return batch_advance(b, n_steps);
+}
+
+int h1d_batch_synchronize(h1d_batch *b)
+{
+    if (!b)
+        return H1D_ERR_INVALID_ARG;
+    return batch_check(b);
+}
+
+int h1d_batch_advance(h1d_batch *b, uint32_t n_steps)
+{
+    TRY(h1d_batch_advance_async(b, n_steps));
+    return h1d_batch_synchronize(b);
+}
+
+int h1d_batch_get_stream(h1d_batch *b, void **stream)
+{
+    if (!b || !stream)
+        return H1D_ERR_INVALID_ARG;
+    *stream = b->stream;
+    return H1D_OK;
+}
+
+int h1d_batch_configure(h1d_batch *b, int sort_interval, int push_ctas_per_sm, int use_graphs)
+{
+    if (!b || sort_interval < 0 || sort_interval > 4096 || push_ctas_per_sm < 0 || push_ctas_per_sm > PIPE_CTAS_PER_SM_MIXED)
+        return bset_err(b, H1D_ERR_INVALID_ARG, "h1d_batch_configure: sort_interval in [0, 4096], CTAs per SM in [0, 3]");
+    if (sort_interval > 0 && sort_interval != b->k)
+        b->k = sort_interval, b->since_block = 1 << 30;
+    b->ctas       = push_ctas_per_sm;
+    b->use_graphs = use_graphs != 0;
+    drop_graph(b);
+    b->graphs_warm = false;
+    return H1D_OK;
+}
+
+int h1d_batch_autotune(h1d_batch *b, uint32_t *steps_taken, int *sort_interval, int *push_ctas_per_sm)
+{
+    if (!b)
+        return H1D_ERR_INVALID_ARG;
+    TRY(batch_prepare(b));
+    TRY(build_field_tables(b));
+    drop_graph(b);
+    b->graphs_warm = false;
+    uint32_t taken = 0;
+    // 1. sort interval, at the default CTA count: two whole blocks per candidate
+    int   best_k  = b->k;
+    float best_ms = 0;
+    for (int k : { 8, 16, 32 }) {
+        b->k           = k;
+        b->since_block = 1 << 30;
+        float ms       = 0;
+        TRY(batch_time(b, 2u * k, &ms));
+        taken += 2u * k;
+        float const per = ms / (2.0f * k);
+        if (best_ms == 0 || per < best_ms)
+            best_ms = per, best_k = k;
+    }
+    b->k = best_k;
+    // 2. CTAs per SM of the particle pass, at the chosen interval
+    bool any_mixed = false;
+    for (h1d_run const *r : b->runs)
+        any_mixed = any_mixed || r->mixed;
+    int const max_c  = any_mixed ? PIPE_CTAS_PER_SM_MIXED : PIPE_CTAS_PER_SM;
+    int       best_c = 0;
+    best_ms          = 0;
+    for (int c = 1; c <= max_c; ++c) {
+        b->ctas        = c;
+        b->since_block = 1 << 30;
+        float ms       = 0;
+        TRY(batch_time(b, 2u * b->k, &ms));
+        taken += 2u * b->k;
+        float const per = ms / (2.0f * b->k);
+        if (best_ms == 0 || per < best_ms)
+            best_ms = per, best_c = c;
+    }
+    b->ctas = best_c;
+    for (h1d_run *r : b->runs)
+        r->sort_interval = b->k, r->ctas_per_sm = b->ctas;
+    if (steps_taken)
+        *steps_taken = taken;
+    if (sort_interval)
+        *sort_interval = b->k;
+    if (push_ctas_per_sm)
+        *push_ctas_per_sm = b->ctas;
+    return H1D_OK;
+}
+
+int h1d_batch_stats_read(h1d_batch *b, h1d_batch_stats *out)
+{
+    if (!b || !out)
+        return H1D_ERR_INVALID_ARG;
+    *out = b->stats;
+    return H1D_OK;
+}
+
+char const *h1d_batch_status_string(h1d_batch *b) { return b ? b->msg.c_str() : "null batch"; }
+
+// ---- tuning of a single run ----------------------------------------------------------------------
+
+int h1d_configure(h1d_run *run, int sort_interval, int push_ctas_per_sm)
+{
+    if (!run || sort_interval < 0 || sort_interval > 4096 || push_ctas_per_sm < 0 || push_ctas_per_sm > PIPE_CTAS_PER_SM_MIXED)
+        return set_err(run, H1D_ERR_INVALID_ARG, "h1d_configure: sort_interval in [0, 4096], CTAs per SM in [0, 3]");
+    if (sort_interval > 0)
+        run->sort_interval = sort_interval;
+    run->ctas_per_sm = push_ctas_per_sm;
+    return H1D_OK;
+}
+
+int h1d_autotune(h1d_run *run, uint32_t *steps_taken, int *sort_interval, int *push_ctas_per_sm)
+{
+    if (!run)
+        return H1D_ERR_INVALID_ARG;
+    if (run->p.algorithm != H1D_ALGO_CAMCL || run->batch_count)
+        return set_err(run, H1D_ERR_INVALID_ARG, "h1d_autotune: a CAM-CL run outside any batch");
+    h1d_batch *b  = nullptr;
+    int        st = h1d_batch_create(&run, 1, &b);
+    if (st == H1D_OK)
+        st = h1d_batch_autotune(b, steps_taken, sort_interval, push_ctas_per_sm);
+    if (st != H1D_OK && b)
+        set_err(run, st, b->msg);
+    h1d_batch_destroy(b);
+    return st;
 }
 
 int h1d_energy(h1d_run *run, double *dB2O2, double *dE2O2, double *KE_lab, double *KE_pla)

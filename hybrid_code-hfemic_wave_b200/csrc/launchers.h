@@ -19,6 +19,12 @@ struct EnergyArgs {
 cudaError_t set_field_smem(size_t bytes);
 cudaError_t launch_camcl_fields(FieldArgs const &a, int blocks, int threads, size_t smem, cudaStream_t st);
 cudaError_t launch_pc_fields(FieldArgs const &a, int blocks, int threads, size_t smem, cudaStream_t st);
+// an ensemble in one launch: block b runs segment map[b].seg of run map[b].run (device arrays)
+cudaError_t set_field_batch_smem(size_t bytes);
+cudaError_t launch_camcl_fields_batch(FieldArgs const *table, FieldBlock const *map, int blocks, int threads,
+                                      size_t smem, cudaStream_t st);
+cudaError_t launch_pc_fields_batch(FieldArgs const *table, FieldBlock const *map, int blocks, int threads,
+                                   size_t smem, cudaStream_t st);
 cudaError_t launch_prep_fields(double *B, double *E, double *EB, float *EBf, int Nx, cudaStream_t st);
 cudaError_t launch_finalize_kinetic(double const *raw, double *out, int Nx, double s1, int reflecting, cudaStream_t st);
 cudaError_t launch_finalize_cold(double const *n_full, double const *nV_full, double *out, int Nx, double w,

@@ -1,0 +1,239 @@
+// Particle kernels outside the particle pass: collect_all of n, nV and nvv for the recorders
+// (PartSpecies::impl_collect_all, PartSpecies.cc:330-349) in both precisions, the FP64 <->
+// mixed-precision conversions of upload and download, and the cell keys and gather of the
+// mixed-precision cell sort.  Compiled in the library's main translation unit only.
+#pragma once
+
+#include "particles_mixed.cuh"
+
+namespace h1d {
+
+// PartSpecies::impl_collect_all (PartSpecies.cc:330-349): n, nV and nvv with CIC, unscaled
+struct MomentArgs {
+    double const  *q1, *vx, *vy, *vz, *w;
+    int64_t        n;
+    int            ppt, Nx;
+    double         half_min;
+    double        *out[10]; // n, nVx, nVy, nVz, xx, yy, zz, xy, yz, zx at cell 0
+    unsigned      *status;
+};
+
+__global__ void __launch_bounds__(256) moments_kernel(MomentArgs a)
+{
+    constexpr int S = 4; // CIC + window of 2
+    int const     lane   = threadIdx.x & 31;
+    int64_t const warp   = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    int64_t const chunk0 = warp * 32 * a.ppt;
+    if (chunk0 >= a.n)
+        return;
+    int first = 0x7fffffff;
+    if (chunk0 + lane < a.n)
+        first = make_shape<1>(a.q1[chunk0 + lane] - a.half_min).i0;
+    int const base = __reduce_min_sync(0xffffffffu, first) - 1;
+    double    acc[10][S];
+#pragma unroll
+    for (int q = 0; q < 10; ++q)
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+            acc[q][s] = 0;
+    unsigned bad = 0;
+    for (int k = 0; k < a.ppt; ++k) {
+        int64_t const idx = chunk0 + static_cast<int64_t>(k) * 32 + lane;
+        if (idx >= a.n)
+            break;
+        double const   q1 = a.q1[idx], vx = a.vx[idx], vy = a.vy[idx], vz = a.vz[idx], w = a.w[idx];
+        Shape<1> const sh = make_shape<1>(q1 - a.half_min);
+        if (!finite_pos(q1) || !stencil_ok(sh, a.Nx)) {
+            bad |= ST_OUT_OF_RANGE;
+            continue;
+        }
+        double const val[10] = { w,           vx * w,      vy * w,      vz * w,      (vx * vx) * w,
+                                 (vy * vy) * w, (vz * vz) * w, (vx * vy) * w, (vy * vz) * w, (vz * vx) * w };
+        int const    r       = sh.i0 - base;
+        if (r >= 0 && r <= S - 2) {
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                double const ws = (s == r) ? sh.w[0] : (s == r + 1) ? sh.w[1] : 0.0;
+#pragma unroll
+                for (int q = 0; q < 10; ++q)
+                    acc[q][s] = fma(val[q], ws, acc[q][s]);
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j <= 1; ++j)
+#pragma unroll
+                for (int q = 0; q < 10; ++q)
+                    atomicAdd(a.out[q] + sh.i0 + j, val[q] * sh.w[j]);
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 10; ++q)
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            double const v = warp_sum(acc[q][s]);
+            if (lane == (q * S + s) % 32 && v != 0.0) {
+                int const cell = base + s;
+                if (cell >= -PAD && cell < a.Nx + PAD)
+                    atomicAdd(a.out[q] + cell, v);
+                else
+                    bad |= ST_OUT_OF_RANGE;
+            }
+        }
+    bad = __reduce_or_sync(0xffffffffu, bad);
+    if (bad && lane == 0)
+        atomicOr(a.status, bad);
+}
+
+// collect_all (n, nV, nvv with CIC, PartSpecies.cc:330-349) from mixed-precision particles: the
+// same per-warp window scheme as moments_kernel (particles.cuh), accumulated in FP64
+struct MomentArgsMixed {
+    int32_t const *cell;
+    float const   *off, *vx, *vy, *vz, *w;
+    int64_t        n;
+    int            ppt, Nx;
+    double        *out[10];
+    unsigned      *status;
+};
+__global__ void __launch_bounds__(256) moments_kernel_mixed(MomentArgsMixed a)
+{
+    constexpr int S = 4;
+    int const     lane   = threadIdx.x & 31;
+    int64_t const warp   = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    int64_t const chunk0 = warp * 32 * a.ppt;
+    if (chunk0 >= a.n)
+        return;
+    int first = 0x7fffffff;
+    if (chunk0 + lane < a.n)
+        first = make_shape_f<1>(a.cell[chunk0 + lane], a.off[chunk0 + lane]).i0;
+    int const base = __reduce_min_sync(0xffffffffu, first) - 1;
+    double    acc[10][S];
+#pragma unroll
+    for (int q = 0; q < 10; ++q)
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+            acc[q][s] = 0;
+    unsigned bad = 0;
+    for (int k = 0; k < a.ppt; ++k) {
+        int64_t const idx = chunk0 + static_cast<int64_t>(k) * 32 + lane;
+        if (idx >= a.n)
+            break;
+        ShapeF<1> const sh = make_shape_f<1>(a.cell[idx], a.off[idx]);
+        if (!stencil_ok_f(sh, a.Nx)) {
+            bad |= ST_OUT_OF_RANGE;
+            continue;
+        }
+        double const w = a.w[idx], vx = a.vx[idx], vy = a.vy[idx], vz = a.vz[idx];
+        double const val[10] = { w,           vx * w,      vy * w,      vz * w,      (vx * vx) * w,
+                                 (vy * vy) * w, (vz * vz) * w, (vx * vy) * w, (vy * vz) * w, (vz * vx) * w };
+        double const w0 = sh.w[0], w1 = sh.w[1];
+        int const    r  = sh.i0 - base;
+        if (r >= 0 && r <= S - 2) {
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+                double const ws = (s == r) ? w0 : (s == r + 1) ? w1 : 0.0;
+#pragma unroll
+                for (int q = 0; q < 10; ++q)
+                    acc[q][s] = fma(val[q], ws, acc[q][s]);
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 10; ++q) {
+                atomicAdd(a.out[q] + sh.i0, val[q] * w0);
+                atomicAdd(a.out[q] + sh.i0 + 1, val[q] * w1);
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 10; ++q)
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+            double const v = warp_sum(acc[q][s]);
+            if (lane == (q * S + s) % 32 && v != 0.0) {
+                int const cell = base + s;
+                if (cell >= -PAD && cell < a.Nx + PAD)
+                    atomicAdd(a.out[q] + cell, v);
+                else
+                    bad |= ST_OUT_OF_RANGE;
+            }
+        }
+    bad = __reduce_or_sync(0xffffffffu, bad);
+    if (bad && lane == 0)
+        atomicOr(a.status, bad);
+}
+
+// FP64 host-layout particles <-> mixed-precision particles (upload and download), one component at
+// a time so that the FP64 staging buffer holds a single array: position q1 <-> (cell, offset) with
+// cell = floor(q1 - q1min), and velocity / weight components FP64 <-> FP32
+__global__ void q1_to_mixed_kernel(double const *q1, int64_t n, double full_min, int32_t *cell, float *off)
+{
+    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    double const x  = q1[i] - full_min;
+    double const f  = floor(x);
+    bool const   ok = f > -1073741824.0 && f < 1073741824.0; // NaN and lost positions map outside the grid
+    float        o  = ok ? static_cast<float>(x - f) : 0.5f;
+    if (o >= 1.0f)
+        o = 0.99999994f;
+    cell[i] = ok ? static_cast<int32_t>(f) : -0x40000000;
+    off[i]  = o;
+}
+__global__ void to_f32_kernel(double const *src, int64_t n, float *dst)
+{
+    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n)
+        dst[i] = static_cast<float>(src[i]);
+}
+// one component at a time, so that the caller's FP64 staging buffer holds a single array
+__global__ void from_mixed_kernel(int32_t const *cell, float const *src, int64_t n, double full_min, double *dst)
+{
+    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    dst[i] = cell ? full_min + static_cast<double>(cell[i]) + static_cast<double>(src[i]) : static_cast<double>(src[i]);
+}
+
+// keys for the cell sort of mixed-precision particles (sort.cuh): the cell itself
+__global__ void keys_kernel_mixed(int32_t const *cell, float const *w, int64_t n, int Nx, uint32_t *keys, uint32_t *idx,
+                                  unsigned long long *dead, unsigned *status)
+{
+    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    int const c = cell[i];
+    uint32_t  k;
+    if (w[i] == 0.0f) {
+        k = static_cast<uint32_t>(Nx);
+        atomicAdd(dead, 1ull);
+    } else if (c < 0 || c >= Nx) {
+        k = c < 0 ? 0u : static_cast<uint32_t>(Nx - 1);
+        atomicOr(status, ST_OUT_OF_RANGE);
+    } else {
+        k = static_cast<uint32_t>(c);
+    }
+    keys[i] = k;
+    idx[i]  = static_cast<uint32_t>(i);
+}
+
+struct GatherArgsMixed {
+    float const   *src[5]; // off, vx, vy, vz, w
+    int32_t const *cell_src, *pid_src;
+    float         *dst[5];
+    int32_t       *cell_dst, *pid_dst;
+    uint32_t const *idx;
+    int64_t        n;
+};
+__global__ void gather_kernel_mixed(GatherArgsMixed a)
+{
+    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n)
+        return;
+    uint32_t const j = a.idx[i];
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+        a.dst[k][i] = a.src[k][j];
+    a.cell_dst[i] = a.cell_src[j];
+    a.pid_dst[i]  = a.pid_src[j];
+}
+
+} // namespace h1d

@@ -289,9 +289,9 @@ __device__ __forceinline__ void flush_rs(Acc<O, S> const &acc, int base, int lan
 }
 
 // A warp's deposit window: register accumulators over cells [base, base + S), S = O + 1 + R,
-// kept across batches and chunks.  When a batch of 32 particles reaches past the window the warp
-// flushes it and re-bases it at the batch minimum; particles below the window (drift since the
-// last sort) deposit with direct atomics.
+// kept across batches and chunks.  When a batch of 32 particles reaches outside the window the
+// warp flushes it and re-bases it at the batch minimum; particles of a batch that spans more than
+// R + 1 stencil bases deposit with direct atomics.
 template <int O, int R, int D>
 struct Window {
     static constexpr int S    = O + 1 + R;
@@ -307,8 +307,8 @@ struct Window {
     // batch step: i0 is this lane's stencil base (valid lanes only)
     __device__ __forceinline__ void prepare(bool valid, int i0, int lane, PushArgs const &a)
     {
-        bool const above = valid && i0 > base + R;
-        if (__any_sync(0xffffffffu, above)) {
+        bool const outside = valid && (i0 > base + R || i0 < base);
+        if (__any_sync(0xffffffffu, outside)) {
             if (base != NONE)
                 flush_rs<O, S, D>(acc, base, lane, a);
             acc_zero(acc);
@@ -326,34 +326,130 @@ struct Window {
     }
 };
 
+// In-warp counting sort of a warp's 32 x PIPE_PPT slots of a chunk by stencil base cell, so that
+// each batch of 32 particles handed to a deposit window spans as few cells as possible even after
+// the particles have drifted since the last global sort.  Slot s = k * 32 + lane holds key[s]
+// (INT_MAX for a slot that deposits nothing); order[] receives the slots in key order, stable in
+// (k, lane).  Keys that span more than 31 cells keep the slot order.  Ranks come from
+// __match_any_sync groups whose leaders update a per-warp histogram, so the order is
+// deterministic.
+struct WarpOrder {
+    int      key[32 * PIPE_PPT];
+    uint16_t order[32 * PIPE_PPT];
+    int      hist[32];
+};
+
+__device__ __forceinline__ void warp_order(WarpOrder &W, int lane)
+{
+    constexpr unsigned FULL = 0xffffffffu;
+    constexpr int      NONE = 0x7fffffff;
+    int                kk[PIPE_PPT];
+    int                lo = NONE, hi = -NONE;
+#pragma unroll
+    for (int k = 0; k < PIPE_PPT; ++k) {
+        kk[k] = W.key[k * 32 + lane];
+        if (kk[k] != NONE)
+            lo = min(lo, kk[k]), hi = max(hi, kk[k]);
+    }
+    lo = __reduce_min_sync(FULL, lo);
+    hi = __reduce_max_sync(FULL, hi);
+    if (lo == NONE || hi - lo > 30) {
+#pragma unroll
+        for (int k = 0; k < PIPE_PPT; ++k)
+            W.order[k * 32 + lane] = static_cast<uint16_t>(k * 32 + lane);
+        __syncwarp();
+        return;
+    }
+    W.hist[lane] = 0;
+    __syncwarp();
+    unsigned const lt = (1u << lane) - 1u;
+    int            rank[PIPE_PPT], bin[PIPE_PPT];
+#pragma unroll
+    for (int k = 0; k < PIPE_PPT; ++k) {
+        int const      b      = kk[k] == NONE ? 31 : kk[k] - lo;
+        unsigned const m      = __match_any_sync(FULL, b);
+        int const      leader = __ffs(m) - 1;
+        int            old    = 0;
+        if (lane == leader) {
+            old       = W.hist[b];
+            W.hist[b] = old + __popc(m);
+        }
+        old     = __shfl_sync(FULL, old, leader);
+        rank[k] = old + __popc(m & lt);
+        bin[k]  = b;
+        __syncwarp();
+    }
+    int const c   = W.hist[lane];
+    int       inc = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int const y = __shfl_up_sync(FULL, inc, o);
+        if (lane >= o)
+            inc += y;
+    }
+    __syncwarp();
+    W.hist[lane] = inc - c; // exclusive start of each bin
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < PIPE_PPT; ++k)
+        W.order[W.hist[bin[k]] + rank[k]] = static_cast<uint16_t>(k * 32 + lane);
+    __syncwarp();
+}
+
 // ------------------------------------------------------------------------------------------------
 // The particle pass.  Warp-specialised pipeline per CTA: one producer warp streams the CTA's
 // contiguous run of chunks (PIPE_CHUNK particles each) global -> shared with 1-D TMA bulk copies
 // completing on mbarriers (PIPE_STAGES deep) and bulk-stores the updated particles back;
 // PIPE_CONSUMER_WARPS warps compute.  A consumer warp owns 32 x PIPE_PPT consecutive
-// (cell-sorted) particles of each chunk and makes two passes over them in shared memory:
-// (1) push at x^N, deposit at x^N, move, boundary, results written in place; (2) deposit at the
-// new position.  Its two deposit windows persist across the chunks of the run.
+// (cell-sorted) particles of each chunk and makes passes over them in shared memory: (A) push at
+// x^N, move, boundary, results written beside the inputs; then, in the cell order of warp_order,
+// (B) deposit at x^N and (C) deposit at the new position.  Its two deposit windows persist
+// across the chunks of the run.
 //
 // CAM-CL (move_steps == 1): push at x^N, deposit, move, BC, deposit.
 // Predictor-corrector (move_steps == 2, Domain_PC.cc:110-124, 169-181): half move, BC, push at
 // the half-step position, half move, BC, deposit.  move_steps == 0: deposit only
 // (Domain_PC.cc:36-44).
 // ------------------------------------------------------------------------------------------------
-template <int O, bool MIRROR, int BC>
-__global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(PushArgs a)
+// The groups of particles one launch of the pass covers: a run's species (one group per launch)
+// or the species of many runs of an ensemble (up to MAXG per launch).  The launch's chunks are
+// numbered consecutively over the groups; a CTA takes a contiguous range of them, and its warps
+// flush their deposit windows and status bits whenever the range crosses into the next group.
+// The table travels as the kernel's parameter block (at most 32 KB).
+template <int MAXG>
+struct PushGroups {
+    int      n;
+    int64_t  chunk0[MAXG + 1]; // first chunk of each group; chunk0[n] = number of chunks
+    PushArgs g[MAXG];
+};
+
+template <int MAXG>
+__device__ __forceinline__ int group_of(PushGroups<MAXG> const &G, int64_t chunk, int from)
+{
+    if constexpr (MAXG == 1) {
+        return 0;
+    } else {
+        int g = from < 0 ? 0 : from;
+        while (g + 1 < G.n && chunk >= G.chunk0[g + 1])
+            ++g;
+        return g;
+    }
+}
+
+template <int O, bool MIRROR, int BC, int MAXG>
+__global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(PushGroups<MAXG> const __grid_constant__ G)
 {
     constexpr int R = 2;
     extern __shared__ __align__(128) unsigned char smraw[];
+    __shared__ WarpOrder worder[PIPE_CONSUMER_WARPS];
     PipeStage    *stage = reinterpret_cast<PipeStage *>(smraw);
     uint64_t     *full  = reinterpret_cast<uint64_t *>(smraw + sizeof(PipeStage) * PIPE_STAGES);
     uint64_t     *empty = full + PIPE_STAGES;
     int const     warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int64_t const nchunks = (a.n + PIPE_CHUNK - 1) / PIPE_CHUNK;
+    int64_t const nchunks = G.chunk0[G.n];
     int64_t const per     = (nchunks + gridDim.x - 1) / gridDim.x;
     int64_t const c0      = static_cast<int64_t>(blockIdx.x) * per;
     int64_t const mine    = c0 < nchunks ? min(per, nchunks - c0) : 0;
-    bool const    load_pid = a.randomize != 0;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < PIPE_STAGES; ++s) {
@@ -366,16 +462,19 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
 
     if (warp == PIPE_CONSUMER_WARPS) { // ---------------- producer ----------------
         if (lane == 0) {
+            int gl = -1, gr = -1; // groups of the chunk being loaded / retired
             for (int64_t i = 0; i < mine + PIPE_STAGES; ++i) {
                 int const s = static_cast<int>(i % PIPE_STAGES);
                 if (i >= PIPE_STAGES && i - PIPE_STAGES < mine) { // retire the chunk held by stage s
-                    int64_t const j = i - PIPE_STAGES;
+                    int64_t const   j = i - PIPE_STAGES;
+                    gr                = group_of(G, c0 + j, gr);
+                    PushArgs const &a = G.g[gr];
                     if (!mbar_wait(&empty[s], static_cast<uint32_t>((j / PIPE_STAGES) & 1))) {
                         atomicOr(a.status, ST_TIMEOUT);
                         break;
                     }
                     if (a.write_back) {
-                        int64_t const  start = (c0 + j) * PIPE_CHUNK;
+                        int64_t const  start = (c0 + j - G.chunk0[gr]) * PIPE_CHUNK;
                         uint32_t const cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
                         uint32_t const b8    = round16(cnt * 8);
                         bulk_store(a.q1 + start, stage[s].q1n, b8);
@@ -389,16 +488,19 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
                     bulk_wait_read_all();
                 }
                 if (i < mine) {
-                    int64_t const  start = (c0 + i) * PIPE_CHUNK;
-                    uint32_t const cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
-                    uint32_t const b8 = round16(cnt * 8), b4 = round16(cnt * 4);
-                    mbar_arrive_expect_tx(&full[s], 5 * b8 + (load_pid ? b4 : 0));
+                    gl                   = group_of(G, c0 + i, gl);
+                    PushArgs const &a    = G.g[gl];
+                    bool const      lpid = a.randomize != 0;
+                    int64_t const   start = (c0 + i - G.chunk0[gl]) * PIPE_CHUNK;
+                    uint32_t const  cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
+                    uint32_t const  b8 = round16(cnt * 8), b4 = round16(cnt * 4);
+                    mbar_arrive_expect_tx(&full[s], 5 * b8 + (lpid ? b4 : 0));
                     bulk_load(stage[s].q1, a.q1 + start, b8, &full[s]);
                     bulk_load(stage[s].vx, a.vx + start, b8, &full[s]);
                     bulk_load(stage[s].vy, a.vy + start, b8, &full[s]);
                     bulk_load(stage[s].vz, a.vz + start, b8, &full[s]);
                     bulk_load(stage[s].w, a.w + start, b8, &full[s]);
-                    if (load_pid)
+                    if (lpid)
                         bulk_load(stage[s].pid, a.pid + start, b4, &full[s]);
                 }
             }
@@ -409,21 +511,40 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
 
     // ---------------- consumers ----------------
     unsigned        bad = 0;
+    int             gc  = -1; // current group
     Window<O, R, 0> win0;
     Window<O, R, 1> win1;
     win0.init();
     win1.init();
     for (int64_t i = 0; i < mine; ++i) {
-        int const s = static_cast<int>(i % PIPE_STAGES);
+        int const s  = static_cast<int>(i % PIPE_STAGES);
+        int const gi = group_of(G, c0 + i, gc);
+        if (gi != gc) { // entering the next group: settle the previous group's windows and status
+            if (gc >= 0) {
+                PushArgs const &ap = G.g[gc];
+                if (ap.deposit_mask & 1)
+                    win0.finish(lane, ap);
+                if (ap.deposit_mask & 2)
+                    win1.finish(lane, ap);
+                bad = __reduce_or_sync(0xffffffffu, bad);
+                if (bad && lane == 0)
+                    atomicOr(ap.status, bad);
+                bad = 0;
+                win0.init();
+                win1.init();
+            }
+            gc = gi;
+        }
+        PushArgs const &a        = G.g[gc];
+        bool const      load_pid = a.randomize != 0;
         if (!mbar_wait(&full[s], static_cast<uint32_t>((i / PIPE_STAGES) & 1))) {
             bad |= ST_TIMEOUT;
             break;
         }
-        int64_t const start = (c0 + i) * PIPE_CHUNK;
+        int64_t const start = (c0 + i - G.chunk0[gc]) * PIPE_CHUNK;
         int const     cnt   = static_cast<int>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
         PipeStage    &P     = stage[s];
         int const     w0    = warp * 32 * PIPE_PPT;
-
         // pass A: push at x^N (half steps around it for PC), move, boundary; no warp collectives,
         // so the compiler interleaves the independent particles of a lane.  Slots past `cnt` hold
         // stale finite data and are processed but never deposited or stored.
@@ -445,7 +566,9 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
                 P.q1[idx] = q1; // PC deposits nothing at the push position
             }
             Shape<O> const sh = make_shape<O>(q1 - a.half_min);
-            if (finite_pos(q1) && stencil_ok(sh, a.Nx)) {
+            bool const     in_grid = finite_pos(q1) && stencil_ok(sh, a.Nx);
+            worder[warp].key[k * 32 + lane] = in_grid && idx < cnt ? sh.i0 : 0x7fffffff;
+            if (in_grid) {
                 if (alive && a.move_steps != 0) {
                     d3 E, dB;
                     interp_EB<O>(a.EB, sh, E, dB);
@@ -487,11 +610,12 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
                 P.wn[idx] = w;
         }
         __syncwarp();
+        warp_order(worder[warp], lane);
         // pass B: deposit at x^N with v^{N+1/2} (CAM-CL)
         if (a.deposit_mask & 1) {
 #pragma unroll 1
             for (int k = 0; k < PIPE_PPT; ++k) {
-                int const      idx   = w0 + k * 32 + lane;
+                int const      idx   = w0 + worder[warp].order[k * 32 + lane];
                 double const   q1    = P.q1[idx];
                 Shape<O> const sh    = make_shape<O>(q1 - a.half_min);
                 bool const     valid = idx < cnt && finite_pos(q1) && stencil_ok(sh, a.Nx);
@@ -504,7 +628,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
         if (a.deposit_mask & 2) {
 #pragma unroll 1
             for (int k = 0; k < PIPE_PPT; ++k) {
-                int const      idx   = w0 + k * 32 + lane;
+                int const      idx   = w0 + worder[warp].order[k * 32 + lane];
                 double const   q1    = P.q1n[idx];
                 Shape<O> const sh    = make_shape<O>(q1 - a.half_min);
                 bool const     valid = idx < cnt && finite_pos(q1) && stencil_ok(sh, a.Nx);
@@ -518,89 +642,17 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
         if (lane == 0)
             mbar_arrive(&empty[s]);
     }
-    if (a.deposit_mask & 1)
-        win0.finish(lane, a);
-    if (a.deposit_mask & 2)
-        win1.finish(lane, a);
-    bad = __reduce_or_sync(0xffffffffu, bad);
-    if (bad && lane == 0)
-        atomicOr(a.status, bad);
-}
-
-// PartSpecies::impl_collect_all (PartSpecies.cc:330-349): n, nV and nvv with CIC, unscaled
-struct MomentArgs {
-    double const  *q1, *vx, *vy, *vz, *w;
-    int64_t        n;
-    int            ppt, Nx;
-    double         half_min;
-    double        *out[10]; // n, nVx, nVy, nVz, xx, yy, zz, xy, yz, zx at cell 0
-    unsigned      *status;
-};
-
-__global__ void __launch_bounds__(256) moments_kernel(MomentArgs a)
-{
-    constexpr int S = 4; // CIC + window of 2
-    int const     lane   = threadIdx.x & 31;
-    int64_t const warp   = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    int64_t const chunk0 = warp * 32 * a.ppt;
-    if (chunk0 >= a.n)
-        return;
-    int first = 0x7fffffff;
-    if (chunk0 + lane < a.n)
-        first = make_shape<1>(a.q1[chunk0 + lane] - a.half_min).i0;
-    int const base = __reduce_min_sync(0xffffffffu, first) - 1;
-    double    acc[10][S];
-#pragma unroll
-    for (int q = 0; q < 10; ++q)
-#pragma unroll
-        for (int s = 0; s < S; ++s)
-            acc[q][s] = 0;
-    unsigned bad = 0;
-    for (int k = 0; k < a.ppt; ++k) {
-        int64_t const idx = chunk0 + static_cast<int64_t>(k) * 32 + lane;
-        if (idx >= a.n)
-            break;
-        double const   q1 = a.q1[idx], vx = a.vx[idx], vy = a.vy[idx], vz = a.vz[idx], w = a.w[idx];
-        Shape<1> const sh = make_shape<1>(q1 - a.half_min);
-        if (!finite_pos(q1) || !stencil_ok(sh, a.Nx)) {
-            bad |= ST_OUT_OF_RANGE;
-            continue;
-        }
-        double const val[10] = { w,           vx * w,      vy * w,      vz * w,      (vx * vx) * w,
-                                 (vy * vy) * w, (vz * vz) * w, (vx * vy) * w, (vy * vz) * w, (vz * vx) * w };
-        int const    r       = sh.i0 - base;
-        if (r >= 0 && r <= S - 2) {
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                double const ws = (s == r) ? sh.w[0] : (s == r + 1) ? sh.w[1] : 0.0;
-#pragma unroll
-                for (int q = 0; q < 10; ++q)
-                    acc[q][s] = fma(val[q], ws, acc[q][s]);
-            }
-        } else {
-#pragma unroll
-            for (int j = 0; j <= 1; ++j)
-#pragma unroll
-                for (int q = 0; q < 10; ++q)
-                    atomicAdd(a.out[q] + sh.i0 + j, val[q] * sh.w[j]);
-        }
+    if (gc >= 0) {
+        PushArgs const &a = G.g[gc];
+        if (a.deposit_mask & 1)
+            win0.finish(lane, a);
+        if (a.deposit_mask & 2)
+            win1.finish(lane, a);
+        bad = __reduce_or_sync(0xffffffffu, bad);
+        if (bad && lane == 0)
+            atomicOr(a.status, bad);
     }
-#pragma unroll
-    for (int q = 0; q < 10; ++q)
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            double const v = warp_sum(acc[q][s]);
-            if (lane == (q * S + s) % 32 && v != 0.0) {
-                int const cell = base + s;
-                if (cell >= -PAD && cell < a.Nx + PAD)
-                    atomicAdd(a.out[q] + cell, v);
-                else
-                    bad |= ST_OUT_OF_RANGE;
-            }
-        }
-    bad = __reduce_or_sync(0xffffffffu, bad);
-    if (bad && lane == 0)
-        atomicOr(a.status, bad);
 }
+
 
 } // namespace h1d

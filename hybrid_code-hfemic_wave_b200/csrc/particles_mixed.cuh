@@ -131,41 +131,48 @@ struct WindowF {
         zero();
         base = NONE;
     }
-    // FP32 reduce-scatter across the warp, then one FP64 atomic per (cell, quantity)
+    // FP32 reduce-scatter across the warp (recursive halving of V = 16 or 32 values, as
+    // reduce_scatter in particles.cuh), then one FP64 atomic per (cell, quantity)
     __device__ __forceinline__ void flush(int lane, PushArgsMixed const &a)
     {
+        constexpr int V  = 4 * S <= 16 ? 16 : 32;
+        constexpr int SH = V == 16 ? 1 : 0;
         static_assert(4 * S <= 32, "window too wide");
-        float x[32];
+        float x[V];
 #pragma unroll
         for (int q = 0; q < 4; ++q)
 #pragma unroll
             for (int s = 0; s < S; ++s)
                 x[q * S + s] = acc.v[q][s];
 #pragma unroll
-        for (int k = 4 * S; k < 32; ++k)
+        for (int k = 4 * S; k < V; ++k)
             x[k] = 0.0f;
 #pragma unroll
-        for (int h = 16; h >= 1; h >>= 1) {
-            bool const up = (lane & h) != 0;
+        for (int h = V / 2, m = 16; h >= 1; h >>= 1, m >>= 1) {
+            bool const up = (lane & m) != 0;
 #pragma unroll
             for (int j = 0; j < h; ++j) {
                 float const send = up ? x[j] : x[j + h];
                 float const keep = up ? x[j + h] : x[j];
-                x[j]             = keep + __shfl_xor_sync(0xffffffffu, send, h);
+                x[j]             = keep + __shfl_xor_sync(0xffffffffu, send, m);
             }
         }
-        if (lane < 4 * S && x[0] != 0.0f) {
-            int const q = lane / S, cell = base + lane % S;
+        float v = x[0];
+        if constexpr (V == 16)
+            v += __shfl_xor_sync(0xffffffffu, v, 1);
+        int const vi = lane >> SH;
+        if ((lane & SH) == 0 && vi < 4 * S && v != 0.0f) {
+            int const q = vi / S, cell = base + vi % S;
             if (cell >= -PAD && cell < a.Nx + PAD)
-                atomicAdd(a.dep[D][q] + cell, static_cast<double>(x[0]));
+                atomicAdd(a.dep[D][q] + cell, static_cast<double>(v));
             else
                 atomicOr(a.status, ST_OUT_OF_RANGE);
         }
     }
     __device__ __forceinline__ void prepare(bool valid, int i0, int lane, PushArgsMixed const &a)
     {
-        bool const above = valid && i0 > base + R;
-        if (__any_sync(0xffffffffu, above)) {
+        bool const outside = valid && (i0 > base + R || i0 < base);
+        if (__any_sync(0xffffffffu, outside)) {
             if (base != NONE)
                 flush(lane, a);
             zero();
@@ -257,21 +264,43 @@ constexpr int    PIPE_STAGES_MIXED = 3;
 constexpr int    PIPE_CTAS_PER_SM_MIXED = 3;
 constexpr size_t PIPE_SMEM_MIXED   = sizeof(PipeStageMixed) * PIPE_STAGES_MIXED + 2 * PIPE_STAGES_MIXED * sizeof(uint64_t);
 
-template <int O, bool MIRROR, int BC>
-__global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED) push_kernel_mixed(PushArgsMixed a)
+// the groups of one launch, as PushGroups in particles.cuh
+template <int MAXG>
+struct PushGroupsMixed {
+    int           n;
+    int64_t       chunk0[MAXG + 1];
+    PushArgsMixed g[MAXG];
+};
+
+template <int MAXG>
+__device__ __forceinline__ int group_of(PushGroupsMixed<MAXG> const &G, int64_t chunk, int from)
+{
+    if constexpr (MAXG == 1) {
+        return 0;
+    } else {
+        int g = from < 0 ? 0 : from;
+        while (g + 1 < G.n && chunk >= G.chunk0[g + 1])
+            ++g;
+        return g;
+    }
+}
+
+template <int O, bool MIRROR, int BC, int MAXG>
+__global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
+    push_kernel_mixed(PushGroupsMixed<MAXG> const __grid_constant__ G)
 {
     constexpr int   R      = 2;
     constexpr int   STAGES = PIPE_STAGES_MIXED;
     extern __shared__ __align__(128) unsigned char smraw[];
+    __shared__ WarpOrder worder[PIPE_CONSUMER_WARPS];
     PipeStageMixed *stage = reinterpret_cast<PipeStageMixed *>(smraw);
     uint64_t       *full  = reinterpret_cast<uint64_t *>(smraw + sizeof(PipeStageMixed) * STAGES);
     uint64_t       *empty = full + STAGES;
     int const       warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int64_t const   nchunks = (a.n + PIPE_CHUNK - 1) / PIPE_CHUNK;
+    int64_t const   nchunks = G.chunk0[G.n];
     int64_t const   per     = (nchunks + gridDim.x - 1) / gridDim.x;
     int64_t const   c0      = static_cast<int64_t>(blockIdx.x) * per;
     int64_t const   mine    = c0 < nchunks ? min(per, nchunks - c0) : 0;
-    bool const      load_pid = a.randomize != 0;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -284,16 +313,19 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED) push_ker
 
     if (warp == PIPE_CONSUMER_WARPS) { // ---------------- producer ----------------
         if (lane == 0) {
+            int gl = -1, gr = -1;
             for (int64_t i = 0; i < mine + STAGES; ++i) {
                 int const s = static_cast<int>(i % STAGES);
                 if (i >= STAGES && i - STAGES < mine) {
-                    int64_t const j = i - STAGES;
+                    int64_t const        j = i - STAGES;
+                    gr                     = group_of(G, c0 + j, gr);
+                    PushArgsMixed const &a = G.g[gr];
                     if (!mbar_wait(&empty[s], static_cast<uint32_t>((j / STAGES) & 1))) {
                         atomicOr(a.status, ST_TIMEOUT);
                         break;
                     }
                     if (a.write_back) {
-                        int64_t const  start = (c0 + j) * PIPE_CHUNK;
+                        int64_t const  start = (c0 + j - G.chunk0[gr]) * PIPE_CHUNK;
                         uint32_t const cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
                         uint32_t const b4    = round16(cnt * 4);
                         bulk_store(a.cell + start, stage[s].celln, b4);
@@ -308,17 +340,20 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED) push_ker
                     bulk_wait_read_all();
                 }
                 if (i < mine) {
-                    int64_t const  start = (c0 + i) * PIPE_CHUNK;
+                    gl                     = group_of(G, c0 + i, gl);
+                    PushArgsMixed const &a = G.g[gl];
+                    bool const     lpid  = a.randomize != 0;
+                    int64_t const  start = (c0 + i - G.chunk0[gl]) * PIPE_CHUNK;
                     uint32_t const cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
                     uint32_t const b4    = round16(cnt * 4);
-                    mbar_arrive_expect_tx(&full[s], (6 + (load_pid ? 1 : 0)) * b4);
+                    mbar_arrive_expect_tx(&full[s], (6 + (lpid ? 1 : 0)) * b4);
                     bulk_load(stage[s].cell, a.cell + start, b4, &full[s]);
                     bulk_load(stage[s].off, a.off + start, b4, &full[s]);
                     bulk_load(stage[s].vx, a.vx + start, b4, &full[s]);
                     bulk_load(stage[s].vy, a.vy + start, b4, &full[s]);
                     bulk_load(stage[s].vz, a.vz + start, b4, &full[s]);
                     bulk_load(stage[s].w, a.w + start, b4, &full[s]);
-                    if (load_pid)
+                    if (lpid)
                         bulk_load(stage[s].pid, a.pid + start, b4, &full[s]);
                 }
             }
@@ -328,21 +363,40 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED) push_ker
     }
 
     unsigned         bad = 0;
+    int              gc  = -1;
     WindowF<O, R, 0> win0;
     WindowF<O, R, 1> win1;
     win0.init();
     win1.init();
     for (int64_t i = 0; i < mine; ++i) {
-        int const s = static_cast<int>(i % STAGES);
+        int const s  = static_cast<int>(i % STAGES);
+        int const gi = group_of(G, c0 + i, gc);
+        if (gi != gc) {
+            if (gc >= 0) {
+                PushArgsMixed const &ap = G.g[gc];
+                if (ap.deposit_mask & 1)
+                    win0.finish(lane, ap);
+                if (ap.deposit_mask & 2)
+                    win1.finish(lane, ap);
+                bad = __reduce_or_sync(0xffffffffu, bad);
+                if (bad && lane == 0)
+                    atomicOr(ap.status, bad);
+                bad = 0;
+                win0.init();
+                win1.init();
+            }
+            gc = gi;
+        }
+        PushArgsMixed const &a        = G.g[gc];
+        bool const           load_pid = a.randomize != 0;
         if (!mbar_wait(&full[s], static_cast<uint32_t>((i / STAGES) & 1))) {
             bad |= ST_TIMEOUT;
             break;
         }
-        int64_t const   start = (c0 + i) * PIPE_CHUNK;
+        int64_t const   start = (c0 + i - G.chunk0[gc]) * PIPE_CHUNK;
         int const       cnt   = static_cast<int>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
         PipeStageMixed &P     = stage[s];
         int const       w0    = warp * 32 * PIPE_PPT;
-
         // pass A: push, move, boundary (FP32)
 #pragma unroll 2
         for (int k = 0; k < PIPE_PPT; ++k) {
@@ -368,8 +422,10 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED) push_ker
                     w = 0.0f, cell = 0, off = 0.5f, v = { 0, 0, 0 };
                 P.cell[idx] = cell, P.off[idx] = off;
             }
-            ShapeF<O> const sh = make_shape_f<O>(cell, off);
-            if (stencil_ok_f(sh, a.Nx)) {
+            ShapeF<O> const sh      = make_shape_f<O>(cell, off);
+            bool const      in_grid = stencil_ok_f(sh, a.Nx);
+            worder[warp].key[k * 32 + lane] = in_grid && idx < cnt ? sh.i0 : 0x7fffffff;
+            if (in_grid) {
                 if (alive && a.move_steps != 0) {
                     f3 E = { 0, 0, 0 }, dB = { 0, 0, 0 };
 #pragma unroll
@@ -397,7 +453,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED) push_ker
                     E = E * a.cDtOc_2O0;
                     v = v + E;
                     f3 const    u  = v + crossf(v, B);
-                    float const sb = 2.0f / (1.0f + (B.x * B.x + B.y * B.y + B.z * B.z));
+                    float const sb = 2.0f * __frcp_rn(1.0f + (B.x * B.x + B.y * B.y + B.z * B.z));
                     v              = v + crossf(u, B * sb) + E;
                     float const dq = (a.inv_D1 * c2) * v.x * (a.move_steps == 2 ? 0.5f * a.dt : a.dt);
                     if (idx < cnt && !(fabsf(dq * a.travel_scale) < 1.0f))
@@ -432,10 +488,11 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED) push_ker
                 P.wn[idx] = w;
         }
         __syncwarp();
+        warp_order(worder[warp], lane);
         if (a.deposit_mask & 1) {
 #pragma unroll 1
             for (int k = 0; k < PIPE_PPT; ++k) {
-                int const       idx   = w0 + k * 32 + lane;
+                int const       idx   = w0 + worder[warp].order[k * 32 + lane];
                 ShapeF<O> const sh    = make_shape_f<O>(P.cell[idx], P.off[idx]);
                 bool const      valid = idx < cnt && stencil_ok_f(sh, a.Nx);
                 win0.prepare(valid, sh.i0, lane, a);
@@ -446,7 +503,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED) push_ker
         if (a.deposit_mask & 2) {
 #pragma unroll 1
             for (int k = 0; k < PIPE_PPT; ++k) {
-                int const       idx   = w0 + k * 32 + lane;
+                int const       idx   = w0 + worder[warp].order[k * 32 + lane];
                 ShapeF<O> const sh    = make_shape_f<O>(P.celln[idx], P.offn[idx]);
                 bool const      valid = idx < cnt && stencil_ok_f(sh, a.Nx);
                 win1.prepare(valid, sh.i0, lane, a);
@@ -459,165 +516,17 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED) push_ker
         if (lane == 0)
             mbar_arrive(&empty[s]);
     }
-    if (a.deposit_mask & 1)
-        win0.finish(lane, a);
-    if (a.deposit_mask & 2)
-        win1.finish(lane, a);
-    bad = __reduce_or_sync(0xffffffffu, bad);
-    if (bad && lane == 0)
-        atomicOr(a.status, bad);
-}
-
-// collect_all (n, nV, nvv with CIC, PartSpecies.cc:330-349) from mixed-precision particles: the
-// same per-warp window scheme as moments_kernel (particles.cuh), accumulated in FP64
-struct MomentArgsMixed {
-    int32_t const *cell;
-    float const   *off, *vx, *vy, *vz, *w;
-    int64_t        n;
-    int            ppt, Nx;
-    double        *out[10];
-    unsigned      *status;
-};
-__global__ void __launch_bounds__(256) moments_kernel_mixed(MomentArgsMixed a)
-{
-    constexpr int S = 4;
-    int const     lane   = threadIdx.x & 31;
-    int64_t const warp   = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    int64_t const chunk0 = warp * 32 * a.ppt;
-    if (chunk0 >= a.n)
-        return;
-    int first = 0x7fffffff;
-    if (chunk0 + lane < a.n)
-        first = make_shape_f<1>(a.cell[chunk0 + lane], a.off[chunk0 + lane]).i0;
-    int const base = __reduce_min_sync(0xffffffffu, first) - 1;
-    double    acc[10][S];
-#pragma unroll
-    for (int q = 0; q < 10; ++q)
-#pragma unroll
-        for (int s = 0; s < S; ++s)
-            acc[q][s] = 0;
-    unsigned bad = 0;
-    for (int k = 0; k < a.ppt; ++k) {
-        int64_t const idx = chunk0 + static_cast<int64_t>(k) * 32 + lane;
-        if (idx >= a.n)
-            break;
-        ShapeF<1> const sh = make_shape_f<1>(a.cell[idx], a.off[idx]);
-        if (!stencil_ok_f(sh, a.Nx)) {
-            bad |= ST_OUT_OF_RANGE;
-            continue;
-        }
-        double const w = a.w[idx], vx = a.vx[idx], vy = a.vy[idx], vz = a.vz[idx];
-        double const val[10] = { w,           vx * w,      vy * w,      vz * w,      (vx * vx) * w,
-                                 (vy * vy) * w, (vz * vz) * w, (vx * vy) * w, (vy * vz) * w, (vz * vx) * w };
-        double const w0 = sh.w[0], w1 = sh.w[1];
-        int const    r  = sh.i0 - base;
-        if (r >= 0 && r <= S - 2) {
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                double const ws = (s == r) ? w0 : (s == r + 1) ? w1 : 0.0;
-#pragma unroll
-                for (int q = 0; q < 10; ++q)
-                    acc[q][s] = fma(val[q], ws, acc[q][s]);
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < 10; ++q) {
-                atomicAdd(a.out[q] + sh.i0, val[q] * w0);
-                atomicAdd(a.out[q] + sh.i0 + 1, val[q] * w1);
-            }
-        }
+    if (gc >= 0) {
+        PushArgsMixed const &a = G.g[gc];
+        if (a.deposit_mask & 1)
+            win0.finish(lane, a);
+        if (a.deposit_mask & 2)
+            win1.finish(lane, a);
+        bad = __reduce_or_sync(0xffffffffu, bad);
+        if (bad && lane == 0)
+            atomicOr(a.status, bad);
     }
-#pragma unroll
-    for (int q = 0; q < 10; ++q)
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            double const v = warp_sum(acc[q][s]);
-            if (lane == (q * S + s) % 32 && v != 0.0) {
-                int const cell = base + s;
-                if (cell >= -PAD && cell < a.Nx + PAD)
-                    atomicAdd(a.out[q] + cell, v);
-                else
-                    bad |= ST_OUT_OF_RANGE;
-            }
-        }
-    bad = __reduce_or_sync(0xffffffffu, bad);
-    if (bad && lane == 0)
-        atomicOr(a.status, bad);
 }
 
-// FP64 host-layout particles <-> mixed-precision particles (upload and download), one component at
-// a time so that the FP64 staging buffer holds a single array: position q1 <-> (cell, offset) with
-// cell = floor(q1 - q1min), and velocity / weight components FP64 <-> FP32
-__global__ void q1_to_mixed_kernel(double const *q1, int64_t n, double full_min, int32_t *cell, float *off)
-{
-    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
-    double const x  = q1[i] - full_min;
-    double const f  = floor(x);
-    bool const   ok = f > -1073741824.0 && f < 1073741824.0; // NaN and lost positions map outside the grid
-    float        o  = ok ? static_cast<float>(x - f) : 0.5f;
-    if (o >= 1.0f)
-        o = 0.99999994f;
-    cell[i] = ok ? static_cast<int32_t>(f) : -0x40000000;
-    off[i]  = o;
-}
-__global__ void to_f32_kernel(double const *src, int64_t n, float *dst)
-{
-    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i < n)
-        dst[i] = static_cast<float>(src[i]);
-}
-// one component at a time, so that the caller's FP64 staging buffer holds a single array
-__global__ void from_mixed_kernel(int32_t const *cell, float const *src, int64_t n, double full_min, double *dst)
-{
-    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
-    dst[i] = cell ? full_min + static_cast<double>(cell[i]) + static_cast<double>(src[i]) : static_cast<double>(src[i]);
-}
-
-// keys for the cell sort of mixed-precision particles (sort.cuh): the cell itself
-__global__ void keys_kernel_mixed(int32_t const *cell, float const *w, int64_t n, int Nx, uint32_t *keys, uint32_t *idx,
-                                  unsigned long long *dead, unsigned *status)
-{
-    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
-    int const c = cell[i];
-    uint32_t  k;
-    if (w[i] == 0.0f) {
-        k = static_cast<uint32_t>(Nx);
-        atomicAdd(dead, 1ull);
-    } else if (c < 0 || c >= Nx) {
-        k = c < 0 ? 0u : static_cast<uint32_t>(Nx - 1);
-        atomicOr(status, ST_OUT_OF_RANGE);
-    } else {
-        k = static_cast<uint32_t>(c);
-    }
-    keys[i] = k;
-    idx[i]  = static_cast<uint32_t>(i);
-}
-
-struct GatherArgsMixed {
-    float const   *src[5]; // off, vx, vy, vz, w
-    int32_t const *cell_src, *pid_src;
-    float         *dst[5];
-    int32_t       *cell_dst, *pid_dst;
-    uint32_t const *idx;
-    int64_t        n;
-};
-__global__ void gather_kernel_mixed(GatherArgsMixed a)
-{
-    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= a.n)
-        return;
-    uint32_t const j = a.idx[i];
-#pragma unroll
-    for (int k = 0; k < 5; ++k)
-        a.dst[k][i] = a.src[k][j];
-    a.cell_dst[i] = a.cell_src[j];
-    a.pid_dst[i]  = a.pid_src[j];
-}
 
 } // namespace h1d

@@ -1,0 +1,24 @@
+// Launches of the particle pass, compiled in their own translation units (push_fp64.cu,
+// push_mixed.cu): one launch covers one group of particles (a species of a run) or up to
+// BATCH_GROUPS groups of an ensemble that share shape order, geometry, boundary and precision.
+#pragma once
+
+#include "particles_mixed.cuh"
+
+#include <cuda_runtime.h>
+
+namespace h1d {
+
+constexpr int BATCH_GROUPS = 64;
+
+// opt every instantiation into its dynamic shared memory, once per process and device
+cudaError_t set_push_smem_fp64();
+cudaError_t set_push_smem_mixed();
+
+// one pass over `n` groups; grid = min(chunks, max_ctas) persistent CTAs
+cudaError_t launch_push_groups(PushArgs const *args, int n, int order, bool mirror, int bc, int max_ctas,
+                               cudaStream_t st);
+cudaError_t launch_push_groups(PushArgsMixed const *args, int n, int order, bool mirror, int bc, int max_ctas,
+                               cudaStream_t st);
+
+} // namespace h1d

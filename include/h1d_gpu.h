@@ -229,6 +229,46 @@ int h1d_collect_moments_noalloc(int64_t Nx, double moment_norm, int particle_bc,
                                 const double *vy, const double *vz, const double *w, int64_t n, double *n_out,
                                 double *nV_out, double *nvv_out, void *stream);
 
+/* Tuning of a run: steps between cell sorts (0 keeps the current value) and CTAs per SM of the
+ * particle pass (0 = the kernel's default, at most 2 for FP64 and 3 for mixed precision).  No
+ * counterpart in the reference, which never sorts. */
+int h1d_configure(h1d_run *run, int sort_interval, int push_ctas_per_sm);
+/* Autotuner (no counterpart in the reference): advances the run by real CAM-CL steps while timing
+ * two sort blocks for each candidate sort interval (8, 16, 32) and then for each CTA count of the
+ * particle pass, and keeps the fastest.  *steps_taken receives the number of steps it advanced. */
+int h1d_autotune(h1d_run *run, uint32_t *steps_taken, int *sort_interval, int *push_ctas_per_sm);
+
+/* ---- Ensembles (no counterpart in the reference) ---------------------------------------------
+ * A batch advances many CAM-CL runs together on one stream of the current device.  A step is one
+ * launch of the particle pass per kind of particle group (shape order, geometry, boundary,
+ * precision) covering every species of every member, and one launch of the field cycle covering
+ * every member's grid.  Steps come in blocks of sort_interval steps, all groups cell-sorted at the
+ * start of a block.  When no member uses absorbing particles or gyrophase randomization, a pair of
+ * blocks is captured once as a CUDA graph and replayed while the members are unchanged (an upload
+ * to a member invalidates it).  Members stay owned by the caller, must outlive the batch and
+ * belong to one batch at a time; while a member, a run's work is ordered on the batch's stream,
+ * and h1d_download_* / h1d_energy on it are allowed between batch calls. */
+typedef struct h1d_batch h1d_batch;
+typedef struct h1d_batch_stats {
+    int64_t steps;           /* batch steps taken */
+    int64_t kernel_launches; /* kernels of this library launched, graph replays included */
+    int64_t graph_launches;  /* CUDA graph replays */
+    int64_t graphs_built;
+} h1d_batch_stats;
+int h1d_batch_create(h1d_run *const *runs, int n_runs, h1d_batch **out);
+int h1d_batch_destroy(h1d_batch *batch);
+int h1d_batch_advance(h1d_batch *batch, uint32_t n_steps);
+int h1d_batch_advance_async(h1d_batch *batch, uint32_t n_steps);
+int h1d_batch_synchronize(h1d_batch *batch);
+int h1d_batch_get_stream(h1d_batch *batch, void **stream);
+/* sort_interval > 0 sets the block length (0 keeps it); push_ctas_per_sm as in h1d_configure;
+ * use_graphs = 0 keeps every step eager */
+int h1d_batch_configure(h1d_batch *batch, int sort_interval, int push_ctas_per_sm, int use_graphs);
+/* the autotuner of h1d_autotune over the whole batch; the choice also becomes every member's */
+int h1d_batch_autotune(h1d_batch *batch, uint32_t *steps_taken, int *sort_interval, int *push_ctas_per_sm);
+int h1d_batch_stats_read(h1d_batch *batch, h1d_batch_stats *out);
+const char *h1d_batch_status_string(h1d_batch *batch);
+
 const char *h1d_status_string(h1d_run *run);
 const char *h1d_error_name(int status);
 

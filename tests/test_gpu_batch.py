@@ -1,0 +1,119 @@
+"""Ensembles (h1d_batch_*) and the autotuner against runs advanced alone.
+
+A batch member computes exactly what the same run computes alone: the kernels are the same and
+only the order of floating-point atomic additions differs.  Tolerances (max-norm relative):
+1e-10 for FP64 members and 1e-4 (the mixed-precision tolerance) for mixed-precision members,
+after 40 steps with CUDA-graph replays in between.  The autotuner only reorders particles, so a
+tuned run still matches the oracle.
+"""
+import numpy as np
+import pytest
+from parity_util import by_pid, rel_err, state_errors
+
+import hfemic_b200 as h
+
+pytestmark = pytest.mark.gpu
+
+
+def _members(precision, n=4, ppc_scale=0.05):
+    from hfemic_b200.loader import initial_state
+
+    cfgs = [h.configs.ensemble_member(seed, precision=precision, ppc_scale=ppc_scale) for seed in range(n)]
+    return cfgs, [initial_state(c, seed=i) for i, c in enumerate(cfgs)]
+
+
+def _field_errs(a, b, cfg):
+    errs = {k: rel_err(a[k], b[k]) for k in ("B", "E", "charge", "current")}
+    for s in range(len(cfg.kinetic)):
+        for key in ("n", "nV", "nvv"):
+            errs[f"moments[{s}].{key}"] = rel_err(a["moments"][s][key], b["moments"][s][key])
+    return errs
+
+
+@pytest.mark.parametrize("precision,tol", [(h.configs.PREC_FP64, 1e-10), (h.configs.PREC_MIXED, 1e-4)])
+def test_batch_members_match_runs_alone(gpu_lib, precision, tol):
+    cfgs, states = _members(precision)
+    alone = []
+    for c, st in zip(cfgs, states):
+        with h.Run(c, gpu_lib) as r:
+            h.abi.configure(r, sort_interval=4)
+            r.upload_state(st)
+            r.advance(40)
+            alone.append(r.state())
+    runs = [h.Run(c, gpu_lib) for c in cfgs]
+    try:
+        for r, st in zip(runs, states):
+            h.abi.configure(r, sort_interval=4)
+            r.upload_state(st)
+        with h.abi.Batch(runs) as b:
+            b.configure(sort_interval=4)
+            b.advance(3)   # part of a block, eager
+            b.advance(37)  # the rest of the block, graph pairs of 8 steps, eager tail
+            stats = b.stats()
+            assert stats["steps"] == 40
+            assert stats["graph_launches"] >= 2 and stats["graphs_built"] == 1
+            together = [r.state() for r in runs]
+    finally:
+        for r in runs:
+            r.close()
+    for c, a, t in zip(cfgs, alone, together):
+        errs = _field_errs(t, a, c)
+        print(c.name, c.Nx, {k: f"{v:.1e}" for k, v in errs.items()})
+        assert max(errs.values()) <= tol, errs
+        pa, pt = by_pid(a["particles"][0]), by_pid(t["particles"][0])
+        assert rel_err(pt["vx"], pa["vx"]) <= tol
+
+
+def test_batch_without_graphs_equals_with_graphs(gpu_lib):
+    cfgs, states = _members(h.configs.PREC_FP64, n=2)
+    out = []
+    for graphs in (False, True):
+        runs = [h.Run(c, gpu_lib) for c in cfgs]
+        for r, st in zip(runs, states):
+            r.upload_state(st)
+        with h.abi.Batch(runs) as b:
+            b.configure(sort_interval=4, use_graphs=graphs)
+            b.advance(24)
+            assert (b.stats()["graph_launches"] > 0) == graphs
+        out.append([r.state() for r in runs])
+        for r in runs:
+            r.close()
+    for c, a, t in zip(cfgs, out[0], out[1]):
+        assert max(_field_errs(t, a, c).values()) <= 1e-10
+
+
+def test_batch_rejects_bad_members(gpu_lib):
+    pc = h.configs.parity_p4()
+    with h.Run(pc, gpu_lib) as r:
+        with pytest.raises(h.H1DError):
+            h.abi.Batch([r])
+    c = h.configs.parity_p1()
+    with h.Run(c, gpu_lib) as r:
+        with pytest.raises(h.H1DError):
+            h.abi.Batch([r, r])
+        with h.abi.Batch([r]):
+            with pytest.raises(h.H1DError):
+                h.abi.Batch([r])
+
+
+def test_autotuned_run_matches_oracle(gpu_lib, oracle_lib):
+    from hfemic_b200.loader import initial_state
+
+    cfg = h.configs.parity_p2().replace(Nx=256, xi=0.01, phase_retardation=(32, 1.0), amplitude_damping=(32, 0.2))
+    for k in cfg.kinetic:
+        k.Nc = 100
+    init = initial_state(cfg, seed=4)
+    with h.Run(cfg, gpu_lib) as g:
+        g.upload_state(init)
+        steps, k, c = h.abi.autotune(g)
+        assert k in (8, 16, 32) and 1 <= c <= 2
+        assert steps == 2 * (8 + 16 + 32) + 2 * 2 * k
+        g.advance(3)
+        gs = g.state()
+    with h.Run(cfg, oracle_lib, "orc_") as o:
+        o.upload_state(init)
+        o.advance(steps + 3)
+        cs = o.state()
+    errs = state_errors(gs, cs, cfg)
+    print("autotuned", steps, k, c, {key: f"{v:.1e}" for key, v in errs.items()})
+    assert max(errs.values()) <= 1e-9
