@@ -379,3 +379,143 @@ class Batch:
 
     def __exit__(self, *a):
         self.close()
+
+
+def populate(run: Run, s: int, seed: int, count: int | None = None):
+    """h1d_populate: load kinetic species s of the run's configuration on the device (the particles
+    loader.load_species computes on the host for the same seed)."""
+    lib = run.lib
+    fn = lib.h1d_populate
+    fn.argtypes = [C.c_void_p, C.c_int, C.c_int64, C.c_uint64, C.c_double, C.c_double]
+    fn.restype = C.c_int
+    k = run.cfg.kinetic[s]
+    n = k.Nc * run.cfg.Nx if count is None else count
+    run._check(fn(run.h, s, n, seed, k.beta1, k.T2_T1))
+
+
+def populate_state(run: Run, seed: int):
+    """The state of loader.initial_state(cfg, seed) built on the device: every kinetic species by
+    h1d_populate, the cold species at rest with unit density, zero fields."""
+    cfg = run.cfg
+    for s in range(len(cfg.kinetic)):
+        populate(run, s, seed)
+    M = cfg.Nx + 2 * PAD
+    for i in range(len(cfg.cold)):
+        n_full = np.zeros(M)
+        n_full[PAD:PAD + cfg.Nx] = 1.0
+        run.upload_cold(i, n_full, np.zeros((M, 3)))
+
+
+# ---------------------------------------------------------------------------------------------
+# serving loop (h1d_server_*)
+# ---------------------------------------------------------------------------------------------
+
+MAXK = 8
+REQ_QUEUED, REQ_ACTIVE, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+
+
+class Request(C.Structure):
+    _fields_ = [("params", Params), ("beta1", C.c_double * MAXK), ("T2_T1", C.c_double * MAXK),
+                ("n_particles", C.c_int64 * MAXK), ("seed", C.c_uint64), ("n_steps", C.c_uint32),
+                ("reserved0", C.c_uint32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(k, C.c_int64) for k in ("submitted", "admitted", "completed", "failed", "steps", "kernel_launches",
+                                         "graph_launches", "batches_built", "bytes_in_use", "peak_bytes")]
+
+
+def make_request(cfg: "_cfg.RunConfig", seed: int, n_steps: int) -> Request:
+    rq = Request()
+    rq.params = make_params(cfg)
+    for s, k in enumerate(cfg.kinetic):
+        rq.beta1[s], rq.T2_T1[s], rq.n_particles[s] = k.beta1, k.T2_T1, k.Nc * cfg.Nx
+    rq.seed, rq.n_steps = seed, n_steps
+    return rq
+
+
+class Server:
+    """Continuous-batching serving loop over the CUDA library (h1d_server_*)."""
+
+    def __init__(self, path: str, hbm_budget_bytes: int, steps_per_tick: int = 64, sort_interval: int = 16):
+        lib = self.lib = C.CDLL(os.path.abspath(path))
+        v, u64 = C.c_void_p, C.c_uint64
+        dp = C.POINTER(C.c_double)
+        spec = {
+            "h1d_server_create": ([C.c_size_t, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+            "h1d_server_configure": ([v, C.c_int], C.c_int),
+            "h1d_server_submit": ([v, C.POINTER(Request), C.POINTER(u64)], C.c_int),
+            "h1d_server_tick": ([v, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+            "h1d_server_poll": ([v, u64, C.POINTER(C.c_int), dp, dp, dp], C.c_int),
+            "h1d_server_result": ([v, u64, dp, dp, dp, dp, dp, dp], C.c_int),
+            "h1d_server_release": ([v, u64], C.c_int),
+            "h1d_server_stats_read": ([v, C.POINTER(ServerStats)], C.c_int),
+            "h1d_server_destroy": ([v], C.c_int),
+        }
+        for name, (args, res) in spec.items():
+            fn = getattr(lib, name)
+            fn.argtypes, fn.restype = args, res
+        h = C.c_void_p()
+        st = lib.h1d_server_create(hbm_budget_bytes, steps_per_tick, C.byref(h))
+        if st != OK:
+            raise H1DError(st, "h1d_server_create failed")
+        self.h = h
+        self.cfgs = {}
+        self._chk(lib.h1d_server_configure(h, sort_interval))
+
+    def _chk(self, st, what="server call"):
+        if st != OK:
+            raise H1DError(st, what)
+
+    def submit(self, cfg, seed: int, n_steps: int) -> int:
+        rq = make_request(cfg, seed, n_steps)
+        i = C.c_uint64()
+        self._chk(self.lib.h1d_server_submit(self.h, C.byref(rq), C.byref(i)), "h1d_server_submit")
+        self.cfgs[i.value] = cfg
+        return i.value
+
+    def tick(self):
+        a, q = C.c_int(), C.c_int()
+        self._chk(self.lib.h1d_server_tick(self.h, C.byref(a), C.byref(q)), "h1d_server_tick")
+        return a.value, q.value
+
+    def poll(self, rid: int):
+        st, t0, t1, t2 = C.c_int(), C.c_double(), C.c_double(), C.c_double()
+        rc = self.lib.h1d_server_poll(self.h, rid, C.byref(st), C.byref(t0), C.byref(t1), C.byref(t2))
+        return dict(state=st.value, status=rc, t_submit=t0.value, t_admit=t1.value, t_done=t2.value)
+
+    def result(self, rid: int):
+        cfg = self.cfgs[rid]
+        M = cfg.Nx + 2 * PAD
+        nk, ns = len(cfg.kinetic), len(cfg.kinetic) + len(cfg.cold)
+        B, E, en = np.empty((M, 3)), np.empty((M, 3)), np.empty(6 + 6 * ns)
+        n, nV, nvv = np.empty((nk, M)), np.empty((nk, M, 3)), np.empty((nk, M, 6))
+        self._chk(self.lib.h1d_server_result(self.h, rid, *[_ptr(a) for a in (B, E, en, n, nV, nvv)]),
+                  "h1d_server_result")
+        return dict(B=B, E=E, dB2O2=en[0:3], dE2O2=en[3:6], KE=en[6:].reshape(ns, 2, 3), n=n, nV=nV, nvv=nvv)
+
+    def release(self, rid: int):
+        self._chk(self.lib.h1d_server_release(self.h, rid), "h1d_server_release")
+        self.cfgs.pop(rid, None)
+
+    def stats(self):
+        s = ServerStats()
+        self._chk(self.lib.h1d_server_stats_read(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.h1d_server_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -10,7 +10,10 @@
 #include "sort.cuh"
 #include "launchers.h"
 
+#include <chrono>
 #include <cmath>
+#include <deque>
+#include <map>
 #include <mutex>
 #include <cstdarg>
 #include <cstdio>
@@ -671,6 +674,52 @@ int noalloc_scratch_address(double **out)
 }
 
 
+// device storage for n particles of species s (both buffer sets and the sort scratch)
+int ensure_capacity(h1d_run *run, int s, int64_t n)
+{
+    SpeciesState &S = run->sp[s];
+    if (n <= S.cap)
+        return H1D_OK;
+    int64_t const cap = n + 64; // slack for the 16-byte rounding of the last bulk copy of a pass
+    for (int k = 0; k < 2; ++k) {
+        if (run->mixed) {
+            for (auto *&b : S.fbuf[k]) {
+                cudaFree(b);
+                b = nullptr;
+                CU(cudaMalloc(&b, sizeof(float) * cap));
+            }
+            cudaFree(S.cell[k]);
+            S.cell[k] = nullptr;
+            CU(cudaMalloc(&S.cell[k], sizeof(int32_t) * cap));
+        } else {
+            for (auto *&b : S.buf[k]) {
+                cudaFree(b);
+                b = nullptr;
+                CU(cudaMalloc(&b, sizeof(double) * cap));
+            }
+        }
+        cudaFree(S.pid[k]), cudaFree(S.keys[k]), cudaFree(S.idx[k]);
+        S.pid[k] = nullptr, S.keys[k] = nullptr, S.idx[k] = nullptr;
+        CU(cudaMalloc(&S.pid[k], sizeof(int32_t) * cap));
+        CU(cudaMalloc(&S.keys[k], sizeof(uint32_t) * cap));
+        CU(cudaMalloc(&S.idx[k], sizeof(uint32_t) * cap));
+    }
+    S.cap = cap;
+    return H1D_OK;
+}
+
+// MaxwellianVDF::N_of_q1 (VDF/MaxwellianVDF.cc:229-239)
+double n_of_q1(h1d_params const &p, double T2OT1, double q1)
+{
+    if (p.xi < 1e-10) {
+        double const xiD1q1 = p.xi * p.Dx * q1;
+        return q1 * (1 - (xiD1q1 * xiD1q1) * (T2OT1 - 1) / 3);
+    }
+    double const s = std::sqrt(T2OT1);
+    return std::atan(s * std::tan(p.xi * p.Dx * q1)) / (s * p.Dx * p.xi);
+}
+
+
 // ------------------------------------------------------------------------------------------------
 // Ensembles (h1d_batch_*): many CAM-CL runs advanced together on one stream.  A step is one
 // launch of the particle pass per kind of group (shape order, geometry, boundary, precision) over
@@ -1230,33 +1279,7 @@ int h1d_upload_particles(h1d_run *run, int s, int64_t n, double const *q1, doubl
         return set_err(run, H1D_ERR_INVALID_ARG, "h1d_upload_particles: bad arguments");
     SpeciesState &S = run->sp[s];
     CU(cudaStreamSynchronize(run->stream));
-    if (n > S.cap) {
-        int64_t const cap = n + 64; // slack for the 16-byte rounding of the last bulk copy of a pass
-        for (int k = 0; k < 2; ++k) {
-            if (run->mixed) {
-                for (auto *&b : S.fbuf[k]) {
-                    cudaFree(b);
-                    b = nullptr;
-                    CU(cudaMalloc(&b, sizeof(float) * cap));
-                }
-                cudaFree(S.cell[k]);
-                S.cell[k] = nullptr;
-                CU(cudaMalloc(&S.cell[k], sizeof(int32_t) * cap));
-            } else {
-                for (auto *&b : S.buf[k]) {
-                    cudaFree(b);
-                    b = nullptr;
-                    CU(cudaMalloc(&b, sizeof(double) * cap));
-                }
-            }
-            cudaFree(S.pid[k]), cudaFree(S.keys[k]), cudaFree(S.idx[k]);
-            S.pid[k] = nullptr, S.keys[k] = nullptr, S.idx[k] = nullptr;
-            CU(cudaMalloc(&S.pid[k], sizeof(int32_t) * cap));
-            CU(cudaMalloc(&S.keys[k], sizeof(uint32_t) * cap));
-            CU(cudaMalloc(&S.idx[k], sizeof(uint32_t) * cap));
-        }
-        S.cap = cap;
-    }
+    TRY(ensure_capacity(run, s, n));
     S.cur              = 0;
     S.n                = n;
     double const *src[5] = { q1, vx, vy, vz, w };
@@ -1284,6 +1307,45 @@ int h1d_upload_particles(h1d_run *run, int s, int64_t n, double const *q1, doubl
             CU(cudaMemcpyAsync(S.buf[0][k], src[k], sizeof(double) * n, cudaMemcpyHostToDevice, run->stream));
     if (n)
         CU(launch_iota(S.pid[0], n, run->stream));
+    S.since_sort       = 1 << 30;
+    run->moments_stale = true;
+    run->gen++;
+    CU(cudaStreamSynchronize(run->stream));
+    return H1D_OK;
+}
+
+
+int h1d_populate(h1d_run *run, int s, int64_t n, uint64_t seed, double beta1, double T2_T1)
+{
+    if (!run || s < 0 || s >= run->p.n_kinetic || n < 0 || n > (int64_t{ 1 } << 31) - 1 || !(beta1 > 0) || !(T2_T1 > 0))
+        return set_err(run, H1D_ERR_INVALID_ARG, "h1d_populate: bad arguments");
+    h1d_params const       &p = run->p;
+    h1d_kinetic_desc const &d = p.kinetic[s];
+    SpeciesState           &S = run->sp[s];
+    CU(cudaStreamSynchronize(run->stream));
+    TRY(ensure_capacity(run, s, n));
+    S.cur = 0, S.n = n;
+    PopulateArgs a{};
+    a.n = n;
+    a.key = populate_key(seed, static_cast<uint64_t>(s));
+    a.offset = populate_offset(a.key);
+    double const q1min = -0.5 * p.Nx, q1max = q1min + p.Nx;
+    a.N_loc = n_of_q1(p, T2_T1, q1min);
+    a.N_len = n_of_q1(p, T2_T1, q1max) - a.N_loc;
+    a.homogeneous = p.xi < 1e-10;
+    a.xiD1 = p.xi * p.Dx, a.T2m1 = T2_T1 - 1, a.sqrtT2 = std::sqrt(T2_T1), a.sDxXi = a.sqrtT2 * p.Dx * p.xi;
+    a.T2 = T2_T1, a.oneMinusT2 = 1 - T2_T1, a.vth1 = std::sqrt(beta1) * p.c * std::fabs(d.Oc) / d.op;
+    a.q1min = q1min, a.q1max_in = std::nextafter(q1max, q1min), a.full_min = q1min;
+    if (run->mixed)
+        a.cell = S.cell[0], a.off = S.fbuf[0][0], a.fvx = S.fbuf[0][1], a.fvy = S.fbuf[0][2], a.fvz = S.fbuf[0][3],
+        a.fw = S.fbuf[0][4];
+    else
+        a.q1 = S.buf[0][0], a.vx = S.buf[0][1], a.vy = S.buf[0][2], a.vz = S.buf[0][3], a.w = S.buf[0][4];
+    if (n) {
+        populate_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, run->stream>>>(a);
+        CU(cudaGetLastError());
+        CU(launch_iota(S.pid[0], n, run->stream));
+    }
     S.since_sort       = 1 << 30;
     run->moments_stale = true;
     run->gen++;
@@ -1739,6 +1801,374 @@ int h1d_energy(h1d_run *run, double *dB2O2, double *dE2O2, double *KE_lab, doubl
     for (int s = 0; s < ns; ++s)
         for (int c = 0; c < 3; ++c)
             KE_lab[3 * s + c] = h[6 + 6 * s + c], KE_pla[3 * s + c] = h[6 + 6 * s + 3 + c];
+    return H1D_OK;
+}
+
+} // extern "C"
+
+// ---- serving loop --------------------------------------------------------------------------------
+// Requests (a run description, a loader seed and a step count) wait in a queue until the HBM they
+// need fits the budget; admitted runs are built on the device (h1d_populate) and advance together
+// as one batch, a quantum of steps per tick; finished runs are read back and freed, which lets the
+// next requests in.  Membership changes rebuild the batch (and its graphs) at the next tick.
+
+namespace {
+
+struct ServerReq {
+    uint64_t            id = 0;
+    h1d_request         rq{};
+    size_t              bytes = 0;
+    int                 state = H1D_REQ_QUEUED, status = H1D_OK;
+    uint32_t            done_steps = 0;
+    h1d_run            *run = nullptr;
+    double              t_submit = 0, t_admit = 0, t_done = 0;
+    std::vector<double> B, E, energy, n, nV, nvv;
+    std::string         msg;
+};
+
+// device bytes a request needs: particles in both buffer sets with ids and sort keys, the grids
+size_t request_bytes(h1d_request const &rq)
+{
+    h1d_params const &p   = rq.params;
+    size_t const      per = p.precision == H1D_PREC_MIXED ? 6 * 4 : 5 * 8;
+    size_t            b   = 0;
+    for (int s = 0; s < p.n_kinetic; ++s) {
+        size_t const n = static_cast<size_t>(std::max<int64_t>(rq.n_particles[s], 0)) + 64;
+        b += 2 * n * (per + 4 + 4 + 4) + (n / SORT_TILE + 1) * 256 * 4 * 2;
+    }
+    size_t const M = static_cast<size_t>(p.Nx + 2 * PAD);
+    b += sizeof(double) * M * (G_COUNT + 6 * 3 + 6 + 1 + 3 + 6 + H1D_MAX_KINETIC * 36 + H1D_MAX_COLD * 17);
+    return b + (size_t{ 1 } << 20);
+}
+
+} // namespace
+
+struct h1d_server {
+    size_t                                budget = 0, used = 0, peak = 0;
+    int                                   quantum = 64, sort_interval = 16;
+    std::deque<ServerReq *>               queue;
+    std::vector<ServerReq *>              active;
+    std::map<uint64_t, ServerReq *>       all;
+    h1d_batch                            *batch = nullptr;
+    bool                                  dirty = false;
+    uint64_t                              next_id = 1;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    h1d_server_stats                      stats{};
+    std::mutex                            mu;
+
+    double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
+};
+
+namespace {
+
+void fold_batch_stats(h1d_server *sv)
+{
+    if (!sv->batch)
+        return;
+    h1d_batch_stats st{};
+    h1d_batch_stats_read(sv->batch, &st);
+    sv->stats.kernel_launches += st.kernel_launches;
+    sv->stats.graph_launches += st.graph_launches;
+    sv->stats.steps += st.steps;
+}
+
+void finish_request(h1d_server *sv, ServerReq *r, int status, std::string const &msg)
+{
+    r->status = status;
+    r->msg    = msg;
+    r->state  = status == H1D_OK ? H1D_REQ_DONE : H1D_REQ_FAILED;
+    r->t_done = sv->now();
+    if (r->run) {
+        h1d_destroy(r->run);
+        r->run = nullptr;
+        sv->used -= r->bytes;
+    }
+    if (status == H1D_OK)
+        sv->stats.completed++;
+    else
+        sv->stats.failed++;
+}
+
+// build a request's run on the device: particles by the device loader, cold fluid at rest
+int admit(h1d_server *sv, ServerReq *r)
+{
+    h1d_params p = r->rq.params;
+    if (p.sort_interval <= 0)
+        p.sort_interval = sv->sort_interval;
+    int st = h1d_create(&p, &r->run);
+    if (st != H1D_OK)
+        return st;
+    sv->used += r->bytes;
+    sv->peak = std::max(sv->peak, sv->used);
+    for (int s = 0; s < p.n_kinetic && st == H1D_OK; ++s)
+        st = h1d_populate(r->run, s, r->rq.n_particles[s], r->rq.seed, r->rq.beta1[s], r->rq.T2_T1[s]);
+    long const          M = p.Nx + 2 * PAD;
+    std::vector<double> n_full(M, 0.0), nV(3 * M, 0.0);
+    for (long i = PAD; i < PAD + p.Nx; ++i)
+        n_full[i] = 1.0;
+    for (int c = 0; c < p.n_cold && st == H1D_OK; ++c)
+        st = h1d_upload_cold(r->run, c, n_full.data(), nV.data());
+    if (st != H1D_OK)
+        r->msg = r->run ? r->run->msg : "";
+    return st;
+}
+
+// read a finished run back into its request
+int collect(ServerReq *r)
+{
+    h1d_params const &p = r->rq.params;
+    long const        M = p.Nx + 2 * PAD;
+    int const         ns = p.n_kinetic + p.n_cold;
+    r->B.resize(3 * M), r->E.resize(3 * M), r->energy.resize(6 + 6 * ns);
+    r->n.resize(static_cast<size_t>(p.n_kinetic) * M), r->nV.resize(3 * r->n.size()), r->nvv.resize(6 * r->n.size());
+    TRY(h1d_download_fields(r->run, r->B.data(), r->E.data()));
+    std::vector<double> lab(3 * ns), pla(3 * ns);
+    TRY(h1d_energy(r->run, r->energy.data(), r->energy.data() + 3, lab.data(), pla.data()));
+    for (int s = 0; s < ns; ++s)
+        for (int c = 0; c < 3; ++c)
+            r->energy[6 + 6 * s + c] = lab[3 * s + c], r->energy[6 + 6 * s + 3 + c] = pla[3 * s + c];
+    for (int s = 0; s < p.n_kinetic; ++s)
+        TRY(h1d_download_moments(r->run, s, r->n.data() + s * M, r->nV.data() + 3 * s * M, r->nvv.data() + 6 * s * M));
+    return H1D_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+int h1d_server_create(size_t hbm_budget_bytes, int steps_per_tick, h1d_server **out)
+{
+    if (!out || steps_per_tick <= 0)
+        return H1D_ERR_INVALID_ARG;
+    *out          = nullptr;
+    h1d_server *sv = new (std::nothrow) h1d_server{};
+    if (!sv)
+        return H1D_ERR_OOM;
+    sv->budget  = hbm_budget_bytes;
+    sv->quantum = steps_per_tick;
+    *out        = sv;
+    return H1D_OK;
+}
+
+int h1d_server_configure(h1d_server *sv, int sort_interval)
+{
+    if (!sv || sort_interval <= 0 || sort_interval > 4096)
+        return H1D_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(sv->mu);
+    sv->sort_interval = sort_interval;
+    sv->dirty         = true;
+    return H1D_OK;
+}
+
+int h1d_server_submit(h1d_server *sv, h1d_request const *rq, uint64_t *id)
+{
+    if (!sv || !rq || !id)
+        return H1D_ERR_INVALID_ARG;
+    std::string m;
+    if (int const st = validate(&rq->params, m)) {
+        std::fprintf(stderr, "h1d_server_submit: %s\n", m.c_str());
+        return st;
+    }
+    if (rq->params.algorithm != H1D_ALGO_CAMCL || rq->n_steps == 0)
+        return H1D_ERR_INVALID_ARG;
+    for (int s = 0; s < rq->params.n_kinetic; ++s)
+        if (rq->n_particles[s] < 0 || rq->n_particles[s] > (int64_t{ 1 } << 31) - 1 || !(rq->beta1[s] > 0)
+            || !(rq->T2_T1[s] > 0))
+            return H1D_ERR_INVALID_ARG;
+    auto *r  = new (std::nothrow) ServerReq{};
+    if (!r)
+        return H1D_ERR_OOM;
+    r->rq    = *rq;
+    r->bytes = request_bytes(*rq);
+    std::lock_guard<std::mutex> lock(sv->mu);
+    if (r->bytes > sv->budget) {
+        delete r;
+        std::fprintf(stderr, "h1d_server_submit: the request needs more device memory than the whole budget\n");
+        return H1D_ERR_OOM;
+    }
+    r->id       = sv->next_id++;
+    r->t_submit = sv->now();
+    sv->queue.push_back(r);
+    sv->all[r->id] = r;
+    sv->stats.submitted++;
+    *id = r->id;
+    return H1D_OK;
+}
+
+int h1d_server_tick(h1d_server *sv, int *n_active, int *n_queued)
+{
+    if (!sv)
+        return H1D_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(sv->mu);
+    // 1. admission: every queued request that fits the budget (in arrival order) and the device
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    for (auto it = sv->queue.begin(); it != sv->queue.end();) {
+        ServerReq *r = *it;
+        if (sv->used + r->bytes > sv->budget || r->bytes + (size_t{ 256 } << 20) > free_b) {
+            ++it;
+            continue;
+        }
+        it = sv->queue.erase(it);
+        int const st = admit(sv, r);
+        if (st != H1D_OK) {
+            finish_request(sv, r, st, r->msg.empty() ? "admission failed" : r->msg);
+            continue;
+        }
+        free_b   = free_b > r->bytes ? free_b - r->bytes : 0;
+        r->state = H1D_REQ_ACTIVE;
+        r->t_admit = sv->now();
+        sv->active.push_back(r);
+        sv->stats.admitted++;
+        sv->dirty = true;
+    }
+    // 2. the batch of the active runs
+    if (sv->dirty) {
+        fold_batch_stats(sv);
+        h1d_batch_destroy(sv->batch);
+        sv->batch = nullptr;
+        if (!sv->active.empty()) {
+            std::vector<h1d_run *> runs;
+            for (ServerReq *r : sv->active)
+                runs.push_back(r->run);
+            int st = h1d_batch_create(runs.data(), static_cast<int>(runs.size()), &sv->batch);
+            if (st == H1D_OK)
+                st = h1d_batch_configure(sv->batch, sv->sort_interval, 0, 1);
+            if (st != H1D_OK) {
+                for (ServerReq *r : sv->active)
+                    finish_request(sv, r, st, "batch creation failed");
+                sv->active.clear();
+                h1d_batch_destroy(sv->batch);
+                sv->batch = nullptr;
+            }
+        }
+        sv->dirty = false;
+        sv->stats.batches_built++;
+    }
+    // 3. one quantum (or up to the nearest completion)
+    if (sv->batch) {
+        uint32_t q = static_cast<uint32_t>(sv->quantum);
+        for (ServerReq *r : sv->active)
+            q = std::min(q, r->rq.n_steps - r->done_steps);
+        int const st = h1d_batch_advance(sv->batch, q);
+        if (st != H1D_OK) { // a member failed: fail every member of the batch
+            std::string const m = h1d_batch_status_string(sv->batch);
+            h1d_batch_destroy(sv->batch);
+            sv->batch = nullptr;
+            for (ServerReq *r : sv->active)
+                finish_request(sv, r, st, m);
+            sv->active.clear();
+        } else {
+            for (ServerReq *r : sv->active)
+                r->done_steps += q;
+        }
+    }
+    // 4. retire finished runs
+    for (auto it = sv->active.begin(); it != sv->active.end();) {
+        ServerReq *r = *it;
+        if (r->done_steps < r->rq.n_steps) {
+            ++it;
+            continue;
+        }
+        if (sv->batch) { // the run leaves the batch before it is read and freed
+            fold_batch_stats(sv);
+            h1d_batch_destroy(sv->batch);
+            sv->batch = nullptr;
+            sv->dirty = true;
+        }
+        int const st = collect(r);
+        finish_request(sv, r, st, st == H1D_OK ? "" : r->run->msg);
+        it = sv->active.erase(it);
+    }
+    if (n_active)
+        *n_active = static_cast<int>(sv->active.size());
+    if (n_queued)
+        *n_queued = static_cast<int>(sv->queue.size());
+    return H1D_OK;
+}
+
+int h1d_server_poll(h1d_server *sv, uint64_t id, int *state, double *t_submit, double *t_admit, double *t_done)
+{
+    if (!sv)
+        return H1D_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(sv->mu);
+    auto const it = sv->all.find(id);
+    if (it == sv->all.end())
+        return H1D_ERR_INVALID_ARG;
+    ServerReq const *r = it->second;
+    if (state)
+        *state = r->state;
+    if (t_submit)
+        *t_submit = r->t_submit;
+    if (t_admit)
+        *t_admit = r->t_admit;
+    if (t_done)
+        *t_done = r->t_done;
+    return r->state == H1D_REQ_FAILED ? r->status : H1D_OK;
+}
+
+int h1d_server_result(h1d_server *sv, uint64_t id, double *B, double *E, double *energy, double *n, double *nV,
+                      double *nvv)
+{
+    if (!sv)
+        return H1D_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(sv->mu);
+    auto const it = sv->all.find(id);
+    if (it == sv->all.end())
+        return H1D_ERR_INVALID_ARG;
+    ServerReq *r = it->second;
+    if (r->state == H1D_REQ_FAILED)
+        return r->status;
+    if (r->state != H1D_REQ_DONE)
+        return H1D_ERR_STATE;
+    auto cp = [](double *dst, std::vector<double> const &v) {
+        if (dst && !v.empty())
+            std::memcpy(dst, v.data(), sizeof(double) * v.size());
+    };
+    cp(B, r->B), cp(E, r->E), cp(energy, r->energy), cp(n, r->n), cp(nV, r->nV), cp(nvv, r->nvv);
+    return H1D_OK;
+}
+
+int h1d_server_release(h1d_server *sv, uint64_t id)
+{
+    if (!sv)
+        return H1D_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(sv->mu);
+    auto const it = sv->all.find(id);
+    if (it == sv->all.end() || (it->second->state != H1D_REQ_DONE && it->second->state != H1D_REQ_FAILED))
+        return H1D_ERR_STATE;
+    delete it->second;
+    sv->all.erase(it);
+    return H1D_OK;
+}
+
+int h1d_server_stats_read(h1d_server *sv, h1d_server_stats *out)
+{
+    if (!sv || !out)
+        return H1D_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lock(sv->mu);
+    *out = sv->stats;
+    if (sv->batch) {
+        h1d_batch_stats st{};
+        h1d_batch_stats_read(sv->batch, &st);
+        out->kernel_launches += st.kernel_launches, out->graph_launches += st.graph_launches, out->steps += st.steps;
+    }
+    out->bytes_in_use = static_cast<int64_t>(sv->used);
+    out->peak_bytes   = static_cast<int64_t>(sv->peak);
+    return H1D_OK;
+}
+
+int h1d_server_destroy(h1d_server *sv)
+{
+    if (!sv)
+        return H1D_OK;
+    h1d_batch_destroy(sv->batch);
+    for (auto &[id, r] : sv->all) {
+        if (r->run)
+            h1d_destroy(r->run);
+        delete r;
+    }
+    delete sv;
     return H1D_OK;
 }
 

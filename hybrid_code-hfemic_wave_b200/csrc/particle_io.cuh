@@ -236,4 +236,97 @@ __global__ void gather_kernel_mixed(GatherArgsMixed a)
     a.pid_dst[i]  = a.pid_src[j];
 }
 
+// ------------------------------------------------------------------------------------------------
+// Device loader of a bi-Maxwellian species (PartSpecies::populate with MaxwellianVDF::load,
+// VDF/MaxwellianVDF.cc:300-319, q1_of_N :240-250, eta :218-228).  Particle i uses the radical
+// inverses in bases 2, 3 and 5 of the sequence index offset + i and two counter-based uniforms (the
+// splitmix64 finalizer of the species key and 2i + 1, 2i + 2).  Every arithmetic step is the one
+// the host loader (loader.py) performs, in the same order and without contraction, so the two
+// agree up to the device's tan/atan/cos/log/sin.
+// ------------------------------------------------------------------------------------------------
+constexpr uint64_t POP_GOLDEN = 0x9E3779B97F4A7C15ULL;
+
+inline uint64_t populate_key(uint64_t seed, uint64_t s)
+{
+    return mix64(mix64(seed ^ 0x243F6A8885A308D3ULL) + s * POP_GOLDEN);
+}
+inline uint64_t populate_offset(uint64_t key) { return 1 + (mix64(key ^ 0x13198A2E03707344ULL) >> 24); }
+
+struct PopulateArgs {
+    int64_t  n;
+    uint64_t key, offset;
+    double   N_loc, N_len, xiD1, T2m1, sqrtT2, sDxXi, T2, oneMinusT2, vth1, q1min, q1max_in, full_min;
+    int      homogeneous;
+    double  *q1, *vx, *vy, *vz, *w;                 // FP64 storage, or
+    int32_t *cell;                                   // mixed-precision storage
+    float   *off, *fvx, *fvy, *fvz, *fw;
+};
+
+__device__ __forceinline__ double radical_inverse_dev(uint64_t k, unsigned base)
+{
+    if (base == 2)
+        return __dmul_rn(static_cast<double>(__brevll(k) >> 11), 0x1p-53);
+    double       out = 0, f = __ddiv_rn(1.0, static_cast<double>(base));
+    double const b   = static_cast<double>(base);
+    while (k) {
+        out = __dadd_rn(out, __dmul_rn(static_cast<double>(k % base), f));
+        k /= base;
+        f = __ddiv_rn(f, b);
+    }
+    return out;
+}
+
+__device__ __forceinline__ double pop_uniform(uint64_t key, uint64_t i, uint64_t j)
+{
+    double const eps = 1e-15;
+    double const u   = __dmul_rn(static_cast<double>(mix64(key + (i * 2 + j) * POP_GOLDEN) >> 11), 0x1p-53);
+    return __dadd_rn(eps, __dmul_rn(1 - 2 * eps, u));
+}
+
+__global__ void populate_kernel(PopulateArgs a)
+{
+    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= a.n)
+        return;
+    double const   eps = 1e-15, one_m = 1 - 2 * eps, two_pi = 2 * 3.141592653589793;
+    uint64_t const idx = a.offset + static_cast<uint64_t>(i);
+    double const   u2  = __dadd_rn(eps, __dmul_rn(one_m, radical_inverse_dev(idx, 2)));
+    double const   u3  = __dadd_rn(eps, __dmul_rn(one_m, radical_inverse_dev(idx, 3)));
+    double const   u5  = __dadd_rn(eps, __dmul_rn(one_m, radical_inverse_dev(idx, 5)));
+    double const   N   = __dadd_rn(__dmul_rn(u2, a.N_len), a.N_loc);
+    double         q1;
+    if (a.homogeneous) {
+        double const x = __dmul_rn(a.xiD1, N);
+        double       t = __dmul_rn(__dmul_rn(x, x), a.T2m1);
+        t              = __dadd_rn(1.0, __ddiv_rn(t, 3.0));
+        q1             = __dmul_rn(N, t);
+    } else {
+        q1 = __ddiv_rn(atan(__ddiv_rn(tan(__dmul_rn(a.sDxXi, N)), a.sqrtT2)), a.xiD1);
+    }
+    q1                  = fmin(fmax(q1, a.q1min), a.q1max_in);
+    double const U1     = pop_uniform(a.key, static_cast<uint64_t>(i), 1);
+    double const U2     = pop_uniform(a.key, static_cast<uint64_t>(i), 2);
+    double const c      = cos(__dmul_rn(a.xiD1, q1));
+    double const eta    = __ddiv_rn(1.0, __dadd_rn(a.T2, __dmul_rn(__dmul_rn(a.oneMinusT2, c), c)));
+    double const T2OT1  = __dmul_rn(a.T2, eta);
+    double const x1     = __dmul_rn(sqrt(-log(U1)), sin(__dmul_rn(two_pi, u3)));
+    double const tmp    = sqrt(__dmul_rn(-log(U2), T2OT1));
+    double const x2     = __dmul_rn(cos(__dmul_rn(two_pi, u5)), tmp);
+    double const x3     = __dmul_rn(sin(__dmul_rn(two_pi, u5)), tmp);
+    double const vx = __dmul_rn(x1, a.vth1), vy = __dmul_rn(x2, a.vth1), vz = __dmul_rn(x3, a.vth1);
+    if (a.q1) {
+        a.q1[i] = q1, a.vx[i] = vx, a.vy[i] = vy, a.vz[i] = vz, a.w[i] = 1.0;
+    } else {
+        double const x = q1 - a.full_min;
+        double const f = floor(x);
+        float        o = static_cast<float>(x - f);
+        if (o >= 1.0f)
+            o = 0.99999994f;
+        a.cell[i] = static_cast<int32_t>(f), a.off[i] = o;
+        a.fvx[i] = static_cast<float>(vx), a.fvy[i] = static_cast<float>(vy), a.fvz[i] = static_cast<float>(vz);
+        a.fw[i] = 1.0f;
+    }
+}
+
+
 } // namespace h1d

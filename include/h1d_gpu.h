@@ -150,6 +150,14 @@ int h1d_destroy(h1d_run *run);
  * Replaces any previous particles of that species. */
 int h1d_upload_particles(h1d_run *run, int s, int64_t n, const double *q1, const double *vx,
                          const double *vy, const double *vz, const double *w);
+/* PartSpecies::populate with a bi-Maxwellian MaxwellianVDF (VDF/MaxwellianVDF.cc:88-134, 300-319),
+ * on the device: n particles of kinetic species `s` with parallel beta `beta1` and T_perp/T_par
+ * `T2_T1`, positions from the base-2 radical inverse through q1_of_N, velocities from base-3/5
+ * radical inverses and two counter-based uniforms of (seed, s, particle), full-f weight 1.
+ * Replaces any previous particles of that species.  The reference seeds its generators with fixed
+ * constants; here `seed` selects the sequences, and loader.py computes the same particles on the
+ * host. */
+int h1d_populate(h1d_run *run, int s, int64_t n, uint64_t seed, double beta1, double T2_T1);
 /* B (full grid) and E (half grid), each (Nx+2*H1D_PAD)*3 doubles, GridArray layout */
 int h1d_upload_fields(h1d_run *run, const double *B, const double *E);
 /* cold species `i`: mom0_full (Nx+2*H1D_PAD doubles), mom1_full ((Nx+2*H1D_PAD)*3) */
@@ -268,6 +276,45 @@ int h1d_batch_configure(h1d_batch *batch, int sort_interval, int push_ctas_per_s
 int h1d_batch_autotune(h1d_batch *batch, uint32_t *steps_taken, int *sort_interval, int *push_ctas_per_sm);
 int h1d_batch_stats_read(h1d_batch *batch, h1d_batch_stats *out);
 const char *h1d_batch_status_string(h1d_batch *batch);
+
+/* ---- Serving loop (no counterpart in the reference) --------------------------------------------
+ * Requests wait in a queue until the device memory they need fits the server's budget; admitted
+ * runs are built on the device (h1d_populate, cold fluid at rest, zero fields), advance together
+ * as one batch by up to `steps_per_tick` steps per h1d_server_tick, and are read back (fields,
+ * energies, moments) and freed when their steps are done, which admits the next requests.  The
+ * caller drives the loop by calling h1d_server_tick; submit, poll, result and release may come
+ * from other threads.  Times are seconds since h1d_server_create on a monotonic clock. */
+typedef struct h1d_server h1d_server;
+typedef struct h1d_request {
+    h1d_params params;                    /* a CAM-CL run */
+    double     beta1[H1D_MAX_KINETIC];    /* loader of each kinetic species: parallel beta */
+    double     T2_T1[H1D_MAX_KINETIC];    /* and T_perp / T_par */
+    int64_t    n_particles[H1D_MAX_KINETIC];
+    uint64_t   seed;                      /* loader seed */
+    uint32_t   n_steps;
+    uint32_t   reserved0;
+} h1d_request;
+enum { H1D_REQ_QUEUED = 0, H1D_REQ_ACTIVE = 1, H1D_REQ_DONE = 2, H1D_REQ_FAILED = 3 };
+typedef struct h1d_server_stats {
+    int64_t submitted, admitted, completed, failed;
+    int64_t steps, kernel_launches, graph_launches, batches_built;
+    int64_t bytes_in_use, peak_bytes; /* device memory of admitted runs, by the admission estimate */
+} h1d_server_stats;
+int h1d_server_create(size_t hbm_budget_bytes, int steps_per_tick, h1d_server **out);
+int h1d_server_configure(h1d_server *server, int sort_interval);
+int h1d_server_submit(h1d_server *server, const h1d_request *request, uint64_t *id);
+/* admit what fits, advance the active runs by one quantum, retire the finished ones */
+int h1d_server_tick(h1d_server *server, int *n_active, int *n_queued);
+/* state is H1D_REQ_*; returns the run's error status for a failed request */
+int h1d_server_poll(h1d_server *server, uint64_t id, int *state, double *t_submit, double *t_admit, double *t_done);
+/* results of a finished request: B and E ((Nx+2*H1D_PAD)*3 each), energy (6 + 6*(n_kinetic+n_cold):
+ * dB2O2[3], dE2O2[3], then per species KE_lab[3], KE_pla[3]), and per kinetic species n, nV, nvv
+ * as h1d_download_moments, species after species; any pointer may be NULL */
+int h1d_server_result(h1d_server *server, uint64_t id, double *B, double *E, double *energy, double *n,
+                      double *nV, double *nvv);
+int h1d_server_release(h1d_server *server, uint64_t id);
+int h1d_server_stats_read(h1d_server *server, h1d_server_stats *out);
+int h1d_server_destroy(h1d_server *server);
 
 const char *h1d_status_string(h1d_run *run);
 const char *h1d_error_name(int status);

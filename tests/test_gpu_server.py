@@ -1,0 +1,110 @@
+"""The serving loop (h1d_server_*): continuous batching under an HBM budget.
+
+A request's results are the same whether it runs alone or among other requests that arrive,
+join and leave while it is on the device: FP64 within 1e-10 and mixed precision within 1e-4
+(max-norm relative over fields, energies and moments).  A request served equals the same run
+built and advanced directly through h1d_create / h1d_populate / h1d_advance.
+"""
+import numpy as np
+import pytest
+from parity_util import rel_err
+
+import hfemic_b200 as h
+
+pytestmark = pytest.mark.gpu
+GB = 1 << 30
+
+
+def _cfg(seed, precision, ppc_scale=0.05):
+    return h.configs.ensemble_member(seed, precision=precision, ppc_scale=ppc_scale)
+
+
+def _drain(sv, ids, max_ticks=100000):
+    for _ in range(max_ticks):
+        a, q = sv.tick()
+        if all(sv.poll(i)["state"] >= h.abi.REQ_DONE for i in ids):
+            return
+    raise AssertionError("requests did not finish")
+
+
+def _errs(x, y):
+    return {k: rel_err(x[k], y[k]) for k in ("B", "E", "dB2O2", "dE2O2", "KE", "n", "nV", "nvv")}
+
+
+@pytest.mark.parametrize("precision,tol", [(h.configs.PREC_FP64, 1e-10), (h.configs.PREC_MIXED, 1e-4)])
+def test_result_same_alone_and_in_mix(gpu_lib, precision, tol):
+    x = _cfg(5, precision)
+    with h.abi.Server(gpu_lib, 8 * GB, steps_per_tick=16, sort_interval=8) as sv:
+        i = sv.submit(x, seed=5, n_steps=96)
+        _drain(sv, [i])
+        alone = sv.result(i)
+    with h.abi.Server(gpu_lib, 8 * GB, steps_per_tick=16, sort_interval=8) as sv:
+        early = [sv.submit(_cfg(s, precision), seed=s, n_steps=n) for s, n in ((1, 40), (2, 200))]
+        sv.tick()
+        i = sv.submit(x, seed=5, n_steps=96)  # joins a running batch
+        sv.tick()
+        late = [sv.submit(_cfg(s, h.configs.PREC_FP64), seed=s, n_steps=n) for s, n in ((3, 24), (4, 130))]
+        _drain(sv, early + [i] + late)
+        mixed = sv.result(i)
+        st = sv.stats()
+        assert st["completed"] == 5 and st["failed"] == 0
+        assert st["batches_built"] >= 4
+    errs = _errs(mixed, alone)
+    print(precision, {k: f"{v:.1e}" for k, v in errs.items()})
+    assert max(errs.values()) <= tol, errs
+
+
+def test_served_equals_direct_run(gpu_lib):
+    cfg = _cfg(6, h.configs.PREC_FP64)
+    with h.abi.Server(gpu_lib, 8 * GB, steps_per_tick=32, sort_interval=16) as sv:
+        i = sv.submit(cfg, seed=6, n_steps=64)
+        _drain(sv, [i])
+        res = sv.result(i)
+    with h.Run(cfg.replace(sort_interval=16), gpu_lib) as r:
+        h.abi.populate_state(r, seed=6)
+        r.advance(64)
+        B, E = r.fields()
+        e = r.energy()
+        n, nV, nvv = r.moments(0)
+    assert rel_err(res["B"], B) <= 1e-10 and rel_err(res["E"], E) <= 1e-10
+    assert rel_err(res["dB2O2"], e["dB2O2"]) <= 1e-10
+    assert rel_err(res["n"][0], n) <= 1e-10 and rel_err(res["nvv"][0], nvv) <= 1e-10
+
+
+def test_admission_respects_budget(gpu_lib):
+    """A budget that holds the two largest requests but not three: the server never exceeds it,
+    never runs all six together, and finishes them all."""
+    cfgs = [_cfg(s, h.configs.PREC_MIXED) for s in range(6)]
+    sizes = sorted((_estimate(c) for c in cfgs), reverse=True)
+    budget = sizes[0] + sizes[1] + sizes[-1] // 2
+    with h.abi.Server(gpu_lib, budget, steps_per_tick=16) as sv:
+        ids = [sv.submit(c, seed=s, n_steps=48) for s, c in enumerate(cfgs)]
+        peak_active = 0
+        for _ in range(100000):
+            a, q = sv.tick()
+            peak_active = max(peak_active, a)
+            assert sv.stats()["bytes_in_use"] <= budget
+            if all(sv.poll(i)["state"] >= h.abi.REQ_DONE for i in ids):
+                break
+        st = sv.stats()
+        assert st["completed"] == 6 and st["peak_bytes"] <= budget
+        assert peak_active < 6
+
+
+def _estimate(cfg):
+    """The server's admission estimate, restated: particles in two buffer sets with ids and sort
+    keys, sort histograms, grids."""
+    M = cfg.Nx + 6
+    per = 24 if cfg.precision == h.configs.PREC_MIXED else 40
+    b = 0
+    for k in cfg.kinetic:
+        n = k.Nc * cfg.Nx + 64
+        b += 2 * n * (per + 12) + (n // 2048 + 1) * 256 * 4 * 2
+    b += 8 * M * (17 + 18 + 6 + 1 + 3 + 6 + 8 * 36 + 4 * 17)
+    return b + (1 << 20)
+
+
+def test_oversize_request_is_refused(gpu_lib):
+    with h.abi.Server(gpu_lib, 1 << 20, steps_per_tick=16) as sv:
+        with pytest.raises(h.H1DError):
+            sv.submit(_cfg(0, h.configs.PREC_FP64), seed=0, n_steps=10)
