@@ -383,6 +383,93 @@ def e2e_measure(h, cfg, st, K, world):
                     "downloads after each chunk, particle download at the end"}
 
 
+def ensemble_measure(h, precision, steps=500, members=64):
+    """The ensemble workload: `members` runs drawn with seeds 0..members-1 (Nx uniform over
+    256..4096, particles per cell log-uniform in [100, 2000], T_perp/T_par, beta_par and xi drawn,
+    TSC), loaded on the device, advanced together by `steps` steps in one batch (one particle-pass
+    launch and one field launch per step, pairs of sort blocks replayed as CUDA graphs) after the
+    autotuner chose the sort interval and CTA count.  Returns runs/s and particle-steps/s."""
+    import torch
+
+    cfgs = [h.configs.ensemble_member(seed, precision=precision, steps=steps) for seed in range(members)]
+    runs = []
+    try:
+        for seed, c in enumerate(cfgs):
+            r = h.open_run(c)
+            h.abi.populate_state(r, seed)
+            runs.append(r)
+        n_particles = sum(c.n_particles for c in cfgs)
+        with h.abi.Batch(runs) as b:
+            tuned_steps, k, ctas = b.autotune()
+            stream = torch.cuda.ExternalStream(b.stream())
+            b.advance(4 * k)  # warm-up: builds and replays the graph of the chosen interval
+            s0 = b.stats()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            b.advance_async(steps)
+            e1.record(stream)
+            b.synchronize()
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            s1 = b.stats()
+    finally:
+        for r in runs:
+            r.close()
+    return {"workload": f"ensemble of {members} runs (seeds 0..{members - 1}), {steps} steps each, TSC",
+            "precision": "mixed" if precision == h.configs.PREC_MIXED else "fp64",
+            "runs_per_s": members / (ms / 1e3), "value": n_particles * steps / (ms / 1e3), "unit": METRIC,
+            "ms": ms, "particles": n_particles, "Nx": [c.Nx for c in cfgs][:8] + ["..."],
+            "autotune": {"steps": tuned_steps, "sort_interval": k, "ctas_per_sm": ctas},
+            "gpu_launches": s1["kernel_launches"] - s0["kernel_launches"],
+            "graph_launches": s1["graph_launches"] - s0["graph_launches"]}
+
+
+def serving_measure(h, precision, n_requests=48, rate=4.0, budget_gb=150, seed=2024):
+    """The serving workload: a seeded Poisson stream (mean `rate` per second) of `n_requests`
+    requests drawn like the ensemble members with steps uniform in [200, 2000], served in real time
+    by the continuous-batching server under a `budget_gb` HBM budget.  Latency = completion time -
+    submission time; throughput = completed runs / (last completion - first submission)."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests)) if rate else np.zeros(n_requests)
+    steps = rng.integers(200, 2001, n_requests)
+    lib = h.library_path()
+    sv = h.abi.Server(lib, int(budget_gb * (1 << 30)), steps_per_tick=64, sort_interval=16)
+    ids = []
+    try:
+        t0 = time.perf_counter()
+        nxt = 0
+        done = set()
+        while len(done) < n_requests:
+            now = time.perf_counter() - t0
+            while nxt < n_requests and arrivals[nxt] <= now:
+                cfg = h.configs.ensemble_member(1000 + nxt, precision=precision)
+                ids.append(sv.submit(cfg, seed=1000 + nxt, n_steps=int(steps[nxt])))
+                nxt += 1
+            active, queued = sv.tick()
+            for i in ids:
+                if i not in done and sv.poll(i)["state"] >= h.abi.REQ_DONE:
+                    done.add(i)
+            if active == 0 and queued == 0 and nxt < n_requests:
+                time.sleep(max(0.0, min(0.05, arrivals[nxt] - (time.perf_counter() - t0))))
+        polls = [sv.poll(i) for i in ids]
+        st = sv.stats()
+    finally:
+        sv.close()
+    lat = np.array([p["t_done"] - p["t_submit"] for p in polls])
+    span = max(p["t_done"] for p in polls) - min(p["t_submit"] for p in polls)
+    failed = sum(p["state"] != h.abi.REQ_DONE for p in polls)
+    stream = f"Poisson stream, mean {rate}/s" if rate else "all submitted at once (saturated)"
+    return {"workload": f"{stream}, {n_requests} requests (ensemble draws, steps U[200, 2000]), {budget_gb} GB HBM budget",
+            "precision": "mixed" if precision == h.configs.PREC_MIXED else "fp64",
+            "runs_per_s": (n_requests - failed) / span, "p50_s": float(np.percentile(lat, 50)),
+            "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()), "failed": int(failed),
+            "peak_hbm_gb": st["peak_bytes"] / (1 << 30), "batches_built": st["batches_built"],
+            "gpu_launches": st["kernel_launches"], "graph_launches": st["graph_launches"]}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -394,6 +481,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the fp64 / error / drop-in side measurements")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble and serving measurements")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference", "at least 3 warm-up steps"
 
@@ -458,6 +546,12 @@ def main():
             del st2
 
     e2e = None if args.no_e2e else e2e_measure(h, cfg, st, args.steps, world)
+    del st
+
+    if not args.no_ensemble:
+        extras["ensemble"] = {p: ensemble_measure(h, getattr(h.configs, "PREC_" + p.upper())) for p in ("mixed", "fp64")}
+        extras["serving"] = {p: serving_measure(h, getattr(h.configs, "PREC_" + p.upper())) for p in ("mixed", "fp64")}
+        extras["serving"]["mixed_saturated"] = serving_measure(h, h.configs.PREC_MIXED, rate=None)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
