@@ -283,7 +283,7 @@ PushArgs push_args(h1d_run *run, int s)
     PushArgs                a{};
     a.q1 = S.buf[S.cur][0], a.vx = S.buf[S.cur][1], a.vy = S.buf[S.cur][2], a.vz = S.buf[S.cur][3];
     a.w = S.buf[S.cur][4], a.pid = S.pid[S.cur];
-    a.n = S.n, a.ppt = ppt_for(run, s), a.Nx = static_cast<int>(run->Nx);
+    a.n = S.n, a.Nx = static_cast<int>(run->Nx);
     a.EB = run->EB + 6 * PAD;
     for (int dd = 0; dd < 2; ++dd)
         for (int q = 0; q < 4; ++q)

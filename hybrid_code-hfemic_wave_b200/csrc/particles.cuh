@@ -7,13 +7,11 @@
 //   PartSpecies::update_pos   x^{N+1} = x^N + v.e^1 dt, travel check                   (PartSpecies.cc:252-264)
 //   Delegate::boundary_pass   periodic wrap / reflection (+ gyro-phase)               (Delegate.cc:116-228)
 //   PartSpecies::collect_part deposit of n and nV at x^{N+1}                          (PartSpecies.cc:315-329)
-// Particles are structure-of-arrays and cell-sorted (sort.cuh), so the 32 x ppt particles of a
-// warp span a couple of cells.  Each lane accumulates its deposits in registers over a small
-// warp-uniform window of cells; the window is reduced across the warp once per warp-chunk and
-// added to the global moment arrays with one atomic per (cell, quantity).  Particles that fall
-// outside the window (rare: drift since the last sort, periodic wrap) add their stencil with
-// direct atomics.  Moments are accumulated unscaled; the 1/Nc factor of collect_part is applied
-// by the field kernel.
+// Particles are structure-of-arrays and cell-sorted (sort.cuh), so the particles of a warp span a
+// few cells.  Each warp deposits into a window of PIPE_W cells held in shared memory as
+// lane-private columns; a window is summed over its 32 columns and added to the global moment
+// arrays (one atomic per cell and quantity) only when it has to move.  Moments are accumulated
+// unscaled; the 1/Nc factor of collect_part is applied by the field kernel.
 #pragma once
 
 #include "device_common.cuh"
@@ -28,7 +26,6 @@ struct PushArgs {
     double        *w; // writable only for absorption (w = 0 marks a removed particle)
     int32_t const *pid;
     int64_t        n;
-    int            ppt; // particles per lane per warp-chunk
     int            Nx;
     double const  *EB; // per cell {Ex, Ey, Ez, dBx, dBy, dBz}: E and B averaged onto the half grid
                        // (PartSpecies.cc:132-139), pointer at interior cell 0
@@ -37,83 +34,13 @@ struct PushArgs {
     double         xi, xi2, xiD1, D1, inv_D1, O0, Oc, dt, travel_scale, xiO0_Oc;
     BorisK         boris;
     unsigned      *status;
-    unsigned long long *fallbacks; // deposits that missed the register window (diagnostic)
+    unsigned long long *fallbacks; // deposits outside their warp's window (diagnostic)
     uint64_t       seed, counter;
     int            species, randomize, homogeneous_poly;
     int            move_steps; // 1: CAM-CL full step; 2: PC half step, push, half step; 0: deposit only
     int            deposit_mask; // bit0: deposit at x^N, bit1: deposit at the end position
     int            write_back;   // 0 for the PC predictor (particles are not kept)
 };
-
-template <int O, int S>
-struct Acc {
-    double v[4][S];
-};
-
-template <int O, int S>
-__device__ __forceinline__ void acc_zero(Acc<O, S> &a)
-{
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int s = 0; s < S; ++s)
-            a.v[q][s] = 0;
-}
-
-// deposit one particle: register window if its stencil fits, else direct atomics
-template <int O, int S, int R>
-__device__ __forceinline__ void deposit_at(Acc<O, S> &acc, Shape<O> const &sh, double const (&vw)[4])
-{
-#pragma unroll
-    for (int j = 0; j <= O; ++j)
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-            acc.v[q][R + j] = fma(vw[q], sh.w[j], acc.v[q][R + j]);
-}
-template <int O, int S, int D>
-__device__ __forceinline__ void deposit(Acc<O, S> &acc, int base, Shape<O> const &sh, double w, d3 v,
-                                        PushArgs const &a)
-{
-    constexpr int RW     = S - O - 1; // window offsets 0..RW
-    double const  vw[4] = { w, v.x * w, v.y * w, v.z * w };
-    int const     r     = sh.i0 - base;
-    static_assert(RW >= 1 && RW <= 3, "window offsets 0..RW with RW in {1, 2, 3}");
-    if (r == 0)
-        deposit_at<O, S, 0>(acc, sh, vw);
-    else if (r == 1)
-        deposit_at<O, S, 1>(acc, sh, vw);
-    else if (RW >= 2 && r == 2)
-        deposit_at<O, S, (RW >= 2 ? 2 : 0)>(acc, sh, vw);
-    else if (RW >= 3 && r == 3)
-        deposit_at<O, S, (RW >= 3 ? 3 : 0)>(acc, sh, vw);
-    else {
-        atomicAdd(a.fallbacks, 1ull);
-#pragma unroll
-        for (int j = 0; j <= O; ++j)
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-                atomicAdd(a.dep[D][q] + sh.i0 + j, vw[q] * sh.w[j]);
-    }
-}
-
-template <int O, int S, int D>
-__device__ __forceinline__ void flush(Acc<O, S> const &acc, int base, int lane, PushArgs const &a)
-{
-    constexpr int tag = D;
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            double const v = warp_sum(acc.v[q][s]);
-            if (lane == ((tag * 4 + q) * S + s) % 32 && v != 0.0) {
-                int const cell = base + s;
-                if (cell >= -PAD && cell < a.Nx + PAD)
-                    atomicAdd(a.dep[D][q] + cell, v);
-                else
-                    atomicOr(a.status, ST_OUT_OF_RANGE);
-            }
-        }
-}
 
 template <int O>
 __device__ __forceinline__ bool stencil_ok(Shape<O> const &sh, int Nx)
@@ -209,32 +136,37 @@ __device__ __forceinline__ void interp_EB(double const *eb, Shape<O> const &sh, 
 }
 
 // ------------------------------------------------------------------------------------------------
-// The particle pass.  Warp-specialised pipeline per CTA: one producer warp streams chunks of
-// PIPE_CHUNK particles global -> shared with 1-D TMA bulk copies completing on mbarriers
-// (PIPE_STAGES deep) and bulk-stores the updated particles back; PIPE_CONSUMER_WARPS warps
-// compute.  A consumer warp owns 32 x PIPE_PPT consecutive (cell-sorted) particles of a chunk and
-// makes two passes over them in shared memory: (1) push at x^N, deposit at x^N, move, boundary,
-// results written in place; (2) deposit at the new position.  Splitting the two deposits halves
-// the register windows.
+// The particle pass.  Warp-specialised pipeline per CTA: one producer warp streams the CTA's
+// contiguous run of chunks (PIPE_CHUNK particles each) global -> shared with 1-D TMA bulk copies
+// completing on mbarriers (PIPE_STAGES deep) and bulk-stores the updated particles back;
+// PIPE_CONSUMER_WARPS warps compute.  A consumer warp owns 32 x PIPE_PPT consecutive (cell-sorted)
+// particles of each chunk and, per particle: pushes at x^N, moves, applies the boundary, writes
+// the result beside the inputs, and deposits at x^N (with the pre-boundary velocity) and at the
+// end position into its shared-memory window.
 //
-// One pass of a species: CAM-CL (move_steps == 1): push at x^N, deposit, move, BC, deposit.
+// CAM-CL (move_steps == 1): push at x^N, deposit, move, BC, deposit.
 // Predictor-corrector (move_steps == 2, Domain_PC.cc:110-124, 169-181): half move, BC, push at
 // the half-step position, half move, BC, deposit.  move_steps == 0: deposit only
 // (Domain_PC.cc:36-44).
 // ------------------------------------------------------------------------------------------------
 constexpr int PIPE_CONSUMER_WARPS = 4;
 constexpr int PIPE_THREADS        = 32 * (PIPE_CONSUMER_WARPS + 1);
-constexpr int PIPE_PPT            = 4;
-constexpr int PIPE_CHUNK          = 32 * PIPE_CONSUMER_WARPS * PIPE_PPT;
+constexpr int PIPE_CHUNK          = 256;
+constexpr int PIPE_PPT            = PIPE_CHUNK / (32 * PIPE_CONSUMER_WARPS);
 constexpr int PIPE_STAGES         = 3;
 constexpr int PIPE_CTAS_PER_SM    = 2;
+constexpr int PIPE_W              = 8; // cells per deposit window
 
 struct PipeStage {
     double  q1[PIPE_CHUNK], vx[PIPE_CHUNK], vy[PIPE_CHUNK], vz[PIPE_CHUNK], w[PIPE_CHUNK];
     double  q1n[PIPE_CHUNK], wn[PIPE_CHUNK]; // position and weight after the move
     int32_t pid[PIPE_CHUNK];
 };
-constexpr size_t PIPE_SMEM = sizeof(PipeStage) * PIPE_STAGES + 2 * PIPE_STAGES * sizeof(uint64_t);
+constexpr size_t PIPE_BAR_OFFSET = sizeof(PipeStage) * PIPE_STAGES;
+constexpr size_t PIPE_COL_OFFSET = PIPE_BAR_OFFSET + 128;
+constexpr size_t PIPE_COL_BYTES  = sizeof(double2) * PIPE_CONSUMER_WARPS * 2 * PIPE_W * 2 * 32;
+constexpr size_t PIPE_SMEM       = PIPE_COL_OFFSET + PIPE_COL_BYTES;
+static_assert(2 * PIPE_STAGES * sizeof(uint64_t) <= 128, "barriers fit before the columns");
 
 __device__ __forceinline__ uint32_t round16(uint32_t b) { return (b + 15u) & ~15u; }
 
@@ -261,156 +193,77 @@ __device__ __forceinline__ double reduce_scatter(double (&x)[V], int lane)
     return v;
 }
 
-// add a warp's register window to the global moments: one atomic per (cell, quantity) and warp
-template <int O, int S, int D>
-__device__ __forceinline__ void flush_rs(Acc<O, S> const &acc, int base, int lane, PushArgs const &a)
-{
-    constexpr int V  = 4 * S <= 16 ? 16 : 32;
-    constexpr int SH = V == 16 ? 1 : 0;
-    static_assert(4 * S <= 32, "window too wide for one reduce-scatter");
-    double x[V];
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-#pragma unroll
-        for (int s = 0; s < S; ++s)
-            x[q * S + s] = acc.v[q][s];
-#pragma unroll
-    for (int k = 4 * S; k < V; ++k)
-        x[k] = 0;
-    double const v  = reduce_scatter<V>(x, lane);
-    int const    vi = lane >> SH;
-    if ((lane & SH) == 0 && vi < 4 * S && v != 0.0) {
-        int const q = vi / S, cell = base + vi % S;
-        if (cell >= -PAD && cell < a.Nx + PAD)
-            atomicAdd(a.dep[D][q] + cell, v);
-        else
-            atomicOr(a.status, ST_OUT_OF_RANGE);
-    }
-}
-
-// A warp's deposit window: register accumulators over cells [base, base + S), S = O + 1 + R,
-// kept across batches and chunks.  When a batch of 32 particles reaches outside the window the
-// warp flushes it and re-bases it at the batch minimum; particles of a batch that spans more than
-// R + 1 stencil bases deposit with direct atomics.
-template <int O, int R, int D>
-struct Window {
-    static constexpr int S    = O + 1 + R;
+// A warp's deposit window of PIPE_W cells from `base`: lane-private columns, for deposit d (at
+// x^N / at the end position) and cell c two double2 {n, nVx}, {nVy, nVz}, lane-contiguous so a
+// warp's access is conflict-free whatever the cells of its lanes.
+struct ColWindow64 {
     static constexpr int NONE = -0x40000000;
-    Acc<O, S> acc;
-    int       base;
+    double2             *col;
+    int                  base;
 
-    __device__ __forceinline__ void init()
+    __device__ __forceinline__ double2 &at(int d, int c, int h, int lane) { return col[((d * PIPE_W + c) * 2 + h) * 32 + lane]; }
+    __device__ __forceinline__ void     zero(int lane)
     {
-        acc_zero(acc);
-        base = NONE;
+#pragma unroll
+        for (int d = 0; d < 2; ++d)
+#pragma unroll
+            for (int c = 0; c < PIPE_W; ++c)
+                at(d, c, 0, lane) = make_double2(0, 0), at(d, c, 1, lane) = make_double2(0, 0);
     }
-    // batch step: i0 is this lane's stencil base (valid lanes only)
-    __device__ __forceinline__ void prepare(bool valid, int i0, int lane, PushArgs const &a)
+    template <int O>
+    __device__ __forceinline__ void add(int d, Shape<O> const &sh, double const (&vw)[4], int lane)
     {
-        bool const outside = valid && (i0 > base + R || i0 < base);
-        if (__any_sync(0xffffffffu, outside)) {
-            if (base != NONE)
-                flush_rs<O, S, D>(acc, base, lane, a);
-            acc_zero(acc);
-            base = __reduce_min_sync(0xffffffffu, valid ? i0 : 0x7fffffff);
+        int const r = sh.i0 - base;
+#pragma unroll
+        for (int j = 0; j <= O; ++j) {
+            double2 &e0 = at(d, r + j, 0, lane);
+            double2 &e1 = at(d, r + j, 1, lane);
+            double2  a0 = e0, a1 = e1;
+            a0.x = fma(vw[0], sh.w[j], a0.x), a0.y = fma(vw[1], sh.w[j], a0.y);
+            a1.x = fma(vw[2], sh.w[j], a1.x), a1.y = fma(vw[3], sh.w[j], a1.y);
+            e0 = a0, e1 = a1;
         }
     }
-    __device__ __forceinline__ void add(Shape<O> const &sh, double w, d3 v, PushArgs const &a)
+    __device__ __forceinline__ void flush_one(int d, int lane, PushArgs const &a)
     {
-        deposit<O, S, D>(acc, base, sh, w, v, a);
+        double x[32];
+#pragma unroll
+        for (int c = 0; c < PIPE_W; ++c) {
+            double2 const u = at(d, c, 0, lane), v = at(d, c, 1, lane);
+            x[4 * c] = u.x, x[4 * c + 1] = u.y, x[4 * c + 2] = v.x, x[4 * c + 3] = v.y;
+            at(d, c, 0, lane) = make_double2(0, 0), at(d, c, 1, lane) = make_double2(0, 0);
+        }
+        double const t = reduce_scatter<32>(x, lane); // lane l: value l = 4 * cell + quantity
+        if (t != 0.0) {
+            int const cell = base + (lane >> 2);
+            if (cell >= -PAD && cell < a.Nx + PAD)
+                atomicAdd(a.dep[d][lane & 3] + cell, t);
+            else
+                atomicOr(a.status, ST_OUT_OF_RANGE);
+        }
     }
-    __device__ __forceinline__ void finish(int lane, PushArgs const &a)
+    __device__ __forceinline__ void flush(int lane, PushArgs const &a)
     {
-        if (base != NONE)
-            flush_rs<O, S, D>(acc, base, lane, a);
+        if (base == NONE)
+            return;
+        if (a.deposit_mask & 1)
+            flush_one(0, lane, a);
+        if (a.deposit_mask & 2)
+            flush_one(1, lane, a);
     }
 };
 
-// In-warp counting sort of a warp's 32 x PIPE_PPT slots of a chunk by stencil base cell, so that
-// each batch of 32 particles handed to a deposit window spans as few cells as possible even after
-// the particles have drifted since the last global sort.  Slot s = k * 32 + lane holds key[s]
-// (INT_MAX for a slot that deposits nothing); order[] receives the slots in key order, stable in
-// (k, lane).  Keys that span more than 31 cells keep the slot order.  Ranks come from
-// __match_any_sync groups whose leaders update a per-warp histogram, so the order is
-// deterministic.
-struct WarpOrder {
-    int      key[32 * PIPE_PPT];
-    uint16_t order[32 * PIPE_PPT];
-    int      hist[32];
-};
-
-__device__ __forceinline__ void warp_order(WarpOrder &W, int lane)
+template <int O>
+__device__ __forceinline__ void deposit_direct(PushArgs const &a, int d, Shape<O> const &sh, double const (&vw)[4])
 {
-    constexpr unsigned FULL = 0xffffffffu;
-    constexpr int      NONE = 0x7fffffff;
-    int                kk[PIPE_PPT];
-    int                lo = NONE, hi = -NONE;
+    atomicAdd(a.fallbacks, 1ull);
 #pragma unroll
-    for (int k = 0; k < PIPE_PPT; ++k) {
-        kk[k] = W.key[k * 32 + lane];
-        if (kk[k] != NONE)
-            lo = min(lo, kk[k]), hi = max(hi, kk[k]);
-    }
-    lo = __reduce_min_sync(FULL, lo);
-    hi = __reduce_max_sync(FULL, hi);
-    if (lo == NONE || hi - lo > 30) {
+    for (int j = 0; j <= O; ++j)
 #pragma unroll
-        for (int k = 0; k < PIPE_PPT; ++k)
-            W.order[k * 32 + lane] = static_cast<uint16_t>(k * 32 + lane);
-        __syncwarp();
-        return;
-    }
-    W.hist[lane] = 0;
-    __syncwarp();
-    unsigned const lt = (1u << lane) - 1u;
-    int            rank[PIPE_PPT], bin[PIPE_PPT];
-#pragma unroll
-    for (int k = 0; k < PIPE_PPT; ++k) {
-        int const      b      = kk[k] == NONE ? 31 : kk[k] - lo;
-        unsigned const m      = __match_any_sync(FULL, b);
-        int const      leader = __ffs(m) - 1;
-        int            old    = 0;
-        if (lane == leader) {
-            old       = W.hist[b];
-            W.hist[b] = old + __popc(m);
-        }
-        old     = __shfl_sync(FULL, old, leader);
-        rank[k] = old + __popc(m & lt);
-        bin[k]  = b;
-        __syncwarp();
-    }
-    int const c   = W.hist[lane];
-    int       inc = c;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        int const y = __shfl_up_sync(FULL, inc, o);
-        if (lane >= o)
-            inc += y;
-    }
-    __syncwarp();
-    W.hist[lane] = inc - c; // exclusive start of each bin
-    __syncwarp();
-#pragma unroll
-    for (int k = 0; k < PIPE_PPT; ++k)
-        W.order[W.hist[bin[k]] + rank[k]] = static_cast<uint16_t>(k * 32 + lane);
-    __syncwarp();
+        for (int q = 0; q < 4; ++q)
+            atomicAdd(a.dep[d][q] + sh.i0 + j, vw[q] * sh.w[j]);
 }
 
-// ------------------------------------------------------------------------------------------------
-// The particle pass.  Warp-specialised pipeline per CTA: one producer warp streams the CTA's
-// contiguous run of chunks (PIPE_CHUNK particles each) global -> shared with 1-D TMA bulk copies
-// completing on mbarriers (PIPE_STAGES deep) and bulk-stores the updated particles back;
-// PIPE_CONSUMER_WARPS warps compute.  A consumer warp owns 32 x PIPE_PPT consecutive
-// (cell-sorted) particles of each chunk and makes passes over them in shared memory: (A) push at
-// x^N, move, boundary, results written beside the inputs; then, in the cell order of warp_order,
-// (B) deposit at x^N and (C) deposit at the new position.  Its two deposit windows persist
-// across the chunks of the run.
-//
-// CAM-CL (move_steps == 1): push at x^N, deposit, move, BC, deposit.
-// Predictor-corrector (move_steps == 2, Domain_PC.cc:110-124, 169-181): half move, BC, push at
-// the half-step position, half move, BC, deposit.  move_steps == 0: deposit only
-// (Domain_PC.cc:36-44).
-// ------------------------------------------------------------------------------------------------
 // The groups of particles one launch of the pass covers: a run's species (one group per launch)
 // or the species of many runs of an ensemble (up to MAXG per launch).  The launch's chunks are
 // numbered consecutively over the groups; a CTA takes a contiguous range of them, and its warps
@@ -439,11 +292,10 @@ __device__ __forceinline__ int group_of(PushGroups<MAXG> const &G, int64_t chunk
 template <int O, bool MIRROR, int BC, int MAXG>
 __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(PushGroups<MAXG> const __grid_constant__ G)
 {
-    constexpr int R = 2;
+    constexpr int SPAN = PIPE_W - 1 - O; // largest stencil base offset inside the window
     extern __shared__ __align__(128) unsigned char smraw[];
-    __shared__ WarpOrder worder[PIPE_CONSUMER_WARPS];
     PipeStage    *stage = reinterpret_cast<PipeStage *>(smraw);
-    uint64_t     *full  = reinterpret_cast<uint64_t *>(smraw + sizeof(PipeStage) * PIPE_STAGES);
+    uint64_t     *full  = reinterpret_cast<uint64_t *>(smraw + PIPE_BAR_OFFSET);
     uint64_t     *empty = full + PIPE_STAGES;
     int const     warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int64_t const nchunks = G.chunk0[G.n];
@@ -510,30 +362,26 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
     }
 
     // ---------------- consumers ----------------
-    unsigned        bad = 0;
-    int             gc  = -1; // current group
-    Window<O, R, 0> win0;
-    Window<O, R, 1> win1;
-    win0.init();
-    win1.init();
+    ColWindow64 win;
+    win.col  = reinterpret_cast<double2 *>(smraw + PIPE_COL_OFFSET) + warp * 2 * PIPE_W * 2 * 32;
+    win.base = ColWindow64::NONE;
+    win.zero(lane);
+    unsigned bad = 0;
+    int      gc  = -1; // current group
     for (int64_t i = 0; i < mine; ++i) {
         int const s  = static_cast<int>(i % PIPE_STAGES);
         int const gi = group_of(G, c0 + i, gc);
-        if (gi != gc) { // entering the next group: settle the previous group's windows and status
+        if (gi != gc) { // entering the next group: settle the previous group's window and status
             if (gc >= 0) {
                 PushArgs const &ap = G.g[gc];
-                if (ap.deposit_mask & 1)
-                    win0.finish(lane, ap);
-                if (ap.deposit_mask & 2)
-                    win1.finish(lane, ap);
+                win.flush(lane, ap);
                 bad = __reduce_or_sync(0xffffffffu, bad);
                 if (bad && lane == 0)
                     atomicOr(ap.status, bad);
                 bad = 0;
-                win0.init();
-                win1.init();
             }
-            gc = gi;
+            win.base = ColWindow64::NONE;
+            gc       = gi;
         }
         PushArgs const &a        = G.g[gc];
         bool const      load_pid = a.randomize != 0;
@@ -545,33 +393,33 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
         int const     cnt   = static_cast<int>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
         PipeStage    &P     = stage[s];
         int const     w0    = warp * 32 * PIPE_PPT;
-        // pass A: push at x^N (half steps around it for PC), move, boundary; no warp collectives,
-        // so the compiler interleaves the independent particles of a lane.  Slots past `cnt` hold
-        // stale finite data and are processed but never deposited or stored.
-#pragma unroll 2
+
+        // slots past `cnt` hold stale finite data and are processed but never deposited or stored
+#pragma unroll
         for (int k = 0; k < PIPE_PPT; ++k) {
-            int const idx   = w0 + k * 32 + lane;
-            double    q1    = P.q1[idx];
-            d3        v     = { P.vx[idx], P.vy[idx], P.vz[idx] };
-            double    w     = P.w[idx];
-            int32_t   pid   = load_pid ? P.pid[idx] : 0;
-            bool      alive = true;
+            int const    idx   = w0 + k * 32 + lane;
+            bool const   live  = idx < cnt;
+            double       q1    = P.q1[idx];
+            d3           v     = { P.vx[idx], P.vy[idx], P.vz[idx] };
+            double       w     = P.w[idx];
+            double const w_in  = w;
+            int32_t      pid   = load_pid ? P.pid[idx] : 0;
+            bool         alive = true;
             if (a.move_steps == 2) {
                 double const moved = move<MIRROR>(a, q1, v.x, 0.5 * a.dt);
-                if (idx < cnt && !(fabs(moved) < 1.0)) // long(moved * scale) != 0 (PartSpecies.cc:261)
+                if (live && !(fabs(moved) < 1.0)) // long(moved * scale) != 0 (PartSpecies.cc:261)
                     bad |= ST_MOVED_TOO_FAR;
                 alive = boundary<BC>(a, q1, v, pid, a.counter);
                 if (!alive)
                     w = 0, q1 = a.full_min + 0.5, v = { 0, 0, 0 };
-                P.q1[idx] = q1; // PC deposits nothing at the push position
             }
-            Shape<O> const sh = make_shape<O>(q1 - a.half_min);
-            bool const     in_grid = finite_pos(q1) && stencil_ok(sh, a.Nx);
-            worder[warp].key[k * 32 + lane] = in_grid && idx < cnt ? sh.i0 : 0x7fffffff;
-            if (in_grid) {
+            Shape<O> const sh0    = make_shape<O>(q1 - a.half_min);
+            bool const     in0    = finite_pos(q1) && stencil_ok(sh0, a.Nx);
+            d3             v_push = v;
+            if (in0) {
                 if (alive && a.move_steps != 0) {
                     d3 E, dB;
-                    interp_EB<O>(a.EB, sh, E, dB);
+                    interp_EB<O>(a.EB, sh0, E, dB);
                     double   c2;
                     d3 const B = background_B<MIRROR>(a, q1, v, c2) + dB;
                     v          = boris_push(a.boris, v, B, E);
@@ -579,27 +427,14 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
                     double moved = (a.inv_D1 * c2) * v.x * (a.move_steps == 2 ? 0.5 * a.dt : a.dt);
                     q1 += moved;
                     moved *= a.travel_scale;
-                    if (idx < cnt && !(fabs(moved) < 1.0))
+                    if (live && !(fabs(moved) < 1.0))
                         bad |= ST_MOVED_TOO_FAR;
-                    d3 const v_push = v;
-                    alive = boundary<BC>(a, q1, v, pid, a.counter + (a.move_steps == 2 ? 1 : 0));
+                    v_push = v;
+                    alive  = boundary<BC>(a, q1, v, pid, a.counter + (a.move_steps == 2 ? 1 : 0));
                     if (!alive)
                         w = 0, q1 = a.full_min + 0.5, v = { 0, 0, 0 };
-                    // the deposit at x^N uses the velocity before the boundary pass: a particle the
-                    // boundary reflected or removed deposits it here and is skipped by pass B
-                    if ((a.deposit_mask & 1) && (v.x != v_push.x || v.y != v_push.y || v.z != v_push.z)) {
-                        if (idx < cnt) {
-                            double const vw[4] = { P.w[idx], v_push.x * P.w[idx], v_push.y * P.w[idx], v_push.z * P.w[idx] };
-#pragma unroll
-                            for (int j = 0; j <= O; ++j)
-#pragma unroll
-                                for (int q = 0; q < 4; ++q)
-                                    atomicAdd(a.dep[0][q] + sh.i0 + j, vw[q] * sh.w[j]);
-                        }
-                        P.q1[idx] = __longlong_as_double(0x7ff8000000000000LL);
-                    }
                 }
-            } else if (idx < cnt) {
+            } else if (live) {
                 bad |= ST_OUT_OF_RANGE;
             }
             P.q1n[idx] = q1;
@@ -608,33 +443,37 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
             P.vz[idx]  = v.z;
             if (BC == BCK_ABSORBING)
                 P.wn[idx] = w;
-        }
-        __syncwarp();
-        warp_order(worder[warp], lane);
-        // pass B: deposit at x^N with v^{N+1/2} (CAM-CL)
-        if (a.deposit_mask & 1) {
-#pragma unroll 1
-            for (int k = 0; k < PIPE_PPT; ++k) {
-                int const      idx   = w0 + worder[warp].order[k * 32 + lane];
-                double const   q1    = P.q1[idx];
-                Shape<O> const sh    = make_shape<O>(q1 - a.half_min);
-                bool const     valid = idx < cnt && finite_pos(q1) && stencil_ok(sh, a.Nx);
-                win0.prepare(valid, sh.i0, lane, a);
-                if (valid)
-                    win0.add(sh, P.w[idx], d3{ P.vx[idx], P.vy[idx], P.vz[idx] }, a);
+
+            // deposits: at x^N with v^{N+1/2} (before the boundary pass) and at the end position
+            Shape<O> const sh1  = make_shape<O>(q1 - a.half_min);
+            bool const     dep0 = live && in0 && (a.deposit_mask & 1);
+            bool const     dep1 = live && (a.deposit_mask & 2) && w != 0.0 && finite_pos(q1) && stencil_ok(sh1, a.Nx);
+            int            lo = 0x7fffffff, hi = -0x7fffffff;
+            if (dep0)
+                lo = min(lo, sh0.i0), hi = max(hi, sh0.i0);
+            if (dep1)
+                lo = min(lo, sh1.i0), hi = max(hi, sh1.i0);
+            bool const outside = (dep0 || dep1) && (lo < win.base || hi > win.base + SPAN);
+            if (__any_sync(0xffffffffu, outside)) { // move the window onto this batch
+                win.flush(lane, a);
+                int const mlo = __reduce_min_sync(0xffffffffu, lo);
+                int const mhi = __reduce_max_sync(0xffffffffu, hi);
+                int const gap = SPAN - (mhi - mlo);
+                win.base      = gap > 0 ? mlo - gap / 2 : mlo;
             }
-        }
-        // pass C: deposit at the end position
-        if (a.deposit_mask & 2) {
-#pragma unroll 1
-            for (int k = 0; k < PIPE_PPT; ++k) {
-                int const      idx   = w0 + worder[warp].order[k * 32 + lane];
-                double const   q1    = P.q1n[idx];
-                Shape<O> const sh    = make_shape<O>(q1 - a.half_min);
-                bool const     valid = idx < cnt && finite_pos(q1) && stencil_ok(sh, a.Nx);
-                win1.prepare(valid, sh.i0, lane, a);
-                if (valid)
-                    win1.add(sh, BC == BCK_ABSORBING ? P.wn[idx] : P.w[idx], d3{ P.vx[idx], P.vy[idx], P.vz[idx] }, a);
+            if (dep0) {
+                double const vw[4] = { w_in, v_push.x * w_in, v_push.y * w_in, v_push.z * w_in };
+                if (sh0.i0 >= win.base && sh0.i0 <= win.base + SPAN)
+                    win.add<O>(0, sh0, vw, lane);
+                else
+                    deposit_direct<O>(a, 0, sh0, vw);
+            }
+            if (dep1) {
+                double const vw[4] = { w, v.x * w, v.y * w, v.z * w };
+                if (sh1.i0 >= win.base && sh1.i0 <= win.base + SPAN)
+                    win.add<O>(1, sh1, vw, lane);
+                else
+                    deposit_direct<O>(a, 1, sh1, vw);
             }
         }
         fence_proxy_async_smem();
@@ -644,15 +483,11 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
     }
     if (gc >= 0) {
         PushArgs const &a = G.g[gc];
-        if (a.deposit_mask & 1)
-            win0.finish(lane, a);
-        if (a.deposit_mask & 2)
-            win1.finish(lane, a);
+        win.flush(lane, a);
         bad = __reduce_or_sync(0xffffffffu, bad);
         if (bad && lane == 0)
             atomicOr(a.status, bad);
     }
 }
-
 
 } // namespace h1d

@@ -2,7 +2,8 @@
 //   - position as an int32 full-grid cell plus an FP32 offset in [0, 1), so the shape weights
 //     come from the in-cell offset and keep ~1e-7 cell resolution anywhere on the grid;
 //   - FP32 velocity, weight, field interpolation, mirror geometry and Boris push;
-//   - FP32 per-warp deposit windows, summed into the FP64 moment arrays per cell.
+//   - FP32 deposits into per-lane shared-memory columns of a per-warp window of cells, summed
+//     into the FP64 moment arrays per cell when the window moves.
 // The field cycle that consumes the moments stays FP64.  Traffic: read cell, offset, v, w
 // (24 B), write cell, offset, v (20 B) per particle-step.
 #pragma once
@@ -96,117 +97,6 @@ __device__ __forceinline__ void sincos_taylor_f(float x, float &s, float &c)
     c              = fmaf(-pc, x2, 1.0f);
 }
 
-template <int O, int S>
-struct AccF {
-    float v[4][S];
-};
-
-template <int O, int S, int R>
-__device__ __forceinline__ void deposit_at_f(AccF<O, S> &acc, ShapeF<O> const &sh, float const (&vw)[4])
-{
-#pragma unroll
-    for (int j = 0; j <= O; ++j)
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-            acc.v[q][R + j] = fmaf(vw[q], sh.w[j], acc.v[q][R + j]);
-}
-
-template <int O, int R, int D>
-struct WindowF {
-    static constexpr int S    = O + 1 + R;
-    static constexpr int NONE = -0x40000000;
-    AccF<O, S> acc;
-    int        base;
-
-    __device__ __forceinline__ void zero()
-    {
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-#pragma unroll
-            for (int s = 0; s < S; ++s)
-                acc.v[q][s] = 0.0f;
-    }
-    __device__ __forceinline__ void init()
-    {
-        zero();
-        base = NONE;
-    }
-    // FP32 reduce-scatter across the warp (recursive halving of V = 16 or 32 values, as
-    // reduce_scatter in particles.cuh), then one FP64 atomic per (cell, quantity)
-    __device__ __forceinline__ void flush(int lane, PushArgsMixed const &a)
-    {
-        constexpr int V  = 4 * S <= 16 ? 16 : 32;
-        constexpr int SH = V == 16 ? 1 : 0;
-        static_assert(4 * S <= 32, "window too wide");
-        float x[V];
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-#pragma unroll
-            for (int s = 0; s < S; ++s)
-                x[q * S + s] = acc.v[q][s];
-#pragma unroll
-        for (int k = 4 * S; k < V; ++k)
-            x[k] = 0.0f;
-#pragma unroll
-        for (int h = V / 2, m = 16; h >= 1; h >>= 1, m >>= 1) {
-            bool const up = (lane & m) != 0;
-#pragma unroll
-            for (int j = 0; j < h; ++j) {
-                float const send = up ? x[j] : x[j + h];
-                float const keep = up ? x[j + h] : x[j];
-                x[j]             = keep + __shfl_xor_sync(0xffffffffu, send, m);
-            }
-        }
-        float v = x[0];
-        if constexpr (V == 16)
-            v += __shfl_xor_sync(0xffffffffu, v, 1);
-        int const vi = lane >> SH;
-        if ((lane & SH) == 0 && vi < 4 * S && v != 0.0f) {
-            int const q = vi / S, cell = base + vi % S;
-            if (cell >= -PAD && cell < a.Nx + PAD)
-                atomicAdd(a.dep[D][q] + cell, static_cast<double>(v));
-            else
-                atomicOr(a.status, ST_OUT_OF_RANGE);
-        }
-    }
-    __device__ __forceinline__ void prepare(bool valid, int i0, int lane, PushArgsMixed const &a)
-    {
-        bool const outside = valid && (i0 > base + R || i0 < base);
-        if (__any_sync(0xffffffffu, outside)) {
-            if (base != NONE)
-                flush(lane, a);
-            zero();
-            base = __reduce_min_sync(0xffffffffu, valid ? i0 : 0x7fffffff);
-        }
-    }
-    __device__ __forceinline__ void add(ShapeF<O> const &sh, float w, f3 v, PushArgsMixed const &a)
-    {
-        float const vw[4] = { w, v.x * w, v.y * w, v.z * w };
-        int const   r     = sh.i0 - base;
-        if (r == 0)
-            deposit_at_f<O, S, 0>(acc, sh, vw);
-        else if (r == 1)
-            deposit_at_f<O, S, 1>(acc, sh, vw);
-        else if (R >= 2 && r == 2)
-            deposit_at_f<O, S, (R >= 2 ? 2 : 0)>(acc, sh, vw);
-        else if (R >= 3 && r == 3)
-            deposit_at_f<O, S, (R >= 3 ? 3 : 0)>(acc, sh, vw);
-        else {
-            atomicAdd(a.fallbacks, 1ull);
-#pragma unroll
-            for (int j = 0; j <= O; ++j)
-#pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    atomicAdd(a.dep[D][q] + sh.i0 + j, static_cast<double>(vw[q] * sh.w[j]));
-        }
-    }
-    __device__ __forceinline__ void finish(int lane, PushArgsMixed const &a)
-    {
-        if (base != NONE)
-            flush(lane, a);
-    }
-};
-
 // move by dq cells (|dq| < 1 is checked by the caller); returns the new (cell, off)
 __device__ __forceinline__ void move_cell(int &cell, float &off, float dq)
 {
@@ -253,16 +143,103 @@ __device__ __forceinline__ bool boundary_mixed(PushArgsMixed const &a, int &cell
     }
 }
 
+// ------------------------------------------------------------------------------------------------
+// The pass.  Same warp-specialised TMA pipeline as push_kernel (particles.cuh) with chunks of
+// MIX_CHUNK particles.  A consumer warp owns 32 x MIX_PPT particles of a chunk and does everything
+// in one loop: push, move, boundary, and both deposits.  Deposits go to a per-warp window of
+// MIX_W cells held in shared memory as lane-private float4 columns {n, nVx, nVy, nVz}: lane l adds
+// its particle to column l of cell (i0 - base + j), so any mix of cells within a warp costs the
+// same (no divergence, no bank conflicts), and lanes never collide.  When a particle's stencil
+// falls outside the window the warp flushes it (per cell and quantity a warp reduce-scatter over
+// the 32 columns, then one FP64 atomic) and re-centres it on the current particles; particles
+// still outside deposit with direct atomics.  The CTA's particles are cell-sorted and contiguous,
+// so the window moves a few times per CTA.
+// ------------------------------------------------------------------------------------------------
+constexpr int MIX_CHUNK = 256;
+constexpr int MIX_PPT   = MIX_CHUNK / (32 * PIPE_CONSUMER_WARPS);
+constexpr int MIX_W     = 8;
+
 struct PipeStageMixed {
-    int32_t cell[PIPE_CHUNK];
-    float   off[PIPE_CHUNK], vx[PIPE_CHUNK], vy[PIPE_CHUNK], vz[PIPE_CHUNK], w[PIPE_CHUNK];
-    int32_t celln[PIPE_CHUNK];
-    float   offn[PIPE_CHUNK], wn[PIPE_CHUNK];
-    int32_t pid[PIPE_CHUNK];
+    int32_t cell[MIX_CHUNK];
+    float   off[MIX_CHUNK], vx[MIX_CHUNK], vy[MIX_CHUNK], vz[MIX_CHUNK], w[MIX_CHUNK];
+    int32_t celln[MIX_CHUNK];
+    float   offn[MIX_CHUNK], wn[MIX_CHUNK];
+    int32_t pid[MIX_CHUNK];
 };
-constexpr int    PIPE_STAGES_MIXED = 3;
+constexpr int    PIPE_STAGES_MIXED      = 3;
 constexpr int    PIPE_CTAS_PER_SM_MIXED = 3;
-constexpr size_t PIPE_SMEM_MIXED   = sizeof(PipeStageMixed) * PIPE_STAGES_MIXED + 2 * PIPE_STAGES_MIXED * sizeof(uint64_t);
+constexpr size_t MIX_BAR_OFFSET         = sizeof(PipeStageMixed) * PIPE_STAGES_MIXED;
+constexpr size_t MIX_COL_OFFSET         = MIX_BAR_OFFSET + 128; // barriers, then 16-byte aligned columns
+constexpr size_t MIX_COL_BYTES          = sizeof(float4) * PIPE_CONSUMER_WARPS * 2 * MIX_W * 32;
+constexpr size_t PIPE_SMEM_MIXED        = MIX_COL_OFFSET + MIX_COL_BYTES;
+static_assert(2 * PIPE_STAGES_MIXED * sizeof(uint64_t) <= 128, "barriers fit before the columns");
+
+// a warp's deposit window: columns [d][c][lane] (d: deposit at x^N / at the end position)
+struct ColWindow {
+    static constexpr int NONE = -0x40000000;
+    float4              *col;
+    int                  base;
+
+    __device__ __forceinline__ float4 &at(int d, int c, int lane) { return col[(d * MIX_W + c) * 32 + lane]; }
+    __device__ __forceinline__ void    zero(int lane)
+    {
+#pragma unroll
+        for (int d = 0; d < 2; ++d)
+#pragma unroll
+            for (int c = 0; c < MIX_W; ++c)
+                at(d, c, lane) = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    template <int O>
+    __device__ __forceinline__ void add(int d, ShapeF<O> const &sh, float4 vw, int lane)
+    {
+        int const r = sh.i0 - base;
+#pragma unroll
+        for (int j = 0; j <= O; ++j) {
+            float4 &e = at(d, r + j, lane);
+            float4  t = e;
+            t.x = fmaf(vw.x, sh.w[j], t.x), t.y = fmaf(vw.y, sh.w[j], t.y);
+            t.z = fmaf(vw.z, sh.w[j], t.z), t.w = fmaf(vw.w, sh.w[j], t.w);
+            e   = t;
+        }
+    }
+    // sum the 32 columns of every (cell, quantity) of deposit d, add to the moments, clear
+    __device__ __forceinline__ void flush_one(int d, int lane, PushArgsMixed const &a)
+    {
+        float x[32];
+#pragma unroll
+        for (int c = 0; c < MIX_W; ++c) {
+            float4 const v = at(d, c, lane);
+            x[4 * c] = v.x, x[4 * c + 1] = v.y, x[4 * c + 2] = v.z, x[4 * c + 3] = v.w;
+            at(d, c, lane) = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int h = 16; h >= 1; h >>= 1) {
+            bool const up = (lane & h) != 0;
+#pragma unroll
+            for (int j = 0; j < h; ++j) {
+                float const send = up ? x[j] : x[j + h];
+                float const keep = up ? x[j + h] : x[j];
+                x[j]             = keep + __shfl_xor_sync(0xffffffffu, send, h);
+            }
+        }
+        if (x[0] != 0.0f) { // lane l holds the total of value l = 4 * cell + quantity
+            int const cell = base + (lane >> 2);
+            if (cell >= -PAD && cell < a.Nx + PAD)
+                atomicAdd(a.dep[d][lane & 3] + cell, static_cast<double>(x[0]));
+            else
+                atomicOr(a.status, ST_OUT_OF_RANGE);
+        }
+    }
+    __device__ __forceinline__ void flush(int lane, PushArgsMixed const &a)
+    {
+        if (base == NONE)
+            return;
+        if (a.deposit_mask & 1)
+            flush_one(0, lane, a);
+        if (a.deposit_mask & 2)
+            flush_one(1, lane, a);
+    }
+};
 
 // the groups of one launch, as PushGroups in particles.cuh
 template <int MAXG>
@@ -285,16 +262,30 @@ __device__ __forceinline__ int group_of(PushGroupsMixed<MAXG> const &G, int64_t 
     }
 }
 
+// direct atomics for a stencil outside the window
+template <int O>
+__device__ __forceinline__ void deposit_direct(PushArgsMixed const &a, int d, ShapeF<O> const &sh, float4 vw)
+{
+    atomicAdd(a.fallbacks, 1ull);
+#pragma unroll
+    for (int j = 0; j <= O; ++j) {
+        double *const p = a.dep[d][0] + sh.i0 + j;
+        atomicAdd(p, static_cast<double>(vw.x * sh.w[j]));
+        atomicAdd(a.dep[d][1] + sh.i0 + j, static_cast<double>(vw.y * sh.w[j]));
+        atomicAdd(a.dep[d][2] + sh.i0 + j, static_cast<double>(vw.z * sh.w[j]));
+        atomicAdd(a.dep[d][3] + sh.i0 + j, static_cast<double>(vw.w * sh.w[j]));
+    }
+}
+
 template <int O, bool MIRROR, int BC, int MAXG>
 __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
     push_kernel_mixed(PushGroupsMixed<MAXG> const __grid_constant__ G)
 {
-    constexpr int   R      = 2;
     constexpr int   STAGES = PIPE_STAGES_MIXED;
+    constexpr int   SPAN   = MIX_W - 1 - O; // largest stencil base offset inside the window
     extern __shared__ __align__(128) unsigned char smraw[];
-    __shared__ WarpOrder worder[PIPE_CONSUMER_WARPS];
     PipeStageMixed *stage = reinterpret_cast<PipeStageMixed *>(smraw);
-    uint64_t       *full  = reinterpret_cast<uint64_t *>(smraw + sizeof(PipeStageMixed) * STAGES);
+    uint64_t       *full  = reinterpret_cast<uint64_t *>(smraw + MIX_BAR_OFFSET);
     uint64_t       *empty = full + STAGES;
     int const       warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int64_t const   nchunks = G.chunk0[G.n];
@@ -325,8 +316,8 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                         break;
                     }
                     if (a.write_back) {
-                        int64_t const  start = (c0 + j - G.chunk0[gr]) * PIPE_CHUNK;
-                        uint32_t const cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
+                        int64_t const  start = (c0 + j - G.chunk0[gr]) * MIX_CHUNK;
+                        uint32_t const cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(MIX_CHUNK), a.n - start));
                         uint32_t const b4    = round16(cnt * 4);
                         bulk_store(a.cell + start, stage[s].celln, b4);
                         bulk_store(a.off + start, stage[s].offn, b4);
@@ -343,8 +334,8 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                     gl                     = group_of(G, c0 + i, gl);
                     PushArgsMixed const &a = G.g[gl];
                     bool const     lpid  = a.randomize != 0;
-                    int64_t const  start = (c0 + i - G.chunk0[gl]) * PIPE_CHUNK;
-                    uint32_t const cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
+                    int64_t const  start = (c0 + i - G.chunk0[gl]) * MIX_CHUNK;
+                    uint32_t const cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(MIX_CHUNK), a.n - start));
                     uint32_t const b4    = round16(cnt * 4);
                     mbar_arrive_expect_tx(&full[s], (6 + (lpid ? 1 : 0)) * b4);
                     bulk_load(stage[s].cell, a.cell + start, b4, &full[s]);
@@ -362,30 +353,27 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
         return;
     }
 
-    unsigned         bad = 0;
-    int              gc  = -1;
-    WindowF<O, R, 0> win0;
-    WindowF<O, R, 1> win1;
-    win0.init();
-    win1.init();
+    // ---------------- consumers ----------------
+    ColWindow win;
+    win.col  = reinterpret_cast<float4 *>(smraw + MIX_COL_OFFSET) + warp * 2 * MIX_W * 32;
+    win.base = ColWindow::NONE;
+    win.zero(lane);
+    unsigned bad = 0;
+    int      gc  = -1;
     for (int64_t i = 0; i < mine; ++i) {
         int const s  = static_cast<int>(i % STAGES);
         int const gi = group_of(G, c0 + i, gc);
-        if (gi != gc) {
+        if (gi != gc) { // entering the next group: settle the previous group's window and status
             if (gc >= 0) {
                 PushArgsMixed const &ap = G.g[gc];
-                if (ap.deposit_mask & 1)
-                    win0.finish(lane, ap);
-                if (ap.deposit_mask & 2)
-                    win1.finish(lane, ap);
+                win.flush(lane, ap);
                 bad = __reduce_or_sync(0xffffffffu, bad);
                 if (bad && lane == 0)
                     atomicOr(ap.status, bad);
                 bad = 0;
-                win0.init();
-                win1.init();
             }
-            gc = gi;
+            win.base = ColWindow::NONE;
+            gc       = gi;
         }
         PushArgsMixed const &a        = G.g[gc];
         bool const           load_pid = a.randomize != 0;
@@ -393,48 +381,49 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
             bad |= ST_TIMEOUT;
             break;
         }
-        int64_t const   start = (c0 + i - G.chunk0[gc]) * PIPE_CHUNK;
-        int const       cnt   = static_cast<int>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
+        int64_t const   start = (c0 + i - G.chunk0[gc]) * MIX_CHUNK;
+        int const       cnt   = static_cast<int>(min(static_cast<int64_t>(MIX_CHUNK), a.n - start));
         PipeStageMixed &P     = stage[s];
-        int const       w0    = warp * 32 * PIPE_PPT;
-        // pass A: push, move, boundary (FP32)
-#pragma unroll 2
-        for (int k = 0; k < PIPE_PPT; ++k) {
+        int const       w0    = warp * 32 * MIX_PPT;
+
+#pragma unroll
+        for (int k = 0; k < MIX_PPT; ++k) {
             int const idx   = w0 + k * 32 + lane;
+            bool const live = idx < cnt; // slots past cnt hold stale data: pushed, never stored or deposited
             int       cell  = P.cell[idx];
             float     off   = P.off[idx];
             f3        v     = { P.vx[idx], P.vy[idx], P.vz[idx] };
             float     w     = P.w[idx];
+            float const w_in = w;
             int32_t   pid   = load_pid ? P.pid[idx] : 0;
             bool      alive = true;
-            if (a.move_steps == 2) {
+            if (a.move_steps == 2) { // predictor-corrector: half move and boundary before the push
                 float dq = a.inv_D1 * v.x * (0.5f * a.dt);
                 if constexpr (MIRROR) {
                     float s_, c_;
                     sincos_taylor_f(a.xiD1 * (static_cast<float>(cell) + a.full_min + off), s_, c_);
                     dq *= c_ * c_;
                 }
-                if (idx < cnt && !(fabsf(dq * a.travel_scale) < 1.0f))
+                if (live && !(fabsf(dq * a.travel_scale) < 1.0f))
                     bad |= ST_MOVED_TOO_FAR;
                 move_cell(cell, off, dq);
                 alive = boundary_mixed<BC>(a, cell, off, v, pid, a.counter);
                 if (!alive)
                     w = 0.0f, cell = 0, off = 0.5f, v = { 0, 0, 0 };
-                P.cell[idx] = cell, P.off[idx] = off;
             }
-            ShapeF<O> const sh      = make_shape_f<O>(cell, off);
-            bool const      in_grid = stencil_ok_f(sh, a.Nx);
-            worder[warp].key[k * 32 + lane] = in_grid && idx < cnt ? sh.i0 : 0x7fffffff;
-            if (in_grid) {
+            ShapeF<O> const sh0    = make_shape_f<O>(cell, off);
+            bool const      in0    = stencil_ok_f(sh0, a.Nx);
+            f3              v_push = v;
+            if (in0) {
                 if (alive && a.move_steps != 0) {
                     f3 E = { 0, 0, 0 }, dB = { 0, 0, 0 };
 #pragma unroll
                     for (int j = 0; j <= O; ++j) {
-                        float const *p  = a.EB + 6 * (sh.i0 + j);
+                        float const *p  = a.EB + 6 * (sh0.i0 + j);
                         float2 const x0 = __ldg(reinterpret_cast<float2 const *>(p));
                         float2 const x1 = __ldg(reinterpret_cast<float2 const *>(p + 2));
                         float2 const x2 = __ldg(reinterpret_cast<float2 const *>(p + 4));
-                        float const  wj = sh.w[j];
+                        float const  wj = sh0.w[j];
                         E.x += x0.x * wj, E.y += x0.y * wj, E.z += x1.x * wj;
                         dB.x += x1.y * wj, dB.y += x2.x * wj, dB.z += x2.y * wj;
                     }
@@ -456,27 +445,15 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                     float const sb = 2.0f * __frcp_rn(1.0f + (B.x * B.x + B.y * B.y + B.z * B.z));
                     v              = v + crossf(u, B * sb) + E;
                     float const dq = (a.inv_D1 * c2) * v.x * (a.move_steps == 2 ? 0.5f * a.dt : a.dt);
-                    if (idx < cnt && !(fabsf(dq * a.travel_scale) < 1.0f))
+                    if (live && !(fabsf(dq * a.travel_scale) < 1.0f))
                         bad |= ST_MOVED_TOO_FAR;
-                    f3 const v_push = v;
+                    v_push = v;
                     move_cell(cell, off, dq);
                     alive = boundary_mixed<BC>(a, cell, off, v, pid, a.counter + (a.move_steps == 2 ? 1 : 0));
                     if (!alive)
                         w = 0.0f, cell = 0, off = 0.5f, v = { 0, 0, 0 };
-                    if ((a.deposit_mask & 1) && (v.x != v_push.x || v.y != v_push.y || v.z != v_push.z)) {
-                        if (idx < cnt) { // deposit at x^N with the pre-boundary velocity
-                            float const wv    = P.w[idx];
-                            float const vw[4] = { wv, v_push.x * wv, v_push.y * wv, v_push.z * wv };
-#pragma unroll
-                            for (int j = 0; j <= O; ++j)
-#pragma unroll
-                                for (int q = 0; q < 4; ++q)
-                                    atomicAdd(a.dep[0][q] + sh.i0 + j, static_cast<double>(vw[q] * sh.w[j]));
-                        }
-                        P.cell[idx] = -0x40000000; // skipped by pass B
-                    }
                 }
-            } else if (idx < cnt) {
+            } else if (live) {
                 bad |= ST_OUT_OF_RANGE;
             }
             P.celln[idx] = cell;
@@ -486,29 +463,37 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
             P.vz[idx]    = v.z;
             if (BC == BCK_ABSORBING)
                 P.wn[idx] = w;
-        }
-        __syncwarp();
-        warp_order(worder[warp], lane);
-        if (a.deposit_mask & 1) {
-#pragma unroll 1
-            for (int k = 0; k < PIPE_PPT; ++k) {
-                int const       idx   = w0 + worder[warp].order[k * 32 + lane];
-                ShapeF<O> const sh    = make_shape_f<O>(P.cell[idx], P.off[idx]);
-                bool const      valid = idx < cnt && stencil_ok_f(sh, a.Nx);
-                win0.prepare(valid, sh.i0, lane, a);
-                if (valid)
-                    win0.add(sh, P.w[idx], f3{ P.vx[idx], P.vy[idx], P.vz[idx] }, a);
+
+            // deposits: at x^N with v^{N+1/2} (before the boundary pass) and at the end position
+            ShapeF<O> const sh1  = make_shape_f<O>(cell, off);
+            bool const      dep0 = live && in0 && (a.deposit_mask & 1);
+            bool const      dep1 = live && (a.deposit_mask & 2) && w != 0.0f && stencil_ok_f(sh1, a.Nx);
+            int             lo = 0x7fffffff, hi = -0x7fffffff;
+            if (dep0)
+                lo = min(lo, sh0.i0), hi = max(hi, sh0.i0);
+            if (dep1)
+                lo = min(lo, sh1.i0), hi = max(hi, sh1.i0);
+            bool const outside = (dep0 || dep1) && (lo < win.base || hi > win.base + SPAN);
+            if (__any_sync(0xffffffffu, outside)) { // move the window onto this batch
+                win.flush(lane, a);
+                int const mlo = __reduce_min_sync(0xffffffffu, lo);
+                int const mhi = __reduce_max_sync(0xffffffffu, hi);
+                int const gap = SPAN - (mhi - mlo);
+                win.base      = gap > 0 ? mlo - gap / 2 : mlo;
             }
-        }
-        if (a.deposit_mask & 2) {
-#pragma unroll 1
-            for (int k = 0; k < PIPE_PPT; ++k) {
-                int const       idx   = w0 + worder[warp].order[k * 32 + lane];
-                ShapeF<O> const sh    = make_shape_f<O>(P.celln[idx], P.offn[idx]);
-                bool const      valid = idx < cnt && stencil_ok_f(sh, a.Nx);
-                win1.prepare(valid, sh.i0, lane, a);
-                if (valid)
-                    win1.add(sh, BC == BCK_ABSORBING ? P.wn[idx] : P.w[idx], f3{ P.vx[idx], P.vy[idx], P.vz[idx] }, a);
+            if (dep0) {
+                float4 const vw = make_float4(w_in, v_push.x * w_in, v_push.y * w_in, v_push.z * w_in);
+                if (sh0.i0 >= win.base && sh0.i0 <= win.base + SPAN)
+                    win.add<O>(0, sh0, vw, lane);
+                else
+                    deposit_direct<O>(a, 0, sh0, vw);
+            }
+            if (dep1) {
+                float4 const vw = make_float4(w, v.x * w, v.y * w, v.z * w);
+                if (sh1.i0 >= win.base && sh1.i0 <= win.base + SPAN)
+                    win.add<O>(1, sh1, vw, lane);
+                else
+                    deposit_direct<O>(a, 1, sh1, vw);
             }
         }
         fence_proxy_async_smem();
@@ -518,15 +503,11 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
     }
     if (gc >= 0) {
         PushArgsMixed const &a = G.g[gc];
-        if (a.deposit_mask & 1)
-            win0.finish(lane, a);
-        if (a.deposit_mask & 2)
-            win1.finish(lane, a);
+        win.flush(lane, a);
         bad = __reduce_or_sync(0xffffffffu, bad);
         if (bad && lane == 0)
             atomicOr(a.status, bad);
     }
 }
-
 
 } // namespace h1d

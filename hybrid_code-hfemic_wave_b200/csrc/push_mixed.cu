@@ -78,7 +78,7 @@ cudaError_t set_smem_once()
     return e;
 }
 
-inline int64_t chunks_of(int64_t n) { return (n + PIPE_CHUNK - 1) / PIPE_CHUNK; }
+inline int64_t chunks_of(int64_t n) { return (n + MIX_CHUNK - 1) / MIX_CHUNK; }
 
 template <class ArgsT, template <int> class GroupsT>
 cudaError_t launch_groups(ArgsT const *args, int n, int order, bool mirror, int bc, int max_ctas, cudaStream_t st)
