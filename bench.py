@@ -231,6 +231,16 @@ class TimedRun:
         self.run._check(self.lib.h1d_advance_async(self.run.h, n))
         self.run._check(self.lib.h1d_synchronize(self.run.h))
 
+    def warm(self, n, autotune=True):
+        """n plain warm-up steps, then (CAM-CL runs) the library's autotuner, which advances the run
+        by real steps while it picks the sort interval and CTA count kept for the timed steps."""
+        self.advance(n)
+        self.tuned = None
+        if autotune and self.cfg.algorithm == self.h.configs.ALGO_CAMCL:
+            steps, k, c = self.h.abi.autotune(self.run)
+            self.tuned = {"steps": steps, "sort_interval": k, "ctas_per_sm": c}
+        return self.tuned
+
     def timed(self, steps, world=1, clocks_index=None):
         """Device time (ms) of `steps` steps, max over ranks, with the library's phase profile."""
         import ctypes
@@ -482,8 +492,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the fp64 / error / drop-in side measurements")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the ensemble and serving measurements")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the library's default sort interval and CTAs")
     args = ap.parse_args()
     assert args.warmup >= 3 or args.impl == "reference", "at least 3 warm-up steps"
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:  # replicas: each rank measures the headline only
+        args.no_extras = args.no_ensemble = True
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -510,7 +523,7 @@ def main():
     traffic = load_traffic()
 
     tr = TimedRun(h, cfg, st)
-    tr.advance(args.warmup)
+    tuned = tr.warm(args.warmup, autotune=not args.no_autotune)
     ms, prof, clocks = tr.timed(args.steps, world, clocks_index=local)
     n_particles = tr.n_particles
     tr.close()
@@ -523,11 +536,11 @@ def main():
     if not args.no_extras:
         if prec == "mixed":
             t64 = TimedRun(h, cfg.replace(precision=h.configs.PREC_FP64), st)
-            t64.advance(args.warmup)
+            tuned64 = t64.warm(args.warmup, autotune=not args.no_autotune)
             ms64, prof64, _ = t64.timed(args.steps, world)
             t64.close()
             v64 = n_particles * args.steps * world / (ms64 / 1e3)
-            extras["fp64"] = {"value": v64, "unit": METRIC, "ms_per_step": ms64 / args.steps,
+            extras["fp64"] = {"value": v64, "unit": METRIC, "ms_per_step": ms64 / args.steps, "autotune": tuned64,
                               "roofline": roofline_of(prof64, "fp64", args.steps, traffic)}
             extras["mixed_over_fp64"] = value / v64
             extras["error_vs_fp64"] = error_vs_fp64(h, cfg, st)
@@ -535,12 +548,13 @@ def main():
             c2 = h.configs.config2()
             st2 = initial_state(c2, seed=2000 + rank)
             t2 = TimedRun(h, c2, st2)
-            t2.advance(args.warmup)
+            tuned2 = t2.warm(args.warmup, autotune=not args.no_autotune)
             k2 = max(args.steps, 100)
             ms2, prof2, _ = t2.timed(k2, world)
             v2 = t2.n_particles * k2 * world / (ms2 / 1e3)
             t2.close()
             extras["drop_in_fp64"] = {"workload": c2.name, "particles_per_gpu": t2.n_particles, "value": v2,
+                                      "autotune": tuned2,
                                       "unit": METRIC, "ms_per_step": ms2 / k2,
                                       "roofline": roofline_of(prof2, "fp64", k2, traffic)}
             del st2
@@ -573,7 +587,9 @@ def main():
                    "algorithm": "CAM-CL" if cfg.algorithm == h.configs.ALGO_CAMCL else "PC",
                    "n_subcycles": cfg.n_subcycles, "precision": prec,
                    "l2": f"particle state ({state_mb:.0f} MB per GPU, one buffer set) larger than L2; no flush",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}",
+                   "autotune": tuned,
+                   "warmup_note": "W plain warm-up steps, then the autotuner's own (real) steps, both untimed"},
         "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": int(prof.kernel_launches),
         **extras,

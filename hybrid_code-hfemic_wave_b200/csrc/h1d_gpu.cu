@@ -1669,7 +1669,7 @@ int h1d_batch_get_stream(h1d_batch *b, void **stream)
 int h1d_batch_configure(h1d_batch *b, int sort_interval, int push_ctas_per_sm, int use_graphs)
 {
     if (!b || sort_interval < 0 || sort_interval > 4096 || push_ctas_per_sm < 0 || push_ctas_per_sm > PIPE_CTAS_PER_SM_MIXED)
-        return bset_err(b, H1D_ERR_INVALID_ARG, "h1d_batch_configure: sort_interval in [0, 4096], CTAs per SM in [0, 3]");
+        return bset_err(b, H1D_ERR_INVALID_ARG, "h1d_batch_configure: sort_interval in [0, 4096], CTAs per SM in [0, 4]");
     if (sort_interval > 0 && sort_interval != b->k)
         b->k = sort_interval, b->since_block = 1 << 30;
     b->ctas       = push_ctas_per_sm;
@@ -1746,7 +1746,7 @@ char const *h1d_batch_status_string(h1d_batch *b) { return b ? b->msg.c_str() : 
 int h1d_configure(h1d_run *run, int sort_interval, int push_ctas_per_sm)
 {
     if (!run || sort_interval < 0 || sort_interval > 4096 || push_ctas_per_sm < 0 || push_ctas_per_sm > PIPE_CTAS_PER_SM_MIXED)
-        return set_err(run, H1D_ERR_INVALID_ARG, "h1d_configure: sort_interval in [0, 4096], CTAs per SM in [0, 3]");
+        return set_err(run, H1D_ERR_INVALID_ARG, "h1d_configure: sort_interval in [0, 4096], CTAs per SM in [0, 4]");
     if (sort_interval > 0)
         run->sort_interval = sort_interval;
     run->ctas_per_sm = push_ctas_per_sm;

@@ -155,7 +155,8 @@ constexpr int PIPE_CHUNK          = 256;
 constexpr int PIPE_PPT            = PIPE_CHUNK / (32 * PIPE_CONSUMER_WARPS);
 constexpr int PIPE_STAGES         = 3;
 constexpr int PIPE_CTAS_PER_SM    = 2;
-constexpr int PIPE_W              = 8; // cells per deposit window
+constexpr int PIPE_W              = 8; // cells per deposit window: 4 quantities x 8 cells = the 32 lanes of a flush
+static_assert(4 * PIPE_W == 32, "a window flush reduce-scatters exactly 32 values");
 
 struct PipeStage {
     double  q1[PIPE_CHUNK], vx[PIPE_CHUNK], vy[PIPE_CHUNK], vz[PIPE_CHUNK], w[PIPE_CHUNK];

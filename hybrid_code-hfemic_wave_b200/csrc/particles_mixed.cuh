@@ -157,7 +157,8 @@ __device__ __forceinline__ bool boundary_mixed(PushArgsMixed const &a, int &cell
 // ------------------------------------------------------------------------------------------------
 constexpr int MIX_CHUNK = 256;
 constexpr int MIX_PPT   = MIX_CHUNK / (32 * PIPE_CONSUMER_WARPS);
-constexpr int MIX_W     = 8;
+constexpr int MIX_W     = 8; // 4 quantities x 8 cells = the 32 lanes of a flush
+static_assert(4 * MIX_W == 32, "a window flush reduce-scatters exactly 32 values");
 
 struct PipeStageMixed {
     int32_t cell[MIX_CHUNK];
@@ -166,8 +167,8 @@ struct PipeStageMixed {
     float   offn[MIX_CHUNK], wn[MIX_CHUNK];
     int32_t pid[MIX_CHUNK];
 };
-constexpr int    PIPE_STAGES_MIXED      = 3;
-constexpr int    PIPE_CTAS_PER_SM_MIXED = 3;
+constexpr int    PIPE_STAGES_MIXED      = 2;
+constexpr int    PIPE_CTAS_PER_SM_MIXED = 4;
 constexpr size_t MIX_BAR_OFFSET         = sizeof(PipeStageMixed) * PIPE_STAGES_MIXED;
 constexpr size_t MIX_COL_OFFSET         = MIX_BAR_OFFSET + 128; // barriers, then 16-byte aligned columns
 constexpr size_t MIX_COL_BYTES          = sizeof(float4) * PIPE_CONSUMER_WARPS * 2 * MIX_W * 32;
