@@ -201,6 +201,21 @@ def run_reference_arm(args, h, rank):
     print(json.dumps(line))
 
 
+def reduce_over_ranks(seconds, units, device="cuda"):
+    """Whole-job figures of a replicated measurement: the time is the max over ranks and the
+    work the sum over ranks (torch.distributed, any backend; the identity on one process)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(seconds), float(units)
+    t = torch.tensor([float(seconds)], dtype=torch.float64, device=device)
+    u = torch.tensor([float(units)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(u.item())
+
+
 def precision_name(cfg, h):
     return "mixed" if cfg.precision == h.configs.PREC_MIXED else "fp64"
 
@@ -271,9 +286,7 @@ class TimedRun:
         r._check(lib.h1d_profile_read(r.h, ctypes.byref(prof)))
         r._check(lib.h1d_profile_enable(r.h, 0))
         if world > 1:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+            ms, _ = reduce_over_ranks(ms, 0.0)
             dist.barrier()
         return ms, prof, (clk.summary() if clk else None)
 
@@ -383,9 +396,7 @@ def e2e_measure(h, cfg, st, K, world):
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
     if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        e2e_s, _ = reduce_over_ranks(e2e_s, 0.0)
     h2d = sum(p["q1"].nbytes * 5 for p in st["particles"]) + st["B"].nbytes + st["E"].nbytes
     return {"value": n_particles * K * world / e2e_s, "unit": METRIC, "h2d_bytes_per_step": h2d / K,
             "d2h_bytes_per_step": d2h / K,
