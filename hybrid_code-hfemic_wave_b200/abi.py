@@ -519,3 +519,61 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+# ---------------------------------------------------------------------------------------------
+# checkpoint / resume (h1d_checkpoint_*) and velocity histograms (h1d_vhistogram)
+# ---------------------------------------------------------------------------------------------
+
+def _declare_ckpt(lib):
+    v, sz = C.c_void_p, C.c_size_t
+    spec = {
+        "h1d_checkpoint_size": ([v, C.POINTER(sz)], C.c_int),
+        "h1d_checkpoint_save": ([v, v, sz, C.POINTER(sz)], C.c_int),
+        "h1d_checkpoint_load": ([v, v, sz], C.c_int),
+        "h1d_step_count": ([v, C.POINTER(C.c_int64)], C.c_int),
+    }
+    for name, (args, res) in spec.items():
+        fn = getattr(lib, name)
+        fn.argtypes, fn.restype = args, res
+    return lib
+
+
+def checkpoint(run: Run) -> bytes:
+    """The run's state as a byte image (h1d_checkpoint_save)."""
+    lib = _declare_ckpt(run.lib)
+    n = C.c_size_t()
+    run._check(lib.h1d_checkpoint_size(run.h, C.byref(n)))
+    buf = C.create_string_buffer(n.value)
+    w = C.c_size_t()
+    run._check(lib.h1d_checkpoint_save(run.h, buf, n.value, C.byref(w)))
+    return buf.raw[:w.value]
+
+
+def restore(run: Run, image: bytes):
+    """Resume the run from a byte image of a run with the same parameters (h1d_checkpoint_load)."""
+    lib = _declare_ckpt(run.lib)
+    run._check(lib.h1d_checkpoint_load(run.h, image, len(image)))
+
+
+def step_count(run: Run) -> int:
+    lib = _declare_ckpt(run.lib)
+    n = C.c_int64()
+    run._check(lib.h1d_step_count(run.h, C.byref(n)))
+    return n.value
+
+
+def vhistogram(run: Run, s: int, extent, v1, v2, prefix: str = "h1d_"):
+    """VHistogramRecorder of kinetic species s: extent = (loc, len) in q1, v1 = (min, len, bins)
+    for the parallel and v2 = (min, len, bins) for the perpendicular speed.  Returns (hist, total)
+    with hist[i1, i2] = (marker count, weight, real_f/marker) / total.  Works on either library
+    (h1d_ or the oracle's orc_ prefix)."""
+    fn = getattr(run.lib, prefix + "vhistogram")
+    fn.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int64, C.c_double,
+                   C.c_double, C.c_int64, _dp, C.POINTER(C.c_int64)]
+    fn.restype = C.c_int
+    out = np.empty((int(v1[2]), int(v2[2]), 3))
+    tot = C.c_int64()
+    run._check(fn(run.h, s, extent[0], extent[1], v1[0], v1[1], int(v1[2]), v2[0], v2[1], int(v2[2]), _ptr(out),
+                  C.byref(tot)))
+    return out, tot.value

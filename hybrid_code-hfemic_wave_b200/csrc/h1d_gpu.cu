@@ -1769,6 +1769,53 @@ int h1d_autotune(h1d_run *run, uint32_t *steps_taken, int *sort_interval, int *p
     return st;
 }
 
+
+int h1d_vhistogram(h1d_run *run, int s, double ext_loc, double ext_len, double v1min, double v1len, int64_t v1dim,
+                   double v2min, double v2len, int64_t v2dim, double *out, int64_t *total)
+{
+    if (!run || s < 0 || s >= run->p.n_kinetic || v1dim <= 0 || v2dim <= 0 || v1dim * v2dim > (int64_t{ 1 } << 24)
+        || !(v1len > 0) || !(v2len > 0) || !out)
+        return set_err(run, H1D_ERR_INVALID_ARG, "h1d_vhistogram: bad arguments");
+    TRY(finalize_moments(run));
+    SpeciesState const &S    = run->sp[s];
+    size_t const        bins = static_cast<size_t>(v1dim * v2dim);
+    double             *d    = nullptr;
+    CU(cudaMalloc(&d, sizeof(double) * (3 * bins + 1)));
+    auto *count = reinterpret_cast<unsigned long long *>(d + 3 * bins);
+    int   st    = H1D_OK;
+    if (cudaMemsetAsync(d, 0, sizeof(double) * (3 * bins + 1), run->stream) != cudaSuccess)
+        st = set_err(run, H1D_ERR_CUDA, "h1d_vhistogram: memset failed");
+    if (st == H1D_OK && S.n > 0) {
+        VHistArgs a{};
+        if (run->mixed)
+            a.cell = S.cell[S.cur], a.off = S.fbuf[S.cur][0], a.fvx = S.fbuf[S.cur][1], a.fvy = S.fbuf[S.cur][2],
+            a.fvz = S.fbuf[S.cur][3], a.fw = S.fbuf[S.cur][4];
+        else
+            a.q1 = S.buf[S.cur][0], a.vx = S.buf[S.cur][1], a.vy = S.buf[S.cur][2], a.vz = S.buf[S.cur][3],
+            a.w = S.buf[S.cur][4];
+        a.n = S.n, a.full_min = -0.5 * run->Nx, a.half_min = a.full_min + 0.5;
+        a.ext_lo = ext_loc, a.ext_hi = ext_loc + ext_len, a.v1min = v1min, a.v1len = v1len, a.v2min = v2min, a.v2len = v2len;
+        a.v1dim = static_cast<int>(v1dim), a.v2dim = static_cast<int>(v2dim);
+        a.mom = S.mom, a.M = run->M, a.out = d, a.count = count;
+        vhist_kernel<<<static_cast<unsigned>((S.n + 255) / 256), 256, 0, run->stream>>>(a);
+        if (cudaGetLastError() != cudaSuccess)
+            st = set_err(run, H1D_ERR_CUDA, "h1d_vhistogram: launch failed");
+    }
+    std::vector<double> h(3 * bins + 1);
+    if (st == H1D_OK && (cudaMemcpyAsync(h.data(), d, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, run->stream) != cudaSuccess
+                         || cudaStreamSynchronize(run->stream) != cudaSuccess))
+        st = set_err(run, H1D_ERR_CUDA, "h1d_vhistogram: copy failed");
+    cudaFree(d);
+    TRY(st);
+    unsigned long long c = 0;
+    std::memcpy(&c, &h[3 * bins], sizeof c);
+    for (size_t i = 0; i < 3 * bins; ++i)
+        out[i] = c ? h[i] / static_cast<double>(c) : 0.0;
+    if (total)
+        *total = static_cast<int64_t>(c);
+    return H1D_OK;
+}
+
 int h1d_energy(h1d_run *run, double *dB2O2, double *dE2O2, double *KE_lab, double *KE_pla)
 {
     if (!run || !dB2O2 || !dE2O2 || !KE_lab || !KE_pla)
@@ -2169,6 +2216,187 @@ int h1d_server_destroy(h1d_server *sv)
         delete r;
     }
     delete sv;
+    return H1D_OK;
+}
+
+} // extern "C"
+
+// ---- checkpoint / resume ------------------------------------------------------------------------
+// The content of the reference's snapshot (Recorder/Snapshot.cc:148-185, 330-375): step count, a
+// signature of the parameters (Hash{serialize(params)}, Snapshot.cc:19, 340-342), B and E, the
+// particles of every kinetic species (here with their ids, in the run's own precision so that a
+// resume is exact) and mom0_full / mom1_full of every cold species.  Sources and the push record
+// are recomputed on the first step after a resume, as after the reference's snapshot load.
+
+namespace {
+
+struct CkptHeader {
+    char     magic[8];
+    uint32_t version, precision;
+    uint64_t signature;
+    int64_t  step, Nx;
+    int32_t  n_kinetic, n_cold;
+    int64_t  n[H1D_MAX_KINETIC];
+};
+constexpr char     CKPT_MAGIC[8] = { 'H', '1', 'D', 'C', 'K', 'P', 'T', 0 };
+constexpr uint32_t CKPT_VERSION  = 1;
+
+// FNV-1a over the run's parameters with the tuning knob (sort interval) cleared
+uint64_t params_signature(h1d_params p)
+{
+    p.sort_interval = 0;
+    unsigned char const *b = reinterpret_cast<unsigned char const *>(&p);
+    uint64_t             h = 1469598103934665603ULL;
+    for (size_t i = 0; i < sizeof p; ++i)
+        h = (h ^ b[i]) * 1099511628211ULL;
+    return h;
+}
+
+size_t particle_bytes(h1d_run const *run, int64_t n)
+{
+    return static_cast<size_t>(n) * (run->mixed ? 6 * 4 + 4 : 5 * 8 + 4);
+}
+
+size_t ckpt_size(h1d_run const *run)
+{
+    size_t b = sizeof(CkptHeader) + sizeof(double) * 6 * run->M + sizeof(double) * 4 * run->M * run->p.n_cold;
+    for (int s = 0; s < run->p.n_kinetic; ++s)
+        b += particle_bytes(run, run->sp[s].n);
+    return b;
+}
+
+} // namespace
+
+extern "C" {
+
+int h1d_checkpoint_size(h1d_run *run, size_t *bytes)
+{
+    if (!run || !bytes)
+        return H1D_ERR_INVALID_ARG;
+    for (int s = 0; s < run->p.n_kinetic; ++s) { // exact counts (absorbed particles trimmed)
+        int64_t n = 0;
+        TRY(h1d_particle_count(run, s, &n));
+    }
+    *bytes = ckpt_size(run);
+    return H1D_OK;
+}
+
+int h1d_checkpoint_save(h1d_run *run, void *buffer, size_t capacity, size_t *written)
+{
+    size_t need = 0;
+    TRY(h1d_checkpoint_size(run, &need));
+    if (!buffer || capacity < need)
+        return set_err(run, H1D_ERR_INVALID_ARG, fmt("h1d_checkpoint_save: the buffer needs %zu bytes", need));
+    if (run->fields_dirty)
+        TRY(prepare_fields(run)); // ghost cells as the first step would fill them
+    CkptHeader hd{};
+    std::memcpy(hd.magic, CKPT_MAGIC, sizeof hd.magic);
+    hd.version = CKPT_VERSION, hd.precision = static_cast<uint32_t>(run->p.precision);
+    hd.signature = params_signature(run->p), hd.step = run->step, hd.Nx = run->Nx;
+    hd.n_kinetic = run->p.n_kinetic, hd.n_cold = run->p.n_cold;
+    for (int s = 0; s < run->p.n_kinetic; ++s)
+        hd.n[s] = run->sp[s].n;
+    auto *out = static_cast<unsigned char *>(buffer);
+    std::memcpy(out, &hd, sizeof hd);
+    size_t off = sizeof hd;
+    auto   d2h = [&](void const *src, size_t bytes) -> cudaError_t {
+        cudaError_t const e = bytes ? cudaMemcpyAsync(out + off, src, bytes, cudaMemcpyDeviceToHost, run->stream) : cudaSuccess;
+        off += bytes;
+        return e;
+    };
+    long const M = run->M;
+    CU(d2h(run->B[run->fcur], sizeof(double) * 3 * M));
+    CU(d2h(run->E[run->fcur], sizeof(double) * 3 * M));
+    for (int c = 0; c < run->p.n_cold; ++c) {
+        CU(d2h(run->cold[c].n, sizeof(double) * M));
+        CU(d2h(run->cold[c].nV[run->cold[c].cur], sizeof(double) * 3 * M));
+    }
+    for (int s = 0; s < run->p.n_kinetic; ++s) {
+        SpeciesState const &S = run->sp[s];
+        size_t const        n = static_cast<size_t>(S.n);
+        if (run->mixed) {
+            CU(d2h(S.cell[S.cur], 4 * n));
+            for (int k = 0; k < 5; ++k)
+                CU(d2h(S.fbuf[S.cur][k], 4 * n));
+        } else {
+            for (int k = 0; k < 5; ++k)
+                CU(d2h(S.buf[S.cur][k], 8 * n));
+        }
+        CU(d2h(S.pid[S.cur], 4 * n));
+    }
+    CU(cudaStreamSynchronize(run->stream));
+    if (written)
+        *written = off;
+    return H1D_OK;
+}
+
+int h1d_checkpoint_load(h1d_run *run, void const *buffer, size_t size)
+{
+    if (!run || !buffer || size < sizeof(CkptHeader))
+        return set_err(run, H1D_ERR_INVALID_ARG, "h1d_checkpoint_load: no checkpoint");
+    CkptHeader hd;
+    std::memcpy(&hd, buffer, sizeof hd);
+    if (std::memcmp(hd.magic, CKPT_MAGIC, sizeof hd.magic) != 0 || hd.version != CKPT_VERSION)
+        return set_err(run, H1D_ERR_INVALID_ARG, "h1d_checkpoint_load: not a checkpoint of this library version");
+    if (hd.signature != params_signature(run->p) || hd.Nx != run->Nx || hd.n_kinetic != run->p.n_kinetic
+        || hd.n_cold != run->p.n_cold)
+        return set_err(run, H1D_ERR_INVALID_ARG, "h1d_checkpoint_load: signature verification failed");
+    size_t need = sizeof hd + sizeof(double) * 6 * run->M + sizeof(double) * 4 * run->M * run->p.n_cold;
+    for (int s = 0; s < run->p.n_kinetic; ++s) {
+        if (hd.n[s] < 0 || hd.n[s] > (int64_t{ 1 } << 31) - 1)
+            return set_err(run, H1D_ERR_INVALID_ARG, "h1d_checkpoint_load: corrupt particle count");
+        need += particle_bytes(run, hd.n[s]);
+    }
+    if (size < need)
+        return set_err(run, H1D_ERR_INVALID_ARG, "h1d_checkpoint_load: truncated checkpoint");
+    CU(cudaStreamSynchronize(run->stream));
+    auto const *in  = static_cast<unsigned char const *>(buffer);
+    size_t      off = sizeof hd;
+    auto        h2d = [&](void *dst, size_t bytes) -> cudaError_t {
+        cudaError_t const e = bytes ? cudaMemcpyAsync(dst, in + off, bytes, cudaMemcpyHostToDevice, run->stream) : cudaSuccess;
+        off += bytes;
+        return e;
+    };
+    long const M = run->M;
+    CU(h2d(run->B[run->fcur], sizeof(double) * 3 * M));
+    CU(h2d(run->E[run->fcur], sizeof(double) * 3 * M));
+    for (int c = 0; c < run->p.n_cold; ++c) {
+        ColdState &C = run->cold[c];
+        CU(h2d(C.n, sizeof(double) * M));
+        CU(h2d(C.nV[C.cur], sizeof(double) * 3 * M));
+        CU(cudaMemcpyAsync(C.nV[1 - C.cur], C.nV[C.cur], sizeof(double) * 3 * M, cudaMemcpyDeviceToDevice, run->stream));
+    }
+    for (int s = 0; s < run->p.n_kinetic; ++s) {
+        SpeciesState &S = run->sp[s];
+        TRY(ensure_capacity(run, s, hd.n[s]));
+        S.cur = 0, S.n = hd.n[s];
+        size_t const n = static_cast<size_t>(S.n);
+        if (run->mixed) {
+            CU(h2d(S.cell[0], 4 * n));
+            for (int k = 0; k < 5; ++k)
+                CU(h2d(S.fbuf[0][k], 4 * n));
+        } else {
+            for (int k = 0; k < 5; ++k)
+                CU(h2d(S.buf[0][k], 8 * n));
+        }
+        CU(h2d(S.pid[0], 4 * n));
+        CU(cudaMemsetAsync(S.dep, 0, sizeof(double) * 16 * M, run->stream)); // no deposit in flight
+        S.since_sort = 1 << 30;
+    }
+    CU(cudaStreamSynchronize(run->stream));
+    run->step          = hd.step;
+    run->recurring     = false; // the next advance starts like the reference's after a snapshot load
+    run->fields_dirty  = true;
+    run->moments_stale = true;
+    run->gen++;
+    return H1D_OK;
+}
+
+int h1d_step_count(h1d_run *run, int64_t *step)
+{
+    if (!run || !step)
+        return H1D_ERR_INVALID_ARG;
+    *step = run->step;
     return H1D_OK;
 }
 

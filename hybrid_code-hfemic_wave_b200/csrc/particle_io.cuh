@@ -329,4 +329,66 @@ __global__ void populate_kernel(PopulateArgs a)
 }
 
 
+// ------------------------------------------------------------------------------------------------
+// VHistogramRecorder::local_counting (Recorder/VHistogramRecorder.cc:289-306): gyro-averaged
+// velocity histogram of the particles in [ext_lo, ext_hi), relative to the bulk velocity nV/n of
+// the recorded moments at the particle (Shape<1>), binned as the recorder's Indexer does
+// (:88-100).  Rounded operations (no contraction) so that the bins equal the host's.  Per bin:
+// marker count, weight sum, real_f / marker sum (1 per full-f particle); the host normalises.
+// ------------------------------------------------------------------------------------------------
+struct VHistArgs {
+    double const  *q1, *vx, *vy, *vz, *w;        // FP64 storage, or
+    int32_t const *cell;                         // mixed-precision storage
+    float const   *off, *fvx, *fvy, *fvz, *fw;
+    int64_t        n;
+    double         half_min, full_min, ext_lo, ext_hi, v1min, v1len, v2min, v2len;
+    int            v1dim, v2dim;
+    double const  *mom; // finalized moments: n (M), nV (3M), GridArray layout
+    long           M;
+    double        *out; // 3 x v1dim x v2dim
+    unsigned long long *count;
+};
+
+__global__ void vhist_kernel(VHistArgs a)
+{
+    int64_t const k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (k >= a.n)
+        return;
+    double q1, vx, vy, vz, w;
+    if (a.q1) {
+        q1 = a.q1[k], vx = a.vx[k], vy = a.vy[k], vz = a.vz[k], w = a.w[k];
+    } else {
+        q1 = a.full_min + static_cast<double>(a.cell[k]) + static_cast<double>(a.off[k]);
+        vx = a.fvx[k], vy = a.fvy[k], vz = a.fvz[k], w = a.fw[k];
+    }
+    if (!(q1 >= a.ext_lo && q1 < a.ext_hi))
+        return;
+    atomicAdd(a.count, 1ull);
+    Shape<1> const sh = make_shape<1>(q1 - a.half_min);
+    if (sh.i0 < -PAD || sh.i0 + 1 >= a.M - PAD)
+        return;
+    double n = 0, V[3] = { 0, 0, 0 };
+#pragma unroll
+    for (int j = 0; j <= 1; ++j) {
+        long const i = sh.i0 + j + PAD;
+        n            = __dadd_rn(n, __dmul_rn(a.mom[i], sh.w[j]));
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            V[c] = __dadd_rn(V[c], __dmul_rn(a.mom[a.M + 3 * i + c], sh.w[j]));
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        V[c] = n < 1e-15 ? 0.0 : __ddiv_rn(V[c], n);
+    double const v1 = vx - V[0], py = vy - V[1], pz = vz - V[2];
+    double const v2 = __dsqrt_rn(__dadd_rn(__dmul_rn(py, py), __dmul_rn(pz, pz)));
+    double const f1 = floor(__ddiv_rn(__dmul_rn(v1 - a.v1min, static_cast<double>(a.v1dim)), a.v1len));
+    double const f2 = floor(__ddiv_rn(__dmul_rn(v2 - a.v2min, static_cast<double>(a.v2dim)), a.v2len));
+    if (f1 >= 0 && f1 < a.v1dim && f2 >= 0 && f2 < a.v2dim) {
+        double *o = a.out + 3 * (static_cast<int64_t>(f1) * a.v2dim + static_cast<int64_t>(f2));
+        atomicAdd(o, 1.0);
+        atomicAdd(o + 1, w);
+        atomicAdd(o + 2, 1.0);
+    }
+}
+
 } // namespace h1d

@@ -190,6 +190,16 @@ int h1d_download_cold(h1d_run *run, int i, double *n, double *nV, double *nvv, d
  * species then every cold species KE_lab[3], KE_pla[3]; computed on the device */
 int h1d_energy(h1d_run *run, double *dB2O2, double *dE2O2, double *KE_lab, double *KE_pla);
 
+/* VHistogramRecorder (Recorder/VHistogramRecorder.cc:222-306) on the device: gyro-averaged velocity
+ * histogram of kinetic species `s` over the particles with q1 in [ext_loc, ext_loc + ext_len),
+ * relative to the bulk velocity of the recorded moments, v1 (parallel) in v1dim bins over
+ * [v1min, v1min + v1len) and v2 (perpendicular speed) in v2dim bins over [v2min, v2min + v2len).
+ * out[3 * (i1 * v2dim + i2) + {0, 1, 2}] = {marker count, weight sum, real_f/marker sum} / total,
+ * total = the particles in the extent (the recorder's normalisation).  Zero-based bins; the
+ * recorder writes them one-based. */
+int h1d_vhistogram(h1d_run *run, int s, double ext_loc, double ext_len, double v1min, double v1len, int64_t v1dim,
+                   double v2min, double v2len, int64_t v2dim, double *out, int64_t *total);
+
 /* Phase timing with CUDA events recorded on the run's stream around each kernel group while
  * profiling is enabled; read() waits for the stream and returns the accumulated figures. */
 typedef struct h1d_profile {
@@ -236,6 +246,18 @@ int h1d_math_check(const double *x, int64_t n, double *out);
 int h1d_collect_moments_noalloc(int64_t Nx, double moment_norm, int particle_bc, const double *q1, const double *vx,
                                 const double *vy, const double *vz, const double *w, int64_t n, double *n_out,
                                 double *nV_out, double *nvv_out, void *stream);
+
+/* Checkpoint / resume, the content of the reference's snapshot (Recorder/Snapshot.cc:148-185,
+ * 330-375; HDF5 there, a flat little-endian byte image here): step count, a signature of the
+ * parameters that a load verifies (Snapshot.cc:340-342: "signature verification failed" ->
+ * H1D_ERR_INVALID_ARG), B, E, every kinetic species' particles with their ids in the run's own
+ * precision, every cold species' mom0_full / mom1_full.  After a load the next advance starts as
+ * the reference's does after loading a snapshot (sources recomputed from the particles). */
+int h1d_checkpoint_size(h1d_run *run, size_t *bytes);
+int h1d_checkpoint_save(h1d_run *run, void *buffer, size_t capacity, size_t *written);
+int h1d_checkpoint_load(h1d_run *run, const void *buffer, size_t size);
+/* the step count (the reference's Driver step count after advance_by calls) */
+int h1d_step_count(h1d_run *run, int64_t *step);
 
 /* Tuning of a run: steps between cell sorts (0 keeps the current value) and CTAs per SM of the
  * particle pass (0 = the kernel's default, at most 2 for FP64 and 4 for mixed precision).  No

@@ -1252,6 +1252,52 @@ int orc_download_cold(orc_run *R, int i, double *n, double *nV, double *nvv, dou
     return H1D_OK;
 }
 
+/* VHistogramRecorder::histogram / local_counting (Recorder/VHistogramRecorder.cc:222-306) on one
+ * process: particles with q1 in [ext_loc, ext_loc + ext_len) (Range::is_member), velocity relative
+ * to the local bulk velocity nV/n interpolated with Shape<1> from the recorded moments (zero where
+ * n < 1e-15), gyro-averaged (v1 = v_par, v2 = |v_perp|; the field-aligned basis is Cartesian on the
+ * field line), binned by floor((v - min) * dim / len); per bin {marker count, weight sum,
+ * real_f/marker sum (1 per full-f particle)} divided by the number of particles in the extent. */
+int orc_vhistogram(orc_run *R, int s, double ext_loc, double ext_len, double v1min, double v1len, int64_t v1dim,
+                   double v2min, double v2len, int64_t v2dim, double *out, int64_t *total)
+{
+    if (!R || s < 0 || s >= R->p.n_kinetic || v1dim <= 0 || v2dim <= 0 || !(v1len > 0) || !(v2len > 0) || !out)
+        return H1D_ERR_INVALID_ARG;
+    memset(out, 0, sizeof(double) * 3 * (size_t)(v1dim * v2dim));
+    Bucket const *b     = &R->part[s];
+    int64_t       count = 0;
+    for (int64_t k = 0; k < b->n; ++k) {
+        double const q1 = b->q1[k];
+        if (!(q1 >= ext_loc && q1 < ext_loc + ext_len))
+            continue;
+        ++count;
+        Shp sh;
+        shape1(&sh, q1 - R->half_min);
+        double n = 0;
+        for (int j = 0; j <= 1; ++j)
+            n += *at1(R->mom0[s], sh.i[j]) * sh.w[j];
+        V3 V = interp3(R->mom1[s], &sh, 1);
+        if (n < 1e-15)
+            V.x = V.y = V.z = 0;
+        else
+            V.x /= n, V.y /= n, V.z /= n;
+        double const v1 = b->vx[k] - V.x, vy = b->vy[k] - V.y, vz = b->vz[k] - V.z;
+        double const v2 = sqrt(vy * vy + vz * vz);
+        double const f1 = floor((v1 - v1min) * (double)v1dim / v1len);
+        double const f2 = floor((v2 - v2min) * (double)v2dim / v2len);
+        if (f1 >= 0 && f1 < (double)v1dim && f2 >= 0 && f2 < (double)v2dim) {
+            double *o = out + 3 * ((int64_t)f1 * v2dim + (int64_t)f2);
+            o[0] += 1, o[1] += b->w[k], o[2] += 1;
+        }
+    }
+    if (count > 0)
+        for (int64_t i = 0; i < 3 * v1dim * v2dim; ++i)
+            out[i] /= (double)count;
+    if (total)
+        *total = count;
+    return H1D_OK;
+}
+
 /* EnergyRecorder::dump (EnergyRecorder.cc:98-140); MFA <-> Cartesian is a pass-through */
 int orc_energy(orc_run *R, double *dB2O2, double *dE2O2, double *KE_lab, double *KE_pla)
 {
