@@ -19,7 +19,7 @@ from . import configs as _cfg
 PAD = 3
 MAX_KINETIC = 8
 MAX_COLD = 4
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 OK, ERR_INVALID_ARG, ERR_MOVED_TOO_FAR, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_NAN, ERR_STATE, \
     ERR_NO_DEVICE = range(9)
@@ -48,6 +48,16 @@ class EFluidDesc(C.Structure):
     _fields_ = [("Oc", C.c_double), ("op", C.c_double), ("beta", C.c_double), ("gamma", C.c_double)]
 
 
+MAX_SOURCES, MAX_SOURCE_POINTS = 2, 16
+
+
+class SourceDesc(C.Structure):
+    _fields_ = [("omega", C.c_double), ("start", C.c_double), ("duration", C.c_double),
+                ("ease_in", C.c_double), ("ease_out", C.c_double), ("n_smooth", C.c_int64),
+                ("n_points", C.c_int64), ("pos", C.c_double * MAX_SOURCE_POINTS),
+                ("J0re", (C.c_double * 3) * MAX_SOURCE_POINTS), ("J0im", (C.c_double * 3) * MAX_SOURCE_POINTS)]
+
+
 class Params(C.Structure):
     _fields_ = [
         ("Nx", C.c_int64), ("Dx", C.c_double), ("xi", C.c_double), ("O0", C.c_double),
@@ -57,8 +67,9 @@ class Params(C.Structure):
         ("phase_retardation_inset", C.c_int64), ("phase_retardation_factor", C.c_double),
         ("amplitude_damping_inset", C.c_int64), ("amplitude_damping_factor", C.c_double),
         ("moment_weighting", C.c_double), ("sort_interval", C.c_int32), ("n_kinetic", C.c_int32),
-        ("n_cold", C.c_int32), ("reserved0", C.c_int32), ("efluid", EFluidDesc),
+        ("n_cold", C.c_int32), ("n_sources", C.c_int32), ("efluid", EFluidDesc),
         ("kinetic", KineticDesc * MAX_KINETIC), ("cold", ColdDesc * MAX_COLD),
+        ("sources", SourceDesc * MAX_SOURCES),
     ]
 
 
@@ -83,6 +94,20 @@ def make_params(cfg: "_cfg.RunConfig") -> Params:
         p.kinetic[i] = KineticDesc(k.Oc, k.op, k.n_smooth, k.Nc, k.shape_order, cfg.moment_norm(k))
     for i, c in enumerate(cfg.cold):
         p.cold[i] = ColdDesc(c.Oc, c.op, c.n_smooth)
+    if len(cfg.sources) > MAX_SOURCES:
+        raise ValueError("too many external sources")
+    p.n_sources = len(cfg.sources)
+    for i, src in enumerate(cfg.sources):
+        d = p.sources[i]
+        d.omega, d.start, d.duration = src.omega, src.start, src.duration
+        d.ease_in, d.ease_out, d.n_smooth = src.ease_in, src.ease_out, src.n_smooth
+        if len(src.points) > MAX_SOURCE_POINTS:
+            raise ValueError("too many source points")
+        d.n_points = len(src.points)
+        for j, (q1, J0) in enumerate(src.points):
+            d.pos[j] = q1
+            for c in range(3):
+                d.J0re[j][c], d.J0im[j][c] = complex(J0[c]).real, complex(J0[c]).imag
     return p
 
 

@@ -66,6 +66,21 @@ class EFluid:
 
 
 @dataclass
+class Source:
+    """An external current source (ExternalSourceDesc<N>, PlasmaDesc.h:363-437): angular frequency,
+    time extent (start, duration) without the ease phases, ease-in/-out durations, smoothing count,
+    and source points (q1, (J0x, J0y, J0z)) with complex field-aligned amplitudes."""
+
+    omega: float
+    start: float
+    duration: float
+    ease_in: float
+    ease_out: float
+    points: list
+    n_smooth: int = 0
+
+
+@dataclass
 class RunConfig:
     name: str
     Nx: int
@@ -76,6 +91,7 @@ class RunConfig:
     efluid: EFluid
     kinetic: List[Kinetic] = field(default_factory=list)
     cold: List[Cold] = field(default_factory=list)
+    sources: List[Source] = field(default_factory=list)
     O0: float = 1.0
     n_subcycles: int = 10
     algorithm: int = ALGO_CAMCL
@@ -246,7 +262,24 @@ def parity_p4() -> RunConfig:
                      amplitude_damping=(6, 0.2), steps=10)
 
 
-PARITY = {f().name: f for f in (parity_p1, parity_p2, parity_p3, parity_p4)}
+def parity_p5() -> RunConfig:
+    """The p2 plasma with an external current source whose ramps and flat top all fall within ten
+    steps (t = 0.005 .. 0.095), at three points, one depositing into the last ghost cell (folded by the reflecting boundary)."""
+    cfg = parity_p2()
+    src = Source(omega=3.0, start=0.03, duration=0.03, ease_in=0.02, ease_out=0.025, n_smooth=1,
+                 points=[(0.3, (0.5, 0.5j, 0.0)), (-20.25, (0.2 + 0.1j, -0.3j, 0.1)), (31.7, (0.0, 1.0, 1.0j))])
+    return cfg.replace(name="p5_tsc_mirror_source", sources=[src])
+
+
+def parity_p6() -> RunConfig:
+    """The predictor-corrector case p4 with an external current source active from the first step."""
+    cfg = parity_p4()
+    src = Source(omega=2.0, start=0.0, duration=0.05, ease_in=0.0, ease_out=0.03, n_smooth=2,
+                 points=[(1.7, (0.4j, 0.6, 0.0)), (30.9, (0.0, 0.3, -0.2j))])
+    return cfg.replace(name="p6_pc_source", sources=[src])
+
+
+PARITY = {f().name: f for f in (parity_p1, parity_p2, parity_p3, parity_p4, parity_p5, parity_p6)}
 PRESETS = {f().name: f for f in (config1, config2, config3)}
 
 

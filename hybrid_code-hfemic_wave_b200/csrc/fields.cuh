@@ -30,6 +30,7 @@ namespace h1d {
 
 constexpr int MAXK = 8;
 constexpr int MAXC = 4;
+constexpr int MAXE = 2; // external current sources
 
 // per-cell geometry table, SoA over the Nx interior cells (index = interior cell)
 enum GeoIdx {
@@ -69,6 +70,10 @@ struct FieldArgs {
     int           nk, nc;
     KinSrc        k[MAXK];
     ColdSrc       c[MAXC];
+    // external sources (Core/ExternalSource.cc:12-66) as species whose raw[0] = raw[1] is the
+    // source's moment<1> (n zero), s1 = 1, charge / current factors 0 / 1, Lambda / Gamma 0 / 1
+    int           ne;
+    KinSrc        e[MAXE];
     double        dt, sub_dt, c_light, sqrt_g, O0, inv_D1;
     int           m; // n_subcycles
     // electron fluid (EField.cc:267-291)
@@ -337,6 +342,13 @@ __device__ __forceinline__ void camcl_field_body(FieldArgs const &a, int blk)
         sst3(S.J1, t, sld3(S.J1, t) + sld3(r.v, t));
         S.rho1[t] += r.a[t];
     }
+    for (int s = 0; s < a.ne; ++s) { // external sources at the half-time step (Domain_CAMCL.cc:93-100)
+        SV const r = collect_kinetic(a, C, S, a.e[s], 0);
+        sst3(S.J0, t, sld3(S.J0, t) + sld3(r.v, t));
+        S.rho0[t] += r.a[t];
+        sst3(S.J1, t, sld3(S.J1, t) + sld3(r.v, t));
+        S.rho1[t] += r.a[t];
+    }
     // 3. averages
     double const rho_avg = (S.rho0[t] + S.rho1[t]) * .5;
     d3 const     J_avg   = (sld3(S.J0, t) + sld3(S.J1, t)) * .5;
@@ -390,12 +402,12 @@ __device__ __forceinline__ void camcl_field_body(FieldArgs const &a, int blk)
     d3 const Bi = { C.hbx + (sld3(S.B0, min(t + 1, C.L - 1)).x + Bavg.x) * 0.5,
                     0 * a.O0 + (sld3(S.B0, min(t + 1, C.L - 1)).y + Bavg.y) * 0.5,
                     0 * a.O0 + (sld3(S.B0, min(t + 1, C.L - 1)).z + Bavg.z) * 0.5 };
-    for (int s = 0; s < a.nk + a.nc; ++s) {
+    for (int s = 0; s < a.nk + a.nc + a.ne; ++s) {
         double lam;
         d3     gam;
         int    nsm;
-        if (s < a.nk) {
-            KinSrc const &K = a.k[s];
+        if (s < a.nk || s >= a.nk + a.nc) {
+            KinSrc const &K = s < a.nk ? a.k[s] : a.e[s - a.nk - a.nc];
             lam             = fold(K.raw[1][0], C.gm, Nx, a.bc, K.s1, K.lamf);
             gam             = { fold(K.raw[1][1], C.gm, Nx, a.bc, K.s1, K.gamf), fold(K.raw[1][2], C.gm, Nx, a.bc, K.s1, K.gamf),
                     fold(K.raw[1][3], C.gm, Nx, a.bc, K.s1, K.gamf) };
@@ -467,6 +479,11 @@ __device__ __forceinline__ void pc_field_body(FieldArgs const &a, int blk)
             S.tr[t] = (K.n[C.gm] * K.w) * K.cdcf;
             sst3(S.tJ, t, (v * K.w) * K.ccf);
             SV const r = smooth_n(C, K.nsm, S.tr, S.tJ, S.ts, S.tJs);
+            rho += r.a[t];
+            J = J + sld3(r.v, t);
+        }
+        for (int s = 0; s < a.ne; ++s) { // external sources (Domain_PC.cc:51-56, 134-140, 189-193)
+            SV const r = collect_kinetic(a, C, S, a.e[s], 1);
             rho += r.a[t];
             J = J + sld3(r.v, t);
         }

@@ -65,6 +65,11 @@ cudaError_t launch_energy(EnergyArgs const &a, cudaStream_t st)
     energy_kernel<<<1, 256, 0, st>>>(a);
     return cudaGetLastError();
 }
+cudaError_t launch_sources(SourceArgs const &a, cudaStream_t st)
+{
+    source_kernel<<<1, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
 cudaError_t launch_iota(int32_t *pid, int64_t n, cudaStream_t st)
 {
     iota_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(pid, n);

@@ -69,6 +69,7 @@ struct h1d_run {
     double      *geo = nullptr;
     double      *B[2] = {}, *E[2] = {}, *EB = nullptr, *charge = nullptr, *current = nullptr;
     float       *EBf = nullptr; // FP32 push record of the mixed-precision particle pass
+    double      *src_dep = nullptr; // per external source: moment<0> (zero), moment<1> x, y, z (M each)
     bool         mixed = false;
     double      *E1[2] = {}; // predictor-corrector: averaged E of phases 1 and 2
     int          fcur = 0; // field parity
@@ -199,6 +200,15 @@ int validate(h1d_params const *p, std::string &m)
     for (int s = 0; s < p->n_cold; ++s)
         if (p->cold[s].Oc == 0 || !(p->cold[s].op > 0) || p->cold[s].n_smooth < 0 || p->cold[s].n_smooth > 64)
             BAD("cold species %d: invalid descriptor", s);
+    if (p->n_sources < 0 || p->n_sources > H1D_MAX_SOURCES)
+        BAD("too many external sources");
+    for (int e = 0; e < p->n_sources; ++e) { // ExternalSourceBase (PlasmaDesc.h:383-403)
+        h1d_source_desc const &d = p->sources[e];
+        if (!(d.ease_in >= 0) || !(d.ease_out >= 0))
+            BAD("external source %d: ease-in/-out should be non-negative", e);
+        if (d.n_points < 0 || d.n_points > H1D_MAX_SOURCE_POINTS || d.n_smooth < 0 || d.n_smooth > 64)
+            BAD("external source %d: invalid descriptor", e);
+    }
     if (p->xi > 0) { // ParamSet.cc:25-29
         double const xd   = p->xi * p->Dx;
         double const e[4] = { -0.5 * p->Nx, -0.5 * p->Nx + p->Nx, -0.5 * p->Nx + 0.5, -0.5 * p->Nx + 0.5 + p->Nx };
@@ -443,6 +453,16 @@ FieldArgs field_args(h1d_run *run)
         K.cdcf = cdcf(p, d.Oc, d.op), K.ccf = ccf(p, d.Oc, d.op), K.lamf = K.cdcf * d.Oc / p.O0, K.gamf = K.ccf * d.Oc / p.O0;
         K.w = p.moment_weighting, K.nsm = static_cast<int>(d.n_smooth);
     }
+    a.ne = p.n_sources;
+    for (int e = 0; e < p.n_sources; ++e) {
+        KinSrc &K = a.e[e];
+        for (int dd = 0; dd < 2; ++dd)
+            for (int q = 0; q < 4; ++q)
+                K.raw[dd][q] = run->src_dep + (static_cast<size_t>(e) * 4 + q) * run->M + PAD, K.zero[dd][q] = nullptr;
+        K.s1 = 1.0, K.cdcf = 0.0, K.ccf = 1.0;
+        K.lamf = 0.0 * p.O0 / p.O0, K.gamf = 1.0 * p.O0 / p.O0; // Oc = O0 (ExternalSource.hh:19)
+        K.nsm = static_cast<int>(p.sources[e].n_smooth);
+    }
     a.dt = p.dt, a.sub_dt = p.dt / p.n_subcycles, a.c_light = p.c, a.sqrt_g = p.Dx * 1 * 1, a.O0 = p.O0, a.inv_D1 = 1 / p.Dx;
     a.m = static_cast<int>(p.n_subcycles);
     h1d_efluid_desc const &ef = p.efluid;
@@ -460,6 +480,26 @@ int prepare_fields(h1d_run *run)
     return H1D_OK;
 }
 
+// ExternalSource::update at time t of every external source (its moment<1> for the field kernel)
+int launch_run_sources(h1d_run *run, double t)
+{
+    h1d_params const &p = run->p;
+    if (p.n_sources == 0)
+        return H1D_OK;
+    SourceArgs a{};
+    a.ne = p.n_sources, a.t = t, a.half_min = -0.5 * p.Nx + 0.5, a.half_len = static_cast<double>(p.Nx);
+    a.weighting = p.moment_weighting, a.M = static_cast<int>(run->M);
+    for (int e = 0; e < p.n_sources; ++e) {
+        a.d[e] = p.sources[e];
+        for (int c = 0; c < 3; ++c)
+            a.J[e][c] = run->src_dep + (static_cast<size_t>(e) * 4 + 1 + c) * run->M + PAD;
+    }
+    CU(launch_sources(a, run->stream));
+    if (run->profiling)
+        run->prof.kernel_launches += 1;
+    return H1D_OK;
+}
+
 int camcl_step(h1d_run *run)
 {
     h1d_params const &p = run->p;
@@ -473,6 +513,7 @@ int camcl_step(h1d_run *run)
             run->prof.particles_pushed += run->sp[s].n;
         run->sp[s].since_sort++;
     }
+    TRY(launch_run_sources(run, static_cast<double>(run->step) * p.dt + 0.5 * p.dt)); // update(0.5 dt)
     FieldArgs const a = field_args(run);
     phase_begin(run, 2);
     CU(launch_camcl_fields(a, run->nblocks_field, run->L, run->field_smem, run->stream));
@@ -538,6 +579,7 @@ int pc_initial_sources(h1d_run *run) // Domain_PC.cc:36-56
 {
     int const X = run->dset, Y = 1 - X;
     TRY(pc_particles(run, 2, Y));
+    TRY(launch_run_sources(run, static_cast<double>(run->step) * run->p.dt + 0)); // a predictor copy's update(0)
     TRY(pc_launch_fields(run, 0, Y, X, nullptr, nullptr));
     return H1D_OK;
 }
@@ -547,6 +589,7 @@ int pc_step(h1d_run *run)
     int const X = run->dset, Y = 1 - X;
     TRY(pc_launch_fields(run, 1, X, X, nullptr, run->E1[0])); // B1, E1 predicted and averaged (clears nothing new)
     TRY(pc_particles(run, 0, X));
+    TRY(launch_run_sources(run, static_cast<double>(run->step) * run->p.dt + run->p.dt)); // update(dt), both passes
     TRY(pc_launch_fields(run, 2, X, Y, run->E1[0], run->E1[1]));
     TRY(pc_particles(run, 1, Y));
     {
@@ -779,8 +822,8 @@ bool graph_eligible(h1d_batch const *b)
 {
     if (!b->use_graphs)
         return false;
-    for (h1d_run const *r : b->runs)
-        if (r->p.particle_bc == H1D_BC_ABSORBING || r->p.randomize_gyrophase)
+    for (h1d_run const *r : b->runs) // host-side trims and per-step draws and times are not capturable
+        if (r->p.particle_bc == H1D_BC_ABSORBING || r->p.randomize_gyrophase || r->p.n_sources > 0)
             return false;
     return true;
 }
@@ -908,7 +951,12 @@ int batch_step(h1d_batch *b)
         size_t const groups = kd.mixed ? mx[ki].size() : fp[ki].size();
         b->stats.kernel_launches += static_cast<int64_t>((groups + BATCH_GROUPS - 1) / BATCH_GROUPS);
     }
-    // field cycle of every member
+    // external sources of the members that have them, then the field cycle of every member
+    for (h1d_run *r : b->runs)
+        if (r->p.n_sources > 0) {
+            BTRY(r, launch_run_sources(r, static_cast<double>(r->step) * r->p.dt + 0.5 * r->p.dt));
+            b->stats.kernel_launches += 1;
+        }
     BCU(launch_camcl_fields_batch(b->d_table + b->parity * b->runs.size(), b->d_map, b->nblocks, b->L, b->smem,
                                   b->stream));
     b->stats.kernel_launches += 1;
@@ -1212,7 +1260,8 @@ int h1d_create(h1d_params const *params, h1d_run **out)
         || dalloc(run, &run->charge, M) || dalloc(run, &run->current, 3 * M) || dalloc(run, &run->d_status, 1)
         || dalloc(run, &run->E1[0], 3 * M) || dalloc(run, &run->E1[1], 3 * M) || dalloc(run, &run->d_fallbacks, 1)
         || dalloc(run, &run->d_energy, 6 + 6 * (H1D_MAX_KINETIC + H1D_MAX_COLD))
-        || (run->mixed && dalloc(run, &run->EBf, 6 * M)))
+        || (run->mixed && dalloc(run, &run->EBf, 6 * M))
+        || (p.n_sources > 0 && dalloc(run, &run->src_dep, 4 * M * p.n_sources)))
         return fail(H1D_ERR_OOM);
     if (cudaMallocHost(&run->h_status, sizeof(unsigned)) != cudaSuccess)
         return fail(H1D_ERR_OOM);
@@ -1245,7 +1294,7 @@ int h1d_destroy(h1d_run *run)
     for (int k = 0; k < 2; ++k)
         cudaFree(run->B[k]), cudaFree(run->E[k]), cudaFree(run->E1[k]);
     cudaFree(run->d_fallbacks);
-    cudaFree(run->EB), cudaFree(run->EBf), cudaFree(run->charge), cudaFree(run->current), cudaFree(run->d_status), cudaFree(run->d_energy);
+    cudaFree(run->EB), cudaFree(run->EBf), cudaFree(run->src_dep), cudaFree(run->charge), cudaFree(run->current), cudaFree(run->d_status), cudaFree(run->d_energy);
     if (run->h_status)
         cudaFreeHost(run->h_status);
     for (auto &S : run->sp) {

@@ -3,6 +3,7 @@
 #pragma once
 
 #include "fields.cuh"
+#include "h1d_gpu.h"
 
 #include <cuda_runtime.h>
 
@@ -31,5 +32,14 @@ cudaError_t launch_finalize_cold(double const *n_full, double const *nV_full, do
                                  cudaStream_t st);
 cudaError_t launch_energy(EnergyArgs const &a, cudaStream_t st);
 cudaError_t launch_iota(int32_t *pid, int64_t n, cudaStream_t st);
+// the external sources of a run at time t (source_kernel, post.cuh)
+struct SourceArgs {
+    h1d_source_desc d[MAXE];
+    int             ne;
+    double          t, half_min, half_len, weighting;
+    double         *J[MAXE][3]; // cell 0 of each component array (Nx + 2 PAD cells)
+    int             M;
+};
+cudaError_t launch_sources(SourceArgs const &a, cudaStream_t st);
 
 } // namespace h1d

@@ -4,6 +4,7 @@
 #pragma once
 
 #include "device_common.cuh"
+#include "h1d_gpu.h"
 #include "launchers.h"
 
 namespace h1d {
@@ -165,6 +166,53 @@ __global__ void energy_kernel(EnergyArgs a)
                 a.out[6 + 6 * s + 3 + c] = P * a.factor[s];
             }
         }
+}
+
+// ExternalSource::update / collect (Core/ExternalSource.cc:12-66): the moment<1> of every external
+// source at time t, deposited with Shape<1> at its points inside the half-grid extent; one block,
+// the points in order on one thread (the reference's order), no contraction (this unit).
+__global__ void source_kernel(SourceArgs a)
+{
+    for (int e = 0; e < a.ne; ++e)
+        for (int c = 0; c < 3; ++c)
+            for (int i = threadIdx.x; i < a.M; i += blockDim.x)
+                a.J[e][c][i - PAD] = 0;
+    __syncthreads();
+    if (threadIdx.x != 0)
+        return;
+    for (int e = 0; e < a.ne; ++e) {
+        h1d_source_desc const &d = a.d[e];
+        // envelope (ExternalSource.cc:44-67) with the ramp slopes of ExternalSource.hh:29-32
+        double const eps       = 1e-15;
+        double const slope_in  = 3.141592653589793 / (d.ease_in > eps ? d.ease_in : 1.0);
+        double const slope_out = 3.141592653589793 / (d.ease_out > eps ? d.ease_out : 1.0);
+        double       tt        = a.t - d.start;
+        double       env;
+        if (tt < -d.ease_in)
+            env = 0;
+        else if (tt < 0)
+            env = .5 * (1 + cos(slope_in * tt));
+        else if (tt < d.duration)
+            env = 1;
+        else if ((tt -= d.duration) < d.ease_out)
+            env = .5 * (1 + cos(slope_out * tt));
+        else
+            env = 0;
+        for (int i = 0; i < d.n_points; ++i) {
+            double const pos = d.pos[i];
+            if (!(pos >= a.half_min && pos < a.half_min + a.half_len))
+                continue;
+            Shape<1> const sx    = make_shape<1>(pos - a.half_min);
+            double const   phase = -d.omega * (a.t - d.start);
+            double const   cs = cos(phase), sn = sin(phase);
+            double const   f  = env * a.weighting;
+            for (int c = 0; c < 3; ++c) {
+                double const v = (d.J0re[i][c] * cs - d.J0im[i][c] * sn) * f;
+                a.J[e][c][sx.i0] += v * sx.w[0];
+                a.J[e][c][sx.i0 + 1] += v * sx.w[1];
+            }
+        }
+    }
 }
 
 } // namespace h1d

@@ -51,12 +51,14 @@
 extern "C" {
 #endif
 
-#define H1D_ABI_VERSION 1
+#define H1D_ABI_VERSION 2
 
 /* number of ghost cells on each side; Input::number_of_ghost_cells (Include/Inputs.h:22) */
 #define H1D_PAD 3
 #define H1D_MAX_KINETIC 8
 #define H1D_MAX_COLD 4
+#define H1D_MAX_SOURCES 2
+#define H1D_MAX_SOURCE_POINTS 16
 
 /* status codes */
 enum {
@@ -105,6 +107,21 @@ typedef struct h1d_efluid_desc {
     double gamma;
 } h1d_efluid_desc;
 
+/* ExternalSourceDesc<N> (LibPIC/PIC/PlasmaDesc.h:363-437): an antenna current of angular frequency
+ * omega applied over [start, start + duration] with cosine ease-in/-out ramps, at n_points source
+ * positions q1 with complex field-aligned amplitudes J0 = J0re + i J0im
+ * (Core/ExternalSource.cc:12-66) */
+typedef struct h1d_source_desc {
+    double  omega;
+    double  start, duration; /* ExternalSourceBase::extent {loc, len} */
+    double  ease_in, ease_out;
+    int64_t n_smooth;        /* PlasmaDesc::number_of_source_smoothings */
+    int64_t n_points;        /* <= H1D_MAX_SOURCE_POINTS */
+    double  pos[H1D_MAX_SOURCE_POINTS];
+    double  J0re[H1D_MAX_SOURCE_POINTS][3];
+    double  J0im[H1D_MAX_SOURCE_POINTS][3];
+} h1d_source_desc;
+
 /* The runtime form of `struct Input` (Include/Inputs.h:13-241) for one run */
 typedef struct h1d_params {
     int64_t Nx;          /* Input::Nx, whole domain (one GPU holds the whole field line) */
@@ -129,10 +146,11 @@ typedef struct h1d_params {
     int32_t sort_interval;    /* steps between particle cell sorts; 0 = library default */
     int32_t n_kinetic;
     int32_t n_cold;
-    int32_t reserved0;
+    int32_t n_sources;        /* external current sources (Input::source_descs) */
     h1d_efluid_desc  efluid;
     h1d_kinetic_desc kinetic[H1D_MAX_KINETIC];
     h1d_cold_desc    cold[H1D_MAX_COLD];
+    h1d_source_desc  sources[H1D_MAX_SOURCES];
 } h1d_params;
 
 typedef struct h1d_run h1d_run;

@@ -69,6 +69,8 @@ typedef struct orc_run {
     double *cn_full[H1D_MAX_COLD], *cnV_full[H1D_MAX_COLD];
     double *cmom0[H1D_MAX_COLD], *cmom1[H1D_MAX_COLD], *cmom2[H1D_MAX_COLD];
     double *pc_n_full, *pc_nV_full;
+    /* external sources: moment<0> (always zero) and moment<1> of the last update */
+    double *smom0[H1D_MAX_SOURCES], *smom1[H1D_MAX_SOURCES];
     /* bucket buffers of the delegate */
     Bucket  bufL, bufR;
     int     recurring;
@@ -633,10 +635,10 @@ static void addto(double *dst, double const *src, long count)
     for (long i = 0; i < count; ++i)
         dst[i] += src[i];
 }
-static double const *collect_smooth_rho(orc_run *R, double const *mom0, double Oc, double op, long n_smooth)
+static double const *collect_smooth_rho_f(orc_run *R, double const *mom0, double factor, long n_smooth)
 {
     memset(R->rho, 0, sizeof(double) * R->M);
-    add_scaled(R->rho, mom0, R->M, cdcf(R, Oc, op));
+    add_scaled(R->rho, mom0, R->M, factor);
     gather_grid(R, R->rho, 1);
     for (long i = 0; i < n_smooth; ++i) {
         pass_grid(R, R->rho, 1);
@@ -645,10 +647,10 @@ static double const *collect_smooth_rho(orc_run *R, double const *mom0, double O
     pass_grid(R, R->rho, 1);
     return R->rho;
 }
-static double const *collect_smooth_J(orc_run *R, double const *mom1, double Oc, double op, long n_smooth)
+static double const *collect_smooth_J_f(orc_run *R, double const *mom1, double factor, long n_smooth)
 {
     memset(R->J, 0, sizeof(double) * 3 * R->M);
-    add_scaled(R->J, mom1, 3 * R->M, ccf(R, Oc, op));
+    add_scaled(R->J, mom1, 3 * R->M, factor);
     gather_grid(R, R->J, 3);
     for (long i = 0; i < n_smooth; ++i) {
         pass_grid(R, R->J, 3);
@@ -656,6 +658,15 @@ static double const *collect_smooth_J(orc_run *R, double const *mom1, double Oc,
     }
     pass_grid(R, R->J, 3);
     return R->J;
+}
+/* Domain::collect_smooth (Domain.hh:35-74) with the species' conversion factors (Species.h:42-49) */
+static double const *collect_smooth_rho(orc_run *R, double const *mom0, double Oc, double op, long n_smooth)
+{
+    return collect_smooth_rho_f(R, mom0, cdcf(R, Oc, op), n_smooth);
+}
+static double const *collect_smooth_J(orc_run *R, double const *mom1, double Oc, double op, long n_smooth)
+{
+    return collect_smooth_J_f(R, mom1, ccf(R, Oc, op), n_smooth);
 }
 
 /* ------------------------------------------------------------------------------------------------
@@ -769,15 +780,17 @@ static void current_advance_impl(orc_run *R, double *J, double const *L, double 
         o[2] += (e[2] * l + gx.z) * dt;
     }
 }
-/* Domain_CAMCL::current_advance (Domain_CAMCL.cc:131-151) */
-static double const *current_advance(orc_run *R, double const *mom0, double const *mom1, double Oc, double op, long n_smooth, double dt_2)
+/* Domain_CAMCL::current_advance (Domain_CAMCL.cc:131-151); Lambda / Gamma take the charge / current
+ * conversion factors times Oc/O0 (Charge.cc:31-36, Current.cc:34-39) */
+static double const *current_advance_f(orc_run *R, double const *mom0, double const *mom1, double lam_f, double gam_f,
+                                       long n_smooth, double dt_2)
 {
     long const M = R->M;
     memset(R->lambda, 0, sizeof(double) * M);
-    add_scaled(R->lambda, mom0, M, cdcf(R, Oc, op) * Oc / R->p.O0);
+    add_scaled(R->lambda, mom0, M, lam_f);
     gather_grid(R, R->lambda, 1);
     memset(R->gamma, 0, sizeof(double) * 3 * M);
-    add_scaled(R->gamma, mom1, 3 * M, ccf(R, Oc, op) * Oc / R->p.O0);
+    add_scaled(R->gamma, mom1, 3 * M, gam_f);
     gather_grid(R, R->gamma, 3);
     memset(R->J, 0, sizeof(double) * 3 * M);
     current_advance_impl(R, R->J, R->lambda, R->gamma, R->B, R->E, dt_2);
@@ -787,6 +800,68 @@ static double const *current_advance(orc_run *R, double const *mom0, double cons
     }
     pass_grid(R, R->J, 3);
     return R->J;
+}
+static double const *current_advance(orc_run *R, double const *mom0, double const *mom1, double Oc, double op, long n_smooth, double dt_2)
+{
+    return current_advance_f(R, mom0, mom1, cdcf(R, Oc, op) * Oc / R->p.O0, ccf(R, Oc, op) * Oc / R->p.O0, n_smooth, dt_2);
+}
+
+/* ------------------------------------------------------------------------------------------------
+ * ExternalSource (Core/ExternalSource.cc:12-66, ExternalSource.hh:16-33): a species whose Oc is O0
+ * and op is 0, with charge / current conversion factors 0 / 1 (ExternalSource.h:36-38), so it adds
+ * its moment<1> to the current, J x B dt/2 to the advanced current, and nothing to the charge.
+ */
+static double src_envelope(h1d_source_desc const *d, double t)
+{
+    double const eps      = 1e-15;
+    double const slope_in = M_PI / (d->ease_in > eps ? d->ease_in : 1.0);
+    double const slope_out = M_PI / (d->ease_out > eps ? d->ease_out : 1.0);
+    t -= d->start;
+    if (t < -d->ease_in) /* before ease-in */
+        return 0;
+    if (t < 0) /* ease-in */
+        return .5 * (1 + cos(slope_in * t));
+    if (t < d->duration) /* middle */
+        return 1;
+    if ((t -= d->duration) < d->ease_out) /* ease-out */
+        return .5 * (1 + cos(slope_out * t));
+    return 0;
+}
+/* ExternalSource::collect: moment<1> = sum over source points inside the half-grid extent of the
+ * Cartesian current (field-aligned = Cartesian on the field line) times envelope x weighting,
+ * deposited with Shape<1> */
+static void src_collect(orc_run *R, int e, double t)
+{
+    h1d_source_desc const *d = &R->p.sources[e];
+    memset(R->smom0[e], 0, sizeof(double) * R->M);
+    memset(R->smom1[e], 0, sizeof(double) * 3 * R->M);
+    double const lo = R->half_min, hi = R->half_min + R->full_len;
+    for (int64_t i = 0; i < d->n_points; ++i) {
+        double const pos = d->pos[i];
+        if (!(pos >= lo && pos < hi))
+            continue;
+        Shp sx;
+        shape1(&sx, pos - lo);
+        double const phase = -d->omega * (t - d->start);
+        double const c = cos(phase), sn = sin(phase);
+        double const f  = src_envelope(d, t) * R->p.moment_weighting;
+        double const J[3] = { d->J0re[i][0] * c - d->J0im[i][0] * sn, d->J0re[i][1] * c - d->J0im[i][1] * sn,
+                              d->J0re[i][2] * c - d->J0im[i][2] * sn };
+        double const v[3] = { J[0] * f, J[1] * f, J[2] * f };
+        for (int j = 0; j <= 1; ++j) {
+            double *a = at3(R->smom1[e], sx.i[j]);
+            a[0] += v[0] * sx.w[j];
+            a[1] += v[1] * sx.w[j];
+            a[2] += v[2] * sx.w[j];
+        }
+    }
+}
+/* the source's contribution to a charge / current pair (collect_smooth with factors 0 and 1) */
+static void src_add(orc_run *R, int e, double *charge, double *current)
+{
+    long const n_smooth = R->p.sources[e].n_smooth;
+    addto(current, collect_smooth_J_f(R, R->smom1[e], 1.0, n_smooth), 3 * R->M);
+    addto(charge, collect_smooth_rho_f(R, R->smom0[e], 0.0, n_smooth), R->M);
 }
 
 /* ColdSpecies::impl_update_nV (ColdSpecies.cc:255-262) */
@@ -853,6 +928,11 @@ static int camcl_cycle(orc_run *R)
         addto(R->current1, collect_smooth_J(R, R->cmom1[ci], d->Oc, d->op, d->n_smooth), 3 * M);
         addto(R->charge1, collect_smooth_rho(R, R->cmom0[ci], d->Oc, d->op, d->n_smooth), M);
     }
+    for (int e = 0; e < R->p.n_sources; ++e) { /* update(0.5 dt): at the half-time step */
+        src_collect(R, e, (double)R->step * dt + 0.5 * dt);
+        src_add(R, e, R->charge, R->current);
+        src_add(R, e, R->charge1, R->current1);
+    }
     /* average */
     for (long i = 0; i < M; ++i)
         R->charge[i] = (R->charge[i] + R->charge1[i]) * .5;
@@ -895,6 +975,9 @@ static int camcl_cycle(orc_run *R)
         h1d_cold_desc const *d = &R->p.cold[ci];
         addto(R->current1, current_advance(R, R->cmom0[ci], R->cmom1[ci], d->Oc, d->op, d->n_smooth, 0.5 * dt), 3 * M);
     }
+    for (int e = 0; e < R->p.n_sources; ++e) /* Oc = O0: Lambda factor 0 * O0/O0, Gamma factor 1 * O0/O0 */
+        addto(R->current1, current_advance_f(R, R->smom0[e], R->smom1[e], 0.0 * R->p.O0 / R->p.O0, 1.0 * R->p.O0 / R->p.O0,
+                                             R->p.sources[e].n_smooth, 0.5 * dt), 3 * M);
     efield_update(R, R->E, R->B, R->charge1, R->current1);
     pass_grid(R, R->E, 3);
     return ok;
@@ -957,6 +1040,10 @@ static int pc_cycle(orc_run *R)
         addto(R->charge, collect_smooth_rho(R, R->pmom0, d->Oc, d->op, d->n_smooth), M);
         addto(R->current, collect_smooth_J(R, R->pmom1, d->Oc, d->op, d->n_smooth), 3 * M);
     }
+    for (int e = 0; e < R->p.n_sources; ++e) { /* a predictor copy's update(dt): at the full-time step */
+        src_collect(R, e, (double)R->step * dt + dt);
+        src_add(R, e, R->charge, R->current);
+    }
     /* corrector */
     memcpy(R->B1, R->B, sizeof(double) * 3 * M);
     bfield_update(R, R->B1, R->E1, dt);
@@ -975,6 +1062,10 @@ static int pc_cycle(orc_run *R)
         cold_collect_part(R, R->cn_full[ci], R->cnV_full[ci], R->cmom0[ci], R->cmom1[ci]);
         addto(R->charge, collect_smooth_rho(R, R->cmom0[ci], d->Oc, d->op, d->n_smooth), M);
         addto(R->current, collect_smooth_J(R, R->cmom1[ci], d->Oc, d->op, d->n_smooth), 3 * M);
+    }
+    for (int e = 0; e < R->p.n_sources; ++e) { /* update(dt) of the source itself */
+        src_collect(R, e, (double)R->step * dt + dt);
+        src_add(R, e, R->charge, R->current);
     }
     bfield_update(R, R->B, R->E1, dt);
     pass_grid(R, R->B, 3);
@@ -1025,6 +1116,15 @@ static int check_params(h1d_params const *p, char *msg, size_t cap)
     for (int s = 0; s < p->n_cold; ++s)
         if (p->cold[s].Oc == 0 || !(p->cold[s].op > 0) || p->cold[s].n_smooth < 0)
             BAD("cold species %d: invalid descriptor", s);
+    if (p->n_sources < 0 || p->n_sources > H1D_MAX_SOURCES)
+        BAD("too many external sources");
+    for (int e = 0; e < p->n_sources; ++e) { /* ExternalSourceBase (PlasmaDesc.h:383-403) */
+        h1d_source_desc const *d = &p->sources[e];
+        if (!(d->ease_in >= 0) || !(d->ease_out >= 0))
+            BAD("external source %d: ease-in/-out should be non-negative", e);
+        if (d->n_points < 0 || d->n_points > H1D_MAX_SOURCE_POINTS || d->n_smooth < 0)
+            BAD("external source %d: invalid descriptor", e);
+    }
     if (p->xi > 0) { /* ParamSet.cc:25-29 */
         double const lim = M_PI_2, xd = p->xi * p->Dx;
         double const e[4] = { -0.5 * p->Nx, -0.5 * p->Nx + p->Nx, -0.5 * p->Nx + 0.5, -0.5 * p->Nx + 0.5 + p->Nx };
@@ -1071,6 +1171,8 @@ int orc_create(h1d_params const *p, orc_run **out)
         R->cmom0[s] = xcalloc(M, 8), R->cmom1[s] = xcalloc(3 * M, 8), R->cmom2[s] = xcalloc(6 * M, 8);
     }
     R->pc_n_full = xcalloc(M, 8), R->pc_nV_full = xcalloc(3 * M, 8);
+    for (int e = 0; e < R->p.n_sources; ++e)
+        R->smom0[e] = xcalloc(M, 8), R->smom1[e] = xcalloc(3 * M, 8);
     *out = R;
     return H1D_OK;
 }
@@ -1088,6 +1190,8 @@ int orc_destroy(orc_run *R)
         free(R->mom0[s]), free(R->mom1[s]), free(R->mom2[s]), bucket_free(&R->part[s]);
     for (int s = 0; s < R->p.n_cold; ++s)
         free(R->cn_full[s]), free(R->cnV_full[s]), free(R->cmom0[s]), free(R->cmom1[s]), free(R->cmom2[s]);
+    for (int e = 0; e < R->p.n_sources; ++e)
+        free(R->smom0[e]), free(R->smom1[e]);
     bucket_free(&R->pred), bucket_free(&R->bufL), bucket_free(&R->bufR);
     free(R);
     return H1D_OK;
@@ -1153,6 +1257,10 @@ int orc_advance(orc_run *R, uint32_t n_steps)
                 cold_collect_part(R, R->cn_full[ci], R->cnV_full[ci], R->cmom0[ci], R->cmom1[ci]);
                 addto(R->charge, collect_smooth_rho(R, R->cmom0[ci], d->Oc, d->op, d->n_smooth), M);
                 addto(R->current, collect_smooth_J(R, R->cmom1[ci], d->Oc, d->op, d->n_smooth), 3 * M);
+            }
+            for (int e = 0; e < R->p.n_sources; ++e) { /* a predictor copy's update(0) */
+                src_collect(R, e, (double)R->step * R->p.dt + 0);
+                src_add(R, e, R->charge, R->current);
             }
         }
     }

@@ -6,7 +6,7 @@ reference build under oracle/_ref/ is compiled once per configuration.  The head
 here holds the same numbers the CUDA library and the C oracle receive at runtime, printed
 with ``repr`` so that the C++ literal parses back to the identical double.
 
-Single process, single subdomain, no worker threads, no external sources; gyro-phase
+Single process, single subdomain, no worker threads; gyro-phase
 randomisation of reflected particles is off (the reference seeds it from
 std::random_device, Boundary/Delegate.cc:231).
 
@@ -47,6 +47,19 @@ def render(cfg) -> str:
         f"BiMaxPlasmaDesc({{ {{ {r(k.Oc)}, {r(k.op)}, {k.n_smooth} }}, {k.Nc}, {SHAPE[k.shape_order]}, full_f }}, "
         f"{r(k.beta1)}, {r(k.T2_T1)})" for k in cfg.kinetic)
     cold = ",\n        ".join(f"ColdPlasmaDesc({{ {r(c.Oc)}, {r(c.op)}, {c.n_smooth} }})" for c in cfg.cold)
+    def cplx(z):
+        z = complex(z)
+        return f"std::complex<double>{{ {r(z.real)}, {r(z.imag)} }}"
+
+    srcs = []
+    for src in cfg.sources:
+        n = len(src.points)
+        J0 = ", ".join(f"ComplexVector{{ {cplx(J[0])}, {cplx(J[1])}, {cplx(J[2])} }}" for _, J in src.points)
+        pos = ", ".join(f"CurviCoord{{ {r(q1)} }}" for q1, _ in src.points)
+        srcs.append(f"ExternalSourceDesc<{n}>{{ ExternalSourceBase{{ {r(src.omega)}, Range{{ {r(src.start)}, {r(src.duration)} }}, "
+                    f"ExternalSourceBase::EasePhase{{ {r(src.ease_in)}, {r(src.ease_out)} }}, {src.n_smooth} }}, "
+                    f"{{ {J0} }}, {{ {pos} }} }}")
+    sources = ",\n        ".join(srcs)
     pr, ad = cfg.phase_retardation, cfg.amplitude_damping
     nk = len(cfg.kinetic)
     ndumps = ", ".join(["0"] * nk)
@@ -76,7 +89,8 @@ struct Input {{
         {kin});
     static constexpr auto cold_descs = std::make_tuple(
         {cold});
-    static constexpr auto source_descs = std::make_tuple();
+    static constexpr auto source_descs = std::make_tuple(
+        {sources});
     static constexpr std::string_view working_directory = "./data";
     static constexpr std::pair<unsigned, Range> energy_recording_frequency = {{ 0, {{}} }};
     static constexpr std::pair<unsigned, Range> field_recording_frequency = {{ 0, {{}} }};

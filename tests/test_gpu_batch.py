@@ -117,3 +117,35 @@ def test_autotuned_run_matches_oracle(gpu_lib, oracle_lib):
     errs = state_errors(gs, cs, cfg)
     print("autotuned", steps, k, c, {key: f"{v:.1e}" for key, v in errs.items()})
     assert max(errs.values()) <= 1e-9
+
+
+def test_batch_member_with_external_source(gpu_lib):
+    """A run with an external current source advances in a batch (eager steps: its source times
+    are per step) exactly as alone."""
+    import os
+
+    from state_io import read_state
+
+    golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    cfgs = [h.configs.parity_p5(), h.configs.parity_p1()]
+    inits = [read_state(os.path.join(golden, f"{c.name}.init.bin")) for c in cfgs]
+    alone = []
+    for c, st in zip(cfgs, inits):
+        with h.Run(c, gpu_lib) as r:
+            r.upload_state(st)
+            r.advance(10)
+            alone.append(r.state())
+    runs = [h.Run(c, gpu_lib) for c in cfgs]
+    try:
+        for r, st in zip(runs, inits):
+            r.upload_state(st)
+        with h.abi.Batch(runs) as b:
+            b.configure(sort_interval=4)
+            b.advance(10)
+            assert b.stats()["graph_launches"] == 0
+            together = [r.state() for r in runs]
+    finally:
+        for r in runs:
+            r.close()
+    for c, a, t in zip(cfgs, alone, together):
+        assert max(_field_errs(t, a, c).values()) <= 1e-12
