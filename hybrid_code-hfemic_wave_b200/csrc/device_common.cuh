@@ -14,6 +14,8 @@
 namespace h1d {
 
 constexpr int PAD = 3;
+// floats per cell of the FP32 push record {Ex, Ey, Ez, dBx, dBy, dBz, 0, 0}: two 16-byte loads per node
+constexpr int EBF_STRIDE = 8;
 
 // device status word bits; read by the host after each advance
 enum : unsigned {

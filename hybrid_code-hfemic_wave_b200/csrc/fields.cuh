@@ -236,7 +236,7 @@ __device__ __forceinline__ void put_eb(double *eb, float *ebf, Cell const &C, in
         if (withB)
             p[3] = Bh.x, p[4] = Bh.y, p[5] = Bh.z;
         if (ebf) {
-            float *f = ebf + 6 * i;
+            float *f = ebf + EBF_STRIDE * i;
             f[0] = static_cast<float>(E.x), f[1] = static_cast<float>(E.y), f[2] = static_cast<float>(E.z);
             if (withB)
                 f[3] = static_cast<float>(Bh.x), f[4] = static_cast<float>(Bh.y), f[5] = static_cast<float>(Bh.z);

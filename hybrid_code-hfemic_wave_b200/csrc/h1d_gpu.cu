@@ -316,7 +316,7 @@ PushArgsMixed mixed_args(h1d_run *run, int s, PushArgs const &a)
     PushArgsMixed m{};
     m.cell = S.cell[S.cur], m.off = S.fbuf[S.cur][0], m.vx = S.fbuf[S.cur][1], m.vy = S.fbuf[S.cur][2];
     m.vz = S.fbuf[S.cur][3], m.w = S.fbuf[S.cur][4], m.pid = S.pid[S.cur], m.n = a.n, m.Nx = a.Nx;
-    m.EB = run->EBf + 6 * PAD;
+    m.EB = run->EBf + EBF_STRIDE * PAD;
     for (int d = 0; d < 2; ++d)
         for (int q = 0; q < 4; ++q)
             m.dep[d][q] = a.dep[d][q];
@@ -431,7 +431,7 @@ FieldArgs field_args(h1d_run *run)
     a.geo = run->geo;
     a.B_in = run->B[run->fcur] + 3 * PAD, a.E_in = run->E[run->fcur] + 3 * PAD;
     a.B_out = run->B[1 - run->fcur] + 3 * PAD, a.E_out = run->E[1 - run->fcur] + 3 * PAD;
-    a.EB_out = run->EB + 6 * PAD, a.EBf_out = run->EBf ? run->EBf + 6 * PAD : nullptr, a.charge_out = run->charge + PAD, a.current_out = run->current + 3 * PAD;
+    a.EB_out = run->EB + 6 * PAD, a.EBf_out = run->EBf ? run->EBf + EBF_STRIDE * PAD : nullptr, a.charge_out = run->charge + PAD, a.current_out = run->current + 3 * PAD;
     a.nk = p.n_kinetic, a.nc = p.n_cold;
     for (int s = 0; s < p.n_kinetic; ++s) {
         h1d_kinetic_desc const &d = p.kinetic[s];
@@ -475,7 +475,7 @@ FieldArgs field_args(h1d_run *run)
 int prepare_fields(h1d_run *run)
 {
     CU(launch_prep_fields(run->B[run->fcur] + 3 * PAD, run->E[run->fcur] + 3 * PAD, run->EB + 6 * PAD,
-                          run->EBf ? run->EBf + 6 * PAD : nullptr, static_cast<int>(run->Nx), run->stream));
+                          run->EBf ? run->EBf + EBF_STRIDE * PAD : nullptr, static_cast<int>(run->Nx), run->stream));
     run->fields_dirty = false;
     return H1D_OK;
 }
@@ -1260,7 +1260,7 @@ int h1d_create(h1d_params const *params, h1d_run **out)
         || dalloc(run, &run->charge, M) || dalloc(run, &run->current, 3 * M) || dalloc(run, &run->d_status, 1)
         || dalloc(run, &run->E1[0], 3 * M) || dalloc(run, &run->E1[1], 3 * M) || dalloc(run, &run->d_fallbacks, 1)
         || dalloc(run, &run->d_energy, 6 + 6 * (H1D_MAX_KINETIC + H1D_MAX_COLD))
-        || (run->mixed && dalloc(run, &run->EBf, 6 * M))
+        || (run->mixed && dalloc(run, &run->EBf, EBF_STRIDE * M))
         || (p.n_sources > 0 && dalloc(run, &run->src_dep, 4 * M * p.n_sources)))
         return fail(H1D_ERR_OOM);
     if (cudaMallocHost(&run->h_status, sizeof(unsigned)) != cudaSuccess)

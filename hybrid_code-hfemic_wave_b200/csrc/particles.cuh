@@ -396,6 +396,11 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
         int const     w0    = warp * 32 * PIPE_PPT;
 
         // slots past `cnt` hold stale finite data and are processed but never deposited or stored
+        // the lane's particles are pushed first, then one window check covers all their deposits
+        Shape<O> ds0[PIPE_PPT], ds1[PIPE_PPT];
+        d3       dv0[PIPE_PPT], dv1[PIPE_PPT];
+        double   dw0[PIPE_PPT], dw1[PIPE_PPT];
+        bool     dd0[PIPE_PPT], dd1[PIPE_PPT];
 #pragma unroll
         for (int k = 0; k < PIPE_PPT; ++k) {
             int const    idx   = w0 + k * 32 + lane;
@@ -445,16 +450,23 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
             if (BC == BCK_ABSORBING)
                 P.wn[idx] = w;
 
-            // deposits: at x^N with v^{N+1/2} (before the boundary pass) and at the end position
-            Shape<O> const sh1  = make_shape<O>(q1 - a.half_min);
-            bool const     dep0 = live && in0 && (a.deposit_mask & 1);
-            bool const     dep1 = live && (a.deposit_mask & 2) && w != 0.0 && finite_pos(q1) && stencil_ok(sh1, a.Nx);
-            int            lo = 0x7fffffff, hi = -0x7fffffff;
-            if (dep0)
-                lo = min(lo, sh0.i0), hi = max(hi, sh0.i0);
-            if (dep1)
-                lo = min(lo, sh1.i0), hi = max(hi, sh1.i0);
-            bool const outside = (dep0 || dep1) && (lo < win.base || hi > win.base + SPAN);
+            ds0[k] = sh0;
+            ds1[k] = make_shape<O>(q1 - a.half_min);
+            dd0[k] = live && in0 && (a.deposit_mask & 1);
+            dd1[k] = live && (a.deposit_mask & 2) && w != 0.0 && finite_pos(q1) && stencil_ok(ds1[k], a.Nx);
+            dv0[k] = v_push, dw0[k] = w_in;
+            dv1[k] = v, dw1[k] = w;
+        }
+        {
+            int lo = 0x7fffffff, hi = -0x7fffffff;
+#pragma unroll
+            for (int k = 0; k < PIPE_PPT; ++k) {
+                if (dd0[k])
+                    lo = min(lo, ds0[k].i0), hi = max(hi, ds0[k].i0);
+                if (dd1[k])
+                    lo = min(lo, ds1[k].i0), hi = max(hi, ds1[k].i0);
+            }
+            bool const outside = lo <= hi && (lo < win.base || hi > win.base + SPAN);
             if (__any_sync(0xffffffffu, outside)) { // move the window onto this batch
                 win.flush(lane, a);
                 int const mlo = __reduce_min_sync(0xffffffffu, lo);
@@ -462,19 +474,22 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
                 int const gap = SPAN - (mhi - mlo);
                 win.base      = gap > 0 ? mlo - gap / 2 : mlo;
             }
-            if (dep0) {
-                double const vw[4] = { w_in, v_push.x * w_in, v_push.y * w_in, v_push.z * w_in };
-                if (sh0.i0 >= win.base && sh0.i0 <= win.base + SPAN)
-                    win.add<O>(0, sh0, vw, lane);
-                else
-                    deposit_direct<O>(a, 0, sh0, vw);
-            }
-            if (dep1) {
-                double const vw[4] = { w, v.x * w, v.y * w, v.z * w };
-                if (sh1.i0 >= win.base && sh1.i0 <= win.base + SPAN)
-                    win.add<O>(1, sh1, vw, lane);
-                else
-                    deposit_direct<O>(a, 1, sh1, vw);
+#pragma unroll
+            for (int k = 0; k < PIPE_PPT; ++k) {
+                if (dd0[k]) {
+                    double const vw[4] = { dw0[k], dv0[k].x * dw0[k], dv0[k].y * dw0[k], dv0[k].z * dw0[k] };
+                    if (ds0[k].i0 >= win.base && ds0[k].i0 <= win.base + SPAN)
+                        win.add<O>(0, ds0[k], vw, lane);
+                    else
+                        deposit_direct<O>(a, 0, ds0[k], vw);
+                }
+                if (dd1[k]) {
+                    double const vw[4] = { dw1[k], dv1[k].x * dw1[k], dv1[k].y * dw1[k], dv1[k].z * dw1[k] };
+                    if (ds1[k].i0 >= win.base && ds1[k].i0 <= win.base + SPAN)
+                        win.add<O>(1, ds1[k], vw, lane);
+                    else
+                        deposit_direct<O>(a, 1, ds1[k], vw);
+                }
             }
         }
         fence_proxy_async_smem();

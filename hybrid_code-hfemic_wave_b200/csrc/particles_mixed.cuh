@@ -18,7 +18,7 @@ struct PushArgsMixed {
     int32_t const *pid;
     int64_t      n;
     int          Nx;
-    float const *EB; // per cell {Ex, Ey, Ez, dBx, dBy, dBz} in FP32, pointer at interior cell 0
+    float const *EB; // per cell {Ex, Ey, Ez, dBx, dBy, dBz, 0, 0} in FP32 (EBF_STRIDE), at interior cell 0
     double      *dep[2][4];
     float        full_min, xiD1, inv_D1, O0, dt, travel_scale, xiO0_Oc, dtOc_2O0, cDtOc_2O0;
     unsigned    *status;
@@ -387,6 +387,10 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
         PipeStageMixed &P     = stage[s];
         int const       w0    = warp * 32 * MIX_PPT;
 
+        // the lane's particles are pushed first, then one window check covers all their deposits
+        ShapeF<O> ds0[MIX_PPT], ds1[MIX_PPT];
+        float4    dv0[MIX_PPT], dv1[MIX_PPT];
+        bool      dd0[MIX_PPT], dd1[MIX_PPT];
 #pragma unroll
         for (int k = 0; k < MIX_PPT; ++k) {
             int const idx   = w0 + k * 32 + lane;
@@ -420,13 +424,12 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                     f3 E = { 0, 0, 0 }, dB = { 0, 0, 0 };
 #pragma unroll
                     for (int j = 0; j <= O; ++j) {
-                        float const *p  = a.EB + 6 * (sh0.i0 + j);
-                        float2 const x0 = __ldg(reinterpret_cast<float2 const *>(p));
-                        float2 const x1 = __ldg(reinterpret_cast<float2 const *>(p + 2));
-                        float2 const x2 = __ldg(reinterpret_cast<float2 const *>(p + 4));
+                        float const *p  = a.EB + EBF_STRIDE * (sh0.i0 + j);
+                        float4 const x0 = __ldg(reinterpret_cast<float4 const *>(p));
+                        float4 const x1 = __ldg(reinterpret_cast<float4 const *>(p + 4));
                         float const  wj = sh0.w[j];
-                        E.x += x0.x * wj, E.y += x0.y * wj, E.z += x1.x * wj;
-                        dB.x += x1.y * wj, dB.y += x2.x * wj, dB.z += x2.y * wj;
+                        E.x += x0.x * wj, E.y += x0.y * wj, E.z += x0.z * wj;
+                        dB.x += x0.w * wj, dB.y += x1.x * wj, dB.z += x1.y * wj;
                     }
                     float c2 = 1.0f;
                     f3    B;
@@ -465,16 +468,23 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
             if (BC == BCK_ABSORBING)
                 P.wn[idx] = w;
 
-            // deposits: at x^N with v^{N+1/2} (before the boundary pass) and at the end position
-            ShapeF<O> const sh1  = make_shape_f<O>(cell, off);
-            bool const      dep0 = live && in0 && (a.deposit_mask & 1);
-            bool const      dep1 = live && (a.deposit_mask & 2) && w != 0.0f && stencil_ok_f(sh1, a.Nx);
-            int             lo = 0x7fffffff, hi = -0x7fffffff;
-            if (dep0)
-                lo = min(lo, sh0.i0), hi = max(hi, sh0.i0);
-            if (dep1)
-                lo = min(lo, sh1.i0), hi = max(hi, sh1.i0);
-            bool const outside = (dep0 || dep1) && (lo < win.base || hi > win.base + SPAN);
+            ds0[k] = sh0;
+            ds1[k] = make_shape_f<O>(cell, off);
+            dd0[k] = live && in0 && (a.deposit_mask & 1);
+            dd1[k] = live && (a.deposit_mask & 2) && w != 0.0f && stencil_ok_f(ds1[k], a.Nx);
+            dv0[k] = make_float4(w_in, v_push.x * w_in, v_push.y * w_in, v_push.z * w_in);
+            dv1[k] = make_float4(w, v.x * w, v.y * w, v.z * w);
+        }
+        {
+            int lo = 0x7fffffff, hi = -0x7fffffff;
+#pragma unroll
+            for (int k = 0; k < MIX_PPT; ++k) {
+                if (dd0[k])
+                    lo = min(lo, ds0[k].i0), hi = max(hi, ds0[k].i0);
+                if (dd1[k])
+                    lo = min(lo, ds1[k].i0), hi = max(hi, ds1[k].i0);
+            }
+            bool const outside = lo <= hi && (lo < win.base || hi > win.base + SPAN);
             if (__any_sync(0xffffffffu, outside)) { // move the window onto this batch
                 win.flush(lane, a);
                 int const mlo = __reduce_min_sync(0xffffffffu, lo);
@@ -482,19 +492,20 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                 int const gap = SPAN - (mhi - mlo);
                 win.base      = gap > 0 ? mlo - gap / 2 : mlo;
             }
-            if (dep0) {
-                float4 const vw = make_float4(w_in, v_push.x * w_in, v_push.y * w_in, v_push.z * w_in);
-                if (sh0.i0 >= win.base && sh0.i0 <= win.base + SPAN)
-                    win.add<O>(0, sh0, vw, lane);
-                else
-                    deposit_direct<O>(a, 0, sh0, vw);
-            }
-            if (dep1) {
-                float4 const vw = make_float4(w, v.x * w, v.y * w, v.z * w);
-                if (sh1.i0 >= win.base && sh1.i0 <= win.base + SPAN)
-                    win.add<O>(1, sh1, vw, lane);
-                else
-                    deposit_direct<O>(a, 1, sh1, vw);
+#pragma unroll
+            for (int k = 0; k < MIX_PPT; ++k) {
+                if (dd0[k]) {
+                    if (ds0[k].i0 >= win.base && ds0[k].i0 <= win.base + SPAN)
+                        win.add<O>(0, ds0[k], dv0[k], lane);
+                    else
+                        deposit_direct<O>(a, 0, ds0[k], dv0[k]);
+                }
+                if (dd1[k]) {
+                    if (ds1[k].i0 >= win.base && ds1[k].i0 <= win.base + SPAN)
+                        win.add<O>(1, ds1[k], dv1[k], lane);
+                    else
+                        deposit_direct<O>(a, 1, ds1[k], dv1[k]);
+                }
             }
         }
         fence_proxy_async_smem();

@@ -37,7 +37,7 @@ __global__ void prep_fields_kernel(double *B, double *E, double *EB, float *EBf,
     }
     if (EBf)
         for (int c = 0; c < 6; ++c)
-            EBf[6 * i + c] = static_cast<float>(p[c]);
+            EBf[EBF_STRIDE * i + c] = static_cast<float>(p[c]);
     if (i < 0 || i >= Nx) {
         st3(B, i, ld3(B, wrap(i, Nx)));
         st3(E, i, e);
