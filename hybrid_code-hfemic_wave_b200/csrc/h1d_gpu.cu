@@ -357,9 +357,9 @@ int sort_species(h1d_run *run, int s)
         return H1D_OK;
     cudaStream_t const st     = run->stream;
     int const          Nx     = static_cast<int>(run->Nx);
-    int const          passes = Nx < 256 ? 1 : 2; // keys in [0, Nx] (Nx = absorbed)
+    SortPlan const     plan   = sort_plan(Nx);
     int64_t const      ntiles = (S.n + SORT_TILE - 1) / SORT_TILE;
-    int64_t const      hlen   = 256 * ntiles;
+    int64_t const      hlen   = (int64_t{1} << std::max(plan.bits[0], plan.bits[1])) * ntiles;
     int64_t const      nparts = (hlen + SCAN_SEG - 1) / SCAN_SEG;
     if (hlen > S.hist_cap) {
         cudaFree(S.hist);
@@ -375,42 +375,61 @@ int sort_species(h1d_run *run, int s)
     }
     phase_begin(run, 1);
     CU(cudaMemsetAsync(S.dead, 0, sizeof(unsigned long long), st));
-    unsigned const nb = static_cast<unsigned>((S.n + 255) / 256);
+    unsigned const nt = static_cast<unsigned>(ntiles);
+    int const      ti = static_cast<int>(ntiles);
+    SortKeys       first{};
+    first.full_min = -0.5 * Nx, first.Nx = Nx, first.dead = S.dead, first.status = run->d_status;
     if (run->mixed)
-        keys_kernel_mixed<<<nb, 256, 0, st>>>(S.cell[S.cur], S.fbuf[S.cur][4], S.n, Nx, S.keys[0], S.idx[0], S.dead,
-                                              run->d_status);
+        first.cell = S.cell[S.cur], first.wf = S.fbuf[S.cur][4];
     else
-        keys_kernel<<<nb, 256, 0, st>>>(S.buf[S.cur][0], S.buf[S.cur][4], S.n, -0.5 * Nx, Nx, S.keys[0], S.idx[0],
-                                        S.dead, run->d_status);
-    int src = 0;
-    for (int pass = 0; pass < passes; ++pass) {
-        int const shift = 8 * pass;
-        hist_kernel<<<static_cast<unsigned>(ntiles), SORT_THREADS, 0, st>>>(S.keys[src], S.n, shift,
-                                                                            static_cast<int>(ntiles), S.hist);
-        scan_reduce_kernel<<<static_cast<unsigned>(nparts), SCAN_THREADS, 0, st>>>(S.hist, hlen, S.part);
-        scan_partials_kernel<<<1, 1024, 0, st>>>(S.part, static_cast<int>(nparts));
-        scan_down_kernel<<<static_cast<unsigned>(nparts), SCAN_THREADS, 0, st>>>(S.hist, hlen, S.part);
-        scatter_kernel<<<static_cast<unsigned>(ntiles), SORT_THREADS, 0, st>>>(
-            S.keys[src], S.idx[src], pass == 0, S.n, shift, static_cast<int>(ntiles), S.hist, S.keys[1 - src],
-            S.idx[1 - src]);
+        first.q1 = S.buf[S.cur][0], first.w = S.buf[S.cur][4];
+    MoveMixed mm{};
+    MoveFP64  md{};
+    for (int k = 0; k < 5; ++k) {
+        mm.src[k] = S.fbuf[S.cur][k], mm.dst[k] = S.fbuf[1 - S.cur][k];
+        md.src[k] = S.buf[S.cur][k], md.dst[k] = S.buf[1 - S.cur][k];
+    }
+    mm.cell_src = S.cell[S.cur], mm.cell_dst = S.cell[1 - S.cur];
+    mm.pid_src = md.pid_src = S.pid[S.cur];
+    mm.pid_dst = md.pid_dst = S.pid[1 - S.cur];
+    int shift = 0, src = 0; // keys/idx buffer the current pass reads (the first pass reads the particles)
+    for (int pass = 0; pass < plan.passes; ++pass) {
+        unsigned const mask = (1u << plan.bits[pass]) - 1u;
+        int64_t const  len  = static_cast<int64_t>(mask + 1) * ntiles;
+        unsigned const np   = static_cast<unsigned>((len + SCAN_SEG - 1) / SCAN_SEG);
+        bool const     last = pass == plan.passes - 1;
+        SortKeys       keys = first;
+        keys.keys           = S.keys[src];
+        if (pass > 0)
+            hist_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, S.n, shift, mask, ti, S.hist);
+        else if (run->mixed)
+            hist_kernel<KEYS_MIXED><<<nt, SORT_THREADS, 0, st>>>(keys, S.n, shift, mask, ti, S.hist);
+        else
+            hist_kernel<KEYS_FP64><<<nt, SORT_THREADS, 0, st>>>(keys, S.n, shift, mask, ti, S.hist);
+        scan_reduce_kernel<<<np, SCAN_THREADS, 0, st>>>(S.hist, len, S.part);
+        scan_partials_kernel<<<1, 1024, 0, st>>>(S.part, static_cast<int>(np));
+        scan_down_kernel<<<np, SCAN_THREADS, 0, st>>>(S.hist, len, S.part);
+        MoveKeys const mk{S.keys[1 - src], S.idx[1 - src]};
+        uint32_t const *idx = S.idx[src];
+        if (pass > 0 && !last)
+            scatter_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mk);
+        else if (pass > 0 && run->mixed)
+            scatter_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mm);
+        else if (pass > 0)
+            scatter_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, md);
+        else if (run->mixed && !last)
+            scatter_kernel<KEYS_MIXED><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mk);
+        else if (run->mixed)
+            scatter_kernel<KEYS_MIXED><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mm);
+        else if (!last)
+            scatter_kernel<KEYS_FP64><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mk);
+        else
+            scatter_kernel<KEYS_FP64><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, md);
+        shift += plan.bits[pass];
         src = 1 - src;
     }
-    if (run->mixed) {
-        GatherArgsMixed g{};
-        for (int k = 0; k < 5; ++k)
-            g.src[k] = S.fbuf[S.cur][k], g.dst[k] = S.fbuf[1 - S.cur][k];
-        g.cell_src = S.cell[S.cur], g.cell_dst = S.cell[1 - S.cur];
-        g.pid_src = S.pid[S.cur], g.pid_dst = S.pid[1 - S.cur], g.idx = S.idx[src], g.n = S.n;
-        gather_kernel_mixed<<<nb, 256, 0, st>>>(g);
-    } else {
-        GatherArgs g{};
-        for (int k = 0; k < 5; ++k)
-            g.src[k] = S.buf[S.cur][k], g.dst[k] = S.buf[1 - S.cur][k];
-        g.pid_src = S.pid[S.cur], g.pid_dst = S.pid[1 - S.cur], g.idx = S.idx[src], g.n = S.n;
-        gather_kernel<<<nb, 256, 0, st>>>(g);
-    }
     CU(cudaGetLastError());
-    phase_end(run, 2 + 5 * passes);
+    phase_end(run, 5 * plan.passes);
     S.cur = 1 - S.cur;
     if (run->p.particle_bc == H1D_BC_ABSORBING) { // trim removed particles (sorted to the end)
         unsigned long long dead = 0;
@@ -905,9 +924,8 @@ int batch_step(h1d_batch *b)
     if (b->since_block >= b->k) {
         for (h1d_run *r : b->runs)
             for (int s = 0; s < r->p.n_kinetic; ++s) {
-                int const passes = r->Nx < 256 ? 1 : 2;
                 BTRY(r, sort_species(r, s));
-                b->stats.kernel_launches += r->sp[s].n > 0 ? 2 + 5 * passes : 0;
+                b->stats.kernel_launches += r->sp[s].n > 0 ? 5 * sort_plan(static_cast<int>(r->Nx)).passes : 0;
             }
         b->since_block = 0;
     }

@@ -193,49 +193,6 @@ __global__ void from_mixed_kernel(int32_t const *cell, float const *src, int64_t
     dst[i] = cell ? full_min + static_cast<double>(cell[i]) + static_cast<double>(src[i]) : static_cast<double>(src[i]);
 }
 
-// keys for the cell sort of mixed-precision particles (sort.cuh): the cell itself
-__global__ void keys_kernel_mixed(int32_t const *cell, float const *w, int64_t n, int Nx, uint32_t *keys, uint32_t *idx,
-                                  unsigned long long *dead, unsigned *status)
-{
-    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
-    int const c = cell[i];
-    uint32_t  k;
-    if (w[i] == 0.0f) {
-        k = static_cast<uint32_t>(Nx);
-        atomicAdd(dead, 1ull);
-    } else if (c < 0 || c >= Nx) {
-        k = c < 0 ? 0u : static_cast<uint32_t>(Nx - 1);
-        atomicOr(status, ST_OUT_OF_RANGE);
-    } else {
-        k = static_cast<uint32_t>(c);
-    }
-    keys[i] = k;
-    idx[i]  = static_cast<uint32_t>(i);
-}
-
-struct GatherArgsMixed {
-    float const   *src[5]; // off, vx, vy, vz, w
-    int32_t const *cell_src, *pid_src;
-    float         *dst[5];
-    int32_t       *cell_dst, *pid_dst;
-    uint32_t const *idx;
-    int64_t        n;
-};
-__global__ void gather_kernel_mixed(GatherArgsMixed a)
-{
-    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= a.n)
-        return;
-    uint32_t const j = a.idx[i];
-#pragma unroll
-    for (int k = 0; k < 5; ++k)
-        a.dst[k][i] = a.src[k][j];
-    a.cell_dst[i] = a.cell_src[j];
-    a.pid_dst[i]  = a.pid_src[j];
-}
-
 // ------------------------------------------------------------------------------------------------
 // Device loader of a bi-Maxwellian species (PartSpecies::populate with MaxwellianVDF::load,
 // VDF/MaxwellianVDF.cc:300-319, q1_of_N :240-250, eta :218-228).  Particle i uses the radical

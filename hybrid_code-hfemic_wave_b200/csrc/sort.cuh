@@ -7,12 +7,19 @@
 // move to the end, where the host trims them.  Sorting is stable, so the order is reproducible
 // and equals std::stable_sort by key on the host.
 //
-// Passes of 8 bits over (key, index) pairs:
-//   keys_kernel      key per particle, identity index
-//   hist_kernel      per-tile digit histograms, stored digit-major [256][tiles]
+// Keys lie in [0, Nx], so ceil(log2(Nx + 1)) bits are sorted, in one pass (up to 8 bits) or two
+// passes of about half the bits each.  Between sorts particles drift by a fraction of a cell to a
+// few cells, so the keys arrive nearly sorted and a tile holds a few distinct digits:
+//   hist_kernel      per-tile digit histograms, stored digit-major [radix][tiles]; each warp adds
+//                    one count per distinct digit of 32 keys (__match_any_sync), so equal digits
+//                    do not serialise on a shared-memory atomic
 //   scan (3 kernels) exclusive prefix over the histogram matrix
-//   scatter_kernel   stable rank within each tile (warp match + per-warp digit counts), scatter
-// then gather_kernel permutes the particle arrays by the sorted index.
+//   scatter_kernel   stable rank within each tile: each warp ranks its own 256 contiguous keys
+//                    (match groups, a per-warp running count per digit), one block-wide prefix
+//                    over the warps' counts, then every item goes to its place
+// The first pass reads the keys straight from the particles and counts absorbed particles; the
+// last pass moves the particle records themselves (no separate index array and gather).  Each
+// thread issues all of its loads before it ranks, so a warp keeps 8 loads in flight.
 #pragma once
 
 #include "device_common.cuh"
@@ -26,43 +33,121 @@ constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_ITEMS   = 16;
 constexpr int SCAN_SEG     = SCAN_THREADS * SCAN_ITEMS;
 
-__global__ void keys_kernel(double const *q1, double const *w, int64_t n, double full_min, int Nx, uint32_t *keys,
-                            uint32_t *idx, unsigned long long *dead, unsigned *status)
+// digit widths of the passes: keys in [0, Nx] need ceil(log2(Nx + 1)) bits (Nx <= 65535)
+struct SortPlan {
+    int passes, bits[2];
+};
+inline SortPlan sort_plan(int Nx)
 {
-    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
-    double const q = q1[i];
-    double const f = floor(q - full_min);
-    uint32_t     k;
-    if (w[i] == 0.0) {
-        k = static_cast<uint32_t>(Nx);
-        atomicAdd(dead, 1ull);
-    } else if (!(f >= 0.0 && f < static_cast<double>(Nx))) {
-        k = f >= 0.0 ? static_cast<uint32_t>(Nx - 1) : 0u; // lost particle: keep it in range, flag it
-        atomicOr(status, ST_OUT_OF_RANGE);
-    } else {
-        k = static_cast<uint32_t>(f);
-    }
-    keys[i] = k;
-    idx[i]  = static_cast<uint32_t>(i);
+    int nbits = 1;
+    while ((1 << nbits) <= Nx)
+        ++nbits;
+    if (nbits <= 8)
+        return {1, {nbits, 0}};
+    return {2, {(nbits + 1) / 2, nbits / 2}};
 }
 
-__global__ void __launch_bounds__(SORT_THREADS) hist_kernel(uint32_t const *keys, int64_t n, int shift, int ntiles,
-                                                            uint32_t *hist)
+// where a pass reads its keys: the key array of the previous pass, or (first pass) the particles
+struct SortKeys {
+    uint32_t const     *keys;   // KEYS_ARRAY
+    double const       *q1, *w; // KEYS_FP64
+    int32_t const      *cell;   // KEYS_MIXED
+    float const        *wf;
+    double              full_min;
+    int                 Nx;
+    unsigned long long *dead;   // absorbed particles, counted once by the first histogram
+    unsigned           *status;
+};
+enum { KEYS_ARRAY = 0, KEYS_FP64 = 1, KEYS_MIXED = 2 };
+
+template <int KIND> struct KeyRaw;
+template <> struct KeyRaw<KEYS_ARRAY> {
+    uint32_t k;
+};
+template <> struct KeyRaw<KEYS_FP64> {
+    double q, w;
+};
+template <> struct KeyRaw<KEYS_MIXED> {
+    int32_t c;
+    float   w;
+};
+
+template <int KIND>
+__device__ __forceinline__ KeyRaw<KIND> key_load(SortKeys const &s, int64_t i)
+{
+    if constexpr (KIND == KEYS_ARRAY)
+        return {s.keys[i]};
+    else if constexpr (KIND == KEYS_FP64)
+        return {s.q1[i], s.w[i]};
+    else
+        return {s.cell[i], s.wf[i]};
+}
+
+// the key of a loaded item; with `account`, absorbed particles are counted and lost ones flagged
+template <int KIND>
+__device__ __forceinline__ uint32_t key_of(SortKeys const &s, KeyRaw<KIND> const &r, bool account)
+{
+    if constexpr (KIND == KEYS_ARRAY) {
+        return r.k;
+    } else {
+        bool     dead, lost;
+        uint32_t k;
+        if constexpr (KIND == KEYS_FP64) {
+            double const f = floor(r.q - s.full_min);
+            dead           = r.w == 0.0;
+            lost           = !(f >= 0.0 && f < static_cast<double>(s.Nx));
+            k              = lost ? (f >= 0.0 ? static_cast<uint32_t>(s.Nx - 1) : 0u) : static_cast<uint32_t>(f);
+        } else {
+            dead = r.w == 0.0f;
+            lost = r.c < 0 || r.c >= s.Nx;
+            k    = lost ? (r.c < 0 ? 0u : static_cast<uint32_t>(s.Nx - 1)) : static_cast<uint32_t>(r.c);
+        }
+        if (dead)
+            k = static_cast<uint32_t>(s.Nx);
+        if (account) {
+            if (dead)
+                atomicAdd(s.dead, 1ull);
+            else if (lost) // a lost particle stays in range and is flagged
+                atomicOr(s.status, ST_OUT_OF_RANGE);
+        }
+        return k;
+    }
+}
+
+// warp w of a tile owns items [w0, w0 + 256); round r of lane l is item w0 + 32 r + l, so the
+// rounds visit the warp's items in index order
+__device__ __forceinline__ int64_t sort_warp_base()
+{
+    return static_cast<int64_t>(blockIdx.x) * SORT_TILE + (threadIdx.x >> 5) * 32 * SORT_ITEMS;
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(SORT_THREADS)
+    hist_kernel(SortKeys s, int64_t n, int shift, unsigned mask, int ntiles, uint32_t *hist)
 {
     __shared__ uint32_t h[256];
     h[threadIdx.x] = 0;
-    __syncthreads();
-    int64_t const t0 = static_cast<int64_t>(blockIdx.x) * SORT_TILE;
+    int const     lane = threadIdx.x & 31;
+    int64_t const w0   = sort_warp_base();
+    KeyRaw<KIND>  raw[SORT_ITEMS];
 #pragma unroll
-    for (int k = 0; k < SORT_ITEMS; ++k) {
-        int64_t const i = t0 + k * SORT_THREADS + threadIdx.x;
+    for (int r = 0; r < SORT_ITEMS; ++r) {
+        int64_t const i = w0 + r * 32 + lane;
         if (i < n)
-            atomicAdd(&h[(keys[i] >> shift) & 255u], 1u);
+            raw[r] = key_load<KIND>(s, i);
     }
     __syncthreads();
-    hist[static_cast<int64_t>(threadIdx.x) * ntiles + blockIdx.x] = h[threadIdx.x];
+#pragma unroll
+    for (int r = 0; r < SORT_ITEMS; ++r) {
+        bool const     valid = w0 + r * 32 + lane < n;
+        unsigned const digit = valid ? (key_of<KIND>(s, raw[r], true) >> shift) & mask : 256u + lane;
+        unsigned const m     = __match_any_sync(0xffffffffu, digit);
+        if (valid && lane == __ffs(m) - 1)
+            atomicAdd(&h[digit], static_cast<uint32_t>(__popc(m)));
+    }
+    __syncthreads();
+    if (threadIdx.x <= mask)
+        hist[static_cast<int64_t>(threadIdx.x) * ntiles + blockIdx.x] = h[threadIdx.x];
 }
 
 // block-wide exclusive scan of one value per thread; returns the block total
@@ -160,73 +245,153 @@ __global__ void __launch_bounds__(SCAN_THREADS) scan_down_kernel(uint32_t *data,
     }
 }
 
-__global__ void __launch_bounds__(SORT_THREADS) scatter_kernel(uint32_t const *keys_in, uint32_t const *idx_in,
-                                                               int identity_idx, int64_t n, int shift, int ntiles,
-                                                               uint32_t const *offsets, uint32_t *keys_out,
-                                                               uint32_t *idx_out)
-{
-    constexpr int       NW = SORT_THREADS / 32;
-    __shared__ uint32_t base[256];      // global offset of each digit for this tile + running count
-    __shared__ uint32_t wcnt[NW][256];  // per-warp digit counts of the current round -> exclusive prefix
-    int const           lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    base[threadIdx.x]        = offsets[static_cast<int64_t>(threadIdx.x) * ntiles + blockIdx.x];
-    int64_t const t0         = static_cast<int64_t>(blockIdx.x) * SORT_TILE;
-    for (int r = 0; r < SORT_ITEMS; ++r) {
-#pragma unroll
-        for (int w = 0; w < NW; ++w)
-            wcnt[w][threadIdx.x] = 0;
-        __syncthreads();
-        int64_t const i     = t0 + r * SORT_THREADS + threadIdx.x;
-        bool const    valid = i < n;
-        uint32_t      key = 0, id = 0, digit = 256 + lane; // invalid lanes get unique non-digits
-        if (valid) {
-            key   = keys_in[i];
-            id    = identity_idx ? static_cast<uint32_t>(i) : idx_in[i];
-            digit = (key >> shift) & 255u;
-        }
-        unsigned const peers = __match_any_sync(0xffffffffu, digit);
-        unsigned const rank  = __popc(peers & ((1u << lane) - 1u));
-        if (valid && rank == 0)
-            wcnt[wid][digit] = __popc(peers);
-        __syncthreads();
-        { // exclusive prefix over warps for digit threadIdx.x, and advance the running base
-            uint32_t run = 0;
-#pragma unroll
-            for (int w = 0; w < NW; ++w) {
-                uint32_t const c = wcnt[w][threadIdx.x];
-                wcnt[w][threadIdx.x] = run;
-                run += c;
-            }
-            __syncthreads();
-            if (valid) {
-                uint32_t const pos = base[digit] + wcnt[wid][digit] + rank;
-                keys_out[pos]      = key;
-                idx_out[pos]       = id;
-            }
-            __syncthreads();
-            base[threadIdx.x] += run;
-        }
+// what the scatter of a pass writes: (key, index) pairs for the next pass ...
+// HOLD: how many of a thread's records are loaded before the block-wide barrier (registers)
+struct MoveKeys {
+    static constexpr int HOLD = SORT_ITEMS;
+    uint32_t            *keys_out, *idx_out;
+    struct Rec {
+        uint32_t key, id;
+    };
+    __device__ __forceinline__ Rec  load(uint32_t key, uint32_t id) const { return {key, id}; }
+    __device__ __forceinline__ void store(uint32_t pos, Rec const &r) const
+    {
+        keys_out[pos] = r.key;
+        idx_out[pos]  = r.id;
     }
-}
-
-struct GatherArgs {
-    double const  *src[5];
+};
+// ... or, in the last pass, the FP64 particle records (q1, vx, vy, vz, w, pid)
+struct MoveFP64 {
+    static constexpr int HOLD = SORT_ITEMS / 2;
+    double const        *src[5];
     int32_t const *pid_src;
     double        *dst[5];
     int32_t       *pid_dst;
-    uint32_t const *idx;
-    int64_t        n;
-};
-__global__ void gather_kernel(GatherArgs a)
-{
-    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= a.n)
-        return;
-    uint32_t const j = a.idx[i];
+    struct Rec {
+        double  v[5];
+        int32_t pid;
+    };
+    __device__ __forceinline__ Rec load(uint32_t, uint32_t j) const
+    {
+        Rec r;
 #pragma unroll
-    for (int k = 0; k < 5; ++k)
-        a.dst[k][i] = a.src[k][j];
-    a.pid_dst[i] = a.pid_src[j];
+        for (int k = 0; k < 5; ++k)
+            r.v[k] = src[k][j];
+        r.pid = pid_src[j];
+        return r;
+    }
+    __device__ __forceinline__ void store(uint32_t pos, Rec const &r) const
+    {
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+            dst[k][pos] = r.v[k];
+        pid_dst[pos] = r.pid;
+    }
+};
+// ... or the mixed-precision records (offset, vx, vy, vz, w as FP32; cell, pid)
+struct MoveMixed {
+    static constexpr int HOLD = SORT_ITEMS;
+    float const         *src[5];
+    int32_t const *cell_src, *pid_src;
+    float         *dst[5];
+    int32_t       *cell_dst, *pid_dst;
+    struct Rec {
+        float   v[5];
+        int32_t cell, pid;
+    };
+    __device__ __forceinline__ Rec load(uint32_t, uint32_t j) const
+    {
+        Rec r;
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+            r.v[k] = src[k][j];
+        r.cell = cell_src[j];
+        r.pid  = pid_src[j];
+        return r;
+    }
+    __device__ __forceinline__ void store(uint32_t pos, Rec const &r) const
+    {
+#pragma unroll
+        for (int k = 0; k < 5; ++k)
+            dst[k][pos] = r.v[k];
+        cell_dst[pos] = r.cell;
+        pid_dst[pos]  = r.pid;
+    }
+};
+
+template <int KIND, class Move>
+__global__ void __launch_bounds__(SORT_THREADS)
+    scatter_kernel(SortKeys s, uint32_t const *idx_in, int64_t n, int shift, unsigned mask, int ntiles,
+                   uint32_t const *offsets, Move const mv)
+{
+    constexpr int       NW = SORT_THREADS / 32;
+    __shared__ uint32_t cnt[NW][256]; // per-warp digit counts, then each warp's start per digit
+    int const           lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int64_t const       w0   = sort_warp_base();
+    unsigned const      lt   = (1u << lane) - 1u;
+    KeyRaw<KIND>        raw[SORT_ITEMS];
+    uint32_t            key[SORT_ITEMS], id[SORT_ITEMS], dig[SORT_ITEMS], rank[SORT_ITEMS];
+#pragma unroll
+    for (int r = 0; r < SORT_ITEMS; ++r) {
+        int64_t const i = w0 + r * 32 + lane;
+        id[r]           = static_cast<uint32_t>(i);
+        if (i < n) {
+            raw[r] = key_load<KIND>(s, i);
+            if constexpr (KIND == KEYS_ARRAY)
+                id[r] = idx_in[i];
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+        cnt[wid][j * 32 + lane] = 0;
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < SORT_ITEMS; ++r) { // rank among the warp's earlier items of equal digit
+        bool const valid    = w0 + r * 32 + lane < n;
+        key[r]              = valid ? key_of<KIND>(s, raw[r], false) : 0u;
+        dig[r]              = valid ? (key[r] >> shift) & mask : 256u + lane;
+        unsigned const m    = __match_any_sync(0xffffffffu, dig[r]);
+        int const      lead = __ffs(m) - 1;
+        uint32_t       old  = 0;
+        if (valid && lane == lead) {
+            old              = cnt[wid][dig[r]];
+            cnt[wid][dig[r]] = old + static_cast<uint32_t>(__popc(m));
+        }
+        rank[r] = __shfl_sync(0xffffffffu, old, lead) + static_cast<uint32_t>(__popc(m & lt));
+        __syncwarp();
+    }
+    constexpr int      H = Move::HOLD;
+    typename Move::Rec rec[H]; // records in flight while the block agrees on places
+#pragma unroll
+    for (int r = 0; r < H; ++r)
+        if (w0 + r * 32 + lane < n)
+            rec[r] = mv.load(key[r], id[r]);
+    __syncthreads();
+    if (threadIdx.x <= mask) { // digit threadIdx.x: the tile's global start plus the earlier warps
+        uint32_t run = offsets[static_cast<int64_t>(threadIdx.x) * ntiles + blockIdx.x];
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            uint32_t const c    = cnt[w][threadIdx.x];
+            cnt[w][threadIdx.x] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < H; ++r)
+        if (w0 + r * 32 + lane < n)
+            mv.store(cnt[wid][dig[r]] + rank[r], rec[r]);
+    if constexpr (H < SORT_ITEMS) {
+        typename Move::Rec more[SORT_ITEMS - H];
+#pragma unroll
+        for (int r = H; r < SORT_ITEMS; ++r)
+            if (w0 + r * 32 + lane < n)
+                more[r - H] = mv.load(key[r], id[r]);
+#pragma unroll
+        for (int r = H; r < SORT_ITEMS; ++r)
+            if (w0 + r * 32 + lane < n)
+                mv.store(cnt[wid][dig[r]] + rank[r], more[r - H]);
+    }
 }
 
 } // namespace h1d
