@@ -153,14 +153,15 @@ constexpr int PIPE_CONSUMER_WARPS = 4;
 constexpr int PIPE_THREADS        = 32 * (PIPE_CONSUMER_WARPS + 1);
 constexpr int PIPE_CHUNK          = 256;
 constexpr int PIPE_PPT            = PIPE_CHUNK / (32 * PIPE_CONSUMER_WARPS);
-constexpr int PIPE_STAGES         = 3;
+constexpr int PIPE_STAGES         = 4;
 constexpr int PIPE_CTAS_PER_SM    = 2;
 constexpr int PIPE_W              = 8; // cells per deposit window: 4 quantities x 8 cells = the 32 lanes of a flush
 static_assert(4 * PIPE_W == 32, "a window flush reduce-scatters exactly 32 values");
 
+// a stage holds one chunk; the consumers overwrite it in place with the new state, which the
+// producer then stores
 struct PipeStage {
     double  q1[PIPE_CHUNK], vx[PIPE_CHUNK], vy[PIPE_CHUNK], vz[PIPE_CHUNK], w[PIPE_CHUNK];
-    double  q1n[PIPE_CHUNK], wn[PIPE_CHUNK]; // position and weight after the move
     int32_t pid[PIPE_CHUNK];
 };
 constexpr size_t PIPE_BAR_OFFSET = sizeof(PipeStage) * PIPE_STAGES;
@@ -330,12 +331,12 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
                         int64_t const  start = (c0 + j - G.chunk0[gr]) * PIPE_CHUNK;
                         uint32_t const cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
                         uint32_t const b8    = round16(cnt * 8);
-                        bulk_store(a.q1 + start, stage[s].q1n, b8);
+                        bulk_store(a.q1 + start, stage[s].q1, b8);
                         bulk_store(a.vx + start, stage[s].vx, b8);
                         bulk_store(a.vy + start, stage[s].vy, b8);
                         bulk_store(a.vz + start, stage[s].vz, b8);
                         if (BC == BCK_ABSORBING)
-                            bulk_store(a.w + start, stage[s].wn, b8);
+                            bulk_store(a.w + start, stage[s].w, b8);
                         bulk_commit();
                     }
                     bulk_wait_read_all();
@@ -443,12 +444,12 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
             } else if (live) {
                 bad |= ST_OUT_OF_RANGE;
             }
-            P.q1n[idx] = q1;
+            P.q1[idx]  = q1;
             P.vx[idx]  = v.x;
             P.vy[idx]  = v.y;
             P.vz[idx]  = v.z;
             if (BC == BCK_ABSORBING)
-                P.wn[idx] = w;
+                P.w[idx] = w;
 
             ds0[k] = sh0;
             ds1[k] = make_shape<O>(q1 - a.half_min);

@@ -35,6 +35,25 @@ __device__ __forceinline__ f3 operator+(f3 a, f3 b) { return { a.x + b.x, a.y + 
 __device__ __forceinline__ f3 operator*(f3 a, float s) { return { a.x * s, a.y * s, a.z * s }; }
 __device__ __forceinline__ f3 crossf(f3 A, f3 B) { return { A.y * B.z - A.z * B.y, A.z * B.x - A.x * B.z, A.x * B.y - A.y * B.x }; }
 
+// pairs of FP32 values (a lane's two particles) on the packed FP32 pipe of sm_100
+__device__ __forceinline__ float2 bc(float s) { return make_float2(s, s); }
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 pneg(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float &el(float2 &p, int k) { return k ? p.y : p.x; }
+__device__ __forceinline__ float  el(float2 const &p, int k) { return k ? p.y : p.x; }
+struct p3 {
+    float2 x, y, z;
+};
+__device__ __forceinline__ p3 padd3(p3 a, p3 b) { return { padd(a.x, b.x), padd(a.y, b.y), padd(a.z, b.z) }; }
+// A x B, each component as one multiply and one fused multiply-subtract
+__device__ __forceinline__ p3 pcross(p3 A, p3 B)
+{
+    return { pfma(A.y, B.z, pneg(pmul(A.z, B.y))), pfma(A.z, B.x, pneg(pmul(A.x, B.z))),
+             pfma(A.x, B.y, pneg(pmul(A.y, B.x))) };
+}
+
 // shape weights from the in-cell offset: x - q1min_half = cell - 1/2 + off (Shape.h:24-176)
 template <int O>
 struct ShapeF {
@@ -97,6 +116,27 @@ __device__ __forceinline__ void sincos_taylor_f(float x, float &s, float &c)
     c              = fmaf(-pc, x2, 1.0f);
 }
 
+// sincos_taylor_f of a pair
+__device__ __forceinline__ void sincos_taylor_f2(float2 x, float2 &s, float2 &c)
+{
+    float2 const x2 = pmul(x, x);
+    float2       ps = bc(-1.6059043836821613e-10f);
+    ps              = pfma(ps, x2, bc(2.505210838544172e-08f));
+    ps              = pfma(ps, x2, bc(-2.7557319223985893e-06f));
+    ps              = pfma(ps, x2, bc(0.0001984126984126984f));
+    ps              = pfma(ps, x2, bc(-0.008333333333333333f));
+    ps              = pfma(ps, x2, bc(0.16666666666666666f));
+    s               = pfma(pneg(pmul(ps, x2)), x, x);
+    float2 pc       = bc(1.1470745597729725e-11f);
+    pc              = pfma(pc, x2, bc(-2.08767569878681e-09f));
+    pc              = pfma(pc, x2, bc(2.755731922398589e-07f));
+    pc              = pfma(pc, x2, bc(-2.48015873015873e-05f));
+    pc              = pfma(pc, x2, bc(0.001388888888888889f));
+    pc              = pfma(pc, x2, bc(-0.041666666666666664f));
+    pc              = pfma(pc, x2, bc(0.5f));
+    c               = pfma(pneg(pc), x2, bc(1.0f));
+}
+
 // move by dq cells (|dq| < 1 is checked by the caller); returns the new (cell, off)
 __device__ __forceinline__ void move_cell(int &cell, float &off, float dq)
 {
@@ -157,17 +197,18 @@ __device__ __forceinline__ bool boundary_mixed(PushArgsMixed const &a, int &cell
 // ------------------------------------------------------------------------------------------------
 constexpr int MIX_CHUNK = 256;
 constexpr int MIX_PPT   = MIX_CHUNK / (32 * PIPE_CONSUMER_WARPS);
+static_assert(MIX_PPT == 2, "a lane pushes one pair of particles per chunk");
 constexpr int MIX_W     = 8; // 4 quantities x 8 cells = the 32 lanes of a flush
 static_assert(4 * MIX_W == 32, "a window flush reduce-scatters exactly 32 values");
 
+// a stage holds one chunk; the consumers overwrite it in place with the new state, which the
+// producer then stores
 struct PipeStageMixed {
     int32_t cell[MIX_CHUNK];
     float   off[MIX_CHUNK], vx[MIX_CHUNK], vy[MIX_CHUNK], vz[MIX_CHUNK], w[MIX_CHUNK];
-    int32_t celln[MIX_CHUNK];
-    float   offn[MIX_CHUNK], wn[MIX_CHUNK];
     int32_t pid[MIX_CHUNK];
 };
-constexpr int    PIPE_STAGES_MIXED      = 2;
+constexpr int    PIPE_STAGES_MIXED      = 3;
 constexpr int    PIPE_CTAS_PER_SM_MIXED = 4;
 constexpr size_t MIX_BAR_OFFSET         = sizeof(PipeStageMixed) * PIPE_STAGES_MIXED;
 constexpr size_t MIX_COL_OFFSET         = MIX_BAR_OFFSET + 128; // barriers, then 16-byte aligned columns
@@ -320,13 +361,13 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                         int64_t const  start = (c0 + j - G.chunk0[gr]) * MIX_CHUNK;
                         uint32_t const cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(MIX_CHUNK), a.n - start));
                         uint32_t const b4    = round16(cnt * 4);
-                        bulk_store(a.cell + start, stage[s].celln, b4);
-                        bulk_store(a.off + start, stage[s].offn, b4);
+                        bulk_store(a.cell + start, stage[s].cell, b4);
+                        bulk_store(a.off + start, stage[s].off, b4);
                         bulk_store(a.vx + start, stage[s].vx, b4);
                         bulk_store(a.vy + start, stage[s].vy, b4);
                         bulk_store(a.vz + start, stage[s].vz, b4);
                         if (BC == BCK_ABSORBING)
-                            bulk_store(a.w + start, stage[s].wn, b4);
+                            bulk_store(a.w + start, stage[s].w, b4);
                         bulk_commit();
                     }
                     bulk_wait_read_all();
@@ -387,98 +428,126 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
         PipeStageMixed &P     = stage[s];
         int const       w0    = warp * 32 * MIX_PPT;
 
-        // the lane's particles are pushed first, then one window check covers all their deposits
-        ShapeF<O> ds0[MIX_PPT], ds1[MIX_PPT];
-        float4    dv0[MIX_PPT], dv1[MIX_PPT];
-        bool      dd0[MIX_PPT], dd1[MIX_PPT];
+        // The lane's two particles are adjacent (i2, i2 + 1) and pushed as a pair on the packed
+        // FP32 pipe (one f32x2 instruction per operation of both); then one window check covers
+        // all their deposits.
+        int const  i2      = w0 + 2 * lane;
+        bool const live[2] = { i2 < cnt, i2 + 1 < cnt }; // slots past cnt hold stale data: pushed, never stored or deposited
+        int2 const c_in    = *reinterpret_cast<int2 const *>(P.cell + i2);
+        int        cell[2] = { c_in.x, c_in.y };
+        float2     off     = *reinterpret_cast<float2 const *>(P.off + i2);
+        p3         v       = { *reinterpret_cast<float2 const *>(P.vx + i2), *reinterpret_cast<float2 const *>(P.vy + i2),
+                               *reinterpret_cast<float2 const *>(P.vz + i2) };
+        float2       w    = *reinterpret_cast<float2 const *>(P.w + i2);
+        float2 const w_in = w;
+        int2 const   pid  = load_pid ? *reinterpret_cast<int2 const *>(P.pid + i2) : make_int2(0, 0);
+        bool         alive[2] = { true, true };
+        if (a.move_steps == 2) { // predictor-corrector: half move and boundary before the push
 #pragma unroll
-        for (int k = 0; k < MIX_PPT; ++k) {
-            int const idx   = w0 + k * 32 + lane;
-            bool const live = idx < cnt; // slots past cnt hold stale data: pushed, never stored or deposited
-            int       cell  = P.cell[idx];
-            float     off   = P.off[idx];
-            f3        v     = { P.vx[idx], P.vy[idx], P.vz[idx] };
-            float     w     = P.w[idx];
-            float const w_in = w;
-            int32_t   pid   = load_pid ? P.pid[idx] : 0;
-            bool      alive = true;
-            if (a.move_steps == 2) { // predictor-corrector: half move and boundary before the push
-                float dq = a.inv_D1 * v.x * (0.5f * a.dt);
+            for (int k = 0; k < 2; ++k) {
+                float dq = a.inv_D1 * el(v.x, k) * (0.5f * a.dt);
                 if constexpr (MIRROR) {
                     float s_, c_;
-                    sincos_taylor_f(a.xiD1 * (static_cast<float>(cell) + a.full_min + off), s_, c_);
+                    sincos_taylor_f(a.xiD1 * (static_cast<float>(cell[k]) + a.full_min + el(off, k)), s_, c_);
                     dq *= c_ * c_;
                 }
-                if (live && !(fabsf(dq * a.travel_scale) < 1.0f))
+                if (live[k] && !(fabsf(dq * a.travel_scale) < 1.0f))
                     bad |= ST_MOVED_TOO_FAR;
-                move_cell(cell, off, dq);
-                alive = boundary_mixed<BC>(a, cell, off, v, pid, a.counter);
-                if (!alive)
-                    w = 0.0f, cell = 0, off = 0.5f, v = { 0, 0, 0 };
+                f3 vk = { el(v.x, k), el(v.y, k), el(v.z, k) };
+                move_cell(cell[k], el(off, k), dq);
+                alive[k] = boundary_mixed<BC>(a, cell[k], el(off, k), vk, k ? pid.y : pid.x, a.counter);
+                if (!alive[k])
+                    el(w, k) = 0.0f, cell[k] = 0, el(off, k) = 0.5f, vk = { 0, 0, 0 };
+                el(v.x, k) = vk.x, el(v.y, k) = vk.y, el(v.z, k) = vk.z;
             }
-            ShapeF<O> const sh0    = make_shape_f<O>(cell, off);
-            bool const      in0    = stencil_ok_f(sh0, a.Nx);
-            f3              v_push = v;
-            if (in0) {
-                if (alive && a.move_steps != 0) {
-                    f3 E = { 0, 0, 0 }, dB = { 0, 0, 0 };
+        }
+        ShapeF<O> ds0[2], ds1[2];
+        bool      in0[2], push[2];
+        p3        E = { { 0, 0 }, { 0, 0 }, { 0, 0 } }, dB = E;
 #pragma unroll
-                    for (int j = 0; j <= O; ++j) {
-                        float const *p  = a.EB + EBF_STRIDE * (sh0.i0 + j);
-                        float4 const x0 = __ldg(reinterpret_cast<float4 const *>(p));
-                        float4 const x1 = __ldg(reinterpret_cast<float4 const *>(p + 4));
-                        float const  wj = sh0.w[j];
-                        E.x += x0.x * wj, E.y += x0.y * wj, E.z += x0.z * wj;
-                        dB.x += x0.w * wj, dB.y += x1.x * wj, dB.z += x1.y * wj;
-                    }
-                    float c2 = 1.0f;
-                    f3    B;
-                    if constexpr (MIRROR) { // background field, as in background_B (particles.cuh)
-                        float s_, c_;
-                        sincos_taylor_f(a.xiD1 * (static_cast<float>(cell) + a.full_min + off), s_, c_);
-                        c2              = c_ * c_;
-                        float const ksc = a.xiO0_Oc * (s_ * c_);
-                        B               = { a.O0 / c2, ksc * v.z, -ksc * v.y };
-                    } else {
-                        B = { a.O0, 0.0f, 0.0f };
-                    }
-                    B = (B + dB) * a.dtOc_2O0;
-                    E = E * a.cDtOc_2O0;
-                    v = v + E;
-                    f3 const    u  = v + crossf(v, B);
-                    float const sb = 2.0f * __frcp_rn(1.0f + (B.x * B.x + B.y * B.y + B.z * B.z));
-                    v              = v + crossf(u, B * sb) + E;
-                    float const dq = (a.inv_D1 * c2) * v.x * (a.move_steps == 2 ? 0.5f * a.dt : a.dt);
-                    if (live && !(fabsf(dq * a.travel_scale) < 1.0f))
-                        bad |= ST_MOVED_TOO_FAR;
-                    v_push = v;
-                    move_cell(cell, off, dq);
-                    alive = boundary_mixed<BC>(a, cell, off, v, pid, a.counter + (a.move_steps == 2 ? 1 : 0));
-                    if (!alive)
-                        w = 0.0f, cell = 0, off = 0.5f, v = { 0, 0, 0 };
-                }
-            } else if (live) {
+        for (int k = 0; k < 2; ++k) { // E and dB at the particles, each into its half of the pairs
+            ds0[k]  = make_shape_f<O>(cell[k], el(off, k));
+            in0[k]  = stencil_ok_f(ds0[k], a.Nx);
+            push[k] = in0[k] && alive[k] && a.move_steps != 0;
+            if (!in0[k] && live[k])
                 bad |= ST_OUT_OF_RANGE;
+            if (push[k]) {
+#pragma unroll
+                for (int j = 0; j <= O; ++j) {
+                    float const *q  = a.EB + EBF_STRIDE * (ds0[k].i0 + j);
+                    float4 const x0 = __ldg(reinterpret_cast<float4 const *>(q));
+                    float4 const x1 = __ldg(reinterpret_cast<float4 const *>(q + 4));
+                    float const  wj = ds0[k].w[j];
+                    el(E.x, k) += x0.x * wj, el(E.y, k) += x0.y * wj, el(E.z, k) += x0.z * wj;
+                    el(dB.x, k) += x0.w * wj, el(dB.y, k) += x1.x * wj, el(dB.z, k) += x1.y * wj;
+                }
             }
-            P.celln[idx] = cell;
-            P.offn[idx]  = off;
-            P.vx[idx]    = v.x;
-            P.vy[idx]    = v.y;
-            P.vz[idx]    = v.z;
-            if (BC == BCK_ABSORBING)
-                P.wn[idx] = w;
-
-            ds0[k] = sh0;
-            ds1[k] = make_shape_f<O>(cell, off);
-            dd0[k] = live && in0 && (a.deposit_mask & 1);
-            dd1[k] = live && (a.deposit_mask & 2) && w != 0.0f && stencil_ok_f(ds1[k], a.Nx);
-            dv0[k] = make_float4(w_in, v_push.x * w_in, v_push.y * w_in, v_push.z * w_in);
-            dv1[k] = make_float4(w, v.x * w, v.y * w, v.z * w);
+        }
+        // the Boris push of both particles (as in boris_push, device_common.cuh)
+        float2 c2 = { 1.0f, 1.0f };
+        p3     B;
+        if constexpr (MIRROR) { // background field, as in background_B (particles.cuh)
+            float2 const x = { a.xiD1 * (static_cast<float>(cell[0]) + a.full_min + off.x),
+                               a.xiD1 * (static_cast<float>(cell[1]) + a.full_min + off.y) };
+            float2       s_, c_;
+            sincos_taylor_f2(x, s_, c_);
+            c2               = pmul(c_, c_);
+            float2 const ksc = pmul(bc(a.xiO0_Oc), pmul(s_, c_));
+            B                = { { __fdividef(a.O0, c2.x), __fdividef(a.O0, c2.y) }, pmul(ksc, v.z), pneg(pmul(ksc, v.y)) };
+        } else {
+            B = { bc(a.O0), { 0.0f, 0.0f }, { 0.0f, 0.0f } };
+        }
+        float2 const hB = bc(a.dtOc_2O0), hE = bc(a.cDtOc_2O0);
+        B               = { pmul(padd(B.x, dB.x), hB), pmul(padd(B.y, dB.y), hB), pmul(padd(B.z, dB.z), hB) };
+        E               = { pmul(E.x, hE), pmul(E.y, hE), pmul(E.z, hE) };
+        p3 const vm     = { padd(v.x, E.x), padd(v.y, E.y), padd(v.z, E.z) };
+        p3 const u      = padd3(vm, pcross(vm, B));
+        float2 const d  = pfma(B.x, B.x, pfma(B.y, B.y, pfma(B.z, B.z, bc(1.0f))));
+        float2 const sb = { __fdividef(2.0f, d.x), __fdividef(2.0f, d.y) };
+        p3 const     Bs = { pmul(B.x, sb), pmul(B.y, sb), pmul(B.z, sb) };
+        p3 const     vp = padd3(padd3(vm, pcross(u, Bs)), E);
+        float2 const dq = pmul(pmul(bc(a.inv_D1), c2), pmul(vp.x, bc(a.move_steps == 2 ? 0.5f * a.dt : a.dt)));
+        p3           v_push = v;
+        float4       dv0[2], dv1[2];
+        bool         dd0[2], dd1[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            if (push[k]) {
+                if (live[k] && !(fabsf(el(dq, k) * a.travel_scale) < 1.0f))
+                    bad |= ST_MOVED_TOO_FAR;
+                f3 vk      = { el(vp.x, k), el(vp.y, k), el(vp.z, k) };
+                el(v_push.x, k) = vk.x, el(v_push.y, k) = vk.y, el(v_push.z, k) = vk.z;
+                move_cell(cell[k], el(off, k), el(dq, k));
+                alive[k] = boundary_mixed<BC>(a, cell[k], el(off, k), vk, k ? pid.y : pid.x,
+                                              a.counter + (a.move_steps == 2 ? 1 : 0));
+                if (!alive[k])
+                    el(w, k) = 0.0f, cell[k] = 0, el(off, k) = 0.5f, vk = { 0, 0, 0 };
+                el(v.x, k) = vk.x, el(v.y, k) = vk.y, el(v.z, k) = vk.z;
+            }
+            ds1[k] = make_shape_f<O>(cell[k], el(off, k));
+            dd0[k] = live[k] && in0[k] && (a.deposit_mask & 1);
+            dd1[k] = live[k] && (a.deposit_mask & 2) && el(w, k) != 0.0f && stencil_ok_f(ds1[k], a.Nx);
+        }
+        *reinterpret_cast<int2 *>(P.cell + i2)  = make_int2(cell[0], cell[1]);
+        *reinterpret_cast<float2 *>(P.off + i2) = off;
+        *reinterpret_cast<float2 *>(P.vx + i2)  = v.x;
+        *reinterpret_cast<float2 *>(P.vy + i2)  = v.y;
+        *reinterpret_cast<float2 *>(P.vz + i2)  = v.z;
+        if (BC == BCK_ABSORBING)
+            *reinterpret_cast<float2 *>(P.w + i2) = w;
+        {
+            p3 const m0 = { pmul(v_push.x, w_in), pmul(v_push.y, w_in), pmul(v_push.z, w_in) };
+            p3 const m1 = { pmul(v.x, w), pmul(v.y, w), pmul(v.z, w) };
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                dv0[k] = make_float4(el(w_in, k), el(m0.x, k), el(m0.y, k), el(m0.z, k));
+                dv1[k] = make_float4(el(w, k), el(m1.x, k), el(m1.y, k), el(m1.z, k));
+            }
         }
         {
             int lo = 0x7fffffff, hi = -0x7fffffff;
 #pragma unroll
-            for (int k = 0; k < MIX_PPT; ++k) {
+            for (int k = 0; k < 2; ++k) {
                 if (dd0[k])
                     lo = min(lo, ds0[k].i0), hi = max(hi, ds0[k].i0);
                 if (dd1[k])
@@ -493,7 +562,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                 win.base      = gap > 0 ? mlo - gap / 2 : mlo;
             }
 #pragma unroll
-            for (int k = 0; k < MIX_PPT; ++k) {
+            for (int k = 0; k < 2; ++k) {
                 if (dd0[k]) {
                     if (ds0[k].i0 >= win.base && ds0[k].i0 <= win.base + SPAN)
                         win.add<O>(0, ds0[k], dv0[k], lane);
