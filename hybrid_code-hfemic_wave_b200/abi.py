@@ -19,7 +19,7 @@ from . import configs as _cfg
 PAD = 3
 MAX_KINETIC = 8
 MAX_COLD = 4
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 OK, ERR_INVALID_ARG, ERR_MOVED_TOO_FAR, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_NAN, ERR_STATE, \
     ERR_NO_DEVICE = range(9)
@@ -37,7 +37,9 @@ class MovedTooFar(H1DError):
 
 class KineticDesc(C.Structure):
     _fields_ = [("Oc", C.c_double), ("op", C.c_double), ("n_smooth", C.c_int64), ("Nc", C.c_int64),
-                ("shape_order", C.c_int64), ("moment_norm", C.c_double)]
+                ("shape_order", C.c_int64), ("moment_norm", C.c_double), ("scheme", C.c_int32),
+                ("reserved", C.c_int32), ("psd_refresh_frequency", C.c_double), ("vth1", C.c_double),
+                ("T2_T1", C.c_double)]
 
 
 class ColdDesc(C.Structure):
@@ -91,7 +93,8 @@ def make_params(cfg: "_cfg.RunConfig") -> Params:
     ef = cfg.efluid
     p.efluid = EFluidDesc(ef.Oc, ef.op, ef.beta, ef.gamma)
     for i, k in enumerate(cfg.kinetic):
-        p.kinetic[i] = KineticDesc(k.Oc, k.op, k.n_smooth, k.Nc, k.shape_order, cfg.moment_norm(k))
+        p.kinetic[i] = KineticDesc(k.Oc, k.op, k.n_smooth, k.Nc, k.shape_order, cfg.moment_norm(k), k.scheme, 0,
+                                   k.psd_refresh_frequency, k.vth1(cfg.c), k.T2_T1)
     for i, c in enumerate(cfg.cold):
         p.cold[i] = ColdDesc(c.Oc, c.op, c.n_smooth)
     if len(cfg.sources) > MAX_SOURCES:
@@ -139,6 +142,8 @@ def _declare(lib, prefix):
         advance=f("advance", v, C.c_uint32),
         particle_count=f("particle_count", v, C.c_int, _lp),
         download_particles=f("download_particles", v, C.c_int, _dp, _dp, _dp, _dp, _dp, _lp),
+        upload_psd=f("upload_psd", v, C.c_int, C.c_int64, _dp, _dp),
+        download_psd=f("download_psd", v, C.c_int, _dp, _dp),
         download_fields=f("download_fields", v, _dp, _dp),
         download_sources=f("download_sources", v, _dp, _dp),
         download_moments=f("download_moments", v, C.c_int, _dp, _dp, _dp),
@@ -223,10 +228,25 @@ class Run:
         v = np.ascontiguousarray(nV_full, dtype=np.float64).reshape(-1)
         self._check(self.fn["upload_cold"](self.h, i, _ptr(n), _ptr(v)))
 
+    def upload_psd(self, s, real_f, marker):
+        """Particle::PSD of species s (real_f, marker), in upload order."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (real_f, marker)]
+        self._check(self.fn["upload_psd"](self.h, s, arrs[0].size, *[_ptr(a) for a in arrs]))
+
+    def psd(self, s):
+        """(real_f, marker) of species s, in the order of particles(s)."""
+        n = self.particle_count(s)
+        real_f, marker = np.empty(n), np.empty(n)
+        self._check(self.fn["download_psd"](self.h, s, _ptr(real_f), _ptr(marker)))
+        return real_f, marker
+
     def upload_state(self, st):
-        """Upload a state dict as read by tests/golden/state_io.read_state."""
+        """Upload a state dict as read by tests/golden/state_io.read_state (the phase-space
+        densities too, for the species whose weights evolve)."""
         for s, p in enumerate(st["particles"]):
             self.upload_particles(s, p["q1"], p["vx"], p["vy"], p["vz"], p["w"])
+            if self.cfg.kinetic[s].has_psd:
+                self.upload_psd(s, p["real_f"], p["marker"])
         self.upload_fields(st["B"], st["E"])
         for i, c in enumerate(st["cold"]):
             self.upload_cold(i, c["n_full"], c["nV_full"])
@@ -241,27 +261,48 @@ class Run:
         self._check(self.fn["particle_count"](self.h, s, C.byref(n)))
         return n.value
 
-    def particles(self, s):
+    def particles(self, s, out=None, with_pid=True):
+        """The particles of species s as FP64 arrays q1, vx, vy, vz, w (+ pid).  `out` may hold
+        caller-owned arrays (for instance in pinned memory) of at least particle_count(s) elements;
+        they are filled and returned as views of that length."""
         n = self.particle_count(s)
-        out = {k: np.empty(n) for k in ("q1", "vx", "vy", "vz", "w")}
-        pid = np.empty(n, dtype=np.int64)
-        self._check(self.fn["download_particles"](self.h, s, *[_ptr(out[k]) for k in ("q1", "vx", "vy", "vz", "w")],
-                                                  _ptr(pid, C.c_int64)))
-        out["pid"] = pid
+        keys = ("q1", "vx", "vy", "vz", "w")
+        if out is None:
+            out = {k: np.empty(n) for k in keys}
+        else:
+            for k in keys:
+                a = out[k]
+                if a.dtype != np.float64 or a.ndim != 1 or a.size < n or not a.flags.c_contiguous:
+                    raise ValueError(f"particles: out[{k!r}] must be a contiguous float64 array of >= {n} elements")
+            out = {k: out[k][:n] for k in keys}
+        pid = np.empty(n, dtype=np.int64) if with_pid else None
+        self._check(self.fn["download_particles"](self.h, s, *[_ptr(out[k]) for k in keys],
+                                                  _ptr(pid, C.c_int64) if with_pid else None))
+        if with_pid:
+            out["pid"] = pid
         return out
 
-    def fields(self):
-        B, E = np.empty((self.M, 3)), np.empty((self.M, 3))
+    def _grids(self, out, shapes):
+        """Caller-owned output grids (checked), or new ones."""
+        if out is None:
+            return [np.empty(sh) for sh in shapes]
+        for a, sh in zip(out, shapes):
+            if a.dtype != np.float64 or a.shape != sh or not a.flags.c_contiguous:
+                raise ValueError(f"output grid must be a contiguous float64 array of shape {sh}")
+        return list(out)
+
+    def fields(self, out=None):
+        B, E = self._grids(out, [(self.M, 3), (self.M, 3)])
         self._check(self.fn["download_fields"](self.h, _ptr(B), _ptr(E)))
         return B, E
 
-    def sources(self):
-        rho, J = np.empty(self.M), np.empty((self.M, 3))
+    def sources(self, out=None):
+        rho, J = self._grids(out, [(self.M,), (self.M, 3)])
         self._check(self.fn["download_sources"](self.h, _ptr(rho), _ptr(J)))
         return rho, J
 
-    def moments(self, s):
-        n, nV, nvv = np.empty(self.M), np.empty((self.M, 3)), np.empty((self.M, 6))
+    def moments(self, s, out=None):
+        n, nV, nvv = self._grids(out, [(self.M,), (self.M, 3), (self.M, 6)])
         self._check(self.fn["download_moments"](self.h, s, _ptr(n), _ptr(nV), _ptr(nvv)))
         return n, nV, nvv
 
@@ -285,6 +326,8 @@ class Run:
         st = dict(B=B, E=E, charge=rho, current=J, particles=[], moments=[], cold=[])
         for s in range(len(self.cfg.kinetic)):
             st["particles"].append(self.particles(s))
+            if self.cfg.kinetic[s].has_psd:
+                st["particles"][-1]["real_f"], st["particles"][-1]["marker"] = self.psd(s)
             n, nV, nvv = self.moments(s)
             st["moments"].append(dict(n=n, nV=nV, nvv=nvv))
         for i in range(len(self.cfg.cold)):

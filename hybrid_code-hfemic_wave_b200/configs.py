@@ -23,6 +23,7 @@ ALGO_PC, ALGO_CAMCL = 0, 1
 BC_PERIODIC, BC_REFLECTING, BC_ABSORBING = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 ISOTHERMAL, ADIABATIC = 11, 53  # Closure (src/LibPIC/PIC/Predefined.h:35-38)
+FULL_F, DELTA_F = 0, 1  # ParticleScheme (src/LibPIC/PIC/Predefined.h)
 
 
 @dataclass
@@ -36,9 +37,20 @@ class Kinetic:
     n_smooth: int = 2
     beta1: float = 0.1  # parallel beta
     T2_T1: float = 1.0  # perpendicular / parallel temperature
+    # phase-space density weighting (KineticPlasmaDesc, PlasmaDesc.h:118-160)
+    scheme: int = FULL_F
+    initial_weight: float = 0.0  # delta-f only: initial weights are initial_weight * U(-1, 1)
+    marker_temp_ratio: float = 1.0  # marker temperature / physical temperature
+    psd_refresh_frequency: float = 0.0  # nu: weights relax toward the equilibrium at this rate
 
     def vth1(self, c: float) -> float:
         return math.sqrt(self.beta1) * c * abs(self.Oc) / self.op
+
+    @property
+    def has_psd(self) -> bool:
+        """Whether the particles carry a phase-space density that changes in time (delta-f, or
+        full-f with PSD refresh): their weights are then updated every step."""
+        return self.scheme == DELTA_F or self.psd_refresh_frequency != 0.0
 
 
 @dataclass
@@ -107,6 +119,10 @@ class RunConfig:
 
     def replace(self, **kw) -> "RunConfig":
         return dataclasses.replace(self, **kw)
+
+    @property
+    def has_psd(self) -> bool:
+        return any(k.has_psd for k in self.kinetic)
 
     @property
     def n_particles(self) -> int:
@@ -186,7 +202,10 @@ def plasma(c: float, species, cold_fraction: float, beta_e: float, closure=ISOTH
         ne += f * Z
         kin.append(Kinetic(Oc=Z / A, op=c * math.sqrt(f * Z * Z / A), Nc=s["Nc"],
                            shape_order=s.get("shape_order", 2), n_smooth=s.get("n_smooth", 2),
-                           beta1=s["beta1"], T2_T1=s.get("T2_T1", 1.0)))
+                           beta1=s["beta1"], T2_T1=s.get("T2_T1", 1.0), scheme=s.get("scheme", FULL_F),
+                           initial_weight=s.get("initial_weight", 0.0),
+                           marker_temp_ratio=s.get("marker_temp_ratio", 1.0),
+                           psd_refresh_frequency=s.get("psd_refresh_frequency", 0.0)))
     cold = []
     if cold_fraction > 0:
         ne += cold_fraction
@@ -279,7 +298,33 @@ def parity_p6() -> RunConfig:
     return cfg.replace(name="p6_pc_source", sources=[src])
 
 
-PARITY = {f().name: f for f in (parity_p1, parity_p2, parity_p3, parity_p4, parity_p5, parity_p6)}
+def parity_p7() -> RunConfig:
+    """Phase-space density weights in a mirror field (CAM-CL, reflecting): a delta-f H+ species
+    (initial weights 0.1 U(-1, 1), PSD refresh at nu = 2) beside a full-f He+ species loaded with
+    markers twice as hot as the plasma (weights f0/g0) and refreshed at nu = 5."""
+    ef, kin, cold = plasma(100.0, [
+        dict(f=0.10, Z=1, A=1, Nc=16, shape_order=2, beta1=0.2, T2_T1=4.0, scheme=DELTA_F, initial_weight=0.1,
+             psd_refresh_frequency=2.0),
+        dict(f=0.05, Z=1, A=4, Nc=12, shape_order=1, beta1=0.05, T2_T1=2.0, marker_temp_ratio=2.0,
+             psd_refresh_frequency=5.0),
+    ], 0.85, 0.1)
+    return RunConfig("p7_psd_tsc_mirror_reflecting", Nx=64, Dx=0.3, xi=0.05, c=100.0, dt=0.01,
+                     efluid=ef, kinetic=kin, cold=cold, particle_bc=BC_REFLECTING,
+                     phase_retardation=(8, 1.0), amplitude_damping=(8, 0.2), steps=10)
+
+
+def parity_p8() -> RunConfig:
+    """p7 under the predictor-corrector cycle, periodic, with a delta-f species without refresh."""
+    cfg = parity_p7()
+    kin = [dataclasses.replace(k) for k in cfg.kinetic]
+    kin[0].psd_refresh_frequency = 0.0
+    kin[0].shape_order = 3
+    return cfg.replace(name="p8_pc_psd_periodic", kinetic=kin, algorithm=ALGO_PC, particle_bc=BC_PERIODIC,
+                       xi=0.03)
+
+
+PARITY = {f().name: f for f in (parity_p1, parity_p2, parity_p3, parity_p4, parity_p5, parity_p6, parity_p7,
+                                parity_p8)}
 PRESETS = {f().name: f for f in (config1, config2, config3)}
 
 

@@ -46,6 +46,7 @@ enum GeoIdx {
 
 struct KinSrc {
     double const *raw[2][4]; // unscaled deposits at x^N and x^{N+1}: n, nVx, nVy, nVz (cell 0)
+    double const *eq;        // delta-f: equilibrium n0 added to the density moment (cell 0), or null
     double       *zero[2][4]; // the deposit set of the next cycle, cleared here
     double        s1;         // 1/Nc (PartSpecies.cc:327-328)
     double        cdcf, ccf;  // charge / current density conversion factors
@@ -97,10 +98,15 @@ struct Cell {
     double fcx, fcy, fcz, fnx, fny, fnz, hcx, hcy, hcz, hnx, hny, hnz, hbx, mp1, mp2, ma1, ma2;
 };
 
-// fold of one raw deposit array onto interior cell gm, times 1/Nc and a conversion factor
-__device__ __forceinline__ double fold(double const *r, int gm, int Nx, int bc, double s1, double f)
+// fold of one raw deposit array onto interior cell gm, times 1/Nc (plus the delta-f equilibrium
+// eq, zero in the ghost cells; PartSpecies.cc:115-128) and a conversion factor
+__device__ __forceinline__ double fold(double const *r, int gm, int Nx, int bc, double s1, double f,
+                                       double const *eq = nullptr)
 {
-    double v = (r[gm] * s1) * f;
+    double m = r[gm] * s1;
+    if (eq)
+        m = m + eq[gm] * 1.0;
+    double v = m * f;
     if (bc == 0) {
         if (gm < PAD)
             v = v + (r[Nx + gm] * s1) * f;
@@ -289,7 +295,7 @@ __device__ __forceinline__ Smem carve(double *sm, int L)
 static __device__ SV collect_kinetic(FieldArgs const &a, Cell const &C, Smem const &S, KinSrc const &K, int d)
 {
     int const gm = C.gm;
-    S.tr[C.t]    = fold(K.raw[d][0], gm, a.Nx, a.bc, K.s1, K.cdcf);
+    S.tr[C.t]    = fold(K.raw[d][0], gm, a.Nx, a.bc, K.s1, K.cdcf, K.eq);
     for (int q = 0; q < 3; ++q)
         S.tJ[3 * C.t + q] = fold(K.raw[d][1 + q], gm, a.Nx, a.bc, K.s1, K.ccf);
     return smooth_n(C, K.nsm, S.tr, S.tJ, S.ts, S.tJs);
@@ -408,7 +414,7 @@ __device__ __forceinline__ void camcl_field_body(FieldArgs const &a, int blk)
         int    nsm;
         if (s < a.nk || s >= a.nk + a.nc) {
             KinSrc const &K = s < a.nk ? a.k[s] : a.e[s - a.nk - a.nc];
-            lam             = fold(K.raw[1][0], C.gm, Nx, a.bc, K.s1, K.lamf);
+            lam             = fold(K.raw[1][0], C.gm, Nx, a.bc, K.s1, K.lamf, K.eq);
             gam             = { fold(K.raw[1][1], C.gm, Nx, a.bc, K.s1, K.gamf), fold(K.raw[1][2], C.gm, Nx, a.bc, K.s1, K.gamf),
                     fold(K.raw[1][3], C.gm, Nx, a.bc, K.s1, K.gamf) };
             nsm             = K.nsm;

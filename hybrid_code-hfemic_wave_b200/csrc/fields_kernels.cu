@@ -49,9 +49,10 @@ cudaError_t launch_prep_fields(double *B, double *E, double *EB, float *EBf, int
     prep_fields_kernel<<<(Nx + 2 * PAD + 255) / 256, 256, 0, st>>>(B, E, EB, EBf, Nx);
     return cudaGetLastError();
 }
-cudaError_t launch_finalize_kinetic(double const *raw, double *out, int Nx, double s1, int reflecting, cudaStream_t st)
+cudaError_t launch_finalize_kinetic(double const *raw, double const *eq, double *out, int Nx, double s1,
+                                    int reflecting, cudaStream_t st)
 {
-    finalize_kinetic_kernel<<<1, 256, 0, st>>>(raw, out, Nx, s1, reflecting);
+    finalize_kinetic_kernel<<<1, 256, 0, st>>>(raw, eq, out, Nx, s1, reflecting);
     return cudaGetLastError();
 }
 cudaError_t launch_finalize_cold(double const *n_full, double const *nV_full, double *out, int Nx, double w,
@@ -68,6 +69,11 @@ cudaError_t launch_energy(EnergyArgs const &a, cudaStream_t st)
 cudaError_t launch_sources(SourceArgs const &a, cudaStream_t st)
 {
     source_kernel<<<1, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+cudaError_t launch_fill(double *a, int64_t n, double v, cudaStream_t st)
+{
+    fill_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(a, n, v);
     return cudaGetLastError();
 }
 cudaError_t launch_iota(int32_t *pid, int64_t n, cudaStream_t st)

@@ -35,7 +35,9 @@ struct SpeciesState {
     int32_t *cell[2]   = {}; // mixed precision: [parity] full-grid cell
     float   *fbuf[2][5] = {}; // mixed precision: [parity][offset in the cell, vx, vy, vz, w]
     int32_t *pid[2]    = {};
+    double  *psd[2][2] = {}; // FP64 with evolving weights: [parity][real_f, marker]
     int      cur       = 0;
+    bool     upload_order = false; // the particles are still in the order of their upload
     // sort scratch
     uint32_t *keys[2] = {}, *idx[2] = {};
     uint32_t *hist = nullptr, *part = nullptr;
@@ -48,6 +50,8 @@ struct SpeciesState {
     double *mom_raw = nullptr;
     // finalized moments (GridArray layout): n (M), nV (3M), nvv (6M)
     double *mom = nullptr;
+    // delta-f: equilibrium moments n0 (M) and nvv0 (6M) on the half grid, ghosts zero
+    double *eq = nullptr;
 };
 
 struct ColdState {
@@ -159,6 +163,33 @@ void phase_end(h1d_run *r, int kernels)
                            fmt("%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__));        \
     } while (0)
 
+// the weights of a species change every step (delta-f, or full-f with PSD refresh)
+bool evolves_psd(h1d_kinetic_desc const &d) { return d.scheme == H1D_DELTA_F || d.psd_refresh_frequency != 0; }
+
+// PartSpecies::populate's cache of the equilibrium moments (PartSpecies.cc:80-87) for the
+// bi-Maxwellian MaxwellianVDF (MaxwellianVDF.h:56-70, .cc:33-43) on the interior half-grid
+// points, times m_moment_weighting_factor as collect_part adds them: n0 (M doubles) then nvv0
+// (6M, {xx, yy, zz, xy, yz, zx}); nV0 = 0; ghost cells zero
+std::vector<double> equilibrium_moments(h1d_params const &p, h1d_kinetic_desc const &d)
+{
+    long const          M = p.Nx + 2 * PAD;
+    std::vector<double> eq(7 * M, 0.0);
+    double const        q1min = -0.5 * p.Nx + 0.5;
+    double const        hv2   = .5 * (d.vth1 * d.vth1);
+    for (long i = 0; i < p.Nx; ++i) {
+        double const q1  = static_cast<double>(i) + q1min;
+        double const cs  = std::cos(p.xi * p.Dx * q1);
+        double const eta = 1 / (d.T2_T1 + (1 - d.T2_T1) * cs * cs);
+        double const n0  = 1 * eta, T = d.T2_T1 * eta;
+        double const w   = p.moment_weighting;
+        eq[i + PAD]      = n0 * w;
+        double *e        = eq.data() + M + 6 * (i + PAD);
+        e[0] = ((1 * hv2) * n0) * w, e[1] = ((T * hv2) * n0) * w, e[2] = ((T * hv2) * n0) * w;
+        e[3] = ((0 * hv2) * n0) * w, e[4] = ((0 * hv2) * n0) * w, e[5] = ((0 * hv2) * n0) * w;
+    }
+    return eq;
+}
+
 int validate(h1d_params const *p, std::string &m)
 {
 #define BAD(...) return m = fmt(__VA_ARGS__), H1D_ERR_INVALID_ARG
@@ -196,6 +227,12 @@ int validate(h1d_params const *p, std::string &m)
             BAD("kinetic species %d: moment_norm must be positive", s);
         if (d.n_smooth < 0 || d.n_smooth > 64)
             BAD("kinetic species %d: smoothing count outside [0, 64]", s);
+        if ((d.scheme != H1D_FULL_F && d.scheme != H1D_DELTA_F) || !(d.psd_refresh_frequency >= 0))
+            BAD("kinetic species %d: unknown particle scheme or negative psd_refresh_frequency", s);
+        if (evolves_psd(d) && (!(d.vth1 > 0) || !(d.T2_T1 > 0)))
+            BAD("kinetic species %d: evolving weights need the equilibrium vth1 > 0 and T2_T1 > 0", s);
+        if (evolves_psd(d) && p->precision == H1D_PREC_MIXED)
+            BAD("kinetic species %d: delta-f and PSD refresh run in FP64 only", s);
     }
     for (int s = 0; s < p->n_cold; ++s)
         if (p->cold[s].Oc == 0 || !(p->cold[s].op > 0) || p->cold[s].n_smooth < 0 || p->cold[s].n_smooth > 64)
@@ -306,6 +343,12 @@ PushArgs push_args(h1d_run *run, int s)
     a.status = run->d_status, a.fallbacks = run->d_fallbacks, a.seed = p.gyrophase_seed, a.counter = static_cast<uint64_t>(run->step) * 8;
     a.species = s, a.randomize = p.randomize_gyrophase, a.homogeneous_poly = p.xi < 1e-10;
     a.move_steps = 1, a.deposit_mask = 3, a.write_back = 1;
+    if (S.psd[S.cur][0]) {
+        a.real_f = S.psd[S.cur][0], a.marker = S.psd[S.cur][1];
+        a.nu_dt = d.psd_refresh_frequency * p.dt, a.psd_refresh = d.psd_refresh_frequency != 0;
+        a.delta_f = d.scheme == H1D_DELTA_F;
+        a.vth1 = d.vth1, a.vth1_cubed = d.vth1 * d.vth1 * d.vth1, a.T2_T1 = d.T2_T1;
+    }
     return a;
 }
 
@@ -340,6 +383,8 @@ int launch_push(h1d_run *run, int s, PushArgs const &a)
         PushArgsMixed const m = mixed_args(run, s, a);
         CU(launch_push_groups(&m, 1, order, mirror, run->p.particle_bc,
                               run->num_sms * (run->ctas_per_sm ? run->ctas_per_sm : PIPE_CTAS_PER_SM_MIXED), run->stream));
+    } else if (a.real_f) {
+        CU(launch_push_psd(a, order, mirror, run->p.particle_bc, run->num_sms * PIPE_CTAS_PER_SM, run->stream));
     } else {
         CU(launch_push_groups(&a, 1, order, mirror, run->p.particle_bc,
                               run->num_sms * (run->ctas_per_sm ? std::min(run->ctas_per_sm, PIPE_CTAS_PER_SM) : PIPE_CTAS_PER_SM),
@@ -353,6 +398,7 @@ int sort_species(h1d_run *run, int s)
 {
     SpeciesState &S = run->sp[s];
     S.since_sort    = 0;
+    S.upload_order  = false;
     if (S.n == 0)
         return H1D_OK;
     cudaStream_t const st     = run->stream;
@@ -383,15 +429,19 @@ int sort_species(h1d_run *run, int s)
         first.cell = S.cell[S.cur], first.wf = S.fbuf[S.cur][4];
     else
         first.q1 = S.buf[S.cur][0], first.w = S.buf[S.cur][4];
-    MoveMixed mm{};
-    MoveFP64  md{};
+    MoveMixed         mm{};
+    MoveFP64          md{};
+    MoveFP64T<true>   mp{};
+    bool const        psd = S.psd[0][0] != nullptr;
     for (int k = 0; k < 5; ++k) {
         mm.src[k] = S.fbuf[S.cur][k], mm.dst[k] = S.fbuf[1 - S.cur][k];
-        md.src[k] = S.buf[S.cur][k], md.dst[k] = S.buf[1 - S.cur][k];
+        md.src[k] = mp.src[k] = S.buf[S.cur][k], md.dst[k] = mp.dst[k] = S.buf[1 - S.cur][k];
     }
+    for (int k = 0; k < 2; ++k)
+        mp.src[5 + k] = S.psd[S.cur][k], mp.dst[5 + k] = S.psd[1 - S.cur][k];
     mm.cell_src = S.cell[S.cur], mm.cell_dst = S.cell[1 - S.cur];
-    mm.pid_src = md.pid_src = S.pid[S.cur];
-    mm.pid_dst = md.pid_dst = S.pid[1 - S.cur];
+    mm.pid_src = md.pid_src = mp.pid_src = S.pid[S.cur];
+    mm.pid_dst = md.pid_dst = mp.pid_dst = S.pid[1 - S.cur];
     int shift = 0, src = 0; // keys/idx buffer the current pass reads (the first pass reads the particles)
     for (int pass = 0; pass < plan.passes; ++pass) {
         unsigned const mask = (1u << plan.bits[pass]) - 1u;
@@ -415,6 +465,8 @@ int sort_species(h1d_run *run, int s)
             scatter_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mk);
         else if (pass > 0 && run->mixed)
             scatter_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mm);
+        else if (pass > 0 && psd)
+            scatter_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mp);
         else if (pass > 0)
             scatter_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, md);
         else if (run->mixed && !last)
@@ -423,6 +475,8 @@ int sort_species(h1d_run *run, int s)
             scatter_kernel<KEYS_MIXED><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mm);
         else if (!last)
             scatter_kernel<KEYS_FP64><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mk);
+        else if (psd)
+            scatter_kernel<KEYS_FP64><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mp);
         else
             scatter_kernel<KEYS_FP64><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, md);
         shift += plan.bits[pass];
@@ -462,6 +516,7 @@ FieldArgs field_args(h1d_run *run)
             }
         K.s1 = 1.0 / d.moment_norm, K.cdcf = cdcf(p, d.Oc, d.op), K.ccf = ccf(p, d.Oc, d.op);
         K.lamf = K.cdcf * d.Oc / p.O0, K.gamf = K.ccf * d.Oc / p.O0, K.nsm = static_cast<int>(d.n_smooth);
+        K.eq = run->sp[s].eq ? run->sp[s].eq + PAD : nullptr;
     }
     for (int c = 0; c < p.n_cold; ++c) {
         h1d_cold_desc const &d = p.cold[c];
@@ -677,7 +732,7 @@ int finalize_moments(h1d_run *run)
             int64_t const chunks = (S.n + 32LL * a.ppt - 1) / (32LL * a.ppt);
             moments_kernel<<<static_cast<unsigned>((chunks + 7) / 8), 256, 0, run->stream>>>(a);
         }
-        CU(launch_finalize_kinetic(S.mom_raw, S.mom, static_cast<int>(run->Nx), 1.0 / p.kinetic[s].moment_norm,
+        CU(launch_finalize_kinetic(S.mom_raw, S.eq, S.mom, static_cast<int>(run->Nx), 1.0 / p.kinetic[s].moment_norm,
                                    p.particle_bc == H1D_BC_PERIODIC ? 0 : 1, run->stream));
     }
     for (int c = 0; c < p.n_cold; ++c) {
@@ -759,6 +814,12 @@ int ensure_capacity(h1d_run *run, int s, int64_t n)
                 b = nullptr;
                 CU(cudaMalloc(&b, sizeof(double) * cap));
             }
+            if (evolves_psd(run->p.kinetic[s]))
+                for (auto *&b : S.psd[k]) {
+                    cudaFree(b);
+                    b = nullptr;
+                    CU(cudaMalloc(&b, sizeof(double) * cap));
+                }
         }
         cudaFree(S.pid[k]), cudaFree(S.keys[k]), cudaFree(S.idx[k]);
         S.pid[k] = nullptr, S.keys[k] = nullptr, S.idx[k] = nullptr;
@@ -1206,7 +1267,7 @@ int h1d_collect_moments_noalloc(int64_t Nx, double moment_norm, int particle_bc,
         if (cudaGetLastError() != cudaSuccess)
             return H1D_ERR_CUDA;
     }
-    if (launch_finalize_kinetic(raw, fin, static_cast<int>(Nx), 1.0 / moment_norm, particle_bc == H1D_BC_PERIODIC ? 0 : 1, st)
+    if (launch_finalize_kinetic(raw, nullptr, fin, static_cast<int>(Nx), 1.0 / moment_norm, particle_bc == H1D_BC_PERIODIC ? 0 : 1, st)
             != cudaSuccess
         || cudaMemcpyAsync(n_out, fin, sizeof(double) * M, cudaMemcpyDeviceToDevice, st) != cudaSuccess
         || cudaMemcpyAsync(nV_out, fin + M, sizeof(double) * 3 * M, cudaMemcpyDeviceToDevice, st) != cudaSuccess
@@ -1288,6 +1349,12 @@ int h1d_create(h1d_params const *params, h1d_run **out)
         if (dalloc(run, &S.dep, 16 * M) || dalloc(run, &S.mom_raw, 10 * M) || dalloc(run, &S.mom, 10 * M)
             || dalloc(run, &S.dead, 1))
             return fail(H1D_ERR_OOM);
+        if (p.kinetic[s].scheme == H1D_DELTA_F) {
+            std::vector<double> const eq = equilibrium_moments(p, p.kinetic[s]);
+            if (dalloc(run, &S.eq, 7 * M)
+                || cudaMemcpy(S.eq, eq.data(), sizeof(double) * eq.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+                return fail(H1D_ERR_OOM);
+        }
     }
     for (int c = 0; c < p.n_cold; ++c) {
         ColdState &C = run->cold[c];
@@ -1323,8 +1390,10 @@ int h1d_destroy(h1d_run *run)
                 cudaFree(b);
             cudaFree(S.cell[k]);
             cudaFree(S.pid[k]), cudaFree(S.keys[k]), cudaFree(S.idx[k]);
+            cudaFree(S.psd[k][0]), cudaFree(S.psd[k][1]);
         }
         cudaFree(S.hist), cudaFree(S.part), cudaFree(S.dead), cudaFree(S.dep), cudaFree(S.mom_raw), cudaFree(S.mom);
+        cudaFree(S.eq);
     }
     for (auto &C : run->cold)
         cudaFree(C.n), cudaFree(C.nV[0]), cudaFree(C.nV[1]), cudaFree(C.mom);
@@ -1372,11 +1441,54 @@ int h1d_upload_particles(h1d_run *run, int s, int64_t n, double const *q1, doubl
     for (int k = 0; k < 5 && !run->mixed; ++k)
         if (n)
             CU(cudaMemcpyAsync(S.buf[0][k], src[k], sizeof(double) * n, cudaMemcpyHostToDevice, run->stream));
+    if (n && S.psd[0][0]) { // until h1d_upload_psd: real_f = w, marker = 1 (weight = real_f / marker)
+        CU(cudaMemcpyAsync(S.psd[0][0], S.buf[0][4], sizeof(double) * n, cudaMemcpyDeviceToDevice, run->stream));
+        CU(launch_fill(S.psd[0][1], n, 1.0, run->stream));
+    }
     if (n)
         CU(launch_iota(S.pid[0], n, run->stream));
     S.since_sort       = 1 << 30;
+    S.upload_order     = true;
     run->moments_stale = true;
     run->gen++;
+    CU(cudaStreamSynchronize(run->stream));
+    return H1D_OK;
+}
+
+
+int h1d_upload_psd(h1d_run *run, int s, int64_t n, double const *real_f, double const *marker)
+{
+    if (!run || s < 0 || s >= run->p.n_kinetic || (n > 0 && (!real_f || !marker)))
+        return set_err(run, H1D_ERR_INVALID_ARG, "h1d_upload_psd: bad arguments");
+    SpeciesState &S = run->sp[s];
+    if (!evolves_psd(run->p.kinetic[s]) || run->mixed)
+        return set_err(run, H1D_ERR_INVALID_ARG, "h1d_upload_psd: the weights of this species do not evolve");
+    if (n != S.n)
+        return set_err(run, H1D_ERR_INVALID_ARG, "h1d_upload_psd: count differs from the uploaded particles");
+    if (n && !S.upload_order)
+        return set_err(run, H1D_ERR_INVALID_ARG, "h1d_upload_psd: the particles were reordered since their upload");
+    CU(cudaStreamSynchronize(run->stream));
+    if (n) {
+        CU(cudaMemcpyAsync(S.psd[S.cur][0], real_f, sizeof(double) * n, cudaMemcpyHostToDevice, run->stream));
+        CU(cudaMemcpyAsync(S.psd[S.cur][1], marker, sizeof(double) * n, cudaMemcpyHostToDevice, run->stream));
+    }
+    CU(cudaStreamSynchronize(run->stream));
+    return H1D_OK;
+}
+
+int h1d_download_psd(h1d_run *run, int s, double *real_f, double *marker)
+{
+    if (!run || s < 0 || s >= run->p.n_kinetic)
+        return H1D_ERR_INVALID_ARG;
+    SpeciesState &S = run->sp[s];
+    if (!evolves_psd(run->p.kinetic[s]) || run->mixed)
+        return set_err(run, H1D_ERR_INVALID_ARG, "h1d_download_psd: the weights of this species do not evolve");
+    if (run->p.particle_bc == H1D_BC_ABSORBING && S.n > 0 && S.since_sort > 0)
+        TRY(sort_species(run, s)); // drop absorbed particles, as h1d_download_particles does
+    if (real_f && S.n)
+        CU(cudaMemcpyAsync(real_f, S.psd[S.cur][0], sizeof(double) * S.n, cudaMemcpyDeviceToHost, run->stream));
+    if (marker && S.n)
+        CU(cudaMemcpyAsync(marker, S.psd[S.cur][1], sizeof(double) * S.n, cudaMemcpyDeviceToHost, run->stream));
     CU(cudaStreamSynchronize(run->stream));
     return H1D_OK;
 }
@@ -1386,6 +1498,9 @@ int h1d_populate(h1d_run *run, int s, int64_t n, uint64_t seed, double beta1, do
 {
     if (!run || s < 0 || s >= run->p.n_kinetic || n < 0 || n > (int64_t{ 1 } << 31) - 1 || !(beta1 > 0) || !(T2_T1 > 0))
         return set_err(run, H1D_ERR_INVALID_ARG, "h1d_populate: bad arguments");
+    if (evolves_psd(run->p.kinetic[s]))
+        return set_err(run, H1D_ERR_INVALID_ARG,
+                       "h1d_populate: species with evolving weights are loaded with h1d_upload_particles and h1d_upload_psd");
     h1d_params const       &p = run->p;
     h1d_kinetic_desc const &d = p.kinetic[s];
     SpeciesState           &S = run->sp[s];
@@ -1414,6 +1529,7 @@ int h1d_populate(h1d_run *run, int s, int64_t n, uint64_t seed, double beta1, do
         CU(launch_iota(S.pid[0], n, run->stream));
     }
     S.since_sort       = 1 << 30;
+    S.upload_order     = true;
     run->moments_stale = true;
     run->gen++;
     CU(cudaStreamSynchronize(run->stream));
@@ -1660,6 +1776,9 @@ int h1d_batch_create(h1d_run *const *runs, int n_runs, h1d_batch **out)
         for (int j = 0; j < i && !why; ++j)
             if (runs[j] == r)
                 why = "run listed twice";
+        for (int s = 0; r && s < r->p.n_kinetic && !why; ++s)
+            if (evolves_psd(r->p.kinetic[s]))
+                why = "species with evolving weights (delta-f, PSD refresh) advance as single runs";
         if (why) {
             std::fprintf(stderr, "h1d_batch_create: member %d: %s\n", i, why);
             return H1D_ERR_INVALID_ARG;
@@ -1859,7 +1978,7 @@ int h1d_vhistogram(h1d_run *run, int s, double ext_loc, double ext_len, double v
             a.fvz = S.fbuf[S.cur][3], a.fw = S.fbuf[S.cur][4];
         else
             a.q1 = S.buf[S.cur][0], a.vx = S.buf[S.cur][1], a.vy = S.buf[S.cur][2], a.vz = S.buf[S.cur][3],
-            a.w = S.buf[S.cur][4];
+            a.w = S.buf[S.cur][4], a.real_f = S.psd[S.cur][0], a.marker = S.psd[S.cur][1];
         a.n = S.n, a.full_min = -0.5 * run->Nx, a.half_min = a.full_min + 0.5;
         a.ext_lo = ext_loc, a.ext_hi = ext_loc + ext_len, a.v1min = v1min, a.v1len = v1len, a.v2min = v2min, a.v2len = v2len;
         a.v1dim = static_cast<int>(v1dim), a.v2dim = static_cast<int>(v2dim);
@@ -2291,9 +2410,11 @@ int h1d_server_destroy(h1d_server *sv)
 // ---- checkpoint / resume ------------------------------------------------------------------------
 // The content of the reference's snapshot (Recorder/Snapshot.cc:148-185, 330-375): step count, a
 // signature of the parameters (Hash{serialize(params)}, Snapshot.cc:19, 340-342), B and E, the
-// particles of every kinetic species (here with their ids, in the run's own precision so that a
-// resume is exact) and mom0_full / mom1_full of every cold species.  Sources and the push record
-// are recomputed on the first step after a resume, as after the reference's snapshot load.
+// particles of every kinetic species (here with their ids and, when their weights evolve, their
+// real_f and marker, in the run's own precision so that a resume is exact) and mom0_full /
+// mom1_full of every cold species.  Sources and the push record are recomputed on the first step
+// after a resume, as after the reference's snapshot load; the delta-f equilibrium moments that the
+// snapshot stores are a function of the parameters and are rebuilt by h1d_create.
 
 namespace {
 
@@ -2306,7 +2427,7 @@ struct CkptHeader {
     int64_t  n[H1D_MAX_KINETIC];
 };
 constexpr char     CKPT_MAGIC[8] = { 'H', '1', 'D', 'C', 'K', 'P', 'T', 0 };
-constexpr uint32_t CKPT_VERSION  = 1;
+constexpr uint32_t CKPT_VERSION  = 2;
 
 // FNV-1a over the run's parameters with the tuning knob (sort interval) cleared
 uint64_t params_signature(h1d_params p)
@@ -2319,16 +2440,18 @@ uint64_t params_signature(h1d_params p)
     return h;
 }
 
-size_t particle_bytes(h1d_run const *run, int64_t n)
+// bytes of species s with n particles: the record, the id, and real_f / marker when its weights evolve
+size_t particle_bytes(h1d_run const *run, int s, int64_t n)
 {
-    return static_cast<size_t>(n) * (run->mixed ? 6 * 4 + 4 : 5 * 8 + 4);
+    size_t const psd = !run->mixed && evolves_psd(run->p.kinetic[s]) ? 2 * 8 : 0;
+    return static_cast<size_t>(n) * ((run->mixed ? 6 * 4 + 4 : 5 * 8 + 4) + psd);
 }
 
 size_t ckpt_size(h1d_run const *run)
 {
     size_t b = sizeof(CkptHeader) + sizeof(double) * 6 * run->M + sizeof(double) * 4 * run->M * run->p.n_cold;
     for (int s = 0; s < run->p.n_kinetic; ++s)
-        b += particle_bytes(run, run->sp[s].n);
+        b += particle_bytes(run, s, run->sp[s].n);
     return b;
 }
 
@@ -2390,6 +2513,9 @@ int h1d_checkpoint_save(h1d_run *run, void *buffer, size_t capacity, size_t *wri
                 CU(d2h(S.buf[S.cur][k], 8 * n));
         }
         CU(d2h(S.pid[S.cur], 4 * n));
+        if (!run->mixed && evolves_psd(run->p.kinetic[s]))
+            for (int k = 0; k < 2; ++k)
+                CU(d2h(S.psd[S.cur][k], 8 * n));
     }
     CU(cudaStreamSynchronize(run->stream));
     if (written)
@@ -2412,7 +2538,7 @@ int h1d_checkpoint_load(h1d_run *run, void const *buffer, size_t size)
     for (int s = 0; s < run->p.n_kinetic; ++s) {
         if (hd.n[s] < 0 || hd.n[s] > (int64_t{ 1 } << 31) - 1)
             return set_err(run, H1D_ERR_INVALID_ARG, "h1d_checkpoint_load: corrupt particle count");
-        need += particle_bytes(run, hd.n[s]);
+        need += particle_bytes(run, s, hd.n[s]);
     }
     if (size < need)
         return set_err(run, H1D_ERR_INVALID_ARG, "h1d_checkpoint_load: truncated checkpoint");
@@ -2447,6 +2573,9 @@ int h1d_checkpoint_load(h1d_run *run, void const *buffer, size_t size)
                 CU(h2d(S.buf[0][k], 8 * n));
         }
         CU(h2d(S.pid[0], 4 * n));
+        if (!run->mixed && evolves_psd(run->p.kinetic[s]))
+            for (int k = 0; k < 2; ++k)
+                CU(h2d(S.psd[0][k], 8 * n));
         CU(cudaMemsetAsync(S.dep, 0, sizeof(double) * 16 * M, run->stream)); // no deposit in flight
         S.since_sort = 1 << 30;
     }

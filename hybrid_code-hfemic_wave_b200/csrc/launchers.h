@@ -27,11 +27,13 @@ cudaError_t launch_camcl_fields_batch(FieldArgs const *table, FieldBlock const *
 cudaError_t launch_pc_fields_batch(FieldArgs const *table, FieldBlock const *map, int blocks, int threads,
                                    size_t smem, cudaStream_t st);
 cudaError_t launch_prep_fields(double *B, double *E, double *EB, float *EBf, int Nx, cudaStream_t st);
-cudaError_t launch_finalize_kinetic(double const *raw, double *out, int Nx, double s1, int reflecting, cudaStream_t st);
+cudaError_t launch_finalize_kinetic(double const *raw, double const *eq, double *out, int Nx, double s1,
+                                    int reflecting, cudaStream_t st);
 cudaError_t launch_finalize_cold(double const *n_full, double const *nV_full, double *out, int Nx, double w,
                                  cudaStream_t st);
 cudaError_t launch_energy(EnergyArgs const &a, cudaStream_t st);
 cudaError_t launch_iota(int32_t *pid, int64_t n, cudaStream_t st);
+cudaError_t launch_fill(double *a, int64_t n, double v, cudaStream_t st);
 // the external sources of a run at time t (source_kernel, post.cuh)
 struct SourceArgs {
     h1d_source_desc d[MAXE];

@@ -294,7 +294,8 @@ __global__ void populate_kernel(PopulateArgs a)
 // marker count, weight sum, real_f / marker sum (1 per full-f particle); the host normalises.
 // ------------------------------------------------------------------------------------------------
 struct VHistArgs {
-    double const  *q1, *vx, *vy, *vz, *w;        // FP64 storage, or
+    double const  *q1, *vx, *vy, *vz, *w;        // FP64 storage (+ real_f, marker when the weights evolve), or
+    double const  *real_f, *marker;
     int32_t const *cell;                         // mixed-precision storage
     float const   *off, *fvx, *fvy, *fvz, *fw;
     int64_t        n;
@@ -344,7 +345,8 @@ __global__ void vhist_kernel(VHistArgs a)
         double *o = a.out + 3 * (static_cast<int64_t>(f1) * a.v2dim + static_cast<int64_t>(f2));
         atomicAdd(o, 1.0);
         atomicAdd(o + 1, w);
-        atomicAdd(o + 2, 1.0);
+        // real_f / marker; without evolving weights real_f = w and marker = 1 (the upload convention)
+        atomicAdd(o + 2, a.real_f ? __ddiv_rn(a.real_f[k], a.marker[k]) : w);
     }
 }
 

@@ -40,6 +40,13 @@ struct PushArgs {
     int            move_steps; // 1: CAM-CL full step; 2: PC half step, push, half step; 0: deposit only
     int            deposit_mask; // bit0: deposit at x^N, bit1: deposit at the end position
     int            write_back;   // 0 for the PC predictor (particles are not kept)
+    // evolving weights (push_kernel<..., PSD = true>): Particle::PSD arrays and the equilibrium
+    // bi-Maxwellian f0 of PartSpecies::impl_update_weight (PartSpecies.cc:178-208)
+    double        *real_f, *marker;
+    double         nu_dt;          // psd_refresh_frequency * dt
+    double         vth1, vth1_cubed, T2_T1;
+    int            psd_refresh;    // nu != 0
+    int            delta_f;        // weight = (real_f - f0) / marker, else real_f / marker
 };
 
 template <int O>
@@ -119,6 +126,33 @@ __device__ __forceinline__ d3 background_B(PushArgs const &a, double q1, d3 v, d
     }
 }
 
+// MaxwellianVDF::f0 (VDF/MaxwellianVDF.cc:33-92) at (v, q1): cart_to_mfa is the identity on the
+// field line (MFABasis.h:96-99), eta = n0 = 1 / (T2OT1_eq + (1 - T2OT1_eq) cos^2(xi D1 q1)),
+// T2OT1 = T2OT1_eq eta, f0 = n0 exp(-x1^2) (2/sqrt(pi))/2 exp(-(x2^2 + x3^2)/T2OT1)/(pi T2OT1)/vth1^3
+__device__ __forceinline__ double equilibrium_f0(PushArgs const &a, d3 v, double cs)
+{
+    double const eta   = 1 / (a.T2_T1 + (1 - a.T2_T1) * cs * cs);
+    double const T2OT1 = a.T2_T1 * eta;
+    double const x1 = v.x / a.vth1, x2 = v.y / a.vth1, x3 = v.z / a.vth1;
+    double const f1 = exp(-x1 * x1) * 1.1283791670955126 * .5;
+    double const f2 = exp(-(x2 * x2 + x3 * x3) / T2OT1) / (3.141592653589793 * T2OT1);
+    return (1 * eta) * ((f1 * f2) / a.vth1_cubed);
+}
+// PartSpecies::impl_update_weight for one particle after its velocity update: the new weight,
+// with real_f relaxed toward f0 when the PSD is refreshed
+__device__ __forceinline__ double update_weight(PushArgs const &a, d3 v, double q1, double &real_f, double marker)
+{
+    double cs = 1;
+    if (a.xi != 0) {
+        double sn;
+        sincos_taylor(a.xiD1 * q1, sn, cs);
+    }
+    double const f0 = equilibrium_f0(a, v, cs);
+    if (a.psd_refresh)
+        real_f = (real_f + a.nu_dt * f0) / (1 + a.nu_dt);
+    return a.delta_f ? (real_f - f0) / marker : real_f / marker;
+}
+
 // E and dB interpolated at the particle (GridArray.h:110-119) from the interleaved cell records
 template <int O>
 __device__ __forceinline__ void interp_EB(double const *eb, Shape<O> const &sh, d3 &E, d3 &B)
@@ -159,16 +193,26 @@ constexpr int PIPE_W              = 8; // cells per deposit window: 4 quantities
 static_assert(4 * PIPE_W == 32, "a window flush reduce-scatters exactly 32 values");
 
 // a stage holds one chunk; the consumers overwrite it in place with the new state, which the
-// producer then stores
-struct PipeStage {
+// producer then stores.  With evolving weights (PSD) a stage also holds real_f and marker, and
+// the pipeline is one stage shorter so that two CTAs still fit an SM.
+template <bool PSD>
+struct PipeStageT {
     double  q1[PIPE_CHUNK], vx[PIPE_CHUNK], vy[PIPE_CHUNK], vz[PIPE_CHUNK], w[PIPE_CHUNK];
     int32_t pid[PIPE_CHUNK];
+    double  real_f[PSD ? PIPE_CHUNK : 2], marker[PSD ? PIPE_CHUNK : 2];
 };
-constexpr size_t PIPE_BAR_OFFSET = sizeof(PipeStage) * PIPE_STAGES;
-constexpr size_t PIPE_COL_OFFSET = PIPE_BAR_OFFSET + 128;
+using PipeStage = PipeStageT<false>;
+template <bool PSD>
+struct PipeLayout {
+    static constexpr int    STAGES     = PSD ? PIPE_STAGES - 1 : PIPE_STAGES;
+    static constexpr size_t BAR_OFFSET = sizeof(PipeStageT<PSD>) * STAGES;
+    static constexpr size_t COL_OFFSET = BAR_OFFSET + 128;
+};
 constexpr size_t PIPE_COL_BYTES  = sizeof(double2) * PIPE_CONSUMER_WARPS * 2 * PIPE_W * 2 * 32;
-constexpr size_t PIPE_SMEM       = PIPE_COL_OFFSET + PIPE_COL_BYTES;
+constexpr size_t PIPE_SMEM       = PipeLayout<false>::COL_OFFSET + PIPE_COL_BYTES;
+constexpr size_t PIPE_SMEM_PSD   = PipeLayout<true>::COL_OFFSET + PIPE_COL_BYTES;
 static_assert(2 * PIPE_STAGES * sizeof(uint64_t) <= 128, "barriers fit before the columns");
+static_assert(2 * (PIPE_SMEM_PSD + 1024) <= 233472, "two CTAs with evolving weights fit an SM");
 
 __device__ __forceinline__ uint32_t round16(uint32_t b) { return (b + 15u) & ~15u; }
 
@@ -273,6 +317,7 @@ __device__ __forceinline__ void deposit_direct(PushArgs const &a, int d, Shape<O
 // The table travels as the kernel's parameter block (at most 32 KB).
 template <int MAXG>
 struct PushGroups {
+    static constexpr int MAX = MAXG;
     int      n;
     int64_t  chunk0[MAXG + 1]; // first chunk of each group; chunk0[n] = number of chunks
     PushArgs g[MAXG];
@@ -291,13 +336,15 @@ __device__ __forceinline__ int group_of(PushGroups<MAXG> const &G, int64_t chunk
     }
 }
 
-template <int O, bool MIRROR, int BC, int MAXG>
+template <int O, bool MIRROR, int BC, int MAXG, bool PSD = false>
 __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(PushGroups<MAXG> const __grid_constant__ G)
 {
-    constexpr int SPAN = PIPE_W - 1 - O; // largest stencil base offset inside the window
+    constexpr int      SPAN        = PIPE_W - 1 - O; // largest stencil base offset inside the window
+    constexpr int      PIPE_STAGES = PipeLayout<PSD>::STAGES;
+    using Stage                    = PipeStageT<PSD>;
     extern __shared__ __align__(128) unsigned char smraw[];
-    PipeStage    *stage = reinterpret_cast<PipeStage *>(smraw);
-    uint64_t     *full  = reinterpret_cast<uint64_t *>(smraw + PIPE_BAR_OFFSET);
+    Stage        *stage = reinterpret_cast<Stage *>(smraw);
+    uint64_t     *full  = reinterpret_cast<uint64_t *>(smraw + PipeLayout<PSD>::BAR_OFFSET);
     uint64_t     *empty = full + PIPE_STAGES;
     int const     warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int64_t const nchunks = G.chunk0[G.n];
@@ -335,8 +382,10 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
                         bulk_store(a.vx + start, stage[s].vx, b8);
                         bulk_store(a.vy + start, stage[s].vy, b8);
                         bulk_store(a.vz + start, stage[s].vz, b8);
-                        if (BC == BCK_ABSORBING)
+                        if (BC == BCK_ABSORBING || PSD)
                             bulk_store(a.w + start, stage[s].w, b8);
+                        if (PSD)
+                            bulk_store(a.real_f + start, stage[s].real_f, b8);
                         bulk_commit();
                     }
                     bulk_wait_read_all();
@@ -348,7 +397,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
                     int64_t const   start = (c0 + i - G.chunk0[gl]) * PIPE_CHUNK;
                     uint32_t const  cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
                     uint32_t const  b8 = round16(cnt * 8), b4 = round16(cnt * 4);
-                    mbar_arrive_expect_tx(&full[s], 5 * b8 + (lpid ? b4 : 0));
+                    mbar_arrive_expect_tx(&full[s], (PSD ? 7 : 5) * b8 + (lpid ? b4 : 0));
                     bulk_load(stage[s].q1, a.q1 + start, b8, &full[s]);
                     bulk_load(stage[s].vx, a.vx + start, b8, &full[s]);
                     bulk_load(stage[s].vy, a.vy + start, b8, &full[s]);
@@ -356,6 +405,10 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
                     bulk_load(stage[s].w, a.w + start, b8, &full[s]);
                     if (lpid)
                         bulk_load(stage[s].pid, a.pid + start, b4, &full[s]);
+                    if (PSD) {
+                        bulk_load(stage[s].real_f, a.real_f + start, b8, &full[s]);
+                        bulk_load(stage[s].marker, a.marker + start, b8, &full[s]);
+                    }
                 }
             }
             bulk_wait_all();
@@ -365,7 +418,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
 
     // ---------------- consumers ----------------
     ColWindow64 win;
-    win.col  = reinterpret_cast<double2 *>(smraw + PIPE_COL_OFFSET) + warp * 2 * PIPE_W * 2 * 32;
+    win.col  = reinterpret_cast<double2 *>(smraw + PipeLayout<PSD>::COL_OFFSET) + warp * 2 * PIPE_W * 2 * 32;
     win.base = ColWindow64::NONE;
     win.zero(lane);
     unsigned bad = 0;
@@ -393,7 +446,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
         }
         int64_t const start = (c0 + i - G.chunk0[gc]) * PIPE_CHUNK;
         int const     cnt   = static_cast<int>(min(static_cast<int64_t>(PIPE_CHUNK), a.n - start));
-        PipeStage    &P     = stage[s];
+        Stage        &P     = stage[s];
         int const     w0    = warp * 32 * PIPE_PPT;
 
         // slots past `cnt` hold stale finite data and are processed but never deposited or stored
@@ -409,7 +462,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
             double       q1    = P.q1[idx];
             d3           v     = { P.vx[idx], P.vy[idx], P.vz[idx] };
             double       w     = P.w[idx];
-            double const w_in  = w;
+            double       w_in  = w;
             int32_t      pid   = load_pid ? P.pid[idx] : 0;
             bool         alive = true;
             if (a.move_steps == 2) {
@@ -430,6 +483,12 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
                     double   c2;
                     d3 const B = background_B<MIRROR>(a, q1, v, c2) + dB;
                     v          = boris_push(a.boris, v, B, E);
+                    if constexpr (PSD) { // the weight at the new velocity and the push position
+                        double rf     = P.real_f[idx];
+                        w             = update_weight(a, v, q1, rf, P.marker[idx]);
+                        w_in          = w;
+                        P.real_f[idx] = rf;
+                    }
                     // contravariant q1-velocity v_x cos^2 / D1 at the position of the push (CurviBasis.h:65-69)
                     double moved = (a.inv_D1 * c2) * v.x * (a.move_steps == 2 ? 0.5 * a.dt : a.dt);
                     q1 += moved;
@@ -448,7 +507,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
             P.vx[idx]  = v.x;
             P.vy[idx]  = v.y;
             P.vz[idx]  = v.z;
-            if (BC == BCK_ABSORBING)
+            if (BC == BCK_ABSORBING || PSD)
                 P.w[idx] = w;
 
             ds0[k] = sh0;

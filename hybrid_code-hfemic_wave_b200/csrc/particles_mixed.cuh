@@ -286,6 +286,7 @@ struct ColWindow {
 // the groups of one launch, as PushGroups in particles.cuh
 template <int MAXG>
 struct PushGroupsMixed {
+    static constexpr int MAX = MAXG;
     int           n;
     int64_t       chunk0[MAXG + 1];
     PushArgsMixed g[MAXG];

@@ -9,6 +9,12 @@
 
 namespace h1d {
 
+__global__ void fill_kernel(double *a, int64_t n, double v)
+{
+    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n)
+        a[i] = v;
+}
 __global__ void iota_kernel(int32_t *pid, int64_t n)
 {
     int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -47,7 +53,10 @@ __global__ void prep_fields_kernel(double *B, double *E, double *EB, float *EBf,
 // collect_all scaling by 1/Nc (PartSpecies.cc:346-348) and boundary_gather of the three moments
 // (SubdomainDelegate.cc:115-181).  raw: 10 arrays of M (n, nV xyz, nvv xx yy zz xy yz zx);
 // out: GridArray layout n[M], nV[3M], nvv[6M].
-__global__ void finalize_kinetic_kernel(double const *raw, double *out, int Nx, double s1, int reflecting)
+// delta-f species (eq != null): + the equilibrium n0 (M) and nvv0 (6M) x m_moment_weighting_factor
+// (PartSpecies.cc:129-143), before the ghost fold as in the reference
+__global__ void finalize_kinetic_kernel(double const *raw, double const *eq, double *out, int Nx, double s1,
+                                        int reflecting)
 {
     int const M = Nx + 2 * PAD;
     double   *n = out, *nV = out + M, *nvv = out + 4 * M;
@@ -57,6 +66,11 @@ __global__ void finalize_kinetic_kernel(double const *raw, double *out, int Nx, 
             nV[3 * i + c] = raw[(1 + c) * M + i] * s1;
         for (int c = 0; c < 6; ++c)
             nvv[6 * i + c] = raw[(4 + c) * M + i] * s1;
+        if (eq) {
+            n[i] = n[i] + eq[i] * 1.0;
+            for (int c = 0; c < 6; ++c)
+                nvv[6 * i + c] = nvv[6 * i + c] + eq[M + 6 * i + c] * 1.0;
+        }
     }
     __syncthreads();
     if (threadIdx.x != 0)

@@ -20,5 +20,7 @@ cudaError_t launch_push_groups(PushArgs const *args, int n, int order, bool mirr
                                cudaStream_t st);
 cudaError_t launch_push_groups(PushArgsMixed const *args, int n, int order, bool mirror, int bc, int max_ctas,
                                cudaStream_t st);
+// one FP64 pass over a species whose weights evolve (push_kernel<..., PSD = true>)
+cudaError_t launch_push_psd(PushArgs const &a, int order, bool mirror, int bc, int max_ctas, cudaStream_t st);
 
 } // namespace h1d

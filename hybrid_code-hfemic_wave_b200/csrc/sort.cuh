@@ -260,22 +260,25 @@ struct MoveKeys {
         idx_out[pos]  = r.id;
     }
 };
-// ... or, in the last pass, the FP64 particle records (q1, vx, vy, vz, w, pid)
-struct MoveFP64 {
+// ... or, in the last pass, the FP64 particle records (q1, vx, vy, vz, w, pid; with PSD also
+// real_f and marker)
+template <bool PSD>
+struct MoveFP64T {
+    static constexpr int NV   = PSD ? 7 : 5;
     static constexpr int HOLD = SORT_ITEMS / 2;
-    double const        *src[5];
-    int32_t const *pid_src;
-    double        *dst[5];
-    int32_t       *pid_dst;
+    double const        *src[NV];
+    int32_t const       *pid_src;
+    double              *dst[NV];
+    int32_t             *pid_dst;
     struct Rec {
-        double  v[5];
+        double  v[NV];
         int32_t pid;
     };
     __device__ __forceinline__ Rec load(uint32_t, uint32_t j) const
     {
         Rec r;
 #pragma unroll
-        for (int k = 0; k < 5; ++k)
+        for (int k = 0; k < NV; ++k)
             r.v[k] = src[k][j];
         r.pid = pid_src[j];
         return r;
@@ -283,11 +286,12 @@ struct MoveFP64 {
     __device__ __forceinline__ void store(uint32_t pos, Rec const &r) const
     {
 #pragma unroll
-        for (int k = 0; k < 5; ++k)
+        for (int k = 0; k < NV; ++k)
             dst[k][pos] = r.v[k];
         pid_dst[pos] = r.pid;
     }
 };
+using MoveFP64 = MoveFP64T<false>;
 // ... or the mixed-precision records (offset, vx, vy, vz, w as FP32; cell, pid)
 struct MoveMixed {
     static constexpr int HOLD = SORT_ITEMS;

@@ -51,7 +51,7 @@
 extern "C" {
 #endif
 
-#define H1D_ABI_VERSION 2
+#define H1D_ABI_VERSION 3
 
 /* number of ghost cells on each side; Input::number_of_ghost_cells (Include/Inputs.h:22) */
 #define H1D_PAD 3
@@ -81,7 +81,12 @@ enum { H1D_BC_PERIODIC = 0, H1D_BC_REFLECTING = 1, H1D_BC_ABSORBING = 2 };
 /* arithmetic of the particle push/deposit; the field cycle is FP64 in both */
 enum { H1D_PREC_FP64 = 0, H1D_PREC_MIXED = 1 };
 
-/* KineticPlasmaDesc (LibPIC/PIC/PlasmaDesc.h:118-177), full-f only */
+/* particle schemes (ParticleScheme, LibPIC/PIC/Predefined.h:28-31) */
+#define H1D_FULL_F  0
+#define H1D_DELTA_F 1
+
+/* KineticPlasmaDesc (LibPIC/PIC/PlasmaDesc.h:118-177) of a bi-Maxwellian species
+ * (BiMaxPlasmaDesc, PlasmaDesc.h:207-236) */
 typedef struct h1d_kinetic_desc {
     double  Oc;          /* PlasmaDesc::Oc, signed cyclotron frequency */
     double  op;          /* PlasmaDesc::op, plasma frequency */
@@ -90,6 +95,18 @@ typedef struct h1d_kinetic_desc {
     int64_t shape_order; /* 1 (CIC), 2 (TSC) or 3 */
     double  moment_norm; /* PartSpecies::Nc (PartSpecies.cc:150-154): Nx*Nc*Nrefcell_div_Ntotal,
                             the particle count of the reference cell used to normalise moments */
+    /* Phase-space density weighting.  With scheme H1D_DELTA_F, or a nonzero psd_refresh_frequency,
+     * every particle carries its physical density real_f and marker density marker
+     * (Particle::PSD, LibPIC/PIC/Particle.h:26-34; h1d_upload_psd) and its weight is recomputed
+     * every step from the equilibrium bi-Maxwellian f0 (vth1, T2_T1) at its new velocity
+     * (PartSpecies::impl_update_weight, Core/PartSpecies.cc:178-208); delta-f moments add the
+     * equilibrium moments n0, nV0 = 0, nvv0 (PartSpecies.cc:115-143). */
+    int32_t scheme;                /* H1D_FULL_F or H1D_DELTA_F (KineticPlasmaDesc::scheme) */
+    int32_t reserved;
+    double  psd_refresh_frequency; /* KineticPlasmaDesc::psd_refresh_frequency (>= 0) */
+    double  vth1;                  /* equilibrium parallel thermal speed, sqrt(beta1) c |Oc| / op
+                                      (MaxwellianVDF.cc:24); used when the weights evolve */
+    double  T2_T1;                 /* equilibrium T_perp / T_par at the equator */
 } h1d_kinetic_desc;
 
 /* ColdPlasmaDesc (PlasmaDesc.h:92-114) */
@@ -168,6 +185,13 @@ int h1d_destroy(h1d_run *run);
  * Replaces any previous particles of that species. */
 int h1d_upload_particles(h1d_run *run, int s, int64_t n, const double *q1, const double *vx,
                          const double *vy, const double *vz, const double *w);
+/* Phase-space densities of the particles of species `s` (Particle::PSD::real_f, ::marker), in the
+ * order of the last h1d_upload_particles; required before the first step of a species whose
+ * weights evolve (scheme H1D_DELTA_F or psd_refresh_frequency != 0), INVALID_ARG otherwise or
+ * when n differs from the uploaded count.  FP64 runs only. */
+int h1d_upload_psd(h1d_run *run, int s, int64_t n, const double *real_f, const double *marker);
+/* ... and back, in the order of h1d_download_particles; either pointer may be NULL. */
+int h1d_download_psd(h1d_run *run, int s, double *real_f, double *marker);
 /* PartSpecies::populate with a bi-Maxwellian MaxwellianVDF (VDF/MaxwellianVDF.cc:88-134, 300-319),
  * on the device: n particles of kinetic species `s` with parallel beta `beta1` and T_perp/T_par
  * `T2_T1`, positions from the base-2 radical inverse through q1_of_N, velocities from base-3/5
@@ -212,7 +236,8 @@ int h1d_energy(h1d_run *run, double *dB2O2, double *dE2O2, double *KE_lab, doubl
  * histogram of kinetic species `s` over the particles with q1 in [ext_loc, ext_loc + ext_len),
  * relative to the bulk velocity of the recorded moments, v1 (parallel) in v1dim bins over
  * [v1min, v1min + v1len) and v2 (perpendicular speed) in v2dim bins over [v2min, v2min + v2len).
- * out[3 * (i1 * v2dim + i2) + {0, 1, 2}] = {marker count, weight sum, real_f/marker sum} / total,
+ * out[3 * (i1 * v2dim + i2) + {0, 1, 2}] = {marker count, weight sum, real_f/marker sum} / total
+ * (real_f/marker = w for species whose weights do not evolve),
  * total = the particles in the extent (the recorder's normalisation).  Zero-based bins; the
  * recorder writes them one-based. */
 int h1d_vhistogram(h1d_run *run, int s, double ext_loc, double ext_len, double v1min, double v1len, int64_t v1dim,

@@ -9,6 +9,8 @@
  *   Domain_PC::advance_by / predictor_step / corrector_step         (Core/Domain_PC.cc:21-205)
  *   Domain::collect_smooth                                          (Core/Domain.hh:155-194)
  *   PartSpecies::update_vel/update_pos/collect_part/collect_all     (Core/PartSpecies.cc:132-139, 210-349)
+ *   PartSpecies::impl_update_weight, equilibrium moments            (Core/PartSpecies.cc:80-87, 115-143, 178-208;
+ *                                                                    VDF/MaxwellianVDF.cc:33-92, .h:56-70)
  *   ColdSpecies::update_vel/collect_part/collect_all                (Core/ColdSpecies.cc:251-297)
  *   BField::update, EField::update, Charge/Current/Lambda/Gamma     (Core/BField.cc:74-124, EField.cc:224-330,
  *                                                                    Charge.cc:70-80, Current.cc:165-188)
@@ -44,6 +46,7 @@ typedef struct {
     int64_t  n, cap;
     double  *q1, *vx, *vy, *vz, *w;
     int64_t *pid;
+    double  *real_f, *marker; /* Particle::PSD (Particle.h:26-34) */
 } Bucket;
 
 typedef struct orc_run {
@@ -64,6 +67,7 @@ typedef struct orc_run {
     Bucket  part[H1D_MAX_KINETIC];
     Bucket  pred;            /* Domain_PC::part_predict bucket */
     double *mom0[H1D_MAX_KINETIC], *mom1[H1D_MAX_KINETIC], *mom2[H1D_MAX_KINETIC];
+    double *eq0[H1D_MAX_KINETIC], *eq2[H1D_MAX_KINETIC]; /* PartSpecies::equilibrium_mom0/2 (nV0 = 0) */
     double *pmom0, *pmom1;   /* predictor moments */
     /* cold species */
     double *cn_full[H1D_MAX_COLD], *cnV_full[H1D_MAX_COLD];
@@ -108,7 +112,9 @@ static void bucket_reserve(Bucket *b, int64_t cap)
     b->vz  = realloc(b->vz, sizeof(double) * nc);
     b->w   = realloc(b->w, sizeof(double) * nc);
     b->pid = realloc(b->pid, sizeof(int64_t) * nc);
-    if (!b->q1 || !b->vx || !b->vy || !b->vz || !b->w || !b->pid) {
+    b->real_f = realloc(b->real_f, sizeof(double) * nc);
+    b->marker = realloc(b->marker, sizeof(double) * nc);
+    if (!b->q1 || !b->vx || !b->vy || !b->vz || !b->w || !b->pid || !b->real_f || !b->marker) {
         fprintf(stderr, "oracle: out of memory\n");
         abort();
     }
@@ -117,6 +123,7 @@ static void bucket_reserve(Bucket *b, int64_t cap)
 static void bucket_free(Bucket *b)
 {
     free(b->q1), free(b->vx), free(b->vy), free(b->vz), free(b->w), free(b->pid);
+    free(b->real_f), free(b->marker);
     memset(b, 0, sizeof *b);
 }
 static void bucket_swap_elems(Bucket *b, int64_t i, int64_t j)
@@ -127,6 +134,8 @@ static void bucket_swap_elems(Bucket *b, int64_t i, int64_t j)
     t = b->vy[i], b->vy[i] = b->vy[j], b->vy[j] = t;
     t = b->vz[i], b->vz[i] = b->vz[j], b->vz[j] = t;
     t = b->w[i], b->w[i] = b->w[j], b->w[j] = t;
+    t = b->real_f[i], b->real_f[i] = b->real_f[j], b->real_f[j] = t;
+    t = b->marker[i], b->marker[i] = b->marker[j], b->marker[j] = t;
     int64_t u = b->pid[i];
     b->pid[i] = b->pid[j], b->pid[j] = u;
 }
@@ -140,6 +149,8 @@ static void bucket_push(Bucket *dst, Bucket const *src, int64_t k)
     dst->vz[i]  = src->vz[k];
     dst->w[i]   = src->w[k];
     dst->pid[i] = src->pid[k];
+    dst->real_f[i] = src->real_f[k];
+    dst->marker[i] = src->marker[k];
 }
 static void bucket_copy(Bucket *dst, Bucket const *src)
 {
@@ -151,6 +162,8 @@ static void bucket_copy(Bucket *dst, Bucket const *src)
     memcpy(dst->vz, src->vz, sizeof(double) * src->n);
     memcpy(dst->w, src->w, sizeof(double) * src->n);
     memcpy(dst->pid, src->pid, sizeof(int64_t) * src->n);
+    memcpy(dst->real_f, src->real_f, sizeof(double) * src->n);
+    memcpy(dst->marker, src->marker, sizeof(double) * src->n);
 }
 
 /* ------------------------------------------------------------------------------------------------
@@ -424,6 +437,8 @@ static void half_grid(orc_run const *R, double *full, double const *half)
 }
 
 /* PartSpecies::impl_update_velocity<O> (PartSpecies.cc:266-281) */
+static void update_weight(orc_run const *R, Bucket *b, h1d_kinetic_desc const *d, double dt);
+static int  evolves_psd(h1d_kinetic_desc const *d);
 static void update_velocity(orc_run *R, Bucket *b, h1d_kinetic_desc const *d, double *dB, double *E, double dt)
 {
     Boris const  boris = boris_make(dt, R->p.c, R->p.O0, d->Oc);
@@ -443,7 +458,86 @@ static void update_velocity(orc_run *R, Bucket *b, h1d_kinetic_desc const *d, do
         boris_push(&boris, &v, Bt, Ei);
         b->vx[k] = v.x, b->vy[k] = v.y, b->vz[k] = v.z;
     }
+    if (evolves_psd(d))
+        update_weight(R, b, d, dt);
 }
+/* MaxwellianVDF (VDF/MaxwellianVDF.cc:33-92) of the equilibrium a species' weights refer to:
+ * eta = n0 / n0_eq, T2OT1(pos) and the physical distribution f0(vel, pos) */
+static double vdf_eta(orc_run const *R, h1d_kinetic_desc const *d, double q1)
+{
+    double const cs = cos(R->xi * R->D1 * q1);
+    return 1 / (d->T2_T1 + (1 - d->T2_T1) * cs * cs);
+}
+static double vdf_f0(orc_run const *R, h1d_kinetic_desc const *d, V3 v, double q1)
+{
+    double const eta   = vdf_eta(R, d, q1);
+    double const T2OT1 = d->T2_T1 * eta;
+    double const vth1  = d->vth1;
+    double const x1 = v.x / vth1, x2 = v.y / vth1, x3 = v.z / vth1; /* cart_to_mfa is the identity on the axis */
+    double const f1 = exp(-x1 * x1) * M_2_SQRTPI * .5;
+    double const xx = x2 * x2 + x3 * x3;
+    double const f2 = exp(-xx / T2OT1) / (M_PI * T2OT1);
+    return (1 * eta) * ((f1 * f2) / (vth1 * vth1 * vth1));
+}
+static int evolves_psd(h1d_kinetic_desc const *d) { return d->scheme == H1D_DELTA_F || d->psd_refresh_frequency != 0; }
+
+/* PartSpecies::impl_update_weight (PartSpecies.cc:178-208) with nu_dt = psd_refresh_frequency * dt */
+static void update_weight(orc_run const *R, Bucket *b, h1d_kinetic_desc const *d, double dt)
+{
+    double const nu_dt   = d->psd_refresh_frequency * dt;
+    int const    refresh = d->psd_refresh_frequency != 0;
+    if (d->scheme == H1D_FULL_F) {
+        if (!refresh)
+            return;
+        for (int64_t k = 0; k < b->n; ++k) {
+            V3 const v  = { b->vx[k], b->vy[k], b->vz[k] };
+            b->real_f[k] = (b->real_f[k] + nu_dt * vdf_f0(R, d, v, b->q1[k])) / (1 + nu_dt);
+            b->w[k]      = b->real_f[k] / b->marker[k];
+        }
+    } else {
+        for (int64_t k = 0; k < b->n; ++k) {
+            V3 const     v  = { b->vx[k], b->vy[k], b->vz[k] };
+            double const f0 = vdf_f0(R, d, v, b->q1[k]);
+            if (refresh)
+                b->real_f[k] = (b->real_f[k] + nu_dt * f0) / (1 + nu_dt);
+            b->w[k] = (b->real_f[k] - f0) / b->marker[k];
+        }
+    }
+}
+
+/* the equilibrium moments cached by PartSpecies::populate (PartSpecies.cc:80-87) at the interior
+ * half-grid points; ghost cells stay zero (MaxwellianVDF.h:56-70) */
+static void cache_equilibrium(orc_run *R, int s)
+{
+    h1d_kinetic_desc const *d = &R->p.kinetic[s];
+    double const            q1min = R->half_min;
+    double const            hv2   = .5 * (d->vth1 * d->vth1);
+    for (long i = 0; i < R->Nx; ++i) {
+        double const q1  = (double)i + q1min;
+        double const eta = vdf_eta(R, d, q1);
+        double const n0  = 1 * eta;
+        double const T   = d->T2_T1 * eta;
+        *at1(R->eq0[s], i) = n0;
+        double *e = at6(R->eq2[s], i);
+        e[0] = (1 * hv2) * n0, e[1] = (T * hv2) * n0, e[2] = (T * hv2) * n0;
+        e[3] = (0 * hv2) * n0, e[4] = (0 * hv2) * n0, e[5] = (0 * hv2) * n0;
+    }
+}
+/* delta-f: moments += equilibrium * m_moment_weighting_factor (PartSpecies.cc:115-143), over all
+ * cells (GridArray dead_begin..dead_end) */
+static void add_equilibrium(orc_run const *R, int s, double *n, double *nV, double *nvv)
+{
+    if (R->p.kinetic[s].scheme != H1D_DELTA_F)
+        return;
+    for (long i = 0; i < R->M; ++i)
+        n[i] = n[i] + R->eq0[s][i] * 1.0;
+    for (long i = 0; i < 3 * R->M; ++i)
+        nV[i] = nV[i] + 0.0 * 1.0;
+    if (nvv)
+        for (long i = 0; i < 6 * R->M; ++i)
+            nvv[i] = nvv[i] + R->eq2[s][i] * 1.0;
+}
+
 /* PartSpecies::impl_update_pos (PartSpecies.cc:252-264): returns 1 if nothing moved too far */
 static int update_pos(orc_run *R, Bucket *b, double dt, double fraction)
 {
@@ -458,7 +552,8 @@ static int update_pos(orc_run *R, Bucket *b, double dt, double fraction)
     }
     return ok;
 }
-/* PartSpecies::impl_collect_part<O> (PartSpecies.cc:315-329) */
+static void add_equilibrium(orc_run const *R, int s, double *n, double *nV, double *nvv);
+/* PartSpecies::impl_collect_part<O> (PartSpecies.cc:315-329), then the delta-f equilibrium */
 static void collect_part(orc_run *R, Bucket const *b, h1d_kinetic_desc const *d, double *n, double *nV)
 {
     double const q1min = R->half_min;
@@ -484,6 +579,7 @@ static void collect_part(orc_run *R, Bucket const *b, h1d_kinetic_desc const *d,
         n[i] *= s;
     for (long i = 0; i < 3 * R->M; ++i)
         nV[i] *= s;
+    add_equilibrium(R, (int)(d - R->p.kinetic), n, nV, NULL);
 }
 /* PartSpecies::impl_collect_all (PartSpecies.cc:330-349): always CIC */
 static void collect_all(orc_run *R, Bucket const *b, h1d_kinetic_desc const *d, double *n, double *nV, double *nvv)
@@ -520,6 +616,7 @@ static void collect_all(orc_run *R, Bucket const *b, h1d_kinetic_desc const *d, 
         nV[i] *= s;
     for (long i = 0; i < 6 * R->M; ++i)
         nvv[i] *= s;
+    add_equilibrium(R, (int)(d - R->p.kinetic), n, nV, nvv);
 }
 
 /* counter-based gyro-phase draw in [-pi, pi) replacing the std::random_device-seeded
@@ -1112,6 +1209,10 @@ static int check_params(h1d_params const *p, char *msg, size_t cap)
             BAD("kinetic species %d: moment_norm must be positive", s);
         if (d->n_smooth < 0)
             BAD("kinetic species %d: negative smoothing count", s);
+        if ((d->scheme != H1D_FULL_F && d->scheme != H1D_DELTA_F) || !(d->psd_refresh_frequency >= 0))
+            BAD("kinetic species %d: unknown particle scheme or negative psd_refresh_frequency", s);
+        if ((d->scheme == H1D_DELTA_F || d->psd_refresh_frequency != 0) && (!(d->vth1 > 0) || !(d->T2_T1 > 0)))
+            BAD("kinetic species %d: evolving weights need the equilibrium vth1 > 0 and T2_T1 > 0", s);
     }
     for (int s = 0; s < p->n_cold; ++s)
         if (p->cold[s].Oc == 0 || !(p->cold[s].op > 0) || p->cold[s].n_smooth < 0)
@@ -1165,6 +1266,11 @@ int orc_create(h1d_params const *p, orc_run **out)
     R->Pe = xcalloc(M, 8), R->dPe = xcalloc(3 * M, 8), R->Je = xcalloc(3 * M, 8), R->covar = xcalloc(3 * M, 8), R->contr = xcalloc(3 * M, 8);
     for (int s = 0; s < p->n_kinetic; ++s)
         R->mom0[s] = xcalloc(M, 8), R->mom1[s] = xcalloc(3 * M, 8), R->mom2[s] = xcalloc(6 * M, 8);
+    for (int s = 0; s < p->n_kinetic; ++s) {
+        R->eq0[s] = xcalloc(M, 8), R->eq2[s] = xcalloc(6 * M, 8);
+        if (evolves_psd(&p->kinetic[s]) || p->kinetic[s].scheme == H1D_DELTA_F)
+            cache_equilibrium(R, s);
+    }
     R->pmom0 = xcalloc(M, 8), R->pmom1 = xcalloc(3 * M, 8);
     for (int s = 0; s < p->n_cold; ++s) {
         R->cn_full[s] = xcalloc(M, 8), R->cnV_full[s] = xcalloc(3 * M, 8);
@@ -1188,6 +1294,8 @@ int orc_destroy(orc_run *R)
         free(all[k]);
     for (int s = 0; s < R->p.n_kinetic; ++s)
         free(R->mom0[s]), free(R->mom1[s]), free(R->mom2[s]), bucket_free(&R->part[s]);
+    for (int s = 0; s < R->p.n_kinetic; ++s)
+        free(R->eq0[s]), free(R->eq2[s]);
     for (int s = 0; s < R->p.n_cold; ++s)
         free(R->cn_full[s]), free(R->cnV_full[s]), free(R->cmom0[s]), free(R->cmom1[s]), free(R->cmom2[s]);
     for (int e = 0; e < R->p.n_sources; ++e)
@@ -1208,7 +1316,23 @@ int orc_upload_particles(orc_run *R, int s, int64_t n, double const *q1, double 
     memcpy(b->q1, q1, 8 * n), memcpy(b->vx, vx, 8 * n), memcpy(b->vy, vy, 8 * n), memcpy(b->vz, vz, 8 * n),
         memcpy(b->w, w, 8 * n);
     for (int64_t k = 0; k < n; ++k)
-        b->pid[k] = k;
+        b->pid[k] = k, b->real_f[k] = w[k], b->marker[k] = 1.0;
+    return H1D_OK;
+}
+int orc_upload_psd(orc_run *R, int s, int64_t n, double const *real_f, double const *marker)
+{
+    if (!R || s < 0 || s >= R->p.n_kinetic || n != R->part[s].n || (n && (!real_f || !marker)))
+        return H1D_ERR_INVALID_ARG;
+    memcpy(R->part[s].real_f, real_f, 8 * n), memcpy(R->part[s].marker, marker, 8 * n);
+    return H1D_OK;
+}
+int orc_download_psd(orc_run *R, int s, double *real_f, double *marker)
+{
+    if (!R || s < 0 || s >= R->p.n_kinetic)
+        return H1D_ERR_INVALID_ARG;
+    Bucket const *b = &R->part[s];
+    if (real_f) memcpy(real_f, b->real_f, 8 * b->n);
+    if (marker) memcpy(marker, b->marker, 8 * b->n);
     return H1D_OK;
 }
 int orc_upload_fields(orc_run *R, double const *B, double const *E)
@@ -1365,7 +1489,8 @@ int orc_download_cold(orc_run *R, int i, double *n, double *nV, double *nvv, dou
  * to the local bulk velocity nV/n interpolated with Shape<1> from the recorded moments (zero where
  * n < 1e-15), gyro-averaged (v1 = v_par, v2 = |v_perp|; the field-aligned basis is Cartesian on the
  * field line), binned by floor((v - min) * dim / len); per bin {marker count, weight sum,
- * real_f/marker sum (1 per full-f particle)} divided by the number of particles in the extent. */
+ * real_f/marker sum} divided by the number of particles in the extent (without a phase-space
+ * density upload real_f = w and marker = 1, so real_f/marker = w). */
 int orc_vhistogram(orc_run *R, int s, double ext_loc, double ext_len, double v1min, double v1len, int64_t v1dim,
                    double v2min, double v2len, int64_t v2dim, double *out, int64_t *total)
 {
@@ -1395,7 +1520,7 @@ int orc_vhistogram(orc_run *R, int s, double ext_loc, double ext_len, double v1m
         double const f2 = floor((v2 - v2min) * (double)v2dim / v2len);
         if (f1 >= 0 && f1 < (double)v1dim && f2 >= 0 && f2 < (double)v2dim) {
             double *o = out + 3 * ((int64_t)f1 * v2dim + (int64_t)f2);
-            o[0] += 1, o[1] += b->w[k], o[2] += 1;
+            o[0] += 1, o[1] += b->w[k], o[2] += b->real_f[k] / b->marker[k];
         }
     }
     if (count > 0)

@@ -43,9 +43,13 @@ def render(cfg) -> str:
     else:
         raise SystemExit("the reference has no absorbing particle boundary")
     closure = "isothermal" if cfg.efluid.closure == C.ISOTHERMAL else "adiabatic"
-    kin = ",\n        ".join(
-        f"BiMaxPlasmaDesc({{ {{ {r(k.Oc)}, {r(k.op)}, {k.n_smooth} }}, {k.Nc}, {SHAPE[k.shape_order]}, full_f }}, "
-        f"{r(k.beta1)}, {r(k.T2_T1)})" for k in cfg.kinetic)
+    def kdesc(k):
+        scheme = "delta_f" if k.scheme == C.DELTA_F else "full_f"
+        return (f"BiMaxPlasmaDesc({{ {{ {r(k.Oc)}, {r(k.op)}, {k.n_smooth} }}, {k.Nc}, {SHAPE[k.shape_order]}, "
+                f"{r(float(k.psd_refresh_frequency))}, {scheme}, {r(float(k.initial_weight))}, "
+                f"{r(float(k.marker_temp_ratio))} }}, {r(k.beta1)}, {r(k.T2_T1)})")
+
+    kin = ",\n        ".join(kdesc(k) for k in cfg.kinetic)
     cold = ",\n        ".join(f"ColdPlasmaDesc({{ {r(c.Oc)}, {r(c.op)}, {c.n_smooth} }})" for c in cfg.cold)
     def cplx(z):
         z = complex(z)

@@ -98,6 +98,25 @@ double moment_norm(ParamSet const &params, Desc const &desc)
         return Np * vdf->Nrefcell_div_Ntotal();
     return 1;
 }
+// the equilibrium moments PartSpecies::populate caches before loading (PartSpecies.cc:80-87), for
+// a species whose particles come from a state file instead (as a snapshot load restores them)
+template <class Desc>
+void cache_equilibrium(ParamSet const &params, Desc const &desc, PartSpecies &sp)
+{
+    auto const vdf   = VDFVariant::make(desc, params.geomtr, params.full_grid_whole_domain_extent, params.c);
+    auto const q1min = params.half_grid_subdomain_extent.min();
+    for (long i = 0; i < sp.equilibrium_mom0.size(); ++i) {
+        CurviCoord const pos{ i + q1min };
+        sp.equilibrium_mom0[i] = vdf->n0(pos);
+        sp.equilibrium_mom1[i] = vdf->nV0(pos);
+        sp.equilibrium_mom2[i] = vdf->nvv0(pos);
+    }
+}
+template <class... Ts, std::size_t... Is>
+void cache_equilibria(ParamSet const &params, std::tuple<Ts...> const &descs, Domain &d, std::index_sequence<Is...>)
+{
+    (cache_equilibrium(params, std::get<Is>(descs), d.part_species.at(Is)), ...);
+}
 template <class... Ts, std::size_t... Is>
 std::vector<double> moment_norms(ParamSet const &params, std::tuple<Ts...> const &descs, std::index_sequence<Is...>)
 {
@@ -155,7 +174,7 @@ constexpr std::size_t count(GridArray<T, N, Pad> const &) { return sizeof(T) / s
 void dump(Domain const &d, ParamSet const &params, char const *path, int64_t step)
 {
     Writer w{ path };
-    w.put("H1DSTATE", 8);
+    w.put("H1DSTAT2", 8);
     w.i64(params.Nx);
     w.i64(Pad);
     w.i64(static_cast<int64_t>(d.part_species.size()));
@@ -177,6 +196,12 @@ void dump(Domain const &d, ParamSet const &params, char const *path, int64_t ste
         for (Particle const &p : sp.bucket)
             ids.push_back(p.id);
         w.put(ids.data(), ids.size());
+        for (int c = 0; c < 2; ++c) { // phase-space density: real_f, marker
+            int64_t k = 0;
+            for (Particle const &p : sp.bucket)
+                a[k++] = c == 0 ? p.psd.real_f : p.psd.marker;
+            w.put(a.data(), n);
+        }
     }
     w.put(raw(d.bfield), count(d.bfield));
     w.put(raw(d.efield), count(d.efield));
@@ -201,7 +226,8 @@ int64_t load(Domain &d, ParamSet const &params, char const *path)
     Reader r{ path };
     char   magic[8];
     r.get(magic, 8);
-    if (std::memcmp(magic, "H1DSTATE", 8) != 0)
+    bool const with_psd = std::memcmp(magic, "H1DSTAT2", 8) == 0;
+    if (!with_psd && std::memcmp(magic, "H1DSTATE", 8) != 0)
         throw std::runtime_error{ "bad state file" };
     if (r.i64() != params.Nx || r.i64() != Pad || r.i64() != int64_t(d.part_species.size())
         || r.i64() != int64_t(d.cold_species.size()))
@@ -216,12 +242,17 @@ int64_t load(Domain &d, ParamSet const &params, char const *path)
             r.get(v.data(), n);
         std::vector<int64_t> ids(n);
         r.get(ids.data(), n);
+        std::vector<double> real_f(a[4]), marker(n, 1.0); // without a PSD: real_f = weight, marker = 1
+        if (with_psd) {
+            r.get(real_f.data(), n);
+            r.get(marker.data(), n);
+        }
         sp.bucket.clear();
         for (int64_t k = 0; k < n; ++k) {
             Particle p;
             p.pos    = CurviCoord{ a[0][k] };
             p.vel    = CartVector{ a[1][k], a[2][k], a[3][k] };
-            p.psd    = Particle::PSD{ a[4][k], a[4][k], 1.0 };
+            p.psd    = Particle::PSD{ a[4][k], real_f[k], marker[k] };
             p.id     = ids[k];
             sp.bucket.push_back(p);
         }
@@ -266,6 +297,7 @@ try {
     }
     if (mode == "run" && argc == 6) {
         int64_t    step   = load(*domain, params, argv[2]);
+        cache_equilibria(params, params.part_descs, *domain, ParamSet::part_indices{});
         long const steps  = std::atol(argv[3]);
         long const chunks = std::atol(argv[4]);
         for (long k = 1; k <= chunks; ++k) {

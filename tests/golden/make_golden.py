@@ -20,7 +20,8 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 NAMES = ["p1_cic_periodic", "p2_tsc_mirror_reflecting", "p3_o3_adiabatic_periodic",
-         "p4_pc_tsc_mirror_reflecting", "p5_tsc_mirror_source", "p6_pc_source"]
+         "p4_pc_tsc_mirror_reflecting", "p5_tsc_mirror_source", "p6_pc_source", "p7_psd_tsc_mirror_reflecting",
+         "p8_pc_psd_periodic"]
 
 
 def main():

@@ -1,8 +1,10 @@
 """Reader for the raw state files written by oracle/ref/ref_driver.cc (``dump``).
 
 layout (little endian):
-  char[8] "H1DSTATE"; int64 Nx, pad, n_kinetic, n_cold, step; double moment_norm[n_kinetic]
-  per kinetic species: int64 n; double q1[n], vx[n], vy[n], vz[n], w[n]; int64 id[n]
+  char[8] "H1DSTAT2" (or "H1DSTATE": no real_f/marker); int64 Nx, pad, n_kinetic, n_cold, step;
+  double moment_norm[n_kinetic]
+  per kinetic species: int64 n; double q1[n], vx[n], vy[n], vz[n], w[n]; int64 id[n];
+                       double real_f[n], marker[n]      (the phase-space density Particle::PSD)
   B[M*3], E[M*3], charge[M], current[M*3]                       (M = Nx + 2*pad)
   per kinetic species: n[M], nV[M*3], nvv[M*6]
   per cold species:    n_full[M], nV_full[M*3], n[M], nV[M*3], nvv[M*6]
@@ -13,8 +15,9 @@ import numpy as np
 def read_state(path):
     with open(path, "rb") as f:
         buf = f.read()
-    if buf[:8] != b"H1DSTATE":
+    if buf[:8] not in (b"H1DSTATE", b"H1DSTAT2"):
         raise ValueError("not a state file")
+    with_psd = buf[:8] == b"H1DSTAT2"
     off = 8
 
     def i64(k=1):
@@ -36,6 +39,10 @@ def read_state(path):
         n = int(i64()[0])
         p = {k: f64(n) for k in ("q1", "vx", "vy", "vz", "w")}
         p["id"] = i64(n).copy()
+        if with_psd:
+            p["real_f"], p["marker"] = f64(n), f64(n)
+        else:
+            p["real_f"], p["marker"] = p["w"].copy(), np.ones(n)
         st["particles"].append(p)
     st["B"] = f64(3 * M).reshape(M, 3)
     st["E"] = f64(3 * M).reshape(M, 3)

@@ -33,8 +33,9 @@ def state_errors(g, c, cfg, interior_only=False):
         for key in ("n", "nV", "nvv"):
             errs[f"moments[{s}].{key}"] = rel_err(g["moments"][s][key][sl], c["moments"][s][key][sl])
         pg, pc = by_pid(g["particles"][s]), by_pid(c["particles"][s])
-        for key in ("q1", "vx", "vy", "vz", "w"):
-            errs[f"particles[{s}].{key}"] = rel_err(pg[key], pc[key])
+        for key in ("q1", "vx", "vy", "vz", "w", "real_f", "marker"):
+            if key in pg and key in pc:  # real_f / marker: species whose weights evolve
+                errs[f"particles[{s}].{key}"] = rel_err(pg[key], pc[key])
     for i in range(len(cfg.cold)):
         for key in ("n", "nV", "nvv", "nV_full"):
             errs[f"cold[{i}].{key}"] = rel_err(g["cold"][i][key][sl], c["cold"][i][key][sl])

@@ -1,0 +1,119 @@
+"""Evolving particle weights on the GPU (FP64): delta-f weights and phase-space density refresh
+(PartSpecies::impl_update_weight, Core/PartSpecies.cc:178-208) with the delta-f equilibrium
+moments (PartSpecies.cc:115-143), against the oracle and the reference's own fixtures.
+
+p7 (CAM-CL, mirror, reflecting) holds a delta-f species with refresh beside a full-f species
+loaded with hot markers (weights f0/g0) and refreshed; p8 is the predictor-corrector variant with
+a delta-f species without refresh.  Tolerances: as test_gpu_parity.py (1e-12 after one step,
+1e-9 after ten), for the weights, real_f and marker too."""
+import os
+
+import numpy as np
+import pytest
+from parity_util import by_pid, rel_err, state_errors
+from state_io import read_state
+
+import hfemic_b200 as h
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+PSD = ["p7_psd_tsc_mirror_reflecting", "p8_pc_psd_periodic"]
+
+
+@pytest.mark.parametrize("name", PSD)
+def test_weights_against_reference_fixture(name, gpu_lib):
+    """Ten steps on the GPU against the reference's own output: fields, weights, real_f and the
+    moments with the delta-f equilibrium added."""
+    cfg = h.configs.PARITY[name]()
+    init = read_state(os.path.join(GOLDEN, f"{name}.init.bin"))
+    ref = read_state(os.path.join(GOLDEN, f"{name}.step10.bin"))
+    with h.Run(cfg, gpu_lib) as g:
+        g.upload_state(init)
+        g.advance(10)
+        st = g.state()
+    for key in ("B", "E", "charge", "current"):
+        assert rel_err(st[key], ref[key]) <= 1e-9, key
+    for s in range(len(cfg.kinetic)):
+        id0 = init["particles"][s]["id"]
+        pg = by_pid(st["particles"][s])
+        order = np.argsort(ref["particles"][s]["id"])  # reference order -> upload order (ids ascend with it)
+        assert np.array_equal(id0, np.sort(id0))
+        for key in ("q1", "w", "real_f", "marker"):
+            assert rel_err(pg[key], ref["particles"][s][key][order]) <= 1e-9, (s, key)
+        for key in ("n", "nV", "nvv"):
+            assert rel_err(st["moments"][s][key], ref["moments"][s][key]) <= 1e-9, (s, key)
+        # the weights did evolve
+        assert rel_err(pg["w"], init["particles"][s]["w"]) > 1e-6
+
+
+def test_mixed_precision_refuses_evolving_weights(gpu_lib):
+    cfg = h.configs.parity_p7().replace(precision=h.configs.PREC_MIXED)
+    with pytest.raises(ValueError):
+        h.Run(cfg, gpu_lib)
+
+
+def test_upload_psd_contract(gpu_lib):
+    cfg = h.configs.parity_p7()
+    init = read_state(os.path.join(GOLDEN, f"{cfg.name}.init.bin"))
+    with h.Run(cfg, gpu_lib) as g:
+        g.upload_state(init)
+        p = init["particles"][0]
+        with pytest.raises(ValueError):  # count differs from the uploaded particles
+            g.upload_psd(0, p["real_f"][:-1], p["marker"][:-1])
+        g.advance(1)
+        with pytest.raises(ValueError):  # the particles were sorted since their upload
+            g.upload_psd(0, p["real_f"], p["marker"])
+    with h.Run(h.configs.parity_p2(), gpu_lib) as g:
+        st = read_state(os.path.join(GOLDEN, "p2_tsc_mirror_reflecting.init.bin"))
+        g.upload_state(st)
+        with pytest.raises(ValueError):  # the weights of this species do not evolve
+            g.upload_psd(0, st["particles"][0]["w"], np.ones(st["particles"][0]["w"].size))
+
+
+def test_resume_with_evolving_weights(gpu_lib):
+    cfg = h.configs.parity_p7()
+    init = read_state(os.path.join(GOLDEN, f"{cfg.name}.init.bin"))
+    with h.Run(cfg, gpu_lib) as a:
+        a.upload_state(init)
+        a.advance(4)
+        image = h.abi.checkpoint(a)
+        a.advance(4)
+        sa = a.state()
+    with h.Run(cfg, gpu_lib) as b:
+        h.abi.restore(b, image)
+        b.advance(4)
+        sb = b.state()
+    errs = state_errors(sb, sa, cfg)
+    assert "particles[0].real_f" in errs
+    assert max(errs.values()) <= 1e-12, errs
+
+
+def test_vhistogram_psd_columns(gpu_lib, oracle_lib):
+    """The recorder's third column is real_f / marker per particle."""
+    cfg = h.configs.parity_p7()
+    init = read_state(os.path.join(GOLDEN, f"{cfg.name}.init.bin"))
+    specs = dict(extent=(cfg.q1min + cfg.Nx / 8, cfg.Nx * 0.75), v1=(-6.0, 12.0, 24), v2=(0.0, 8.0, 16))
+    with h.Run(cfg, gpu_lib) as g, h.Run(cfg, oracle_lib, "orc_") as o:
+        g.upload_state(init)
+        o.upload_state(init)
+        g.advance(3)
+        o.advance(3)
+        for s in range(len(cfg.kinetic)):
+            hg, tg = h.abi.vhistogram(g, s, **specs)
+            ho, to = h.abi.vhistogram(o, s, prefix="orc_", **specs)
+            assert tg == to and to > 0
+            assert np.abs(hg[..., 0] - ho[..., 0]).sum() * to <= 2
+            same = hg[..., 0] == ho[..., 0]  # bins holding the same particles on both sides
+            assert same.mean() > 0.95
+            np.testing.assert_allclose(hg[..., 2][same], ho[..., 2][same], rtol=1e-9, atol=1e-14)
+            if s == 1:  # full-f with hot markers: real_f / marker is the weight, not 1
+                np.testing.assert_allclose(hg[..., 2][same], hg[..., 1][same], rtol=1e-9, atol=1e-14)
+
+
+def test_batches_and_device_loader_refuse_evolving_weights(gpu_lib):
+    cfg = h.configs.parity_p7()
+    with h.Run(cfg, gpu_lib) as r:
+        with pytest.raises(h.H1DError):
+            h.abi.Batch([r])
+        with pytest.raises(ValueError):
+            h.abi.populate(r, 0, seed=1, count=1000)

@@ -33,6 +33,9 @@ def compare_states(mine, ref, cfg, exact=True, rtol=0.0):
         p, q = mine["particles"][s], ref["particles"][s]
         for key in ("q1", "vx", "vy", "vz", "w"):
             cmp(f"particles[{s}].{key}", p[key], q[key])
+        if cfg.kinetic[s].has_psd:  # phase-space densities of evolving weights
+            for key in ("real_f", "marker"):
+                cmp(f"particles[{s}].{key}", p[key], q[key])
         m, r = mine["moments"][s], ref["moments"][s]
         for key in ("n", "nV", "nvv"):
             cmp(f"moments[{s}].{key}", m[key], r[key])
