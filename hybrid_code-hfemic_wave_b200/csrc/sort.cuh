@@ -294,7 +294,7 @@ struct MoveFP64T {
 using MoveFP64 = MoveFP64T<false>;
 // ... or the mixed-precision records (offset, vx, vy, vz, w as FP32; cell, pid)
 struct MoveMixed {
-    static constexpr int HOLD = SORT_ITEMS;
+    static constexpr int HOLD = SORT_ITEMS / 2;
     float const         *src[5];
     int32_t const *cell_src, *pid_src;
     float         *dst[5];
