@@ -474,6 +474,13 @@ def serving_measure(h, precision, n_requests=48, rate=4.0, budget_gb=150, seed=2
     sv = h.abi.Server(lib, int(budget_gb * (1 << 30)), steps_per_tick=64, sort_interval=16)
     ids = []
     try:
+        # warm-up outside the measurement: two short requests load the kernels a served run uses
+        warm = [sv.submit(h.configs.ensemble_member(seed, precision=precision), seed=seed, n_steps=64)
+                for seed in (7, 11)]
+        while any(sv.poll(i)["state"] < h.abi.REQ_DONE for i in warm):
+            sv.tick()
+        for i in warm:
+            sv.release(i)
         t0 = time.perf_counter()
         nxt = 0
         done = set()

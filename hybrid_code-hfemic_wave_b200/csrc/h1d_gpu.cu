@@ -1877,7 +1877,7 @@ int h1d_batch_autotune(h1d_batch *b, uint32_t *steps_taken, int *sort_interval, 
     // 1. sort interval, at the default CTA count: two whole blocks per candidate
     int   best_k  = b->k;
     float best_ms = 0;
-    for (int k : { 8, 16, 32 }) {
+    for (int k : { 8, 12, 16, 24, 32 }) {
         b->k           = k;
         b->since_block = 1 << 30;
         float ms       = 0;

@@ -307,7 +307,7 @@ int h1d_step_count(h1d_run *run, int64_t *step);
  * counterpart in the reference, which never sorts. */
 int h1d_configure(h1d_run *run, int sort_interval, int push_ctas_per_sm);
 /* Autotuner (no counterpart in the reference): advances the run by real CAM-CL steps while timing
- * two sort blocks for each candidate sort interval (8, 16, 32) and then for each CTA count of the
+ * two sort blocks for each candidate sort interval (8, 12, 16, 24, 32) and then for each CTA count of the
  * particle pass, and keeps the fastest.  *steps_taken receives the number of steps it advanced. */
 int h1d_autotune(h1d_run *run, uint32_t *steps_taken, int *sort_interval, int *push_ctas_per_sm);
 
