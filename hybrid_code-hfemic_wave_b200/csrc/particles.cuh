@@ -187,10 +187,10 @@ constexpr int PIPE_CONSUMER_WARPS = 4;
 constexpr int PIPE_THREADS        = 32 * (PIPE_CONSUMER_WARPS + 1);
 constexpr int PIPE_CHUNK          = 256;
 constexpr int PIPE_PPT            = PIPE_CHUNK / (32 * PIPE_CONSUMER_WARPS);
-constexpr int PIPE_STAGES         = 4;
-constexpr int PIPE_CTAS_PER_SM    = 2;
-constexpr int PIPE_W              = 8; // cells per deposit window: 4 quantities x 8 cells = the 32 lanes of a flush
-static_assert(4 * PIPE_W == 32, "a window flush reduce-scatters exactly 32 values");
+constexpr int PIPE_STAGES         = 2;
+constexpr int PIPE_CTAS_PER_SM    = 3;
+constexpr int PIPE_W              = 6; // cells per deposit window: 4 quantities x 6 cells, flushed over 32 lanes
+static_assert(4 * PIPE_W <= 32, "a window flush reduce-scatters at most 32 values");
 
 // a stage holds one chunk; the consumers overwrite it in place with the new state, which the
 // producer then stores.  With evolving weights (PSD) a stage also holds real_f and marker, and
@@ -204,7 +204,7 @@ struct PipeStageT {
 using PipeStage = PipeStageT<false>;
 template <bool PSD>
 struct PipeLayout {
-    static constexpr int    STAGES     = PSD ? PIPE_STAGES - 1 : PIPE_STAGES;
+    static constexpr int    STAGES     = PIPE_STAGES;
     static constexpr size_t BAR_OFFSET = sizeof(PipeStageT<PSD>) * STAGES;
     static constexpr size_t COL_OFFSET = BAR_OFFSET + 128;
 };
@@ -279,6 +279,9 @@ struct ColWindow64 {
             x[4 * c] = u.x, x[4 * c + 1] = u.y, x[4 * c + 2] = v.x, x[4 * c + 3] = v.y;
             at(d, c, 0, lane) = make_double2(0, 0), at(d, c, 1, lane) = make_double2(0, 0);
         }
+#pragma unroll
+        for (int k = 4 * PIPE_W; k < 32; ++k)
+            x[k] = 0.0;
         double const t = reduce_scatter<32>(x, lane); // lane l: value l = 4 * cell + quantity
         if (t != 0.0) {
             int const cell = base + (lane >> 2);

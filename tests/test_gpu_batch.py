@@ -106,8 +106,8 @@ def test_autotuned_run_matches_oracle(gpu_lib, oracle_lib):
     with h.Run(cfg, gpu_lib) as g:
         g.upload_state(init)
         steps, k, c = h.abi.autotune(g)
-        assert k in (8, 12, 16, 24, 32) and 1 <= c <= 2
-        assert steps == 2 * (8 + 12 + 16 + 24 + 32) + 2 * 2 * k
+        assert k in (8, 12, 16, 24, 32) and 1 <= c <= 3  # FP64 pass: up to 3 CTAs per SM
+        assert steps == 2 * (8 + 12 + 16 + 24 + 32) + 3 * 2 * k
         g.advance(3)
         gs = g.state()
     with h.Run(cfg, oracle_lib, "orc_") as o:
