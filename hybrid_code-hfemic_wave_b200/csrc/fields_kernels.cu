@@ -52,7 +52,8 @@ cudaError_t launch_prep_fields(double *B, double *E, double *EB, float *EBf, int
 cudaError_t launch_finalize_kinetic(double const *raw, double const *eq, double *out, int Nx, double s1,
                                     int reflecting, cudaStream_t st)
 {
-    finalize_kinetic_kernel<<<1, 256, 0, st>>>(raw, eq, out, Nx, s1, reflecting);
+    finalize_kinetic_kernel<<<(Nx + 2 * PAD + 127) / 128, 128, 0, st>>>(raw, eq, out, Nx, s1);
+    fold_moments_kernel<<<1, 32, 0, st>>>(out, Nx, reflecting);
     return cudaGetLastError();
 }
 cudaError_t launch_finalize_cold(double const *n_full, double const *nV_full, double *out, int Nx, double w,

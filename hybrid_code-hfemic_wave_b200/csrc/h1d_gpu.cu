@@ -28,6 +28,7 @@ using namespace h1d;
 namespace {
 
 constexpr int FIELD_BLOCK_MIN = 256;
+constexpr int64_t STAGE_N      = int64_t{ 1 } << 22; // doubles in a mixed run's staging buffer (32 MB)
 
 struct SpeciesState {
     int64_t  n = 0, cap = 0;
@@ -73,6 +74,8 @@ struct h1d_run {
     double      *geo = nullptr;
     double      *B[2] = {}, *E[2] = {}, *EB = nullptr, *charge = nullptr, *current = nullptr;
     float       *EBf = nullptr; // FP32 push record of the mixed-precision particle pass
+    double      *stage = nullptr; // mixed precision: FP64 staging of particle uploads and downloads
+    int64_t      stage_n = 0;     // its length in doubles
     double      *src_dep = nullptr; // per external source: moment<0> (zero), moment<1> x, y, z (M each)
     bool         mixed = false;
     double      *E1[2] = {}; // predictor-corrector: averaged E of phases 1 and 2
@@ -317,9 +320,7 @@ double *dep_ptr(h1d_run *run, int s, int set, int d, int q)
 
 int ppt_for(h1d_run const *run, int s)
 {
-    double const ppc = static_cast<double>(run->sp[s].n) / static_cast<double>(run->Nx);
-    int          k   = static_cast<int>(ppc / 128);
-    return k < 1 ? 1 : k > 16 ? 16 : k;
+    return mom_ppt(static_cast<double>(run->sp[s].n) / static_cast<double>(run->Nx));
 }
 
 PushArgs push_args(h1d_run *run, int s)
@@ -712,25 +713,29 @@ int finalize_moments(h1d_run *run)
     h1d_params const &p = run->p;
     for (int s = 0; s < p.n_kinetic; ++s) {
         SpeciesState &S = run->sp[s];
+        // particles that drifted since their last sort are sorted first: a warp's particles then
+        // share a few cells and collect_all accumulates in registers (the next steps gain too)
+        if (S.n > 0 && S.since_sort > 0)
+            TRY(sort_species(run, s));
         CU(cudaMemsetAsync(S.mom_raw, 0, sizeof(double) * 10 * run->M, run->stream));
         if (S.n > 0 && run->mixed) {
             MomentArgsMixed a{};
             a.cell = S.cell[S.cur], a.off = S.fbuf[S.cur][0], a.vx = S.fbuf[S.cur][1], a.vy = S.fbuf[S.cur][2];
-            a.vz = S.fbuf[S.cur][3], a.w = S.fbuf[S.cur][4], a.n = S.n, a.ppt = ppt_for(run, s);
+            a.vz = S.fbuf[S.cur][3], a.w = S.fbuf[S.cur][4], a.n = S.n, a.ppt = ppt_for(run, s), a.vec = 1;
             a.Nx = static_cast<int>(run->Nx), a.status = run->d_status;
             for (int q = 0; q < 10; ++q)
                 a.out[q] = S.mom_raw + static_cast<size_t>(q) * run->M + PAD;
             int64_t const chunks = (S.n + 32LL * a.ppt - 1) / (32LL * a.ppt);
-            moments_kernel_mixed<<<static_cast<unsigned>((chunks + 7) / 8), 256, 0, run->stream>>>(a);
+            moments_kernel<<<static_cast<unsigned>((chunks + 3) / 4), MOM_THREADS, 0, run->stream>>>(a);
         } else if (S.n > 0) {
             MomentArgs a{};
             a.q1 = S.buf[S.cur][0], a.vx = S.buf[S.cur][1], a.vy = S.buf[S.cur][2], a.vz = S.buf[S.cur][3];
-            a.w = S.buf[S.cur][4], a.n = S.n, a.ppt = ppt_for(run, s), a.Nx = static_cast<int>(run->Nx);
+            a.w = S.buf[S.cur][4], a.n = S.n, a.ppt = ppt_for(run, s), a.Nx = static_cast<int>(run->Nx), a.vec = 1;
             a.half_min = -0.5 * p.Nx + 0.5, a.status = run->d_status;
             for (int q = 0; q < 10; ++q)
                 a.out[q] = S.mom_raw + static_cast<size_t>(q) * run->M + PAD;
             int64_t const chunks = (S.n + 32LL * a.ppt - 1) / (32LL * a.ppt);
-            moments_kernel<<<static_cast<unsigned>((chunks + 7) / 8), 256, 0, run->stream>>>(a);
+            moments_kernel<<<static_cast<unsigned>((chunks + 3) / 4), MOM_THREADS, 0, run->stream>>>(a);
         }
         CU(launch_finalize_kinetic(S.mom_raw, S.eq, S.mom, static_cast<int>(run->Nx), 1.0 / p.kinetic[s].moment_norm,
                                    p.particle_bc == H1D_BC_PERIODIC ? 0 : 1, run->stream));
@@ -1257,13 +1262,15 @@ int h1d_collect_moments_noalloc(int64_t Nx, double moment_norm, int particle_bc,
         MomentArgs a{};
         a.q1 = q1, a.vx = vx, a.vy = vy, a.vz = vz, a.w = w, a.n = n, a.Nx = static_cast<int>(Nx);
         double const ppc = static_cast<double>(n) / static_cast<double>(Nx);
-        a.ppt            = ppc < 128 ? 1 : ppc >= 16 * 128 ? 16 : static_cast<int>(ppc / 128);
+        a.ppt            = mom_ppt(ppc);
+        auto const al16  = [](void const *p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+        a.vec            = al16(q1) && al16(vx) && al16(vy) && al16(vz) && al16(w); // caller buffers
         a.half_min       = -0.5 * static_cast<double>(Nx) + 0.5;
         a.status         = status;
         for (int q = 0; q < 10; ++q)
             a.out[q] = raw + static_cast<int64_t>(q) * M + PAD;
         int64_t const chunks = (n + 32LL * a.ppt - 1) / (32LL * a.ppt);
-        moments_kernel<<<static_cast<unsigned>((chunks + 7) / 8), 256, 0, st>>>(a);
+        moments_kernel<<<static_cast<unsigned>((chunks + 3) / 4), MOM_THREADS, 0, st>>>(a);
         if (cudaGetLastError() != cudaSuccess)
             return H1D_ERR_CUDA;
     }
@@ -1328,6 +1335,9 @@ int h1d_create(h1d_params const *params, h1d_run **out)
     run->nblocks_field = static_cast<int>((run->Nx + run->seg - 1) / run->seg);
     run->field_smem    = sizeof(double) * static_cast<size_t>(L) * (SMEM_SCALARS + 3 * SMEM_VECTORS);
     run->mixed = p.precision == H1D_PREC_MIXED;
+    run->stage_n = 1 << 16;
+    for (int s = 0; s < p.n_kinetic; ++s)
+        run->stage_n = std::max<int64_t>(run->stage_n, std::min<int64_t>(STAGE_N, p.Nx * std::max<int64_t>(p.kinetic[s].Nc, 0)));
     if (set_field_smem(run->field_smem) != cudaSuccess || set_push_smem_fp64() != cudaSuccess
         || set_push_smem_mixed() != cudaSuccess)
         return fail(H1D_ERR_CUDA);
@@ -1340,6 +1350,7 @@ int h1d_create(h1d_params const *params, h1d_run **out)
         || dalloc(run, &run->E1[0], 3 * M) || dalloc(run, &run->E1[1], 3 * M) || dalloc(run, &run->d_fallbacks, 1)
         || dalloc(run, &run->d_energy, 6 + 6 * (H1D_MAX_KINETIC + H1D_MAX_COLD))
         || (run->mixed && dalloc(run, &run->EBf, EBF_STRIDE * M))
+        || (run->mixed && dalloc(run, &run->stage, run->stage_n))
         || (p.n_sources > 0 && dalloc(run, &run->src_dep, 4 * M * p.n_sources)))
         return fail(H1D_ERR_OOM);
     if (cudaMallocHost(&run->h_status, sizeof(unsigned)) != cudaSuccess)
@@ -1361,6 +1372,11 @@ int h1d_create(h1d_params const *params, h1d_run **out)
         if (dalloc(run, &C.n, M) || dalloc(run, &C.nV[0], 3 * M) || dalloc(run, &C.nV[1], 3 * M) || dalloc(run, &C.mom, 10 * M))
             return fail(H1D_ERR_OOM);
     }
+    // the particle buffers of the declared load (Nx x Nc per species), so that the first upload
+    // or populate allocates nothing
+    for (int s = 0; s < p.n_kinetic; ++s)
+        if (p.kinetic[s].Nc > 0 && p.kinetic[s].Nc <= (int64_t{ 1 } << 31) / p.Nx && ensure_capacity(run, s, p.Nx * p.kinetic[s].Nc) != H1D_OK)
+            return fail(H1D_ERR_OOM);
     std::vector<double> const g = geometry_table(p);
     if (cudaMemcpyAsync(run->geo, g.data(), sizeof(double) * g.size(), cudaMemcpyHostToDevice, run->stream) != cudaSuccess
         || cudaStreamSynchronize(run->stream) != cudaSuccess)
@@ -1380,6 +1396,7 @@ int h1d_destroy(h1d_run *run)
         cudaFree(run->B[k]), cudaFree(run->E[k]), cudaFree(run->E1[k]);
     cudaFree(run->d_fallbacks);
     cudaFree(run->EB), cudaFree(run->EBf), cudaFree(run->src_dep), cudaFree(run->charge), cudaFree(run->current), cudaFree(run->d_status), cudaFree(run->d_energy);
+    cudaFree(run->stage);
     if (run->h_status)
         cudaFreeHost(run->h_status);
     for (auto &S : run->sp) {
@@ -1419,24 +1436,19 @@ int h1d_upload_particles(h1d_run *run, int s, int64_t n, double const *q1, doubl
     S.cur              = 0;
     S.n                = n;
     double const *src[5] = { q1, vx, vy, vz, w };
-    if (run->mixed && n) { // stage each FP64 component on the device and convert it
-        double *tmp = nullptr;
-        CU(cudaMalloc(&tmp, sizeof(double) * n));
-        unsigned const nb = static_cast<unsigned>((n + 255) / 256);
-        int            st = H1D_OK;
-        for (int k = 0; k < 5 && st == H1D_OK; ++k) {
-            if (cudaMemcpyAsync(tmp, src[k], sizeof(double) * n, cudaMemcpyHostToDevice, run->stream) != cudaSuccess)
-                st = set_err(run, H1D_ERR_CUDA, "h1d_upload_particles: copy failed");
-            else if (k == 0)
-                q1_to_mixed_kernel<<<nb, 256, 0, run->stream>>>(tmp, n, -0.5 * run->Nx, S.cell[0], S.fbuf[0][0]);
-            else
-                to_f32_kernel<<<nb, 256, 0, run->stream>>>(tmp, n, S.fbuf[0][k]);
-            if (st == H1D_OK && cudaGetLastError() != cudaSuccess)
-                st = set_err(run, H1D_ERR_CUDA, "h1d_upload_particles: conversion failed");
-        }
-        cudaStreamSynchronize(run->stream);
-        cudaFree(tmp);
-        TRY(st);
+    if (run->mixed && n) { // each FP64 component through the staging buffer, converted chunk by chunk
+        for (int k = 0; k < 5; ++k)
+            for (int64_t o = 0; o < n; o += run->stage_n) {
+                int64_t const  c  = std::min<int64_t>(run->stage_n, n - o);
+                unsigned const nb = static_cast<unsigned>((c + 255) / 256);
+                CU(cudaMemcpyAsync(run->stage, src[k] + o, sizeof(double) * c, cudaMemcpyHostToDevice, run->stream));
+                if (k == 0)
+                    q1_to_mixed_kernel<<<nb, 256, 0, run->stream>>>(run->stage, c, -0.5 * run->Nx, S.cell[0] + o,
+                                                                    S.fbuf[0][0] + o);
+                else
+                    to_f32_kernel<<<nb, 256, 0, run->stream>>>(run->stage, c, S.fbuf[0][k] + o);
+                CU(cudaGetLastError());
+            }
     }
     for (int k = 0; k < 5 && !run->mixed; ++k)
         if (n)
@@ -1655,23 +1667,19 @@ int h1d_download_particles(h1d_run *run, int s, double *q1, double *vx, double *
     if (run->p.particle_bc == H1D_BC_ABSORBING && S.n > 0 && S.since_sort > 0)
         TRY(sort_species(run, s)); // drop absorbed particles
     double *dst[5] = { q1, vx, vy, vz, w };
-    if (run->mixed && S.n) { // convert each component to FP64 in a device staging buffer
-        double *tmp = nullptr;
-        CU(cudaMalloc(&tmp, sizeof(double) * S.n));
-        unsigned const nb = static_cast<unsigned>((S.n + 255) / 256);
-        int            st = H1D_OK;
-        for (int k = 0; k < 5 && st == H1D_OK; ++k) {
+    if (run->mixed && S.n) { // each component converted to FP64 chunk by chunk in the staging buffer
+        for (int k = 0; k < 5; ++k) {
             if (!dst[k])
                 continue;
-            from_mixed_kernel<<<nb, 256, 0, run->stream>>>(k == 0 ? S.cell[S.cur] : nullptr, S.fbuf[S.cur][k], S.n,
-                                                           -0.5 * run->Nx, tmp);
-            if (cudaGetLastError() != cudaSuccess
-                || cudaMemcpyAsync(dst[k], tmp, sizeof(double) * S.n, cudaMemcpyDeviceToHost, run->stream) != cudaSuccess
-                || cudaStreamSynchronize(run->stream) != cudaSuccess)
-                st = set_err(run, H1D_ERR_CUDA, "h1d_download_particles: conversion failed");
+            for (int64_t o = 0; o < S.n; o += run->stage_n) {
+                int64_t const  c  = std::min<int64_t>(run->stage_n, S.n - o);
+                unsigned const nb = static_cast<unsigned>((c + 255) / 256);
+                from_mixed_kernel<<<nb, 256, 0, run->stream>>>(k == 0 ? S.cell[S.cur] + o : nullptr, S.fbuf[S.cur][k] + o,
+                                                               c, -0.5 * run->Nx, run->stage);
+                CU(cudaGetLastError());
+                CU(cudaMemcpyAsync(dst[k] + o, run->stage, sizeof(double) * c, cudaMemcpyDeviceToHost, run->stream));
+            }
         }
-        cudaFree(tmp);
-        TRY(st);
     }
     for (int k = 0; k < 5 && !run->mixed; ++k)
         if (dst[k] && S.n)
@@ -2071,6 +2079,12 @@ size_t request_bytes(h1d_request const &rq)
     }
     size_t const M = static_cast<size_t>(p.Nx + 2 * PAD);
     b += sizeof(double) * M * (G_COUNT + 6 * 3 + 6 + 1 + 3 + 6 + H1D_MAX_KINETIC * 36 + H1D_MAX_COLD * 17);
+    if (p.precision == H1D_PREC_MIXED) { // the FP64 staging buffer of uploads and downloads
+        int64_t stage = 1 << 16;
+        for (int s = 0; s < p.n_kinetic; ++s)
+            stage = std::max<int64_t>(stage, std::min<int64_t>(STAGE_N, p.Nx * std::max<int64_t>(p.kinetic[s].Nc, 0)));
+        b += sizeof(double) * static_cast<size_t>(stage);
+    }
     return b + (size_t{ 1 } << 20);
 }
 

@@ -8,147 +8,111 @@
 
 namespace h1d {
 
-// PartSpecies::impl_collect_all (PartSpecies.cc:330-349): n, nV and nvv with CIC, unscaled
+// PartSpecies::impl_collect_all (PartSpecies.cc:330-349): n, nV and nvv with CIC, unscaled.
+// A warp takes 32 x ppt consecutive (cell-sorted) particles, one round of 32 at a time with the
+// next round's loads in flight, and accumulates the ten quantities in registers over a window of
+// MOM_S cells.  When a round has a stencil outside the window, the warp adds the window to the
+// moments (one warp sum per cell and quantity, one FP64 atomic) and re-centres it on that round;
+// stencils still outside (a round spanning more than the window) go to atomics.
+constexpr int MOM_S = 4;
+
 struct MomentArgs {
     double const  *q1, *vx, *vy, *vz, *w;
     int64_t        n;
     int            ppt, Nx;
+    int            vec; // every array 16-byte aligned: vector loads
     double         half_min;
     double        *out[10]; // n, nVx, nVy, nVz, xx, yy, zz, xy, yz, zx at cell 0
     unsigned      *status;
 };
-
-__global__ void __launch_bounds__(256) moments_kernel(MomentArgs a)
-{
-    constexpr int S = 4; // CIC + window of 2
-    int const     lane   = threadIdx.x & 31;
-    int64_t const warp   = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    int64_t const chunk0 = warp * 32 * a.ppt;
-    if (chunk0 >= a.n)
-        return;
-    int first = 0x7fffffff;
-    if (chunk0 + lane < a.n)
-        first = make_shape<1>(a.q1[chunk0 + lane] - a.half_min).i0;
-    int const base = __reduce_min_sync(0xffffffffu, first) - 1;
-    double    acc[10][S];
-#pragma unroll
-    for (int q = 0; q < 10; ++q)
-#pragma unroll
-        for (int s = 0; s < S; ++s)
-            acc[q][s] = 0;
-    unsigned bad = 0;
-    for (int k = 0; k < a.ppt; ++k) {
-        int64_t const idx = chunk0 + static_cast<int64_t>(k) * 32 + lane;
-        if (idx >= a.n)
-            break;
-        double const   q1 = a.q1[idx], vx = a.vx[idx], vy = a.vy[idx], vz = a.vz[idx], w = a.w[idx];
-        Shape<1> const sh = make_shape<1>(q1 - a.half_min);
-        if (!finite_pos(q1) || !stencil_ok(sh, a.Nx)) {
-            bad |= ST_OUT_OF_RANGE;
-            continue;
-        }
-        double const val[10] = { w,           vx * w,      vy * w,      vz * w,      (vx * vx) * w,
-                                 (vy * vy) * w, (vz * vz) * w, (vx * vy) * w, (vy * vz) * w, (vz * vx) * w };
-        int const    r       = sh.i0 - base;
-        if (r >= 0 && r <= S - 2) {
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                double const ws = (s == r) ? sh.w[0] : (s == r + 1) ? sh.w[1] : 0.0;
-#pragma unroll
-                for (int q = 0; q < 10; ++q)
-                    acc[q][s] = fma(val[q], ws, acc[q][s]);
-            }
-        } else {
-#pragma unroll
-            for (int j = 0; j <= 1; ++j)
-#pragma unroll
-                for (int q = 0; q < 10; ++q)
-                    atomicAdd(a.out[q] + sh.i0 + j, val[q] * sh.w[j]);
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < 10; ++q)
-#pragma unroll
-        for (int s = 0; s < S; ++s) {
-            double const v = warp_sum(acc[q][s]);
-            if (lane == (q * S + s) % 32 && v != 0.0) {
-                int const cell = base + s;
-                if (cell >= -PAD && cell < a.Nx + PAD)
-                    atomicAdd(a.out[q] + cell, v);
-                else
-                    bad |= ST_OUT_OF_RANGE;
-            }
-        }
-    bad = __reduce_or_sync(0xffffffffu, bad);
-    if (bad && lane == 0)
-        atomicOr(a.status, bad);
-}
-
-// collect_all (n, nV, nvv with CIC, PartSpecies.cc:330-349) from mixed-precision particles: the
-// same per-warp window scheme as moments_kernel (particles.cuh), accumulated in FP64
 struct MomentArgsMixed {
     int32_t const *cell;
     float const   *off, *vx, *vy, *vz, *w;
     int64_t        n;
     int            ppt, Nx;
+    int            vec; // every array 16-byte aligned: vector loads
     double        *out[10];
     unsigned      *status;
 };
-__global__ void __launch_bounds__(256) moments_kernel_mixed(MomentArgsMixed a)
+
+// one particle as the collect_all loop needs it: CIC stencil, weight and velocity in FP64
+struct MomParticle {
+    int    i0;
+    double s0, s1, w, vx, vy, vz;
+    bool   ok;
+};
+// NP consecutive particles of a lane, loaded with 16-byte vector loads (NP = 4 FP32 / 2 FP64)
+template <class Args> struct MomTile;
+template <> struct MomTile<MomentArgs> {
+    static constexpr int NP = 2;
+    double2              q1, vx, vy, vz, w;
+};
+template <> struct MomTile<MomentArgsMixed> {
+    static constexpr int NP = 4;
+    int4                 cell;
+    float4               off, vx, vy, vz, w;
+};
+__device__ __forceinline__ double el2(double2 const &v, int j) { return j ? v.y : v.x; }
+__device__ __forceinline__ float  el4(float4 const &v, int j) { return j == 0 ? v.x : j == 1 ? v.y : j == 2 ? v.z : v.w; }
+__device__ __forceinline__ int    el4(int4 const &v, int j) { return j == 0 ? v.x : j == 1 ? v.y : j == 2 ? v.z : v.w; }
+
+// the tile at particle i (a multiple of NP); past the end it repeats the last particle (never used)
+__device__ __forceinline__ MomTile<MomentArgs> mom_load(MomentArgs const &a, int64_t i)
 {
-    constexpr int S = 4;
-    int const     lane   = threadIdx.x & 31;
-    int64_t const warp   = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-    int64_t const chunk0 = warp * 32 * a.ppt;
-    if (chunk0 >= a.n)
-        return;
-    int first = 0x7fffffff;
-    if (chunk0 + lane < a.n)
-        first = make_shape_f<1>(a.cell[chunk0 + lane], a.off[chunk0 + lane]).i0;
-    int const base = __reduce_min_sync(0xffffffffu, first) - 1;
-    double    acc[10][S];
-#pragma unroll
-    for (int q = 0; q < 10; ++q)
-#pragma unroll
-        for (int s = 0; s < S; ++s)
-            acc[q][s] = 0;
-    unsigned bad = 0;
-    for (int k = 0; k < a.ppt; ++k) {
-        int64_t const idx = chunk0 + static_cast<int64_t>(k) * 32 + lane;
-        if (idx >= a.n)
-            break;
-        ShapeF<1> const sh = make_shape_f<1>(a.cell[idx], a.off[idx]);
-        if (!stencil_ok_f(sh, a.Nx)) {
-            bad |= ST_OUT_OF_RANGE;
-            continue;
-        }
-        double const w = a.w[idx], vx = a.vx[idx], vy = a.vy[idx], vz = a.vz[idx];
-        double const val[10] = { w,           vx * w,      vy * w,      vz * w,      (vx * vx) * w,
-                                 (vy * vy) * w, (vz * vz) * w, (vx * vy) * w, (vy * vz) * w, (vz * vx) * w };
-        double const w0 = sh.w[0], w1 = sh.w[1];
-        int const    r  = sh.i0 - base;
-        if (r >= 0 && r <= S - 2) {
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                double const ws = (s == r) ? w0 : (s == r + 1) ? w1 : 0.0;
-#pragma unroll
-                for (int q = 0; q < 10; ++q)
-                    acc[q][s] = fma(val[q], ws, acc[q][s]);
-            }
-        } else {
-#pragma unroll
-            for (int q = 0; q < 10; ++q) {
-                atomicAdd(a.out[q] + sh.i0, val[q] * w0);
-                atomicAdd(a.out[q] + sh.i0 + 1, val[q] * w1);
-            }
-        }
+    MomTile<MomentArgs> t;
+    if (a.vec && i + 1 < a.n) {
+        t.q1 = *reinterpret_cast<double2 const *>(a.q1 + i), t.vx = *reinterpret_cast<double2 const *>(a.vx + i);
+        t.vy = *reinterpret_cast<double2 const *>(a.vy + i), t.vz = *reinterpret_cast<double2 const *>(a.vz + i);
+        t.w  = *reinterpret_cast<double2 const *>(a.w + i);
+    } else {
+        int64_t const j0 = min(i, a.n - 1), j1 = min(i + 1, a.n - 1);
+        t.q1 = make_double2(a.q1[j0], a.q1[j1]), t.vx = make_double2(a.vx[j0], a.vx[j1]);
+        t.vy = make_double2(a.vy[j0], a.vy[j1]), t.vz = make_double2(a.vz[j0], a.vz[j1]);
+        t.w  = make_double2(a.w[j0], a.w[j1]);
     }
+    return t;
+}
+__device__ __forceinline__ MomTile<MomentArgsMixed> mom_load(MomentArgsMixed const &a, int64_t i)
+{
+    MomTile<MomentArgsMixed> t;
+    if (a.vec && i + 3 < a.n) {
+        t.cell = *reinterpret_cast<int4 const *>(a.cell + i), t.off = *reinterpret_cast<float4 const *>(a.off + i);
+        t.vx   = *reinterpret_cast<float4 const *>(a.vx + i), t.vy = *reinterpret_cast<float4 const *>(a.vy + i);
+        t.vz   = *reinterpret_cast<float4 const *>(a.vz + i), t.w = *reinterpret_cast<float4 const *>(a.w + i);
+    } else {
+        int64_t const j[4] = { min(i, a.n - 1), min(i + 1, a.n - 1), min(i + 2, a.n - 1), min(i + 3, a.n - 1) };
+        t.cell = make_int4(a.cell[j[0]], a.cell[j[1]], a.cell[j[2]], a.cell[j[3]]);
+        t.off  = make_float4(a.off[j[0]], a.off[j[1]], a.off[j[2]], a.off[j[3]]);
+        t.vx   = make_float4(a.vx[j[0]], a.vx[j[1]], a.vx[j[2]], a.vx[j[3]]);
+        t.vy   = make_float4(a.vy[j[0]], a.vy[j[1]], a.vy[j[2]], a.vy[j[3]]);
+        t.vz   = make_float4(a.vz[j[0]], a.vz[j[1]], a.vz[j[2]], a.vz[j[3]]);
+        t.w    = make_float4(a.w[j[0]], a.w[j[1]], a.w[j[2]], a.w[j[3]]);
+    }
+    return t;
+}
+__device__ __forceinline__ MomParticle mom_particle(MomentArgs const &a, MomTile<MomentArgs> const &t, int j)
+{
+    double const   q1 = el2(t.q1, j);
+    Shape<1> const sh = make_shape<1>(q1 - a.half_min);
+    return { sh.i0, sh.w[0], sh.w[1], el2(t.w, j), el2(t.vx, j), el2(t.vy, j), el2(t.vz, j),
+             finite_pos(q1) && stencil_ok(sh, a.Nx) };
+}
+__device__ __forceinline__ MomParticle mom_particle(MomentArgsMixed const &a, MomTile<MomentArgsMixed> const &t, int j)
+{
+    ShapeF<1> const sh = make_shape_f<1>(el4(t.cell, j), el4(t.off, j));
+    return { sh.i0, sh.w[0], sh.w[1], el4(t.w, j), el4(t.vx, j), el4(t.vy, j), el4(t.vz, j), stencil_ok_f(sh, a.Nx) };
+}
+
+template <class Args>
+__device__ __forceinline__ void mom_flush(Args const &a, double (&acc)[10][MOM_S], int base, int lane, unsigned &bad)
+{
 #pragma unroll
     for (int q = 0; q < 10; ++q)
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
+        for (int s = 0; s < MOM_S; ++s) {
             double const v = warp_sum(acc[q][s]);
-            if (lane == (q * S + s) % 32 && v != 0.0) {
+            acc[q][s]      = 0;
+            if (lane == (q * MOM_S + s) % 32 && v != 0.0) {
                 int const cell = base + s;
                 if (cell >= -PAD && cell < a.Nx + PAD)
                     atomicAdd(a.out[q] + cell, v);
@@ -156,6 +120,88 @@ __global__ void __launch_bounds__(256) moments_kernel_mixed(MomentArgsMixed a)
                     bad |= ST_OUT_OF_RANGE;
             }
         }
+}
+
+// A warp takes 32 x ppt consecutive particles in rounds of 32 x NP (lane l: NP consecutive
+// particles), with the next round's vector loads in flight while the current one is accumulated.
+constexpr int MOM_THREADS = 128;
+// particles per lane of a collect_all warp: a multiple of 4 (whole rounds of either tile) from 4
+// to 16, growing with the particles per cell
+inline int mom_ppt(double ppc)
+{
+    int const k = static_cast<int>(ppc / 128);
+    return k < 4 ? 4 : k > 16 ? 16 : k & ~3;
+}
+template <class Args>
+__global__ void __launch_bounds__(MOM_THREADS, 3) moments_kernel(Args a)
+{
+    constexpr int S      = MOM_S;
+    constexpr int NP     = MomTile<Args>::NP;
+    int const     lane   = threadIdx.x & 31;
+    int64_t const warp   = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+    int64_t const chunk0 = warp * 32 * a.ppt;
+    if (chunk0 >= a.n)
+        return;
+    double acc[10][S];
+#pragma unroll
+    for (int q = 0; q < 10; ++q)
+#pragma unroll
+        for (int s = 0; s < S; ++s)
+            acc[q][s] = 0;
+    unsigned bad  = 0;
+    int      base = 0x40000000; // no window yet: the first round places it
+    auto     cur  = mom_load(a, chunk0 + NP * lane);
+    for (int k = 0; k < a.ppt / NP && chunk0 + 32LL * NP * k < a.n; ++k) {
+        int64_t const i0  = chunk0 + 32LL * NP * k + NP * lane;
+        auto const    nxt = mom_load(a, i0 + 32 * NP); // next round in flight
+        bool out = false;
+        int  lo  = 0x3fffffff;
+#pragma unroll
+        for (int j = 0; j < NP; ++j) { // stencils first: does the round fit the window?
+            MomParticle const p     = mom_particle(a, cur, j);
+            bool const        valid = i0 + j < a.n;
+            bool const        in    = valid && p.ok;
+            if (valid && !p.ok)
+                bad |= ST_OUT_OF_RANGE;
+            int const r = p.i0 - base;
+            out         = out || (in && (r < 0 || r > S - 2));
+            if (in)
+                lo = min(lo, p.i0);
+        }
+        if (__any_sync(0xffffffffu, out)) { // move the window onto this round
+            if (base != 0x40000000)
+                mom_flush(a, acc, base, lane, bad);
+            base = __reduce_min_sync(0xffffffffu, lo) - 1;
+        }
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+            MomParticle const q = mom_particle(a, cur, j);
+            if (!(i0 + j < a.n && q.ok))
+                continue;
+            double const val[10] = { q.w,               q.vx * q.w,        q.vy * q.w,        q.vz * q.w,
+                                     (q.vx * q.vx) * q.w, (q.vy * q.vy) * q.w, (q.vz * q.vz) * q.w, (q.vx * q.vy) * q.w,
+                                     (q.vy * q.vz) * q.w, (q.vz * q.vx) * q.w };
+            int const r = q.i0 - base;
+            if (r < 0 || r > S - 2) { // this round spans more than the window
+#pragma unroll
+                for (int c = 0; c < 10; ++c) {
+                    atomicAdd(a.out[c] + q.i0, val[c] * q.s0);
+                    atomicAdd(a.out[c] + q.i0 + 1, val[c] * q.s1);
+                }
+            } else {
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    double const ws = (s == r) ? q.s0 : (s == r + 1) ? q.s1 : 0.0;
+#pragma unroll
+                    for (int c = 0; c < 10; ++c)
+                        acc[c][s] = fma(val[c], ws, acc[c][s]);
+                }
+            }
+        }
+        cur = nxt;
+    }
+    if (base != 0x40000000)
+        mom_flush(a, acc, base, lane, bad);
     bad = __reduce_or_sync(0xffffffffu, bad);
     if (bad && lane == 0)
         atomicOr(a.status, bad);

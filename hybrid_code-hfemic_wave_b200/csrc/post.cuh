@@ -55,56 +55,51 @@ __global__ void prep_fields_kernel(double *B, double *E, double *EB, float *EBf,
 // out: GridArray layout n[M], nV[3M], nvv[6M].
 // delta-f species (eq != null): + the equilibrium n0 (M) and nvv0 (6M) x m_moment_weighting_factor
 // (PartSpecies.cc:129-143), before the ghost fold as in the reference
-__global__ void finalize_kinetic_kernel(double const *raw, double const *eq, double *out, int Nx, double s1,
-                                        int reflecting)
+__global__ void finalize_kinetic_kernel(double const *raw, double const *eq, double *out, int Nx, double s1)
 {
     int const M = Nx + 2 * PAD;
-    double   *n = out, *nV = out + M, *nvv = out + 4 * M;
-    for (int i = threadIdx.x; i < M; i += blockDim.x) {
-        n[i] = raw[i] * s1;
-        for (int c = 0; c < 3; ++c)
-            nV[3 * i + c] = raw[(1 + c) * M + i] * s1;
-        for (int c = 0; c < 6; ++c)
-            nvv[6 * i + c] = raw[(4 + c) * M + i] * s1;
-        if (eq) {
-            n[i] = n[i] + eq[i] * 1.0;
-            for (int c = 0; c < 6; ++c)
-                nvv[6 * i + c] = nvv[6 * i + c] + eq[M + 6 * i + c] * 1.0;
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x != 0)
+    int const i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= M)
         return;
-    struct G {
-        double *a;
-        int     nc;
-    } const grids[3] = { { n, 1 }, { nV, 3 }, { nvv, 6 } };
-    for (G const &g : grids) {
-        double *a = g.a;
-        int const nc = g.nc;
-        if (reflecting) {
-            for (int i = 0; i < PAD; ++i) // cells -3 -> -2 -> -1 -> 0
-                for (int c = 0; c < nc; ++c) {
-                    a[nc * (i + 1) + c] += a[nc * i + c];
-                    a[nc * i + c] = 0;
-                }
-            for (int i = M - 1; i >= Nx + PAD; --i)
-                for (int c = 0; c < nc; ++c) {
-                    a[nc * (i - 1) + c] += a[nc * i + c];
-                    a[nc * i + c] = 0;
-                }
-        }
-        double left[6 * PAD], right[6 * PAD];
-        for (int k = 0; k < PAD; ++k)
-            for (int c = 0; c < nc; ++c)
-                left[nc * k + c] = a[nc * k + c], right[nc * k + c] = a[nc * (Nx + PAD + k) + c];
-        for (int k = 0; k < PAD; ++k)
-            for (int c = 0; c < nc; ++c)
-                a[nc * (Nx + k) + c] += left[nc * k + c];
-        for (int k = 0; k < PAD; ++k)
-            for (int c = 0; c < nc; ++c)
-                a[nc * (PAD + k) + c] += right[nc * k + c];
+    double *n = out, *nV = out + M, *nvv = out + 4 * M;
+    n[i]      = raw[i] * s1;
+    for (int c = 0; c < 3; ++c)
+        nV[3 * i + c] = raw[(1 + c) * M + i] * s1;
+    for (int c = 0; c < 6; ++c)
+        nvv[6 * i + c] = raw[(4 + c) * M + i] * s1;
+    if (eq) {
+        n[i] = n[i] + eq[i] * 1.0;
+        for (int c = 0; c < 6; ++c)
+            nvv[6 * i + c] = nvv[6 * i + c] + eq[M + 6 * i + c] * 1.0;
     }
+}
+// the ghost fold of the finalized moments, one thread per component (n; nV xyz; nvv x 6)
+__global__ void fold_moments_kernel(double *out, int Nx, int reflecting)
+{
+    int const t = threadIdx.x;
+    if (t >= 10)
+        return;
+    int const M  = Nx + 2 * PAD;
+    int const nc = t == 0 ? 1 : t < 4 ? 3 : 6;
+    int const c  = t == 0 ? 0 : t < 4 ? t - 1 : t - 4;
+    double   *a  = t == 0 ? out : t < 4 ? out + M : out + 4 * M;
+    if (reflecting) {
+        for (int i = 0; i < PAD; ++i) { // cells -3 -> -2 -> -1 -> 0
+            a[nc * (i + 1) + c] += a[nc * i + c];
+            a[nc * i + c] = 0;
+        }
+        for (int i = M - 1; i >= Nx + PAD; --i) {
+            a[nc * (i - 1) + c] += a[nc * i + c];
+            a[nc * i + c] = 0;
+        }
+    }
+    double left[PAD], right[PAD];
+    for (int k = 0; k < PAD; ++k)
+        left[k] = a[nc * k + c], right[k] = a[nc * (Nx + PAD + k) + c];
+    for (int k = 0; k < PAD; ++k)
+        a[nc * (Nx + k) + c] += left[k];
+    for (int k = 0; k < PAD; ++k)
+        a[nc * (PAD + k) + c] += right[k];
 }
 
 // ColdSpecies::collect_all (ColdSpecies.cc:268-297): moments x weight on the interior,

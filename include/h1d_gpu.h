@@ -91,7 +91,8 @@ typedef struct h1d_kinetic_desc {
     double  Oc;          /* PlasmaDesc::Oc, signed cyclotron frequency */
     double  op;          /* PlasmaDesc::op, plasma frequency */
     int64_t n_smooth;    /* PlasmaDesc::number_of_source_smoothings */
-    int64_t Nc;          /* KineticPlasmaDesc::Nc, particles per cell (informational) */
+    int64_t Nc;          /* KineticPlasmaDesc::Nc, particles per cell: h1d_create reserves device
+                            buffers for Nx * Nc particles (more are allocated on upload if needed) */
     int64_t shape_order; /* 1 (CIC), 2 (TSC) or 3 */
     double  moment_norm; /* PartSpecies::Nc (PartSpecies.cc:150-154): Nx*Nc*Nrefcell_div_Ntotal,
                             the particle count of the reference cell used to normalise moments */
