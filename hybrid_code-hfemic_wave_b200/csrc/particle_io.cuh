@@ -8,13 +8,8 @@
 
 namespace h1d {
 
-// PartSpecies::impl_collect_all (PartSpecies.cc:330-349): n, nV and nvv with CIC, unscaled.
-// A warp takes 32 x ppt consecutive (cell-sorted) particles, one round of 32 at a time with the
-// next round's loads in flight, and accumulates the ten quantities in registers over a window of
-// MOM_S cells.  When a round has a stencil outside the window, the warp adds the window to the
-// moments (one warp sum per cell and quantity, one FP64 atomic) and re-centres it on that round;
-// stencils still outside (a round spanning more than the window) go to atomics.
-constexpr int MOM_S = 4;
+// PartSpecies::impl_collect_all (PartSpecies.cc:330-349): n, nV and nvv with CIC, unscaled, from
+// cell-sorted particles (moments_kernel below).
 
 struct MomentArgs {
     double const  *q1, *vx, *vy, *vz, *w;
@@ -103,27 +98,6 @@ __device__ __forceinline__ MomParticle mom_particle(MomentArgsMixed const &a, Mo
     return { sh.i0, sh.w[0], sh.w[1], el4(t.w, j), el4(t.vx, j), el4(t.vy, j), el4(t.vz, j), stencil_ok_f(sh, a.Nx) };
 }
 
-template <class Args>
-__device__ __forceinline__ void mom_flush(Args const &a, double (&acc)[10][MOM_S], int base, int lane, unsigned &bad)
-{
-#pragma unroll
-    for (int q = 0; q < 10; ++q)
-#pragma unroll
-        for (int s = 0; s < MOM_S; ++s) {
-            double const v = warp_sum(acc[q][s]);
-            acc[q][s]      = 0;
-            if (lane == (q * MOM_S + s) % 32 && v != 0.0) {
-                int const cell = base + s;
-                if (cell >= -PAD && cell < a.Nx + PAD)
-                    atomicAdd(a.out[q] + cell, v);
-                else
-                    bad |= ST_OUT_OF_RANGE;
-            }
-        }
-}
-
-// A warp takes 32 x ppt consecutive particles in rounds of 32 x NP (lane l: NP consecutive
-// particles), with the next round's vector loads in flight while the current one is accumulated.
 constexpr int MOM_THREADS = 128;
 // particles per lane of a collect_all warp: a multiple of 4 (whole rounds of either tile) from 4
 // to 16, growing with the particles per cell
@@ -132,76 +106,134 @@ inline int mom_ppt(double ppc)
     int const k = static_cast<int>(ppc / 128);
     return k < 4 ? 4 : k > 16 ? 16 : k & ~3;
 }
+
+// A warp's collect_all window of MOM_W cells from `base` in shared memory: lane-private FP64
+// columns, per cell five double2 {n, nVx}, {nVy, nVz}, {xx, yy}, {zz, xy}, {yz, zx}, so a
+// particle's deposit is ten 16-byte read-modify-writes whatever the mix of cells in the warp.
+constexpr int MOM_W    = 4;
+constexpr int MOM_WARP = MOM_W * 5 * 32; // double2 per warp
+struct MomWindow {
+    double2 *col;
+    int      base;
+    __device__ __forceinline__ double2 &at(int c, int pq, int lane) { return col[(c * 5 + pq) * 32 + lane]; }
+    // the column sums of every cell and quantity into the moments, then clear
+    template <class Args>
+    __device__ __forceinline__ void flush(Args const &a, int lane, unsigned &bad)
+    {
+        double x[32], y[2 * 5 * MOM_W - 32];
+#pragma unroll
+        for (int c = 0; c < MOM_W; ++c)
+#pragma unroll
+            for (int pq = 0; pq < 5; ++pq) {
+                double2 const v = at(c, pq, lane);
+                at(c, pq, lane) = make_double2(0, 0);
+                int const k     = c * 10 + 2 * pq; // value index: cell * 10 + quantity
+                if (k < 32)
+                    x[k] = v.x;
+                else
+                    y[k - 32] = v.x;
+                if (k + 1 < 32)
+                    x[k + 1] = v.y;
+                else
+                    y[k + 1 - 32] = v.y;
+            }
+        auto add = [&](int k, double t) {
+            if (t == 0.0)
+                return;
+            int const cell = base + k / 10;
+            if (cell >= -PAD && cell < a.Nx + PAD)
+                atomicAdd(a.out[k % 10] + cell, t);
+            else
+                bad |= ST_OUT_OF_RANGE;
+        };
+        double const t = reduce_scatter<32>(x, lane); // lane l: value l
+        add(lane, t);
+#pragma unroll
+        for (int k = 0; k < 2 * 5 * MOM_W - 32; ++k) {
+            double const u = warp_sum(y[k]);
+            if (lane == k)
+                add(32 + k, u);
+        }
+    }
+};
+
+// A warp takes 32 x ppt consecutive particles in rounds of 32 x NP (lane l: NP consecutive
+// particles), with the next round's vector loads in flight while the current one is deposited.
+// The window moves to a round that does not fit it (after a flush); stencils still outside
+// (a round spanning more than the window) go to atomics.
 template <class Args>
-__global__ void __launch_bounds__(MOM_THREADS, 3) moments_kernel(Args a)
+__global__ void __launch_bounds__(MOM_THREADS, 4) moments_kernel(Args a)
 {
-    constexpr int S      = MOM_S;
-    constexpr int NP     = MomTile<Args>::NP;
+    constexpr int NP   = MomTile<Args>::NP;
+    constexpr int NONE = 0x40000000;
+    __shared__ double2 cols[MOM_THREADS / 32][MOM_WARP];
     int const     lane   = threadIdx.x & 31;
     int64_t const warp   = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     int64_t const chunk0 = warp * 32 * a.ppt;
     if (chunk0 >= a.n)
         return;
-    double acc[10][S];
+    MomWindow win{ cols[threadIdx.x >> 5], NONE };
 #pragma unroll
-    for (int q = 0; q < 10; ++q)
+    for (int c = 0; c < MOM_W; ++c)
 #pragma unroll
-        for (int s = 0; s < S; ++s)
-            acc[q][s] = 0;
-    unsigned bad  = 0;
-    int      base = 0x40000000; // no window yet: the first round places it
-    auto     cur  = mom_load(a, chunk0 + NP * lane);
+        for (int pq = 0; pq < 5; ++pq)
+            win.at(c, pq, lane) = make_double2(0, 0);
+    unsigned bad = 0;
+    auto     cur = mom_load(a, chunk0 + NP * lane);
     for (int k = 0; k < a.ppt / NP && chunk0 + 32LL * NP * k < a.n; ++k) {
         int64_t const i0  = chunk0 + 32LL * NP * k + NP * lane;
         auto const    nxt = mom_load(a, i0 + 32 * NP); // next round in flight
-        bool out = false;
-        int  lo  = 0x3fffffff;
+        MomParticle   p[NP];
+        bool          out = false;
+        int           lo  = 0x3fffffff;
 #pragma unroll
-        for (int j = 0; j < NP; ++j) { // stencils first: does the round fit the window?
-            MomParticle const p     = mom_particle(a, cur, j);
-            bool const        valid = i0 + j < a.n;
-            bool const        in    = valid && p.ok;
-            if (valid && !p.ok)
+        for (int j = 0; j < NP; ++j) {
+            p[j]             = mom_particle(a, cur, j);
+            bool const valid = i0 + j < a.n;
+            if (valid && !p[j].ok)
                 bad |= ST_OUT_OF_RANGE;
-            int const r = p.i0 - base;
-            out         = out || (in && (r < 0 || r > S - 2));
-            if (in)
-                lo = min(lo, p.i0);
+            p[j].ok     = valid && p[j].ok;
+            int const r = p[j].i0 - win.base;
+            out         = out || (p[j].ok && (r < 0 || r > MOM_W - 2));
+            if (p[j].ok)
+                lo = min(lo, p[j].i0);
         }
         if (__any_sync(0xffffffffu, out)) { // move the window onto this round
-            if (base != 0x40000000)
-                mom_flush(a, acc, base, lane, bad);
-            base = __reduce_min_sync(0xffffffffu, lo) - 1;
+            if (win.base != NONE)
+                win.flush(a, lane, bad);
+            win.base = __reduce_min_sync(0xffffffffu, lo);
         }
 #pragma unroll
         for (int j = 0; j < NP; ++j) {
-            MomParticle const q = mom_particle(a, cur, j);
-            if (!(i0 + j < a.n && q.ok))
+            MomParticle const &q = p[j];
+            if (!q.ok)
                 continue;
-            double const val[10] = { q.w,               q.vx * q.w,        q.vy * q.w,        q.vz * q.w,
-                                     (q.vx * q.vx) * q.w, (q.vy * q.vy) * q.w, (q.vz * q.vz) * q.w, (q.vx * q.vy) * q.w,
-                                     (q.vy * q.vz) * q.w, (q.vz * q.vx) * q.w };
-            int const r = q.i0 - base;
-            if (r < 0 || r > S - 2) { // this round spans more than the window
+            double const v[10] = { q.w,               q.vx * q.w,        q.vy * q.w,        q.vz * q.w,
+                                   (q.vx * q.vx) * q.w, (q.vy * q.vy) * q.w, (q.vz * q.vz) * q.w, (q.vx * q.vy) * q.w,
+                                   (q.vy * q.vz) * q.w, (q.vz * q.vx) * q.w };
+            int const r = q.i0 - win.base;
+            if (r < 0 || r > MOM_W - 2) { // this round spans more than the window
 #pragma unroll
                 for (int c = 0; c < 10; ++c) {
-                    atomicAdd(a.out[c] + q.i0, val[c] * q.s0);
-                    atomicAdd(a.out[c] + q.i0 + 1, val[c] * q.s1);
+                    atomicAdd(a.out[c] + q.i0, v[c] * q.s0);
+                    atomicAdd(a.out[c] + q.i0 + 1, v[c] * q.s1);
                 }
-            } else {
+                continue;
+            }
 #pragma unroll
-                for (int s = 0; s < S; ++s) {
-                    double const ws = (s == r) ? q.s0 : (s == r + 1) ? q.s1 : 0.0;
-#pragma unroll
-                    for (int c = 0; c < 10; ++c)
-                        acc[c][s] = fma(val[c], ws, acc[c][s]);
-                }
+            for (int pq = 0; pq < 5; ++pq) {
+                double2 &e0 = win.at(r, pq, lane);
+                double2 &e1 = win.at(r + 1, pq, lane);
+                double2  t0 = e0, t1 = e1;
+                t0.x = fma(v[2 * pq], q.s0, t0.x), t0.y = fma(v[2 * pq + 1], q.s0, t0.y);
+                t1.x = fma(v[2 * pq], q.s1, t1.x), t1.y = fma(v[2 * pq + 1], q.s1, t1.y);
+                e0 = t0, e1 = t1;
             }
         }
         cur = nxt;
     }
-    if (base != 0x40000000)
-        mom_flush(a, acc, base, lane, bad);
+    if (win.base != NONE)
+        win.flush(a, lane, bad);
     bad = __reduce_or_sync(0xffffffffu, bad);
     if (bad && lane == 0)
         atomicOr(a.status, bad);
