@@ -107,133 +107,96 @@ inline int mom_ppt(double ppc)
     return k < 4 ? 4 : k > 16 ? 16 : k & ~3;
 }
 
-// A warp's collect_all window of MOM_W cells from `base` in shared memory: lane-private FP64
-// columns, per cell five double2 {n, nVx}, {nVy, nVz}, {xx, yy}, {zz, xy}, {yz, zx}, so a
-// particle's deposit is ten 16-byte read-modify-writes whatever the mix of cells in the warp.
-constexpr int MOM_W    = 4;
-constexpr int MOM_WARP = MOM_W * 5 * 32; // double2 per warp
-struct MomWindow {
-    double2 *col;
-    int      base;
-    __device__ __forceinline__ double2 &at(int c, int pq, int lane) { return col[(c * 5 + pq) * 32 + lane]; }
-    // the column sums of every cell and quantity into the moments, then clear
-    template <class Args>
-    __device__ __forceinline__ void flush(Args const &a, int lane, unsigned &bad)
-    {
-        double x[32], y[2 * 5 * MOM_W - 32];
-#pragma unroll
-        for (int c = 0; c < MOM_W; ++c)
-#pragma unroll
-            for (int pq = 0; pq < 5; ++pq) {
-                double2 const v = at(c, pq, lane);
-                at(c, pq, lane) = make_double2(0, 0);
-                int const k     = c * 10 + 2 * pq; // value index: cell * 10 + quantity
-                if (k < 32)
-                    x[k] = v.x;
-                else
-                    y[k - 32] = v.x;
-                if (k + 1 < 32)
-                    x[k + 1] = v.y;
-                else
-                    y[k + 1 - 32] = v.y;
-            }
-        auto add = [&](int k, double t) {
-            if (t == 0.0)
-                return;
-            int const cell = base + k / 10;
-            if (cell >= -PAD && cell < a.Nx + PAD)
-                atomicAdd(a.out[k % 10] + cell, t);
-            else
-                bad |= ST_OUT_OF_RANGE;
-        };
-        double const t = reduce_scatter<32>(x, lane); // lane l: value l
-        add(lane, t);
-#pragma unroll
-        for (int k = 0; k < 2 * 5 * MOM_W - 32; ++k) {
-            double const u = warp_sum(y[k]);
-            if (lane == k)
-                add(32 + k, u);
-        }
-    }
-};
+// collect_all by cells.  A lane takes ppt consecutive (cell-sorted) particles and sums, per
+// quantity, the total T of its particles in one cell c, the part L that CIC gives the left
+// neighbour c - 1 and the part R it gives the right neighbour c + 1; cell c receives T - L - R.
+// The sums go to the moments when the lane reaches another cell (rare: a lane's particles are
+// consecutive in cell order) and once at the end, one warp sum per distinct cell among the lanes.
+__device__ __forceinline__ void mom_add(double *const (&out)[10], int q, int cell, int Nx, double v, unsigned &bad)
+{
+    if (v == 0.0)
+        return;
+    if (cell >= -PAD && cell < Nx + PAD)
+        atomicAdd(out[q] + cell, v);
+    else
+        bad |= ST_OUT_OF_RANGE;
+}
 
-// A warp takes 32 x ppt consecutive particles in rounds of 32 x NP (lane l: NP consecutive
-// particles), with the next round's vector loads in flight while the current one is deposited.
-// The window moves to a round that does not fit it (after a flush); stencils still outside
-// (a round spanning more than the window) go to atomics.
 template <class Args>
-__global__ void __launch_bounds__(MOM_THREADS, 4) moments_kernel(Args a)
+__global__ void __launch_bounds__(MOM_THREADS) moments_kernel(Args a)
 {
     constexpr int NP   = MomTile<Args>::NP;
     constexpr int NONE = 0x40000000;
-    __shared__ double2 cols[MOM_THREADS / 32][MOM_WARP];
     int const     lane   = threadIdx.x & 31;
     int64_t const warp   = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
     int64_t const chunk0 = warp * 32 * a.ppt;
     if (chunk0 >= a.n)
         return;
-    MomWindow win{ cols[threadIdx.x >> 5], NONE };
+    int64_t const first = chunk0 + static_cast<int64_t>(lane) * a.ppt; // this lane's particles
+    double        T[10], L[10], R[10];
 #pragma unroll
-    for (int c = 0; c < MOM_W; ++c)
-#pragma unroll
-        for (int pq = 0; pq < 5; ++pq)
-            win.at(c, pq, lane) = make_double2(0, 0);
+    for (int q = 0; q < 10; ++q)
+        T[q] = L[q] = R[q] = 0;
+    int      rc  = NONE; // the cell T, L and R belong to
     unsigned bad = 0;
-    auto     cur = mom_load(a, chunk0 + NP * lane);
-    for (int k = 0; k < a.ppt / NP && chunk0 + 32LL * NP * k < a.n; ++k) {
-        int64_t const i0  = chunk0 + 32LL * NP * k + NP * lane;
-        auto const    nxt = mom_load(a, i0 + 32 * NP); // next round in flight
-        MomParticle   p[NP];
-        bool          out = false;
-        int           lo  = 0x3fffffff;
+    auto     cur = mom_load(a, first);
+    for (int k = 0; k < a.ppt / NP; ++k) {
+        int64_t const i0  = first + NP * k;
+        auto const    nxt = mom_load(a, i0 + NP); // next particles in flight
 #pragma unroll
         for (int j = 0; j < NP; ++j) {
-            p[j]             = mom_particle(a, cur, j);
-            bool const valid = i0 + j < a.n;
-            if (valid && !p[j].ok)
+            if (i0 + j >= a.n)
+                break;
+            MomParticle const p = mom_particle(a, cur, j);
+            if (!p.ok) {
                 bad |= ST_OUT_OF_RANGE;
-            p[j].ok     = valid && p[j].ok;
-            int const r = p[j].i0 - win.base;
-            out         = out || (p[j].ok && (r < 0 || r > MOM_W - 2));
-            if (p[j].ok)
-                lo = min(lo, p[j].i0);
-        }
-        if (__any_sync(0xffffffffu, out)) { // move the window onto this round
-            if (win.base != NONE)
-                win.flush(a, lane, bad);
-            win.base = __reduce_min_sync(0xffffffffu, lo);
-        }
-#pragma unroll
-        for (int j = 0; j < NP; ++j) {
-            MomParticle const &q = p[j];
-            if (!q.ok)
-                continue;
-            double const v[10] = { q.w,               q.vx * q.w,        q.vy * q.w,        q.vz * q.w,
-                                   (q.vx * q.vx) * q.w, (q.vy * q.vy) * q.w, (q.vz * q.vz) * q.w, (q.vx * q.vy) * q.w,
-                                   (q.vy * q.vz) * q.w, (q.vz * q.vx) * q.w };
-            int const r = q.i0 - win.base;
-            if (r < 0 || r > MOM_W - 2) { // this round spans more than the window
-#pragma unroll
-                for (int c = 0; c < 10; ++c) {
-                    atomicAdd(a.out[c] + q.i0, v[c] * q.s0);
-                    atomicAdd(a.out[c] + q.i0 + 1, v[c] * q.s1);
-                }
                 continue;
             }
+            bool const up = p.s1 >= 0.5; // the particle's cell is i0 + 1, its left neighbour gets s0
+            int const  c  = p.i0 + (up ? 1 : 0);
+            if (c != rc) {
+                if (rc != NONE) {
 #pragma unroll
-            for (int pq = 0; pq < 5; ++pq) {
-                double2 &e0 = win.at(r, pq, lane);
-                double2 &e1 = win.at(r + 1, pq, lane);
-                double2  t0 = e0, t1 = e1;
-                t0.x = fma(v[2 * pq], q.s0, t0.x), t0.y = fma(v[2 * pq + 1], q.s0, t0.y);
-                t1.x = fma(v[2 * pq], q.s1, t1.x), t1.y = fma(v[2 * pq + 1], q.s1, t1.y);
-                e0 = t0, e1 = t1;
+                    for (int q = 0; q < 10; ++q) {
+                        mom_add(a.out, q, rc, a.Nx, T[q] - L[q] - R[q], bad);
+                        mom_add(a.out, q, rc - 1, a.Nx, L[q], bad);
+                        mom_add(a.out, q, rc + 1, a.Nx, R[q], bad);
+                        T[q] = L[q] = R[q] = 0;
+                    }
+                }
+                rc = c;
+            }
+            double const left = up ? p.s0 : 0.0, right = up ? 0.0 : p.s1;
+            double const v[10] = { p.w,               p.vx * p.w,        p.vy * p.w,        p.vz * p.w,
+                                   (p.vx * p.vx) * p.w, (p.vy * p.vy) * p.w, (p.vz * p.vz) * p.w, (p.vx * p.vy) * p.w,
+                                   (p.vy * p.vz) * p.w, (p.vz * p.vx) * p.w };
+#pragma unroll
+            for (int q = 0; q < 10; ++q) {
+                T[q] += v[q];
+                L[q] = fma(v[q], left, L[q]);
+                R[q] = fma(v[q], right, R[q]);
             }
         }
         cur = nxt;
     }
-    if (win.base != NONE)
-        win.flush(a, lane, bad);
+    // one warp sum per distinct cell among the lanes; lane 3q + m adds quantity q's share m
+    for (unsigned pending = __ballot_sync(0xffffffffu, rc != NONE); pending;) {
+        int const  key  = __shfl_sync(0xffffffffu, rc, __ffs(pending) - 1);
+        bool const mine = rc == key;
+#pragma unroll
+        for (int q = 0; q < 10; ++q) {
+            double const t = warp_sum(mine ? T[q] : 0.0);
+            double const l = warp_sum(mine ? L[q] : 0.0);
+            double const r = warp_sum(mine ? R[q] : 0.0);
+            if (lane == 3 * q)
+                mom_add(a.out, q, key, a.Nx, t - l - r, bad);
+            else if (lane == 3 * q + 1)
+                mom_add(a.out, q, key - 1, a.Nx, l, bad);
+            else if (lane == 3 * q + 2)
+                mom_add(a.out, q, key + 1, a.Nx, r, bad);
+        }
+        pending &= ~__ballot_sync(0xffffffffu, mine);
+    }
     bad = __reduce_or_sync(0xffffffffu, bad);
     if (bad && lane == 0)
         atomicOr(a.status, bad);
