@@ -77,6 +77,11 @@ cudaError_t launch_fill(double *a, int64_t n, double v, cudaStream_t st)
     fill_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(a, n, v);
     return cudaGetLastError();
 }
+cudaError_t launch_fill_f(float *a, int64_t n, float v, cudaStream_t st)
+{
+    fill_f_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(a, n, v);
+    return cudaGetLastError();
+}
 cudaError_t launch_iota(int32_t *pid, int64_t n, cudaStream_t st)
 {
     iota_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, st>>>(pid, n);

@@ -37,6 +37,7 @@ struct SpeciesState {
     float   *fbuf[2][5] = {}; // mixed precision: [parity][offset in the cell, vx, vy, vz, w]
     int32_t *pid[2]    = {};
     double  *psd[2][2] = {}; // FP64 with evolving weights: [parity][real_f, marker]
+    float   *fpsd[2][2] = {}; // the same in FP32 for mixed precision
     int      cur       = 0;
     bool     upload_order = false; // the particles are still in the order of their upload
     // sort scratch
@@ -234,8 +235,6 @@ int validate(h1d_params const *p, std::string &m)
             BAD("kinetic species %d: unknown particle scheme or negative psd_refresh_frequency", s);
         if (evolves_psd(d) && (!(d.vth1 > 0) || !(d.T2_T1 > 0)))
             BAD("kinetic species %d: evolving weights need the equilibrium vth1 > 0 and T2_T1 > 0", s);
-        if (evolves_psd(d) && p->precision == H1D_PREC_MIXED)
-            BAD("kinetic species %d: delta-f and PSD refresh run in FP64 only", s);
     }
     for (int s = 0; s < p->n_cold; ++s)
         if (p->cold[s].Oc == 0 || !(p->cold[s].op > 0) || p->cold[s].n_smooth < 0 || p->cold[s].n_smooth > 64)
@@ -371,6 +370,13 @@ PushArgsMixed mixed_args(h1d_run *run, int s, PushArgs const &a)
     m.status = a.status, m.fallbacks = a.fallbacks, m.seed = a.seed, m.counter = a.counter;
     m.species = a.species, m.randomize = a.randomize;
     m.move_steps = a.move_steps, m.deposit_mask = a.deposit_mask, m.write_back = a.write_back;
+    if (S.fpsd[S.cur][0]) {
+        h1d_kinetic_desc const &d = run->p.kinetic[s];
+        m.real_f = S.fpsd[S.cur][0], m.marker = S.fpsd[S.cur][1];
+        m.nu_dt = static_cast<float>(d.psd_refresh_frequency * run->p.dt), m.psd_refresh = d.psd_refresh_frequency != 0;
+        m.delta_f = d.scheme == H1D_DELTA_F, m.vth1 = static_cast<float>(d.vth1);
+        m.vth1_cubed = static_cast<float>(d.vth1 * d.vth1 * d.vth1), m.T2_T1 = static_cast<float>(d.T2_T1);
+    }
     return m;
 }
 
@@ -380,7 +386,10 @@ int launch_push(h1d_run *run, int s, PushArgs const &a)
         return H1D_OK;
     int const  order  = run->p.kinetic[s].shape_order;
     bool const mirror = run->p.xi != 0;
-    if (run->mixed) {
+    if (run->mixed && run->sp[s].fpsd[0][0]) {
+        PushArgsMixed const m = mixed_args(run, s, a);
+        CU(launch_push_psd(m, order, mirror, run->p.particle_bc, run->num_sms * PIPE_CTAS_PER_SM_MIXED, run->stream));
+    } else if (run->mixed) {
         PushArgsMixed const m = mixed_args(run, s, a);
         CU(launch_push_groups(&m, 1, order, mirror, run->p.particle_bc,
                               run->num_sms * (run->ctas_per_sm ? run->ctas_per_sm : PIPE_CTAS_PER_SM_MIXED), run->stream));
@@ -431,15 +440,22 @@ int sort_species(h1d_run *run, int s)
     else
         first.q1 = S.buf[S.cur][0], first.w = S.buf[S.cur][4];
     MoveMixed         mm{};
+    MoveMixedT<true>  mq{};
     MoveFP64          md{};
     MoveFP64T<true>   mp{};
-    bool const        psd = S.psd[0][0] != nullptr;
+    bool const        psd = S.psd[0][0] != nullptr || S.fpsd[0][0] != nullptr;
     for (int k = 0; k < 5; ++k) {
         mm.src[k] = S.fbuf[S.cur][k], mm.dst[k] = S.fbuf[1 - S.cur][k];
         md.src[k] = mp.src[k] = S.buf[S.cur][k], md.dst[k] = mp.dst[k] = S.buf[1 - S.cur][k];
     }
-    for (int k = 0; k < 2; ++k)
+    for (int k = 0; k < 5; ++k)
+        mq.src[k] = S.fbuf[S.cur][k], mq.dst[k] = S.fbuf[1 - S.cur][k];
+    for (int k = 0; k < 2; ++k) {
         mp.src[5 + k] = S.psd[S.cur][k], mp.dst[5 + k] = S.psd[1 - S.cur][k];
+        mq.src[5 + k] = S.fpsd[S.cur][k], mq.dst[5 + k] = S.fpsd[1 - S.cur][k];
+    }
+    mq.cell_src = S.cell[S.cur], mq.cell_dst = S.cell[1 - S.cur];
+    mq.pid_src = S.pid[S.cur], mq.pid_dst = S.pid[1 - S.cur];
     mm.cell_src = S.cell[S.cur], mm.cell_dst = S.cell[1 - S.cur];
     mm.pid_src = md.pid_src = mp.pid_src = S.pid[S.cur];
     mm.pid_dst = md.pid_dst = mp.pid_dst = S.pid[1 - S.cur];
@@ -464,6 +480,8 @@ int sort_species(h1d_run *run, int s)
         uint32_t const *idx = S.idx[src];
         if (pass > 0 && !last)
             scatter_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mk);
+        else if (pass > 0 && run->mixed && psd)
+            scatter_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mq);
         else if (pass > 0 && run->mixed)
             scatter_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mm);
         else if (pass > 0 && psd)
@@ -472,6 +490,8 @@ int sort_species(h1d_run *run, int s)
             scatter_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, md);
         else if (run->mixed && !last)
             scatter_kernel<KEYS_MIXED><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mk);
+        else if (run->mixed && psd)
+            scatter_kernel<KEYS_MIXED><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mq);
         else if (run->mixed)
             scatter_kernel<KEYS_MIXED><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mm);
         else if (!last)
@@ -813,6 +833,12 @@ int ensure_capacity(h1d_run *run, int s, int64_t n)
             cudaFree(S.cell[k]);
             S.cell[k] = nullptr;
             CU(cudaMalloc(&S.cell[k], sizeof(int32_t) * cap));
+            if (evolves_psd(run->p.kinetic[s]))
+                for (auto *&b : S.fpsd[k]) {
+                    cudaFree(b);
+                    b = nullptr;
+                    CU(cudaMalloc(&b, sizeof(float) * cap));
+                }
         } else {
             for (auto *&b : S.buf[k]) {
                 cudaFree(b);
@@ -1408,6 +1434,7 @@ int h1d_destroy(h1d_run *run)
             cudaFree(S.cell[k]);
             cudaFree(S.pid[k]), cudaFree(S.keys[k]), cudaFree(S.idx[k]);
             cudaFree(S.psd[k][0]), cudaFree(S.psd[k][1]);
+            cudaFree(S.fpsd[k][0]), cudaFree(S.fpsd[k][1]);
         }
         cudaFree(S.hist), cudaFree(S.part), cudaFree(S.dead), cudaFree(S.dep), cudaFree(S.mom_raw), cudaFree(S.mom);
         cudaFree(S.eq);
@@ -1457,6 +1484,10 @@ int h1d_upload_particles(h1d_run *run, int s, int64_t n, double const *q1, doubl
         CU(cudaMemcpyAsync(S.psd[0][0], S.buf[0][4], sizeof(double) * n, cudaMemcpyDeviceToDevice, run->stream));
         CU(launch_fill(S.psd[0][1], n, 1.0, run->stream));
     }
+    if (n && S.fpsd[0][0]) {
+        CU(cudaMemcpyAsync(S.fpsd[0][0], S.fbuf[0][4], sizeof(float) * n, cudaMemcpyDeviceToDevice, run->stream));
+        CU(launch_fill_f(S.fpsd[0][1], n, 1.0f, run->stream));
+    }
     if (n)
         CU(launch_iota(S.pid[0], n, run->stream));
     S.since_sort       = 1 << 30;
@@ -1473,17 +1504,25 @@ int h1d_upload_psd(h1d_run *run, int s, int64_t n, double const *real_f, double 
     if (!run || s < 0 || s >= run->p.n_kinetic || (n > 0 && (!real_f || !marker)))
         return set_err(run, H1D_ERR_INVALID_ARG, "h1d_upload_psd: bad arguments");
     SpeciesState &S = run->sp[s];
-    if (!evolves_psd(run->p.kinetic[s]) || run->mixed)
+    if (!evolves_psd(run->p.kinetic[s]))
         return set_err(run, H1D_ERR_INVALID_ARG, "h1d_upload_psd: the weights of this species do not evolve");
     if (n != S.n)
         return set_err(run, H1D_ERR_INVALID_ARG, "h1d_upload_psd: count differs from the uploaded particles");
     if (n && !S.upload_order)
         return set_err(run, H1D_ERR_INVALID_ARG, "h1d_upload_psd: the particles were reordered since their upload");
     CU(cudaStreamSynchronize(run->stream));
-    if (n) {
+    if (n && !run->mixed) {
         CU(cudaMemcpyAsync(S.psd[S.cur][0], real_f, sizeof(double) * n, cudaMemcpyHostToDevice, run->stream));
         CU(cudaMemcpyAsync(S.psd[S.cur][1], marker, sizeof(double) * n, cudaMemcpyHostToDevice, run->stream));
     }
+    double const *src[2] = { real_f, marker };
+    for (int k = 0; k < 2 && n && run->mixed; ++k) // FP32 on the device, through the staging buffer
+        for (int64_t o = 0; o < n; o += run->stage_n) {
+            int64_t const c = std::min<int64_t>(run->stage_n, n - o);
+            CU(cudaMemcpyAsync(run->stage, src[k] + o, sizeof(double) * c, cudaMemcpyHostToDevice, run->stream));
+            to_f32_kernel<<<static_cast<unsigned>((c + 255) / 256), 256, 0, run->stream>>>(run->stage, c, S.fpsd[S.cur][k] + o);
+            CU(cudaGetLastError());
+        }
     CU(cudaStreamSynchronize(run->stream));
     return H1D_OK;
 }
@@ -1493,14 +1532,23 @@ int h1d_download_psd(h1d_run *run, int s, double *real_f, double *marker)
     if (!run || s < 0 || s >= run->p.n_kinetic)
         return H1D_ERR_INVALID_ARG;
     SpeciesState &S = run->sp[s];
-    if (!evolves_psd(run->p.kinetic[s]) || run->mixed)
+    if (!evolves_psd(run->p.kinetic[s]))
         return set_err(run, H1D_ERR_INVALID_ARG, "h1d_download_psd: the weights of this species do not evolve");
     if (run->p.particle_bc == H1D_BC_ABSORBING && S.n > 0 && S.since_sort > 0)
         TRY(sort_species(run, s)); // drop absorbed particles, as h1d_download_particles does
-    if (real_f && S.n)
+    if (real_f && S.n && !run->mixed)
         CU(cudaMemcpyAsync(real_f, S.psd[S.cur][0], sizeof(double) * S.n, cudaMemcpyDeviceToHost, run->stream));
-    if (marker && S.n)
+    if (marker && S.n && !run->mixed)
         CU(cudaMemcpyAsync(marker, S.psd[S.cur][1], sizeof(double) * S.n, cudaMemcpyDeviceToHost, run->stream));
+    double *dst[2] = { real_f, marker };
+    for (int k = 0; k < 2 && S.n && run->mixed; ++k) // FP32 on the device, through the staging buffer
+        for (int64_t o = 0; dst[k] && o < S.n; o += run->stage_n) {
+            int64_t const c = std::min<int64_t>(run->stage_n, S.n - o);
+            from_mixed_kernel<<<static_cast<unsigned>((c + 255) / 256), 256, 0, run->stream>>>(nullptr, S.fpsd[S.cur][k] + o, c,
+                                                                                             0.0, run->stage);
+            CU(cudaGetLastError());
+            CU(cudaMemcpyAsync(dst[k] + o, run->stage, sizeof(double) * c, cudaMemcpyDeviceToHost, run->stream));
+        }
     CU(cudaStreamSynchronize(run->stream));
     return H1D_OK;
 }
@@ -1983,7 +2031,7 @@ int h1d_vhistogram(h1d_run *run, int s, double ext_loc, double ext_len, double v
         VHistArgs a{};
         if (run->mixed)
             a.cell = S.cell[S.cur], a.off = S.fbuf[S.cur][0], a.fvx = S.fbuf[S.cur][1], a.fvy = S.fbuf[S.cur][2],
-            a.fvz = S.fbuf[S.cur][3], a.fw = S.fbuf[S.cur][4];
+            a.fvz = S.fbuf[S.cur][3], a.fw = S.fbuf[S.cur][4], a.freal_f = S.fpsd[S.cur][0], a.fmarker = S.fpsd[S.cur][1];
         else
             a.q1 = S.buf[S.cur][0], a.vx = S.buf[S.cur][1], a.vy = S.buf[S.cur][2], a.vz = S.buf[S.cur][3],
             a.w = S.buf[S.cur][4], a.real_f = S.psd[S.cur][0], a.marker = S.psd[S.cur][1];
@@ -2457,7 +2505,7 @@ uint64_t params_signature(h1d_params p)
 // bytes of species s with n particles: the record, the id, and real_f / marker when its weights evolve
 size_t particle_bytes(h1d_run const *run, int s, int64_t n)
 {
-    size_t const psd = !run->mixed && evolves_psd(run->p.kinetic[s]) ? 2 * 8 : 0;
+    size_t const psd = evolves_psd(run->p.kinetic[s]) ? 2 * (run->mixed ? 4 : 8) : 0;
     return static_cast<size_t>(n) * ((run->mixed ? 6 * 4 + 4 : 5 * 8 + 4) + psd);
 }
 
@@ -2527,9 +2575,9 @@ int h1d_checkpoint_save(h1d_run *run, void *buffer, size_t capacity, size_t *wri
                 CU(d2h(S.buf[S.cur][k], 8 * n));
         }
         CU(d2h(S.pid[S.cur], 4 * n));
-        if (!run->mixed && evolves_psd(run->p.kinetic[s]))
+        if (evolves_psd(run->p.kinetic[s]))
             for (int k = 0; k < 2; ++k)
-                CU(d2h(S.psd[S.cur][k], 8 * n));
+                CU(run->mixed ? d2h(S.fpsd[S.cur][k], 4 * n) : d2h(S.psd[S.cur][k], 8 * n));
     }
     CU(cudaStreamSynchronize(run->stream));
     if (written)
@@ -2587,9 +2635,9 @@ int h1d_checkpoint_load(h1d_run *run, void const *buffer, size_t size)
                 CU(h2d(S.buf[0][k], 8 * n));
         }
         CU(h2d(S.pid[0], 4 * n));
-        if (!run->mixed && evolves_psd(run->p.kinetic[s]))
+        if (evolves_psd(run->p.kinetic[s]))
             for (int k = 0; k < 2; ++k)
-                CU(h2d(S.psd[0][k], 8 * n));
+                CU(run->mixed ? h2d(S.fpsd[0][k], 4 * n) : h2d(S.psd[0][k], 8 * n));
         CU(cudaMemsetAsync(S.dep, 0, sizeof(double) * 16 * M, run->stream)); // no deposit in flight
         S.since_sort = 1 << 30;
     }

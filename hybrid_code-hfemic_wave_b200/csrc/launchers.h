@@ -34,6 +34,7 @@ cudaError_t launch_finalize_cold(double const *n_full, double const *nV_full, do
 cudaError_t launch_energy(EnergyArgs const &a, cudaStream_t st);
 cudaError_t launch_iota(int32_t *pid, int64_t n, cudaStream_t st);
 cudaError_t launch_fill(double *a, int64_t n, double v, cudaStream_t st);
+cudaError_t launch_fill_f(float *a, int64_t n, float v, cudaStream_t st);
 // the external sources of a run at time t (source_kernel, post.cuh)
 struct SourceArgs {
     h1d_source_desc d[MAXE];

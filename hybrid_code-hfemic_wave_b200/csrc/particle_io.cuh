@@ -338,7 +338,7 @@ struct VHistArgs {
     double const  *q1, *vx, *vy, *vz, *w;        // FP64 storage (+ real_f, marker when the weights evolve), or
     double const  *real_f, *marker;
     int32_t const *cell;                         // mixed-precision storage
-    float const   *off, *fvx, *fvy, *fvz, *fw;
+    float const   *off, *fvx, *fvy, *fvz, *fw, *freal_f, *fmarker;
     int64_t        n;
     double         half_min, full_min, ext_lo, ext_hi, v1min, v1len, v2min, v2len;
     int            v1dim, v2dim;
@@ -387,7 +387,10 @@ __global__ void vhist_kernel(VHistArgs a)
         atomicAdd(o, 1.0);
         atomicAdd(o + 1, w);
         // real_f / marker; without evolving weights real_f = w and marker = 1 (the upload convention)
-        atomicAdd(o + 2, a.real_f ? __ddiv_rn(a.real_f[k], a.marker[k]) : w);
+        double const rm = a.real_f  ? __ddiv_rn(a.real_f[k], a.marker[k])
+                          : a.freal_f ? static_cast<double>(a.freal_f[k]) / static_cast<double>(a.fmarker[k])
+                                      : w;
+        atomicAdd(o + 2, rm);
     }
 }
 

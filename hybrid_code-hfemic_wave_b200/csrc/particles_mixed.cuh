@@ -26,6 +26,11 @@ struct PushArgsMixed {
     uint64_t     seed, counter;
     int          species, randomize;
     int          move_steps, deposit_mask, write_back;
+    // evolving weights (push_kernel_mixed<..., PSD = true>): FP32 Particle::PSD arrays and the
+    // equilibrium bi-Maxwellian of PartSpecies::impl_update_weight, as in PushArgs
+    float       *real_f, *marker;
+    float        nu_dt, vth1, vth1_cubed, T2_T1;
+    int          psd_refresh, delta_f;
 };
 
 struct f3 {
@@ -202,19 +207,45 @@ constexpr int MIX_W     = 8; // 4 quantities x 8 cells = the 32 lanes of a flush
 static_assert(4 * MIX_W == 32, "a window flush reduce-scatters exactly 32 values");
 
 // a stage holds one chunk; the consumers overwrite it in place with the new state, which the
-// producer then stores
-struct PipeStageMixed {
+// producer then stores.  With evolving weights (PSD) a stage also holds real_f and marker and the
+// pipeline is one stage shorter, so that four CTAs still fit an SM.
+template <bool PSD>
+struct PipeStageMixedT {
     int32_t cell[MIX_CHUNK];
     float   off[MIX_CHUNK], vx[MIX_CHUNK], vy[MIX_CHUNK], vz[MIX_CHUNK], w[MIX_CHUNK];
     int32_t pid[MIX_CHUNK];
+    float   real_f[PSD ? MIX_CHUNK : 4], marker[PSD ? MIX_CHUNK : 4];
 };
+using PipeStageMixed = PipeStageMixedT<false>;
 constexpr int    PIPE_STAGES_MIXED      = 3;
 constexpr int    PIPE_CTAS_PER_SM_MIXED = 4;
-constexpr size_t MIX_BAR_OFFSET         = sizeof(PipeStageMixed) * PIPE_STAGES_MIXED;
-constexpr size_t MIX_COL_OFFSET         = MIX_BAR_OFFSET + 128; // barriers, then 16-byte aligned columns
-constexpr size_t MIX_COL_BYTES          = sizeof(float4) * PIPE_CONSUMER_WARPS * 2 * MIX_W * 32;
-constexpr size_t PIPE_SMEM_MIXED        = MIX_COL_OFFSET + MIX_COL_BYTES;
+template <bool PSD>
+struct MixLayout {
+    static constexpr int    STAGES     = PSD ? PIPE_STAGES_MIXED - 1 : PIPE_STAGES_MIXED;
+    static constexpr size_t BAR_OFFSET = sizeof(PipeStageMixedT<PSD>) * STAGES;
+    static constexpr size_t COL_OFFSET = BAR_OFFSET + 128; // barriers, then 16-byte aligned columns
+};
+constexpr size_t MIX_COL_BYTES        = sizeof(float4) * PIPE_CONSUMER_WARPS * 2 * MIX_W * 32;
+constexpr size_t PIPE_SMEM_MIXED      = MixLayout<false>::COL_OFFSET + MIX_COL_BYTES;
+constexpr size_t PIPE_SMEM_MIXED_PSD  = MixLayout<true>::COL_OFFSET + MIX_COL_BYTES;
 static_assert(2 * PIPE_STAGES_MIXED * sizeof(uint64_t) <= 128, "barriers fit before the columns");
+static_assert(PIPE_CTAS_PER_SM_MIXED * (PIPE_SMEM_MIXED_PSD + 1024) <= 233472, "four CTAs with evolving weights fit an SM");
+
+// PartSpecies::impl_update_weight in FP32 for one particle after its velocity update (as
+// update_weight, particles.cuh): f0 of the equilibrium bi-Maxwellian at velocity v and at the
+// push position (c2 = cos^2(xi D1 q1)), then real_f and the weight
+__device__ __forceinline__ float update_weight_f(PushArgsMixed const &a, f3 v, float c2, float &real_f, float marker)
+{
+    float const eta   = 1.0f / (a.T2_T1 + (1.0f - a.T2_T1) * c2);
+    float const T2OT1 = a.T2_T1 * eta;
+    float const x1 = v.x / a.vth1, x2 = v.y / a.vth1, x3 = v.z / a.vth1;
+    float const f1 = expf(-x1 * x1) * 0.5641895835477563f;
+    float const f2 = expf(-(x2 * x2 + x3 * x3) / T2OT1) / (3.14159265358979f * T2OT1);
+    float const f0 = eta * ((f1 * f2) / a.vth1_cubed);
+    if (a.psd_refresh)
+        real_f = (real_f + a.nu_dt * f0) / (1.0f + a.nu_dt);
+    return a.delta_f ? (real_f - f0) / marker : real_f / marker;
+}
 
 // a warp's deposit window: columns [d][c][lane] (d: deposit at x^N / at the end position)
 struct ColWindow {
@@ -320,15 +351,16 @@ __device__ __forceinline__ void deposit_direct(PushArgsMixed const &a, int d, Sh
     }
 }
 
-template <int O, bool MIRROR, int BC, int MAXG>
+template <int O, bool MIRROR, int BC, int MAXG, bool PSD = false>
 __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
     push_kernel_mixed(PushGroupsMixed<MAXG> const __grid_constant__ G)
 {
-    constexpr int   STAGES = PIPE_STAGES_MIXED;
+    constexpr int   STAGES = MixLayout<PSD>::STAGES;
     constexpr int   SPAN   = MIX_W - 1 - O; // largest stencil base offset inside the window
+    using Stage            = PipeStageMixedT<PSD>;
     extern __shared__ __align__(128) unsigned char smraw[];
-    PipeStageMixed *stage = reinterpret_cast<PipeStageMixed *>(smraw);
-    uint64_t       *full  = reinterpret_cast<uint64_t *>(smraw + MIX_BAR_OFFSET);
+    Stage          *stage = reinterpret_cast<Stage *>(smraw);
+    uint64_t       *full  = reinterpret_cast<uint64_t *>(smraw + MixLayout<PSD>::BAR_OFFSET);
     uint64_t       *empty = full + STAGES;
     int const       warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int64_t const   nchunks = G.chunk0[G.n];
@@ -367,8 +399,10 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                         bulk_store(a.vx + start, stage[s].vx, b4);
                         bulk_store(a.vy + start, stage[s].vy, b4);
                         bulk_store(a.vz + start, stage[s].vz, b4);
-                        if (BC == BCK_ABSORBING)
+                        if (BC == BCK_ABSORBING || PSD)
                             bulk_store(a.w + start, stage[s].w, b4);
+                        if (PSD)
+                            bulk_store(a.real_f + start, stage[s].real_f, b4);
                         bulk_commit();
                     }
                     bulk_wait_read_all();
@@ -380,7 +414,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                     int64_t const  start = (c0 + i - G.chunk0[gl]) * MIX_CHUNK;
                     uint32_t const cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(MIX_CHUNK), a.n - start));
                     uint32_t const b4    = round16(cnt * 4);
-                    mbar_arrive_expect_tx(&full[s], (6 + (lpid ? 1 : 0)) * b4);
+                    mbar_arrive_expect_tx(&full[s], (6 + (lpid ? 1 : 0) + (PSD ? 2 : 0)) * b4);
                     bulk_load(stage[s].cell, a.cell + start, b4, &full[s]);
                     bulk_load(stage[s].off, a.off + start, b4, &full[s]);
                     bulk_load(stage[s].vx, a.vx + start, b4, &full[s]);
@@ -389,6 +423,10 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                     bulk_load(stage[s].w, a.w + start, b4, &full[s]);
                     if (lpid)
                         bulk_load(stage[s].pid, a.pid + start, b4, &full[s]);
+                    if (PSD) {
+                        bulk_load(stage[s].real_f, a.real_f + start, b4, &full[s]);
+                        bulk_load(stage[s].marker, a.marker + start, b4, &full[s]);
+                    }
                 }
             }
             bulk_wait_all();
@@ -398,7 +436,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
 
     // ---------------- consumers ----------------
     ColWindow win;
-    win.col  = reinterpret_cast<float4 *>(smraw + MIX_COL_OFFSET) + warp * 2 * MIX_W * 32;
+    win.col  = reinterpret_cast<float4 *>(smraw + MixLayout<PSD>::COL_OFFSET) + warp * 2 * MIX_W * 32;
     win.base = ColWindow::NONE;
     win.zero(lane);
     unsigned bad = 0;
@@ -426,7 +464,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
         }
         int64_t const   start = (c0 + i - G.chunk0[gc]) * MIX_CHUNK;
         int const       cnt   = static_cast<int>(min(static_cast<int64_t>(MIX_CHUNK), a.n - start));
-        PipeStageMixed &P     = stage[s];
+        Stage          &P     = stage[s];
         int const       w0    = warp * 32 * MIX_PPT;
 
         // The lane's two particles are adjacent (i2, i2 + 1) and pushed as a pair on the packed
@@ -440,7 +478,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
         p3         v       = { *reinterpret_cast<float2 const *>(P.vx + i2), *reinterpret_cast<float2 const *>(P.vy + i2),
                                *reinterpret_cast<float2 const *>(P.vz + i2) };
         float2       w    = *reinterpret_cast<float2 const *>(P.w + i2);
-        float2 const w_in = w;
+        float2       w_in = w;
         int2 const   pid  = load_pid ? *reinterpret_cast<int2 const *>(P.pid + i2) : make_int2(0, 0);
         bool         alive[2] = { true, true };
         if (a.move_steps == 2) { // predictor-corrector: half move and boundary before the push
@@ -517,6 +555,12 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                 if (live[k] && !(fabsf(el(dq, k) * a.travel_scale) < 1.0f))
                     bad |= ST_MOVED_TOO_FAR;
                 f3 vk      = { el(vp.x, k), el(vp.y, k), el(vp.z, k) };
+                if constexpr (PSD) { // the weight at the new velocity and the push position
+                    float rf       = P.real_f[i2 + k];
+                    el(w, k)       = update_weight_f(a, vk, el(c2, k), rf, P.marker[i2 + k]);
+                    el(w_in, k)    = el(w, k);
+                    P.real_f[i2 + k] = rf;
+                }
                 el(v_push.x, k) = vk.x, el(v_push.y, k) = vk.y, el(v_push.z, k) = vk.z;
                 move_cell(cell[k], el(off, k), el(dq, k));
                 alive[k] = boundary_mixed<BC>(a, cell[k], el(off, k), vk, k ? pid.y : pid.x,
@@ -534,7 +578,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
         *reinterpret_cast<float2 *>(P.vx + i2)  = v.x;
         *reinterpret_cast<float2 *>(P.vy + i2)  = v.y;
         *reinterpret_cast<float2 *>(P.vz + i2)  = v.z;
-        if (BC == BCK_ABSORBING)
+        if (BC == BCK_ABSORBING || PSD)
             *reinterpret_cast<float2 *>(P.w + i2) = w;
         {
             p3 const m0 = { pmul(v_push.x, w_in), pmul(v_push.y, w_in), pmul(v_push.z, w_in) };

@@ -15,6 +15,12 @@ __global__ void fill_kernel(double *a, int64_t n, double v)
     if (i < n)
         a[i] = v;
 }
+__global__ void fill_f_kernel(float *a, int64_t n, float v)
+{
+    int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n)
+        a[i] = v;
+}
 __global__ void iota_kernel(int32_t *pid, int64_t n)
 {
     int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;

@@ -20,7 +20,8 @@ cudaError_t launch_push_groups(PushArgs const *args, int n, int order, bool mirr
                                cudaStream_t st);
 cudaError_t launch_push_groups(PushArgsMixed const *args, int n, int order, bool mirror, int bc, int max_ctas,
                                cudaStream_t st);
-// one FP64 pass over a species whose weights evolve (push_kernel<..., PSD = true>)
+// one pass over a species whose weights evolve (push_kernel<..., PSD = true>, push_kernel_mixed<..., PSD = true>)
 cudaError_t launch_push_psd(PushArgs const &a, int order, bool mirror, int bc, int max_ctas, cudaStream_t st);
+cudaError_t launch_push_psd(PushArgsMixed const &a, int order, bool mirror, int bc, int max_ctas, cudaStream_t st);
 
 } // namespace h1d

@@ -9,41 +9,41 @@
 namespace h1d {
 namespace {
 
-template <int O, bool M, int BC, int MAXG>
+template <int O, bool M, int BC, int MAXG, bool PSD>
 void pk(PushGroupsMixed<MAXG> const &G, dim3 g, cudaStream_t st)
 {
-    push_kernel_mixed<O, M, BC, MAXG><<<g, PIPE_THREADS, PIPE_SMEM_MIXED, st>>>(G);
+    push_kernel_mixed<O, M, BC, MAXG, PSD><<<g, PIPE_THREADS, PSD ? PIPE_SMEM_MIXED_PSD : PIPE_SMEM_MIXED, st>>>(G);
 }
-template <int O, bool M, int BC, int MAXG>
+template <int O, bool M, int BC, int MAXG, bool PSD>
 cudaError_t pk_attr()
 {
-    return cudaFuncSetAttribute(push_kernel_mixed<O, M, BC, MAXG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                static_cast<int>(PIPE_SMEM_MIXED));
+    return cudaFuncSetAttribute(push_kernel_mixed<O, M, BC, MAXG, PSD>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(PSD ? PIPE_SMEM_MIXED_PSD : PIPE_SMEM_MIXED));
 }
 
 
-template <int O, bool M, class GR>
+template <int O, bool M, bool PSD, class GR>
 void pk_bc(GR const &G, int bc, dim3 g, cudaStream_t st)
 {
     if (bc == 0)
-        pk<O, M, BCK_PERIODIC>(G, g, st);
+        pk<O, M, BCK_PERIODIC, GR::MAX, PSD>(G, g, st);
     else if (bc == 1)
-        pk<O, M, BCK_REFLECTING>(G, g, st);
+        pk<O, M, BCK_REFLECTING, GR::MAX, PSD>(G, g, st);
     else
-        pk<O, M, BCK_ABSORBING>(G, g, st);
+        pk<O, M, BCK_ABSORBING, GR::MAX, PSD>(G, g, st);
 }
-template <class GR>
+template <bool PSD = false, class GR>
 void pk_dispatch(GR const &G, int order, bool mirror, int bc, dim3 g, cudaStream_t st)
 {
     if (order == 1)
-        mirror ? pk_bc<1, true>(G, bc, g, st) : pk_bc<1, false>(G, bc, g, st);
+        mirror ? pk_bc<1, true, PSD>(G, bc, g, st) : pk_bc<1, false, PSD>(G, bc, g, st);
     else if (order == 2)
-        mirror ? pk_bc<2, true>(G, bc, g, st) : pk_bc<2, false>(G, bc, g, st);
+        mirror ? pk_bc<2, true, PSD>(G, bc, g, st) : pk_bc<2, false, PSD>(G, bc, g, st);
     else
-        mirror ? pk_bc<3, true>(G, bc, g, st) : pk_bc<3, false>(G, bc, g, st);
+        mirror ? pk_bc<3, true, PSD>(G, bc, g, st) : pk_bc<3, false, PSD>(G, bc, g, st);
 }
 
-template <int MAXG>
+template <int MAXG, bool PSD>
 cudaError_t pk_attrs()
 {
     cudaError_t e = cudaSuccess;
@@ -51,12 +51,12 @@ cudaError_t pk_attrs()
         if (e == cudaSuccess)
             e = x;
     };
-    k(pk_attr<1, false, 0, MAXG>()), k(pk_attr<1, false, 1, MAXG>()), k(pk_attr<1, false, 2, MAXG>());
-    k(pk_attr<1, true, 0, MAXG>()), k(pk_attr<1, true, 1, MAXG>()), k(pk_attr<1, true, 2, MAXG>());
-    k(pk_attr<2, false, 0, MAXG>()), k(pk_attr<2, false, 1, MAXG>()), k(pk_attr<2, false, 2, MAXG>());
-    k(pk_attr<2, true, 0, MAXG>()), k(pk_attr<2, true, 1, MAXG>()), k(pk_attr<2, true, 2, MAXG>());
-    k(pk_attr<3, false, 0, MAXG>()), k(pk_attr<3, false, 1, MAXG>()), k(pk_attr<3, false, 2, MAXG>());
-    k(pk_attr<3, true, 0, MAXG>()), k(pk_attr<3, true, 1, MAXG>()), k(pk_attr<3, true, 2, MAXG>());
+    k(pk_attr<1, false, 0, MAXG, PSD>()), k(pk_attr<1, false, 1, MAXG, PSD>()), k(pk_attr<1, false, 2, MAXG, PSD>());
+    k(pk_attr<1, true, 0, MAXG, PSD>()), k(pk_attr<1, true, 1, MAXG, PSD>()), k(pk_attr<1, true, 2, MAXG, PSD>());
+    k(pk_attr<2, false, 0, MAXG, PSD>()), k(pk_attr<2, false, 1, MAXG, PSD>()), k(pk_attr<2, false, 2, MAXG, PSD>());
+    k(pk_attr<2, true, 0, MAXG, PSD>()), k(pk_attr<2, true, 1, MAXG, PSD>()), k(pk_attr<2, true, 2, MAXG, PSD>());
+    k(pk_attr<3, false, 0, MAXG, PSD>()), k(pk_attr<3, false, 1, MAXG, PSD>()), k(pk_attr<3, false, 2, MAXG, PSD>());
+    k(pk_attr<3, true, 0, MAXG, PSD>()), k(pk_attr<3, true, 1, MAXG, PSD>()), k(pk_attr<3, true, 2, MAXG, PSD>());
     return e;
 }
 
@@ -70,9 +70,11 @@ cudaError_t set_smem_once()
     std::lock_guard<std::mutex> lock(m);
     if (dev >= 0 && dev < 64 && done[dev])
         return cudaSuccess;
-    cudaError_t e = pk_attrs<1>();
+    cudaError_t e = pk_attrs<1, false>();
     if (e == cudaSuccess)
-        e = pk_attrs<BATCH_GROUPS>();
+        e = pk_attrs<BATCH_GROUPS, false>();
+    if (e == cudaSuccess)
+        e = pk_attrs<1, true>();
     if (e == cudaSuccess && dev >= 0 && dev < 64)
         done[dev] = true;
     return e;
@@ -124,6 +126,17 @@ cudaError_t launch_push_groups(PushArgsMixed const *args, int n, int order, bool
                                cudaStream_t st)
 {
     return launch_groups<PushArgsMixed, PushGroupsMixed>(args, n, order, mirror, bc, max_ctas, st);
+}
+
+cudaError_t launch_push_psd(PushArgsMixed const &a, int order, bool mirror, int bc, int max_ctas, cudaStream_t st)
+{
+    int64_t const total = chunks_of(a.n);
+    if (total == 0)
+        return cudaSuccess;
+    PushGroupsMixed<1> G{};
+    G.n = 1, G.chunk0[0] = 0, G.chunk0[1] = total, G.g[0] = a;
+    pk_dispatch<true>(G, order, mirror, bc, dim3(static_cast<unsigned>(std::min<int64_t>(total, max_ctas))), st);
+    return cudaGetLastError();
 }
 
 } // namespace h1d

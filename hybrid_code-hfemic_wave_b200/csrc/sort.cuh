@@ -292,22 +292,25 @@ struct MoveFP64T {
     }
 };
 using MoveFP64 = MoveFP64T<false>;
-// ... or the mixed-precision records (offset, vx, vy, vz, w as FP32; cell, pid)
-struct MoveMixed {
+// ... or the mixed-precision records (offset, vx, vy, vz, w as FP32, with PSD also real_f and
+// marker; cell, pid)
+template <bool PSD>
+struct MoveMixedT {
+    static constexpr int NV   = PSD ? 7 : 5;
     static constexpr int HOLD = SORT_ITEMS / 2;
-    float const         *src[5];
-    int32_t const *cell_src, *pid_src;
-    float         *dst[5];
-    int32_t       *cell_dst, *pid_dst;
+    float const         *src[NV];
+    int32_t const       *cell_src, *pid_src;
+    float               *dst[NV];
+    int32_t             *cell_dst, *pid_dst;
     struct Rec {
-        float   v[5];
+        float   v[NV];
         int32_t cell, pid;
     };
     __device__ __forceinline__ Rec load(uint32_t, uint32_t j) const
     {
         Rec r;
 #pragma unroll
-        for (int k = 0; k < 5; ++k)
+        for (int k = 0; k < NV; ++k)
             r.v[k] = src[k][j];
         r.cell = cell_src[j];
         r.pid  = pid_src[j];
@@ -316,12 +319,13 @@ struct MoveMixed {
     __device__ __forceinline__ void store(uint32_t pos, Rec const &r) const
     {
 #pragma unroll
-        for (int k = 0; k < 5; ++k)
+        for (int k = 0; k < NV; ++k)
             dst[k][pos] = r.v[k];
         cell_dst[pos] = r.cell;
         pid_dst[pos]  = r.pid;
     }
 };
+using MoveMixed = MoveMixedT<false>;
 
 template <int KIND, class Move>
 __global__ void __launch_bounds__(SORT_THREADS)

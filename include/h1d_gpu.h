@@ -187,9 +187,10 @@ int h1d_destroy(h1d_run *run);
 int h1d_upload_particles(h1d_run *run, int s, int64_t n, const double *q1, const double *vx,
                          const double *vy, const double *vz, const double *w);
 /* Phase-space densities of the particles of species `s` (Particle::PSD::real_f, ::marker), in the
- * order of the last h1d_upload_particles; required before the first step of a species whose
- * weights evolve (scheme H1D_DELTA_F or psd_refresh_frequency != 0), INVALID_ARG otherwise or
- * when n differs from the uploaded count.  FP64 runs only. */
+ * order of the last h1d_upload_particles and before the first step, for a species whose weights
+ * evolve (scheme H1D_DELTA_F or psd_refresh_frequency != 0); INVALID_ARG for other species, when
+ * n differs from the uploaded count or after the particles were reordered.  Until it is called,
+ * real_f = w and marker = 1.  Mixed-precision runs keep them in FP32. */
 int h1d_upload_psd(h1d_run *run, int s, int64_t n, const double *real_f, const double *marker);
 /* ... and back, in the order of h1d_download_particles; either pointer may be NULL. */
 int h1d_download_psd(h1d_run *run, int s, double *real_f, double *marker);

@@ -17,8 +17,7 @@ import hfemic_b200 as h
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-# delta-f and PSD refresh run in FP64 only (test_gpu_psd.py checks that mixed runs refuse them)
-ALL = [n for n in sorted(h.configs.PARITY) if not h.configs.PARITY[n]().has_psd]
+ALL = sorted(h.configs.PARITY)
 TOL = 1e-4
 MIXED = h.configs.PREC_MIXED
 
