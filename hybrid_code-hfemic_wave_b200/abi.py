@@ -19,7 +19,7 @@ from . import configs as _cfg
 PAD = 3
 MAX_KINETIC = 8
 MAX_COLD = 4
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 OK, ERR_INVALID_ARG, ERR_MOVED_TOO_FAR, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_NAN, ERR_STATE, \
     ERR_NO_DEVICE = range(9)
@@ -38,8 +38,8 @@ class MovedTooFar(H1DError):
 class KineticDesc(C.Structure):
     _fields_ = [("Oc", C.c_double), ("op", C.c_double), ("n_smooth", C.c_int64), ("Nc", C.c_int64),
                 ("shape_order", C.c_int64), ("moment_norm", C.c_double), ("scheme", C.c_int32),
-                ("reserved", C.c_int32), ("psd_refresh_frequency", C.c_double), ("vth1", C.c_double),
-                ("T2_T1", C.c_double)]
+                ("vdf", C.c_int32), ("psd_refresh_frequency", C.c_double), ("vth1", C.c_double),
+                ("T2_T1", C.c_double), ("vdf_param", C.c_double * 3)]
 
 
 class ColdDesc(C.Structure):
@@ -93,8 +93,8 @@ def make_params(cfg: "_cfg.RunConfig") -> Params:
     ef = cfg.efluid
     p.efluid = EFluidDesc(ef.Oc, ef.op, ef.beta, ef.gamma)
     for i, k in enumerate(cfg.kinetic):
-        p.kinetic[i] = KineticDesc(k.Oc, k.op, k.n_smooth, k.Nc, k.shape_order, cfg.moment_norm(k), k.scheme, 0,
-                                   k.psd_refresh_frequency, k.vth1(cfg.c), k.T2_T1)
+        p.kinetic[i] = KineticDesc(k.Oc, k.op, k.n_smooth, k.Nc, k.shape_order, cfg.moment_norm(k), k.scheme, k.vdf,
+                                   k.psd_refresh_frequency, k.vth1(cfg.c), k.T2_T1, (C.c_double * 3)(*k.vdf_param()))
     for i, c in enumerate(cfg.cold):
         p.cold[i] = ColdDesc(c.Oc, c.op, c.n_smooth)
     if len(cfg.sources) > MAX_SOURCES:

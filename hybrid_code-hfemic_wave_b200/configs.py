@@ -24,11 +24,17 @@ BC_PERIODIC, BC_REFLECTING, BC_ABSORBING = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 ISOTHERMAL, ADIABATIC = 11, 53  # Closure (src/LibPIC/PIC/Predefined.h:35-38)
 FULL_F, DELTA_F = 0, 1  # ParticleScheme (src/LibPIC/PIC/Predefined.h)
+# the equilibrium distribution of a kinetic species (VDFVariant, src/LibPIC/PIC/VDFVariant.h)
+VDF_BIMAXWELLIAN, VDF_LOSSCONE, VDF_PARTIAL_SHELL, VDF_COUNTER_BEAM = 0, 1, 2, 3
 
 
 @dataclass
 class Kinetic:
-    """A bi-Maxwellian kinetic species (BiMaxPlasmaDesc, PlasmaDesc.h:207-236)."""
+    """A kinetic species (KineticPlasmaDesc, PlasmaDesc.h:118-177) with its equilibrium
+    distribution: bi-Maxwellian (BiMaxPlasmaDesc, :207-236, the default), loss-cone
+    (LossconePlasmaDesc, :244-284: ``losscone_beta``; ``T2_T1`` is the BiMaxPlasmaDesc value),
+    partial shell (PartialShellPlasmaDesc, :290-320: thermal spread ``beta1``, ``zeta``, ``vs``) or
+    counter-beam (CounterBeamPlasmaDesc, :326-345: thermal spread ``beta1``, ``nu``, ``vs``)."""
 
     Oc: float
     op: float
@@ -42,6 +48,22 @@ class Kinetic:
     initial_weight: float = 0.0  # delta-f only: initial weights are initial_weight * U(-1, 1)
     marker_temp_ratio: float = 1.0  # marker temperature / physical temperature
     psd_refresh_frequency: float = 0.0  # nu: weights relax toward the equilibrium at this rate
+    vdf: int = VDF_BIMAXWELLIAN
+    losscone_beta: float = 0.0
+    zeta: int = 0  # partial shell: sin^zeta pitch-angle exponent
+    vs: float = 0.0  # partial shell, counter-beam: shell speed
+    nu: float = 0.0  # counter-beam: pitch-angle width at the equator
+    norm: float | None = None  # PartSpecies::Nc when given by the caller (else computed)
+
+    def vdf_param(self):
+        """h1d_kinetic_desc::vdf_param of this distribution."""
+        if self.vdf == VDF_LOSSCONE:
+            return (self.losscone_beta, 0.0, 0.0)
+        if self.vdf == VDF_PARTIAL_SHELL:
+            return (float(self.zeta), self.vs, 0.0)
+        if self.vdf == VDF_COUNTER_BEAM:
+            return (self.nu, self.vs, 0.0)
+        return (0.0, 0.0, 0.0)
 
     def vth1(self, c: float) -> float:
         return math.sqrt(self.beta1) * c * abs(self.Oc) / self.op
@@ -142,8 +164,11 @@ class RunConfig:
         return self.xi < 1e-10  # MirrorGeometry.h:109, :185
 
     def moment_norm(self, k: Kinetic) -> float:
-        """PartSpecies::Nc = Nx*Nc*Nrefcell_div_Ntotal (PartSpecies.cc:150-154) for a
-        bi-Maxwellian (MaxwellianVDF.cc:213-215, N_of_q1 :229-239)."""
+        """PartSpecies::Nc = Nx*Nc*Nrefcell_div_Ntotal (PartSpecies.cc:150-154), with the
+        distribution's N_of_q1 (MaxwellianVDF.cc:213-239, LossconeVDF.cc:36-38, 79-95,
+        PartialShellVDF.cc:84-93); ``k.norm`` when the caller gives it."""
+        if k.norm is not None:
+            return k.norm
         if self.Nx * k.Nc == 0:
             return 1.0
         return self.Nx * k.Nc * nrefcell_div_ntotal(self, k)
@@ -163,8 +188,54 @@ class RunConfig:
                     raise ValueError("invalid domain extent: |xi*D1*q1| >= pi/2")
 
 
+def _int_cos_zeta(zeta: int, a: float, x: float, small_a: bool) -> float:
+    """int_0^x cos^zeta(a t) dt by the recurrence of VDFHelper.h:148-170 (zeta - 2 -> zeta)."""
+    ax = a * x
+    if zeta == 0:
+        return x
+    if zeta == 1:
+        return (1 - ax * ax * 0.1666666666666666666666666666666666666667) * x if small_a else math.sin(ax) / a
+    addendum = _int_cos_zeta(zeta - 2, a, x, small_a) * float(zeta - 1) / zeta
+    if small_a:
+        return (1 + ax * ax * 0.1666666666666666666666666666666666666667 * (2 - 3 * float(zeta))) * (x / zeta) + addendum
+    return math.cos(ax) ** (zeta - 1) * math.sin(ax) / (zeta * a) + addendum
+
+
+def _losscone_beta(k: Kinetic) -> float:
+    b = k.losscone_beta
+    if b < 1e-10:
+        return 1e-10
+    if abs(b - 1) < 1e-10:
+        return b + math.copysign(1e-10, b - 1)
+    return b
+
+
 def _n_of_q1(cfg: RunConfig, k: Kinetic, q1: float) -> float:
-    """MaxwellianVDF::N_of_q1 (MaxwellianVDF.cc:229-239)."""
+    """N_of_q1 of the species' distribution: MaxwellianVDF.cc:229-239, LossconeVDF.cc:79-95,
+    PartialShellVDF.cc:84-93; counter-beam: the integral of n0 by Gauss-Legendre quadrature
+    (the reference integrates it numerically to about 1e-8, VDFHelper.h:43-64)."""
+    if k.vdf == VDF_LOSSCONE:
+        b = _losscone_beta(k)
+        X = k.T2_T1 / (1 + b)
+        if cfg.homogeneous:
+            xiD1q1 = cfg.xi * cfg.Dx * q1
+            t1 = 1 - (X - 1) / 3 * xiD1q1 * xiD1q1
+            t2 = 1 - (b * X - 1) / 3 * xiD1q1 * xiD1q1
+            return q1 * (t1 - b * t2) / (1 - b)
+        sb, sx = math.sqrt(b), math.sqrt(X)
+        tan = math.tan(cfg.xi * cfg.Dx * q1)
+        t1 = math.atan(sx * tan) / (sx * cfg.Dx * cfg.xi)
+        t2 = math.atan(sb * sx * tan) / (sb * sx * cfg.Dx * cfg.xi)
+        return (t1 - b * t2) / (1 - b)
+    if k.vdf == VDF_PARTIAL_SHELL:
+        return _int_cos_zeta(k.zeta, cfg.xi, cfg.Dx * q1, cfg.homogeneous)
+    if k.vdf == VDF_COUNTER_BEAM:
+        import numpy as np
+        t, w = np.polynomial.legendre.leggauss(64)
+        q = 0.5 * q1 * (t + 1)
+        nu = k.nu / np.cos(cfg.xi * cfg.Dx * q)
+        bnu = np.array([2 * v * dawson(1 / v) for v in nu])
+        return float(0.5 * q1 * np.sum(w * bnu)) / (2 * k.nu * dawson(1 / k.nu))
     T2OT1 = k.T2_T1
     if cfg.homogeneous:
         xiD1q1 = cfg.xi * cfg.Dx * q1
@@ -181,6 +252,25 @@ def _q1_of_n(cfg: RunConfig, k: Kinetic, N: float) -> float:
         return N * (1 + (xiD1N * xiD1N) * (T2OT1 - 1) / 3)
     s = math.sqrt(T2OT1)
     return math.atan(math.tan(s * cfg.Dx * cfg.xi * N) / s) / (cfg.xi * cfg.Dx)
+
+
+def dawson(x: float) -> float:
+    """Dawson's integral F(x) = exp(-x^2) int_0^x exp(t^2) dt, x > 0: Maclaurin series below 0.2,
+    Rybicki's sum pi^-1/2 sum_{n odd} exp(-(x - 0.2 n)^2)/n up to 50, asymptotic series beyond."""
+    if x < 0.2:
+        t = s = x
+        for n in range(1, 40):
+            t *= -2 * x * x / (2 * n + 1)
+            s += t
+        return s
+    if x > 50:
+        r, t, s = 1 / (2 * x * x), 1.0, 1.0
+        for j in range(1, 12):
+            t *= (2 * j - 1) * r
+            s += t
+        return s / (2 * x)
+    lo, hi = int(math.floor((x - 7) / 0.2)) | 1, int(math.ceil((x + 7) / 0.2))
+    return sum(math.exp(-(x - n * 0.2) ** 2) / n for n in range(lo, hi + 1, 2)) / math.sqrt(math.pi)
 
 
 def nrefcell_div_ntotal(cfg: RunConfig, k: Kinetic) -> float:
@@ -205,7 +295,9 @@ def plasma(c: float, species, cold_fraction: float, beta_e: float, closure=ISOTH
                            beta1=s["beta1"], T2_T1=s.get("T2_T1", 1.0), scheme=s.get("scheme", FULL_F),
                            initial_weight=s.get("initial_weight", 0.0),
                            marker_temp_ratio=s.get("marker_temp_ratio", 1.0),
-                           psd_refresh_frequency=s.get("psd_refresh_frequency", 0.0)))
+                           psd_refresh_frequency=s.get("psd_refresh_frequency", 0.0),
+                           vdf=s.get("vdf", VDF_BIMAXWELLIAN), losscone_beta=s.get("losscone_beta", 0.0),
+                           zeta=s.get("zeta", 0), vs=s.get("vs", 0.0), nu=s.get("nu", 0.0)))
     cold = []
     if cold_fraction > 0:
         ne += cold_fraction
@@ -323,8 +415,42 @@ def parity_p8() -> RunConfig:
                        xi=0.03)
 
 
+def parity_p9() -> RunConfig:
+    """Delta-f loss-cone H+ (losscone beta 0.3, refreshed at nu = 2) beside a full-f loss-cone He+
+    loaded with hot markers and refreshed, in a mirror field (CAM-CL, reflecting)."""
+    cfg = parity_p7()
+    kin = [dataclasses.replace(k, vdf=VDF_LOSSCONE) for k in cfg.kinetic]
+    kin[0].losscone_beta, kin[0].T2_T1 = 0.3, 1.3 * 3.0
+    kin[1].losscone_beta, kin[1].T2_T1 = 0.6, 1.6 * 1.5
+    return cfg.replace(name="p9_losscone_psd_mirror", kinetic=kin)
+
+
+def parity_p10() -> RunConfig:
+    """Partial-shell species (sin^2 and isotropic shells, vs = 0.5 and 1 thermal speeds) with
+    evolving weights under the predictor-corrector cycle in a mirror field, periodic."""
+    cfg = parity_p7()
+    kin = [dataclasses.replace(k, vdf=VDF_PARTIAL_SHELL) for k in cfg.kinetic]
+    kin[0].zeta, kin[0].vs = 2, 0.5 * kin[0].vth1(cfg.c)
+    kin[1].zeta, kin[1].vs = 0, 1.0 * kin[1].vth1(cfg.c)
+    return cfg.replace(name="p10_pc_shell_psd_mirror", kinetic=kin, algorithm=ALGO_PC, particle_bc=BC_PERIODIC,
+                       xi=0.03)
+
+
+def parity_p11() -> RunConfig:
+    """Counter-beam species (pitch-angle widths 0.5 and 1, vs = 0.3 thermal speeds) with evolving
+    weights in a mirror field (CAM-CL, reflecting)."""
+    cfg = parity_p7()
+    kin = [dataclasses.replace(k, vdf=VDF_COUNTER_BEAM) for k in cfg.kinetic]
+    kin[0].nu, kin[0].vs = 0.5, 0.3 * kin[0].vth1(cfg.c)
+    kin[1].nu, kin[1].vs = 1.0, 0.3 * kin[1].vth1(cfg.c)
+    return cfg.replace(name="p11_counterbeam_psd_mirror", kinetic=kin)
+
+
 PARITY = {f().name: f for f in (parity_p1, parity_p2, parity_p3, parity_p4, parity_p5, parity_p6, parity_p7,
-                                parity_p8)}
+                                parity_p8, parity_p9, parity_p10, parity_p11)}
+# parity cases whose equilibrium needs Dawson's integral, which the reference evaluates with its
+# own implementation: their oracle agrees with the reference to rounding, not bit for bit
+PARITY_ROUNDING = {"p11_counterbeam_psd_mirror"}
 PRESETS = {f().name: f for f in (config1, config2, config3)}
 
 

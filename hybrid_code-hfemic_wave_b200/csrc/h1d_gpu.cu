@@ -170,26 +170,141 @@ void phase_end(h1d_run *r, int kernels)
 // the weights of a species change every step (delta-f, or full-f with PSD refresh)
 bool evolves_psd(h1d_kinetic_desc const &d) { return d.scheme == H1D_DELTA_F || d.psd_refresh_frequency != 0; }
 
-// PartSpecies::populate's cache of the equilibrium moments (PartSpecies.cc:80-87) for the
-// bi-Maxwellian MaxwellianVDF (MaxwellianVDF.h:56-70, .cc:33-43) on the interior half-grid
-// points, times m_moment_weighting_factor as collect_part adds them: n0 (M doubles) then nvv0
-// (6M, {xx, yy, zz, xy, yz, zx}); nV0 = 0; ghost cells zero
+// Dawson's integral F(x) = exp(-x^2) int_0^x exp(t^2) dt for x > 0: its Maclaurin series
+// sum_n (-2x^2)^n x / (2n+1)!! below 0.2, Rybicki's sampling-theorem sum
+// F(x) = pi^-1/2 sum_{n odd} exp(-(x - n h)^2) / n with h = 0.2 (G. B. Rybicki, Computers in
+// Physics 3(2), 85 (1989)) up to 50, and the asymptotic series (1/2x) sum_k (2k-1)!! / (2x^2)^k
+// beyond; relative error below 2e-15 against an independent evaluation.  CounterBeamVDF needs it
+// through B(nu) = 2 nu F(1/nu) (CounterBeamVDF.cc:14-17).
+double dawson(double x)
+{
+    if (x < 0.2) {
+        double t = x, sum = x;
+        for (int n = 1; n < 40 && std::fabs(t) > 1e-18 * sum; ++n)
+            sum += (t *= -2 * x * x / (2 * n + 1));
+        return sum;
+    }
+    if (x > 50) {
+        double const r = 1 / (2 * x * x);
+        double       t = 1, sum = 1;
+        for (int k = 1; k < 12; ++k)
+            sum += (t *= (2 * k - 1) * r);
+        return sum / (2 * x);
+    }
+    constexpr double h    = 0.2, span = 7;
+    long const       lo   = static_cast<long>(std::floor((x - span) / h)) | 1;
+    long const       hi   = static_cast<long>(std::ceil((x + span) / h));
+    double           sum  = 0;
+    for (long n = lo; n <= hi; n += 2) {
+        double const d = x - static_cast<double>(n) * h;
+        sum += std::exp(-d * d) / static_cast<double>(n);
+    }
+    return sum / std::sqrt(M_PI);
+}
+
+// the constants of a species' equilibrium distribution (h1d_kinetic_desc::vdf) that its f0 on the
+// device (equilibrium_f0 / update_weight_f) and its equilibrium moments need; layout of vc as
+// PushArgs::vc
+struct VdfConsts {
+    double vc[4]     = { 0, 0, 0, 0 };
+    double T1_by_vth2 = 0; // partial shell: T_par / vth^2 (PartialShellVDF.cc:19-21)
+    double T_by_vth2  = 0; // counter-beam: T / vth^2 (CounterBeamVDF.cc:30-34)
+};
+// A(xs) = (xs exp(-xs^2) + sqrt(pi) (1/2 + xs^2) erfc(-xs)) / 2, the speed normalisation of the
+// shell distributions, and the second speed moment (1/2A)(xs (5/2 + xs^2) exp(-xs^2) +
+// sqrt(pi) (3/4 + xs^2 (3 + xs^2)) erfc(-xs)) = T / vth^2 (PartialShellVDF.cc:14-22)
+void shell_speed_moments(double xs, double &Ab, double &T_vth2)
+{
+    double const sqrt_pi = 2 / M_2_SQRTPI;
+    Ab     = .5 * (xs * std::exp(-xs * xs) + sqrt_pi * (.5 + xs * xs) * std::erfc(-xs));
+    T_vth2 = .5 / Ab * (xs * (2.5 + xs * xs) * std::exp(-xs * xs) + sqrt_pi * (0.75 + xs * xs * (3 + xs * xs)) * std::erfc(-xs));
+}
+VdfConsts vdf_consts(h1d_kinetic_desc const &d)
+{
+    VdfConsts k;
+    switch (d.vdf) {
+        case H1D_VDF_LOSSCONE: { // LossconeVDF.cc:15-35: beta kept 1e-10 away from 0 and 1
+            double b = d.vdf_param[0];
+            if (b < 1e-10)
+                b = 1e-10;
+            else if (std::fabs(b - 1) < 1e-10)
+                b += std::copysign(1e-10, b - 1);
+            k.vc[0] = b, k.vc[1] = d.T2_T1 / (1 + b), k.vc[2] = b * k.vc[1];
+            break;
+        }
+        case H1D_VDF_PARTIAL_SHELL: { // B(zeta) = sqrt(pi) Gamma(1 + zeta/2) / Gamma(3/2 + zeta/2)
+            double const zeta = d.vdf_param[0], xs = d.vdf_param[1] / d.vth1;
+            double       Ab, T_vth2;
+            shell_speed_moments(xs, Ab, T_vth2);
+            k.vc[0] = zeta, k.vc[1] = xs, k.vc[2] = Ab;
+            k.vc[3] = 2 / M_2_SQRTPI * std::tgamma(1 + .5 * zeta) / std::tgamma(1.5 + .5 * zeta);
+            k.T1_by_vth2 = T_vth2 / (3 + zeta);
+            break;
+        }
+        case H1D_VDF_COUNTER_BEAM: { // B(nu) = 2 nu F(1/nu)
+            double const nu0 = d.vdf_param[0], xs = d.vdf_param[1] / d.vth1;
+            double       Ab, T_vth2;
+            shell_speed_moments(xs, Ab, T_vth2);
+            k.vc[0] = nu0, k.vc[1] = xs, k.vc[2] = Ab, k.vc[3] = 2 * nu0 * dawson(1 / nu0);
+            k.T_by_vth2 = T_vth2;
+            break;
+        }
+        default:
+            break;
+    }
+    return k;
+}
+
+// PartSpecies::populate's cache of the equilibrium moments (PartSpecies.cc:80-87) on the interior
+// half-grid points, times m_moment_weighting_factor as collect_part adds them: n0 (M doubles) then
+// nvv0 (6M, {xx, yy, zz, xy, yz, zx}; mfa_to_cart is the identity on the field line); nV0 = 0;
+// ghost cells zero.  Per distribution (impl_n / impl_nvv):
+//   bi-Maxwellian (MaxwellianVDF.h:56-70, .cc:33-43): n0 = eta, nvv0 = n0 vth1^2/2 {1, T2OT1, T2OT1};
+//   loss-cone (LossconeVDF.h:69-83): n0 = (eta - beta eta_b) / (1 - beta),
+//     nvv0 = n0 vth1^2/2 {1, T, T} with T = (1 + beta(q1)) xth2^2(q1);
+//   partial shell (PartialShellVDF.h:62-76): n0 = cos^zeta, nvv0 = n0 T1 {1, T, T}, T = (2 + zeta)/2;
+//   counter-beam (CounterBeamVDF.h:62-75, .cc:117-133): n0 = B(nu)/B(nu0),
+//     nvv0 = n0 T {T1/T, T2/T, T2/T} with T1/T = nu (1/F(1/nu) - nu)/2, T2/T = (1 - T1/T)/2.
 std::vector<double> equilibrium_moments(h1d_params const &p, h1d_kinetic_desc const &d)
 {
     long const          M = p.Nx + 2 * PAD;
     std::vector<double> eq(7 * M, 0.0);
     double const        q1min = -0.5 * p.Nx + 0.5;
-    double const        hv2   = .5 * (d.vth1 * d.vth1);
+    VdfConsts const     k     = vdf_consts(d);
+    double const        w     = p.moment_weighting;
     for (long i = 0; i < p.Nx; ++i) {
-        double const q1  = static_cast<double>(i) + q1min;
-        double const cs  = std::cos(p.xi * p.Dx * q1);
-        double const eta = 1 / (d.T2_T1 + (1 - d.T2_T1) * cs * cs);
-        double const n0  = 1 * eta, T = d.T2_T1 * eta;
-        double const w   = p.moment_weighting;
-        eq[i + PAD]      = n0 * w;
-        double *e        = eq.data() + M + 6 * (i + PAD);
-        e[0] = ((1 * hv2) * n0) * w, e[1] = ((T * hv2) * n0) * w, e[2] = ((T * hv2) * n0) * w;
-        e[3] = ((0 * hv2) * n0) * w, e[4] = ((0 * hv2) * n0) * w, e[5] = ((0 * hv2) * n0) * w;
+        double const q1 = static_cast<double>(i) + q1min;
+        double const cs = std::cos(p.xi * p.Dx * q1);
+        double       n0, vv[3]; // n0 and the diagonal of nvv0 / n0 in field-aligned components
+        if (d.vdf == H1D_VDF_LOSSCONE) {
+            double const X = k.vc[1], beq = k.vc[0];
+            double const eta   = 1 / (X + (1 - X) * cs * cs);
+            double const eta_b = 1 / (k.vc[2] + (1 - k.vc[2]) * cs * cs);
+            double       beta  = beq * eta_b / eta;
+            if (std::fabs(beta - 1) < 1e-10)
+                beta += std::copysign(1e-10, beta - 1);
+            double const T = (1 + beta) * (X * eta), hv2 = .5 * d.vth1 * d.vth1;
+            n0 = 1 * (eta - beq * eta_b) / (1 - beq);
+            vv[0] = 1 * hv2, vv[1] = T * hv2, vv[2] = T * hv2;
+        } else if (d.vdf == H1D_VDF_PARTIAL_SHELL) {
+            double const zeta = k.vc[0], T = (2 + zeta) / 2, T1 = k.T1_by_vth2 * (d.vth1 * d.vth1);
+            n0 = 1 * (zeta == 0 ? 1 : std::pow(cs, zeta));
+            vv[0] = 1 * T1, vv[1] = T * T1, vv[2] = T * T1;
+        } else if (d.vdf == H1D_VDF_COUNTER_BEAM) {
+            double const nu0 = k.vc[0], nu = nu0 * std::sqrt((1 / cs) * (1 / cs));
+            double const F = dawson(1 / nu), T1OT = 0.5 * nu * (1 / F - nu), T2OT = 0.5 * (1 - T1OT);
+            n0 = 1 * ((2 * nu * F) / k.vc[3]);
+            double const T = k.T_by_vth2 * (d.vth1 * d.vth1);
+            vv[0] = T1OT * T, vv[1] = T2OT * T, vv[2] = T2OT * T;
+        } else {
+            double const eta = 1 / (d.T2_T1 + (1 - d.T2_T1) * cs * cs), hv2 = .5 * (d.vth1 * d.vth1);
+            n0 = 1 * eta;
+            vv[0] = 1 * hv2, vv[1] = (d.T2_T1 * eta) * hv2, vv[2] = (d.T2_T1 * eta) * hv2;
+        }
+        eq[i + PAD] = n0 * w;
+        double *e   = eq.data() + M + 6 * (i + PAD);
+        for (int c = 0; c < 3; ++c)
+            e[c] = (vv[c] * n0) * w, e[c + 3] = (0 * n0) * w;
     }
     return eq;
 }
@@ -233,8 +348,20 @@ int validate(h1d_params const *p, std::string &m)
             BAD("kinetic species %d: smoothing count outside [0, 64]", s);
         if ((d.scheme != H1D_FULL_F && d.scheme != H1D_DELTA_F) || !(d.psd_refresh_frequency >= 0))
             BAD("kinetic species %d: unknown particle scheme or negative psd_refresh_frequency", s);
-        if (evolves_psd(d) && (!(d.vth1 > 0) || !(d.T2_T1 > 0)))
-            BAD("kinetic species %d: evolving weights need the equilibrium vth1 > 0 and T2_T1 > 0", s);
+        if (d.vdf < H1D_VDF_BIMAXWELLIAN || d.vdf > H1D_VDF_COUNTER_BEAM)
+            BAD("kinetic species %d: unknown equilibrium distribution %d", s, d.vdf);
+        if (evolves_psd(d)) {
+            bool const bimax = d.vdf == H1D_VDF_BIMAXWELLIAN || d.vdf == H1D_VDF_LOSSCONE;
+            double const *v  = d.vdf_param;
+            if (!(d.vth1 > 0) || (bimax && !(d.T2_T1 > 0)))
+                BAD("kinetic species %d: evolving weights need the equilibrium vth1 > 0 (and T2_T1 > 0)", s);
+            if (d.vdf == H1D_VDF_LOSSCONE && !(v[0] >= 0))
+                BAD("kinetic species %d: losscone.beta should be non-negative", s);
+            if (d.vdf == H1D_VDF_PARTIAL_SHELL && (!(v[0] >= 0 && v[0] <= 64) || v[0] != std::floor(v[0]) || !(v[1] >= 0)))
+                BAD("kinetic species %d: partial shell zeta should be an integer in [0, 64] and vs non-negative", s);
+            if (d.vdf == H1D_VDF_COUNTER_BEAM && (!(v[0] > 0) || !(v[1] >= 0)))
+                BAD("kinetic species %d: counter-beam nu should be positive and vs non-negative", s);
+        }
     }
     for (int s = 0; s < p->n_cold; ++s)
         if (p->cold[s].Oc == 0 || !(p->cold[s].op > 0) || p->cold[s].n_smooth < 0 || p->cold[s].n_smooth > 64)
@@ -348,6 +475,10 @@ PushArgs push_args(h1d_run *run, int s)
         a.nu_dt = d.psd_refresh_frequency * p.dt, a.psd_refresh = d.psd_refresh_frequency != 0;
         a.delta_f = d.scheme == H1D_DELTA_F;
         a.vth1 = d.vth1, a.vth1_cubed = d.vth1 * d.vth1 * d.vth1, a.T2_T1 = d.T2_T1;
+        VdfConsts const k = vdf_consts(d);
+        a.vdf = d.vdf;
+        for (int j = 0; j < 4; ++j)
+            a.vc[j] = k.vc[j];
     }
     return a;
 }
@@ -376,6 +507,10 @@ PushArgsMixed mixed_args(h1d_run *run, int s, PushArgs const &a)
         m.nu_dt = static_cast<float>(d.psd_refresh_frequency * run->p.dt), m.psd_refresh = d.psd_refresh_frequency != 0;
         m.delta_f = d.scheme == H1D_DELTA_F, m.vth1 = static_cast<float>(d.vth1);
         m.vth1_cubed = static_cast<float>(d.vth1 * d.vth1 * d.vth1), m.T2_T1 = static_cast<float>(d.T2_T1);
+        VdfConsts const k = vdf_consts(d); // push_args fills its copy only for FP64 PSD arrays
+        m.vdf = d.vdf;
+        for (int j = 0; j < 4; ++j)
+            m.vc[j] = static_cast<float>(k.vc[j]);
     }
     return m;
 }

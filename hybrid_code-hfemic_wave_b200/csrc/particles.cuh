@@ -15,6 +15,7 @@
 #pragma once
 
 #include "device_common.cuh"
+#include "h1d_gpu.h"
 #include "tma.cuh"
 
 namespace h1d {
@@ -41,10 +42,12 @@ struct PushArgs {
     int            deposit_mask; // bit0: deposit at x^N, bit1: deposit at the end position
     int            write_back;   // 0 for the PC predictor (particles are not kept)
     // evolving weights (push_kernel<..., PSD = true>): Particle::PSD arrays and the equilibrium
-    // bi-Maxwellian f0 of PartSpecies::impl_update_weight (PartSpecies.cc:178-208)
+    // f0 of PartSpecies::impl_update_weight (PartSpecies.cc:178-208)
     double        *real_f, *marker;
     double         nu_dt;          // psd_refresh_frequency * dt
     double         vth1, vth1_cubed, T2_T1;
+    double         vc[4];          // constants of the distribution `vdf` (equilibrium_f0)
+    int            vdf;            // H1D_VDF_*
     int            psd_refresh;    // nu != 0
     int            delta_f;        // weight = (real_f - f0) / marker, else real_f / marker
 };
@@ -126,16 +129,59 @@ __device__ __forceinline__ d3 background_B(PushArgs const &a, double q1, d3 v, d
     }
 }
 
-// MaxwellianVDF::f0 (VDF/MaxwellianVDF.cc:33-92) at (v, q1): cart_to_mfa is the identity on the
-// field line (MFABasis.h:96-99), eta = n0 = 1 / (T2OT1_eq + (1 - T2OT1_eq) cos^2(xi D1 q1)),
-// T2OT1 = T2OT1_eq eta, f0 = n0 exp(-x1^2) (2/sqrt(pi))/2 exp(-(x2^2 + x3^2)/T2OT1)/(pi T2OT1)/vth1^3
+// The equilibrium f0(v, q1) of a species' distribution (VDF::real_f0), with cs = cos(xi D1 q1).
+// cart_to_mfa is the identity on the field line (MFABasis.h:96-99), so v is field-aligned; every
+// f0 is n0(q1) times a velocity distribution normalised to one.
+//  - bi-Maxwellian (MaxwellianVDF.cc:33-92): n0 = eta = 1 / (T + (1 - T) cs^2), T = T2OT1_eq
+//    (T2_T1), T2OT1 = T eta; f0 = n0 exp(-x1^2) pi^-1/2 exp(-x_perp^2 / T2OT1) / (pi T2OT1) / vth1^3,
+//    x = v / vth1.
+//  - loss-cone (LossconeVDF.cc:44-117): vc = {beta_eq, X = xth2_eq^2, beta_eq X}; eta as above with
+//    X, eta_b with beta_eq X, n0 = (eta - beta_eq eta_b) / (1 - beta_eq), xth2^2 = X eta,
+//    beta = beta_eq eta_b / eta (kept 1e-10 away from 1); the perpendicular factor is
+//    (exp(-y) - exp(-y / beta)) / (pi xth2^2 (1 - beta)) with y = x_perp^2 / xth2^2.
+//  - partial shell (PartialShellVDF.cc:96-145): vc = {zeta, xs, A(xs), B(zeta)}; n0 = cs^zeta;
+//    f0 = n0 exp(-(x - xs)^2) / A sin^zeta(alpha) / B / (2 pi vth^3), x = |v| / vth,
+//    cos(alpha) = x1 / x.
+//  - counter-beam (CounterBeamVDF.cc:134-178): vc = {nu0, xs, A(xs), B(nu0)}; nu = nu0 / cs
+//    (B/B0 = 1/cs^2), n0 = B(nu) / B(nu0) and the pitch-angle factor
+//    exp(-sin^2(alpha) / nu^2) / B(nu): their product needs no B(nu), so
+//    f0 = exp(-(x - xs)^2) / A exp(-sin^2(alpha) cs^2 / nu0^2) / B(nu0) / (2 pi vth^3).
 __device__ __forceinline__ double equilibrium_f0(PushArgs const &a, d3 v, double cs)
 {
+    constexpr double PI = 3.141592653589793, HALF_2_SQRTPI = 1.1283791670955126 * .5;
+    double const     x1 = v.x / a.vth1, x2 = v.y / a.vth1, x3 = v.z / a.vth1;
+    if (a.vdf == H1D_VDF_LOSSCONE) {
+        double const X = a.vc[1], bX = a.vc[2], beq = a.vc[0];
+        double const eta   = 1 / (X + (1 - X) * cs * cs);
+        double const eta_b = 1 / (bX + (1 - bX) * cs * cs);
+        double       beta  = beq * eta_b / eta;
+        if (fabs(beta - 1) < 1e-10)
+            beta += copysign(1e-10, beta - 1);
+        double const n0 = (eta - beq * eta_b) / (1 - beq);
+        double const x2s = X * eta;
+        double const y   = (x2 * x2 + x3 * x3) / x2s;
+        double const f1  = exp(-x1 * x1) * HALF_2_SQRTPI;
+        double const f2  = (exp(-y) - exp(-y / beta)) / (PI * x2s * (1 - beta));
+        return n0 * ((f1 * f2) / a.vth1_cubed);
+    }
+    if (a.vdf == H1D_VDF_PARTIAL_SHELL || a.vdf == H1D_VDF_COUNTER_BEAM) {
+        double const x  = sqrt(x1 * x1 + x2 * x2 + x3 * x3);
+        double const t  = x - a.vc[1];
+        double const fv = exp(-t * t) / a.vc[2];
+        double const u  = x1 / x; // cos(alpha)
+        if (a.vdf == H1D_VDF_PARTIAL_SHELL) {
+            bool const   iso = a.vc[0] == 0;
+            double const fa  = (iso ? 1 : pow((1 - u) * (1 + u), .5 * a.vc[0])) / a.vc[3];
+            double const n0  = iso ? 1 : pow(cs, a.vc[0]);
+            return n0 * (.5 * fv * fa / (PI * a.vth1_cubed));
+        }
+        double const fa = exp(-((1 - u) * (1 + u)) * (cs * cs) / (a.vc[0] * a.vc[0])) / a.vc[3];
+        return fv * fa / (2 * PI * a.vth1_cubed);
+    }
     double const eta   = 1 / (a.T2_T1 + (1 - a.T2_T1) * cs * cs);
     double const T2OT1 = a.T2_T1 * eta;
-    double const x1 = v.x / a.vth1, x2 = v.y / a.vth1, x3 = v.z / a.vth1;
-    double const f1 = exp(-x1 * x1) * 1.1283791670955126 * .5;
-    double const f2 = exp(-(x2 * x2 + x3 * x3) / T2OT1) / (3.141592653589793 * T2OT1);
+    double const f1    = exp(-x1 * x1) * HALF_2_SQRTPI;
+    double const f2    = exp(-(x2 * x2 + x3 * x3) / T2OT1) / (PI * T2OT1);
     return (1 * eta) * ((f1 * f2) / a.vth1_cubed);
 }
 // PartSpecies::impl_update_weight for one particle after its velocity update: the new weight,

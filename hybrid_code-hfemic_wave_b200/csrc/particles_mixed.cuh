@@ -27,10 +27,11 @@ struct PushArgsMixed {
     int          species, randomize;
     int          move_steps, deposit_mask, write_back;
     // evolving weights (push_kernel_mixed<..., PSD = true>): FP32 Particle::PSD arrays and the
-    // equilibrium bi-Maxwellian of PartSpecies::impl_update_weight, as in PushArgs
+    // equilibrium distribution of PartSpecies::impl_update_weight, as in PushArgs
     float       *real_f, *marker;
     float        nu_dt, vth1, vth1_cubed, T2_T1;
-    int          psd_refresh, delta_f;
+    float        vc[4];
+    int          vdf, psd_refresh, delta_f;
 };
 
 struct f3 {
@@ -232,16 +233,45 @@ static_assert(2 * PIPE_STAGES_MIXED * sizeof(uint64_t) <= 128, "barriers fit bef
 static_assert(PIPE_CTAS_PER_SM_MIXED * (PIPE_SMEM_MIXED_PSD + 1024) <= 233472, "four CTAs with evolving weights fit an SM");
 
 // PartSpecies::impl_update_weight in FP32 for one particle after its velocity update (as
-// update_weight, particles.cuh): f0 of the equilibrium bi-Maxwellian at velocity v and at the
-// push position (c2 = cos^2(xi D1 q1)), then real_f and the weight
+// update_weight and equilibrium_f0, particles.cuh): f0 of the equilibrium distribution at velocity
+// v and at the push position (c2 = cos^2(xi D1 q1)), then real_f and the weight
 __device__ __forceinline__ float update_weight_f(PushArgsMixed const &a, f3 v, float c2, float &real_f, float marker)
 {
-    float const eta   = 1.0f / (a.T2_T1 + (1.0f - a.T2_T1) * c2);
-    float const T2OT1 = a.T2_T1 * eta;
-    float const x1 = v.x / a.vth1, x2 = v.y / a.vth1, x3 = v.z / a.vth1;
-    float const f1 = expf(-x1 * x1) * 0.5641895835477563f;
-    float const f2 = expf(-(x2 * x2 + x3 * x3) / T2OT1) / (3.14159265358979f * T2OT1);
-    float const f0 = eta * ((f1 * f2) / a.vth1_cubed);
+    constexpr float PI = 3.14159265358979f, INV_SQRTPI = 0.5641895835477563f;
+    float const     x1 = v.x / a.vth1, x2 = v.y / a.vth1, x3 = v.z / a.vth1;
+    float           f0;
+    if (a.vdf == H1D_VDF_LOSSCONE) {
+        float const X = a.vc[1], bX = a.vc[2], beq = a.vc[0];
+        float const eta   = 1.0f / (X + (1.0f - X) * c2);
+        float const eta_b = 1.0f / (bX + (1.0f - bX) * c2);
+        float       beta  = beq * eta_b / eta;
+        if (fabsf(beta - 1.0f) < 1e-6f) // beta = 1 is a removable singularity; FP32 resolves 1e-6
+            beta = beta < 1.0f ? 1.0f - 1e-6f : 1.0f + 1e-6f;
+        float const x2s = X * eta;
+        float const y   = (x2 * x2 + x3 * x3) / x2s;
+        float const f2  = (expf(-y) - expf(-y / beta)) / (PI * x2s * (1.0f - beta));
+        f0 = ((eta - beq * eta_b) / (1.0f - beq)) * ((expf(-x1 * x1) * INV_SQRTPI * f2) / a.vth1_cubed);
+    } else if (a.vdf == H1D_VDF_PARTIAL_SHELL || a.vdf == H1D_VDF_COUNTER_BEAM) {
+        float const x  = sqrtf(x1 * x1 + x2 * x2 + x3 * x3);
+        float const t  = x - a.vc[1];
+        float const fv = expf(-t * t) / a.vc[2];
+        float const u  = x1 / x;
+        float const s2 = (1.0f - u) * (1.0f + u); // sin^2(alpha)
+        if (a.vdf == H1D_VDF_PARTIAL_SHELL) {
+            bool const iso = a.vc[0] == 0.0f;
+            // sin^zeta(alpha) cs^zeta = (s2 c2)^(zeta/2)
+            float const fa = iso ? 1.0f : powf(s2 * c2, 0.5f * a.vc[0]);
+            f0 = 0.5f * fv * fa / (a.vc[3] * PI * a.vth1_cubed);
+        } else {
+            f0 = fv * expf(-s2 * c2 / (a.vc[0] * a.vc[0])) / (a.vc[3] * 2.0f * PI * a.vth1_cubed);
+        }
+    } else {
+        float const eta   = 1.0f / (a.T2_T1 + (1.0f - a.T2_T1) * c2);
+        float const T2OT1 = a.T2_T1 * eta;
+        float const f1    = expf(-x1 * x1) * INV_SQRTPI;
+        float const f2    = expf(-(x2 * x2 + x3 * x3) / T2OT1) / (PI * T2OT1);
+        f0 = eta * ((f1 * f2) / a.vth1_cubed);
+    }
     if (a.psd_refresh)
         real_f = (real_f + a.nu_dt * f0) / (1.0f + a.nu_dt);
     return a.delta_f ? (real_f - f0) / marker : real_f / marker;

@@ -51,7 +51,7 @@
 extern "C" {
 #endif
 
-#define H1D_ABI_VERSION 3
+#define H1D_ABI_VERSION 4
 
 /* number of ghost cells on each side; Input::number_of_ghost_cells (Include/Inputs.h:22) */
 #define H1D_PAD 3
@@ -85,8 +85,17 @@ enum { H1D_PREC_FP64 = 0, H1D_PREC_MIXED = 1 };
 #define H1D_FULL_F  0
 #define H1D_DELTA_F 1
 
-/* KineticPlasmaDesc (LibPIC/PIC/PlasmaDesc.h:118-177) of a bi-Maxwellian species
- * (BiMaxPlasmaDesc, PlasmaDesc.h:207-236) */
+/* the equilibrium distribution of a kinetic species (the alternatives of VDFVariant,
+ * LibPIC/PIC/VDFVariant.h): its f0 and its moments n0, nV0 = 0, nvv0 enter the step only when the
+ * species' weights evolve (delta-f or PSD refresh) */
+#define H1D_VDF_BIMAXWELLIAN  0 /* MaxwellianVDF (VDF/MaxwellianVDF.cc), BiMaxPlasmaDesc */
+#define H1D_VDF_LOSSCONE      1 /* LossconeVDF (VDF/LossconeVDF.cc), LossconePlasmaDesc */
+#define H1D_VDF_PARTIAL_SHELL 2 /* PartialShellVDF (VDF/PartialShellVDF.cc), PartialShellPlasmaDesc */
+#define H1D_VDF_COUNTER_BEAM  3 /* CounterBeamVDF (VDF/CounterBeamVDF.cc), CounterBeamPlasmaDesc */
+
+/* KineticPlasmaDesc (LibPIC/PIC/PlasmaDesc.h:118-177) with the parameters of its equilibrium
+ * distribution (BiMaxPlasmaDesc, LossconePlasmaDesc, PartialShellPlasmaDesc, CounterBeamPlasmaDesc:
+ * PlasmaDesc.h:207-345) */
 typedef struct h1d_kinetic_desc {
     double  Oc;          /* PlasmaDesc::Oc, signed cyclotron frequency */
     double  op;          /* PlasmaDesc::op, plasma frequency */
@@ -99,15 +108,23 @@ typedef struct h1d_kinetic_desc {
     /* Phase-space density weighting.  With scheme H1D_DELTA_F, or a nonzero psd_refresh_frequency,
      * every particle carries its physical density real_f and marker density marker
      * (Particle::PSD, LibPIC/PIC/Particle.h:26-34; h1d_upload_psd) and its weight is recomputed
-     * every step from the equilibrium bi-Maxwellian f0 (vth1, T2_T1) at its new velocity
+     * every step from the equilibrium f0 of the species' distribution `vdf` at its new velocity
      * (PartSpecies::impl_update_weight, Core/PartSpecies.cc:178-208); delta-f moments add the
-     * equilibrium moments n0, nV0 = 0, nvv0 (PartSpecies.cc:115-143). */
+     * equilibrium moments n0, nV0 = 0, nvv0 (PartSpecies.cc:115-143).  The fields below the
+     * scheme are read only for such species. */
     int32_t scheme;                /* H1D_FULL_F or H1D_DELTA_F (KineticPlasmaDesc::scheme) */
-    int32_t reserved;
+    int32_t vdf;                   /* H1D_VDF_*; 0 (bi-Maxwellian) in a zero-initialised desc */
     double  psd_refresh_frequency; /* KineticPlasmaDesc::psd_refresh_frequency (>= 0) */
-    double  vth1;                  /* equilibrium parallel thermal speed, sqrt(beta1) c |Oc| / op
-                                      (MaxwellianVDF.cc:24); used when the weights evolve */
-    double  T2_T1;                 /* equilibrium T_perp / T_par at the equator */
+    double  vth1;                  /* thermal speed sqrt(beta) c |Oc| / op of the distribution: beta1
+                                      (bi-Maxwellian, loss-cone: MaxwellianVDF.cc:24, LossconeVDF.cc:32)
+                                      or the thermal spread beta (partial shell, counter-beam:
+                                      PartialShellVDF.cc:27, CounterBeamVDF.cc:40) */
+    double  T2_T1;                 /* bi-Maxwellian, loss-cone: BiMaxPlasmaDesc::T2_T1 at the
+                                      equator (for a LossconePlasmaDesc built from a vth_ratio,
+                                      (1 + beta) vth_ratio, PlasmaDesc.h:254); others: unused */
+    double  vdf_param[3];          /* loss-cone: {losscone.beta, -, -};
+                                      partial shell: {zeta (a non-negative integer), vs, -};
+                                      counter-beam: {nu, vs, -}; bi-Maxwellian: unused */
 } h1d_kinetic_desc;
 
 /* ColdPlasmaDesc (PlasmaDesc.h:92-114) */

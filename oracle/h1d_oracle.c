@@ -10,7 +10,7 @@
  *   Domain::collect_smooth                                          (Core/Domain.hh:155-194)
  *   PartSpecies::update_vel/update_pos/collect_part/collect_all     (Core/PartSpecies.cc:132-139, 210-349)
  *   PartSpecies::impl_update_weight, equilibrium moments            (Core/PartSpecies.cc:80-87, 115-143, 178-208;
- *                                                                    VDF/MaxwellianVDF.cc:33-92, .h:56-70)
+ *                                                                    VDF/{Maxwellian,Losscone,PartialShell,CounterBeam}VDF)
  *   ColdSpecies::update_vel/collect_part/collect_all                (Core/ColdSpecies.cc:251-297)
  *   BField::update, EField::update, Charge/Current/Lambda/Gamma     (Core/BField.cc:74-124, EField.cc:224-330,
  *                                                                    Charge.cc:70-80, Current.cc:165-188)
@@ -461,23 +461,150 @@ static void update_velocity(orc_run *R, Bucket *b, h1d_kinetic_desc const *d, do
     if (evolves_psd(d))
         update_weight(R, b, d, dt);
 }
-/* MaxwellianVDF (VDF/MaxwellianVDF.cc:33-92) of the equilibrium a species' weights refer to:
- * eta = n0 / n0_eq, T2OT1(pos) and the physical distribution f0(vel, pos) */
-static double vdf_eta(orc_run const *R, h1d_kinetic_desc const *d, double q1)
+/* The equilibrium distribution a species' weights refer to (h1d_kinetic_desc::vdf): n0(q1), the
+ * diagonal of nvv0(q1) (field-aligned = Cartesian on the axis) and the physical f0(vel, q1).
+ *   MaxwellianVDF    (VDF/MaxwellianVDF.cc:33-92, .h:56-70)
+ *   LossconeVDF      (VDF/LossconeVDF.cc:15-117, .h:69-83)
+ *   PartialShellVDF  (VDF/PartialShellVDF.cc:14-145, .h:62-76)
+ *   CounterBeamVDF   (VDF/CounterBeamVDF.cc:14-178, .h:62-75) */
+
+/* Dawson's integral F(x), x > 0 (CounterBeamVDF's B(nu) = 2 nu F(1/nu)); the reference evaluates it
+ * with the Faddeeva package (Misc/Faddeeva.cc).  Here: Maclaurin series below 0.2, Rybicki's
+ * sampling-theorem sum pi^-1/2 sum_{n odd} exp(-(x - n h)^2)/n with h = 0.2 up to 50 (G. B. Rybicki,
+ * Computers in Physics 3(2), 85 (1989)), the asymptotic series beyond; relative error < 2e-15. */
+static double orc_dawson(double x)
 {
-    double const cs = cos(R->xi * R->D1 * q1);
-    return 1 / (d->T2_T1 + (1 - d->T2_T1) * cs * cs);
+    if (x < 0.2) {
+        double t = x, sum = x;
+        for (int n = 1; n < 40; ++n)
+            sum += (t *= -2 * x * x / (2 * n + 1));
+        return sum;
+    }
+    if (x > 50) {
+        double const r = 1 / (2 * x * x);
+        double       t = 1, sum = 1;
+        for (int k = 1; k < 12; ++k)
+            sum += (t *= (2 * k - 1) * r);
+        return sum / (2 * x);
+    }
+    long const lo  = (long)floor((x - 7) / 0.2) | 1, hi = (long)ceil((x + 7) / 0.2);
+    double     sum = 0;
+    for (long n = lo; n <= hi; n += 2)
+        sum += exp(-(x - (double)n * 0.2) * (x - (double)n * 0.2)) / (double)n;
+    return sum / sqrt(M_PI);
+}
+static double bnu(double nu) { return 2 * nu * orc_dawson(1 / nu); }
+
+/* loss-cone beta kept 1e-10 away from 0 and 1 (LossconeVDF.cc:25-30, 68-76) */
+static double lc_nudge(double beta) { return fabs(beta - 1) < 1e-10 ? beta + copysign(1e-10, beta - 1) : beta; }
+static double lc_beta_eq(h1d_kinetic_desc const *d) { return d->vdf_param[0] < 1e-10 ? 1e-10 : lc_nudge(d->vdf_param[0]); }
+
+/* speed normalisation A(xs) and T / vth^2 of the shell distributions (PartialShellVDF.cc:14-22,
+ * CounterBeamVDF.cc:19-35) */
+static void shell_params(double xs, double *Ab, double *T_vth2)
+{
+    *Ab     = .5 * (xs * exp(-xs * xs) + 2 / M_2_SQRTPI * (.5 + xs * xs) * erfc(-xs));
+    *T_vth2 = .5 / *Ab * (xs * (2.5 + xs * xs) * exp(-xs * xs) + 2 / M_2_SQRTPI * (0.75 + xs * xs * (3 + xs * xs)) * erfc(-xs));
+}
+
+static double vdf_cos(orc_run const *R, double q1) { return cos(R->xi * R->D1 * q1); }
+/* n0(q1) and, when vv is given, the diagonal of nvv0(q1) */
+static double vdf_n0(orc_run const *R, h1d_kinetic_desc const *d, double q1, double vv[3])
+{
+    double const cs = vdf_cos(R, q1);
+    switch (d->vdf) {
+        case H1D_VDF_LOSSCONE: {
+            double const beq   = lc_beta_eq(d), X = d->T2_T1 / (1 + beq);
+            double const eta   = 1 / (X + (1 - X) * cs * cs);
+            double const tmp   = beq * X;
+            double const eta_b = 1 / (tmp + (1 - tmp) * cs * cs);
+            double const n0    = 1 * (eta - beq * eta_b) / (1 - beq);
+            if (vv) {
+                double const T2OT1 = (1 + lc_nudge(beq * eta_b / eta)) * (X * eta);
+                double const h     = .5 * d->vth1 * d->vth1;
+                vv[0] = (1 * h) * n0, vv[1] = (T2OT1 * h) * n0, vv[2] = (T2OT1 * h) * n0;
+            }
+            return n0;
+        }
+        case H1D_VDF_PARTIAL_SHELL: {
+            long const   zeta = (long)d->vdf_param[0];
+            double const n0   = 1 * (zeta == 0 ? 1 : pow(cs, (double)zeta));
+            if (vv) {
+                double Ab, T_vth2;
+                shell_params(d->vdf_param[1] / d->vth1, &Ab, &T_vth2);
+                double const T1    = T_vth2 / (double)(3 + zeta) * (d->vth1 * d->vth1);
+                double const T2OT1 = (double)(2 + zeta) / 2;
+                vv[0] = (1 * T1) * n0, vv[1] = (T2OT1 * T1) * n0, vv[2] = (T2OT1 * T1) * n0;
+            }
+            return n0;
+        }
+        case H1D_VDF_COUNTER_BEAM: {
+            double const nu0 = d->vdf_param[0], nu = nu0 * sqrt((1 / cs) * (1 / cs));
+            double const n0  = 1 * (bnu(nu) / bnu(nu0));
+            if (vv) {
+                double Ab, T_vth2;
+                shell_params(d->vdf_param[1] / d->vth1, &Ab, &T_vth2);
+                double const T1OT = 0.5 * nu * (1 / orc_dawson(1 / nu) - nu), T2OT = 0.5 * (1 - T1OT);
+                double const nT   = n0 * T_vth2 * (d->vth1 * d->vth1);
+                vv[0] = T1OT * nT, vv[1] = T2OT * nT, vv[2] = T2OT * nT;
+            }
+            return n0;
+        }
+        default: {
+            double const eta = 1 / (d->T2_T1 + (1 - d->T2_T1) * cs * cs);
+            if (vv) {
+                double const T = d->T2_T1 * eta, hv2 = .5 * (d->vth1 * d->vth1);
+                vv[0] = (1 * hv2) * eta, vv[1] = (T * hv2) * eta, vv[2] = (T * hv2) * eta;
+            }
+            return 1 * eta;
+        }
+    }
 }
 static double vdf_f0(orc_run const *R, h1d_kinetic_desc const *d, V3 v, double q1)
 {
-    double const eta   = vdf_eta(R, d, q1);
-    double const T2OT1 = d->T2_T1 * eta;
-    double const vth1  = d->vth1;
+    double const vth1 = d->vth1, vth1_cubed = vth1 * vth1 * vth1;
     double const x1 = v.x / vth1, x2 = v.y / vth1, x3 = v.z / vth1; /* cart_to_mfa is the identity on the axis */
-    double const f1 = exp(-x1 * x1) * M_2_SQRTPI * .5;
-    double const xx = x2 * x2 + x3 * x3;
-    double const f2 = exp(-xx / T2OT1) / (M_PI * T2OT1);
-    return (1 * eta) * ((f1 * f2) / (vth1 * vth1 * vth1));
+    double const n0 = vdf_n0(R, d, q1, NULL);
+    double const cs = vdf_cos(R, q1);
+    switch (d->vdf) {
+        case H1D_VDF_LOSSCONE: {
+            double const beq   = lc_beta_eq(d), X = d->T2_T1 / (1 + beq);
+            double const eta   = 1 / (X + (1 - X) * cs * cs);
+            double const tmp   = beq * X;
+            double const eta_b = 1 / (tmp + (1 - tmp) * cs * cs);
+            double const beta  = lc_nudge(beq * eta_b / eta);
+            double const xth2  = X * eta;
+            double const f1    = exp(-x1 * x1) * M_2_SQRTPI * .5;
+            double const y     = (x2 * x2 + x3 * x3) / xth2;
+            double const f2    = ((1 - 0 * beta) * exp(-y) - (1 - 0) * exp(-y / beta)) / (M_PI * xth2 * (1 - beta));
+            return n0 * ((f1 * f2) / vth1_cubed);
+        }
+        case H1D_VDF_PARTIAL_SHELL:
+        case H1D_VDF_COUNTER_BEAM: {
+            double Ab, T_vth2;
+            shell_params(d->vdf_param[1] / vth1, &Ab, &T_vth2);
+            double const x  = sqrt(x1 * x1 + x2 * x2 + x3 * x3);
+            double const t  = x - d->vdf_param[1] / vth1;
+            double const fv = exp(-t * t) / Ab;
+            double const u  = x1 / x;
+            if (d->vdf == H1D_VDF_PARTIAL_SHELL) {
+                long const   zeta = (long)d->vdf_param[0];
+                double const Bz   = 2 / M_2_SQRTPI * tgamma(1 + .5 * (double)zeta) / tgamma(1.5 + .5 * (double)zeta);
+                double const fa   = (zeta == 0 ? 1 : pow((1 - u) * (1 + u), .5 * (double)zeta)) / Bz;
+                return n0 * (.5 * fv * fa / (M_PI * vth1_cubed));
+            }
+            double const nu = d->vdf_param[0] * sqrt((1 / cs) * (1 / cs));
+            double const fa = exp(-((1 - u) * (1 + u)) / (nu * nu)) / bnu(nu);
+            return n0 * (fv * fa / (2 * M_PI * vth1_cubed));
+        }
+        default: {
+            double const T2OT1 = d->T2_T1 * n0;
+            double const f1    = exp(-x1 * x1) * M_2_SQRTPI * .5;
+            double const xx    = x2 * x2 + x3 * x3;
+            double const f2    = exp(-xx / T2OT1) / (M_PI * T2OT1);
+            return n0 * ((f1 * f2) / vth1_cubed);
+        }
+    }
 }
 static int evolves_psd(h1d_kinetic_desc const *d) { return d->scheme == H1D_DELTA_F || d->psd_refresh_frequency != 0; }
 
@@ -506,21 +633,17 @@ static void update_weight(orc_run const *R, Bucket *b, h1d_kinetic_desc const *d
 }
 
 /* the equilibrium moments cached by PartSpecies::populate (PartSpecies.cc:80-87) at the interior
- * half-grid points; ghost cells stay zero (MaxwellianVDF.h:56-70) */
+ * half-grid points; ghost cells stay zero */
 static void cache_equilibrium(orc_run *R, int s)
 {
     h1d_kinetic_desc const *d = &R->p.kinetic[s];
     double const            q1min = R->half_min;
-    double const            hv2   = .5 * (d->vth1 * d->vth1);
     for (long i = 0; i < R->Nx; ++i) {
-        double const q1  = (double)i + q1min;
-        double const eta = vdf_eta(R, d, q1);
-        double const n0  = 1 * eta;
-        double const T   = d->T2_T1 * eta;
-        *at1(R->eq0[s], i) = n0;
+        double const q1 = (double)i + q1min;
+        double       vv[3];
+        *at1(R->eq0[s], i) = vdf_n0(R, d, q1, vv);
         double *e = at6(R->eq2[s], i);
-        e[0] = (1 * hv2) * n0, e[1] = (T * hv2) * n0, e[2] = (T * hv2) * n0;
-        e[3] = (0 * hv2) * n0, e[4] = (0 * hv2) * n0, e[5] = (0 * hv2) * n0;
+        e[0] = vv[0], e[1] = vv[1], e[2] = vv[2], e[3] = 0, e[4] = 0, e[5] = 0;
     }
 }
 /* delta-f: moments += equilibrium * m_moment_weighting_factor (PartSpecies.cc:115-143), over all
@@ -1211,8 +1334,12 @@ static int check_params(h1d_params const *p, char *msg, size_t cap)
             BAD("kinetic species %d: negative smoothing count", s);
         if ((d->scheme != H1D_FULL_F && d->scheme != H1D_DELTA_F) || !(d->psd_refresh_frequency >= 0))
             BAD("kinetic species %d: unknown particle scheme or negative psd_refresh_frequency", s);
-        if ((d->scheme == H1D_DELTA_F || d->psd_refresh_frequency != 0) && (!(d->vth1 > 0) || !(d->T2_T1 > 0)))
-            BAD("kinetic species %d: evolving weights need the equilibrium vth1 > 0 and T2_T1 > 0", s);
+        if (d->vdf < H1D_VDF_BIMAXWELLIAN || d->vdf > H1D_VDF_COUNTER_BEAM)
+            BAD("kinetic species %d: unknown equilibrium distribution", s);
+        if ((d->scheme == H1D_DELTA_F || d->psd_refresh_frequency != 0)
+            && (!(d->vth1 > 0) || ((d->vdf == H1D_VDF_BIMAXWELLIAN || d->vdf == H1D_VDF_LOSSCONE) && !(d->T2_T1 > 0))
+                || (d->vdf == H1D_VDF_COUNTER_BEAM && !(d->vdf_param[0] > 0))))
+            BAD("kinetic species %d: evolving weights need the equilibrium vth1 > 0 (and T2_T1 > 0, nu > 0)", s);
     }
     for (int s = 0; s < p->n_cold; ++s)
         if (p->cold[s].Oc == 0 || !(p->cold[s].op > 0) || p->cold[s].n_smooth < 0)

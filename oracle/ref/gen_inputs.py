@@ -45,9 +45,17 @@ def render(cfg) -> str:
     closure = "isothermal" if cfg.efluid.closure == C.ISOTHERMAL else "adiabatic"
     def kdesc(k):
         scheme = "delta_f" if k.scheme == C.DELTA_F else "full_f"
-        return (f"BiMaxPlasmaDesc({{ {{ {r(k.Oc)}, {r(k.op)}, {k.n_smooth} }}, {k.Nc}, {SHAPE[k.shape_order]}, "
+        base = (f"{{ {{ {r(k.Oc)}, {r(k.op)}, {k.n_smooth} }}, {k.Nc}, {SHAPE[k.shape_order]}, "
                 f"{r(float(k.psd_refresh_frequency))}, {scheme}, {r(float(k.initial_weight))}, "
-                f"{r(float(k.marker_temp_ratio))} }}, {r(k.beta1)}, {r(k.T2_T1)})")
+                f"{r(float(k.marker_temp_ratio))} }}")
+        bimax = f"BiMaxPlasmaDesc({base}, {r(k.beta1)}, {r(k.T2_T1)})"
+        if k.vdf == C.VDF_LOSSCONE:  # PlasmaDesc.h:244-250
+            return f"LossconePlasmaDesc({{ {r(k.losscone_beta)} }}, {bimax})"
+        if k.vdf == C.VDF_PARTIAL_SHELL:  # PlasmaDesc.h:290-305
+            return f"PartialShellPlasmaDesc(KineticPlasmaDesc{base}, {r(k.beta1)}, {int(k.zeta)}U, {r(k.vs)})"
+        if k.vdf == C.VDF_COUNTER_BEAM:  # PlasmaDesc.h:326-340
+            return f"CounterBeamPlasmaDesc(KineticPlasmaDesc{base}, {r(k.beta1)}, {r(k.nu)}, {r(k.vs)})"
+        return bimax
 
     kin = ",\n        ".join(kdesc(k) for k in cfg.kinetic)
     cold = ",\n        ".join(f"ColdPlasmaDesc({{ {r(c.Oc)}, {r(c.op)}, {c.n_smooth} }})" for c in cfg.cold)

@@ -3,8 +3,9 @@
 Builds the reference hot path (oracle/Makefile ``ref`` target: the unmodified
 src/hybrid_1d/Core and src/LibPIC sources of kyungguk1/hybrid_code-hfemic_wave compiled in
 place, one binary per configuration) and, for every parity configuration, writes
-    <name>.init.bin    particles from the reference's own loader (PartSpecies::populate,
-                       MaxwellianVDF::load) and the initial fields
+    <name>.init.bin    particles from the reference's own loader (PartSpecies::populate with
+                       the species' VDF: Maxwellian, loss-cone, partial shell or counter-beam)
+                       and the initial fields
     <name>.step1.bin   after Domain::advance_by(1)
     <name>.step10.bin  after Domain::advance_by(10) from the same initial state
 into tests/golden/.  Needs the reference tree (default /root/reference, or $H1D_REFERENCE).
@@ -21,7 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 NAMES = ["p1_cic_periodic", "p2_tsc_mirror_reflecting", "p3_o3_adiabatic_periodic",
          "p4_pc_tsc_mirror_reflecting", "p5_tsc_mirror_source", "p6_pc_source", "p7_psd_tsc_mirror_reflecting",
-         "p8_pc_psd_periodic"]
+         "p8_pc_psd_periodic", "p9_losscone_psd_mirror", "p10_pc_shell_psd_mirror", "p11_counterbeam_psd_mirror"]
 
 
 def main():

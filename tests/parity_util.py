@@ -1,5 +1,15 @@
 """Comparison helpers shared by the GPU parity tests."""
+import dataclasses
+
 import numpy as np
+
+
+def with_reference_norms(cfg, init):
+    """``cfg`` with every kinetic species' moment normalisation (PartSpecies::Nc) taken from the
+    header of a reference state file, as an integration of the reference passes it to the C ABI;
+    the reference integrates the counter-beam density numerically (VDFHelper.h:43-64)."""
+    kin = [dataclasses.replace(k, norm=float(n)) for k, n in zip(cfg.kinetic, init["moment_norm"])]
+    return cfg.replace(kinetic=kin)
 
 
 def rel_err(a, b):

@@ -13,7 +13,7 @@ import os
 
 import numpy as np
 import pytest
-from parity_util import by_pid, cell_keys, cell_mismatches, rel_err, state_errors
+from parity_util import by_pid, cell_keys, cell_mismatches, rel_err, state_errors, with_reference_norms
 from state_io import read_state
 
 import hfemic_b200 as h
@@ -65,8 +65,8 @@ def test_ten_steps(name, gpu_lib, oracle_lib):
 @pytest.mark.parametrize("name", ALL)
 def test_against_reference_fixture(name, gpu_lib):
     """The GPU path against the reference's own output after ten steps (golden fixture)."""
-    cfg = h.configs.PARITY[name]()
     init = read_state(os.path.join(GOLDEN, f"{name}.init.bin"))
+    cfg = with_reference_norms(h.configs.PARITY[name](), init)
     ref = read_state(os.path.join(GOLDEN, f"{name}.step10.bin"))
     with h.Run(cfg, gpu_lib, "h1d_") as g:
         g.upload_state(init)
@@ -149,6 +149,16 @@ def test_invalid_params(gpu_lib):
     handle = ctypes.c_void_p()
     assert fn["create"](ctypes.byref(p), ctypes.byref(handle)) == h.abi.ERR_INVALID_ARG
     assert not handle.value
+    # equilibrium distributions of evolving weights: unknown kind, out-of-range parameters
+    C = h.configs
+    for kind, param in ((7, (0, 0, 0)), (C.VDF_LOSSCONE, (-0.1, 0, 0)), (C.VDF_PARTIAL_SHELL, (1.5, 0, 0)),
+                        (C.VDF_PARTIAL_SHELL, (2, -1, 0)), (C.VDF_COUNTER_BEAM, (0, 0, 0))):
+        p = h.abi.make_params(C.parity_p7())
+        p.kinetic[0].vdf = kind
+        for j in range(3):
+            p.kinetic[0].vdf_param[j] = param[j]
+        assert fn["create"](ctypes.byref(p), ctypes.byref(handle)) == h.abi.ERR_INVALID_ARG, (kind, param)
+        assert not handle.value
 
 
 def test_device_rounding_and_trig(gpu_lib):

@@ -4,28 +4,31 @@ moments (PartSpecies.cc:115-143), against the oracle and the reference's own fix
 
 p7 (CAM-CL, mirror, reflecting) holds a delta-f species with refresh beside a full-f species
 loaded with hot markers (weights f0/g0) and refreshed; p8 is the predictor-corrector variant with
-a delta-f species without refresh.  Tolerances: as test_gpu_parity.py (1e-12 after one step,
-1e-9 after ten), for the weights, real_f and marker too; mixed precision within 1e-4 of FP64."""
+a delta-f species without refresh.  p9, p10 and p11 repeat p7 / p8 with the other equilibrium
+distributions, loaded by the reference's own loaders: loss-cone, partial shell (PC, periodic) and
+counter-beam.  Tolerances: as test_gpu_parity.py (1e-12 after one step, 1e-9 after ten), for the
+weights, real_f and marker too; mixed precision within 1e-4 of FP64."""
 import os
 
 import numpy as np
 import pytest
-from parity_util import by_pid, rel_err, state_errors
+from parity_util import by_pid, rel_err, state_errors, with_reference_norms
 from state_io import read_state
 
 import hfemic_b200 as h
 
 pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-PSD = ["p7_psd_tsc_mirror_reflecting", "p8_pc_psd_periodic"]
+PSD = ["p7_psd_tsc_mirror_reflecting", "p8_pc_psd_periodic", "p9_losscone_psd_mirror", "p10_pc_shell_psd_mirror",
+       "p11_counterbeam_psd_mirror"]
 
 
 @pytest.mark.parametrize("name", PSD)
 def test_weights_against_reference_fixture(name, gpu_lib):
     """Ten steps on the GPU against the reference's own output: fields, weights, real_f and the
     moments with the delta-f equilibrium added."""
-    cfg = h.configs.PARITY[name]()
     init = read_state(os.path.join(GOLDEN, f"{name}.init.bin"))
+    cfg = with_reference_norms(h.configs.PARITY[name](), init)
     ref = read_state(os.path.join(GOLDEN, f"{name}.step10.bin"))
     with h.Run(cfg, gpu_lib) as g:
         g.upload_state(init)

@@ -5,6 +5,7 @@ import os
 
 import numpy as np
 import pytest
+from parity_util import with_reference_norms
 from state_io import read_state
 
 import hfemic_b200 as h
@@ -50,16 +51,28 @@ def compare_states(mine, ref, cfg, exact=True, rtol=0.0):
 @pytest.mark.parametrize("name", sorted(h.configs.PARITY))
 @pytest.mark.parametrize("steps", [1, 10])
 def test_oracle_bit_exact_vs_reference(oracle_lib, name, steps):
+    """Bit for bit, except for the counter-beam equilibrium (configs.PARITY_ROUNDING): its density
+    and f0 need Dawson's integral, which the reference takes from the Faddeeva package
+    (LibPIC/PIC/Misc/Faddeeva.cc) and the oracle evaluates by its own method, and its PartSpecies::Nc
+    comes from the reference's numerical integration of the density (VDFHelper.h:43-64, about
+    1e-9 from the exact integral), so there the oracle takes Nc from the state file and agrees to
+    rounding (8e-15 in the weights after ten steps; bound 1e-13)."""
     cfg = h.configs.PARITY[name]()
     init = read_state(os.path.join(GOLDEN, f"{name}.init.bin"))
     ref = read_state(os.path.join(GOLDEN, f"{name}.step{steps}.bin"))
+    exact = name not in h.configs.PARITY_ROUNDING
     # the reference normalises moments with PartSpecies::Nc; the config must give the same value
-    assert [cfg.moment_norm(k) for k in cfg.kinetic] == list(init["moment_norm"])
+    norms = [cfg.moment_norm(k) for k in cfg.kinetic]
+    if exact:
+        assert norms == list(init["moment_norm"])
+    else:
+        np.testing.assert_allclose(norms, init["moment_norm"], rtol=1e-8)
+        cfg = with_reference_norms(cfg, init)
     with h.Run(cfg, oracle_lib, "orc_") as run:
         run.upload_state(init)
         run.advance(steps)
         mine = run.state()
-    errs = compare_states(mine, ref, cfg, exact=True)
+    errs = compare_states(mine, ref, cfg, exact=exact, rtol=1e-13)
     assert not errs, errs
     # particle order: the oracle's upload index maps to the reference's global particle id
     for s in range(len(cfg.kinetic)):
