@@ -570,6 +570,7 @@ int sort_species(h1d_run *run, int s)
     int const      ti = static_cast<int>(ntiles);
     SortKeys       first{};
     first.full_min = -0.5 * Nx, first.Nx = Nx, first.dead = S.dead, first.status = run->d_status;
+    first.absorbing = run->p.particle_bc == H1D_BC_ABSORBING;
     if (run->mixed)
         first.cell = S.cell[S.cur], first.wf = S.fbuf[S.cur][4];
     else

@@ -3,8 +3,9 @@
 // The reference keeps particles in a std::deque in load order and never sorts them; here the
 // particles are kept cell-sorted so that a warp's particles share a few cells (coalesced field
 // reads, register-window deposits).  The key of a particle is its full-grid cell
-// floor(q1 - q1min) in [0, Nx) (ParamSet.cc:22); absorbed particles (weight 0) get key Nx and
-// move to the end, where the host trims them.  Sorting is stable, so the order is reproducible
+// floor(q1 - q1min) in [0, Nx) (ParamSet.cc:22); under the absorbing boundary, absorbed particles
+// (weight 0) get key Nx and move to the end, where the host trims them (under the other
+// boundaries a weight of 0 is an ordinary particle: a test particle, or a delta-f one).  Sorting is stable, so the order is reproducible
 // and equals std::stable_sort by key on the host.
 //
 // Keys lie in [0, Nx], so ceil(log2(Nx + 1)) bits are sorted, in one pass (up to 8 bits) or two
@@ -55,6 +56,7 @@ struct SortKeys {
     float const        *wf;
     double              full_min;
     int                 Nx;
+    int                 absorbing; // weight 0 marks a removed particle only under the absorbing BC
     unsigned long long *dead;   // absorbed particles, counted once by the first histogram
     unsigned           *status;
 };
@@ -94,11 +96,11 @@ __device__ __forceinline__ uint32_t key_of(SortKeys const &s, KeyRaw<KIND> const
         uint32_t k;
         if constexpr (KIND == KEYS_FP64) {
             double const f = floor(r.q - s.full_min);
-            dead           = r.w == 0.0;
+            dead           = s.absorbing && r.w == 0.0;
             lost           = !(f >= 0.0 && f < static_cast<double>(s.Nx));
             k              = lost ? (f >= 0.0 ? static_cast<uint32_t>(s.Nx - 1) : 0u) : static_cast<uint32_t>(f);
         } else {
-            dead = r.w == 0.0f;
+            dead = s.absorbing && r.w == 0.0f;
             lost = r.c < 0 || r.c >= s.Nx;
             k    = lost ? (r.c < 0 ? 0u : static_cast<uint32_t>(s.Nx - 1)) : static_cast<uint32_t>(r.c);
         }

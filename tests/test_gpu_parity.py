@@ -129,6 +129,23 @@ def test_absorbing_boundary(gpu_lib, oracle_lib):
     assert not bad, bad
 
 
+def test_test_particles(gpu_lib, oracle_lib):
+    """Test particles (TestParticleVDF, VDF/TestParticleVDF.cc:15-24: weight 0, f0 = 0) run as a
+    full-f species without refresh: they are pushed and moved like the oracle's, and deposit
+    nothing."""
+    cfg = h.configs.parity_p2()
+    init = read_state(os.path.join(GOLDEN, f"{cfg.name}.init.bin"))
+    init["particles"][1]["w"] = np.zeros_like(init["particles"][1]["w"])
+    g, c, _, _ = run_both(cfg, init, 5, gpu_lib, oracle_lib, chunks=2)
+    errs = state_errors(g, c, cfg)
+    bad = {k: v for k, v in errs.items() if not v <= TOL10}
+    assert not bad, bad
+    for key in ("n", "nV", "nvv"):
+        assert not np.any(g["moments"][1][key]), key
+    moved = by_pid(g["particles"][1])["q1"] - init["particles"][1]["q1"]
+    assert np.count_nonzero(moved) > 0.9 * moved.size
+
+
 def test_moved_too_far(gpu_lib):
     cfg = h.configs.parity_p1()
     init = read_state(os.path.join(GOLDEN, f"{cfg.name}.init.bin"))
