@@ -30,11 +30,19 @@ struct MomentArgsMixed {
     unsigned      *status;
 };
 
-// one particle as the collect_all loop needs it: CIC stencil, weight and velocity in FP64
-struct MomParticle {
-    int    i0;
-    double s0, s1, w, vx, vy, vz;
-    bool   ok;
+// the arithmetic of a lane's collect_all sums: FP64 for FP64 particles; FP32 for mixed-precision
+// particles (a lane sums at most 16 FP32 particles per cell; warp sums and atomics are FP64)
+template <class Args> struct MomReal {
+    using type = double;
+};
+template <> struct MomReal<MomentArgsMixed> {
+    using type = float;
+};
+// one particle as the collect_all loop needs it: CIC stencil, weight and velocity
+template <class R> struct MomParticle {
+    int  i0;
+    R    s0, s1, w, vx, vy, vz;
+    bool ok;
 };
 // NP consecutive particles of a lane, loaded with 16-byte vector loads (NP = 4 FP32 / 2 FP64)
 template <class Args> struct MomTile;
@@ -85,20 +93,24 @@ __device__ __forceinline__ MomTile<MomentArgsMixed> mom_load(MomentArgsMixed con
     }
     return t;
 }
-__device__ __forceinline__ MomParticle mom_particle(MomentArgs const &a, MomTile<MomentArgs> const &t, int j)
+__device__ __forceinline__ MomParticle<double> mom_particle(MomentArgs const &a, MomTile<MomentArgs> const &t, int j)
 {
     double const   q1 = el2(t.q1, j);
     Shape<1> const sh = make_shape<1>(q1 - a.half_min);
     return { sh.i0, sh.w[0], sh.w[1], el2(t.w, j), el2(t.vx, j), el2(t.vy, j), el2(t.vz, j),
              finite_pos(q1) && stencil_ok(sh, a.Nx) };
 }
-__device__ __forceinline__ MomParticle mom_particle(MomentArgsMixed const &a, MomTile<MomentArgsMixed> const &t, int j)
+__device__ __forceinline__ MomParticle<float> mom_particle(MomentArgsMixed const &a, MomTile<MomentArgsMixed> const &t, int j)
 {
     ShapeF<1> const sh = make_shape_f<1>(el4(t.cell, j), el4(t.off, j));
     return { sh.i0, sh.w[0], sh.w[1], el4(t.w, j), el4(t.vx, j), el4(t.vy, j), el4(t.vz, j), stencil_ok_f(sh, a.Nx) };
 }
 
 constexpr int MOM_THREADS = 128;
+// resident blocks per SM: FP32 lane sums fit five blocks in 96 registers without spills (0.235 ->
+// about 0.165 ms per collect_all of 16.4M particles, against three blocks of FP64 sums); six
+// spill and are slower
+constexpr int MOM_MIN_BLOCKS_MIXED = 5;
 // particles per lane of a collect_all warp: a multiple of 4 (whole rounds of either tile) from 4
 // to 16, growing with the particles per cell
 inline int mom_ppt(double ppc)
@@ -122,8 +134,12 @@ __device__ __forceinline__ void mom_add(double *const (&out)[10], int q, int cel
         bad |= ST_OUT_OF_RANGE;
 }
 
+// resident blocks of MOM_THREADS per SM the register budget is set for
+template <class Args> constexpr int mom_min_blocks = 4;
+template <> constexpr int mom_min_blocks<MomentArgsMixed> = MOM_MIN_BLOCKS_MIXED;
+
 template <class Args>
-__global__ void __launch_bounds__(MOM_THREADS) moments_kernel(Args a)
+__global__ void __launch_bounds__(MOM_THREADS, mom_min_blocks<Args>) moments_kernel(Args a)
 {
     constexpr int NP   = MomTile<Args>::NP;
     constexpr int NONE = 0x40000000;
@@ -133,7 +149,8 @@ __global__ void __launch_bounds__(MOM_THREADS) moments_kernel(Args a)
     if (chunk0 >= a.n)
         return;
     int64_t const first = chunk0 + static_cast<int64_t>(lane) * a.ppt; // this lane's particles
-    double        T[10], L[10], R[10];
+    using Real          = typename MomReal<Args>::type;
+    Real          T[10], L[10], R[10];
 #pragma unroll
     for (int q = 0; q < 10; ++q)
         T[q] = L[q] = R[q] = 0;
@@ -147,27 +164,28 @@ __global__ void __launch_bounds__(MOM_THREADS) moments_kernel(Args a)
         for (int j = 0; j < NP; ++j) {
             if (i0 + j >= a.n)
                 break;
-            MomParticle const p = mom_particle(a, cur, j);
+            auto const p = mom_particle(a, cur, j);
             if (!p.ok) {
                 bad |= ST_OUT_OF_RANGE;
                 continue;
             }
-            bool const up = p.s1 >= 0.5; // the particle's cell is i0 + 1, its left neighbour gets s0
+            bool const up = p.s1 >= Real(0.5); // the particle's cell is i0 + 1, its left neighbour gets s0
             int const  c  = p.i0 + (up ? 1 : 0);
             if (c != rc) {
                 if (rc != NONE) {
 #pragma unroll
                     for (int q = 0; q < 10; ++q) {
-                        mom_add(a.out, q, rc, a.Nx, T[q] - L[q] - R[q], bad);
-                        mom_add(a.out, q, rc - 1, a.Nx, L[q], bad);
-                        mom_add(a.out, q, rc + 1, a.Nx, R[q], bad);
+                        double const t = T[q], l = L[q], r = R[q];
+                        mom_add(a.out, q, rc, a.Nx, t - l - r, bad);
+                        mom_add(a.out, q, rc - 1, a.Nx, l, bad);
+                        mom_add(a.out, q, rc + 1, a.Nx, r, bad);
                         T[q] = L[q] = R[q] = 0;
                     }
                 }
                 rc = c;
             }
-            double const left = up ? p.s0 : 0.0, right = up ? 0.0 : p.s1;
-            double const v[10] = { p.w,               p.vx * p.w,        p.vy * p.w,        p.vz * p.w,
+            Real const left = up ? p.s0 : Real(0), right = up ? Real(0) : p.s1;
+            Real const v[10] = { p.w,               p.vx * p.w,        p.vy * p.w,        p.vz * p.w,
                                    (p.vx * p.vx) * p.w, (p.vy * p.vy) * p.w, (p.vz * p.vz) * p.w, (p.vx * p.vy) * p.w,
                                    (p.vy * p.vz) * p.w, (p.vz * p.vx) * p.w };
 #pragma unroll
@@ -185,9 +203,9 @@ __global__ void __launch_bounds__(MOM_THREADS) moments_kernel(Args a)
         bool const mine = rc == key;
 #pragma unroll
         for (int q = 0; q < 10; ++q) {
-            double const t = warp_sum(mine ? T[q] : 0.0);
-            double const l = warp_sum(mine ? L[q] : 0.0);
-            double const r = warp_sum(mine ? R[q] : 0.0);
+            double const t = warp_sum(mine ? static_cast<double>(T[q]) : 0.0);
+            double const l = warp_sum(mine ? static_cast<double>(L[q]) : 0.0);
+            double const r = warp_sum(mine ? static_cast<double>(R[q]) : 0.0);
             if (lane == 3 * q)
                 mom_add(a.out, q, key, a.Nx, t - l - r, bad);
             else if (lane == 3 * q + 1)
