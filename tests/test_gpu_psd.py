@@ -87,9 +87,10 @@ def test_upload_psd_contract(gpu_lib):
             g.upload_psd(0, st["particles"][0]["w"], np.ones(st["particles"][0]["w"].size))
 
 
+@pytest.mark.parametrize("name", ["p7_psd_tsc_mirror_reflecting", "p11_counterbeam_psd_mirror"])
 @pytest.mark.parametrize("precision,tol", [(h.configs.PREC_FP64, 1e-12), (h.configs.PREC_MIXED, 1e-5)])
-def test_resume_with_evolving_weights(gpu_lib, precision, tol):
-    cfg = h.configs.parity_p7().replace(precision=precision)
+def test_resume_with_evolving_weights(gpu_lib, name, precision, tol):
+    cfg = h.configs.PARITY[name]().replace(precision=precision)
     init = read_state(os.path.join(GOLDEN, f"{cfg.name}.init.bin"))
     with h.Run(cfg, gpu_lib) as a:
         a.upload_state(init)
@@ -135,3 +136,23 @@ def test_batches_and_device_loader_refuse_evolving_weights(gpu_lib):
             h.abi.Batch([r])
         with pytest.raises(ValueError):
             h.abi.populate(r, 0, seed=1, count=1000)
+
+
+@pytest.mark.parametrize("name", PSD[2:])
+def test_loader_states_against_oracle(name, gpu_lib, oracle_lib):
+    """States drawn by the host loader for each equilibrium distribution (128 and 96 particles per
+    cell, real_f / marker included) advance on the GPU as in the oracle: ten steps within 1e-9."""
+    from hfemic_b200.loader import initial_state
+
+    cfg = h.configs.PARITY[name]()
+    for k in cfg.kinetic:
+        k.Nc *= 8
+    init = initial_state(cfg, seed=17)
+    with h.Run(cfg, gpu_lib, "h1d_") as g, h.Run(cfg, oracle_lib, "orc_") as c:
+        g.upload_state(init)
+        c.upload_state(init)
+        g.advance(10)
+        c.advance(10)
+        errs = state_errors(g.state(), c.state(), cfg)
+    bad = {k: v for k, v in errs.items() if not v <= 1e-9}
+    assert not bad, bad
