@@ -1697,6 +1697,9 @@ int h1d_populate(h1d_run *run, int s, int64_t n, uint64_t seed, double beta1, do
     if (evolves_psd(run->p.kinetic[s]))
         return set_err(run, H1D_ERR_INVALID_ARG,
                        "h1d_populate: species with evolving weights are loaded with h1d_upload_particles and h1d_upload_psd");
+    if (run->p.kinetic[s].vdf != H1D_VDF_BIMAXWELLIAN)
+        return set_err(run, H1D_ERR_INVALID_ARG,
+                       "h1d_populate: draws bi-Maxwellian particles; other distributions are uploaded");
     h1d_params const       &p = run->p;
     h1d_kinetic_desc const &d = p.kinetic[s];
     SpeciesState           &S = run->sp[s];
@@ -2402,9 +2405,9 @@ int h1d_server_submit(h1d_server *sv, h1d_request const *rq, uint64_t *id)
     }
     if (rq->params.algorithm != H1D_ALGO_CAMCL || rq->n_steps == 0)
         return H1D_ERR_INVALID_ARG;
-    for (int s = 0; s < rq->params.n_kinetic; ++s)
+    for (int s = 0; s < rq->params.n_kinetic; ++s) // built by h1d_populate: bi-Maxwellian, full-f
         if (rq->n_particles[s] < 0 || rq->n_particles[s] > (int64_t{ 1 } << 31) - 1 || !(rq->beta1[s] > 0)
-            || !(rq->T2_T1[s] > 0))
+            || !(rq->T2_T1[s] > 0) || rq->params.kinetic[s].vdf != H1D_VDF_BIMAXWELLIAN || evolves_psd(rq->params.kinetic[s]))
             return H1D_ERR_INVALID_ARG;
     auto *r  = new (std::nothrow) ServerReq{};
     if (!r)

@@ -217,7 +217,8 @@ int h1d_download_psd(h1d_run *run, int s, double *real_f, double *marker);
  * radical inverses and two counter-based uniforms of (seed, s, particle), full-f weight 1.
  * Replaces any previous particles of that species.  The reference seeds its generators with fixed
  * constants; here `seed` selects the sequences, and loader.py computes the same particles on the
- * host. */
+ * host.  Refuses species whose weights evolve or whose `vdf` is not H1D_VDF_BIMAXWELLIAN
+ * (H1D_ERR_INVALID_ARG): those are loaded on the host and uploaded. */
 int h1d_populate(h1d_run *run, int s, int64_t n, uint64_t seed, double beta1, double T2_T1);
 /* B (full grid) and E (half grid), each (Nx+2*H1D_PAD)*3 doubles, GridArray layout */
 int h1d_upload_fields(h1d_run *run, const double *B, const double *E);

@@ -136,6 +136,14 @@ def test_batches_and_device_loader_refuse_evolving_weights(gpu_lib):
             h.abi.Batch([r])
         with pytest.raises(ValueError):
             h.abi.populate(r, 0, seed=1, count=1000)
+    # a full-f species of another distribution: the device loader draws bi-Maxwellians only
+    import dataclasses
+    cfg = h.configs.parity_p9()
+    kin = [dataclasses.replace(k, scheme=h.configs.FULL_F, psd_refresh_frequency=0.0, marker_temp_ratio=1.0)
+           for k in cfg.kinetic]
+    with h.Run(cfg.replace(kinetic=kin), gpu_lib) as r:
+        with pytest.raises(ValueError):
+            h.abi.populate(r, 0, seed=1, count=1000)
 
 
 @pytest.mark.parametrize("name", PSD[2:])

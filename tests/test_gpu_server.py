@@ -108,3 +108,15 @@ def test_oversize_request_is_refused(gpu_lib):
     with h.abi.Server(gpu_lib, 1 << 20, steps_per_tick=16) as sv:
         with pytest.raises(h.H1DError):
             sv.submit(_cfg(0, h.configs.PREC_FP64), seed=0, n_steps=10)
+
+
+def test_requests_the_device_loader_cannot_build_are_refused(gpu_lib):
+    """Served runs are built by h1d_populate (bi-Maxwellian, full-f): a species of another
+    distribution, or with evolving weights, is refused at submission."""
+    import dataclasses
+    base = _cfg(0, h.configs.PREC_FP64)
+    with h.abi.Server(gpu_lib, 8 << 30, steps_per_tick=16) as sv:
+        for change in (dict(vdf=h.configs.VDF_LOSSCONE, losscone_beta=0.3), dict(scheme=h.configs.DELTA_F)):
+            cfg = base.replace(kinetic=[dataclasses.replace(base.kinetic[0], **change)] + base.kinetic[1:])
+            with pytest.raises(h.H1DError):
+                sv.submit(cfg, seed=0, n_steps=10)
