@@ -37,7 +37,7 @@ import math
 import numpy as np
 
 from .configs import (VDF_BIMAXWELLIAN, VDF_COUNTER_BEAM, VDF_LOSSCONE, VDF_PARTIAL_SHELL, DELTA_F, RunConfig,
-                      _q1_of_n, _n_of_q1)
+                      _q1_of_n, _n_of_q1, dawson)
 
 PAD = 3
 
@@ -140,43 +140,6 @@ def load_species(cfg: RunConfig, s: int, seed: int = 0, count: int | None = None
 # every equilibrium distribution, with its phase-space density
 # ---------------------------------------------------------------------------------------------
 
-def dawson(x: np.ndarray) -> np.ndarray:
-    """Dawson's integral of positive x (vectorised configs.dawson): Maclaurin series below 0.2,
-    Rybicki's sampling-theorem sum up to 50, asymptotic series above."""
-    x = np.asarray(x, dtype=np.float64)
-    out = np.empty_like(x)
-    small, large = x < 0.2, x > 50
-    mid = ~(small | large)
-    if small.any():
-        xs = x[small]
-        t = xs.copy()
-        acc = xs.copy()
-        for j in range(1, 40):
-            t = t * (-2 * xs * xs / (2 * j + 1))
-            acc += t
-        out[small] = acc
-    if large.any():
-        xl = x[large]
-        r = 1 / (2 * xl * xl)
-        t = np.ones_like(xl)
-        acc = np.ones_like(xl)
-        for j in range(1, 12):
-            t = t * ((2 * j - 1) * r)
-            acc += t
-        out[large] = acc / (2 * xl)
-    if mid.any():
-        xm = x[mid]
-        lo = np.floor((xm - 7) / 0.2).astype(np.int64) | 1
-        hi = np.ceil((xm + 7) / 0.2).astype(np.int64)
-        acc = np.zeros_like(xm)
-        for j in range(0, 80, 2):
-            nn = lo + j
-            term = np.exp(-(xm - nn * 0.2) ** 2) / nn
-            acc += np.where(nn <= hi, term, 0.0)
-        out[mid] = acc / math.sqrt(math.pi)
-    return out
-
-
 def _losscone_beta_eq(k) -> float:
     b = k.losscone_beta
     if b < 1e-10:
@@ -215,7 +178,7 @@ def equilibrium(cfg: RunConfig, k, q1):
         nu = k.nu / c
         F = dawson(1 / nu)
         t1 = 0.5 * nu * (1 / F - nu)
-        n0 = (2 * nu * F) / (2 * k.nu * float(dawson(np.array([1 / k.nu]))[0]))
+        n0 = (2 * nu * F) / (2 * k.nu * dawson(1 / k.nu))
         return n0, t1 * T * vth * vth, 0.5 * (1 - t1) * T * vth * vth
     eta = 1 / (k.T2_T1 + (1 - k.T2_T1) * c * c)
     return eta, np.full_like(q1, .5 * vth * vth), .5 * vth * vth * k.T2_T1 * eta
@@ -250,7 +213,7 @@ def phase_space_density(cfg: RunConfig, k, q1, vx, vy, vz, temp_ratio: float = 1
             Bz = math.sqrt(math.pi) * math.gamma(1 + .5 * k.zeta) / math.gamma(1.5 + .5 * k.zeta)
             fa = (1.0 if k.zeta == 0 else ((1 - u) * (1 + u)) ** (.5 * k.zeta)) / Bz
             return n0 * (.5 * fv * fa / (math.pi * vth ** 3))
-        B0 = 2 * k.nu * float(dawson(np.array([1 / k.nu]))[0])
+        B0 = 2 * k.nu * dawson(1 / k.nu)
         return fv * np.exp(-((1 - u) * (1 + u)) * c * c / (k.nu * k.nu)) / B0 / (2 * math.pi * vth ** 3)
     T2OT1 = k.T2_T1 * n0
     return n0 * (np.exp(-x1 * x1) / math.sqrt(math.pi) * np.exp(-(x2 * x2 + x3 * x3) / T2OT1) / (math.pi * T2OT1) / vth ** 3)
