@@ -164,3 +164,13 @@ def test_loader_states_against_oracle(name, gpu_lib, oracle_lib):
         errs = state_errors(g.state(), c.state(), cfg)
     bad = {k: v for k, v in errs.items() if not v <= 1e-9}
     assert not bad, bad
+
+
+@pytest.mark.parametrize("name", PSD[:1] + PSD[2:])
+def test_equilibrium_moments(name, gpu_lib):
+    """The library's delta-f equilibrium moments (n0, nvv0 of every distribution, computed on the
+    host at create) against the loader's independent evaluation: zero weights after
+    advance_by(0) leave the equilibrium alone."""
+    from test_vdf import _equilibrium_only, check_equilibrium_moments
+
+    check_equilibrium_moments(*_equilibrium_only(gpu_lib, "h1d_", name))

@@ -142,3 +142,41 @@ def test_loader_against_reference_loader(name):
         if cfg.kinetic[s].scheme == h.configs.FULL_F:
             assert abs(np.mean(p["w"]) / np.mean(r["w"]) - 1) < 0.25, (name, s)
             assert abs(np.mean(p["marker"]) / np.mean(r["marker"]) - 1) < 0.25, (name, s)
+
+
+def _equilibrium_only(lib, prefix, name):
+    """moments of species 0 (delta-f) with every weight 0 after advance_by(0): the equilibrium
+    n0, nvv0 times the moment weighting alone (PartSpecies.cc:129-143)"""
+    import os
+
+    import numpy as np
+    from parity_util import with_reference_norms
+    from state_io import read_state
+    init = read_state(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", f"{name}.init.bin"))
+    cfg = with_reference_norms(h.configs.PARITY[name](), init)
+    init["particles"][0]["w"][:] = 0.0
+    with h.Run(cfg, lib, prefix) as r:
+        r.upload_state(init)
+        r.advance(0)
+        return cfg, r.moments(0)
+
+
+def check_equilibrium_moments(cfg, moments):
+    import numpy as np
+
+    from hfemic_b200.loader import equilibrium
+    n, nV, nvv = moments
+    P, Nx = 3, cfg.Nx
+    n0, vpar2, vperp2 = equilibrium(cfg, cfg.kinetic[0], np.arange(Nx) + cfg.q1min + 0.5)
+    np.testing.assert_allclose(n[P:P + Nx], n0, rtol=1e-13)
+    np.testing.assert_allclose(nvv[P:P + Nx, 0], n0 * vpar2, rtol=1e-13)
+    np.testing.assert_allclose(nvv[P:P + Nx, 1], n0 * vperp2, rtol=1e-13)
+    np.testing.assert_allclose(nvv[P:P + Nx, 2], n0 * vperp2, rtol=1e-13)
+    assert not np.any(nV) and not np.any(nvv[:, 3:]) and not np.any(n[:P]) and not np.any(n[P + Nx:])
+
+
+@pytest.mark.parametrize("name", FAMILIES)
+def test_oracle_equilibrium_moments(oracle_lib, name):
+    """The oracle's delta-f equilibrium moments of every distribution against the loader's
+    independent evaluation of the same formulas (agreement to rounding)."""
+    check_equilibrium_moments(*_equilibrium_only(oracle_lib, "orc_", name))
