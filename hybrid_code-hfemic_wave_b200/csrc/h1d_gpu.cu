@@ -1173,6 +1173,11 @@ int batch_step(h1d_batch *b)
         for (int s = 0; s < r->p.n_kinetic; ++s) {
             if (r->sp[s].n == 0)
                 continue;
+            if (evolves_psd(r->p.kinetic[s])) { // the weight-evolving pass, one species per launch
+                BTRY(r, launch_push(r, s, push_args(r, s)));
+                b->stats.kernel_launches += 1;
+                continue;
+            }
             Kind const kd{ static_cast<int>(r->p.kinetic[s].shape_order), r->p.particle_bc, r->p.xi != 0, r->mixed };
             size_t     ki = 0;
             while (ki < kinds.size() && !(kinds[ki] == kd))
@@ -1971,9 +1976,6 @@ int h1d_batch_create(h1d_run *const *runs, int n_runs, h1d_batch **out)
         for (int j = 0; j < i && !why; ++j)
             if (runs[j] == r)
                 why = "run listed twice";
-        for (int s = 0; r && s < r->p.n_kinetic && !why; ++s)
-            if (evolves_psd(r->p.kinetic[s]))
-                why = "species with evolving weights (delta-f, PSD refresh) advance as single runs";
         if (why) {
             std::fprintf(stderr, "h1d_batch_create: member %d: %s\n", i, why);
             return H1D_ERR_INVALID_ARG;

@@ -334,8 +334,9 @@ int h1d_autotune(h1d_run *run, uint32_t *steps_taken, int *sort_interval, int *p
 /* ---- Ensembles (no counterpart in the reference) ---------------------------------------------
  * A batch advances many CAM-CL runs together on one stream of the current device.  A step is one
  * launch of the particle pass per kind of particle group (shape order, geometry, boundary,
- * precision) covering every species of every member, and one launch of the field cycle covering
- * every member's grid.  Steps come in blocks of sort_interval steps, all groups cell-sorted at the
+ * precision) covering every species of every member (a species with evolving weights, delta-f or
+ * PSD refresh, takes a launch of its own), and one launch of the field cycle covering every
+ * member's grid.  Steps come in blocks of sort_interval steps, all groups cell-sorted at the
  * start of a block.  When no member uses absorbing particles or gyrophase randomization, a pair of
  * blocks is captured once as a CUDA graph and replayed while the members are unchanged (an upload
  * to a member invalidates it).  Members stay owned by the caller, must outlive the batch and

@@ -149,3 +149,45 @@ def test_batch_member_with_external_source(gpu_lib):
             r.close()
     for c, a, t in zip(cfgs, alone, together):
         assert max(_field_errs(t, a, c).values()) <= 1e-12
+
+
+@pytest.mark.parametrize("precision,tol", [(h.configs.PREC_FP64, 1e-10), (h.configs.PREC_MIXED, 1e-4)])
+def test_batch_with_evolving_weights(gpu_lib, precision, tol):
+    """Members whose weights evolve (delta-f over bi-Maxwellian, loss-cone and counter-beam
+    equilibria, PSD refresh) beside a plain member: 20 batch steps (graph replays included) equal
+    each run alone, weights and phase-space densities included."""
+    import os
+
+    from parity_util import with_reference_norms
+    from state_io import read_state
+
+    golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    names = ["p7_psd_tsc_mirror_reflecting", "p9_losscone_psd_mirror", "p11_counterbeam_psd_mirror",
+             "p2_tsc_mirror_reflecting"]
+    states = [read_state(os.path.join(golden, f"{n}.init.bin")) for n in names]
+    cfgs = [with_reference_norms(h.configs.PARITY[n](), st).replace(precision=precision) for n, st in zip(names, states)]
+    alone = []
+    for c, st in zip(cfgs, states):
+        with h.Run(c, gpu_lib) as r:
+            h.abi.configure(r, sort_interval=4)
+            r.upload_state(st)
+            r.advance(20)
+            alone.append(r.state())
+    runs = [h.Run(c, gpu_lib) for c in cfgs]
+    try:
+        for r, st in zip(runs, states):
+            h.abi.configure(r, sort_interval=4)
+            r.upload_state(st)
+        with h.abi.Batch(runs) as b:
+            b.configure(sort_interval=4)
+            b.advance(20)
+            assert b.stats()["steps"] == 20
+            together = [r.state() for r in runs]
+    finally:
+        for r in runs:
+            r.close()
+    for c, a, t in zip(cfgs, alone, together):
+        errs = state_errors(t, a, c)
+        assert any(k.endswith("real_f") for k in errs) or not any(k.has_psd for k in c.kinetic)
+        bad = {k: v for k, v in errs.items() if not v <= tol}
+        assert not bad, (c.name, bad)

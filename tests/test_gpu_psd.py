@@ -129,11 +129,9 @@ def test_vhistogram_psd_columns(gpu_lib, oracle_lib):
                 np.testing.assert_allclose(hg[..., 2][same], hg[..., 1][same], rtol=1e-9, atol=1e-14)
 
 
-def test_batches_and_device_loader_refuse_evolving_weights(gpu_lib):
+def test_device_loader_refuses_evolving_weights(gpu_lib):
     cfg = h.configs.parity_p7()
     with h.Run(cfg, gpu_lib) as r:
-        with pytest.raises(h.H1DError):
-            h.abi.Batch([r])
         with pytest.raises(ValueError):
             h.abi.populate(r, 0, seed=1, count=1000)
     # a full-f species of another distribution: the device loader draws bi-Maxwellians only
