@@ -762,7 +762,9 @@ int camcl_step(h1d_run *run)
 // re-predicted fields, corrector pass, corrected fields.  Deposit set X = dset takes the
 // predictor's deposit, Y = 1 - dset the corrector's; each field phase clears the set the next
 // particle pass uses.
-int pc_launch_fields(h1d_run *run, int phase, int raw_set, int zero_set, double const *E1_in, double *E1_out)
+// the field arguments of predictor-corrector phase `phase` (0: initial sources, 1: B1 and E1
+// predicted, 2: re-predicted, 3: corrected) reading deposit set raw_set and clearing zero_set
+FieldArgs pc_field_args(h1d_run *run, int phase, int raw_set, int zero_set, double const *E1_in, double *E1_out)
 {
     FieldArgs a = field_args(run);
     for (int s = 0; s < run->p.n_kinetic; ++s)
@@ -771,15 +773,38 @@ int pc_launch_fields(h1d_run *run, int phase, int raw_set, int zero_set, double 
                 a.k[s].raw[d][q]  = dep_ptr(run, s, raw_set, d, q);
                 a.k[s].zero[d][q] = dep_ptr(run, s, zero_set, d, q);
             }
-    a.phase      = phase;
-    a.charge_in  = run->charge + PAD;
-    a.current_in = run->current + 3 * PAD;
-    a.E1_in      = E1_in ? E1_in + 3 * PAD : nullptr;
-    a.E1_out     = E1_out ? E1_out + 3 * PAD : nullptr;
+    a.phase = phase;
+    if (phase != 3) {
+        a.charge_in  = run->charge + PAD;
+        a.current_in = run->current + 3 * PAD;
+    }
+    a.E1_in  = E1_in ? E1_in + 3 * PAD : nullptr;
+    a.E1_out = E1_out ? E1_out + 3 * PAD : nullptr;
+    return a;
+}
+
+int pc_launch_fields(h1d_run *run, int phase, int raw_set, int zero_set, double const *E1_in, double *E1_out)
+{
+    FieldArgs const a = pc_field_args(run, phase, raw_set, zero_set, E1_in, E1_out);
     phase_begin(run, 2);
     CU(launch_pc_fields(a, run->nblocks_field, run->L, run->field_smem, run->stream));
     phase_end(run, 1);
     return H1D_OK;
+}
+
+// the particle-pass arguments of species s in predictor-corrector pass `pass` (0 predictor:
+// particles not kept; 1 corrector; 2 initial deposit only), depositing into set dep_set
+PushArgs pc_pass_args(h1d_run *run, int s, int pass, int dep_set)
+{
+    PushArgs a = push_args(run, s);
+    for (int q = 0; q < 4; ++q)
+        a.dep[0][q] = dep_ptr(run, s, dep_set, 0, q), a.dep[1][q] = dep_ptr(run, s, dep_set, 1, q);
+    a.move_steps   = pass == 2 ? 0 : 2;
+    a.deposit_mask = 2;
+    a.write_back   = pass == 1;
+    a.travel_scale = 1.0 / 0.5;
+    a.counter      = static_cast<uint64_t>(run->step) * 8 + (pass == 1 ? 2 : 0);
+    return a;
 }
 
 int pc_particles(h1d_run *run, int pass, int dep_set) // pass 0 predictor, 1 corrector, 2 initial deposit
@@ -787,14 +812,7 @@ int pc_particles(h1d_run *run, int pass, int dep_set) // pass 0 predictor, 1 cor
     for (int s = 0; s < run->p.n_kinetic; ++s) {
         if (pass != 2 && run->sp[s].since_sort >= run->sort_interval)
             TRY(sort_species(run, s));
-        PushArgs a = push_args(run, s);
-        for (int q = 0; q < 4; ++q)
-            a.dep[0][q] = dep_ptr(run, s, dep_set, 0, q), a.dep[1][q] = dep_ptr(run, s, dep_set, 1, q);
-        a.move_steps   = pass == 2 ? 0 : 2;
-        a.deposit_mask = 2;
-        a.write_back   = pass == 1;
-        a.travel_scale = 1.0 / 0.5;
-        a.counter      = static_cast<uint64_t>(run->step) * 8 + (pass == 1 ? 2 : 0);
+        PushArgs const a = pc_pass_args(run, s, pass, dep_set);
         phase_begin(run, 0);
         TRY(launch_push(run, s, a));
         phase_end(run, run->sp[s].n > 0 ? 1 : 0);
@@ -823,21 +841,7 @@ int pc_step(h1d_run *run)
     TRY(launch_run_sources(run, static_cast<double>(run->step) * run->p.dt + run->p.dt)); // update(dt), both passes
     TRY(pc_launch_fields(run, 2, X, Y, run->E1[0], run->E1[1]));
     TRY(pc_particles(run, 1, Y));
-    {
-        FieldArgs a = field_args(run);
-        for (int s = 0; s < run->p.n_kinetic; ++s)
-            for (int d = 0; d < 2; ++d)
-                for (int q = 0; q < 4; ++q) {
-                    a.k[s].raw[d][q]  = dep_ptr(run, s, Y, d, q);
-                    a.k[s].zero[d][q] = dep_ptr(run, s, X, d, q);
-                }
-        a.phase  = 3;
-        a.E1_in  = run->E1[1] + 3 * PAD;
-        a.E1_out = nullptr;
-        phase_begin(run, 2);
-        CU(launch_pc_fields(a, run->nblocks_field, run->L, run->field_smem, run->stream));
-        phase_end(run, 1);
-    }
+    TRY(pc_launch_fields(run, 3, Y, X, run->E1[1], nullptr));
     run->fcur = 1 - run->fcur;
     for (int c = 0; c < run->p.n_cold; ++c)
         run->cold[c].cur = 1 - run->cold[c].cur;
@@ -1031,7 +1035,8 @@ struct h1d_batch {
     int                        since_block = 1 << 30;
     int                        L = 0, nblocks = 0;
     size_t                     smem = 0;
-    FieldArgs                 *d_table = nullptr; // [2][runs]: state parity 0 and 1
+    bool                       pc = false;        // predictor-corrector members (else CAM-CL)
+    FieldArgs                 *d_table = nullptr; // CAM-CL: [parity][runs]; PC: [phase 1-3][parity][runs]
     FieldBlock                *d_map = nullptr;
     int                        parity = 0;
     cudaGraph_t                graph = nullptr;
@@ -1106,7 +1111,7 @@ int build_field_tables(h1d_batch *b)
     int L = FIELD_BLOCK_MIN;
     for (h1d_run const *r : b->runs)
         L = std::max(L, r->L);
-    std::vector<FieldArgs>  tab(2 * b->runs.size());
+    std::vector<FieldArgs>  tab((b->pc ? 6 : 2) * b->runs.size());
     std::vector<FieldBlock> map;
     for (size_t i = 0; i < b->runs.size(); ++i) {
         h1d_run *r   = b->runs[i];
@@ -1115,19 +1120,31 @@ int build_field_tables(h1d_batch *b)
         for (int blk = 0; blk < nb; ++blk)
             map.push_back({ static_cast<int>(i), blk });
         for (int par = 0; par < 2; ++par) {
-            if (par) { // the state after one step
-                r->fcur ^= 1, r->dset ^= 1;
+            auto const flip = [&] { // the state after one step (a PC step keeps its deposit sets)
+                r->fcur ^= 1;
+                if (!b->pc)
+                    r->dset ^= 1;
                 for (int c = 0; c < r->p.n_cold; ++c)
                     r->cold[c].cur ^= 1;
+            };
+            if (par)
+                flip();
+            if (b->pc) { // the three field phases of pc_step
+                int const X = r->dset, Y = 1 - X;
+                FieldArgs ph[3] = { pc_field_args(r, 1, X, X, nullptr, r->E1[0]),
+                                    pc_field_args(r, 2, X, Y, r->E1[0], r->E1[1]),
+                                    pc_field_args(r, 3, Y, X, r->E1[1], nullptr) };
+                for (int f = 0; f < 3; ++f) {
+                    ph[f].seg = seg;
+                    tab[(f * 2 + par) * b->runs.size() + i] = ph[f];
+                }
+            } else {
+                FieldArgs a = field_args(r);
+                a.seg       = seg;
+                tab[par * b->runs.size() + i] = a;
             }
-            FieldArgs a = field_args(r);
-            a.seg       = seg;
-            tab[par * b->runs.size() + i] = a;
-            if (par) {
-                r->fcur ^= 1, r->dset ^= 1;
-                for (int c = 0; c < r->p.n_cold; ++c)
-                    r->cold[c].cur ^= 1;
-            }
+            if (par)
+                flip();
         }
     }
     size_t const smem = sizeof(double) * static_cast<size_t>(L) * (SMEM_SCALARS + 3 * SMEM_VECTORS);
@@ -1146,8 +1163,8 @@ int build_field_tables(h1d_batch *b)
     return H1D_OK;
 }
 
-// one CAM-CL step of every member (sorting all groups first at a block start)
-int batch_step(h1d_batch *b)
+// sort every group at the start of a block of b->k steps
+int batch_sort_block(h1d_batch *b)
 {
     if (b->since_block >= b->k) {
         for (h1d_run *r : b->runs)
@@ -1157,7 +1174,13 @@ int batch_step(h1d_batch *b)
             }
         b->since_block = 0;
     }
-    // particle pass: one launch per kind of group
+    return H1D_OK;
+}
+
+// one particle pass of every member: one launch per kind of group, and one per species whose
+// weights evolve; `pass` < 0 is the CAM-CL pass, else the predictor-corrector pass of pc_pass_args
+int batch_push(h1d_batch *b, int pass)
+{
     struct Kind {
         int  order, bc;
         bool mirror, mixed;
@@ -1173,8 +1196,10 @@ int batch_step(h1d_batch *b)
         for (int s = 0; s < r->p.n_kinetic; ++s) {
             if (r->sp[s].n == 0)
                 continue;
+            int const      X = r->dset;
+            PushArgs const a = pass < 0 ? push_args(r, s) : pc_pass_args(r, s, pass, pass == 1 ? 1 - X : X);
             if (evolves_psd(r->p.kinetic[s])) { // the weight-evolving pass, one species per launch
-                BTRY(r, launch_push(r, s, push_args(r, s)));
+                BTRY(r, launch_push(r, s, a));
                 b->stats.kernel_launches += 1;
                 continue;
             }
@@ -1184,7 +1209,6 @@ int batch_step(h1d_batch *b)
                 ++ki;
             if (ki == kinds.size())
                 kinds.push_back(kd), fp.emplace_back(), mx.emplace_back();
-            PushArgs const a = push_args(r, s);
             if (kd.mixed)
                 mx[ki].push_back(mixed_args(r, s, a));
             else
@@ -1202,17 +1226,16 @@ int batch_step(h1d_batch *b)
         size_t const groups = kd.mixed ? mx[ki].size() : fp[ki].size();
         b->stats.kernel_launches += static_cast<int64_t>((groups + BATCH_GROUPS - 1) / BATCH_GROUPS);
     }
-    // external sources of the members that have them, then the field cycle of every member
-    for (h1d_run *r : b->runs)
-        if (r->p.n_sources > 0) {
-            BTRY(r, launch_run_sources(r, static_cast<double>(r->step) * r->p.dt + 0.5 * r->p.dt));
-            b->stats.kernel_launches += 1;
-        }
-    BCU(launch_camcl_fields_batch(b->d_table + b->parity * b->runs.size(), b->d_map, b->nblocks, b->L, b->smem,
-                                  b->stream));
-    b->stats.kernel_launches += 1;
+    return H1D_OK;
+}
+
+// the host side of one step of every member
+void batch_step_done(h1d_batch *b)
+{
     for (h1d_run *r : b->runs) {
-        r->fcur ^= 1, r->dset ^= 1;
+        r->fcur ^= 1;
+        if (!b->pc)
+            r->dset ^= 1;
         for (int c = 0; c < r->p.n_cold; ++c)
             r->cold[c].cur ^= 1;
         for (int s = 0; s < r->p.n_kinetic; ++s)
@@ -1223,6 +1246,47 @@ int batch_step(h1d_batch *b)
     b->parity ^= 1;
     b->since_block++;
     b->stats.steps++;
+}
+
+// one Domain_PC::cycle of every member (pc_step): three batched field phases around the predictor
+// and corrector particle passes
+int batch_step_pc(h1d_batch *b)
+{
+    TRY(batch_sort_block(b));
+    size_t const R     = b->runs.size();
+    auto const   table = [&](int phase) { return b->d_table + ((phase - 1) * 2 + b->parity) * R; };
+    BCU(launch_pc_fields_batch(table(1), b->d_map, b->nblocks, b->L, b->smem, b->stream));
+    TRY(batch_push(b, 0));
+    for (h1d_run *r : b->runs)
+        if (r->p.n_sources > 0) {
+            BTRY(r, launch_run_sources(r, static_cast<double>(r->step) * r->p.dt + r->p.dt));
+            b->stats.kernel_launches += 1;
+        }
+    BCU(launch_pc_fields_batch(table(2), b->d_map, b->nblocks, b->L, b->smem, b->stream));
+    TRY(batch_push(b, 1));
+    BCU(launch_pc_fields_batch(table(3), b->d_map, b->nblocks, b->L, b->smem, b->stream));
+    b->stats.kernel_launches += 3;
+    batch_step_done(b);
+    return H1D_OK;
+}
+
+// one CAM-CL step of every member (sorting all groups first at a block start)
+int batch_step(h1d_batch *b)
+{
+    if (b->pc)
+        return batch_step_pc(b);
+    TRY(batch_sort_block(b));
+    TRY(batch_push(b, -1));
+    // external sources of the members that have them, then the field cycle of every member
+    for (h1d_run *r : b->runs)
+        if (r->p.n_sources > 0) {
+            BTRY(r, launch_run_sources(r, static_cast<double>(r->step) * r->p.dt + 0.5 * r->p.dt));
+            b->stats.kernel_launches += 1;
+        }
+    BCU(launch_camcl_fields_batch(b->d_table + b->parity * b->runs.size(), b->d_map, b->nblocks, b->L, b->smem,
+                                  b->stream));
+    b->stats.kernel_launches += 1;
+    batch_step_done(b);
     return H1D_OK;
 }
 
@@ -1230,10 +1294,13 @@ int batch_step(h1d_batch *b)
 int batch_prepare(h1d_batch *b)
 {
     for (h1d_run *r : b->runs) {
-        if (!r->recurring || r->fields_dirty) {
+        bool const first = !r->recurring;
+        if (first || r->fields_dirty) {
             BTRY(r, prepare_fields(r));
             b->stats.kernel_launches += 1;
         }
+        if (first && r->p.algorithm == H1D_ALGO_PC) // Domain_PC::advance_by's initial sources
+            BTRY(r, pc_initial_sources(r));
         r->recurring = true;
     }
     return H1D_OK;
@@ -1969,7 +2036,7 @@ int h1d_batch_create(h1d_run *const *runs, int n_runs, h1d_batch **out)
     for (int i = 0; i < n_runs; ++i) {
         h1d_run *r = runs[i];
         char const *why = !r ? "null run"
-                          : r->p.algorithm != H1D_ALGO_CAMCL ? "batches advance CAM-CL runs only"
+                          : r->p.algorithm != runs[0]->p.algorithm ? "members advance by one algorithm (all CAM-CL or all PC)"
                           : r->device != dev                ? "run lives on another device"
                           : r->batch_count                  ? "run is already a member of a batch"
                                                             : nullptr;
@@ -1985,6 +2052,7 @@ int h1d_batch_create(h1d_run *const *runs, int n_runs, h1d_batch **out)
     if (!b)
         return H1D_ERR_OOM;
     b->device = dev;
+    b->pc     = runs[0]->p.algorithm == H1D_ALGO_PC;
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete b;
         return H1D_ERR_CUDA;

@@ -332,11 +332,12 @@ int h1d_configure(h1d_run *run, int sort_interval, int push_ctas_per_sm);
 int h1d_autotune(h1d_run *run, uint32_t *steps_taken, int *sort_interval, int *push_ctas_per_sm);
 
 /* ---- Ensembles (no counterpart in the reference) ---------------------------------------------
- * A batch advances many CAM-CL runs together on one stream of the current device.  A step is one
- * launch of the particle pass per kind of particle group (shape order, geometry, boundary,
- * precision) covering every species of every member (a species with evolving weights, delta-f or
- * PSD refresh, takes a launch of its own), and one launch of the field cycle covering every
- * member's grid.  Steps come in blocks of sort_interval steps, all groups cell-sorted at the
+ * A batch advances many runs of one algorithm together on one stream of the current device: all
+ * CAM-CL, or all predictor-corrector.  A CAM-CL step is one launch of the particle pass per kind
+ * of particle group (shape order, geometry, boundary, precision) covering every species of every
+ * member (a species with evolving weights, delta-f or PSD refresh, takes a launch of its own), and
+ * one launch of the field cycle covering every member's grid; a predictor-corrector step is three
+ * such field launches (Domain_PC.cc:79-205) around the predictor and the corrector particle passes.  Steps come in blocks of sort_interval steps, all groups cell-sorted at the
  * start of a block.  When no member uses absorbing particles or gyrophase randomization, a pair of
  * blocks is captured once as a CUDA graph and replayed while the members are unchanged (an upload
  * to a member invalidates it).  Members stay owned by the caller, must outlive the batch and

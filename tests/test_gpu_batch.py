@@ -83,10 +83,6 @@ def test_batch_without_graphs_equals_with_graphs(gpu_lib):
 
 
 def test_batch_rejects_bad_members(gpu_lib):
-    pc = h.configs.parity_p4()
-    with h.Run(pc, gpu_lib) as r:
-        with pytest.raises(h.H1DError):
-            h.abi.Batch([r])
     c = h.configs.parity_p1()
     with h.Run(c, gpu_lib) as r:
         with pytest.raises(h.H1DError):
@@ -191,3 +187,80 @@ def test_batch_with_evolving_weights(gpu_lib, precision, tol):
         assert any(k.endswith("real_f") for k in errs) or not any(k.has_psd for k in c.kinetic)
         bad = {k: v for k, v in errs.items() if not v <= tol}
         assert not bad, (c.name, bad)
+
+
+def _fixture_members(names, precision):
+    import os
+
+    from parity_util import with_reference_norms
+    from state_io import read_state
+
+    golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    states = [read_state(os.path.join(golden, f"{n}.init.bin")) for n in names]
+    return [with_reference_norms(h.configs.PARITY[n](), st).replace(precision=precision)
+            for n, st in zip(names, states)], states
+
+
+def _alone_and_together(gpu_lib, cfgs, states, steps, chunks=(3,)):
+    alone = []
+    for c, st in zip(cfgs, states):
+        with h.Run(c, gpu_lib) as r:
+            h.abi.configure(r, sort_interval=4)
+            r.upload_state(st)
+            r.advance(steps)
+            alone.append(r.state())
+    runs = [h.Run(c, gpu_lib) for c in cfgs]
+    try:
+        for r, st in zip(runs, states):
+            h.abi.configure(r, sort_interval=4)
+            r.upload_state(st)
+        with h.abi.Batch(runs) as b:
+            b.configure(sort_interval=4)
+            done = 0
+            for k in chunks:
+                b.advance(k)
+                done += k
+            b.advance(steps - done)
+            stats = b.stats()
+            together = [r.state() for r in runs]
+    finally:
+        for r in runs:
+            r.close()
+    return alone, together, stats
+
+
+@pytest.mark.parametrize("precision,tol", [(h.configs.PREC_FP64, 1e-10), (h.configs.PREC_MIXED, 1e-4)])
+def test_pc_batch_members_match_runs_alone(gpu_lib, precision, tol):
+    """Predictor-corrector members (TSC mirror reflecting, delta-f periodic, partial-shell delta-f):
+    40 batch steps with CUDA-graph replays equal each run alone (Domain_PC::advance_by)."""
+    names = ["p4_pc_tsc_mirror_reflecting", "p8_pc_psd_periodic", "p10_pc_shell_psd_mirror"]
+    cfgs, states = _fixture_members(names, precision)
+    alone, together, stats = _alone_and_together(gpu_lib, cfgs, states, 40)
+    assert stats["steps"] == 40 and stats["graph_launches"] >= 2
+    for c, a, t in zip(cfgs, alone, together):
+        errs = state_errors(t, a, c)
+        bad = {k: v for k, v in errs.items() if not v <= tol}
+        assert not bad, (c.name, bad)
+
+
+def test_pc_batch_with_external_source(gpu_lib):
+    """A predictor-corrector member with an antenna current (its source times change every step,
+    so the batch runs eagerly) beside a plain one."""
+    names = ["p6_pc_source", "p4_pc_tsc_mirror_reflecting"]
+    cfgs, states = _fixture_members(names, h.configs.PREC_FP64)
+    alone, together, stats = _alone_and_together(gpu_lib, cfgs, states, 12)
+    assert stats["graph_launches"] == 0
+    for c, a, t in zip(cfgs, alone, together):
+        errs = state_errors(t, a, c)
+        bad = {k: v for k, v in errs.items() if not v <= 1e-10}
+        assert not bad, (c.name, bad)
+
+
+def test_batch_members_share_one_algorithm(gpu_lib):
+    a = h.Run(h.configs.parity_p2(), gpu_lib)
+    c = h.Run(h.configs.parity_p4(), gpu_lib)
+    try:
+        with pytest.raises(h.H1DError):
+            h.abi.Batch([a, c])
+    finally:
+        a.close(), c.close()
