@@ -2353,7 +2353,7 @@ struct h1d_server {
     std::deque<ServerReq *>               queue;
     std::vector<ServerReq *>              active;
     std::map<uint64_t, ServerReq *>       all;
-    h1d_batch                            *batch = nullptr;
+    h1d_batch                            *batch[2] = { nullptr, nullptr }; // the active runs by algorithm (H1D_ALGO_*)
     bool                                  dirty = false;
     uint64_t                              next_id = 1;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
@@ -2365,15 +2365,20 @@ struct h1d_server {
 
 namespace {
 
-void fold_batch_stats(h1d_server *sv)
+// fold the statistics of the server's batches into its own and destroy them (the active runs stay)
+void drop_batches(h1d_server *sv)
 {
-    if (!sv->batch)
-        return;
-    h1d_batch_stats st{};
-    h1d_batch_stats_read(sv->batch, &st);
-    sv->stats.kernel_launches += st.kernel_launches;
-    sv->stats.graph_launches += st.graph_launches;
-    sv->stats.steps += st.steps;
+    for (h1d_batch *&b : sv->batch) {
+        if (!b)
+            continue;
+        h1d_batch_stats st{};
+        h1d_batch_stats_read(b, &st);
+        sv->stats.kernel_launches += st.kernel_launches;
+        sv->stats.graph_launches += st.graph_launches;
+        sv->stats.steps += st.steps;
+        h1d_batch_destroy(b);
+        b = nullptr;
+    }
 }
 
 void finish_request(h1d_server *sv, ServerReq *r, int status, std::string const &msg)
@@ -2473,7 +2478,7 @@ int h1d_server_submit(h1d_server *sv, h1d_request const *rq, uint64_t *id)
         std::fprintf(stderr, "h1d_server_submit: %s\n", m.c_str());
         return st;
     }
-    if (rq->params.algorithm != H1D_ALGO_CAMCL || rq->n_steps == 0)
+    if (rq->n_steps == 0)
         return H1D_ERR_INVALID_ARG;
     for (int s = 0; s < rq->params.n_kinetic; ++s) // built by h1d_populate: bi-Maxwellian, full-f
         if (rq->n_particles[s] < 0 || rq->n_particles[s] > (int64_t{ 1 } << 31) - 1 || !(rq->beta1[s] > 0)
@@ -2526,45 +2531,59 @@ int h1d_server_tick(h1d_server *sv, int *n_active, int *n_queued)
         sv->stats.admitted++;
         sv->dirty = true;
     }
-    // 2. the batch of the active runs
+    // 2. the batches of the active runs, one per algorithm
     if (sv->dirty) {
-        fold_batch_stats(sv);
-        h1d_batch_destroy(sv->batch);
-        sv->batch = nullptr;
-        if (!sv->active.empty()) {
+        drop_batches(sv);
+        for (int alg = 0; alg < 2; ++alg) {
             std::vector<h1d_run *> runs;
             for (ServerReq *r : sv->active)
-                runs.push_back(r->run);
-            int st = h1d_batch_create(runs.data(), static_cast<int>(runs.size()), &sv->batch);
+                if (r->rq.params.algorithm == alg)
+                    runs.push_back(r->run);
+            if (runs.empty())
+                continue;
+            int st = h1d_batch_create(runs.data(), static_cast<int>(runs.size()), &sv->batch[alg]);
             if (st == H1D_OK)
-                st = h1d_batch_configure(sv->batch, sv->sort_interval, 0, 1);
+                st = h1d_batch_configure(sv->batch[alg], sv->sort_interval, 0, 1);
             if (st != H1D_OK) {
-                for (ServerReq *r : sv->active)
-                    finish_request(sv, r, st, "batch creation failed");
-                sv->active.clear();
-                h1d_batch_destroy(sv->batch);
-                sv->batch = nullptr;
+                h1d_batch_destroy(sv->batch[alg]);
+                sv->batch[alg] = nullptr;
+                for (auto it = sv->active.begin(); it != sv->active.end();)
+                    if ((*it)->rq.params.algorithm == alg) {
+                        finish_request(sv, *it, st, "batch creation failed");
+                        it = sv->active.erase(it);
+                    } else {
+                        ++it;
+                    }
             }
         }
         sv->dirty = false;
         sv->stats.batches_built++;
     }
-    // 3. one quantum (or up to the nearest completion)
-    if (sv->batch) {
-        uint32_t q = static_cast<uint32_t>(sv->quantum);
-        for (ServerReq *r : sv->active)
-            q = std::min(q, r->rq.n_steps - r->done_steps);
-        int const st = h1d_batch_advance(sv->batch, q);
-        if (st != H1D_OK) { // a member failed: fail every member of the batch
-            std::string const m = h1d_batch_status_string(sv->batch);
-            h1d_batch_destroy(sv->batch);
-            sv->batch = nullptr;
-            for (ServerReq *r : sv->active)
-                finish_request(sv, r, st, m);
-            sv->active.clear();
-        } else {
-            for (ServerReq *r : sv->active)
+    // 3. one quantum (or up to the nearest completion) of every batch
+    uint32_t q = static_cast<uint32_t>(sv->quantum);
+    for (ServerReq *r : sv->active)
+        q = std::min(q, r->rq.n_steps - r->done_steps);
+    for (int alg = 0; alg < 2; ++alg) {
+        if (!sv->batch[alg])
+            continue;
+        int const   st = h1d_batch_advance(sv->batch[alg], q);
+        std::string m;
+        if (st != H1D_OK) { // a member failed: the batch goes (before its runs are freed), then every member
+            m = h1d_batch_status_string(sv->batch[alg]);
+            h1d_batch_destroy(sv->batch[alg]);
+            sv->batch[alg] = nullptr;
+        }
+        for (auto it = sv->active.begin(); it != sv->active.end();) {
+            ServerReq *r = *it;
+            if (r->rq.params.algorithm != alg) {
+                ++it;
+            } else if (st == H1D_OK) {
                 r->done_steps += q;
+                ++it;
+            } else {
+                finish_request(sv, r, st, m);
+                it = sv->active.erase(it);
+            }
         }
     }
     // 4. retire finished runs
@@ -2574,10 +2593,8 @@ int h1d_server_tick(h1d_server *sv, int *n_active, int *n_queued)
             ++it;
             continue;
         }
-        if (sv->batch) { // the run leaves the batch before it is read and freed
-            fold_batch_stats(sv);
-            h1d_batch_destroy(sv->batch);
-            sv->batch = nullptr;
+        if (sv->batch[r->rq.params.algorithm]) { // the run leaves the batches before it is read and freed
+            drop_batches(sv);
             sv->dirty = true;
         }
         int const st = collect(r);
@@ -2652,11 +2669,12 @@ int h1d_server_stats_read(h1d_server *sv, h1d_server_stats *out)
         return H1D_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lock(sv->mu);
     *out = sv->stats;
-    if (sv->batch) {
-        h1d_batch_stats st{};
-        h1d_batch_stats_read(sv->batch, &st);
-        out->kernel_launches += st.kernel_launches, out->graph_launches += st.graph_launches, out->steps += st.steps;
-    }
+    for (h1d_batch *b : sv->batch)
+        if (b) {
+            h1d_batch_stats st{};
+            h1d_batch_stats_read(b, &st);
+            out->kernel_launches += st.kernel_launches, out->graph_launches += st.graph_launches, out->steps += st.steps;
+        }
     out->bytes_in_use = static_cast<int64_t>(sv->used);
     out->peak_bytes   = static_cast<int64_t>(sv->peak);
     return H1D_OK;
@@ -2666,7 +2684,7 @@ int h1d_server_destroy(h1d_server *sv)
 {
     if (!sv)
         return H1D_OK;
-    h1d_batch_destroy(sv->batch);
+    drop_batches(sv);
     for (auto &[id, r] : sv->all) {
         if (r->run)
             h1d_destroy(r->run);

@@ -373,7 +373,7 @@ const char *h1d_batch_status_string(h1d_batch *batch);
  * from other threads.  Times are seconds since h1d_server_create on a monotonic clock. */
 typedef struct h1d_server h1d_server;
 typedef struct h1d_request {
-    h1d_params params;                    /* a CAM-CL run */
+    h1d_params params;                    /* a CAM-CL or predictor-corrector run */
     double     beta1[H1D_MAX_KINETIC];    /* loader of each kinetic species: parallel beta */
     double     T2_T1[H1D_MAX_KINETIC];    /* and T_perp / T_par */
     int64_t    n_particles[H1D_MAX_KINETIC];

@@ -71,6 +71,26 @@ def test_served_equals_direct_run(gpu_lib):
     assert rel_err(res["n"][0], n) <= 1e-10 and rel_err(res["nvv"][0], nvv) <= 1e-10
 
 
+def test_predictor_corrector_requests(gpu_lib):
+    """Predictor-corrector requests are served beside CAM-CL ones (one batch per algorithm) and
+    equal the same runs driven directly (Domain_PC::advance_by)."""
+    pc = [_cfg(s, h.configs.PREC_FP64).replace(algorithm=h.configs.ALGO_PC) for s in (7, 8)]
+    with h.abi.Server(gpu_lib, 8 * GB, steps_per_tick=16, sort_interval=16) as sv:
+        ids = [sv.submit(c, seed=s, n_steps=n) for c, s, n in zip(pc, (7, 8), (48, 80))]
+        ids.append(sv.submit(_cfg(9, h.configs.PREC_FP64), seed=9, n_steps=64))
+        _drain(sv, ids)
+        res = [sv.result(i) for i in ids[:2]]
+        assert sv.stats()["completed"] == 3 and sv.stats()["failed"] == 0
+    for c, s, n, got in zip(pc, (7, 8), (48, 80), res):
+        with h.Run(c.replace(sort_interval=16), gpu_lib) as r:
+            h.abi.populate_state(r, seed=s)
+            r.advance(n)
+            B, E = r.fields()
+            nn, _, nvv = r.moments(0)
+        assert rel_err(got["B"], B) <= 1e-10 and rel_err(got["E"], E) <= 1e-10
+        assert rel_err(got["n"][0], nn) <= 1e-10 and rel_err(got["nvv"][0], nvv) <= 1e-10
+
+
 def test_admission_respects_budget(gpu_lib):
     """A budget that holds the two largest requests but not three: the server never exceeds it,
     never runs all six together, and finishes them all."""
