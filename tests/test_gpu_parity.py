@@ -129,6 +129,33 @@ def test_absorbing_boundary(gpu_lib, oracle_lib):
     assert not bad, bad
 
 
+@pytest.mark.parametrize("precision,tol", [(h.configs.PREC_FP64, 1e-11), (h.configs.PREC_MIXED, 1e-4)])
+def test_empty_and_ragged_species(gpu_lib, oracle_lib, precision, tol):
+    """Particle counts at the edges of the pass's tiling (a 256-particle chunk of 4 warps x 32
+    lanes x 2 particles, the mixed pass's lane pairs, the 4-wide vector tiles of collect_all):
+    no particles, one, a pair, a warp minus and plus one, a chunk minus and plus one; five steps
+    against the oracle."""
+    import copy
+
+    cfg = h.configs.parity_p2().replace(precision=precision)
+    init = read_state(os.path.join(GOLDEN, f"{cfg.name}.init.bin"))
+    for k in (0, 1, 2, 31, 33, 255, 257, 1023):
+        st = copy.deepcopy(init)
+        st["particles"][0] = {key: v[:k] for key, v in st["particles"][0].items()}
+        with h.Run(cfg, gpu_lib, "h1d_") as g, h.Run(cfg.replace(precision=h.configs.PREC_FP64), oracle_lib, "orc_") as c:
+            g.upload_state(st)
+            c.upload_state(st)
+            g.advance(5)
+            c.advance(5)
+            sg, sc = g.state(), c.state()
+        assert sg["particles"][0]["q1"].size == k
+        errs = state_errors(sg, sc, cfg)
+        if k == 0:
+            assert not np.any(sg["moments"][0]["n"])
+        bad = {key: v for key, v in errs.items() if not v <= tol}
+        assert not bad, (k, bad)
+
+
 def test_test_particles(gpu_lib, oracle_lib):
     """Test particles (TestParticleVDF, VDF/TestParticleVDF.cc:15-24: weight 0, f0 = 0) run as a
     full-f species without refresh: they are pushed and moved like the oracle's, and deposit
