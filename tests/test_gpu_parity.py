@@ -156,6 +156,28 @@ def test_empty_and_ragged_species(gpu_lib, oracle_lib, precision, tol):
         assert not bad, (k, bad)
 
 
+@pytest.mark.parametrize("precision,tol", [(h.configs.PREC_FP64, 1e-11), (h.configs.PREC_MIXED, 1e-4)])
+def test_largest_grid(gpu_lib, oracle_lib, precision, tol):
+    """A grid near the C ABI's largest (Nx = 65534 cells: 16-bit sort keys in two 8-bit passes,
+    hundreds of field-kernel blocks, a mirror field near its validity limit), two TSC species of
+    2 particles per cell, three steps against the oracle."""
+    from hfemic_b200.loader import initial_state
+
+    cfg = h.configs.parity_p2().replace(Nx=65534, xi=4e-5, phase_retardation=(512, 1.0),
+                                       amplitude_damping=(512, 0.2), precision=precision)
+    for k in cfg.kinetic:
+        k.Nc = 2
+    init = initial_state(cfg, seed=21)
+    with h.Run(cfg, gpu_lib, "h1d_") as g, h.Run(cfg.replace(precision=h.configs.PREC_FP64), oracle_lib, "orc_") as c:
+        g.upload_state(init)
+        c.upload_state(init)
+        g.advance(3)
+        c.advance(3)
+        errs = state_errors(g.state(), c.state(), cfg)
+    bad = {k: v for k, v in errs.items() if not v <= tol}
+    assert not bad, bad
+
+
 def test_test_particles(gpu_lib, oracle_lib):
     """Test particles (TestParticleVDF, VDF/TestParticleVDF.cc:15-24: weight 0, f0 = 0) run as a
     full-f species without refresh: they are pushed and moved like the oracle's, and deposit
