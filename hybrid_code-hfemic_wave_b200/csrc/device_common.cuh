@@ -192,6 +192,17 @@ __host__ __device__ inline uint64_t mix64(uint64_t z)
     z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
     return z ^ (z >> 31);
 }
+// sin and cos of an angle in [-pi, pi) (a gyrophase): one half-turn brought onto |x| <= pi/2 for
+// sincos_taylor, so the particle pass carries no general range reduction
+__device__ __forceinline__ void sincos_half_turn(double x, double &s, double &c)
+{
+    constexpr double PI   = 3.141592653589793;
+    bool const       flip = fabs(x) > 0.5 * PI;
+    sincos_taylor(flip ? x - copysign(PI, x) : x, s, c);
+    if (flip)
+        s = -s, c = -c;
+}
+
 __host__ __device__ inline double gyrophase(uint64_t seed, uint64_t counter, uint64_t species, uint64_t pid)
 {
     uint64_t h = mix64(seed + 0x9e3779b97f4a7c15ULL);

@@ -98,7 +98,7 @@ __device__ __forceinline__ bool boundary(PushArgs const &a, double &q1, d3 &v, i
             v.x = v.x - 2 * v.x; // v -= 2 (v.e1) e1 with e1 = x^
             if (a.randomize) {
                 double s, c;
-                sincos(gyrophase(a.seed, counter, (uint64_t)a.species, (uint64_t)pid), &s, &c);
+                sincos_half_turn(gyrophase(a.seed, counter, (uint64_t)a.species, (uint64_t)pid), s, c);
                 double const vy = v.y, vz = v.z;
                 v.y = vy * c - vz * s;
                 v.z = vy * s + vz * c;

@@ -177,7 +177,11 @@ __device__ __forceinline__ bool boundary_mixed(PushArgsMixed const &a, int &cell
             v.x = -v.x;
             if (a.randomize) {
                 float s, c;
-                sincosf(static_cast<float>(gyrophase(a.seed, counter, (uint64_t)a.species, (uint64_t)pid)), &s, &c);
+                float const x    = static_cast<float>(gyrophase(a.seed, counter, (uint64_t)a.species, (uint64_t)pid));
+                bool const  flip = fabsf(x) > 1.5707963f; // one half-turn onto |x| <= pi/2 for the series
+                sincos_taylor_f(flip ? x - copysignf(3.14159265f, x) : x, s, c);
+                if (flip)
+                    s = -s, c = -c;
                 float const vy = v.y, vz = v.z;
                 v.y = vy * c - vz * s;
                 v.z = vy * s + vz * c;

@@ -178,6 +178,22 @@ def test_largest_grid(gpu_lib, oracle_lib, precision, tol):
     assert not bad, bad
 
 
+@pytest.mark.parametrize("name", ["p2_tsc_mirror_reflecting", "p4_pc_tsc_mirror_reflecting"])
+def test_gyrophase_randomization(gpu_lib, oracle_lib, name):
+    """Reflected particles with their gyrophase randomised (Delegate::randomize_gyrophase,
+    Boundary/Delegate.cc:146-156; the angle from a counter-based hash of seed, step, species and
+    particle id instead of std::random_device): ten steps against the oracle's same draws."""
+    cfg = h.configs.PARITY[name]().replace(randomize_gyrophase=True, gyrophase_seed=12345)
+    init = read_state(os.path.join(GOLDEN, f"{name}.init.bin"))
+    g, c, _, _ = run_both(cfg, init, 5, gpu_lib, oracle_lib, chunks=2)
+    errs = state_errors(g, c, cfg)
+    bad = {k: v for k, v in errs.items() if not v <= TOL10}
+    assert not bad, bad
+    # the randomisation acted: the same run without it differs
+    g0, _, _, _ = run_both(cfg.replace(randomize_gyrophase=False), init, 5, gpu_lib, oracle_lib, chunks=2)
+    assert rel_err(by_pid(g["particles"][0])["vy"], by_pid(g0["particles"][0])["vy"]) > 1e-3
+
+
 def test_test_particles(gpu_lib, oracle_lib):
     """Test particles (TestParticleVDF, VDF/TestParticleVDF.cc:15-24: weight 0, f0 = 0) run as a
     full-f species without refresh: they are pushed and moved like the oracle's, and deposit
