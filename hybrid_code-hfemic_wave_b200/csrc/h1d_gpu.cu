@@ -731,15 +731,57 @@ int launch_run_sources(h1d_run *run, double t)
     return H1D_OK;
 }
 
+// the CAM-CL particle pass of every species of a run: species of one shape order whose weights do
+// not evolve share one launch, as the groups of a batch do
+int push_run(h1d_run *run)
+{
+    h1d_params const &p = run->p;
+    int const         K = p.n_kinetic;
+    bool              done[H1D_MAX_KINETIC] = {};
+    for (int s = 0; s < K; ++s) {
+        if (done[s])
+            continue;
+        int grp[H1D_MAX_KINETIC], m = 0;
+        grp[m++] = s;
+        done[s]  = true;
+        if (!evolves_psd(p.kinetic[s]) && run->sp[s].n > 0)
+            for (int t = s + 1; t < K; ++t)
+                if (!done[t] && run->sp[t].n > 0 && !evolves_psd(p.kinetic[t]) && p.kinetic[t].shape_order == p.kinetic[s].shape_order)
+                    grp[m++] = t, done[t] = true;
+        phase_begin(run, 0);
+        if (m == 1) {
+            TRY(launch_push(run, s, push_args(run, s)));
+        } else {
+            int const  order  = static_cast<int>(p.kinetic[s].shape_order);
+            bool const mirror = p.xi != 0;
+            if (run->mixed) {
+                PushArgsMixed g[H1D_MAX_KINETIC];
+                for (int i = 0; i < m; ++i)
+                    g[i] = mixed_args(run, grp[i], push_args(run, grp[i]));
+                CU(launch_push_groups(g, m, order, mirror, p.particle_bc,
+                                      run->num_sms * (run->ctas_per_sm ? run->ctas_per_sm : PIPE_CTAS_PER_SM_MIXED), run->stream));
+            } else {
+                PushArgs g[H1D_MAX_KINETIC];
+                for (int i = 0; i < m; ++i)
+                    g[i] = push_args(run, grp[i]);
+                CU(launch_push_groups(g, m, order, mirror, p.particle_bc,
+                                      run->num_sms * (run->ctas_per_sm ? std::min(run->ctas_per_sm, PIPE_CTAS_PER_SM) : PIPE_CTAS_PER_SM),
+                                      run->stream));
+            }
+        }
+        phase_end(run, run->sp[s].n > 0 ? 1 : 0);
+    }
+    return H1D_OK;
+}
+
 int camcl_step(h1d_run *run)
 {
     h1d_params const &p = run->p;
-    for (int s = 0; s < p.n_kinetic; ++s) {
+    for (int s = 0; s < p.n_kinetic; ++s)
         if (run->sp[s].since_sort >= run->sort_interval)
             TRY(sort_species(run, s));
-        phase_begin(run, 0);
-        TRY(launch_push(run, s, push_args(run, s)));
-        phase_end(run, run->sp[s].n > 0 ? 1 : 0);
+    TRY(push_run(run));
+    for (int s = 0; s < p.n_kinetic; ++s) {
         if (run->profiling)
             run->prof.particles_pushed += run->sp[s].n;
         run->sp[s].since_sort++;
