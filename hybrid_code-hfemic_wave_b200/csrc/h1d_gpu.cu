@@ -731,9 +731,10 @@ int launch_run_sources(h1d_run *run, double t)
     return H1D_OK;
 }
 
-// the CAM-CL particle pass of every species of a run: species of one shape order whose weights do
-// not evolve share one launch, as the groups of a batch do
-int push_run(h1d_run *run)
+// a particle pass of every species of a run with the arguments args_of(s): species of one shape
+// order whose weights do not evolve share one launch, as the groups of a batch do
+template <class ArgsOf>
+int push_run(h1d_run *run, ArgsOf const &args_of)
 {
     h1d_params const &p = run->p;
     int const         K = p.n_kinetic;
@@ -750,20 +751,20 @@ int push_run(h1d_run *run)
                     grp[m++] = t, done[t] = true;
         phase_begin(run, 0);
         if (m == 1) {
-            TRY(launch_push(run, s, push_args(run, s)));
+            TRY(launch_push(run, s, args_of(s)));
         } else {
             int const  order  = static_cast<int>(p.kinetic[s].shape_order);
             bool const mirror = p.xi != 0;
             if (run->mixed) {
                 PushArgsMixed g[H1D_MAX_KINETIC];
                 for (int i = 0; i < m; ++i)
-                    g[i] = mixed_args(run, grp[i], push_args(run, grp[i]));
+                    g[i] = mixed_args(run, grp[i], args_of(grp[i]));
                 CU(launch_push_groups(g, m, order, mirror, p.particle_bc,
                                       run->num_sms * (run->ctas_per_sm ? run->ctas_per_sm : PIPE_CTAS_PER_SM_MIXED), run->stream));
             } else {
                 PushArgs g[H1D_MAX_KINETIC];
                 for (int i = 0; i < m; ++i)
-                    g[i] = push_args(run, grp[i]);
+                    g[i] = args_of(grp[i]);
                 CU(launch_push_groups(g, m, order, mirror, p.particle_bc,
                                       run->num_sms * (run->ctas_per_sm ? std::min(run->ctas_per_sm, PIPE_CTAS_PER_SM) : PIPE_CTAS_PER_SM),
                                       run->stream));
@@ -780,7 +781,7 @@ int camcl_step(h1d_run *run)
     for (int s = 0; s < p.n_kinetic; ++s)
         if (run->sp[s].since_sort >= run->sort_interval)
             TRY(sort_species(run, s));
-    TRY(push_run(run));
+    TRY(push_run(run, [run](int s) { return push_args(run, s); }));
     for (int s = 0; s < p.n_kinetic; ++s) {
         if (run->profiling)
             run->prof.particles_pushed += run->sp[s].n;
@@ -851,13 +852,11 @@ PushArgs pc_pass_args(h1d_run *run, int s, int pass, int dep_set)
 
 int pc_particles(h1d_run *run, int pass, int dep_set) // pass 0 predictor, 1 corrector, 2 initial deposit
 {
-    for (int s = 0; s < run->p.n_kinetic; ++s) {
+    for (int s = 0; s < run->p.n_kinetic; ++s)
         if (pass != 2 && run->sp[s].since_sort >= run->sort_interval)
             TRY(sort_species(run, s));
-        PushArgs const a = pc_pass_args(run, s, pass, dep_set);
-        phase_begin(run, 0);
-        TRY(launch_push(run, s, a));
-        phase_end(run, run->sp[s].n > 0 ? 1 : 0);
+    TRY(push_run(run, [&](int s) { return pc_pass_args(run, s, pass, dep_set); }));
+    for (int s = 0; s < run->p.n_kinetic; ++s) {
         if (run->profiling)
             run->prof.particles_pushed += run->sp[s].n;
         if (pass == 1)
