@@ -194,6 +194,23 @@ def test_gyrophase_randomization(gpu_lib, oracle_lib, name):
     assert rel_err(by_pid(g["particles"][0])["vy"], by_pid(g0["particles"][0])["vy"]) > 1e-3
 
 
+@pytest.mark.parametrize("precision,tol", [(h.configs.PREC_FP64, TOL10), (h.configs.PREC_MIXED, 1e-4)])
+def test_pc_species_sharing_a_launch(gpu_lib, oracle_lib, precision, tol):
+    """Two TSC species under the predictor-corrector cycle: both particle passes of a step cover
+    them in one launch (two parameter groups); ten steps against the oracle."""
+    name = "p2_tsc_mirror_reflecting"
+    cfg = h.configs.PARITY[name]().replace(algorithm=h.configs.ALGO_PC, precision=precision)
+    init = read_state(os.path.join(GOLDEN, f"{name}.init.bin"))
+    with h.Run(cfg, gpu_lib, "h1d_") as g, h.Run(cfg.replace(precision=h.configs.PREC_FP64), oracle_lib, "orc_") as c:
+        g.upload_state(init)
+        c.upload_state(init)
+        g.advance(10)
+        c.advance(10)
+        errs = state_errors(g.state(), c.state(), cfg)
+    bad = {k: v for k, v in errs.items() if not v <= tol}
+    assert not bad, bad
+
+
 def test_test_particles(gpu_lib, oracle_lib):
     """Test particles (TestParticleVDF, VDF/TestParticleVDF.cc:15-24: weight 0, f0 = 0) run as a
     full-f species without refresh: they are pushed and moved like the oracle's, and deposit
