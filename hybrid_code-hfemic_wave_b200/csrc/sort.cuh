@@ -79,10 +79,10 @@ __device__ __forceinline__ KeyRaw<KIND> key_load(SortKeys const &s, int64_t i)
 {
     if constexpr (KIND == KEYS_ARRAY)
         return {s.keys[i]};
-    else if constexpr (KIND == KEYS_FP64)
-        return {s.q1[i], s.w[i]};
+    else if constexpr (KIND == KEYS_FP64) // the weight only marks absorbed particles
+        return {s.q1[i], s.absorbing ? s.w[i] : 1.0};
     else
-        return {s.cell[i], s.wf[i]};
+        return {s.cell[i], s.absorbing ? s.wf[i] : 1.0f};
 }
 
 // the key of a loaded item; with `account`, absorbed particles are counted and lost ones flagged
