@@ -4,7 +4,7 @@
 points are looked up with a name prefix, ``h1d_`` for the CUDA library).  Errors come back
 as the exceptions the reference raises for the same condition: ``H1D_ERR_MOVED_TOO_FAR``
 is ``std::domain_error`` "particle(s) moved too far" in PartSpecies::update_pos
-(src/hybrid_1d/Core/PartSpecies.cc:215-219) and becomes :class:`MovedTooFar`;
+(src/hybrid_1d/Core/PartSpecies.cc:113) and becomes :class:`MovedTooFar`;
 ``H1D_ERR_INVALID_ARG`` (std::invalid_argument) becomes :class:`ValueError`.
 """
 from __future__ import annotations

@@ -10,7 +10,7 @@ number ``A``) and converted with the reference's own normalisation: O0 = 1 (prot
 cyclotron frequency), ``c`` = c/vA, so a species has ``Oc = Z/A`` and
 ``op = c*sqrt(f*Z**2/A)``; the electron fluid is ``eFluidDesc({-1836, c*sqrt(1836*ne)}, beta_e,
 closure)`` with ``ne = sum(f*Z)``.  The thermal speed of a bi-Maxwellian is
-``vth1 = sqrt(beta1)*c*|Oc|/op`` (src/LibPIC/PIC/VDF/MaxwellianVDF.cc:209).
+``vth1 = sqrt(beta1)*c*|Oc|/op`` (src/LibPIC/PIC/VDF/MaxwellianVDF.cc:24).
 """
 from __future__ import annotations
 
@@ -22,7 +22,7 @@ from typing import List
 ALGO_PC, ALGO_CAMCL = 0, 1
 BC_PERIODIC, BC_REFLECTING, BC_ABSORBING = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
-ISOTHERMAL, ADIABATIC = 11, 53  # Closure (src/LibPIC/PIC/Predefined.h:35-38)
+ISOTHERMAL, ADIABATIC = 11, 53  # Closure (src/LibPIC/PIC/Predefined.h:42-45)
 FULL_F, DELTA_F = 0, 1  # ParticleScheme (src/LibPIC/PIC/Predefined.h)
 # the equilibrium distribution of a kinetic species (VDFVariant, src/LibPIC/PIC/VDFVariant.h)
 VDF_BIMAXWELLIAN, VDF_LOSSCONE, VDF_PARTIAL_SHELL, VDF_COUNTER_BEAM = 0, 1, 2, 3
@@ -161,11 +161,11 @@ class RunConfig:
 
     @property
     def homogeneous(self) -> bool:
-        return self.xi < 1e-10  # MirrorGeometry.h:109, :185
+        return self.xi < 1e-10  # MirrorGeometry.h:19, MirrorGeometry.cc:20
 
     def moment_norm(self, k: Kinetic) -> float:
-        """PartSpecies::Nc = Nx*Nc*Nrefcell_div_Ntotal (PartSpecies.cc:150-154), with the
-        distribution's N_of_q1 (MaxwellianVDF.cc:213-239, LossconeVDF.cc:36-38, 79-95,
+        """PartSpecies::Nc = Nx*Nc*Nrefcell_div_Ntotal (PartSpecies.cc:45-49), with the
+        distribution's N_of_q1 (MaxwellianVDF.cc:28-30, 44-54, LossconeVDF.cc:37-39, 71-88,
         PartialShellVDF.cc:84-93); ``k.norm`` when the caller gives it."""
         if k.norm is not None:
             return k.norm
@@ -189,7 +189,7 @@ class RunConfig:
 
 
 def _int_cos_zeta(zeta: int, a: float, x: float, small_a: bool) -> float:
-    """int_0^x cos^zeta(a t) dt by the recurrence of VDFHelper.h:148-170 (zeta - 2 -> zeta)."""
+    """int_0^x cos^zeta(a t) dt by the recurrence of VDFHelper.h:125-147 (zeta - 2 -> zeta)."""
     ax = a * x
     if zeta == 0:
         return x
@@ -211,9 +211,9 @@ def _losscone_beta(k: Kinetic) -> float:
 
 
 def _n_of_q1(cfg: RunConfig, k: Kinetic, q1: float) -> float:
-    """N_of_q1 of the species' distribution: MaxwellianVDF.cc:229-239, LossconeVDF.cc:79-95,
+    """N_of_q1 of the species' distribution: MaxwellianVDF.cc:44-54, LossconeVDF.cc:71-88,
     PartialShellVDF.cc:84-93; counter-beam: the integral of n0 by Gauss-Legendre quadrature
-    (the reference integrates it numerically to about 1e-8, VDFHelper.h:43-64)."""
+    (the reference integrates it numerically to about 1e-8, VDFHelper.h:47-70)."""
     if k.vdf == VDF_LOSSCONE:
         b = _losscone_beta(k)
         X = k.T2_T1 / (1 + b)
@@ -245,7 +245,7 @@ def _n_of_q1(cfg: RunConfig, k: Kinetic, q1: float) -> float:
 
 
 def _q1_of_n(cfg: RunConfig, k: Kinetic, N: float) -> float:
-    """MaxwellianVDF::q1_of_N (MaxwellianVDF.cc:240-250)."""
+    """MaxwellianVDF::q1_of_N (MaxwellianVDF.cc:55-65)."""
     T2OT1 = k.T2_T1
     if cfg.homogeneous:
         xiD1N = cfg.xi * cfg.Dx * N

@@ -3,8 +3,8 @@
 // Shape functions, Boris push and the mirror-field geometry follow
 //   Shape<1..3>            src/LibPIC/PIC/Shape.h:29-35, 77-99, 149-176
 //   BorisPush              src/LibPIC/PIC/BorisPush.h:25-30, 57-73, 99-102
-//   CurviBasis / MFABasis  src/LibPIC/PIC/Geometry/CurviBasis.h:40-69, MFABasis.h:252-290
-//   MirrorGeometry         src/LibPIC/PIC/Geometry/MirrorGeometry.cc:199-212
+//   CurviBasis / MFABasis  src/LibPIC/PIC/Geometry/CurviBasis.h:40-69, MFABasis.h:37-80
+//   MirrorGeometry         src/LibPIC/PIC/Geometry/MirrorGeometry.cc:34-47
 // of kyungguk1/hybrid_code-hfemic_wave.
 #pragma once
 
@@ -19,7 +19,7 @@ constexpr int EBF_STRIDE = 8;
 
 // device status word bits; read by the host after each advance
 enum : unsigned {
-    ST_MOVED_TOO_FAR = 1u << 0, // |dq1| >= allowed fraction of a cell (PartSpecies.cc:252-264)
+    ST_MOVED_TOO_FAR = 1u << 0, // |dq1| >= allowed fraction of a cell (PartSpecies.cc:147-159)
     ST_OUT_OF_RANGE  = 1u << 1, // a particle's stencil fell outside the padded grid (non-finite or lost particle)
     ST_NAN           = 1u << 2,
     ST_SORT_OVERFLOW = 1u << 3,
@@ -185,7 +185,7 @@ __device__ __forceinline__ double warp_sum(double v)
 }
 
 // counter-based draw in [-pi, pi) for the gyro-phase of reflected particles; replaces the
-// std::random_device-seeded generator of Delegate::randomize_gyrophase (Delegate.cc:229-239)
+// std::random_device-seeded generator of Delegate::randomize_gyrophase (Delegate.cc:146-156)
 __host__ __device__ inline uint64_t mix64(uint64_t z)
 {
     z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;

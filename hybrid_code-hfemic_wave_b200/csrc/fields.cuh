@@ -2,12 +2,12 @@
 // loop, in one kernel launch.
 //
 // CAM-CL (src/hybrid_1d/Core/Domain_CAMCL.cc:57-193):
-//   per species collect_smooth of n/nV at x^N and x^{N+1} (Domain.hh:155-194): 1/Nc scale,
+//   per species collect_smooth of n/nV at x^N and x^{N+1} (Domain.hh:35-74): 1/Nc scale,
 //   charge/current conversion factors (Species.h:42-49), ghost fold (SubdomainDelegate.cc:122-181),
-//   3-point smoothing (GridArray.h:134-142); cold fluid push and moments (ColdSpecies.cc:251-285);
-//   averaging; the B subcycle with Ohm's-law E (BField.cc:74-124, EField.cc:245-330);
-//   E*, current advance with Lambda/Gamma (Domain_CAMCL.cc:131-151, Current.cc:181-188); final E;
-//   B on the half grid for the next push (PartSpecies.cc:132-139).
+//   3-point smoothing (GridArray.h:134-142); cold fluid push and moments (ColdSpecies.cc:31-65);
+//   averaging; the B subcycle with Ohm's-law E (BField.cc:24-74, EField.cc:41-126);
+//   E*, current advance with Lambda/Gamma (Domain_CAMCL.cc:131-151, Current.cc:45-52); final E;
+//   B on the half grid for the next push (PartSpecies.cc:27-34).
 // Predictor-corrector (src/hybrid_1d/Core/Domain_PC.cc:84-205) uses the same building blocks in
 // three phases around its two particle passes.
 //
@@ -38,9 +38,9 @@ enum GeoIdx {
     G_FCON_X, G_FCON_Y, G_FCON_Z, // contravariant basis at full-grid points (CurviBasis.h:65-69)
     G_HCOV_X, G_HCOV_Y, G_HCOV_Z, // same at half-grid points
     G_HCON_X, G_HCON_Y, G_HCON_Z,
-    G_HBX,                        // Bcart(half point).x = O0/cos^2 (MFABasis.h:262)
+    G_HBX,                        // Bcart(half point).x = O0/cos^2 (MFABasis.h:47)
     G_MP1, G_MP2, G_MA1, G_MA2,   // phase-retardation / amplitude-damping factors, in the order
-                                  // the reference applies them (BField.cc:90-98)
+                                  // the reference applies them (BField.cc:40-48)
     G_COUNT
 };
 
@@ -48,9 +48,9 @@ struct KinSrc {
     double const *raw[2][4]; // unscaled deposits at x^N and x^{N+1}: n, nVx, nVy, nVz (cell 0)
     double const *eq;        // delta-f: equilibrium n0 added to the density moment (cell 0), or null
     double       *zero[2][4]; // the deposit set of the next cycle, cleared here
-    double        s1;         // 1/Nc (PartSpecies.cc:327-328)
+    double        s1;         // 1/Nc (PartSpecies.cc:222-223)
     double        cdcf, ccf;  // charge / current density conversion factors
-    double        lamf, gamf; // Lambda / Gamma factors (Charge.cc:75-80, Current.cc:170-175)
+    double        lamf, gamf; // Lambda / Gamma factors (Charge.cc:31-36, Current.cc:34-39)
     int           nsm;
 };
 struct ColdSrc {
@@ -77,7 +77,7 @@ struct FieldArgs {
     KinSrc        e[MAXE];
     double        dt, sub_dt, c_light, sqrt_g, O0, inv_D1;
     int           m; // n_subcycles
-    // electron fluid (EField.cc:267-291)
+    // electron fluid (EField.cc:63-87)
     double        mOeOO0oe2, gamma, O02beO2, cO2, cOsqrtg;
     // predictor-corrector (Domain_PC.cc:84-205): phase 0 initial sources, 1 predicted fields,
     // 2 after the predictor deposit, 3 after the corrector deposit
@@ -155,7 +155,7 @@ __device__ __forceinline__ d3 contr_half(Cell const &C, d3 b) { return { C.hnx *
 __device__ __forceinline__ d3 mask_p(Cell const &C, d3 v) { return (v * C.mp1) * C.mp2; }
 __device__ __forceinline__ d3 mask_a(Cell const &C, d3 v) { return (v * C.ma1) * C.ma2; }
 
-// electron pressure gradient, masked (EField.cc:267-291, 248): needs Pe of the neighbours
+// electron pressure gradient, masked (EField.cc:63-87, 44): needs Pe of the neighbours
 __device__ __forceinline__ double dPe_at(FieldArgs const &a, Cell const &C, double const *Pe)
 {
     int const tl = max(C.t - 1, 0), tr = min(C.t + 1, C.L - 1);
@@ -166,7 +166,7 @@ __device__ __forceinline__ double Pe_of(FieldArgs const &a, double rho)
     return pow(a.mOeOO0oe2 * rho, a.gamma) * a.O02beO2;
 }
 
-// Ohm's law at this cell (EField.cc:292-330) from Bcov/Bcon of the current B (with the
+// Ohm's law at this cell (EField.cc:88-126) from Bcov/Bcon of the current B (with the
 // neighbour at t+1), contravariant current jc, masked dPe and rho; returns the masked E
 __device__ __forceinline__ d3 E_at(FieldArgs const &a, Cell const &C, double const *Bcov, double const *Bcon, d3 jc,
                                    double dPe, double rho)
@@ -182,7 +182,7 @@ __device__ __forceinline__ d3 E_at(FieldArgs const &a, Cell const &C, double con
     return mask_a(C, contr_half(C, Ec));
 }
 
-// Faraday at this cell (BField.cc:74-114) from Ecov at t and t-1; returns the new masked B
+// Faraday at this cell (BField.cc:50-64) from Ecov at t and t-1; returns the new masked B
 __device__ __forceinline__ d3 B_at(FieldArgs const &a, Cell const &C, double const *Ecov, d3 Bprev, double dtp)
 {
     int const    t = C.t, tl = max(t - 1, 0);
@@ -214,7 +214,7 @@ __device__ __forceinline__ void load_cell(FieldArgs const &a, Cell &C, int blk)
     C.mp1 = G[G_MP1 * N + i], C.mp2 = G[G_MP2 * N + i], C.ma1 = G[G_MA1 * N + i], C.ma2 = G[G_MA2 * N + i];
 }
 
-// owner writes of an interior value and of its ghost images (periodic fill, Delegate.cc:159-170)
+// owner writes of an interior value and of its ghost images (periodic fill, Delegate.cc:76-87)
 __device__ __forceinline__ void put3(double *g, Cell const &C, int Nx, d3 v)
 {
     st3(g, C.gm, v);
@@ -233,7 +233,7 @@ __device__ __forceinline__ void put1(double *g, Cell const &C, int Nx, double v)
 }
 
 // owner write of the interleaved push record {E, B averaged onto the half grid} and its ghost
-// images; the half-grid B of the last ghost cell stays NaN (PartSpecies.cc:137)
+// images; the half-grid B of the last ghost cell stays NaN (PartSpecies.cc:32)
 __device__ __forceinline__ void put_eb(double *eb, float *ebf, Cell const &C, int Nx, d3 E, d3 Bh)
 {
     auto put = [&](int i, bool withB) {
@@ -301,7 +301,7 @@ static __device__ SV collect_kinetic(FieldArgs const &a, Cell const &C, Smem con
     return smooth_n(C, K.nsm, S.tr, S.tJ, S.ts, S.tJs);
 }
 
-// cold species (ColdSpecies.cc:251-285): push nV with E and the background field, moments x w
+// cold species (ColdSpecies.cc:31-65): push nV with E and the background field, moments x w
 static __device__ d3 cold_push(FieldArgs const &a, Cell const &C, ColdSrc const &K, double const *E_cell0)
 {
     d3 const     E  = ld3(E_cell0, C.gm);
@@ -404,7 +404,7 @@ __device__ __forceinline__ void camcl_field_body(FieldArgs const &a, int blk)
     d3 const Es = E_at(a, C, S.Bcov, S.Bcon, jc, dPe1, S.rho1[t]);
     sst3(S.E, t, Es);
     __syncthreads();
-    // current advance (Domain_CAMCL.cc:131-151, Current.cc:181-188)
+    // current advance (Domain_CAMCL.cc:131-151, Current.cc:45-52)
     d3 const Bi = { C.hbx + (sld3(S.B0, min(t + 1, C.L - 1)).x + Bavg.x) * 0.5,
                     0 * a.O0 + (sld3(S.B0, min(t + 1, C.L - 1)).y + Bavg.y) * 0.5,
                     0 * a.O0 + (sld3(S.B0, min(t + 1, C.L - 1)).z + Bavg.z) * 0.5 };

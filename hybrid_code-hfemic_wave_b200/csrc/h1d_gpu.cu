@@ -255,7 +255,7 @@ VdfConsts vdf_consts(h1d_kinetic_desc const &d)
     return k;
 }
 
-// PartSpecies::populate's cache of the equilibrium moments (PartSpecies.cc:80-87) on the interior
+// PartSpecies::populate's cache of the equilibrium moments (PartSpecies.cc:82-89) on the interior
 // half-grid points, times m_moment_weighting_factor as collect_part adds them: n0 (M doubles) then
 // nvv0 (6M, {xx, yy, zz, xy, yz, zx}; mfa_to_cart is the identity on the field line); nV0 = 0;
 // ghost cells zero.  Per distribution (impl_n / impl_nvv):
@@ -395,8 +395,8 @@ double mask_fn(long inset, double factor, double offset)
     return (1 - tmp) * (1 + tmp);
 }
 
-// per-cell geometry, computed on the host with libm (CurviBasis.h:42, 52-69; MFABasis.h:262;
-// MaskingFunction.h:28-35 applied as in BField.cc:90-98)
+// per-cell geometry, computed on the host with libm (CurviBasis.h:42, 52-69; MFABasis.h:47;
+// MaskingFunction.h:28-35 applied as in BField.cc:40-48)
 std::vector<double> geometry_table(h1d_params const &p)
 {
     long const          N = p.Nx;
@@ -1043,7 +1043,7 @@ int ensure_capacity(h1d_run *run, int s, int64_t n)
     return H1D_OK;
 }
 
-// MaxwellianVDF::N_of_q1 (VDF/MaxwellianVDF.cc:229-239)
+// MaxwellianVDF::N_of_q1 (VDF/MaxwellianVDF.cc:44-54)
 double n_of_q1(h1d_params const &p, double T2OT1, double q1)
 {
     if (p.xi < 1e-10) {

@@ -1,5 +1,5 @@
 // Particle kernels outside the particle pass: collect_all of n, nV and nvv for the recorders
-// (PartSpecies::impl_collect_all, PartSpecies.cc:330-349) in both precisions, the FP64 <->
+// (PartSpecies::impl_collect_all, PartSpecies.cc:225-244) in both precisions, the FP64 <->
 // mixed-precision conversions of upload and download, and the cell keys and gather of the
 // mixed-precision cell sort.  Compiled in the library's main translation unit only.
 #pragma once
@@ -8,7 +8,7 @@
 
 namespace h1d {
 
-// PartSpecies::impl_collect_all (PartSpecies.cc:330-349): n, nV and nvv with CIC, unscaled, from
+// PartSpecies::impl_collect_all (PartSpecies.cc:225-244): n, nV and nvv with CIC, unscaled, from
 // cell-sorted particles (moments_kernel below).
 
 struct MomentArgs {
@@ -254,7 +254,7 @@ __global__ void from_mixed_kernel(int32_t const *cell, float const *src, int64_t
 
 // ------------------------------------------------------------------------------------------------
 // Device loader of a bi-Maxwellian species (PartSpecies::populate with MaxwellianVDF::load,
-// VDF/MaxwellianVDF.cc:300-319, q1_of_N :240-250, eta :218-228).  Particle i uses the radical
+// VDF/MaxwellianVDF.cc:115-134, q1_of_N :55-65, eta :33-43).  Particle i uses the radical
 // inverses in bases 2, 3 and 5 of the sequence index offset + i and two counter-based uniforms (the
 // splitmix64 finalizer of the species key and 2i + 1, 2i + 2).  Every arithmetic step is the one
 // the host loader (loader.py) performs, in the same order and without contraction, so the two

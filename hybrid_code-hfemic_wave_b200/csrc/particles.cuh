@@ -2,11 +2,11 @@
 //
 // One fused pass per species and CAM-CL step does what the reference does in four loops over
 // the particle deque (src/hybrid_1d/Core/Domain_CAMCL.cc:69-82):
-//   PartSpecies::update_vel   interp of E and dB at x^N, mirror-field B, Boris push   (PartSpecies.cc:266-281)
-//   PartSpecies::collect_part deposit of n and nV at x^N with v^{N+1/2}                (PartSpecies.cc:315-329)
-//   PartSpecies::update_pos   x^{N+1} = x^N + v.e^1 dt, travel check                   (PartSpecies.cc:252-264)
-//   Delegate::boundary_pass   periodic wrap / reflection (+ gyro-phase)               (Delegate.cc:116-228)
-//   PartSpecies::collect_part deposit of n and nV at x^{N+1}                          (PartSpecies.cc:315-329)
+//   PartSpecies::update_vel   interp of E and dB at x^N, mirror-field B, Boris push   (PartSpecies.cc:105-109, 161-176)
+//   PartSpecies::collect_part deposit of n and nV at x^N with v^{N+1/2}                (PartSpecies.cc:115-128, 210-224)
+//   PartSpecies::update_pos   x^{N+1} = x^N + v.e^1 dt, travel check                   (PartSpecies.cc:110-114, 147-159)
+//   Delegate::boundary_pass   periodic wrap / reflection (+ gyro-phase)               (Delegate.cc:51-74, 101-156)
+//   PartSpecies::collect_part deposit of n and nV at x^{N+1}                          (PartSpecies.cc:115-128, 210-224)
 // Particles are structure-of-arrays and cell-sorted (sort.cuh), so the particles of a warp span a
 // few cells.  Each warp deposits into a window of PIPE_W cells held in shared memory as
 // lane-private columns; a window is summed over its 32 columns and added to the global moment
@@ -29,7 +29,7 @@ struct PushArgs {
     int64_t        n;
     int            Nx;
     double const  *EB; // per cell {Ex, Ey, Ez, dBx, dBy, dBz}: E and B averaged onto the half grid
-                       // (PartSpecies.cc:132-139), pointer at interior cell 0
+                       // (PartSpecies.cc:27-34), pointer at interior cell 0
     double        *dep[2][4]; // [deposit at x^N | x^{N+1}][n, nVx, nVy, nVz], at cell 0
     double         half_min, full_min, full_max, full_len;
     double         xi, xi2, xiD1, D1, inv_D1, O0, Oc, dt, travel_scale, xiO0_Oc;
@@ -110,8 +110,8 @@ __device__ __forceinline__ bool boundary(PushArgs const &a, double &q1, d3 &v, i
     }
 }
 
-// background mirror field at the particle with its gyro-radius offset (PartSpecies.cc:274-279;
-// MFABasis.h:287-290; MirrorGeometry.cc:199-212).  With c = cos(xi D1 q1), s = sin(xi D1 q1):
+// background mirror field at the particle with its gyro-radius offset (PartSpecies.cc:169-174;
+// MFABasis.h:72-75; MirrorGeometry.h:68-71; MirrorGeometry.cc:34-47).  With c = cos(xi D1 q1), s = sin(xi D1 q1):
 // B/B0 = 1/c^2, x = tan/xi, rL = (-vz, vy) c^2/Oc, so the transverse components
 // -xi^2 x rL O0 reduce to (xi O0/Oc) s c (vz, -vy).  Also returns c^2 for the move.
 template <bool MIRROR>
@@ -130,19 +130,19 @@ __device__ __forceinline__ d3 background_B(PushArgs const &a, double q1, d3 v, d
 }
 
 // The equilibrium f0(v, q1) of a species' distribution (VDF::real_f0), with cs = cos(xi D1 q1).
-// cart_to_mfa is the identity on the field line (MFABasis.h:96-99), so v is field-aligned; every
+// cart_to_mfa is the identity on the field line (MFABasis.h:98-100), so v is field-aligned; every
 // f0 is n0(q1) times a velocity distribution normalised to one.
-//  - bi-Maxwellian (MaxwellianVDF.cc:33-92): n0 = eta = 1 / (T + (1 - T) cs^2), T = T2OT1_eq
+//  - bi-Maxwellian (MaxwellianVDF.cc:33-43, 67-81): n0 = eta = 1 / (T + (1 - T) cs^2), T = T2OT1_eq
 //    (T2_T1), T2OT1 = T eta; f0 = n0 exp(-x1^2) pi^-1/2 exp(-x_perp^2 / T2OT1) / (pi T2OT1) / vth1^3,
 //    x = v / vth1.
-//  - loss-cone (LossconeVDF.cc:44-117): vc = {beta_eq, X = xth2_eq^2, beta_eq X}; eta as above with
+//  - loss-cone (LossconeVDF.cc:46-117): vc = {beta_eq, X = xth2_eq^2, beta_eq X}; eta as above with
 //    X, eta_b with beta_eq X, n0 = (eta - beta_eq eta_b) / (1 - beta_eq), xth2^2 = X eta,
 //    beta = beta_eq eta_b / eta (kept 1e-10 away from 1); the perpendicular factor is
 //    (exp(-y) - exp(-y / beta)) / (pi xth2^2 (1 - beta)) with y = x_perp^2 / xth2^2.
-//  - partial shell (PartialShellVDF.cc:96-145): vc = {zeta, xs, A(xs), B(zeta)}; n0 = cs^zeta;
+//  - partial shell (PartialShellVDF.cc:78-93, 125-140): vc = {zeta, xs, A(xs), B(zeta)}; n0 = cs^zeta;
 //    f0 = n0 exp(-(x - xs)^2) / A sin^zeta(alpha) / B / (2 pi vth^3), x = |v| / vth,
 //    cos(alpha) = x1 / x.
-//  - counter-beam (CounterBeamVDF.cc:134-178): vc = {nu0, xs, A(xs), B(nu0)}; nu = nu0 / cs
+//  - counter-beam (CounterBeamVDF.cc:99-132): vc = {nu0, xs, A(xs), B(nu0)}; nu = nu0 / cs
 //    (B/B0 = 1/cs^2), n0 = B(nu) / B(nu0) and the pitch-angle factor
 //    exp(-sin^2(alpha) / nu^2) / B(nu): their product needs no B(nu), so
 //    f0 = exp(-(x - xs)^2) / A exp(-sin^2(alpha) cs^2 / nu0^2) / B(nu0) / (2 pi vth^3).
@@ -516,7 +516,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
             bool         alive = true;
             if (a.move_steps == 2) {
                 double const moved = move<MIRROR>(a, q1, v.x, 0.5 * a.dt);
-                if (live && !(fabs(moved) < 1.0)) // long(moved * scale) != 0 (PartSpecies.cc:261)
+                if (live && !(fabs(moved) < 1.0)) // long(moved * scale) != 0 (PartSpecies.cc:156)
                     bad |= ST_MOVED_TOO_FAR;
                 alive = boundary<BC>(a, q1, v, pid, a.counter);
                 if (!alive)

@@ -166,7 +166,7 @@ __device__ __forceinline__ bool boundary_mixed(PushArgsMixed const &a, int &cell
         return true;
     } else if constexpr (BC == BCK_REFLECTING) {
         bool const left = cell < 0, right = cell >= a.Nx;
-        if (left || right) { // q1 -> 2 q1_boundary - q1 (Delegate.cc:199-228)
+        if (left || right) { // q1 -> 2 q1_boundary - q1 (Delegate.cc:116-145)
             if (left) {      // q1 - q1min = -1 + off -> 1 - off
                 cell = off > 0.0f ? 0 : 1;
                 off  = off > 0.0f ? 1.0f - off : 0.0f;

@@ -30,8 +30,8 @@ __global__ void iota_kernel(int32_t *pid, int64_t n)
 
 __device__ __forceinline__ int wrap(int i, int Nx) { return i < 0 ? i + Nx : i >= Nx ? i - Nx : i; }
 
-// boundary_pass of E and B (periodic ghost fill, Delegate.cc:159-170) and the push record
-// {E, B on the half grid} (PartSpecies.cc:132-139; the last ghost's half-grid B stays NaN)
+// boundary_pass of E and B (periodic ghost fill, Delegate.cc:76-87) and the push record
+// {E, B on the half grid} (PartSpecies.cc:27-34; the last ghost's half-grid B stays NaN)
 __global__ void prep_fields_kernel(double *B, double *E, double *EB, float *EBf, int Nx)
 {
     int const i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x) - PAD;
@@ -56,7 +56,7 @@ __global__ void prep_fields_kernel(double *B, double *E, double *EB, float *EBf,
     }
 }
 
-// collect_all scaling by 1/Nc (PartSpecies.cc:346-348) and boundary_gather of the three moments
+// collect_all scaling by 1/Nc (PartSpecies.cc:241-243) and boundary_gather of the three moments
 // (SubdomainDelegate.cc:115-181).  raw: 10 arrays of M (n, nV xyz, nvv xx yy zz xy yz zx);
 // out: GridArray layout n[M], nV[3M], nvv[6M].
 // delta-f species (eq != null): + the equilibrium n0 (M) and nvv0 (6M) x m_moment_weighting_factor
@@ -108,7 +108,7 @@ __global__ void fold_moments_kernel(double *out, int Nx, int reflecting)
         a[nc * (PAD + k) + c] += right[k];
 }
 
-// ColdSpecies::collect_all (ColdSpecies.cc:268-297): moments x weight on the interior,
+// ColdSpecies::collect_all (ColdSpecies.cc:48-77): moments x weight on the interior,
 // zero ghosts, nvv = (nV/n) nV
 __global__ void finalize_cold_kernel(double const *n_full, double const *nV_full, double *out, int Nx, double w)
 {

@@ -3,7 +3,7 @@ distribution (bi-Maxwellian, loss-cone, partial shell or counter-beam), cold flu
 wave fields.
 
 Follows the distributions of the reference loader MaxwellianVDF::load
-(src/LibPIC/PIC/VDF/MaxwellianVDF.cc:300-319, with N_of_q1 / q1_of_N :229-250 and eta :218-228):
+(src/LibPIC/PIC/VDF/MaxwellianVDF.cc:115-134, with N_of_q1 / q1_of_N :44-65 and eta :33-43):
   - position: q1 = q1_of_N(u2 * N_len + N_loc) with u2 the base-2 radical inverse of the particle's
     sequence index;
   - v_par = sqrt(-log U1) sin(2 pi u3) vth1, v_perp = sqrt(-log U2 * T2/T1(q1)) (cos, sin)(2 pi u5)
@@ -14,21 +14,21 @@ at index 1.  Here a run's seed picks the sequences' starting index and U1, U2 ar
 draws (the splitmix64 finalizer of seed, species and particle index), so that runs with different
 seeds are independent and the same draws can be made on the device: h1d_populate computes exactly
 these particles (up to the last bit of the device's tan/atan/log/sin/cos).  Cold species start with
-n = 1, nV = 0 (ColdSpecies.cc:238-249); B and E start at zero.
+n = 1, nV = 0 (ColdSpecies.cc:18-29); B and E start at zero.
 
 The other distributions follow their reference loaders with the same kind of draws
 (load_other_species): positions from the inverse of N(q1) = int n0 dq1 at the base-2 radical
-inverse (LossconeVDF.cc:145-147, PartialShellVDF.cc:165-167, CounterBeamVDF.cc:200-207; here the
+inverse (LossconeVDF.cc:154, PartialShellVDF.cc:177, CounterBeamVDF.cc:169-175; here the
 inverse is a fine table of the integral of n0 instead of the reference's closed forms or its
 stepped integration); loss-cone perpendicular speeds by the reference's rejection sampler against
-a Gaussian of spread alpha = max(beta, 1) + 0.3 (LossconeVDF.cc:149-213); partial-shell pitch
-angles and shell speeds by inverting their cumulative distributions (PartialShellVDF.cc:47-81,
-168-180); counter-beam pitch angles by rejection under exp(-sin^2 a / nu^2) sin a with a coin
-flip into the second quadrant (CounterBeamVDF.cc:182-224).  Velocities are drawn from the marker
+a Gaussian of spread alpha = max(beta, 1) + 0.3 (LossconeVDF.cc:162, 171-213); partial-shell pitch
+angles and shell speeds by inverting their cumulative distributions (PartialShellVDF.cc:94-124,
+173-192); counter-beam pitch angles by rejection under exp(-sin^2 a / nu^2) sin a with a coin
+flip into the second quadrant (CounterBeamVDF.cc:165-224).  Velocities are drawn from the marker
 distribution g0 (the physical one heated by marker_temp_ratio); every species carries its
 phase-space density real_f = f0, marker = g0 and the weight of its scheme: f0/g0 (full-f) or
 initial_weight U(-1, 1) with real_f = f0 + w g0 (delta-f), as the reference's emit functions set
-them (MaxwellianVDF.cc:113-134, LossconeVDF.cc:117-137).
+them (MaxwellianVDF.cc:96-114, LossconeVDF.cc:131-149).
 """
 from __future__ import annotations
 

@@ -16,9 +16,9 @@
  *                             Core/Domain.cc:42-55) with the compile-time `Input` of
  *                            src/hybrid_1d/Include/Inputs.h:13-241 passed as a runtime struct
  *   h1d_upload_particles  <- PartSpecies::bucket after populate/load_ptls
- *                            (Core/PartSpecies.h:33-34, Core/PartSpecies.cc:180-206)
+ *                            (Core/PartSpecies.h:33-34, Core/PartSpecies.cc:75-101)
  *   h1d_upload_fields     <- Domain::bfield / Domain::efield contents (Core/Domain.h:30-31)
- *   h1d_upload_cold       <- ColdSpecies::mom0_full / mom1_full (Core/ColdSpecies.h:191-192)
+ *   h1d_upload_cold       <- ColdSpecies::mom0_full / mom1_full (Core/ColdSpecies.h:21-22)
  *   h1d_advance           <- Domain::advance_by(unsigned) (Core/Domain.h:46,
  *                            Core/Domain_CAMCL.cc:21-56, Core/Domain_PC.cc:21-78)
  *   h1d_download_*        <- what the recorders read after advance_by: bfield, efield,
@@ -29,7 +29,7 @@
  * Conventions
  *   - Every function returns an int status (H1D_OK = 0).  Nonzero codes map to the
  *     reference's exceptions: H1D_ERR_MOVED_TOO_FAR is the std::domain_error
- *     "particle(s) moved too far" of PartSpecies::update_pos (Core/PartSpecies.cc:215-219);
+ *     "particle(s) moved too far" of PartSpecies::update_pos (Core/PartSpecies.cc:113);
  *     H1D_ERR_INVALID_ARG is std::invalid_argument of the descriptors/ParamSet checks.
  *     h1d_status_string() gives the detail of the last error of a run.
  *   - Grid buffers use the reference GridArray layout (LibPIC/PIC/GridArray.h:36-38):
@@ -64,7 +64,7 @@ extern "C" {
 enum {
     H1D_OK                = 0,
     H1D_ERR_INVALID_ARG   = 1, /* std::invalid_argument in the reference */
-    H1D_ERR_MOVED_TOO_FAR = 2, /* std::domain_error, PartSpecies.cc:218 */
+    H1D_ERR_MOVED_TOO_FAR = 2, /* std::domain_error, PartSpecies.cc:113 */
     H1D_ERR_OOM           = 3,
     H1D_ERR_CUDA          = 4,
     H1D_ERR_TIMEOUT       = 5,
@@ -73,7 +73,7 @@ enum {
     H1D_ERR_NO_DEVICE     = 8
 };
 
-/* Algorithm (LibPIC/PIC/Predefined.h:27-30): same numeric values */
+/* Algorithm (LibPIC/PIC/Predefined.h:35-38): same numeric values */
 enum { H1D_ALGO_PC = 0, H1D_ALGO_CAMCL = 1 };
 /* BC (Predefined.h:49-52): same numeric values; ABSORBING is an extension without a
  * reference counterpart (particles leaving the domain are dropped) */
@@ -103,7 +103,7 @@ typedef struct h1d_kinetic_desc {
     int64_t Nc;          /* KineticPlasmaDesc::Nc, particles per cell: h1d_create reserves device
                             buffers for Nx * Nc particles (more are allocated on upload if needed) */
     int64_t shape_order; /* 1 (CIC), 2 (TSC) or 3 */
-    double  moment_norm; /* PartSpecies::Nc (PartSpecies.cc:150-154): Nx*Nc*Nrefcell_div_Ntotal,
+    double  moment_norm; /* PartSpecies::Nc (PartSpecies.cc:45-49): Nx*Nc*Nrefcell_div_Ntotal,
                             the particle count of the reference cell used to normalise moments */
     /* Phase-space density weighting.  With scheme H1D_DELTA_F, or a nonzero psd_refresh_frequency,
      * every particle carries its physical density real_f and marker density marker
@@ -116,12 +116,12 @@ typedef struct h1d_kinetic_desc {
     int32_t vdf;                   /* H1D_VDF_*; 0 (bi-Maxwellian) in a zero-initialised desc */
     double  psd_refresh_frequency; /* KineticPlasmaDesc::psd_refresh_frequency (>= 0) */
     double  vth1;                  /* thermal speed sqrt(beta) c |Oc| / op of the distribution: beta1
-                                      (bi-Maxwellian, loss-cone: MaxwellianVDF.cc:24, LossconeVDF.cc:32)
+                                      (bi-Maxwellian, loss-cone: MaxwellianVDF.cc:24, LossconeVDF.cc:33)
                                       or the thermal spread beta (partial shell, counter-beam:
                                       PartialShellVDF.cc:27, CounterBeamVDF.cc:40) */
     double  T2_T1;                 /* bi-Maxwellian, loss-cone: BiMaxPlasmaDesc::T2_T1 at the
                                       equator (for a LossconePlasmaDesc built from a vth_ratio,
-                                      (1 + beta) vth_ratio, PlasmaDesc.h:254); others: unused */
+                                      (1 + beta) vth_ratio, PlasmaDesc.h:271-272); others: unused */
     double  vdf_param[3];          /* loss-cone: {losscone.beta, -, -};
                                       partial shell: {zeta (a non-negative integer), vs, -};
                                       counter-beam: {nu, vs, -}; bi-Maxwellian: unused */
@@ -177,7 +177,7 @@ typedef struct h1d_params {
     double  phase_retardation_factor;
     int64_t amplitude_damping_inset;  /* Input::amplitude_damping */
     double  amplitude_damping_factor;
-    double  moment_weighting; /* Species::m_moment_weighting_factor = 1/clones (Species.cc:110-117); 1 */
+    double  moment_weighting; /* Species::m_moment_weighting_factor = 1/clones (Species.cc:10-17); 1 */
     int32_t sort_interval;    /* steps between particle cell sorts; 0 = library default */
     int32_t n_kinetic;
     int32_t n_cold;
@@ -211,7 +211,7 @@ int h1d_upload_particles(h1d_run *run, int s, int64_t n, const double *q1, const
 int h1d_upload_psd(h1d_run *run, int s, int64_t n, const double *real_f, const double *marker);
 /* ... and back, in the order of h1d_download_particles; either pointer may be NULL. */
 int h1d_download_psd(h1d_run *run, int s, double *real_f, double *marker);
-/* PartSpecies::populate with a bi-Maxwellian MaxwellianVDF (VDF/MaxwellianVDF.cc:88-134, 300-319),
+/* PartSpecies::populate with a bi-Maxwellian MaxwellianVDF (VDF/MaxwellianVDF.cc:88-134),
  * on the device: n particles of kinetic species `s` with parallel beta `beta1` and T_perp/T_par
  * `T2_T1`, positions from the base-2 radical inverse through q1_of_N, velocities from base-3/5
  * radical inverses and two counter-based uniforms of (seed, s, particle), full-f weight 1.
@@ -243,9 +243,9 @@ int h1d_download_fields(h1d_run *run, double *B, double *E);
 /* Domain::charge and Domain::current after the last step ((Nx+2*H1D_PAD) and *3 doubles) */
 int h1d_download_sources(h1d_run *run, double *charge, double *current);
 /* Species::moment<0..2>() of kinetic species `s` after the post-process collect_all
- * (PartSpecies.cc:234-248, 330-349, always CIC) and boundary_gather; any pointer may be NULL */
+ * (PartSpecies.cc:129-143, 225-244, always CIC) and boundary_gather; any pointer may be NULL */
 int h1d_download_moments(h1d_run *run, int s, double *n, double *nV, double *nvv);
-/* cold species moments after collect_all (ColdSpecies.cc:268-297) and mom0_full/mom1_full */
+/* cold species moments after collect_all (ColdSpecies.cc:48-77) and mom0_full/mom1_full */
 int h1d_download_cold(h1d_run *run, int i, double *n, double *nV, double *nvv, double *n_full,
                       double *nV_full);
 /* EnergyRecorder::dump (EnergyRecorder.cc:98-140): dB2O2[3], dE2O2[3], and for every kinetic

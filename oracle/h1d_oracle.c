@@ -7,17 +7,17 @@
  * It restates, with runtime sizes instead of the reference's template constants:
  *   Domain_CAMCL::advance_by / cycle / subcycle / current_advance  (src/hybrid_1d/Core/Domain_CAMCL.cc:21-193)
  *   Domain_PC::advance_by / predictor_step / corrector_step         (Core/Domain_PC.cc:21-205)
- *   Domain::collect_smooth                                          (Core/Domain.hh:155-194)
- *   PartSpecies::update_vel/update_pos/collect_part/collect_all     (Core/PartSpecies.cc:132-139, 210-349)
- *   PartSpecies::impl_update_weight, equilibrium moments            (Core/PartSpecies.cc:80-87, 115-143, 178-208;
+ *   Domain::collect_smooth                                          (Core/Domain.hh:35-74)
+ *   PartSpecies::update_vel/update_pos/collect_part/collect_all     (Core/PartSpecies.cc:27-34, 105-244)
+ *   PartSpecies::impl_update_weight, equilibrium moments            (Core/PartSpecies.cc:82-89, 115-143, 178-208;
  *                                                                    VDF/{Maxwellian,Losscone,PartialShell,CounterBeam}VDF)
- *   ColdSpecies::update_vel/collect_part/collect_all                (Core/ColdSpecies.cc:251-297)
- *   BField::update, EField::update, Charge/Current/Lambda/Gamma     (Core/BField.cc:74-124, EField.cc:224-330,
- *                                                                    Charge.cc:70-80, Current.cc:165-188)
+ *   ColdSpecies::update_vel/collect_part/collect_all                (Core/ColdSpecies.cc:31-77)
+ *   BField::update, EField::update, Charge/Current/Lambda/Gamma     (Core/BField.cc:24-74, EField.cc:41-126,
+ *                                                                    Charge.cc:26-36, Current.cc:29-52)
  *   BorisPush::non_relativistic, Shape<1..3>, GridArray interp/deposit/smooth, MaskingFunction,
  *   CurviBasis/MFABasis/MirrorGeometry                              (LibPIC/PIC headers)
  *   Delegate particle partition / periodic / reflecting pass, ghost pass and gather semantics of
- *   SubdomainDelegate with a single subdomain (Boundary/Delegate.cc:116-228,
+ *   SubdomainDelegate with a single subdomain (Boundary/Delegate.cc:51-156,
  *   Boundary/SubdomainDelegate.cc:58-181)
  *   EnergyRecorder::dump                                            (Recorder/EnergyRecorder.cc:98-140)
  *
@@ -26,7 +26,7 @@
  * partition of libstdc++ for bidirectional iterators), so that with -ffp-contract=off on both
  * sides this code reproduces the compiled reference bit for bit.  The one deliberate
  * difference: gyro-phase randomisation of reflected particles draws from a counter-based hash
- * instead of std::random_device (Delegate.cc:231), so that it is reproducible.
+ * instead of std::random_device (Delegate.cc:148), so that it is reproducible.
  */
 #define _DEFAULT_SOURCE
 #include "../include/h1d_gpu.h"
@@ -53,7 +53,7 @@ typedef struct orc_run {
     h1d_params p;
     long       Nx, M; /* M = Nx + 2P */
     double     full_min, full_len, half_min; /* extents (ParamSet.cc:22-23) */
-    /* geometry (MirrorGeometry.cc:178-187, CurviBasis.h:32-35, MFABasis.h:244-247) */
+    /* geometry (MirrorGeometry.cc:13-22, CurviBasis.h:32-35, MFABasis.h:29-32) */
     double xi, xi2, D1, D2, D3, inv_D1, inv_D2, inv_D3, sqrt_g;
     int    homogeneous;
     /* grids, GridArray layout (M elements, ghosts included) */
@@ -169,7 +169,7 @@ static void bucket_copy(Bucket *dst, Bucket const *src)
 /* ------------------------------------------------------------------------------------------------
  * geometry (LibPIC/PIC/Geometry/CurviBasis.h, MFABasis.h, MirrorGeometry.cc)
  */
-/* inv_sqrt_BOB0(CurviCoord) = cos(xi*D1*q1)   (CurviBasis.h:42, MFABasis.h:254) */
+/* inv_sqrt_BOB0(CurviCoord) = cos(xi*D1*q1)   (CurviBasis.h:42, MFABasis.h:39) */
 static inline double g_cos(orc_run const *R, double q1) { return cos(R->xi * R->D1 * q1); }
 /* BOB0(CurviCoord) = pow2(1/inv_sqrt_BOB0)     (CurviBasis.h:43) */
 static inline double g_BOB0(orc_run const *R, double q1)
@@ -201,21 +201,21 @@ static inline V3 g_cart_to_contr(orc_run const *R, V3 v, double q1)
 static inline V3 g_contr_to_cart(orc_run const *R, V3 v, double q1) { return g_cart_to_covar(R, v, q1); }
 /* covar_to_cart = v . contr_basis<0>   (CurviBasis.h:164, 212) */
 static inline V3 g_covar_to_cart(orc_run const *R, V3 v, double q1) { return g_cart_to_contr(R, v, q1); }
-/* Bcart(CurviCoord) = {BOB0, 0, 0} * O0   (MFABasis.h:262, Geometry.h:44) */
+/* Bcart(CurviCoord) = {BOB0, 0, 0} * O0   (MFABasis.h:47, Geometry.h:44) */
 static inline V3 g_Bcart(orc_run const *R, double q1)
 {
     double const O0 = R->p.O0;
     V3 r = { g_BOB0(R, q1) * O0, 0 * O0, 0 * O0 };
     return r;
 }
-/* Bcontr(CurviCoord) = {1/D1, 0, 0} * O0   (MFABasis.h:258, Geometry.h:36) */
+/* Bcontr(CurviCoord) = {1/D1, 0, 0} * O0   (MFABasis.h:43, Geometry.h:36) */
 static inline V3 g_Bcontr(orc_run const *R)
 {
     double const O0 = R->p.O0;
     V3 r = { R->inv_D1 * O0, 0 * O0, 0 * O0 };
     return r;
 }
-/* curvilinear -> Cartesian x (MirrorGeometry.cc:199-212) */
+/* curvilinear -> Cartesian x (MirrorGeometry.cc:34-47) */
 static inline double g_curvi_to_cart(orc_run const *R, double q1)
 {
     if (R->homogeneous) {
@@ -226,7 +226,7 @@ static inline double g_curvi_to_cart(orc_run const *R, double q1)
         return tan(xiD1q1) / R->xi;
     }
 }
-/* Bcart(CurviCoord, y, z) = Bcart_div_B0(cotrans(pos), y, z) * B0  (MirrorGeometry.h:158-161, MFABasis.h:287-290) */
+/* Bcart(CurviCoord, y, z) = Bcart_div_B0(cotrans(pos), y, z) * B0  (MirrorGeometry.h:68-71, MFABasis.h:72-75) */
 static inline V3 g_Bcart_yz(orc_run const *R, double q1, double y, double z)
 {
     double const x  = g_curvi_to_cart(R, q1);
@@ -244,7 +244,7 @@ static inline double mask_fn(long inset, double factor, double offset)
     double const tmp = factor * (1 - a / (double)inset);
     return (1 - tmp) * (1 + tmp);
 }
-/* BField::mask / EField::mask (BField.cc:90-98, EField.cc:256-265): whole-domain subdomain, offsets 0 */
+/* BField::mask / EField::mask (BField.cc:40-48, EField.cc:52-61): whole-domain subdomain, offsets 0 */
 static void mask_grid(orc_run const *R, double *g, int ncomp, long inset, double factor)
 {
     long const N = R->Nx;
@@ -425,7 +425,7 @@ static void smooth_grid(orc_run *R, double *g, int nc)
 static double cdcf(orc_run const *R, double Oc, double op) { return ((op * op) * R->p.O0) / Oc; } /* Species.h:42-45 */
 static double ccf(orc_run const *R, double Oc, double op) { return cdcf(R, Oc, op) / R->p.c; }   /* Species.h:46-49 */
 
-/* half_grid (PartSpecies.cc:132-139): B averaged onto the half grid; last ghost NaN */
+/* half_grid (PartSpecies.cc:27-34): B averaged onto the half grid; last ghost NaN */
 static void half_grid(orc_run const *R, double *full, double const *half)
 {
     long const N = R->Nx;
@@ -436,7 +436,7 @@ static void half_grid(orc_run const *R, double *full, double const *half)
         full[3 * (R->M - 1) + c] = NAN;
 }
 
-/* PartSpecies::impl_update_velocity<O> (PartSpecies.cc:266-281) */
+/* PartSpecies::impl_update_velocity<O> (PartSpecies.cc:161-176) */
 static void update_weight(orc_run const *R, Bucket *b, h1d_kinetic_desc const *d, double dt);
 static int  evolves_psd(h1d_kinetic_desc const *d);
 static void update_velocity(orc_run *R, Bucket *b, h1d_kinetic_desc const *d, double *dB, double *E, double dt)
@@ -463,7 +463,7 @@ static void update_velocity(orc_run *R, Bucket *b, h1d_kinetic_desc const *d, do
 }
 /* The equilibrium distribution a species' weights refer to (h1d_kinetic_desc::vdf): n0(q1), the
  * diagonal of nvv0(q1) (field-aligned = Cartesian on the axis) and the physical f0(vel, q1).
- *   MaxwellianVDF    (VDF/MaxwellianVDF.cc:33-92, .h:56-70)
+ *   MaxwellianVDF    (VDF/MaxwellianVDF.cc:33-86, .h:56-70)
  *   LossconeVDF      (VDF/LossconeVDF.cc:15-117, .h:69-83)
  *   PartialShellVDF  (VDF/PartialShellVDF.cc:14-145, .h:62-76)
  *   CounterBeamVDF   (VDF/CounterBeamVDF.cc:14-178, .h:62-75) */
@@ -500,7 +500,7 @@ static double lc_nudge(double beta) { return fabs(beta - 1) < 1e-10 ? beta + cop
 static double lc_beta_eq(h1d_kinetic_desc const *d) { return d->vdf_param[0] < 1e-10 ? 1e-10 : lc_nudge(d->vdf_param[0]); }
 
 /* speed normalisation A(xs) and T / vth^2 of the shell distributions (PartialShellVDF.cc:14-22,
- * CounterBeamVDF.cc:19-35) */
+ * CounterBeamVDF.cc:20-35) */
 static void shell_params(double xs, double *Ab, double *T_vth2)
 {
     *Ab     = .5 * (xs * exp(-xs * xs) + 2 / M_2_SQRTPI * (.5 + xs * xs) * erfc(-xs));
@@ -632,7 +632,7 @@ static void update_weight(orc_run const *R, Bucket *b, h1d_kinetic_desc const *d
     }
 }
 
-/* the equilibrium moments cached by PartSpecies::populate (PartSpecies.cc:80-87) at the interior
+/* the equilibrium moments cached by PartSpecies::populate (PartSpecies.cc:82-89) at the interior
  * half-grid points; ghost cells stay zero */
 static void cache_equilibrium(orc_run *R, int s)
 {
@@ -661,7 +661,7 @@ static void add_equilibrium(orc_run const *R, int s, double *n, double *nV, doub
             nvv[i] = nvv[i] + R->eq2[s][i] * 1.0;
 }
 
-/* PartSpecies::impl_update_pos (PartSpecies.cc:252-264): returns 1 if nothing moved too far */
+/* PartSpecies::impl_update_pos (PartSpecies.cc:147-159): returns 1 if nothing moved too far */
 static int update_pos(orc_run *R, Bucket *b, double dt, double fraction)
 {
     double const scale = 1.0 / fraction;
@@ -676,7 +676,7 @@ static int update_pos(orc_run *R, Bucket *b, double dt, double fraction)
     return ok;
 }
 static void add_equilibrium(orc_run const *R, int s, double *n, double *nV, double *nvv);
-/* PartSpecies::impl_collect_part<O> (PartSpecies.cc:315-329), then the delta-f equilibrium */
+/* PartSpecies::impl_collect_part<O> (PartSpecies.cc:210-224), then the delta-f equilibrium */
 static void collect_part(orc_run *R, Bucket const *b, h1d_kinetic_desc const *d, double *n, double *nV)
 {
     double const q1min = R->half_min;
@@ -704,7 +704,7 @@ static void collect_part(orc_run *R, Bucket const *b, h1d_kinetic_desc const *d,
         nV[i] *= s;
     add_equilibrium(R, (int)(d - R->p.kinetic), n, nV, NULL);
 }
-/* PartSpecies::impl_collect_all (PartSpecies.cc:330-349): always CIC */
+/* PartSpecies::impl_collect_all (PartSpecies.cc:225-244): always CIC */
 static void collect_all(orc_run *R, Bucket const *b, h1d_kinetic_desc const *d, double *n, double *nV, double *nvv)
 {
     double const q1min = R->half_min;
@@ -743,7 +743,7 @@ static void collect_all(orc_run *R, Bucket const *b, h1d_kinetic_desc const *d, 
 }
 
 /* counter-based gyro-phase draw in [-pi, pi) replacing the std::random_device-seeded
- * generator of Delegate::randomize_gyrophase (Delegate.cc:229-239) */
+ * generator of Delegate::randomize_gyrophase (Delegate.cc:146-156) */
 static inline uint64_t mix64(uint64_t z)
 {
     z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
@@ -760,7 +760,7 @@ double orc_gyrophase(uint64_t seed, uint64_t counter, uint64_t species, uint64_t
 }
 
 /* Delegate::boundary_pass(Domain, PartSpecies) with partition + periodic/reflecting pass
- * (Delegate.cc:116-157, 184-228) and SubdomainDelegate's self-exchange (SubdomainDelegate.cc:183-251) */
+ * (Delegate.cc:51-74, 101-145) and SubdomainDelegate's self-exchange (SubdomainDelegate.cc:183-251) */
 static int64_t partition(Bucket *b, int64_t first, int64_t last, int (*pred)(double, double), double ref)
 { /* libstdc++ __partition for bidirectional iterators (two-pointer) */
     for (;;) {
@@ -835,7 +835,7 @@ static void particle_bc(orc_run *R, Bucket *b, int species, uint64_t counter)
     } else { /* absorbing: crossing particles leave the system */
         L->n = Rb->n = 0;
     }
-    /* swap_bucket, then append L then R (Delegate.cc:144, 155-156) */
+    /* swap_bucket, then append L then R (Delegate.cc:61, 72-73) */
     for (int64_t k = 0; k < Rb->n; ++k)
         bucket_push(b, Rb, k);
     for (int64_t k = 0; k < L->n; ++k)
@@ -843,7 +843,7 @@ static void particle_bc(orc_run *R, Bucket *b, int species, uint64_t counter)
 }
 
 /* ------------------------------------------------------------------------------------------------
- * collect_smooth (Domain.hh:155-194) with the charge/current conversion factors
+ * collect_smooth (Domain.hh:35-74) with the charge/current conversion factors
  */
 static void add_scaled(double *dst, double const *src, long count, double f)
 {
@@ -890,7 +890,7 @@ static double const *collect_smooth_J(orc_run *R, double const *mom1, double Oc,
 }
 
 /* ------------------------------------------------------------------------------------------------
- * EField::update (EField.cc:224-330)
+ * EField::update (EField.cc:41-126)
  */
 static void efield_update(orc_run *R, double *E, double const *B, double const *rho, double const *Ji)
 {
@@ -953,7 +953,7 @@ static void efield_update(orc_run *R, double *E, double const *B, double const *
     mask_grid(R, E, 3, R->p.amplitude_damping_inset, R->p.amplitude_damping_factor);
 }
 
-/* BField::update (BField.cc:74-124) */
+/* BField::update (BField.cc:24-74) */
 static void bfield_update(orc_run *R, double *B, double const *E, double dt)
 {
     long const   N         = R->Nx;
@@ -980,7 +980,7 @@ static void bfield_update(orc_run *R, double *B, double const *E, double dt)
     mask_grid(R, B, 3, R->p.amplitude_damping_inset, R->p.amplitude_damping_factor);
 }
 
-/* Current::impl_advance (Current.cc:181-188) on a zeroed J */
+/* Current::impl_advance (Current.cc:45-52) on a zeroed J */
 static void current_advance_impl(orc_run *R, double *J, double const *L, double const *G, double const *B, double const *E, double dt)
 {
     long const N = R->Nx;
@@ -1084,7 +1084,7 @@ static void src_add(orc_run *R, int e, double *charge, double *current)
     addto(charge, collect_smooth_rho_f(R, R->smom0[e], 0.0, n_smooth), R->M);
 }
 
-/* ColdSpecies::impl_update_nV (ColdSpecies.cc:255-262) */
+/* ColdSpecies::impl_update_nV (ColdSpecies.cc:35-42) */
 static void cold_update_vel(orc_run *R, int ci, double const *E, double dt)
 {
     h1d_cold_desc const *d     = &R->p.cold[ci];
@@ -1101,7 +1101,7 @@ static void cold_update_vel(orc_run *R, int ci, double const *E, double dt)
         v[0] = vv.x, v[1] = vv.y, v[2] = vv.z;
     }
 }
-/* ColdSpecies::impl_collect_part (ColdSpecies.cc:273-285) */
+/* ColdSpecies::impl_collect_part (ColdSpecies.cc:53-65) */
 static void cold_collect_part(orc_run *R, double const *n_full, double const *nV_full, double *n, double *nV)
 {
     double const w = R->p.moment_weighting;
@@ -1726,7 +1726,7 @@ void orc_boris(double dt, double c, double O0, double Oc, double *v, double cons
     v[0] = vv.x, v[1] = vv.y, v[2] = vv.z;
 }
 double orc_mask(int64_t inset, double factor, double offset) { return mask_fn((long)inset, factor, offset); }
-/* out: [0] curvi q1 of Cartesian x (MirrorGeometry.cc:189-198), [1] x back from q1,
+/* out: [0] curvi q1 of Cartesian x (MirrorGeometry.cc:24-33), [1] x back from q1,
  *      [2..4] Bcart_div_B0(q1, y, z), [5] Bmag_div_B0(q1), [6] contravariant q1-velocity of v=(1,0,0) */
 void orc_geometry(double xi, double D1, double x, double y, double z, double *out)
 {

@@ -8,7 +8,7 @@ with ``repr`` so that the C++ literal parses back to the identical double.
 
 Single process, single subdomain, no worker threads; gyro-phase
 randomisation of reflected particles is off (the reference seeds it from
-std::random_device, Boundary/Delegate.cc:231).
+std::random_device, Boundary/Delegate.cc:148).
 
 usage: python oracle/ref/gen_inputs.py <config-name> <out-dir>
 """

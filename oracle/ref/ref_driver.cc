@@ -10,9 +10,13 @@
 //   - a raw binary state format to load/dump particles, fields and moments.
 //
 // usage:
-//   ref_driver init  <out.bin>                                   populate with the reference loader
-//   ref_driver run   <in.bin> <steps> <chunks> <out-prefix>      advance_by(steps) x chunks
-//   ref_driver bench <steps> [color divisor]                     time advance_by(steps)
+//   ref_driver init   <out.bin> [color divisor]                   populate with the reference loader
+//                                                                 (PartSpecies::populate(color, divisor))
+//   ref_driver run    <in.bin> <steps> <chunks> <out-prefix>      advance_by(steps) x chunks
+//   ref_driver at     <in.bin> <out-prefix> <s1> <s2> ...         states after s1 < s2 < ... steps in all
+//   ref_driver series <in.bin> <every> <chunks> <out.bin>         advance_by(every) x chunks, the
+//                                                                 EnergyRecorder sums after each chunk
+//   ref_driver bench  <steps> [color divisor]                     time advance_by(steps)
 #include "Boundary/Delegate.h"
 #include "Core/Domain_CAMCL.h"
 #include "Core/Domain_PC.h"
@@ -89,7 +93,7 @@ std::unique_ptr<Domain> make_domain(ParamSet const &params, Delegate *delegate)
     return std::make_unique<Domain_PC>(params, delegate);
 }
 
-// PartSpecies::Nc is private; recompute it the way its constructor does (PartSpecies.cc:150-154)
+// PartSpecies::Nc is private; recompute it the way its constructor does (PartSpecies.cc:45-49)
 template <class Desc>
 double moment_norm(ParamSet const &params, Desc const &desc)
 {
@@ -98,7 +102,7 @@ double moment_norm(ParamSet const &params, Desc const &desc)
         return Np * vdf->Nrefcell_div_Ntotal();
     return 1;
 }
-// the equilibrium moments PartSpecies::populate caches before loading (PartSpecies.cc:80-87), for
+// the equilibrium moments PartSpecies::populate caches before loading (PartSpecies.cc:82-89), for
 // a species whose particles come from a state file instead (as a snapshot load restores them)
 template <class Desc>
 void cache_equilibrium(ParamSet const &params, Desc const &desc, PartSpecies &sp)
@@ -275,6 +279,50 @@ int64_t load(Domain &d, ParamSet const &params, char const *path)
     }
     return step;
 }
+
+// The sums of EnergyRecorder::dump (src/hybrid_1d/Recorder/EnergyRecorder.cc:98-140), which
+// cannot be compiled here (its Recorder base needs MPI): dB^2/2 and dE^2/2 per field-aligned
+// component over the interior / (2 Nx), then for every kinetic and every cold species KE_lab and
+// KE_pla from its moments.  cart_to_mfa is the identity on the field line (MFABasis.h:98-100).
+// Appends 6 + 6 (kinetic + cold) doubles to `out`.
+void energies(Domain const &d, ParamSet const &params, std::vector<double> &out)
+{
+    double dB[3] = {}, dE[3] = {};
+    for (long i = 0; i < d.bfield.size(); ++i) {
+        CartVector const b = d.bfield[i], e = d.efield[i];
+        dB[0] += b.x * b.x, dB[1] += b.y * b.y, dB[2] += b.z * b.z;
+        dE[0] += e.x * e.x, dE[1] += e.y * e.y, dE[2] += e.z * e.z;
+    }
+    for (double v : dB)
+        out.push_back(v / (2 * params.Nx));
+    for (double v : dE)
+        out.push_back(v / (2 * params.Nx));
+    auto species = [&](Species const &sp) {
+        double lab[3] = {}, pla[3] = {};
+        for (long i = 0; i < sp.moment<0>().size(); ++i) {
+            double const n = Real{ sp.moment<0>()[i] };
+            if (n < 1e-15)
+                continue;
+            CartTensor const nvv = sp.moment<2>()[i];
+            CartVector const nV  = sp.moment<1>()[i];
+            double const     diag[3] = { nvv.xx, nvv.yy, nvv.zz };
+            double const     v[3]    = { nV.x, nV.y, nV.z };
+            for (int k = 0; k < 3; ++k) {
+                lab[k] += diag[k];
+                pla[k] += diag[k] - v[k] * v[k] / n;
+            }
+        }
+        double const f = sp.energy_density_conversion_factor() / (2 * params.Nx);
+        for (double x : lab)
+            out.push_back(x * f);
+        for (double x : pla)
+            out.push_back(x * f);
+    };
+    for (PartSpecies const &sp : d.part_species)
+        species(sp);
+    for (ColdSpecies const &sp : d.cold_species)
+        species(sp);
+}
 } // namespace
 
 int main(int argc, char **argv)
@@ -287,12 +335,43 @@ try {
     SerialDelegate    delegate;
     auto              domain = make_domain(params, &delegate);
 
-    if (mode == "init" && argc == 3) {
+    if (mode == "init" && (argc == 3 || argc == 5)) {
+        long const color   = argc == 5 ? std::atol(argv[3]) : 0;
+        long const divisor = argc == 5 ? std::atol(argv[4]) : 1;
         for (PartSpecies &sp : domain->part_species)
-            sp.populate(0, 1);
+            sp.populate(color, divisor);
         for (ColdSpecies &sp : domain->cold_species)
-            sp.populate(0, 1);
+            sp.populate(color, divisor);
         dump(*domain, params, argv[2], 0);
+        return 0;
+    }
+    if (mode == "at" && argc >= 5) {
+        int64_t step = load(*domain, params, argv[2]);
+        cache_equilibria(params, params.part_descs, *domain, ParamSet::part_indices{});
+        long done = 0;
+        for (int k = 4; k < argc; ++k) {
+            long const target = std::atol(argv[k]);
+            if (target <= done)
+                throw std::invalid_argument{ "step counts must increase" };
+            domain->advance_by(static_cast<unsigned>(target - done));
+            step += target - done;
+            done = target;
+            dump(*domain, params, (std::string{ argv[3] } + std::to_string(target) + ".bin").c_str(), step);
+        }
+        return 0;
+    }
+    if (mode == "series" && argc == 6) {
+        load(*domain, params, argv[2]);
+        cache_equilibria(params, params.part_descs, *domain, ParamSet::part_indices{});
+        long const          every  = std::atol(argv[3]);
+        long const          chunks = std::atol(argv[4]);
+        std::vector<double> out;
+        for (long k = 0; k < chunks; ++k) {
+            domain->advance_by(static_cast<unsigned>(every));
+            energies(*domain, params, out);
+        }
+        Writer w{ argv[5] };
+        w.put(out.data(), out.size());
         return 0;
     }
     if (mode == "run" && argc == 6) {

@@ -7,7 +7,7 @@ import numpy as np
 def with_reference_norms(cfg, init):
     """``cfg`` with every kinetic species' moment normalisation (PartSpecies::Nc) taken from the
     header of a reference state file, as an integration of the reference passes it to the C ABI;
-    the reference integrates the counter-beam density numerically (VDFHelper.h:43-64)."""
+    the reference integrates the counter-beam density numerically (VDFHelper.h:47-70)."""
     kin = [dataclasses.replace(k, norm=float(n)) for k, n in zip(cfg.kinetic, init["moment_norm"])]
     return cfg.replace(kinetic=kin)
 
@@ -26,6 +26,20 @@ def by_pid(p):
     """Particle arrays reordered by upload index."""
     order = np.argsort(p["pid"], kind="stable")
     return {k: np.asarray(v)[order] for k, v in p.items()}
+
+
+def attach_pid(ref, init):
+    """A reference state (tests/golden/state_io.read_state) with every particle's "pid" set to its
+    index in the initial state ``init`` it was advanced from (the upload index the C ABI reports),
+    found through the reference's particle ids; returns ``ref``."""
+    for p, p0 in zip(ref["particles"], init["particles"]):
+        id0 = np.asarray(p0["id"])
+        order = np.argsort(id0, kind="stable")
+        k = np.searchsorted(id0[order], p["id"])
+        if not np.array_equal(id0[order][np.minimum(k, id0.size - 1)], p["id"]):
+            raise ValueError("reference state holds particle ids the initial state does not")
+        p["pid"] = order[k]
+    return ref
 
 
 def cell_keys(q1, Nx):

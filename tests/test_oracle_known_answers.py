@@ -127,7 +127,7 @@ def test_geometry_known_answers(lib):  # test-Geometry.cc:100-213
     assert g[6] == pytest.approx(1 / (2 * 3.637376), rel=1e-10)
 
 
-def test_masking_function(lib):  # test-MaskingFunction.cc:12-56
+def test_masking_function(lib):  # test-MaskingFunction.cc:12-51
     assert lib.orc_mask(0, 0.0, 0) == 1 and lib.orc_mask(0, 0.0, 1) == 1
     for off in (0, 1, 2):
         assert lib.orc_mask(0, 0.5, off) == pytest.approx(1, rel=1e-10)

@@ -54,7 +54,7 @@ def test_oracle_bit_exact_vs_reference(oracle_lib, name, steps):
     """Bit for bit, except for the counter-beam equilibrium (configs.PARITY_ROUNDING): its density
     and f0 need Dawson's integral, which the reference takes from the Faddeeva package
     (LibPIC/PIC/Misc/Faddeeva.cc) and the oracle evaluates by its own method, and its PartSpecies::Nc
-    comes from the reference's numerical integration of the density (VDFHelper.h:43-64, about
+    comes from the reference's numerical integration of the density (VDFHelper.h:47-70, about
     1e-9 from the exact integral), so there the oracle takes Nc from the state file and agrees to
     rounding (8e-15 in the weights after ten steps; bound 1e-13)."""
     cfg = h.configs.PARITY[name]()
