@@ -890,19 +890,29 @@ int pc_step(h1d_run *run)
     return H1D_OK;
 }
 
+// The C-ABI status of a device status word and its message: the first of its bits in the order
+// moved too far, timeout, outside the grid / non-finite; a bit the kernels do not define is a CUDA
+// error.
+int status_of_bits(unsigned s, std::string &msg)
+{
+    if (s & ST_MOVED_TOO_FAR)
+        return msg = "PartSpecies::update_pos - particle(s) moved too far", H1D_ERR_MOVED_TOO_FAR;
+    if (s & ST_TIMEOUT)
+        return msg = "a particle-pipeline barrier wait timed out", H1D_ERR_TIMEOUT;
+    if (s & (ST_OUT_OF_RANGE | ST_NAN))
+        return msg = "particle(s) outside the padded grid (non-finite or lost particle state)", H1D_ERR_NAN;
+    if (s)
+        return msg = fmt("device status 0x%x", s), H1D_ERR_CUDA;
+    return H1D_OK;
+}
+
 int check_status(h1d_run *run)
 {
     CU(cudaStreamSynchronize(run->stream));
     CU(cudaMemcpy(run->h_status, run->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost));
-    unsigned const s = *run->h_status;
-    if (s & ST_MOVED_TOO_FAR)
-        return set_err(run, H1D_ERR_MOVED_TOO_FAR, "PartSpecies::update_pos - particle(s) moved too far");
-    if (s & ST_TIMEOUT)
-        return set_err(run, H1D_ERR_TIMEOUT, "a particle-pipeline barrier wait timed out");
-    if (s & ST_OUT_OF_RANGE)
-        return set_err(run, H1D_ERR_NAN, "particle(s) outside the padded grid (non-finite or lost particle state)");
-    if (s)
-        return set_err(run, H1D_ERR_CUDA, fmt("device status 0x%x", s));
+    std::string m;
+    if (int const st = status_of_bits(*run->h_status, m))
+        return set_err(run, st, m);
     return H1D_OK;
 }
 
@@ -1529,10 +1539,16 @@ int h1d_collect_moments_noalloc(int64_t Nx, double moment_norm, int particle_bc,
     double            *raw    = scratch;
     double            *fin    = scratch + 10 * M;
     unsigned          *status = reinterpret_cast<unsigned *>(scratch + 20 * NOALLOC_M);
+    // a failure after work was queued waits for that work first, so that a failed call leaves
+    // nothing running on the shared scratch
+    auto const fail = [st] {
+        cudaStreamSynchronize(st);
+        return H1D_ERR_CUDA;
+    };
     // the raw sums are accumulated with atomics and must start at zero, as must the status word
     if (cudaMemsetAsync(raw, 0, sizeof(double) * 10 * M, st) != cudaSuccess
         || cudaMemsetAsync(status, 0, sizeof(unsigned), st) != cudaSuccess)
-        return H1D_ERR_CUDA;
+        return fail();
     if (n > 0) {
         MomentArgs a{};
         a.q1 = q1, a.vx = vx, a.vy = vy, a.vz = vz, a.w = w, a.n = n, a.Nx = static_cast<int>(Nx);
@@ -1547,21 +1563,23 @@ int h1d_collect_moments_noalloc(int64_t Nx, double moment_norm, int particle_bc,
         int64_t const chunks = (n + 32LL * a.ppt - 1) / (32LL * a.ppt);
         moments_kernel<<<static_cast<unsigned>((chunks + 3) / 4), MOM_THREADS, 0, st>>>(a);
         if (cudaGetLastError() != cudaSuccess)
-            return H1D_ERR_CUDA;
+            return fail();
     }
     if (launch_finalize_kinetic(raw, nullptr, fin, static_cast<int>(Nx), 1.0 / moment_norm, particle_bc == H1D_BC_PERIODIC ? 0 : 1, st)
             != cudaSuccess
         || cudaMemcpyAsync(n_out, fin, sizeof(double) * M, cudaMemcpyDeviceToDevice, st) != cudaSuccess
         || cudaMemcpyAsync(nV_out, fin + M, sizeof(double) * 3 * M, cudaMemcpyDeviceToDevice, st) != cudaSuccess
         || cudaMemcpyAsync(nvv_out, fin + 4 * M, sizeof(double) * 6 * M, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
-        return H1D_ERR_CUDA;
+        return fail();
     unsigned hstatus = 0;
     if (cudaMemcpyAsync(&hstatus, status, sizeof hstatus, cudaMemcpyDeviceToHost, st) != cudaSuccess
         || cudaStreamSynchronize(st) != cudaSuccess)
-        return H1D_ERR_CUDA;
-    if (hstatus & ST_OUT_OF_RANGE)
-        return H1D_ERR_NAN;
-    return hstatus ? H1D_ERR_CUDA : H1D_OK;
+        return fail();
+    std::string msg;
+    int const   code = status_of_bits(hstatus, msg);
+    if (code)
+        std::fprintf(stderr, "h1d_collect_moments_noalloc: %s\n", msg.c_str());
+    return code;
 }
 
 int h1d_create(h1d_params const *params, h1d_run **out)

@@ -9,7 +9,7 @@
  *   predictor-corrector B/E/current cycle that consumes the moments.
  *
  * Every entry point replaces one piece of the reference's `Domain` interface, so that a
- * `Domain` subclass can forward `advance_by` here (see INTEGRATION.md for the adapter):
+ * `Domain` subclass can forward `advance_by` here:
  *
  *   h1d_create            <- Domain_CAMCL / Domain_PC constructors
  *                            (src/hybrid_1d/Core/Domain_CAMCL.cc:11, Core/Domain_PC.cc:11,
@@ -291,12 +291,16 @@ int h1d_math_check(const double *x, int64_t n, double *out);
  * defeats its accounting), or a latency-critical loop where an allocation, which may
  * synchronise the device, is not acceptable.
  *
- * Computes what h1d_download_moments returns -- n, nV, nvv with the CIC shape, scaled by
+ * Computes the weighted sums of h1d_download_moments -- n, nV, nvv with the CIC shape, scaled by
  * 1/moment_norm and ghost-folded for the given particle boundary (PartSpecies::collect_all +
  * boundary_gather) -- from particles the caller holds in device memory, into device buffers the
- * caller provides (GridArray layout: n[Nx+6], nV[(Nx+6)*3], nvv[(Nx+6)*6]).  Work is enqueued on
- * `stream` (a cudaStream_t; NULL for the legacy default stream) and the call returns after that
- * stream has finished it.
+ * caller provides (GridArray layout: n[Nx+6], nV[(Nx+6)*3], nvv[(Nx+6)*6]).  These are the moments
+ * of a full-f species; for a delta-f species h1d_download_moments also adds the equilibrium
+ * moments n0 and nvv0 on the interior (PartSpecies.cc:134-142), which a caller of this entry point
+ * adds itself.  Work is enqueued on `stream` (a cudaStream_t; NULL for the legacy default stream)
+ * and the call returns after that stream has finished it.  A particle outside the padded grid
+ * (or with a non-finite position) gives H1D_ERR_NAN; a failed call has finished its queued work
+ * before it returns.
  *
  * Scratch space is a fixed array compiled into this library (a static __device__ array of
  * 20 * (H1D_NOALLOC_MAX_NX + 6) doubles plus a status word, about 0.65 MB, held on every GPU that
@@ -304,7 +308,8 @@ int h1d_math_check(const double *x, int64_t n, double *out);
  * H1D_ERR_INVALID_ARG.  The first call on a device looks up that array's device address (once per
  * device, with the device current); make that first call before any stream capture.  All calls
  * share the one array: calls that overlap on the GPU (concurrent streams or threads) race and
- * must be serialised by the caller. */
+ * must be serialised by the caller.  The looked-up address is kept for the life of the process:
+ * do not call this entry point again on a device after cudaDeviceReset. */
 #define H1D_NOALLOC_MAX_NX 4096
 int h1d_collect_moments_noalloc(int64_t Nx, double moment_norm, int particle_bc, const double *q1, const double *vx,
                                 const double *vy, const double *vz, const double *w, int64_t n, double *n_out,
