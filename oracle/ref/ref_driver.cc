@@ -17,9 +17,17 @@
 //   ref_driver series <in.bin> <every> <chunks> <out.bin>         advance_by(every) x chunks, the
 //                                                                 EnergyRecorder sums after each chunk
 //   ref_driver bench  <steps> [color divisor]                     time advance_by(steps)
+//
+// Built with -DH1D_GPU_DOMAIN (oracle/Makefile target `gpu`, binary ref_driver_gpu) it also runs
+// the drop-in GPU Domain of the library (hybrid_code-hfemic_wave_b200/adapter/Domain_GPU.h) in
+// place of Domain_CAMCL / Domain_PC, through the same state files:
+//   ref_driver_gpu gpu_run <in.bin> <steps> <chunks> <out-prefix> fp64|mixed
 #include "Boundary/Delegate.h"
 #include "Core/Domain_CAMCL.h"
 #include "Core/Domain_PC.h"
+#if defined(H1D_GPU_DOMAIN)
+#include "Domain_GPU.h"
+#endif
 
 #include <chrono>
 #include <cstdint>
@@ -386,6 +394,30 @@ try {
         }
         return 0;
     }
+#if defined(H1D_GPU_DOMAIN)
+    if (mode == "gpu_run" && argc == 7) {
+        std::string const prec = argv[6];
+        if (prec != "fp64" && prec != "mixed")
+            throw std::invalid_argument{ "precision must be fp64 or mixed" };
+        int const                   precision = prec == "fp64" ? H1D_PREC_FP64 : H1D_PREC_MIXED;
+        std::unique_ptr<Domain_GPU> gpu;
+        if (ParamSet::algorithm == CAMCL)
+            gpu = std::make_unique<Domain_CAMCL_GPU>(params, &delegate, precision);
+        else
+            gpu = std::make_unique<Domain_PC_GPU>(params, &delegate, precision);
+        int64_t step = load(*gpu, params, argv[2]);
+        cache_equilibria(params, params.part_descs, *gpu, ParamSet::part_indices{});
+        long const steps  = std::atol(argv[3]);
+        long const chunks = std::atol(argv[4]);
+        for (long k = 1; k <= chunks; ++k) {
+            gpu->advance_by(static_cast<unsigned>(steps));
+            step += steps;
+            gpu->sync_particles(); // as the Driver does before particle recorders and snapshots
+            dump(*gpu, params, (std::string{ argv[5] } + std::to_string(k) + ".bin").c_str(), step);
+        }
+        return 0;
+    }
+#endif
     if (mode == "bench" && (argc == 3 || argc == 5)) {
         long const steps   = std::atol(argv[2]);
         long const color   = argc == 5 ? std::atol(argv[3]) : 0;
@@ -412,6 +444,9 @@ try {
         return 0;
     }
     throw std::invalid_argument{ "bad arguments" };
+} catch (std::domain_error const &e) { // PartSpecies::update_pos (Core/PartSpecies.cc:113)
+    std::fprintf(stderr, "ref_driver: std::domain_error: %s\n", e.what());
+    return 1;
 } catch (std::exception const &e) {
     std::fprintf(stderr, "ref_driver: %s\n", e.what());
     return 1;

@@ -56,3 +56,27 @@ def read_state(path):
     if off != len(buf):
         raise ValueError("trailing bytes in state file")
     return st
+
+
+def write_state(path, st):
+    """Write a state dict (as read_state returns it) in the "H1DSTAT2" layout above."""
+    nk, nc = len(st["particles"]), len(st["cold"])
+    with open(path, "wb") as f:
+        f.write(b"H1DSTAT2")
+        np.array([st["Nx"], st["pad"], nk, nc, st["step"]], dtype="<i8").tofile(f)
+        np.asarray(st["moment_norm"], dtype="<f8").tofile(f)
+        for p in st["particles"]:
+            np.array([p["q1"].size], dtype="<i8").tofile(f)
+            for k in ("q1", "vx", "vy", "vz", "w"):
+                np.asarray(p[k], dtype="<f8").tofile(f)
+            np.asarray(p["id"], dtype="<i8").tofile(f)
+            np.asarray(p["real_f"], dtype="<f8").tofile(f)
+            np.asarray(p["marker"], dtype="<f8").tofile(f)
+        for k in ("B", "E", "charge", "current"):
+            np.asarray(st[k], dtype="<f8").tofile(f)
+        for m in st["moments"]:
+            for k in ("n", "nV", "nvv"):
+                np.asarray(m[k], dtype="<f8").tofile(f)
+        for c in st["cold"]:
+            for k in ("n_full", "nV_full", "n", "nV", "nvv"):
+                np.asarray(c[k], dtype="<f8").tofile(f)
