@@ -70,34 +70,84 @@ def measured_peak():
 
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+    """SM clock and clock-event reasons while the timed region runs, read (never set) through NVML:
+    one sample when the region opens, samples about every millisecond while it runs, and one when
+    it closes, so that even a region of a few milliseconds carries its own clock record.  Falls
+    back to an nvidia-smi polling loop when NVML cannot be loaded."""
 
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index):
         self.index = index
+        self.samples = []  # (sm_mhz, max_mhz, reasons)
+        self.nvml = None
         self.proc = None
-        self.lines = []
+        self.stop = threading.Event()
+        self.thread = None
+
+    def _sample_nvml(self):
+        nv = self.nvml
+        sm = nv.nvmlDeviceGetClockInfo(self.handle, nv.NVML_CLOCK_SM)
+        mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self.handle)
+        reasons = [name for name, const in self.REASONS if mask & getattr(nv, const)]
+        self.samples.append((float(sm), self.max_mhz, reasons))
+
+    def _loop_nvml(self):
+        while not self.stop.wait(0.001):
+            try:
+                self._sample_nvml()
+            except Exception:
+                return
+
+    def _loop_smi(self):
+        for line in self.proc.stdout:
+            f = [x.strip() for x in line.split(",")]
+            try:
+                reasons = [n for n, v in zip([r[0] for r in self.REASONS], f[5:9]) if v.lower().startswith("active")]
+                self.samples.append((float(f[1]), float(f[2]), reasons))
+            except (ValueError, IndexError):
+                continue
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "50"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.handle = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.handle, pynvml.NVML_CLOCK_SM))
+            self._sample_nvml()
+            self.thread = threading.Thread(target=self._loop_nvml, daemon=True)
             self.thread.start()
         except Exception:
-            self.proc = None
+            self.nvml = None
+            try:
+                self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                              "--format=csv,noheader,nounits", "-lms", "50"],
+                                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.thread = threading.Thread(target=self._loop_smi, daemon=True)
+                self.thread.start()
+            except Exception:
+                self.proc = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
-
     def __exit__(self, *a):
-        if self.proc:
+        self.stop.set()
+        if self.nvml is not None:
+            if self.thread:
+                self.thread.join(timeout=1)
+            try:
+                self._sample_nvml()
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
+        elif self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -105,22 +155,11 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        sm = [s[0] for s in self.samples]
+        reasons = sorted({r for s in self.samples for r in s[2]})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": self.samples[-1][1] if self.samples else None, "reasons": reasons,
+                "samples": len(sm), "source": "nvml" if self.nvml is not None else "nvidia-smi"}
 
 
 def workload(h, name):
@@ -167,6 +206,80 @@ def cpu_baseline_port(h, cfg, budget_s=15.0):
         dt = time.perf_counter() - t0
     return {"value": n * steps / dt, "unit": METRIC, "cores": 1, "kind": "port",
             "sample": f"{cfg.name} with 1/16 of the particles ({n}) x {steps} steps, one core"}
+
+
+def _cpu_member_rate(job):
+    """Worker: particle-steps/s of the C oracle (the reference's step restated in C, pinned bit for
+    bit to the reference build; one core) on a bounded sample of one run of the ensemble
+    distribution -- at most `target` of its particles, a few steps -- and its full particle count."""
+    seed, target = job
+    h = _package()
+    from hfemic_b200.loader import initial_state
+
+    cfg = h.configs.ensemble_member(seed, precision=h.configs.PREC_FP64)
+    full = cfg.n_particles
+    st = initial_state(cfg, seed=seed, fraction=min(1.0, target / full))
+    n = sum(p["q1"].size for p in st["particles"])
+    with h.Run(cfg, os.path.join(ROOT, "oracle", "liboracle.so"), "orc_") as r:
+        r.upload_state(st)
+        r.advance(1)
+        k = max(2, int(2e6 / max(n, 1)))
+        t0 = time.perf_counter()
+        r.advance(k)
+        dt = time.perf_counter() - t0
+    return full, n * k / dt, n, k
+
+
+def cpu_ensemble_serving_baselines(h, members=64, steps=500, n_requests=48, rate=4.0, seed=2024, target=100_000):
+    """CPU baselines of the ensemble and the serving workloads on all host cores (P processes).
+    Every run's CPU rate is measured on a bounded sample (<= `target` particles, a few steps, one
+    core each, C oracle); the ensemble's time is the makespan of its runs' full work
+    (particles x steps / rate) on P cores (longest first onto the least loaded core), and the
+    serving stream -- the same seeded Poisson arrivals and step counts as serving_measure -- is
+    replayed on a P-core first-come-first-served pool with those service times."""
+    import heapq
+    import multiprocessing as mp
+
+    import numpy as np
+
+    P = max(1, os.cpu_count() or 1)
+    ens_seeds = list(range(members))
+    srv_seeds = [1000 + i for i in range(n_requests)]
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(min(P, len(ens_seeds) + len(srv_seeds))) as pool:
+        res = pool.map(_cpu_member_rate, [(sd, target) for sd in ens_seeds + srv_seeds], chunksize=1)
+    wall = time.perf_counter() - t0
+    ens, srv = res[:members], res[members:]
+    work = sorted((full * steps / r for full, r, _, _ in ens), reverse=True)
+    loads = [0.0] * P
+    for w in work:
+        i = loads.index(min(loads))
+        loads[i] += w
+    makespan = max(loads)
+    sample = (f"each run on <= {target} of its particles for a few steps (C oracle, one core per run), "
+              f"scaled to its full particles x steps; {P} host cores; sampling took {wall:.1f} s")
+    ens_line = {"runs_per_s": members / makespan, "value": sum(f for f, _, _, _ in ens) * steps / makespan,
+                "unit": METRIC, "cores": P, "kind": "port", "makespan_s": makespan,
+                "sample": f"{members} runs x {steps} steps scheduled longest-first on {P} cores; " + sample}
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+    req_steps = rng.integers(200, 2001, n_requests)
+    free = [0.0] * P
+    heapq.heapify(free)
+    lat, done = [], []
+    for a, (full, r, _, _), k in zip(arrivals, srv, req_steps):
+        start = max(a, heapq.heappop(free))
+        end = start + full * int(k) / r
+        heapq.heappush(free, end)
+        lat.append(end - a)
+        done.append(end)
+    lat = np.array(lat)
+    srv_line = {"runs_per_s": n_requests / (max(done) - arrivals[0]), "p50_s": float(np.percentile(lat, 50)),
+                "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()), "cores": P, "kind": "port",
+                "sample": f"the serving stream (Poisson, mean {rate}/s, {n_requests} requests, steps U[200, 2000], "
+                          f"seed {seed}) replayed first-come-first-served on {P} cores with service times "
+                          "particles x steps / rate; " + sample}
+    return ens_line, srv_line
 
 
 def run_reference_arm(args, h, rank):
@@ -577,18 +690,24 @@ def main():
             extras["mixed_over_fp64"] = value / v64
             extras["error_vs_fp64"] = error_vs_fp64(h, cfg, st)
         if cfg.name != "config2_tsc_mirror_nx2048":
+            # the FP64 drop-in configuration with the reference's reflecting walls (the parity form)
+            # and with the particle-absorbing walls the configuration names (an extension: the
+            # reference has periodic and reflecting particle boundaries only)
             c2 = h.configs.config2()
             st2 = initial_state(c2, seed=2000 + rank)
-            t2 = TimedRun(h, c2, st2)
-            tuned2 = t2.warm(args.warmup, autotune=not args.no_autotune)
-            k2 = max(args.steps, 100)
-            ms2, prof2, _ = t2.timed(k2, world)
-            v2 = t2.n_particles * k2 * world / (ms2 / 1e3)
-            t2.close()
-            extras["drop_in_fp64"] = {"workload": c2.name, "particles_per_gpu": t2.n_particles, "value": v2,
-                                      "autotune": tuned2,
-                                      "unit": METRIC, "ms_per_step": ms2 / k2,
-                                      "roofline": roofline_of(prof2, "fp64", k2, traffic)}
+            for key, bc in (("drop_in_fp64", h.configs.BC_REFLECTING), ("drop_in_fp64_absorbing", h.configs.BC_ABSORBING)):
+                cb = c2.replace(particle_bc=bc)
+                t2 = TimedRun(h, cb, st2)
+                tuned2 = t2.warm(args.warmup, autotune=not args.no_autotune)
+                k2 = max(args.steps, 100)
+                ms2, prof2, _ = t2.timed(k2, world)
+                v2 = t2.n_particles * k2 * world / (ms2 / 1e3)
+                t2.close()
+                extras[key] = {"workload": c2.name, "particle_bc": "reflecting" if bc == h.configs.BC_REFLECTING else
+                               "absorbing (extension; the reference has no absorbing boundary)",
+                               "particles_per_gpu": t2.n_particles, "value": v2, "autotune": tuned2,
+                               "unit": METRIC, "ms_per_step": ms2 / k2,
+                               "roofline": roofline_of(prof2, "fp64", k2, traffic)}
             del st2
 
     e2e = None if args.no_e2e else e2e_measure(h, cfg, st, args.steps, world)
@@ -602,6 +721,10 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_reference(cfg) or cpu_baseline_port(h, cfg)
+        if not args.no_ensemble:
+            ens_cpu, srv_cpu = cpu_ensemble_serving_baselines(h)
+            extras["ensemble"]["cpu_baseline"] = ens_cpu
+            extras["serving"]["cpu_baseline"] = srv_cpu
 
     if world > 1:
         dist.destroy_process_group()

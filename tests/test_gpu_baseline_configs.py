@@ -1,0 +1,149 @@
+"""Parity of the CUDA path with the reference itself on the BASELINE run configurations.
+
+The reference's hot path, compiled from its sources with each configuration's Inputs.h
+(oracle/_ref/<config>/ref_driver), loads the particles with its own loader and advances them on
+the host; the CUDA path starts from the identical state file.  Three parts:
+
+  1. one step at the configurations' own sizes -- config 2 (Nx 2048, mirror xi 0.002, masking over
+     128 cells, H+ and He+ with 1000 TSC particles per cell each: 4.1M particles) in full, and
+     config 3 (Nx 4096, CIC) with 1/4 of its 16.4M particles (PartSpecies::populate(0, 4)):
+     fields, sources, moments and particles within 1e-12 (max-norm relative), every particle's
+     cell index identical; the mixed-precision path within 1e-4;
+  2. the error-growth curve: FP64 after 1, 10, 30 and 100 steps (config 2 with 1/4, config 3 with
+     1/16 of the particles) under bounds that grow with the step count, as round-off differences
+     of the deposit order are amplified by the plasma's dynamics;
+  3. the energy time series of EnergyRecorder::dump over config 1's full 1000 steps, every step,
+     FP64 and mixed precision, against the reference's own series.
+
+The tolerances of parts 2 and 3 are written next to each check; they are set from the measured
+curves with a margin and stay far below the quantities' own variation over the run.
+"""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+from parity_util import attach_pid, cell_mismatches, state_errors, with_reference_norms
+from state_io import read_state
+
+import hfemic_b200 as h
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+C1, C2, C3 = "config1_cic_periodic_nx256", "config2_tsc_mirror_nx2048", "config3_cic_periodic_nx4096"
+
+# FP64 max-norm relative error bounds of the growth curve, by step count (part 2)
+GROWTH_FP64 = {1: 1e-12, 10: 1e-10, 30: 1e-9, 100: 1e-7}
+# part 3: |dB^2/2 (GPU) - dB^2/2 (reference)| / max over the run of dB^2/2 (reference), every step;
+# the same for every particle-energy component relative to its own maximum
+SERIES_FP64, SERIES_MIXED = 1e-6, 1e-3
+
+
+def _driver(name):
+    path = os.path.join(ROOT, "oracle", "_ref", name, "ref_driver")
+    if not os.path.exists(path):
+        pytest.fail(f"{path} is not built (make -C oracle ref REF=<reference tree>)")
+    return path
+
+
+@pytest.fixture(scope="module")
+def workdir():
+    with tempfile.TemporaryDirectory(prefix="h1d_baseline_") as d:
+        yield d
+
+
+def _init(workdir, name, div):
+    path = os.path.join(workdir, f"{name}_d{div}.init.bin")
+    if not os.path.exists(path):
+        subprocess.run([_driver(name), "init", path, "0", str(div)], check=True, timeout=900)
+    return path
+
+
+def _reference_at(workdir, name, div, steps):
+    ip = _init(workdir, name, div)
+    prefix = os.path.join(workdir, f"{name}_d{div}_at")
+    if any(not os.path.exists(f"{prefix}{s}.bin") for s in steps):
+        subprocess.run([_driver(name), "at", ip, prefix, *map(str, steps)], check=True, timeout=1800)
+    return ip, {s: f"{prefix}{s}.bin" for s in steps}
+
+
+def _cfg(name, init, precision):
+    cfg = with_reference_norms(h.configs.PRESETS[name](), init)
+    return cfg.replace(precision=precision)
+
+
+@pytest.mark.parametrize("name, div", [(C2, 1), (C3, 4)])
+def test_one_step_at_baseline_size(workdir, gpu_lib, name, div):
+    ip, at = _reference_at(workdir, name, div, [1])
+    init = read_state(ip)
+    ref = attach_pid(read_state(at[1]), init)
+    for prec, tol in ((h.configs.PREC_FP64, 1e-12), (h.configs.PREC_MIXED, 1e-4)):
+        cfg = _cfg(name, init, prec)
+        with h.Run(cfg, gpu_lib, "h1d_") as g:
+            g.upload_state(init)
+            g.advance(1)
+            st = g.state()
+        errs = state_errors(st, ref, cfg)
+        if prec == h.configs.PREC_MIXED:
+            errs = {k: v for k, v in errs.items() if "particles" not in k}
+        print(name, div, "mixed" if prec else "fp64", f"max {max(errs.values()):.2e}",
+              {k: f"{v:.1e}" for k, v in errs.items()})
+        bad = {k: v for k, v in errs.items() if not v <= tol}
+        assert not bad, bad
+        if prec == h.configs.PREC_FP64:
+            mism = cell_mismatches(st, ref, cfg)
+            assert all(d < 1e-12 for _, _, d in mism), mism[:10]
+
+
+@pytest.mark.parametrize("name, div", [(C2, 4), (C3, 16)])
+def test_error_growth(workdir, gpu_lib, name, div):
+    steps = sorted(GROWTH_FP64)
+    ip, at = _reference_at(workdir, name, div, steps)
+    init = read_state(ip)
+    cfg = _cfg(name, init, h.configs.PREC_FP64)
+    curve = {}
+    with h.Run(cfg, gpu_lib, "h1d_") as g:
+        g.upload_state(init)
+        done = 0
+        for s in steps:
+            g.advance(s - done)
+            done = s
+            errs = state_errors(g.state(), attach_pid(read_state(at[s]), init), cfg)
+            curve[s] = max(errs.values())
+    print(name, div, "FP64 error growth:", {s: f"{e:.2e}" for s, e in curve.items()})
+    for s in steps:
+        assert curve[s] <= GROWTH_FP64[s], (s, curve[s])
+
+
+def test_energy_series_config1(workdir, gpu_lib):
+    ip = _init(workdir, C1, 1)
+    init = read_state(ip)
+    steps = h.configs.PRESETS[C1]().steps
+    ns = 2  # one kinetic and one cold species
+    out = os.path.join(workdir, "c1_series.bin")
+    subprocess.run([_driver(C1), "series", ip, "1", str(steps), out], check=True, timeout=900)
+    ref = np.fromfile(out).reshape(steps, 6 + 6 * ns)
+    wave_ref = ref[:, :3].sum(axis=1)
+    scale = wave_ref.max()
+    assert scale > 10 * wave_ref[0]  # the instability grows the wave energy over the run
+    kin_ref = ref[:, 6:]
+    kin_scale = np.abs(kin_ref).max(axis=0)
+    cols = kin_scale > 0
+    for prec, tol in ((h.configs.PREC_FP64, SERIES_FP64), (h.configs.PREC_MIXED, SERIES_MIXED)):
+        cfg = _cfg(C1, init, prec)
+        rows = []
+        with h.Run(cfg, gpu_lib, "h1d_") as g:
+            g.upload_state(init)
+            for _ in range(steps):
+                g.advance(1)
+                e = g.energy()
+                rows.append(np.concatenate([e["dB2O2"], e["dE2O2"], e["KE_lab"].ravel(), e["KE_pla"].ravel()]))
+        rows = np.array(rows)
+        err = np.abs(rows[:, :3].sum(axis=1) - wave_ref) / scale
+        kin = (np.abs(rows[:, 6:] - kin_ref)[:, cols] / kin_scale[cols]).max(axis=0)
+        print("config1", "mixed" if prec else "fp64", f"wave max {err.max():.2e} at step {err.argmax() + 1},",
+              f"particle energies max {kin.max():.2e}; wave error every 100 steps:",
+              [f"{x:.1e}" for x in err[99::100]])
+        assert err.max() <= tol, (err.max(), int(err.argmax()) + 1)
+        assert kin.max() <= tol
