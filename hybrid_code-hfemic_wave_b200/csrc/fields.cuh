@@ -76,7 +76,8 @@ struct FieldArgs {
     int           ne;
     KinSrc        e[MAXE];
     double        dt, sub_dt, c_light, sqrt_g, O0, inv_D1;
-    int           m; // n_subcycles
+    int           m;  // n_subcycles
+    int           fb; // CAM-CL: sources smoothed together per group of barrier phases (<= FB_MAX)
     // electron fluid (EField.cc:63-87)
     double        mOeOO0oe2, gamma, O02beO2, cO2, cOsqrtg;
     // predictor-corrector (Domain_PC.cc:84-205): phase 0 initial sources, 1 predicted fields,
@@ -148,12 +149,22 @@ static __device__ SV smooth_n(Cell const &C, int n, double *a, double *v, double
     return { a, v };
 }
 
+// the half-grid geometry and masking factors of one cell, as Ohm's law needs them (a Cell has them
+// too, so the helpers below take either)
+struct HalfGeo {
+    double hcx, hcy, hcz, hnx, hny, hnz, mp1, mp2, ma1, ma2;
+};
+
 __device__ __forceinline__ d3 covar_full(Cell const &C, d3 b) { return { C.fcx * b.x, C.fcy * b.y, C.fcz * b.z }; }
 __device__ __forceinline__ d3 contr_full(Cell const &C, d3 b) { return { C.fnx * b.x, C.fny * b.y, C.fnz * b.z }; }
-__device__ __forceinline__ d3 covar_half(Cell const &C, d3 b) { return { C.hcx * b.x, C.hcy * b.y, C.hcz * b.z }; }
-__device__ __forceinline__ d3 contr_half(Cell const &C, d3 b) { return { C.hnx * b.x, C.hny * b.y, C.hnz * b.z }; }
-__device__ __forceinline__ d3 mask_p(Cell const &C, d3 v) { return (v * C.mp1) * C.mp2; }
-__device__ __forceinline__ d3 mask_a(Cell const &C, d3 v) { return (v * C.ma1) * C.ma2; }
+template <class G>
+__device__ __forceinline__ d3 covar_half(G const &C, d3 b) { return { C.hcx * b.x, C.hcy * b.y, C.hcz * b.z }; }
+template <class G>
+__device__ __forceinline__ d3 contr_half(G const &C, d3 b) { return { C.hnx * b.x, C.hny * b.y, C.hnz * b.z }; }
+template <class G>
+__device__ __forceinline__ d3 mask_p(G const &C, d3 v) { return (v * C.mp1) * C.mp2; }
+template <class G>
+__device__ __forceinline__ d3 mask_a(G const &C, d3 v) { return (v * C.ma1) * C.ma2; }
 
 // electron pressure gradient, masked (EField.cc:63-87, 44): needs Pe of the neighbours
 __device__ __forceinline__ double dPe_at(FieldArgs const &a, Cell const &C, double const *Pe)
@@ -161,17 +172,21 @@ __device__ __forceinline__ double dPe_at(FieldArgs const &a, Cell const &C, doub
     int const tl = max(C.t - 1, 0), tr = min(C.t + 1, C.L - 1);
     return ((Pe[tr] - Pe[tl]) * a.cO2 * C.mp1) * C.mp2;
 }
+// pow(x, 1) is x exactly (the isothermal closure), so that case skips the library pow
 __device__ __forceinline__ double Pe_of(FieldArgs const &a, double rho)
 {
-    return pow(a.mOeOO0oe2 * rho, a.gamma) * a.O02beO2;
+    double const x = a.mOeOO0oe2 * rho;
+    return (a.gamma == 1.0 ? x : pow(x, a.gamma)) * a.O02beO2;
 }
 
-// Ohm's law at this cell (EField.cc:88-126) from Bcov/Bcon of the current B (with the
-// neighbour at t+1), contravariant current jc, masked dPe and rho; returns the masked E
-__device__ __forceinline__ d3 E_at(FieldArgs const &a, Cell const &C, double const *Bcov, double const *Bcon, d3 jc,
-                                   double dPe, double rho)
+// Ohm's law at local cell t with half-grid geometry C (EField.cc:88-126) from Bcov/Bcon of the
+// current B (with the neighbour at t+1), contravariant current jc, masked dPe and rho; returns
+// the masked E
+template <class G>
+__device__ __forceinline__ d3 E_at_g(FieldArgs const &a, G const &C, int t, int L, double const *Bcov, double const *Bcon,
+                                     d3 jc, double dPe, double rho)
 {
-    int const t = C.t, tr = min(t + 1, C.L - 1);
+    int const tr = min(t + 1, L - 1);
     d3 const  B1 = sld3(Bcov, tr), B0 = sld3(Bcov, t);
     d3        Je = { 0 - jc.x, (-B1.z + B0.z) * a.cOsqrtg - jc.y, (+B1.y - B0.y) * a.cOsqrtg - jc.z };
     Je           = mask_p(C, Je);
@@ -181,19 +196,29 @@ __device__ __forceinline__ d3 E_at(FieldArgs const &a, Cell const &C, double con
     d3 const  Ec = { (lz.x - dPe) / rho, (lz.y - 0.0) / rho, (lz.z - 0.0) / rho };
     return mask_a(C, contr_half(C, Ec));
 }
-
-// Faraday at this cell (BField.cc:50-64) from Ecov at t and t-1; returns the new masked B
-__device__ __forceinline__ d3 B_at(FieldArgs const &a, Cell const &C, double const *Ecov, d3 Bprev, double dtp)
+__device__ __forceinline__ d3 E_at(FieldArgs const &a, Cell const &C, double const *Bcov, double const *Bcon, d3 jc,
+                                   double dPe, double rho)
 {
-    int const    t = C.t, tl = max(t - 1, 0);
+    return E_at_g(a, C, C.t, C.L, Bcov, Bcon, jc, dPe, rho);
+}
+
+// Faraday at this cell (BField.cc:50-64) from the covariant E at this cell (E1) and at the one
+// before (E0); returns the new masked B
+__device__ __forceinline__ d3 B_at_e(FieldArgs const &a, Cell const &C, d3 E1, d3 E0, d3 Bprev, double dtp)
+{
     double const k = dtp * a.c_light / a.sqrt_g;
-    d3 const     E1 = sld3(Ecov, t), E0 = sld3(Ecov, tl);
     d3 const     Bc = { 0, (-E1.z + E0.z) * k, (+E1.y - E0.y) * k };
     d3 const     Bk = covar_full(C, Bc); // contr_to_cart uses the covariant basis
     d3           B  = { 0 - Bk.x, 0 - Bk.y, 0 - Bk.z };
     B               = mask_p(C, B);
     B               = B + Bprev;
     return mask_a(C, B);
+}
+// the same with Ecov from shared memory (at t and t-1)
+__device__ __forceinline__ d3 B_at(FieldArgs const &a, Cell const &C, double const *Ecov, d3 Bprev, double dtp)
+{
+    int const t = C.t, tl = max(t - 1, 0);
+    return B_at_e(a, C, sld3(Ecov, t), sld3(Ecov, tl), Bprev, dtp);
 }
 
 __device__ __forceinline__ void load_cell(FieldArgs const &a, Cell &C, int blk)
@@ -310,7 +335,145 @@ static __device__ d3 cold_push(FieldArgs const &a, Cell const &C, ColdSrc const 
     return boris_push(K.boris, ld3(K.nV_in, C.gm), Bc, E * n);
 }
 
+// shared memory of the CAM-CL field body with smoothing groups of fb items (see below)
+constexpr int FB_MAX     = 8;  // items per smoothing group
+constexpr int FS_FIXED_L = 22; // arrays of L doubles outside the groups
+constexpr int FS_ITEM_L  = 8;  // per item: a, ta (L each), v, tv (3L each)
+constexpr int FS_GHOST   = 24; // per item: 4 quantities x 6 ghost-fold partners
+__host__ __device__ constexpr size_t camcl_smem_bytes(int L, int fb)
+{
+    return sizeof(double) * (static_cast<size_t>(L) * (FS_FIXED_L + FS_ITEM_L * fb) + static_cast<size_t>(FS_GHOST) * fb);
+}
+
 #ifdef H1D_FIELD_TU
+// ------------------------------------------------------------------------------------------------
+// CAM-CL cycle: shared-memory layout and the sources' smoothing in groups.
+//
+// The sources of every species (kinetic deposits at x^N and x^{N+1}, cold fluid, external
+// sources) and the current-advance terms are smoothed in groups of up to `fb` items that share
+// their barrier phases: an item is a (scalar, vector) pair of arrays with its own smoothing
+// count, and a group takes max(count) + 1 barriers however many items it holds.  The raw deposits
+// of a group are staged in shared memory first, every thread loading its cell and threads 0..23
+// the ghost-fold partners, so the group pays one round of L2 latency.  Each value is computed
+// with the same operations, in the same order, as per-species collect_smooth.
+// ------------------------------------------------------------------------------------------------
+struct CamclSmem {
+    double *rho_avg, *Pe, *Pe1, *Javg; // Javg: 3L
+    double *Bcov[2], *Bcon[2], *Bavg;  // 3L each; Bcov / Bcon ping-pong across the subcycles
+    double *items;                     // per item j at items + 8 L j: a (L), ta (L), v (3L), tv (3L)
+    double *gh;                        // ghost-fold partners: [item][quantity][6]
+    int     L;
+    __device__ __forceinline__ double *a(int j) const { return items + FS_ITEM_L * L * j; }
+    __device__ __forceinline__ double *ta(int j) const { return items + FS_ITEM_L * L * j + L; }
+    __device__ __forceinline__ double *v(int j) const { return items + FS_ITEM_L * L * j + 2 * L; }
+    __device__ __forceinline__ double *tv(int j) const { return items + FS_ITEM_L * L * j + 5 * L; }
+};
+__device__ __forceinline__ CamclSmem carve_camcl(double *p, int L, int fb)
+{
+    CamclSmem s;
+    s.L       = L;
+    s.rho_avg = p, p += L;
+    s.Pe = p, p += L;
+    s.Pe1 = p, p += L;
+    s.Javg = p, p += 3 * L;
+    for (int k = 0; k < 2; ++k) {
+        s.Bcov[k] = p, p += 3 * L;
+        s.Bcon[k] = p, p += 3 * L;
+    }
+    s.Bavg = p, p += 3 * L;
+    s.items = p, p += FS_ITEM_L * L * fb;
+    s.gh = p;
+    return s;
+}
+
+// stage the raw deposit arrays r[0..3] of item j: this cell into ta (n) / tv (nV), and the six
+// ghost-fold partners r[-3..-1], r[Nx..Nx+2] of every quantity into gh (threads 0..23)
+__device__ __forceinline__ void stage_raw(FieldArgs const &a, Cell const &C, CamclSmem const &S, int j,
+                                          double const *const (&r)[4])
+{
+    int const t = C.t;
+    S.ta(j)[t]  = __ldg(r[0] + C.gm);
+#pragma unroll
+    for (int q = 1; q < 4; ++q)
+        S.tv(j)[3 * t + q - 1] = __ldg(r[q] + C.gm);
+    if (t < 24) {
+        int const q = t / 6, k = t % 6;
+        S.gh[(j * 4 + q) * 6 + k] = __ldg(r[q] + (k < 3 ? k - 3 : a.Nx + k - 3));
+    }
+}
+// fold of staged quantity q of item j onto interior cell gm, as fold() computes it from the raw array
+__device__ __forceinline__ double fold_staged(FieldArgs const &a, Cell const &C, CamclSmem const &S, int j, int q,
+                                              double s1, double f, double const *eq)
+{
+    int const     gm = C.gm, Nx = a.Nx;
+    double const *g  = S.gh + (j * 4 + q) * 6; // g[0..2] = r[-3..-1], g[3..5] = r[Nx..Nx+2]
+    double        m  = (q == 0 ? S.ta(j)[C.t] : S.tv(j)[3 * C.t + q - 1]) * s1;
+    if (eq)
+        m = m + eq[gm] * 1.0;
+    double v = m * f;
+    if (a.bc == 0) {
+        if (gm < PAD)
+            v = v + (g[3 + gm] * s1) * f;
+        if (gm >= Nx - PAD)
+            v = v + (g[gm - Nx + 3] * s1) * f;
+    } else {
+        if (gm == 0)
+            v = v + ((g[2] * s1) * f + ((g[1] * s1) * f + (g[0] * s1) * f));
+        if (gm == Nx - 1)
+            v = v + ((g[3] * s1) * f + ((g[4] * s1) * f + (g[5] * s1) * f));
+    }
+    return v;
+}
+
+// nsm[j] smoothings of item j's arrays (a, v) for every j < n together, ping-ponging with (ta, tv);
+// with_scalar = false smooths the vectors only.  Item j's result is in (a, v) when nsm[j] is even
+// and in (ta, tv) when it is odd.  Ends synchronised.
+__device__ __forceinline__ void smooth_group(Cell const &C, CamclSmem const &S, int n, int const (&nsm)[FB_MAX],
+                                             bool with_scalar)
+{
+    int const tl = max(C.t - 1, 0), tr = min(C.t + 1, C.L - 1), t = C.t;
+    int       most = 0;
+#pragma unroll
+    for (int j = 0; j < FB_MAX; ++j)
+        if (j < n)
+            most = max(most, nsm[j]);
+    for (int it = 0; it < most; ++it) {
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < FB_MAX; ++j) {
+            if (j >= n || it >= nsm[j])
+                continue;
+            bool const    odd = it & 1;
+            double const *a   = odd ? S.ta(j) : S.a(j);
+            double       *ta  = odd ? S.a(j) : S.ta(j);
+            double const *v   = odd ? S.tv(j) : S.v(j);
+            double       *tv  = odd ? S.v(j) : S.tv(j);
+            if (with_scalar)
+                ta[t] = (a[tl] + 2 * a[t] + a[tr]) * .25;
+            for (int k = 0; k < 3; ++k)
+                tv[3 * t + k] = (v[3 * tl + k] + 2 * v[3 * t + k] + v[3 * tr + k]) * .25;
+        }
+    }
+    __syncthreads();
+}
+__device__ __forceinline__ double const *smoothed_a(CamclSmem const &S, int j, int nsm) { return nsm & 1 ? S.ta(j) : S.a(j); }
+__device__ __forceinline__ double const *smoothed_v(CamclSmem const &S, int j, int nsm) { return nsm & 1 ? S.tv(j) : S.v(j); }
+
+// one source item of the CAM-CL cycle: kinetic species s at deposit d, cold species c, or
+// external source e (their order is the reference's accumulation order)
+struct SrcItem {
+    int kind, idx, d; // kind 0 kinetic, 1 cold, 2 external
+};
+__device__ __forceinline__ SrcItem src_item(FieldArgs const &a, int i)
+{
+    if (i < 2 * a.nk)
+        return { 0, i >> 1, i & 1 };
+    i -= 2 * a.nk;
+    if (i < a.nc)
+        return { 1, i, 0 };
+    return { 2, i - a.nc, 0 };
+}
+
 // ------------------------------------------------------------------------------------------------
 // CAM-CL cycle (Domain_CAMCL.cc:57-193)
 // ------------------------------------------------------------------------------------------------
@@ -319,128 +482,182 @@ __device__ __forceinline__ void camcl_field_body(FieldArgs const &a, int blk)
     extern __shared__ double sm[];
     Cell C;
     load_cell(a, C, blk);
-    Smem const S = carve(sm, C.L);
-    int const  t = C.t, Nx = a.Nx;
+    CamclSmem const S = carve_camcl(sm, C.L, a.fb);
+    int const       t = C.t, Nx = a.Nx, L = C.L;
 
-    // 1-2. sources at x^N and x^{N+1}
-    S.rho0[t] = 0, S.rho1[t] = 0;
-    sst3(S.J0, t, { 0, 0, 0 });
-    sst3(S.J1, t, { 0, 0, 0 });
-    for (int s = 0; s < a.nk; ++s) {
-        KinSrc const &K = a.k[s];
-        for (int d = 0; d < 2; ++d) {
-            SV const r   = collect_kinetic(a, C, S, K, d);
-            double  *rho = d ? S.rho1 : S.rho0;
-            double  *J   = d ? S.J1 : S.J0;
-            sst3(J, t, sld3(J, t) + sld3(r.v, t));
-            rho[t] += r.a[t];
+    // the half-grid geometry of the cell before this one, for its E in the fused subcycle
+    HalfGeo Cm;
+    {
+        long const    N = Nx, i = (C.gm + Nx - 1) % Nx;
+        double const *G = a.geo;
+        Cm = { G[G_HCOV_X * N + i], G[G_HCOV_Y * N + i], G[G_HCOV_Z * N + i], G[G_HCON_X * N + i],
+               G[G_HCON_Y * N + i], G[G_HCON_Z * N + i], G[G_MP1 * N + i],    G[G_MP2 * N + i],
+               G[G_MA1 * N + i],    G[G_MA2 * N + i] };
+    }
+    d3 const Bn = ld3(a.B_in, C.gm);
+    d3       cold_nV[MAXC];
+    for (int ci = 0; ci < a.nc; ++ci)
+        cold_nV[ci] = cold_push(a, C, a.c[ci], a.E_in);
+
+    // 1-2. sources at x^N and x^{N+1}, every species' collect_smooth in groups
+    double    rho0 = 0, rho1 = 0;
+    d3        J0 = { 0, 0, 0 }, J1 = { 0, 0, 0 };
+    int const n_src = 2 * a.nk + a.nc + a.ne;
+    for (int i0 = 0; i0 < n_src; i0 += a.fb) {
+        int const n = min(a.fb, n_src - i0);
+        int       nsm[FB_MAX];
+#pragma unroll
+        for (int j = 0; j < FB_MAX; ++j) {
+            nsm[j] = 0;
+            if (j >= n)
+                continue;
+            SrcItem const it = src_item(a, i0 + j);
+            if (it.kind == 0)
+                stage_raw(a, C, S, j, a.k[it.idx].raw[it.d]);
+            else if (it.kind == 2)
+                stage_raw(a, C, S, j, a.e[it.idx].raw[0]);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < FB_MAX; ++j) {
+            if (j >= n)
+                continue;
+            SrcItem const it = src_item(a, i0 + j);
+            if (it.kind == 1) {
+                ColdSrc const &K = a.c[it.idx];
+                S.a(j)[t]        = (K.n[C.gm] * K.w) * K.cdcf;
+                sst3(S.v(j), t, (cold_nV[it.idx] * K.w) * K.ccf);
+                nsm[j] = K.nsm;
+            } else {
+                KinSrc const &K = it.kind == 0 ? a.k[it.idx] : a.e[it.idx];
+                S.a(j)[t]       = fold_staged(a, C, S, j, 0, K.s1, K.cdcf, K.eq);
+                for (int q = 0; q < 3; ++q)
+                    S.v(j)[3 * t + q] = fold_staged(a, C, S, j, 1 + q, K.s1, K.ccf, nullptr);
+                nsm[j] = K.nsm;
+            }
+        }
+        smooth_group(C, S, n, nsm, true);
+#pragma unroll
+        for (int j = 0; j < FB_MAX; ++j) {
+            if (j >= n)
+                continue;
+            SrcItem const it = src_item(a, i0 + j);
+            double const  r  = smoothed_a(S, j, nsm[j])[t];
+            d3 const      v  = sld3(smoothed_v(S, j, nsm[j]), t);
+            if (it.kind == 0 && it.d == 1) {
+                J1 = J1 + v;
+                rho1 += r;
+            } else if (it.kind == 0) {
+                J0 = J0 + v;
+                rho0 += r;
+            } else { // cold and external sources enter both
+                J0 = J0 + v;
+                rho0 += r;
+                J1 = J1 + v;
+                rho1 += r;
+            }
         }
     }
-    d3 cold_nV[MAXC];
-    for (int ci = 0; ci < a.nc; ++ci) {
-        ColdSrc const &K = a.c[ci];
-        cold_nV[ci]      = cold_push(a, C, K, a.E_in);
-        S.tr[t]          = (K.n[C.gm] * K.w) * K.cdcf;
-        sst3(S.tJ, t, (cold_nV[ci] * K.w) * K.ccf);
-        SV const r = smooth_n(C, K.nsm, S.tr, S.tJ, S.ts, S.tJs);
-        sst3(S.J0, t, sld3(S.J0, t) + sld3(r.v, t));
-        S.rho0[t] += r.a[t];
-        sst3(S.J1, t, sld3(S.J1, t) + sld3(r.v, t));
-        S.rho1[t] += r.a[t];
-    }
-    for (int s = 0; s < a.ne; ++s) { // external sources at the half-time step (Domain_CAMCL.cc:93-100)
-        SV const r = collect_kinetic(a, C, S, a.e[s], 0);
-        sst3(S.J0, t, sld3(S.J0, t) + sld3(r.v, t));
-        S.rho0[t] += r.a[t];
-        sst3(S.J1, t, sld3(S.J1, t) + sld3(r.v, t));
-        S.rho1[t] += r.a[t];
-    }
     // 3. averages
-    double const rho_avg = (S.rho0[t] + S.rho1[t]) * .5;
-    d3 const     J_avg   = (sld3(S.J0, t) + sld3(S.J1, t)) * .5;
+    double const rho_avg = (rho0 + rho1) * .5;
+    d3 const     J_avg   = (J0 + J1) * .5;
     S.rho_avg[t]         = rho_avg;
     sst3(S.Javg, t, J_avg);
     S.Pe[t]  = Pe_of(a, rho_avg);
-    S.Pe1[t] = Pe_of(a, S.rho1[t]);
-    // B0 = B1 = B^N; covariant/contravariant components of B0
-    d3 const Bn = ld3(a.B_in, C.gm);
-    sst3(S.B0, t, Bn);
-    sst3(S.B1, t, Bn);
-    sst3(S.Bcov, t, covar_full(C, Bn));
-    sst3(S.Bcon, t, contr_full(C, Bn));
+    S.Pe1[t] = Pe_of(a, rho1);
+    sst3(S.Bcov[0], t, covar_full(C, Bn));
+    sst3(S.Bcon[0], t, contr_full(C, Bn));
     __syncthreads();
     double const dPe  = dPe_at(a, C, S.Pe);
     double const dPe1 = dPe_at(a, C, S.Pe1);
     d3 const     jc   = contr_half(C, J_avg);
+    // the same for the cell before (dPe_at of cell t - 1 reads Pe at t - 2 and t)
+    double const dPe_m = ((S.Pe[t] - S.Pe[max(t - 2, 0)]) * a.cO2 * Cm.mp1) * Cm.mp2;
+    d3 const     jc_m  = contr_half(Cm, sld3(S.Javg, max(t - 1, 0)));
+    double const rho_m = S.rho_avg[max(t - 1, 0)];
 
-    // 4. subcycle: X is updated, Y holds the newest B
-    double *X = S.B1, *Y = S.B0; // prologue: E from b0, then b1 = b1 + dt*curl E
+    // 4. subcycle, one barrier per sub-step: each thread computes E at its cell and at the one
+    // before (the value that cell's thread computes, operation for operation), then Faraday's law
+    d3 X = Bn, Y = Bn; // X is updated, Y holds the newest B
     for (int i = 0; i <= a.m; ++i) {
-        d3 const E = E_at(a, C, S.Bcov, S.Bcon, jc, dPe, rho_avg);
-        sst3(S.Ecov, t, covar_half(C, E));
+        int const    p    = i & 1;
+        d3 const     E    = E_at_g(a, C, t, L, S.Bcov[p], S.Bcon[p], jc, dPe, rho_avg);
+        d3 const     Ec   = covar_half(C, E);
+        d3 const     Em   = t > 0 ? covar_half(Cm, E_at_g(a, Cm, t - 1, L, S.Bcov[p], S.Bcon[p], jc_m, dPe_m, rho_m)) : Ec;
+        double const dtp  = (i == 0 || i == a.m) ? a.sub_dt : 2.0 * a.sub_dt;
+        d3 const     Bnew = B_at_e(a, C, Ec, Em, X, dtp);
+        X                 = Bnew;
+        sst3(S.Bcov[1 - p], t, covar_full(C, Bnew));
+        sst3(S.Bcon[1 - p], t, contr_full(C, Bnew));
         __syncthreads();
-        double const dtp = (i == 0 || i == a.m) ? a.sub_dt : 2.0 * a.sub_dt;
-        if (i == 0) {
-            X = S.B1, Y = S.B0;
-        }
-        d3 const Bnew = B_at(a, C, S.Ecov, sld3(X, t), dtp);
-        sst3(X, t, Bnew);
-        sst3(S.Bcov, t, covar_full(C, Bnew));
-        sst3(S.Bcon, t, contr_full(C, Bnew));
-        __syncthreads();
-        double *tmp = X; // the older array is updated next
-        X           = Y;
-        Y           = tmp;
+        d3 const tmp = X; // the older one is updated next
+        X            = Y;
+        Y            = tmp;
     }
     // after the loop Y is b0 (updated last) and X is b1; average into B
-    d3 const Bavg = (sld3(Y, t) + sld3(X, t)) * .5;
-    __syncthreads();
-    sst3(S.B0, t, Bavg);
-    sst3(S.Bcov, t, covar_full(C, Bavg));
-    sst3(S.Bcon, t, contr_full(C, Bavg));
+    int const pb   = (a.m + 1) & 1; // the buffer nobody reads any more
+    d3 const  Bavg = (Y + X) * .5;
+    sst3(S.Bavg, t, Bavg);
+    sst3(S.Bcov[pb], t, covar_full(C, Bavg));
+    sst3(S.Bcon[pb], t, contr_full(C, Bavg));
     __syncthreads();
 
     // 5. E* from (B, rho^{N+1}, J^{N+1/2})
-    d3 const Es = E_at(a, C, S.Bcov, S.Bcon, jc, dPe1, S.rho1[t]);
-    sst3(S.E, t, Es);
-    __syncthreads();
+    d3 const Es = E_at_g(a, C, t, L, S.Bcov[pb], S.Bcon[pb], jc, dPe1, rho1);
     // current advance (Domain_CAMCL.cc:131-151, Current.cc:45-52)
-    d3 const Bi = { C.hbx + (sld3(S.B0, min(t + 1, C.L - 1)).x + Bavg.x) * 0.5,
-                    0 * a.O0 + (sld3(S.B0, min(t + 1, C.L - 1)).y + Bavg.y) * 0.5,
-                    0 * a.O0 + (sld3(S.B0, min(t + 1, C.L - 1)).z + Bavg.z) * 0.5 };
-    for (int s = 0; s < a.nk + a.nc + a.ne; ++s) {
-        double lam;
-        d3     gam;
-        int    nsm;
-        if (s < a.nk || s >= a.nk + a.nc) {
-            KinSrc const &K = s < a.nk ? a.k[s] : a.e[s - a.nk - a.nc];
-            lam             = fold(K.raw[1][0], C.gm, Nx, a.bc, K.s1, K.lamf, K.eq);
-            gam             = { fold(K.raw[1][1], C.gm, Nx, a.bc, K.s1, K.gamf), fold(K.raw[1][2], C.gm, Nx, a.bc, K.s1, K.gamf),
-                    fold(K.raw[1][3], C.gm, Nx, a.bc, K.s1, K.gamf) };
-            nsm             = K.nsm;
-        } else {
-            ColdSrc const &K = a.c[s - a.nk];
-            lam              = (K.n[C.gm] * K.w) * K.lamf;
-            gam              = (cold_nV[s - a.nk] * K.w) * K.gamf;
-            nsm              = K.nsm;
+    d3 const  Bnext = sld3(S.Bavg, min(t + 1, L - 1));
+    d3 const  Bi    = { C.hbx + (Bnext.x + Bavg.x) * 0.5, 0 * a.O0 + (Bnext.y + Bavg.y) * 0.5,
+                        0 * a.O0 + (Bnext.z + Bavg.z) * 0.5 };
+    int const n_adv = a.nk + a.nc + a.ne;
+    for (int i0 = 0; i0 < n_adv; i0 += a.fb) {
+        int const n = min(a.fb, n_adv - i0);
+        int       nsm[FB_MAX];
+#pragma unroll
+        for (int j = 0; j < FB_MAX; ++j) {
+            int const s = i0 + j;
+            if (j < n && (s < a.nk || s >= a.nk + a.nc))
+                stage_raw(a, C, S, j, (s < a.nk ? a.k[s] : a.e[s - a.nk - a.nc]).raw[1]);
         }
-        d3 const Jadv = (Es * lam + cross(gam, Bi)) * (0.5 * a.dt);
-        S.t2[t]       = 0;
-        sst3(S.tJ, t, { 0 + Jadv.x, 0 + Jadv.y, 0 + Jadv.z });
-        SV const r = smooth_n(C, nsm, S.t2, S.tJ, S.ts, S.tJs);
-        sst3(S.J1, t, sld3(S.J1, t) + sld3(r.v, t));
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < FB_MAX; ++j) {
+            nsm[j] = 0;
+            if (j >= n)
+                continue;
+            int const s = i0 + j;
+            double    lam;
+            d3        gam;
+            if (s < a.nk || s >= a.nk + a.nc) {
+                KinSrc const &K = s < a.nk ? a.k[s] : a.e[s - a.nk - a.nc];
+                lam             = fold_staged(a, C, S, j, 0, K.s1, K.lamf, K.eq);
+                gam             = { fold_staged(a, C, S, j, 1, K.s1, K.gamf, nullptr),
+                                    fold_staged(a, C, S, j, 2, K.s1, K.gamf, nullptr),
+                                    fold_staged(a, C, S, j, 3, K.s1, K.gamf, nullptr) };
+                nsm[j]          = K.nsm;
+            } else {
+                ColdSrc const &K = a.c[s - a.nk];
+                lam              = (K.n[C.gm] * K.w) * K.lamf;
+                gam              = (cold_nV[s - a.nk] * K.w) * K.gamf;
+                nsm[j]           = K.nsm;
+            }
+            d3 const Jadv = (Es * lam + cross(gam, Bi)) * (0.5 * a.dt);
+            sst3(S.v(j), t, { 0 + Jadv.x, 0 + Jadv.y, 0 + Jadv.z });
+        }
+        smooth_group(C, S, n, nsm, false);
+#pragma unroll
+        for (int j = 0; j < FB_MAX; ++j)
+            if (j < n)
+                J1 = J1 + sld3(smoothed_v(S, j, nsm[j]), t);
     }
     // 6. E from (B, rho^{N+1}, J^+ advanced)
-    d3 const Ef = E_at(a, C, S.Bcov, S.Bcon, contr_half(C, sld3(S.J1, t)), dPe1, S.rho1[t]);
-    sst3(S.E, t, Ef);
-    __syncthreads();
+    d3 const Ef = E_at_g(a, C, t, L, S.Bcov[pb], S.Bcon[pb], contr_half(C, J1), dPe1, rho1);
 
     if (C.owner) {
         put3(a.B_out, C, Nx, Bavg);
         put3(a.E_out, C, Nx, Ef);
         put1(a.charge_out, C, Nx, rho_avg);
         put3(a.current_out, C, Nx, J_avg);
-        d3 const Bh = (sld3(S.B0, min(t + 1, C.L - 1)) + Bavg) * 0.5;
+        d3 const Bh = (Bnext + Bavg) * 0.5;
         put_eb(a.EB_out, a.EBf_out, C, Nx, Ef, Bh);
         for (int ci = 0; ci < a.nc; ++ci)
             st3(a.c[ci].nV_out, C.gm, cold_nV[ci]);

@@ -28,6 +28,25 @@ using namespace h1d;
 namespace {
 
 constexpr int FIELD_BLOCK_MIN = 256;
+
+// shared memory of a field launch of L threads: the predictor-corrector layout or the CAM-CL
+// layout with smoothing groups of fb items, whichever is larger
+size_t field_smem_bytes(int L, int fb)
+{
+    return std::max(sizeof(double) * static_cast<size_t>(L) * (SMEM_SCALARS + 3 * SMEM_VECTORS), camcl_smem_bytes(L, fb));
+}
+// the largest CAM-CL smoothing group whose layout fits `budget` bytes of shared memory: a single
+// run's launch (a few CTAs, one per SM) takes what a block can have; a batched launch (hundreds of
+// CTAs) keeps two CTAs per SM beside their FieldArgs copies
+constexpr size_t FIELD_SMEM_RUN   = 227 * 1024 - sizeof(FieldArgs) - 1024;
+constexpr size_t FIELD_SMEM_BATCH = 113 * 1024 - sizeof(FieldArgs) - 1024;
+int field_group(int L, size_t budget)
+{
+    int fb = FB_MAX;
+    while (fb > 1 && field_smem_bytes(L, fb) > budget)
+        --fb;
+    return fb;
+}
 constexpr int64_t STAGE_N      = int64_t{ 1 } << 22; // doubles in a mixed run's staging buffer (32 MB)
 
 struct SpeciesState {
@@ -70,7 +89,7 @@ struct h1d_run {
     int          device = 0, num_sms = 148;
     cudaStream_t stream = nullptr;
     long         Nx = 0, M = 0;
-    int          H = 0, seg = 0, L = 0, nblocks_field = 0;
+    int          H = 0, seg = 0, L = 0, nblocks_field = 0, fb = 1;
     size_t       field_smem = 0;
     double      *geo = nullptr;
     double      *B[2] = {}, *E[2] = {}, *EB = nullptr, *charge = nullptr, *current = nullptr;
@@ -696,6 +715,7 @@ FieldArgs field_args(h1d_run *run)
     }
     a.dt = p.dt, a.sub_dt = p.dt / p.n_subcycles, a.c_light = p.c, a.sqrt_g = p.Dx * 1 * 1, a.O0 = p.O0, a.inv_D1 = 1 / p.Dx;
     a.m = static_cast<int>(p.n_subcycles);
+    a.fb = run->fb;
     h1d_efluid_desc const &ef = p.efluid;
     a.O02beO2 = (p.O0 * p.O0) * ef.beta * 0.5, a.mOeOO0oe2 = -ef.Oc / (p.O0 * (ef.op * ef.op)), a.gamma = ef.gamma;
     a.cO2 = p.c / 2, a.cOsqrtg = p.c / a.sqrt_g;
@@ -1198,7 +1218,10 @@ int build_field_tables(h1d_batch *b)
                 flip();
         }
     }
-    size_t const smem = sizeof(double) * static_cast<size_t>(L) * (SMEM_SCALARS + 3 * SMEM_VECTORS);
+    int const    fb   = field_group(L, FIELD_SMEM_BATCH);
+    for (FieldArgs &a : tab)
+        a.fb = fb;
+    size_t const smem = field_smem_bytes(L, fb);
     if (L != b->L || static_cast<int>(map.size()) != b->nblocks || !b->d_table) {
         cudaFree(b->d_table), cudaFree(b->d_map);
         b->d_table = nullptr, b->d_map = nullptr;
@@ -1626,7 +1649,8 @@ int h1d_create(h1d_params const *params, h1d_run **out)
     run->L             = L;
     run->seg           = static_cast<int>(std::min<long>(L - 2 * run->H, run->Nx));
     run->nblocks_field = static_cast<int>((run->Nx + run->seg - 1) / run->seg);
-    run->field_smem    = sizeof(double) * static_cast<size_t>(L) * (SMEM_SCALARS + 3 * SMEM_VECTORS);
+    run->fb            = field_group(L, FIELD_SMEM_RUN);
+    run->field_smem    = field_smem_bytes(L, run->fb);
     run->mixed = p.precision == H1D_PREC_MIXED;
     run->stage_n = 1 << 16;
     for (int s = 0; s < p.n_kinetic; ++s)
