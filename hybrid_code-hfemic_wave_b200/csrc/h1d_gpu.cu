@@ -10,6 +10,7 @@
 #include "sort.cuh"
 #include "launchers.h"
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <deque>
@@ -2390,8 +2391,18 @@ int h1d_energy(h1d_run *run, double *dB2O2, double *dE2O2, double *KE_lab, doubl
 // ---- serving loop --------------------------------------------------------------------------------
 // Requests (a run description, a loader seed and a step count) wait in a queue until the HBM they
 // need fits the budget; admitted runs are built on the device (h1d_populate) and advance together
-// as one batch, a quantum of steps per tick; finished runs are read back and freed, which lets the
-// next requests in.  Membership changes rebuild the batch (and its graphs) at the next tick.
+// as one batch per algorithm, a quantum of steps per tick; finished runs are read back and freed,
+// which lets the next requests in.
+//
+// Threads.  One thread drives the loop with h1d_server_tick; it alone owns the active runs and
+// their batches.  The mutex guards what other threads see -- the queue, every request's state,
+// times and results, the memory accounting and the statistics -- and is held only for those short
+// updates, never while the GPU works, so submit, poll, result and release return at once while a
+// tick runs.  Within a tick the batches' quantum is enqueued first and the requests admitted in
+// that tick are built on their own streams while it runs; they join the batches at the next tick.
+// A member whose run fails (moved too far, non-finite state) fails alone; the others keep their
+// progress.  Served batches run eagerly: their membership changes too often for graph capture to
+// pay for itself.
 
 namespace {
 
@@ -2434,64 +2445,66 @@ struct h1d_server {
     size_t                                budget = 0, used = 0, peak = 0;
     int                                   quantum = 64, sort_interval = 16;
     std::deque<ServerReq *>               queue;
-    std::vector<ServerReq *>              active;
     std::map<uint64_t, ServerReq *>       all;
-    h1d_batch                            *batch[2] = { nullptr, nullptr }; // the active runs by algorithm (H1D_ALGO_*)
-    bool                                  dirty = false;
     uint64_t                              next_id = 1;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
-    h1d_server_stats                      stats{};
-    std::mutex                            mu;
+    h1d_server_stats                      stats{}; // retired batches' counts included
+    h1d_batch_stats                       live{};  // the current batches' counts, as of the last tick
+    std::mutex                            mu;      // the state other threads see (see above)
+    // owned by the thread that ticks
+    std::mutex                            tick_mu; // one tick at a time
+    std::vector<ServerReq *>              active;
+    h1d_batch                            *batch[2] = { nullptr, nullptr }; // the active runs by algorithm (H1D_ALGO_*)
+    bool                                  dirty = false;
 
     double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
 };
 
 namespace {
 
-// fold the statistics of the server's batches into its own and destroy them (the active runs stay)
+// destroy the batches (their runs stay), their counts folded into the statistics; tick thread
 void drop_batches(h1d_server *sv)
 {
     for (h1d_batch *&b : sv->batch) {
         if (!b)
             continue;
-        h1d_batch_stats st{};
-        h1d_batch_stats_read(b, &st);
-        sv->stats.kernel_launches += st.kernel_launches;
-        sv->stats.graph_launches += st.graph_launches;
-        sv->stats.steps += st.steps;
+        {
+            h1d_batch_stats st{};
+            h1d_batch_stats_read(b, &st);
+            std::lock_guard<std::mutex> lock(sv->mu);
+            sv->stats.kernel_launches += st.kernel_launches;
+            sv->stats.graph_launches += st.graph_launches;
+            sv->stats.steps += st.steps;
+        }
         h1d_batch_destroy(b);
         b = nullptr;
     }
 }
 
-void finish_request(h1d_server *sv, ServerReq *r, int status, std::string const &msg)
+// publish the end of a request (caller holds mu); its run is destroyed by the caller
+void finish_locked(h1d_server *sv, ServerReq *r, int status, std::string const &msg)
 {
     r->status = status;
     r->msg    = msg;
     r->state  = status == H1D_OK ? H1D_REQ_DONE : H1D_REQ_FAILED;
     r->t_done = sv->now();
-    if (r->run) {
-        h1d_destroy(r->run);
-        r->run = nullptr;
-        sv->used -= r->bytes;
-    }
+    sv->used -= r->bytes;
     if (status == H1D_OK)
         sv->stats.completed++;
     else
         sv->stats.failed++;
 }
 
-// build a request's run on the device: particles by the device loader, cold fluid at rest
-int admit(h1d_server *sv, ServerReq *r)
+// build a request's run on the device: particles by the device loader, cold fluid at rest; the
+// work is enqueued on the run's own stream (tick thread, without the lock)
+int admit(int sort_interval, ServerReq *r)
 {
     h1d_params p = r->rq.params;
     if (p.sort_interval <= 0)
-        p.sort_interval = sv->sort_interval;
+        p.sort_interval = sort_interval;
     int st = h1d_create(&p, &r->run);
     if (st != H1D_OK)
         return st;
-    sv->used += r->bytes;
-    sv->peak = std::max(sv->peak, sv->used);
     for (int s = 0; s < p.n_kinetic && st == H1D_OK; ++s)
         st = h1d_populate(r->run, s, r->rq.n_particles[s], r->rq.seed, r->rq.beta1[s], r->rq.T2_T1[s]);
     long const          M = p.Nx + 2 * PAD;
@@ -2546,7 +2559,7 @@ int h1d_server_configure(h1d_server *sv, int sort_interval)
 {
     if (!sv || sort_interval <= 0 || sort_interval > 4096)
         return H1D_ERR_INVALID_ARG;
-    std::lock_guard<std::mutex> lock(sv->mu);
+    std::lock_guard<std::mutex> tick(sv->tick_mu);
     sv->sort_interval = sort_interval;
     sv->dirty         = true;
     return H1D_OK;
@@ -2591,30 +2604,9 @@ int h1d_server_tick(h1d_server *sv, int *n_active, int *n_queued)
 {
     if (!sv)
         return H1D_ERR_INVALID_ARG;
-    std::lock_guard<std::mutex> lock(sv->mu);
-    // 1. admission: every queued request that fits the budget (in arrival order) and the device
-    size_t free_b = 0, total_b = 0;
-    cudaMemGetInfo(&free_b, &total_b);
-    for (auto it = sv->queue.begin(); it != sv->queue.end();) {
-        ServerReq *r = *it;
-        if (sv->used + r->bytes > sv->budget || r->bytes + (size_t{ 256 } << 20) > free_b) {
-            ++it;
-            continue;
-        }
-        it = sv->queue.erase(it);
-        int const st = admit(sv, r);
-        if (st != H1D_OK) {
-            finish_request(sv, r, st, r->msg.empty() ? "admission failed" : r->msg);
-            continue;
-        }
-        free_b   = free_b > r->bytes ? free_b - r->bytes : 0;
-        r->state = H1D_REQ_ACTIVE;
-        r->t_admit = sv->now();
-        sv->active.push_back(r);
-        sv->stats.admitted++;
-        sv->dirty = true;
-    }
-    // 2. the batches of the active runs, one per algorithm
+    std::lock_guard<std::mutex> tick(sv->tick_mu);
+
+    // 1. the batches of the active runs, one per algorithm, after a change of membership
     if (sv->dirty) {
         drop_batches(sv);
         for (int alg = 0; alg < 2; ++alg) {
@@ -2626,68 +2618,148 @@ int h1d_server_tick(h1d_server *sv, int *n_active, int *n_queued)
                 continue;
             int st = h1d_batch_create(runs.data(), static_cast<int>(runs.size()), &sv->batch[alg]);
             if (st == H1D_OK)
-                st = h1d_batch_configure(sv->batch[alg], sv->sort_interval, 0, 1);
-            if (st != H1D_OK) {
+                st = h1d_batch_configure(sv->batch[alg], sv->sort_interval, 0, 0);
+            if (st != H1D_OK) { // the algorithm's runs fail (the batch goes before its runs)
                 h1d_batch_destroy(sv->batch[alg]);
                 sv->batch[alg] = nullptr;
+                std::vector<ServerReq *> gone;
                 for (auto it = sv->active.begin(); it != sv->active.end();)
-                    if ((*it)->rq.params.algorithm == alg) {
-                        finish_request(sv, *it, st, "batch creation failed");
-                        it = sv->active.erase(it);
-                    } else {
+                    if ((*it)->rq.params.algorithm == alg)
+                        gone.push_back(*it), it = sv->active.erase(it);
+                    else
                         ++it;
-                    }
+                {
+                    std::lock_guard<std::mutex> lock(sv->mu);
+                    for (ServerReq *r : gone)
+                        finish_locked(sv, r, st, "batch creation failed");
+                }
+                for (ServerReq *r : gone)
+                    h1d_destroy(r->run), r->run = nullptr;
             }
         }
         sv->dirty = false;
+        std::lock_guard<std::mutex> lock(sv->mu);
         sv->stats.batches_built++;
     }
-    // 3. one quantum (or up to the nearest completion) of every batch
+
+    // 2. the quantum of every batch (up to the nearest completion), enqueued without waiting
     uint32_t q = static_cast<uint32_t>(sv->quantum);
     for (ServerReq *r : sv->active)
         q = std::min(q, r->rq.n_steps - r->done_steps);
+    int launched[2] = { H1D_OK, H1D_OK };
+    for (int alg = 0; alg < 2; ++alg)
+        if (sv->batch[alg])
+            launched[alg] = h1d_batch_advance_async(sv->batch[alg], q);
+
+    // 3. admission while the batches run: every queued request that fits the budget (in arrival
+    // order) and the device, its memory reserved under the lock, its run built outside it
+    std::vector<ServerReq *> admitted;
+    {
+        size_t                      free_b = 0, total_b = 0;
+        bool                        asked  = false;
+        std::lock_guard<std::mutex> lock(sv->mu);
+        for (auto it = sv->queue.begin(); it != sv->queue.end();) {
+            ServerReq *r = *it;
+            if (sv->used + r->bytes > sv->budget) {
+                ++it;
+                continue;
+            }
+            if (!asked)
+                cudaMemGetInfo(&free_b, &total_b), asked = true;
+            if (r->bytes + (size_t{ 256 } << 20) > free_b) {
+                ++it;
+                continue;
+            }
+            it         = sv->queue.erase(it);
+            free_b     = free_b > r->bytes ? free_b - r->bytes : 0;
+            sv->used  += r->bytes;
+            sv->peak   = std::max(sv->peak, sv->used);
+            r->state   = H1D_REQ_ACTIVE;
+            r->t_admit = sv->now();
+            sv->stats.admitted++;
+            admitted.push_back(r);
+        }
+    }
+    std::vector<std::pair<ServerReq *, int>> ended;  // (request, status) to publish
+    std::vector<ServerReq *>                 joined; // built: they join the batches at the next tick
+    for (ServerReq *r : admitted) {
+        int const st = admit(sv->sort_interval, r);
+        if (st != H1D_OK)
+            ended.push_back({ r, st });
+        else
+            joined.push_back(r);
+    }
+
+    // 4. the end of the quantum: members whose run failed fail alone
     for (int alg = 0; alg < 2; ++alg) {
         if (!sv->batch[alg])
             continue;
-        int const   st = h1d_batch_advance(sv->batch[alg], q);
-        std::string m;
-        if (st != H1D_OK) { // a member failed: the batch goes (before its runs are freed), then every member
-            m = h1d_batch_status_string(sv->batch[alg]);
-            h1d_batch_destroy(sv->batch[alg]);
-            sv->batch[alg] = nullptr;
-        }
-        for (auto it = sv->active.begin(); it != sv->active.end();) {
-            ServerReq *r = *it;
-            if (r->rq.params.algorithm != alg) {
-                ++it;
-            } else if (st == H1D_OK) {
+        int const st = launched[alg] != H1D_OK ? launched[alg] : h1d_batch_synchronize(sv->batch[alg]);
+        for (ServerReq *r : sv->active) {
+            if (r->rq.params.algorithm != alg)
+                continue;
+            if (st == H1D_OK) {
                 r->done_steps += q;
-                ++it;
-            } else {
-                finish_request(sv, r, st, m);
-                it = sv->active.erase(it);
+                continue;
             }
+            // a failed launch fails every member; otherwise only the members whose run reports an error
+            int const own = launched[alg] != H1D_OK ? st : h1d_synchronize(r->run);
+            if (own != H1D_OK)
+                ended.push_back({ r, own }), r->msg = h1d_status_string(r->run);
+            else
+                r->done_steps += q;
         }
     }
-    // 4. retire finished runs
+
+    // 5. finished and failed runs leave the batches, are read back and freed; new runs join
+    std::vector<ServerReq *> leaving;
     for (auto it = sv->active.begin(); it != sv->active.end();) {
-        ServerReq *r = *it;
-        if (r->done_steps < r->rq.n_steps) {
+        ServerReq *r      = *it;
+        bool const failed = std::any_of(ended.begin(), ended.end(), [r](auto const &e) { return e.first == r; });
+        if (failed || r->done_steps >= r->rq.n_steps) {
+            leaving.push_back(r);
+            it = sv->active.erase(it);
+        } else {
             ++it;
-            continue;
         }
-        if (sv->batch[r->rq.params.algorithm]) { // the run leaves the batches before it is read and freed
-            drop_batches(sv);
-            sv->dirty = true;
-        }
-        int const st = collect(r);
-        finish_request(sv, r, st, st == H1D_OK ? "" : r->run->msg);
-        it = sv->active.erase(it);
     }
-    if (n_active)
-        *n_active = static_cast<int>(sv->active.size());
-    if (n_queued)
-        *n_queued = static_cast<int>(sv->queue.size());
+    if (!leaving.empty()) {
+        drop_batches(sv);
+        sv->dirty = true;
+    }
+    if (!joined.empty()) {
+        sv->active.insert(sv->active.end(), joined.begin(), joined.end());
+        sv->dirty = true;
+    }
+    std::vector<std::pair<ServerReq *, int>> results;
+    for (ServerReq *r : leaving) {
+        auto const f  = std::find_if(ended.begin(), ended.end(), [r](auto const &e) { return e.first == r; });
+        int const  st = f != ended.end() ? f->second : collect(r);
+        results.push_back({ r, st });
+    }
+    for (auto const &e : ended) // failed admissions are not in `leaving`
+        if (std::find(leaving.begin(), leaving.end(), e.first) == leaving.end())
+            results.push_back(e);
+    {
+        std::lock_guard<std::mutex> lock(sv->mu);
+        for (auto const &[r, st] : results)
+            finish_locked(sv, r, st, st == H1D_OK ? "" : (r->msg.empty() ? "run failed" : r->msg));
+        sv->live = {};
+        for (h1d_batch *b : sv->batch)
+            if (b) {
+                h1d_batch_stats st{};
+                h1d_batch_stats_read(b, &st);
+                sv->live.kernel_launches += st.kernel_launches, sv->live.graph_launches += st.graph_launches;
+                sv->live.steps += st.steps;
+            }
+        if (n_active)
+            *n_active = static_cast<int>(sv->active.size());
+        if (n_queued)
+            *n_queued = static_cast<int>(sv->queue.size());
+    }
+    for (auto const &[r, st] : results)
+        if (r->run)
+            h1d_destroy(r->run), r->run = nullptr;
     return H1D_OK;
 }
 
@@ -2752,12 +2824,8 @@ int h1d_server_stats_read(h1d_server *sv, h1d_server_stats *out)
         return H1D_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lock(sv->mu);
     *out = sv->stats;
-    for (h1d_batch *b : sv->batch)
-        if (b) {
-            h1d_batch_stats st{};
-            h1d_batch_stats_read(b, &st);
-            out->kernel_launches += st.kernel_launches, out->graph_launches += st.graph_launches, out->steps += st.steps;
-        }
+    out->kernel_launches += sv->live.kernel_launches, out->graph_launches += sv->live.graph_launches;
+    out->steps += sv->live.steps;
     out->bytes_in_use = static_cast<int64_t>(sv->used);
     out->peak_bytes   = static_cast<int64_t>(sv->peak);
     return H1D_OK;
@@ -2767,7 +2835,10 @@ int h1d_server_destroy(h1d_server *sv)
 {
     if (!sv)
         return H1D_OK;
-    drop_batches(sv);
+    std::lock_guard<std::mutex> tick(sv->tick_mu);
+    for (h1d_batch *&b : sv->batch)
+        if (b)
+            h1d_batch_destroy(b), b = nullptr;
     for (auto &[id, r] : sv->all) {
         if (r->run)
             h1d_destroy(r->run);

@@ -374,8 +374,11 @@ const char *h1d_batch_status_string(h1d_batch *batch);
  * runs are built on the device (h1d_populate, cold fluid at rest, zero fields), advance together
  * as one batch by up to `steps_per_tick` steps per h1d_server_tick, and are read back (fields,
  * energies, moments) and freed when their steps are done, which admits the next requests.  The
- * caller drives the loop by calling h1d_server_tick; submit, poll, result and release may come
- * from other threads.  Times are seconds since h1d_server_create on a monotonic clock. */
+ * caller drives the loop by calling h1d_server_tick from one thread; submit, poll, result and
+ * release may come from other threads and do not wait for a tick in progress (the server's lock is
+ * not held while the GPU works).  Requests admitted during a tick are built while the batches
+ * advance and join them at the next tick; a request whose run fails (e.g. moved too far) fails
+ * alone.  Times are seconds since h1d_server_create on a monotonic clock. */
 typedef struct h1d_server h1d_server;
 typedef struct h1d_request {
     h1d_params params;                    /* a CAM-CL or predictor-corrector run */

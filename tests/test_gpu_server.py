@@ -140,3 +140,63 @@ def test_requests_the_device_loader_cannot_build_are_refused(gpu_lib):
             cfg = base.replace(kinetic=[dataclasses.replace(base.kinetic[0], **change)] + base.kinetic[1:])
             with pytest.raises(h.H1DError):
                 sv.submit(cfg, seed=0, n_steps=10)
+
+
+def test_failing_member_fails_alone(gpu_lib):
+    """A request whose particles move more than a cell per step (PartSpecies::update_pos's
+    domain_error) fails with H1D_ERR_MOVED_TOO_FAR while the requests batched with it complete
+    with the results they have alone."""
+    good = [(_cfg(s, h.configs.PREC_FP64), s, n) for s, n in ((11, 48), (12, 80))]
+    hot = _cfg(13, h.configs.PREC_FP64)
+    hot.kinetic[0].beta1 = 500.0  # thermal speed of a few cells per step
+    with h.abi.Server(gpu_lib, 8 * GB, steps_per_tick=16, sort_interval=8) as sv:
+        ids = [sv.submit(c, seed=s, n_steps=n) for c, s, n in good]
+        bad = sv.submit(hot, seed=13, n_steps=64)
+        _drain(sv, ids + [bad])
+        assert sv.poll(bad)["state"] == h.abi.REQ_FAILED and sv.poll(bad)["status"] == h.abi.ERR_MOVED_TOO_FAR
+        assert all(sv.poll(i)["state"] == h.abi.REQ_DONE for i in ids)
+        got = [sv.result(i) for i in ids]
+        st = sv.stats()
+        assert st["completed"] == 2 and st["failed"] == 1
+    for (c, s, n), res in zip(good, got):
+        with h.abi.Server(gpu_lib, 8 * GB, steps_per_tick=16, sort_interval=8) as sv:
+            i = sv.submit(c, seed=s, n_steps=n)
+            _drain(sv, [i])
+            alone = sv.result(i)
+        errs = _errs(res, alone)
+        assert max(errs.values()) <= 1e-10, errs
+
+
+def test_submit_and_poll_do_not_wait_for_a_tick(gpu_lib):
+    """While one thread runs a long tick (a large request, a quantum of many steps), submit and
+    poll from another thread return at once: the server's lock is not held while the GPU works."""
+    import threading
+    import time
+
+    big = h.configs.ensemble_member(21, precision=h.configs.PREC_FP64, ppc_scale=1.0).replace(Nx=4096, xi=0.001)
+    big.kinetic[0].Nc = 1000
+    with h.abi.Server(gpu_lib, 40 * GB, steps_per_tick=1500, sort_interval=16) as sv:
+        i = sv.submit(big, seed=21, n_steps=1500)
+        sv.tick()  # admits and builds the run; it joins the batch at the next tick
+        t = {}
+
+        def long_tick():
+            t0 = time.perf_counter()
+            sv.tick()
+            t["tick"] = time.perf_counter() - t0
+
+        th = threading.Thread(target=long_tick)
+        th.start()
+        time.sleep(0.05)
+        calls = []
+        while th.is_alive():
+            t0 = time.perf_counter()
+            j = sv.submit(_cfg(22, h.configs.PREC_FP64), seed=22, n_steps=8)
+            sv.poll(i)
+            sv.poll(j)
+            calls.append(time.perf_counter() - t0)
+            time.sleep(0.01)
+        th.join()
+        print(f"tick {t['tick']:.3f} s, {len(calls)} submit+poll rounds, slowest {max(calls) * 1e3:.2f} ms")
+        assert t["tick"] > 0.2 and len(calls) >= 5
+        assert max(calls) < 0.05 * t["tick"]
