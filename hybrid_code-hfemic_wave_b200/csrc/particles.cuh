@@ -229,14 +229,29 @@ __device__ __forceinline__ void interp_EB(double const *eb, Shape<O> const &sh, 
 // the half-step position, half move, BC, deposit.  move_steps == 0: deposit only
 // (Domain_PC.cc:36-44).
 // ------------------------------------------------------------------------------------------------
+// The pipeline's shape: particles per chunk (128 or 256: one or two per consumer lane), stages,
+// CTAs per SM and cells per deposit window; a build may set them with -DH1D_FP64_<NAME>=value.
+#ifndef H1D_FP64_CHUNK
+#define H1D_FP64_CHUNK 256
+#endif
+#ifndef H1D_FP64_STAGES
+#define H1D_FP64_STAGES 2
+#endif
+#ifndef H1D_FP64_CTAS
+#define H1D_FP64_CTAS 3
+#endif
+#ifndef H1D_FP64_W
+#define H1D_FP64_W 6
+#endif
 constexpr int PIPE_CONSUMER_WARPS = 4;
 constexpr int PIPE_THREADS        = 32 * (PIPE_CONSUMER_WARPS + 1);
-constexpr int PIPE_CHUNK          = 256;
+constexpr int PIPE_CHUNK          = H1D_FP64_CHUNK;
 constexpr int PIPE_PPT            = PIPE_CHUNK / (32 * PIPE_CONSUMER_WARPS);
-constexpr int PIPE_STAGES         = 2;
-constexpr int PIPE_CTAS_PER_SM    = 3;
-constexpr int PIPE_W              = 6; // cells per deposit window: 4 quantities x 6 cells, flushed over 32 lanes
-static_assert(4 * PIPE_W <= 32, "a window flush reduce-scatters at most 32 values");
+constexpr int PIPE_STAGES         = H1D_FP64_STAGES;
+constexpr int PIPE_CTAS_PER_SM    = H1D_FP64_CTAS;
+constexpr int PIPE_W              = H1D_FP64_W; // cells per deposit window: 4 quantities x W cells, flushed over 32 lanes
+static_assert(PIPE_PPT == 1 || PIPE_PPT == 2, "one or two particles per consumer lane and chunk");
+static_assert(4 * PIPE_W <= 32 && PIPE_W >= 4, "a window flush reduce-scatters at most 32 values; a cubic stencil fits");
 
 // a stage holds one chunk; the consumers overwrite it in place with the new state, which the
 // producer then stores.  With evolving weights (PSD) a stage also holds real_f and marker, and
