@@ -6,13 +6,13 @@
 Workload (default): the config-1 plasma at Nx=4096 with 4000 particles per cell -- uniform B0,
 periodic, one kinetic H+ species (beta_par 0.1, T_perp/T_par 3, CIC; 16.4M particles) plus a
 cold H+ background, isothermal electrons, dt=0.02, CAM-CL with 10 B subcycles -- run with the
-mixed-precision particle pass (int32 cell + FP32 offset, FP32 velocity / interpolation / push,
+mixed-precision particle pass (int32 fixed-point position, FP32 velocity / interpolation / push,
 FP32 warp deposits summed into FP64 cells; FP64 field cycle).  One bench step is one CAM-CL
 cycle of every particle (push, two deposits, move, boundary, field cycle), cell sorts included.
 Beside it the same workload in plain FP64 (`fp64`), the mixed run's error against FP64 after
 100 steps from the same state (`error_vs_fp64`, wave energy, particle energy and moments), and
 the FP64 drop-in configuration (mirror field, Nx=2048, two TSC species, 4.1M particles,
-`drop_in_fp64`).  Synthetic seeded bi-Maxwellian particles; the particle state (459 MB mixed,
+`drop_in_fp64`).  Synthetic seeded bi-Maxwellian particles; the particle state (393 MB mixed,
 722 MB FP64) is larger than L2, so no flush is needed between steps.
 
 Multi-GPU: every rank runs an independent replica of the workload (the path does not shard;
@@ -53,11 +53,11 @@ METRIC = "particle-steps/s"
 # algorithmic HBM bytes per particle-step of the particle pass
 BYTES_PER_PARTICLE_STEP = {
     "fp64": 72,   # read q1, vx, vy, vz, w (40 B), write q1, vx, vy, vz (32 B)
-    "mixed": 44,  # read cell, offset, vx, vy, vz, w (24 B), write cell, offset, vx, vy, vz (20 B)
+    "mixed": 36,  # read position (int32 fixed point), vx, vy, vz, w (20 B), write position, vx, vy, vz (16 B)
 }
-STATE_BYTES = {"fp64": 44, "mixed": 28}  # stored bytes per particle, id included
+STATE_BYTES = {"fp64": 44, "mixed": 24}  # stored bytes per particle, id included
 KERNEL = {"fp64": "push_kernel (fused push + 2 deposits + move + BC, FP64)",
-          "mixed": "push_kernel_mixed (fused push + 2 deposits + move + BC, FP32 with int32 cell)"}
+          "mixed": "push_kernel_mixed (fused push + 2 deposits + move + BC, FP32 with int32 fixed-point position)"}
 
 
 def measured_peak():

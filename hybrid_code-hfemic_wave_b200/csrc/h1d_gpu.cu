@@ -53,8 +53,8 @@ constexpr int64_t STAGE_N      = int64_t{ 1 } << 22; // doubles in a mixed run's
 struct SpeciesState {
     int64_t  n = 0, cap = 0;
     double  *buf[2][5] = {}; // FP64: [parity][q1, vx, vy, vz, w]
-    int32_t *cell[2]   = {}; // mixed precision: [parity] full-grid cell
-    float   *fbuf[2][5] = {}; // mixed precision: [parity][offset in the cell, vx, vy, vz, w]
+    int32_t *pos[2]    = {}; // mixed precision: [parity] fixed-point position (pos_cell, pos_off)
+    float   *fbuf[2][4] = {}; // mixed precision: [parity][vx, vy, vz, w]
     int32_t *pid[2]    = {};
     double  *psd[2][2] = {}; // FP64 with evolving weights: [parity][real_f, marker]
     float   *fpsd[2][2] = {}; // the same in FP32 for mixed precision
@@ -99,6 +99,8 @@ struct h1d_run {
     int64_t      stage_n = 0;     // its length in doubles
     double      *src_dep = nullptr; // per external source: moment<0> (zero), moment<1> x, y, z (M each)
     bool         mixed = false;
+    int          fbits = 0;     // mixed precision: fraction bits F of the fixed-point positions,
+    double       pos_scale = 1; // 2^F, with (Nx + 2) 2^F <= 2^31
     double      *E1[2] = {}; // predictor-corrector: averaged E of phases 1 and 2
     int          fcur = 0; // field parity
     int          dset = 0; // deposit set parity
@@ -508,8 +510,9 @@ PushArgsMixed mixed_args(h1d_run *run, int s, PushArgs const &a)
 {
     SpeciesState &S = run->sp[s];
     PushArgsMixed m{};
-    m.cell = S.cell[S.cur], m.off = S.fbuf[S.cur][0], m.vx = S.fbuf[S.cur][1], m.vy = S.fbuf[S.cur][2];
-    m.vz = S.fbuf[S.cur][3], m.w = S.fbuf[S.cur][4], m.pid = S.pid[S.cur], m.n = a.n, m.Nx = a.Nx;
+    m.pos = S.pos[S.cur], m.vx = S.fbuf[S.cur][0], m.vy = S.fbuf[S.cur][1], m.vz = S.fbuf[S.cur][2];
+    m.w = S.fbuf[S.cur][3], m.pid = S.pid[S.cur], m.n = a.n, m.Nx = a.Nx;
+    m.fbits = run->fbits, m.scale = static_cast<float>(run->pos_scale), m.inv_scale = static_cast<float>(1 / run->pos_scale);
     m.EB = run->EBf + EBF_STRIDE * PAD;
     for (int d = 0; d < 2; ++d)
         for (int q = 0; q < 4; ++q)
@@ -592,7 +595,7 @@ int sort_species(h1d_run *run, int s)
     first.full_min = -0.5 * Nx, first.Nx = Nx, first.dead = S.dead, first.status = run->d_status;
     first.absorbing = run->p.particle_bc == H1D_BC_ABSORBING;
     if (run->mixed)
-        first.cell = S.cell[S.cur], first.wf = S.fbuf[S.cur][4];
+        first.pos = S.pos[S.cur], first.fbits = run->fbits, first.wf = S.fbuf[S.cur][3];
     else
         first.q1 = S.buf[S.cur][0], first.w = S.buf[S.cur][4];
     MoveMixed         mm{};
@@ -600,19 +603,19 @@ int sort_species(h1d_run *run, int s)
     MoveFP64          md{};
     MoveFP64T<true>   mp{};
     bool const        psd = S.psd[0][0] != nullptr || S.fpsd[0][0] != nullptr;
-    for (int k = 0; k < 5; ++k) {
-        mm.src[k] = S.fbuf[S.cur][k], mm.dst[k] = S.fbuf[1 - S.cur][k];
-        md.src[k] = mp.src[k] = S.buf[S.cur][k], md.dst[k] = mp.dst[k] = S.buf[1 - S.cur][k];
-    }
     for (int k = 0; k < 5; ++k)
+        md.src[k] = mp.src[k] = S.buf[S.cur][k], md.dst[k] = mp.dst[k] = S.buf[1 - S.cur][k];
+    for (int k = 0; k < 4; ++k) {
+        mm.src[k] = S.fbuf[S.cur][k], mm.dst[k] = S.fbuf[1 - S.cur][k];
         mq.src[k] = S.fbuf[S.cur][k], mq.dst[k] = S.fbuf[1 - S.cur][k];
+    }
     for (int k = 0; k < 2; ++k) {
         mp.src[5 + k] = S.psd[S.cur][k], mp.dst[5 + k] = S.psd[1 - S.cur][k];
-        mq.src[5 + k] = S.fpsd[S.cur][k], mq.dst[5 + k] = S.fpsd[1 - S.cur][k];
+        mq.src[4 + k] = S.fpsd[S.cur][k], mq.dst[4 + k] = S.fpsd[1 - S.cur][k];
     }
-    mq.cell_src = S.cell[S.cur], mq.cell_dst = S.cell[1 - S.cur];
+    mq.pos_src = S.pos[S.cur], mq.pos_dst = S.pos[1 - S.cur];
     mq.pid_src = S.pid[S.cur], mq.pid_dst = S.pid[1 - S.cur];
-    mm.cell_src = S.cell[S.cur], mm.cell_dst = S.cell[1 - S.cur];
+    mm.pos_src = S.pos[S.cur], mm.pos_dst = S.pos[1 - S.cur];
     mm.pid_src = md.pid_src = mp.pid_src = S.pid[S.cur];
     mm.pid_dst = md.pid_dst = mp.pid_dst = S.pid[1 - S.cur];
     int shift = 0, src = 0; // keys/idx buffer the current pass reads (the first pass reads the particles)
@@ -952,8 +955,9 @@ int finalize_moments(h1d_run *run)
         CU(cudaMemsetAsync(S.mom_raw, 0, sizeof(double) * 10 * run->M, run->stream));
         if (S.n > 0 && run->mixed) {
             MomentArgsMixed a{};
-            a.cell = S.cell[S.cur], a.off = S.fbuf[S.cur][0], a.vx = S.fbuf[S.cur][1], a.vy = S.fbuf[S.cur][2];
-            a.vz = S.fbuf[S.cur][3], a.w = S.fbuf[S.cur][4], a.n = S.n, a.ppt = ppt_for(run, s), a.vec = 1;
+            a.pos = S.pos[S.cur], a.vx = S.fbuf[S.cur][0], a.vy = S.fbuf[S.cur][1], a.vz = S.fbuf[S.cur][2];
+            a.w = S.fbuf[S.cur][3], a.n = S.n, a.ppt = ppt_for(run, s), a.vec = 1;
+            a.fbits = run->fbits, a.inv_scale = static_cast<float>(1 / run->pos_scale);
             a.Nx = static_cast<int>(run->Nx), a.status = run->d_status;
             for (int q = 0; q < 10; ++q)
                 a.out[q] = S.mom_raw + static_cast<size_t>(q) * run->M + PAD;
@@ -1042,9 +1046,9 @@ int ensure_capacity(h1d_run *run, int s, int64_t n)
                 b = nullptr;
                 CU(cudaMalloc(&b, sizeof(float) * cap));
             }
-            cudaFree(S.cell[k]);
-            S.cell[k] = nullptr;
-            CU(cudaMalloc(&S.cell[k], sizeof(int32_t) * cap));
+            cudaFree(S.pos[k]);
+            S.pos[k] = nullptr;
+            CU(cudaMalloc(&S.pos[k], sizeof(int32_t) * cap));
             if (evolves_psd(run->p.kinetic[s]))
                 for (auto *&b : S.fpsd[k]) {
                     cudaFree(b);
@@ -1653,6 +1657,11 @@ int h1d_create(h1d_params const *params, h1d_run **out)
     run->fb            = field_group(L, FIELD_SMEM_RUN);
     run->field_smem    = field_smem_bytes(L, run->fb);
     run->mixed = p.precision == H1D_PREC_MIXED;
+    // the most fraction bits (at most FP32's 24) with positions in (-2, Nx + 2) cells inside an int32
+    run->fbits = 24;
+    while (run->fbits > 0 && ((static_cast<int64_t>(p.Nx) + 2) << run->fbits) > (int64_t{ 1 } << 31))
+        --run->fbits;
+    run->pos_scale = std::ldexp(1.0, run->fbits);
     run->stage_n = 1 << 16;
     for (int s = 0; s < p.n_kinetic; ++s)
         run->stage_n = std::max<int64_t>(run->stage_n, std::min<int64_t>(STAGE_N, p.Nx * std::max<int64_t>(p.kinetic[s].Nc, 0)));
@@ -1723,7 +1732,7 @@ int h1d_destroy(h1d_run *run)
                 cudaFree(b);
             for (auto *b : S.fbuf[k])
                 cudaFree(b);
-            cudaFree(S.cell[k]);
+            cudaFree(S.pos[k]);
             cudaFree(S.pid[k]), cudaFree(S.keys[k]), cudaFree(S.idx[k]);
             cudaFree(S.psd[k][0]), cudaFree(S.psd[k][1]);
             cudaFree(S.fpsd[k][0]), cudaFree(S.fpsd[k][1]);
@@ -1762,10 +1771,10 @@ int h1d_upload_particles(h1d_run *run, int s, int64_t n, double const *q1, doubl
                 unsigned const nb = static_cast<unsigned>((c + 255) / 256);
                 CU(cudaMemcpyAsync(run->stage, src[k] + o, sizeof(double) * c, cudaMemcpyHostToDevice, run->stream));
                 if (k == 0)
-                    q1_to_mixed_kernel<<<nb, 256, 0, run->stream>>>(run->stage, c, -0.5 * run->Nx, S.cell[0] + o,
-                                                                    S.fbuf[0][0] + o);
+                    q1_to_pos_kernel<<<nb, 256, 0, run->stream>>>(run->stage, c, -0.5 * run->Nx, run->pos_scale,
+                                                                  S.pos[0] + o);
                 else
-                    to_f32_kernel<<<nb, 256, 0, run->stream>>>(run->stage, c, S.fbuf[0][k] + o);
+                    to_f32_kernel<<<nb, 256, 0, run->stream>>>(run->stage, c, S.fbuf[0][k - 1] + o);
                 CU(cudaGetLastError());
             }
     }
@@ -1777,7 +1786,7 @@ int h1d_upload_particles(h1d_run *run, int s, int64_t n, double const *q1, doubl
         CU(launch_fill(S.psd[0][1], n, 1.0, run->stream));
     }
     if (n && S.fpsd[0][0]) {
-        CU(cudaMemcpyAsync(S.fpsd[0][0], S.fbuf[0][4], sizeof(float) * n, cudaMemcpyDeviceToDevice, run->stream));
+        CU(cudaMemcpyAsync(S.fpsd[0][0], S.fbuf[0][3], sizeof(float) * n, cudaMemcpyDeviceToDevice, run->stream));
         CU(launch_fill_f(S.fpsd[0][1], n, 1.0f, run->stream));
     }
     if (n)
@@ -1837,7 +1846,7 @@ int h1d_download_psd(h1d_run *run, int s, double *real_f, double *marker)
         for (int64_t o = 0; dst[k] && o < S.n; o += run->stage_n) {
             int64_t const c = std::min<int64_t>(run->stage_n, S.n - o);
             from_mixed_kernel<<<static_cast<unsigned>((c + 255) / 256), 256, 0, run->stream>>>(nullptr, S.fpsd[S.cur][k] + o, c,
-                                                                                             0.0, run->stage);
+                                                                                             0.0, 1.0, run->stage);
             CU(cudaGetLastError());
             CU(cudaMemcpyAsync(dst[k] + o, run->stage, sizeof(double) * c, cudaMemcpyDeviceToHost, run->stream));
         }
@@ -1874,8 +1883,8 @@ int h1d_populate(h1d_run *run, int s, int64_t n, uint64_t seed, double beta1, do
     a.T2 = T2_T1, a.oneMinusT2 = 1 - T2_T1, a.vth1 = std::sqrt(beta1) * p.c * std::fabs(d.Oc) / d.op;
     a.q1min = q1min, a.q1max_in = std::nextafter(q1max, q1min), a.full_min = q1min;
     if (run->mixed)
-        a.cell = S.cell[0], a.off = S.fbuf[0][0], a.fvx = S.fbuf[0][1], a.fvy = S.fbuf[0][2], a.fvz = S.fbuf[0][3],
-        a.fw = S.fbuf[0][4];
+        a.pos = S.pos[0], a.fvx = S.fbuf[0][0], a.fvy = S.fbuf[0][1], a.fvz = S.fbuf[0][2], a.fw = S.fbuf[0][3],
+        a.scale = run->pos_scale;
     else
         a.q1 = S.buf[0][0], a.vx = S.buf[0][1], a.vy = S.buf[0][2], a.vz = S.buf[0][3], a.w = S.buf[0][4];
     if (n) {
@@ -2017,8 +2026,9 @@ int h1d_download_particles(h1d_run *run, int s, double *q1, double *vx, double *
             for (int64_t o = 0; o < S.n; o += run->stage_n) {
                 int64_t const  c  = std::min<int64_t>(run->stage_n, S.n - o);
                 unsigned const nb = static_cast<unsigned>((c + 255) / 256);
-                from_mixed_kernel<<<nb, 256, 0, run->stream>>>(k == 0 ? S.cell[S.cur] + o : nullptr, S.fbuf[S.cur][k] + o,
-                                                               c, -0.5 * run->Nx, run->stage);
+                from_mixed_kernel<<<nb, 256, 0, run->stream>>>(k == 0 ? S.pos[S.cur] + o : nullptr,
+                                                               k == 0 ? nullptr : S.fbuf[S.cur][k - 1] + o, c, -0.5 * run->Nx,
+                                                               1 / run->pos_scale, run->stage);
                 CU(cudaGetLastError());
                 CU(cudaMemcpyAsync(dst[k] + o, run->stage, sizeof(double) * c, cudaMemcpyDeviceToHost, run->stream));
             }
@@ -2323,8 +2333,9 @@ int h1d_vhistogram(h1d_run *run, int s, double ext_loc, double ext_len, double v
     if (st == H1D_OK && S.n > 0) {
         VHistArgs a{};
         if (run->mixed)
-            a.cell = S.cell[S.cur], a.off = S.fbuf[S.cur][0], a.fvx = S.fbuf[S.cur][1], a.fvy = S.fbuf[S.cur][2],
-            a.fvz = S.fbuf[S.cur][3], a.fw = S.fbuf[S.cur][4], a.freal_f = S.fpsd[S.cur][0], a.fmarker = S.fpsd[S.cur][1];
+            a.pos = S.pos[S.cur], a.fvx = S.fbuf[S.cur][0], a.fvy = S.fbuf[S.cur][1], a.fvz = S.fbuf[S.cur][2],
+            a.fw = S.fbuf[S.cur][3], a.freal_f = S.fpsd[S.cur][0], a.fmarker = S.fpsd[S.cur][1],
+            a.inv_scale = 1 / run->pos_scale;
         else
             a.q1 = S.buf[S.cur][0], a.vx = S.buf[S.cur][1], a.vy = S.buf[S.cur][2], a.vz = S.buf[S.cur][3],
             a.w = S.buf[S.cur][4], a.real_f = S.psd[S.cur][0], a.marker = S.psd[S.cur][1];
@@ -2422,7 +2433,7 @@ struct ServerReq {
 size_t request_bytes(h1d_request const &rq)
 {
     h1d_params const &p   = rq.params;
-    size_t const      per = p.precision == H1D_PREC_MIXED ? 6 * 4 : 5 * 8;
+    size_t const      per = p.precision == H1D_PREC_MIXED ? 5 * 4 : 5 * 8;
     size_t            b   = 0;
     for (int s = 0; s < p.n_kinetic; ++s) {
         size_t const n = static_cast<size_t>(std::max<int64_t>(rq.n_particles[s], 0)) + 64;
@@ -2870,7 +2881,7 @@ struct CkptHeader {
     int64_t  n[H1D_MAX_KINETIC];
 };
 constexpr char     CKPT_MAGIC[8] = { 'H', '1', 'D', 'C', 'K', 'P', 'T', 0 };
-constexpr uint32_t CKPT_VERSION  = 2;
+constexpr uint32_t CKPT_VERSION  = 3;
 
 // FNV-1a over the run's parameters with the tuning knob (sort interval) cleared
 uint64_t params_signature(h1d_params p)
@@ -2887,7 +2898,7 @@ uint64_t params_signature(h1d_params p)
 size_t particle_bytes(h1d_run const *run, int s, int64_t n)
 {
     size_t const psd = evolves_psd(run->p.kinetic[s]) ? 2 * (run->mixed ? 4 : 8) : 0;
-    return static_cast<size_t>(n) * ((run->mixed ? 6 * 4 + 4 : 5 * 8 + 4) + psd);
+    return static_cast<size_t>(n) * ((run->mixed ? 5 * 4 + 4 : 5 * 8 + 4) + psd);
 }
 
 size_t ckpt_size(h1d_run const *run)
@@ -2948,8 +2959,8 @@ int h1d_checkpoint_save(h1d_run *run, void *buffer, size_t capacity, size_t *wri
         SpeciesState const &S = run->sp[s];
         size_t const        n = static_cast<size_t>(S.n);
         if (run->mixed) {
-            CU(d2h(S.cell[S.cur], 4 * n));
-            for (int k = 0; k < 5; ++k)
+            CU(d2h(S.pos[S.cur], 4 * n));
+            for (int k = 0; k < 4; ++k)
                 CU(d2h(S.fbuf[S.cur][k], 4 * n));
         } else {
             for (int k = 0; k < 5; ++k)
@@ -3008,8 +3019,8 @@ int h1d_checkpoint_load(h1d_run *run, void const *buffer, size_t size)
         S.cur = 0, S.n = hd.n[s];
         size_t const n = static_cast<size_t>(S.n);
         if (run->mixed) {
-            CU(h2d(S.cell[0], 4 * n));
-            for (int k = 0; k < 5; ++k)
+            CU(h2d(S.pos[0], 4 * n));
+            for (int k = 0; k < 4; ++k)
                 CU(h2d(S.fbuf[0][k], 4 * n));
         } else {
             for (int k = 0; k < 5; ++k)

@@ -21,10 +21,11 @@ struct MomentArgs {
     unsigned      *status;
 };
 struct MomentArgsMixed {
-    int32_t const *cell;
-    float const   *off, *vx, *vy, *vz, *w;
+    int32_t const *pos; // fixed-point positions (pos_cell, pos_off)
+    float const   *vx, *vy, *vz, *w;
     int64_t        n;
-    int            ppt, Nx;
+    int            ppt, Nx, fbits;
+    float          inv_scale;
     int            vec; // every array 16-byte aligned: vector loads
     double        *out[10];
     unsigned      *status;
@@ -52,8 +53,8 @@ template <> struct MomTile<MomentArgs> {
 };
 template <> struct MomTile<MomentArgsMixed> {
     static constexpr int NP = 4;
-    int4                 cell;
-    float4               off, vx, vy, vz, w;
+    int4                 pos;
+    float4               vx, vy, vz, w;
 };
 __device__ __forceinline__ double el2(double2 const &v, int j) { return j ? v.y : v.x; }
 __device__ __forceinline__ float  el4(float4 const &v, int j) { return j == 0 ? v.x : j == 1 ? v.y : j == 2 ? v.z : v.w; }
@@ -79,13 +80,12 @@ __device__ __forceinline__ MomTile<MomentArgsMixed> mom_load(MomentArgsMixed con
 {
     MomTile<MomentArgsMixed> t;
     if (a.vec && i + 3 < a.n) {
-        t.cell = *reinterpret_cast<int4 const *>(a.cell + i), t.off = *reinterpret_cast<float4 const *>(a.off + i);
+        t.pos  = *reinterpret_cast<int4 const *>(a.pos + i);
         t.vx   = *reinterpret_cast<float4 const *>(a.vx + i), t.vy = *reinterpret_cast<float4 const *>(a.vy + i);
         t.vz   = *reinterpret_cast<float4 const *>(a.vz + i), t.w = *reinterpret_cast<float4 const *>(a.w + i);
     } else {
         int64_t const j[4] = { min(i, a.n - 1), min(i + 1, a.n - 1), min(i + 2, a.n - 1), min(i + 3, a.n - 1) };
-        t.cell = make_int4(a.cell[j[0]], a.cell[j[1]], a.cell[j[2]], a.cell[j[3]]);
-        t.off  = make_float4(a.off[j[0]], a.off[j[1]], a.off[j[2]], a.off[j[3]]);
+        t.pos  = make_int4(a.pos[j[0]], a.pos[j[1]], a.pos[j[2]], a.pos[j[3]]);
         t.vx   = make_float4(a.vx[j[0]], a.vx[j[1]], a.vx[j[2]], a.vx[j[3]]);
         t.vy   = make_float4(a.vy[j[0]], a.vy[j[1]], a.vy[j[2]], a.vy[j[3]]);
         t.vz   = make_float4(a.vz[j[0]], a.vz[j[1]], a.vz[j[2]], a.vz[j[3]]);
@@ -102,7 +102,8 @@ __device__ __forceinline__ MomParticle<double> mom_particle(MomentArgs const &a,
 }
 __device__ __forceinline__ MomParticle<float> mom_particle(MomentArgsMixed const &a, MomTile<MomentArgsMixed> const &t, int j)
 {
-    ShapeF<1> const sh = make_shape_f<1>(el4(t.cell, j), el4(t.off, j));
+    int32_t const   X  = el4(t.pos, j);
+    ShapeF<1> const sh = make_shape_f<1>(pos_cell(X, a.fbits), pos_off(X, a.fbits, a.inv_scale));
     return { sh.i0, sh.w[0], sh.w[1], el4(t.w, j), el4(t.vx, j), el4(t.vy, j), el4(t.vz, j), stencil_ok_f(sh, a.Nx) };
 }
 
@@ -221,21 +222,19 @@ __global__ void __launch_bounds__(MOM_THREADS, mom_min_blocks<Args>) moments_ker
 }
 
 // FP64 host-layout particles <-> mixed-precision particles (upload and download), one component at
-// a time so that the FP64 staging buffer holds a single array: position q1 <-> (cell, offset) with
-// cell = floor(q1 - q1min), and velocity / weight components FP64 <-> FP32
-__global__ void q1_to_mixed_kernel(double const *q1, int64_t n, double full_min, int32_t *cell, float *off)
+// a time so that the FP64 staging buffer holds a single array: position q1 <-> the fixed-point
+// X = round((q1 - q1min) 2^F), and velocity / weight components FP64 <-> FP32
+__device__ __forceinline__ int32_t q1_to_pos(double q1, double full_min, double scale)
+{
+    double const y  = (q1 - full_min) * scale;
+    bool const   ok = y > -1073741824.0 && y < 2147483520.0; // NaN and lost positions map outside the grid
+    return ok ? static_cast<int32_t>(__double2ll_rn(y)) : -0x40000000;
+}
+__global__ void q1_to_pos_kernel(double const *q1, int64_t n, double full_min, double scale, int32_t *pos)
 {
     int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= n)
-        return;
-    double const x  = q1[i] - full_min;
-    double const f  = floor(x);
-    bool const   ok = f > -1073741824.0 && f < 1073741824.0; // NaN and lost positions map outside the grid
-    float        o  = ok ? static_cast<float>(x - f) : 0.5f;
-    if (o >= 1.0f)
-        o = 0.99999994f;
-    cell[i] = ok ? static_cast<int32_t>(f) : -0x40000000;
-    off[i]  = o;
+    if (i < n)
+        pos[i] = q1_to_pos(q1[i], full_min, scale);
 }
 __global__ void to_f32_kernel(double const *src, int64_t n, float *dst)
 {
@@ -243,13 +242,15 @@ __global__ void to_f32_kernel(double const *src, int64_t n, float *dst)
     if (i < n)
         dst[i] = static_cast<float>(src[i]);
 }
-// one component at a time, so that the caller's FP64 staging buffer holds a single array
-__global__ void from_mixed_kernel(int32_t const *cell, float const *src, int64_t n, double full_min, double *dst)
+// one component at a time, so that the caller's FP64 staging buffer holds a single array: the
+// position (exact in FP64) from `pos`, or an FP32 component from `src`
+__global__ void from_mixed_kernel(int32_t const *pos, float const *src, int64_t n, double full_min, double inv_scale,
+                                  double *dst)
 {
     int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    dst[i] = cell ? full_min + static_cast<double>(cell[i]) + static_cast<double>(src[i]) : static_cast<double>(src[i]);
+    dst[i] = pos ? full_min + static_cast<double>(pos[i]) * inv_scale : static_cast<double>(src[i]);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -274,8 +275,9 @@ struct PopulateArgs {
     double   N_loc, N_len, xiD1, T2m1, sqrtT2, sDxXi, T2, oneMinusT2, vth1, q1min, q1max_in, full_min;
     int      homogeneous;
     double  *q1, *vx, *vy, *vz, *w;                 // FP64 storage, or
-    int32_t *cell;                                   // mixed-precision storage
-    float   *off, *fvx, *fvy, *fvz, *fw;
+    int32_t *pos;                                    // mixed-precision storage
+    float   *fvx, *fvy, *fvz, *fw;
+    double   scale;                                  // 2^F of the fixed-point positions
 };
 
 __device__ __forceinline__ double radical_inverse_dev(uint64_t k, unsigned base)
@@ -333,12 +335,7 @@ __global__ void populate_kernel(PopulateArgs a)
     if (a.q1) {
         a.q1[i] = q1, a.vx[i] = vx, a.vy[i] = vy, a.vz[i] = vz, a.w[i] = 1.0;
     } else {
-        double const x = q1 - a.full_min;
-        double const f = floor(x);
-        float        o = static_cast<float>(x - f);
-        if (o >= 1.0f)
-            o = 0.99999994f;
-        a.cell[i] = static_cast<int32_t>(f), a.off[i] = o;
+        a.pos[i] = q1_to_pos(q1, a.full_min, a.scale);
         a.fvx[i] = static_cast<float>(vx), a.fvy[i] = static_cast<float>(vy), a.fvz[i] = static_cast<float>(vz);
         a.fw[i] = 1.0f;
     }
@@ -355,8 +352,9 @@ __global__ void populate_kernel(PopulateArgs a)
 struct VHistArgs {
     double const  *q1, *vx, *vy, *vz, *w;        // FP64 storage (+ real_f, marker when the weights evolve), or
     double const  *real_f, *marker;
-    int32_t const *cell;                         // mixed-precision storage
-    float const   *off, *fvx, *fvy, *fvz, *fw, *freal_f, *fmarker;
+    int32_t const *pos;                          // mixed-precision storage
+    float const   *fvx, *fvy, *fvz, *fw, *freal_f, *fmarker;
+    double         inv_scale;                    // 2^-F of the fixed-point positions
     int64_t        n;
     double         half_min, full_min, ext_lo, ext_hi, v1min, v1len, v2min, v2len;
     int            v1dim, v2dim;
@@ -375,7 +373,7 @@ __global__ void vhist_kernel(VHistArgs a)
     if (a.q1) {
         q1 = a.q1[k], vx = a.vx[k], vy = a.vy[k], vz = a.vz[k], w = a.w[k];
     } else {
-        q1 = a.full_min + static_cast<double>(a.cell[k]) + static_cast<double>(a.off[k]);
+        q1 = a.full_min + static_cast<double>(a.pos[k]) * a.inv_scale;
         vx = a.fvx[k], vy = a.fvy[k], vz = a.fvz[k], w = a.fw[k];
     }
     if (!(q1 >= a.ext_lo && q1 < a.ext_hi))

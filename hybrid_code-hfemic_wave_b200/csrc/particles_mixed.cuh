@@ -1,11 +1,14 @@
 // Mixed-precision particle pass: the same cycle as push_kernel (particles.cuh) with
-//   - position as an int32 full-grid cell plus an FP32 offset in [0, 1), so the shape weights
-//     come from the in-cell offset and keep ~1e-7 cell resolution anywhere on the grid;
+//   - position as one int32 in fixed point: x = q1 - q1min (full grid, in cells) times 2^F, F =
+//     31 - ceil(log2(Nx + 2)) fraction bits (18 at Nx = 4096), so the cell is X >> F and the
+//     in-cell offset the low F bits; the shape weights come from the offset, a move is an exact
+//     integer addition of the displacement rounded to 2^-F cell, and the resolution is the same
+//     anywhere on the grid;
 //   - FP32 velocity, weight, field interpolation, mirror geometry and Boris push;
 //   - FP32 deposits into per-lane shared-memory columns of a per-warp window of cells, summed
 //     into the FP64 moment arrays per cell when the window moves.
-// The field cycle that consumes the moments stays FP64.  Traffic: read cell, offset, v, w
-// (24 B), write cell, offset, v (20 B) per particle-step.
+// The field cycle that consumes the moments stays FP64.  Traffic: read position, v, w (20 B),
+// write position, v (16 B) per particle-step.
 #pragma once
 
 #include "particles.cuh"
@@ -13,14 +16,16 @@
 namespace h1d {
 
 struct PushArgsMixed {
-    int32_t     *cell;
-    float       *off, *vx, *vy, *vz, *w;
+    int32_t     *pos; // fixed-point position (pos_cell, pos_off)
+    float       *vx, *vy, *vz, *w;
     int32_t const *pid;
     int64_t      n;
     int          Nx;
     float const *EB; // per cell {Ex, Ey, Ez, dBx, dBy, dBz, 0, 0} in FP32 (EBF_STRIDE), at interior cell 0
     double      *dep[2][4];
     float        full_min, xiD1, inv_D1, O0, dt, travel_scale, xiO0_Oc, dtOc_2O0, cDtOc_2O0;
+    int          fbits;            // F, the fraction bits of a position
+    float        scale, inv_scale; // 2^F, 2^-F
     unsigned    *status;
     unsigned long long *fallbacks;
     uint64_t     seed, counter;
@@ -143,37 +148,32 @@ __device__ __forceinline__ void sincos_taylor_f2(float2 x, float2 &s, float2 &c)
     c               = pfma(pneg(pc), x2, bc(1.0f));
 }
 
-// move by dq cells (|dq| < 1 is checked by the caller); returns the new (cell, off)
-__device__ __forceinline__ void move_cell(int &cell, float &off, float dq)
+// a fixed-point position: its full-grid cell and its offset in the cell, [0, 1) exactly
+__device__ __forceinline__ int   pos_cell(int32_t X, int F) { return X >> F; }
+__device__ __forceinline__ float pos_off(int32_t X, int F, float inv_scale)
 {
-    float o = off + dq;
-    if (o >= 1.0f)
-        cell += 1, o -= 1.0f;
-    else if (o < 0.0f)
-        cell -= 1, o += 1.0f;
-    off = o < 1.0f ? o : 0.99999994f;
+    return static_cast<float>(X & ((1 << F) - 1)) * inv_scale;
 }
+// move by dq cells (|dq| < 1 is checked by the caller): an integer addition of dq rounded to 2^-F
+__device__ __forceinline__ void move_pos(int32_t &X, float dq, float scale) { X += __float2int_rn(dq * scale); }
 
 template <int BC>
-__device__ __forceinline__ bool boundary_mixed(PushArgsMixed const &a, int &cell, float &off, f3 &v, int32_t pid,
-                                               uint64_t counter)
+__device__ __forceinline__ bool boundary_mixed(PushArgsMixed const &a, int32_t &X, f3 &v, int32_t pid, uint64_t counter)
 {
+    int32_t const len = a.Nx << a.fbits; // the domain [0, Nx) in fixed point
     if constexpr (BC == BCK_PERIODIC) {
-        if (cell < 0)
-            cell += a.Nx;
-        else if (cell >= a.Nx)
-            cell -= a.Nx;
+        if (X < 0)
+            X += len;
+        else if (X >= len)
+            X -= len;
         return true;
     } else if constexpr (BC == BCK_REFLECTING) {
-        bool const left = cell < 0, right = cell >= a.Nx;
+        bool const left = X < 0, right = X >= len;
         if (left || right) { // q1 -> 2 q1_boundary - q1 (Delegate.cc:116-145)
-            if (left) {      // q1 - q1min = -1 + off -> 1 - off
-                cell = off > 0.0f ? 0 : 1;
-                off  = off > 0.0f ? 1.0f - off : 0.0f;
-            } else { // q1 - q1min = Nx + off -> Nx - off
-                cell = a.Nx - 1;
-                off  = off > 0.0f ? 1.0f - off : 0.99999994f;
-            }
+            if (left)        // x -> -x
+                X = -X;
+            else // x -> 2 Nx - x; x = Nx exactly stays inside, at the last position of the grid
+                X = X > len ? len - (X - len) : len - 1;
             v.x = -v.x;
             if (a.randomize) {
                 float s, c;
@@ -189,7 +189,7 @@ __device__ __forceinline__ bool boundary_mixed(PushArgsMixed const &a, int &cell
         }
         return true;
     } else {
-        return cell >= 0 && cell < a.Nx;
+        return X >= 0 && X < len;
     }
 }
 
@@ -216,8 +216,8 @@ static_assert(4 * MIX_W == 32, "a window flush reduce-scatters exactly 32 values
 // pipeline is one stage shorter, so that four CTAs still fit an SM.
 template <bool PSD>
 struct PipeStageMixedT {
-    int32_t cell[MIX_CHUNK];
-    float   off[MIX_CHUNK], vx[MIX_CHUNK], vy[MIX_CHUNK], vz[MIX_CHUNK], w[MIX_CHUNK];
+    int32_t pos[MIX_CHUNK];
+    float   vx[MIX_CHUNK], vy[MIX_CHUNK], vz[MIX_CHUNK], w[MIX_CHUNK];
     int32_t pid[MIX_CHUNK];
     float   real_f[PSD ? MIX_CHUNK : 4], marker[PSD ? MIX_CHUNK : 4];
 };
@@ -428,8 +428,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                         int64_t const  start = (c0 + j - G.chunk0[gr]) * MIX_CHUNK;
                         uint32_t const cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(MIX_CHUNK), a.n - start));
                         uint32_t const b4    = round16(cnt * 4);
-                        bulk_store(a.cell + start, stage[s].cell, b4);
-                        bulk_store(a.off + start, stage[s].off, b4);
+                        bulk_store(a.pos + start, stage[s].pos, b4);
                         bulk_store(a.vx + start, stage[s].vx, b4);
                         bulk_store(a.vy + start, stage[s].vy, b4);
                         bulk_store(a.vz + start, stage[s].vz, b4);
@@ -448,9 +447,8 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                     int64_t const  start = (c0 + i - G.chunk0[gl]) * MIX_CHUNK;
                     uint32_t const cnt   = static_cast<uint32_t>(min(static_cast<int64_t>(MIX_CHUNK), a.n - start));
                     uint32_t const b4    = round16(cnt * 4);
-                    mbar_arrive_expect_tx(&full[s], (6 + (lpid ? 1 : 0) + (PSD ? 2 : 0)) * b4);
-                    bulk_load(stage[s].cell, a.cell + start, b4, &full[s]);
-                    bulk_load(stage[s].off, a.off + start, b4, &full[s]);
+                    mbar_arrive_expect_tx(&full[s], (5 + (lpid ? 1 : 0) + (PSD ? 2 : 0)) * b4);
+                    bulk_load(stage[s].pos, a.pos + start, b4, &full[s]);
                     bulk_load(stage[s].vx, a.vx + start, b4, &full[s]);
                     bulk_load(stage[s].vy, a.vy + start, b4, &full[s]);
                     bulk_load(stage[s].vz, a.vz + start, b4, &full[s]);
@@ -506,9 +504,9 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
         // all their deposits.
         int const  i2      = w0 + 2 * lane;
         bool const live[2] = { i2 < cnt, i2 + 1 < cnt }; // slots past cnt hold stale data: pushed, never stored or deposited
-        int2 const c_in    = *reinterpret_cast<int2 const *>(P.cell + i2);
-        int        cell[2] = { c_in.x, c_in.y };
-        float2     off     = *reinterpret_cast<float2 const *>(P.off + i2);
+        int2 const x_in    = *reinterpret_cast<int2 const *>(P.pos + i2);
+        int32_t    X[2]    = { x_in.x, x_in.y };
+        int32_t const half = int32_t{ 1 } << (a.fbits - 1); // a removed particle: cell 0, offset 1/2
         p3         v       = { *reinterpret_cast<float2 const *>(P.vx + i2), *reinterpret_cast<float2 const *>(P.vy + i2),
                                *reinterpret_cast<float2 const *>(P.vz + i2) };
         float2       w    = *reinterpret_cast<float2 const *>(P.w + i2);
@@ -521,24 +519,29 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                 float dq = a.inv_D1 * el(v.x, k) * (0.5f * a.dt);
                 if constexpr (MIRROR) {
                     float s_, c_;
-                    sincos_taylor_f(a.xiD1 * (static_cast<float>(cell[k]) + a.full_min + el(off, k)), s_, c_);
+                    sincos_taylor_f(a.xiD1 * (static_cast<float>(pos_cell(X[k], a.fbits)) + a.full_min
+                                              + pos_off(X[k], a.fbits, a.inv_scale)),
+                                    s_, c_);
                     dq *= c_ * c_;
                 }
                 if (live[k] && !(fabsf(dq * a.travel_scale) < 1.0f))
                     bad |= ST_MOVED_TOO_FAR;
                 f3 vk = { el(v.x, k), el(v.y, k), el(v.z, k) };
-                move_cell(cell[k], el(off, k), dq);
-                alive[k] = boundary_mixed<BC>(a, cell[k], el(off, k), vk, k ? pid.y : pid.x, a.counter);
+                move_pos(X[k], dq, a.scale);
+                alive[k] = boundary_mixed<BC>(a, X[k], vk, k ? pid.y : pid.x, a.counter);
                 if (!alive[k])
-                    el(w, k) = 0.0f, cell[k] = 0, el(off, k) = 0.5f, vk = { 0, 0, 0 };
+                    el(w, k) = 0.0f, X[k] = half, vk = { 0, 0, 0 };
                 el(v.x, k) = vk.x, el(v.y, k) = vk.y, el(v.z, k) = vk.z;
             }
         }
         ShapeF<O> ds0[2], ds1[2];
         bool      in0[2], push[2];
         p3        E = { { 0, 0 }, { 0, 0 }, { 0, 0 } }, dB = E;
+        int       cell[2];
+        float2    off;
 #pragma unroll
         for (int k = 0; k < 2; ++k) { // E and dB at the particles, each into its half of the pairs
+            cell[k] = pos_cell(X[k], a.fbits), el(off, k) = pos_off(X[k], a.fbits, a.inv_scale);
             ds0[k]  = make_shape_f<O>(cell[k], el(off, k));
             in0[k]  = stencil_ok_f(ds0[k], a.Nx);
             push[k] = in0[k] && alive[k] && a.move_steps != 0;
@@ -596,19 +599,17 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                     P.real_f[i2 + k] = rf;
                 }
                 el(v_push.x, k) = vk.x, el(v_push.y, k) = vk.y, el(v_push.z, k) = vk.z;
-                move_cell(cell[k], el(off, k), el(dq, k));
-                alive[k] = boundary_mixed<BC>(a, cell[k], el(off, k), vk, k ? pid.y : pid.x,
-                                              a.counter + (a.move_steps == 2 ? 1 : 0));
+                move_pos(X[k], el(dq, k), a.scale);
+                alive[k] = boundary_mixed<BC>(a, X[k], vk, k ? pid.y : pid.x, a.counter + (a.move_steps == 2 ? 1 : 0));
                 if (!alive[k])
-                    el(w, k) = 0.0f, cell[k] = 0, el(off, k) = 0.5f, vk = { 0, 0, 0 };
+                    el(w, k) = 0.0f, X[k] = half, vk = { 0, 0, 0 };
                 el(v.x, k) = vk.x, el(v.y, k) = vk.y, el(v.z, k) = vk.z;
             }
-            ds1[k] = make_shape_f<O>(cell[k], el(off, k));
+            ds1[k] = make_shape_f<O>(pos_cell(X[k], a.fbits), pos_off(X[k], a.fbits, a.inv_scale));
             dd0[k] = live[k] && in0[k] && (a.deposit_mask & 1);
             dd1[k] = live[k] && (a.deposit_mask & 2) && el(w, k) != 0.0f && stencil_ok_f(ds1[k], a.Nx);
         }
-        *reinterpret_cast<int2 *>(P.cell + i2)  = make_int2(cell[0], cell[1]);
-        *reinterpret_cast<float2 *>(P.off + i2) = off;
+        *reinterpret_cast<int2 *>(P.pos + i2)   = make_int2(X[0], X[1]);
         *reinterpret_cast<float2 *>(P.vx + i2)  = v.x;
         *reinterpret_cast<float2 *>(P.vy + i2)  = v.y;
         *reinterpret_cast<float2 *>(P.vz + i2)  = v.z;

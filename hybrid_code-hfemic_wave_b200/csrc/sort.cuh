@@ -52,7 +52,8 @@ inline SortPlan sort_plan(int Nx)
 struct SortKeys {
     uint32_t const     *keys;   // KEYS_ARRAY
     double const       *q1, *w; // KEYS_FP64
-    int32_t const      *cell;   // KEYS_MIXED
+    int32_t const      *pos;    // KEYS_MIXED: fixed-point positions with fbits fraction bits
+    int                 fbits;
     float const        *wf;
     double              full_min;
     int                 Nx;
@@ -82,7 +83,7 @@ __device__ __forceinline__ KeyRaw<KIND> key_load(SortKeys const &s, int64_t i)
     else if constexpr (KIND == KEYS_FP64) // the weight only marks absorbed particles
         return {s.q1[i], s.absorbing ? s.w[i] : 1.0};
     else
-        return {s.cell[i], s.absorbing ? s.wf[i] : 1.0f};
+        return {s.pos[i] >> s.fbits, s.absorbing ? s.wf[i] : 1.0f};
 }
 
 // the key of a loaded item; with `account`, absorbed particles are counted and lost ones flagged
@@ -294,19 +295,19 @@ struct MoveFP64T {
     }
 };
 using MoveFP64 = MoveFP64T<false>;
-// ... or the mixed-precision records (offset, vx, vy, vz, w as FP32, with PSD also real_f and
-// marker; cell, pid)
+// ... or the mixed-precision records (vx, vy, vz, w as FP32, with PSD also real_f and marker;
+// the fixed-point position, pid)
 template <bool PSD>
 struct MoveMixedT {
-    static constexpr int NV   = PSD ? 7 : 5;
+    static constexpr int NV   = PSD ? 6 : 4;
     static constexpr int HOLD = SORT_ITEMS / 2;
     float const         *src[NV];
-    int32_t const       *cell_src, *pid_src;
+    int32_t const       *pos_src, *pid_src;
     float               *dst[NV];
-    int32_t             *cell_dst, *pid_dst;
+    int32_t             *pos_dst, *pid_dst;
     struct Rec {
         float   v[NV];
-        int32_t cell, pid;
+        int32_t pos, pid;
     };
     __device__ __forceinline__ Rec load(uint32_t, uint32_t j) const
     {
@@ -314,8 +315,8 @@ struct MoveMixedT {
 #pragma unroll
         for (int k = 0; k < NV; ++k)
             r.v[k] = src[k][j];
-        r.cell = cell_src[j];
-        r.pid  = pid_src[j];
+        r.pos = pos_src[j];
+        r.pid = pid_src[j];
         return r;
     }
     __device__ __forceinline__ void store(uint32_t pos, Rec const &r) const
@@ -323,8 +324,8 @@ struct MoveMixedT {
 #pragma unroll
         for (int k = 0; k < NV; ++k)
             dst[k][pos] = r.v[k];
-        cell_dst[pos] = r.cell;
-        pid_dst[pos]  = r.pid;
+        pos_dst[pos] = r.pos;
+        pid_dst[pos] = r.pid;
     }
 };
 using MoveMixed = MoveMixedT<false>;

@@ -115,7 +115,7 @@ def _estimate(cfg):
     """The server's admission estimate, restated: particles in two buffer sets with ids and sort
     keys, sort histograms, grids."""
     M = cfg.Nx + 6
-    per = 24 if cfg.precision == h.configs.PREC_MIXED else 40
+    per = 20 if cfg.precision == h.configs.PREC_MIXED else 40
     b = 0
     for k in cfg.kinetic:
         n = k.Nc * cfg.Nx + 64
