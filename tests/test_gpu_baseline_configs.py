@@ -10,13 +10,14 @@ the host; the CUDA path starts from the identical state file.  Three parts:
      fields, sources, moments and particles within 1e-12 (max-norm relative), every particle's
      cell index identical; the mixed-precision path within 1e-4;
   2. the error-growth curve: FP64 after 1, 10, 30 and 100 steps (config 2 with 1/4, config 3 with
-     1/16 of the particles) under bounds that grow with the step count, as round-off differences
-     of the deposit order are amplified by the plasma's dynamics;
+     1/16 of the particles).  The differences are round-off of the deposit summation order; on a
+     B200 they stayed near 1e-14 over the 100 steps (no particle changed cell), so the bounds are
+     1e-12 up to 30 steps and 1e-11 at 100;
   3. the energy time series of EnergyRecorder::dump over config 1's full 1000 steps, every step,
      FP64 and mixed precision, against the reference's own series.
 
 The tolerances of parts 2 and 3 are written next to each check; they are set from the measured
-curves with a margin and stay far below the quantities' own variation over the run.
+curves with a margin of about 100 and stay far below the quantities' own variation over the run.
 """
 import os
 import subprocess
@@ -34,10 +35,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 C1, C2, C3 = "config1_cic_periodic_nx256", "config2_tsc_mirror_nx2048", "config3_cic_periodic_nx4096"
 
 # FP64 max-norm relative error bounds of the growth curve, by step count (part 2)
-GROWTH_FP64 = {1: 1e-12, 10: 1e-10, 30: 1e-9, 100: 1e-7}
+GROWTH_FP64 = {1: 1e-12, 10: 1e-12, 30: 1e-12, 100: 1e-11}
 # part 3: |dB^2/2 (GPU) - dB^2/2 (reference)| / max over the run of dB^2/2 (reference), every step;
 # the same for every particle-energy component relative to its own maximum
-SERIES_FP64, SERIES_MIXED = 1e-6, 1e-3
+SERIES_FP64, SERIES_MIXED = 1e-12, 1e-3
 
 
 def _driver(name):
@@ -120,7 +121,8 @@ def test_energy_series_config1(workdir, gpu_lib):
     ip = _init(workdir, C1, 1)
     init = read_state(ip)
     steps = h.configs.PRESETS[C1]().steps
-    ns = 2  # one kinetic and one cold species
+    ns = 2  # one kinetic and one cold species; columns: dB2O2 (3), dE2O2 (3), then per species
+    # (kinetic first, then cold) its KE_lab (3) followed by its KE_pla (3)
     out = os.path.join(workdir, "c1_series.bin")
     subprocess.run([_driver(C1), "series", ip, "1", str(steps), out], check=True, timeout=900)
     ref = np.fromfile(out).reshape(steps, 6 + 6 * ns)
@@ -138,7 +140,8 @@ def test_energy_series_config1(workdir, gpu_lib):
             for _ in range(steps):
                 g.advance(1)
                 e = g.energy()
-                rows.append(np.concatenate([e["dB2O2"], e["dE2O2"], e["KE_lab"].ravel(), e["KE_pla"].ravel()]))
+                per_species = [np.concatenate([lab, pla]) for lab, pla in zip(e["KE_lab"], e["KE_pla"])]
+                rows.append(np.concatenate([e["dB2O2"], e["dE2O2"], *per_species]))
         rows = np.array(rows)
         err = np.abs(rows[:, :3].sum(axis=1) - wave_ref) / scale
         kin = (np.abs(rows[:, 6:] - kin_ref)[:, cols] / kin_scale[cols]).max(axis=0)
