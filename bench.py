@@ -336,7 +336,8 @@ def precision_name(cfg, h):
 class TimedRun:
     """A run behind the C-ABI with its stream, for device-timed advances."""
 
-    def __init__(self, h, cfg, st):
+    def __init__(self, h, cfg, st, populate_seed=None):
+        """From the host state `st`, or (st None) from the device loader with `populate_seed`."""
         import ctypes
 
         import torch
@@ -349,11 +350,14 @@ class TimedRun:
         lib.h1d_get_stream.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
         lib.h1d_profile_enable.argtypes = [ctypes.c_void_p, ctypes.c_int]
         lib.h1d_profile_read.argtypes = [ctypes.c_void_p, ctypes.POINTER(h.abi.Profile)]
-        self.run.upload_state(st)
+        if st is None:
+            h.abi.populate_state(self.run, populate_seed)
+        else:
+            self.run.upload_state(st)
         sp = ctypes.c_void_p()
         self.run._check(lib.h1d_get_stream(self.run.h, ctypes.byref(sp)))
         self.stream = torch.cuda.ExternalStream(sp.value)
-        self.n_particles = sum(p["q1"].size for p in st["particles"])
+        self.n_particles = cfg.n_particles if st is None else sum(p["q1"].size for p in st["particles"])
 
     def advance(self, n):
         self.run._check(self.lib.h1d_advance_async(self.run.h, n))
@@ -437,8 +441,9 @@ def load_traffic():
 
 
 def error_vs_fp64(h, cfg, st, steps=100):
-    """Max-norm relative error of the mixed run against the FP64 run after `steps` steps from the
-    same state: wave energy (dB^2/2, dE^2/2 per component), particle energies and the moments."""
+    """Max-norm relative error of the mixed run against the FP64 CUDA run after `steps` steps from
+    the same full-size state: wave energy (dB^2/2, dE^2/2 per component), particle energies and
+    the moments."""
     import numpy as np
 
     out = {}
@@ -461,8 +466,67 @@ def error_vs_fp64(h, cfg, st, steps=100):
     for s in range(len(cfg.kinetic)):
         for k, key in enumerate(("n", "nV", "nvv")):
             errs[f"moments[{s}].{key}"] = rel(m1[s][k], m0[s][k])
-    return {"steps": steps, "max": max(errs.values()), "tolerance": 1e-4,
-            "within_tolerance": max(errs.values()) <= 1e-4, "errors": errs}
+    return {"comparator": "the FP64 CUDA path, same full-size state", "steps": steps, "max": max(errs.values()),
+            "tolerance": 1e-4, "within_tolerance": max(errs.values()) <= 1e-4, "errors": errs}
+
+
+def error_vs_reference(h, cfg, divisor=64, every=10):
+    """The CUDA path, mixed precision and FP64, against the reference itself over the
+    configuration's whole length.  The reference binary (oracle/_ref/<name>/ref_driver: the
+    reference's Domain_CAMCL compiled from its sources, FP64 on one host core) loads 1/divisor of
+    the particles with its own loader (PartSpecies::populate(0, divisor)) and records the
+    EnergyRecorder sums (dB^2/2, dE^2/2, and per species KE_lab and KE_pla) every `every` steps
+    for cfg.steps steps; the CUDA path starts from the same state file and records the same sums
+    through h1d_energy.  Errors: the largest |W - W_ref| over the run relative to the largest
+    W_ref, for the wave energy (sum of the six components) and for each particle-energy component
+    (the worst one is reported).  Returns None when the reference binary is absent."""
+    import tempfile
+
+    import numpy as np
+
+    drv = os.path.join(ROOT, "oracle", "_ref", cfg.name, "ref_driver")
+    if not os.path.exists(drv):
+        return None
+    sys.path[:0] = [os.path.join(ROOT, "tests", "golden"), os.path.join(ROOT, "tests")]
+    from parity_util import with_reference_norms
+    from state_io import read_state
+
+    chunks = cfg.steps // every
+    with tempfile.TemporaryDirectory(prefix="h1d_bench_") as tmp:
+        init, series = os.path.join(tmp, "init.bin"), os.path.join(tmp, "series.bin")
+        subprocess.run([drv, "init", init, "0", str(divisor)], check=True, timeout=600, capture_output=True)
+        t0 = time.perf_counter()
+        subprocess.run([drv, "series", init, str(every), str(chunks), series], check=True, timeout=1200,
+                       capture_output=True)
+        ref_s = time.perf_counter() - t0
+        st = read_state(init)
+        ref = np.fromfile(series).reshape(chunks, -1)
+    n = sum(p["q1"].size for p in st["particles"])
+    wave_ref = ref[:, :6].sum(axis=1)
+    kin_ref = ref[:, 6:]
+    kin_scale = np.abs(kin_ref).max(axis=0)
+    cols = kin_scale > 0
+    res = {"comparator": "reference binary (oracle/_ref ref_driver: Domain_CAMCL from the reference sources, "
+                         "FP64, one host core), EnergyRecorder sums",
+           "workload": f"{cfg.name} with 1/{divisor} of the particles ({n}), the reference loader's state",
+           "steps": chunks * every, "every": every, "reference_s": ref_s}
+    for prec, key in ((h.configs.PREC_MIXED, "mixed"), (h.configs.PREC_FP64, "fp64")):
+        rows = []
+        with h.open_run(with_reference_norms(cfg, st).replace(precision=prec)) as r:
+            r.upload_state(st)
+            for _ in range(chunks):
+                r.advance(every)
+                e = r.energy()
+                per_species = [np.concatenate([lab, pla]) for lab, pla in zip(e["KE_lab"], e["KE_pla"])]
+                rows.append(np.concatenate([e["dB2O2"], e["dE2O2"], *per_species]))
+        rows = np.array(rows)
+        wave = np.abs(rows[:, :6].sum(axis=1) - wave_ref) / wave_ref.max()
+        kin = (np.abs(rows[:, 6:] - kin_ref)[:, cols] / kin_scale[cols]).max(axis=1)
+        res[key] = {"wave_energy": float(wave.max()), "particle_energy": float(kin.max()),
+                    "wave_energy_at": {str((i + 1) * every): float(wave[i]) for i in
+                                       sorted({0, chunks // 10, chunks // 2, chunks - 1})}}
+    res["wave_energy_range"] = [float(wave_ref.min()), float(wave_ref.max())]
+    return res
 
 
 def e2e_measure(h, cfg, st, K, world):
@@ -564,9 +628,26 @@ def ensemble_measure(h, precision, steps=500, members=64):
     finally:
         for r in runs:
             r.close()
+    # the same physics as one run: the first Nx=4096 member's plasma holding as many particles as
+    # the whole ensemble, advanced alone (its own autotuned sort interval and CTAs)
+    import dataclasses
+
+    base = next(c for c in cfgs if c.Nx == max(x.Nx for x in cfgs))
+    one = base.replace(kinetic=[dataclasses.replace(base.kinetic[0], Nc=max(1, n_particles // base.Nx))])
+    tr = TimedRun(h, one, None, populate_seed=0)
+    try:
+        tr.warm(4)
+        ms1, _, _ = tr.timed(steps)
+        single = {"workload": f"{base.name} plasma at Nx {base.Nx} with {one.kinetic[0].Nc} particles per cell "
+                              f"({tr.n_particles} particles), alone", "value": tr.n_particles * steps / (ms1 / 1e3),
+                  "autotune": tr.tuned}
+    finally:
+        tr.close()
+    value = n_particles * steps / (ms / 1e3)
     return {"workload": f"ensemble of {members} runs (seeds 0..{members - 1}), {steps} steps each, TSC",
             "precision": "mixed" if precision == h.configs.PREC_MIXED else "fp64",
-            "runs_per_s": members / (ms / 1e3), "value": n_particles * steps / (ms / 1e3), "unit": METRIC,
+            "runs_per_s": members / (ms / 1e3), "value": value, "unit": METRIC,
+            "single_run_same_physics": single, "over_single_run": value / single["value"],
             "ms": ms, "particles": n_particles, "Nx": [c.Nx for c in cfgs][:8] + ["..."],
             "autotune": {"steps": tuned_steps, "sort_interval": k, "ctas_per_sm": ctas},
             "gpu_launches": s1["kernel_launches"] - s0["kernel_launches"],
@@ -689,6 +770,7 @@ def main():
                               "roofline": roofline_of(prof64, "fp64", args.steps, traffic)}
             extras["mixed_over_fp64"] = value / v64
             extras["error_vs_fp64"] = error_vs_fp64(h, cfg, st)
+            extras["error_vs_reference"] = error_vs_reference(h, cfg)
         if cfg.name != "config2_tsc_mirror_nx2048":
             # the FP64 drop-in configuration with the reference's reflecting walls (the parity form)
             # and with the particle-absorbing walls the configuration names (an extension: the
@@ -731,8 +813,16 @@ def main():
     if rank != 0:
         return
     state_mb = n_particles * STATE_BYTES[prec] / 1e6
+    head = {}  # the headline comparisons first, so that a truncated line still carries them
+    if "fp64" in extras:
+        head = {"mixed_over_fp64": extras.pop("mixed_over_fp64"), "fp64_value": extras["fp64"]["value"],
+                "frac": roofline["frac"], "fp64_frac": extras["fp64"]["roofline"]["frac"]}
+    if "drop_in_fp64" in extras:
+        head["drop_in_fp64_frac"] = extras["drop_in_fp64"]["roofline"]["frac"]
+        head["field_ms"] = roofline.get("phase_ms_per_step", {}).get("field")
+        head["drop_in_field_ms"] = extras["drop_in_fp64"]["roofline"].get("phase_ms_per_step", {}).get("field")
     line = {
-        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "metric": METRIC, "value": value, **head, "unit": METRIC, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+i32 particles, f64 fields" if prec == "mixed" else "f64",
         "data": "synthetic (seeded bi-Maxwellian loader)",

@@ -188,6 +188,16 @@ class RunConfig:
                     raise ValueError("invalid domain extent: |xi*D1*q1| >= pi/2")
 
 
+def position_fraction_bits(Nx: int) -> int:
+    """Fraction bits F of the mixed-precision fixed-point position (an int32 holding
+    (q1 - q1min) 2^F): the most bits, at most FP32's 24, that keep (Nx + 2) 2^F within 2^31.  A
+    position is stored to the nearest 2^-F cell."""
+    f = 24
+    while f > 0 and (Nx + 2) << f > 1 << 31:
+        f -= 1
+    return f
+
+
 def _int_cos_zeta(zeta: int, a: float, x: float, small_a: bool) -> float:
     """int_0^x cos^zeta(a t) dt by the recurrence of VDFHelper.h:125-147 (zeta - 2 -> zeta)."""
     ax = a * x

@@ -15,6 +15,7 @@
 #include <cmath>
 #include <deque>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <cstdarg>
 #include <cstdio>
@@ -62,8 +63,6 @@ struct SpeciesState {
     bool     upload_order = false; // the particles are still in the order of their upload
     // sort scratch
     uint32_t *keys[2] = {}, *idx[2] = {};
-    uint32_t *hist = nullptr, *part = nullptr;
-    int64_t   hist_cap = 0, part_cap = 0;
     unsigned long long *dead = nullptr;
     int       since_sort = 1 << 30;
     // deposits [set][deposit][q] -> M doubles each, contiguous
@@ -74,6 +73,17 @@ struct SpeciesState {
     double *mom = nullptr;
     // delta-f: equilibrium moments n0 (M) and nvv0 (6M) on the half grid, ghosts zero
     double *eq = nullptr;
+};
+
+// histogram and scan partials of the cell sort, grown to the largest launch set sorted so far
+struct SortScratch {
+    uint32_t *hist = nullptr, *part = nullptr;
+    int64_t   hist_cap = 0, part_cap = 0;
+    void      release()
+    {
+        cudaFree(hist), cudaFree(part);
+        hist = part = nullptr, hist_cap = part_cap = 0;
+    }
 };
 
 struct ColdState {
@@ -105,6 +115,7 @@ struct h1d_run {
     int          fcur = 0; // field parity
     int          dset = 0; // deposit set parity
     SpeciesState sp[H1D_MAX_KINETIC];
+    SortScratch  sorter;
     ColdState    cold[H1D_MAX_COLD];
     unsigned    *d_status = nullptr;
     unsigned long long *d_fallbacks = nullptr;
@@ -561,119 +572,249 @@ int launch_push(h1d_run *run, int s, PushArgs const &a)
     return H1D_OK;
 }
 
-// stable cell sort of species s (sort.cuh)
-int sort_species(h1d_run *run, int s)
+// ---- cell sort (sort.cuh): the species of one run, or of every member of an ensemble, sorted
+// together, one launch per kernel for up to SORT_SEGS species ----
+constexpr int      SORT_SEGS    = 64;
+constexpr uint64_t SORT_SET_MAX = 0xffffffffull; // particles of one launch set (32-bit places)
+
+struct SortItem {
+    h1d_run *run;
+    int      s;
+};
+
+bool has_psd(SpeciesState const &S) { return S.psd[0][0] != nullptr || S.fpsd[0][0] != nullptr; }
+
+cudaError_t grow(uint32_t *&buf, int64_t &cap, int64_t need)
 {
-    SpeciesState &S = run->sp[s];
-    S.since_sort    = 0;
-    S.upload_order  = false;
-    if (S.n == 0)
-        return H1D_OK;
-    cudaStream_t const st     = run->stream;
-    int const          Nx     = static_cast<int>(run->Nx);
-    SortPlan const     plan   = sort_plan(Nx);
-    int64_t const      ntiles = (S.n + SORT_TILE - 1) / SORT_TILE;
-    int64_t const      hlen   = (int64_t{1} << std::max(plan.bits[0], plan.bits[1])) * ntiles;
-    int64_t const      nparts = (hlen + SCAN_SEG - 1) / SCAN_SEG;
-    if (hlen > S.hist_cap) {
-        cudaFree(S.hist);
-        S.hist = nullptr;
-        CU(cudaMalloc(&S.hist, sizeof(uint32_t) * hlen));
-        S.hist_cap = hlen;
-    }
-    if (nparts > S.part_cap) {
-        cudaFree(S.part);
-        S.part = nullptr;
-        CU(cudaMalloc(&S.part, sizeof(uint32_t) * nparts));
-        S.part_cap = nparts;
-    }
-    phase_begin(run, 1);
-    CU(cudaMemsetAsync(S.dead, 0, sizeof(unsigned long long), st));
-    unsigned const nt = static_cast<unsigned>(ntiles);
-    int const      ti = static_cast<int>(ntiles);
-    SortKeys       first{};
-    first.full_min = -0.5 * Nx, first.Nx = Nx, first.dead = S.dead, first.status = run->d_status;
-    first.absorbing = run->p.particle_bc == H1D_BC_ABSORBING;
-    if (run->mixed)
-        first.pos = S.pos[S.cur], first.fbits = run->fbits, first.wf = S.fbuf[S.cur][3];
-    else
-        first.q1 = S.buf[S.cur][0], first.w = S.buf[S.cur][4];
-    MoveMixed         mm{};
-    MoveMixedT<true>  mq{};
-    MoveFP64          md{};
-    MoveFP64T<true>   mp{};
-    bool const        psd = S.psd[0][0] != nullptr || S.fpsd[0][0] != nullptr;
+    if (need <= cap)
+        return cudaSuccess;
+    cudaFree(buf);
+    buf = nullptr, cap = 0;
+    cudaError_t const e = cudaMalloc(&buf, sizeof(uint32_t) * need);
+    if (e == cudaSuccess)
+        cap = need;
+    return e;
+}
+
+template <bool PSD>
+void fill_move(MoveFP64T<PSD> &m, SpeciesState const &P)
+{
     for (int k = 0; k < 5; ++k)
-        md.src[k] = mp.src[k] = S.buf[S.cur][k], md.dst[k] = mp.dst[k] = S.buf[1 - S.cur][k];
-    for (int k = 0; k < 4; ++k) {
-        mm.src[k] = S.fbuf[S.cur][k], mm.dst[k] = S.fbuf[1 - S.cur][k];
-        mq.src[k] = S.fbuf[S.cur][k], mq.dst[k] = S.fbuf[1 - S.cur][k];
+        m.src[k] = P.buf[P.cur][k], m.dst[k] = P.buf[1 - P.cur][k];
+    if constexpr (PSD)
+        for (int k = 0; k < 2; ++k)
+            m.src[5 + k] = P.psd[P.cur][k], m.dst[5 + k] = P.psd[1 - P.cur][k];
+    m.pid_src = P.pid[P.cur], m.pid_dst = P.pid[1 - P.cur];
+}
+template <bool PSD>
+void fill_move(MoveMixedT<PSD> &m, SpeciesState const &P)
+{
+    for (int k = 0; k < 4; ++k)
+        m.src[k] = P.fbuf[P.cur][k], m.dst[k] = P.fbuf[1 - P.cur][k];
+    if constexpr (PSD)
+        for (int k = 0; k < 2; ++k)
+            m.src[4 + k] = P.fpsd[P.cur][k], m.dst[4 + k] = P.fpsd[1 - P.cur][k];
+    m.pos_src = P.pos[P.cur], m.pos_dst = P.pos[1 - P.cur];
+    m.pid_src = P.pid[P.cur], m.pid_dst = P.pid[1 - P.cur];
+}
+
+// the last pass: the particle records of every segment move to their places
+template <int KIND, class Move, int MAXS>
+cudaError_t scatter_records(SortSegs<MAXS> const &S, SortItem const *it, int shift, unsigned mask,
+                            uint32_t const *offsets, unsigned nt, cudaStream_t st)
+{
+    std::unique_ptr<MoveSegs<Move, MAXS>> M(new (std::nothrow) MoveSegs<Move, MAXS>{});
+    if (!M)
+        return cudaErrorMemoryAllocation;
+    for (int g = 0; g < S.n; ++g)
+        fill_move(M->mv[g], it[g].run->sp[it[g].s]);
+    scatter_kernel<KIND, Move, MAXS><<<nt, SORT_THREADS, 0, st>>>(S, *M, shift, mask, offsets);
+    return cudaGetLastError();
+}
+template <int KIND, int MAXS>
+cudaError_t scatter_records(SortSegs<MAXS> const &S, SortItem const *it, bool mixed, bool psd, int shift,
+                            unsigned mask, uint32_t const *offsets, unsigned nt, cudaStream_t st)
+{
+    if (mixed)
+        return psd ? scatter_records<KIND, MoveMixedT<true>>(S, it, shift, mask, offsets, nt, st)
+                   : scatter_records<KIND, MoveMixedT<false>>(S, it, shift, mask, offsets, nt, st);
+    return psd ? scatter_records<KIND, MoveFP64T<true>>(S, it, shift, mask, offsets, nt, st)
+               : scatter_records<KIND, MoveFP64T<false>>(S, it, shift, mask, offsets, nt, st);
+}
+
+// one launch set: m non-empty species of one precision and one PSD kind, fewer than 2^32
+// particles in all; sorts them into their other parity buffers (the caller flips `cur`)
+template <int MAXS>
+cudaError_t sort_set(SortItem const *it, int m, SortScratch &sc, cudaStream_t st, int64_t &launches)
+{
+    std::unique_ptr<SortSegs<MAXS>> S(new (std::nothrow) SortSegs<MAXS>{});
+    if (!S)
+        return cudaErrorMemoryAllocation;
+    bool const mixed = it[0].run->mixed;
+    bool const psd   = has_psd(it[0].run->sp[it[0].s]);
+    int        Nx    = 1;
+    int64_t    tiles = 0, first = 0;
+    S->n             = m;
+    for (int g = 0; g < m; ++g) {
+        h1d_run *const      r = it[g].run;
+        SpeciesState const &P = r->sp[it[g].s];
+        S->tile0[g]           = static_cast<int>(tiles);
+        S->first[g]           = static_cast<uint32_t>(first);
+        S->count[g]           = static_cast<uint32_t>(P.n);
+        tiles += (P.n + SORT_TILE - 1) / SORT_TILE;
+        first += P.n;
+        SortKeys &k = S->key[g];
+        k.full_min = -0.5 * static_cast<double>(r->Nx), k.Nx = static_cast<int>(r->Nx);
+        k.dead = P.dead, k.status = r->d_status, k.absorbing = r->p.particle_bc == H1D_BC_ABSORBING;
+        if (mixed)
+            k.pos = P.pos[P.cur], k.fbits = r->fbits, k.wf = P.fbuf[P.cur][3];
+        else
+            k.q1 = P.buf[P.cur][0], k.w = P.buf[P.cur][4];
+        if (k.absorbing) { // absorbed particles are counted by the first histogram
+            cudaError_t const e = cudaMemsetAsync(P.dead, 0, sizeof(unsigned long long), st);
+            if (e != cudaSuccess)
+                return e;
+        }
+        Nx = std::max(Nx, k.Nx);
     }
-    for (int k = 0; k < 2; ++k) {
-        mp.src[5 + k] = S.psd[S.cur][k], mp.dst[5 + k] = S.psd[1 - S.cur][k];
-        mq.src[4 + k] = S.fpsd[S.cur][k], mq.dst[4 + k] = S.fpsd[1 - S.cur][k];
-    }
-    mq.pos_src = S.pos[S.cur], mq.pos_dst = S.pos[1 - S.cur];
-    mq.pid_src = S.pid[S.cur], mq.pid_dst = S.pid[1 - S.cur];
-    mm.pos_src = S.pos[S.cur], mm.pos_dst = S.pos[1 - S.cur];
-    mm.pid_src = md.pid_src = mp.pid_src = S.pid[S.cur];
-    mm.pid_dst = md.pid_dst = mp.pid_dst = S.pid[1 - S.cur];
-    int shift = 0, src = 0; // keys/idx buffer the current pass reads (the first pass reads the particles)
+    S->tile0[m]          = static_cast<int>(tiles);
+    SortPlan const plan  = sort_plan(Nx); // the widest grid's digits serve every segment
+    int64_t const  hlen  = (int64_t{1} << std::max(plan.bits[0], plan.bits[1])) * tiles;
+    cudaError_t    e     = grow(sc.hist, sc.hist_cap, hlen);
+    if (e == cudaSuccess)
+        e = grow(sc.part, sc.part_cap, (hlen + SCAN_SEG - 1) / SCAN_SEG);
+    if (e != cudaSuccess)
+        return e;
+    unsigned const nt    = static_cast<unsigned>(tiles);
+    int            shift = 0, src = 0; // keys/idx buffer the current pass reads (the first pass reads the particles)
     for (int pass = 0; pass < plan.passes; ++pass) {
         unsigned const mask = (1u << plan.bits[pass]) - 1u;
-        int64_t const  len  = static_cast<int64_t>(mask + 1) * ntiles;
+        int64_t const  len  = static_cast<int64_t>(mask + 1) * tiles;
         unsigned const np   = static_cast<unsigned>((len + SCAN_SEG - 1) / SCAN_SEG);
         bool const     last = pass == plan.passes - 1;
-        SortKeys       keys = first;
-        keys.keys           = S.keys[src];
+        for (int g = 0; g < m; ++g) {
+            SpeciesState const &P = it[g].run->sp[it[g].s];
+            S->key[g].keys        = P.keys[src];
+            S->idx_in[g]          = P.idx[src];
+        }
         if (pass > 0)
-            hist_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, S.n, shift, mask, ti, S.hist);
-        else if (run->mixed)
-            hist_kernel<KEYS_MIXED><<<nt, SORT_THREADS, 0, st>>>(keys, S.n, shift, mask, ti, S.hist);
+            hist_kernel<KEYS_ARRAY, MAXS><<<nt, SORT_THREADS, 0, st>>>(*S, shift, mask, sc.hist);
+        else if (mixed)
+            hist_kernel<KEYS_MIXED, MAXS><<<nt, SORT_THREADS, 0, st>>>(*S, shift, mask, sc.hist);
         else
-            hist_kernel<KEYS_FP64><<<nt, SORT_THREADS, 0, st>>>(keys, S.n, shift, mask, ti, S.hist);
-        scan_reduce_kernel<<<np, SCAN_THREADS, 0, st>>>(S.hist, len, S.part);
-        scan_partials_kernel<<<1, 1024, 0, st>>>(S.part, static_cast<int>(np));
-        scan_down_kernel<<<np, SCAN_THREADS, 0, st>>>(S.hist, len, S.part);
-        MoveKeys const mk{S.keys[1 - src], S.idx[1 - src]};
-        uint32_t const *idx = S.idx[src];
-        if (pass > 0 && !last)
-            scatter_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mk);
-        else if (pass > 0 && run->mixed && psd)
-            scatter_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mq);
-        else if (pass > 0 && run->mixed)
-            scatter_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mm);
-        else if (pass > 0 && psd)
-            scatter_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mp);
-        else if (pass > 0)
-            scatter_kernel<KEYS_ARRAY><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, md);
-        else if (run->mixed && !last)
-            scatter_kernel<KEYS_MIXED><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mk);
-        else if (run->mixed && psd)
-            scatter_kernel<KEYS_MIXED><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mq);
-        else if (run->mixed)
-            scatter_kernel<KEYS_MIXED><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mm);
-        else if (!last)
-            scatter_kernel<KEYS_FP64><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mk);
-        else if (psd)
-            scatter_kernel<KEYS_FP64><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, mp);
-        else
-            scatter_kernel<KEYS_FP64><<<nt, SORT_THREADS, 0, st>>>(keys, idx, S.n, shift, mask, ti, S.hist, md);
+            hist_kernel<KEYS_FP64, MAXS><<<nt, SORT_THREADS, 0, st>>>(*S, shift, mask, sc.hist);
+        scan_reduce_kernel<<<np, SCAN_THREADS, 0, st>>>(sc.hist, len, sc.part);
+        scan_partials_kernel<<<1, 1024, 0, st>>>(sc.part, static_cast<int>(np));
+        scan_down_kernel<<<np, SCAN_THREADS, 0, st>>>(sc.hist, len, sc.part);
+        if (!last) { // (key, index) pairs for the next pass
+            std::unique_ptr<MoveSegs<MoveKeys, MAXS>> K(new (std::nothrow) MoveSegs<MoveKeys, MAXS>{});
+            if (!K)
+                return cudaErrorMemoryAllocation;
+            for (int g = 0; g < m; ++g) {
+                SpeciesState const &P = it[g].run->sp[it[g].s];
+                K->mv[g]              = MoveKeys{ P.keys[1 - src], P.idx[1 - src] };
+            }
+            if (pass > 0)
+                scatter_kernel<KEYS_ARRAY, MoveKeys, MAXS><<<nt, SORT_THREADS, 0, st>>>(*S, *K, shift, mask, sc.hist);
+            else if (mixed)
+                scatter_kernel<KEYS_MIXED, MoveKeys, MAXS><<<nt, SORT_THREADS, 0, st>>>(*S, *K, shift, mask, sc.hist);
+            else
+                scatter_kernel<KEYS_FP64, MoveKeys, MAXS><<<nt, SORT_THREADS, 0, st>>>(*S, *K, shift, mask, sc.hist);
+            e = cudaGetLastError();
+        } else if (pass > 0) {
+            e = scatter_records<KEYS_ARRAY>(*S, it, mixed, psd, shift, mask, sc.hist, nt, st);
+        } else if (mixed) {
+            e = scatter_records<KEYS_MIXED>(*S, it, mixed, psd, shift, mask, sc.hist, nt, st);
+        } else {
+            e = scatter_records<KEYS_FP64>(*S, it, mixed, psd, shift, mask, sc.hist, nt, st);
+        }
+        if (e != cudaSuccess)
+            return e;
         shift += plan.bits[pass];
         src = 1 - src;
     }
-    CU(cudaGetLastError());
-    phase_end(run, 5 * plan.passes);
-    S.cur = 1 - S.cur;
-    if (run->p.particle_bc == H1D_BC_ABSORBING) { // trim removed particles (sorted to the end)
-        unsigned long long dead = 0;
-        CU(cudaMemcpyAsync(&dead, S.dead, sizeof dead, cudaMemcpyDeviceToHost, st));
-        CU(cudaStreamSynchronize(st));
-        S.n -= static_cast<int64_t>(dead);
-        if (dead)
-            run->gen++;
+    launches += 5 * plan.passes;
+    return cudaGetLastError();
+}
+
+// sorts the listed species (any runs, any mix of precisions) in as few launch sets as their
+// kinds allow; under the absorbing boundary the absorbed particles are then trimmed (one host
+// synchronisation for all of them)
+cudaError_t sort_items(std::vector<SortItem> const &items, SortScratch &sc, cudaStream_t st, int64_t &launches)
+{
+    std::vector<SortItem> todo;
+    bool                  absorbing = false;
+    for (SortItem const &x : items) {
+        SpeciesState &P = x.run->sp[x.s];
+        P.since_sort    = 0;
+        P.upload_order  = false;
+        if (P.n > 0)
+            todo.push_back(x), absorbing |= x.run->p.particle_bc == H1D_BC_ABSORBING;
     }
+    for (int kind = 0; kind < 4; ++kind) { // (mixed, psd) kinds, in turn
+        std::vector<SortItem> set;
+        uint64_t              total = 0;
+        auto const            flush = [&]() -> cudaError_t {
+            if (set.empty())
+                return cudaSuccess;
+            cudaError_t const e = set.size() == 1 ? sort_set<1>(set.data(), 1, sc, st, launches)
+                                                  : sort_set<SORT_SEGS>(set.data(), static_cast<int>(set.size()), sc, st, launches);
+            set.clear(), total = 0;
+            return e;
+        };
+        for (SortItem const &x : todo) {
+            SpeciesState const &P = x.run->sp[x.s];
+            if ((x.run->mixed ? 2 : 0) + (has_psd(P) ? 1 : 0) != kind)
+                continue;
+            if (set.size() == SORT_SEGS || total + static_cast<uint64_t>(P.n) > SORT_SET_MAX)
+                if (cudaError_t const e = flush())
+                    return e;
+            set.push_back(x), total += static_cast<uint64_t>(P.n);
+        }
+        if (cudaError_t const e = flush())
+            return e;
+    }
+    for (SortItem const &x : todo)
+        x.run->sp[x.s].cur ^= 1;
+    if (!absorbing)
+        return cudaSuccess;
+    std::vector<unsigned long long> dead(todo.size(), 0);
+    for (size_t i = 0; i < todo.size(); ++i)
+        if (todo[i].run->p.particle_bc == H1D_BC_ABSORBING)
+            if (cudaError_t const e = cudaMemcpyAsync(&dead[i], todo[i].run->sp[todo[i].s].dead, sizeof(unsigned long long),
+                                                      cudaMemcpyDeviceToHost, st))
+                return e;
+    if (cudaError_t const e = cudaStreamSynchronize(st))
+        return e;
+    for (size_t i = 0; i < todo.size(); ++i) // removed particles were sorted to the end
+        if (dead[i]) {
+            todo[i].run->sp[todo[i].s].n -= static_cast<int64_t>(dead[i]);
+            todo[i].run->gen++;
+        }
+    return cudaSuccess;
+}
+
+// stable cell sort of the listed species of one run
+int sort_run(h1d_run *run, std::vector<SortItem> const &items)
+{
+    if (items.empty())
+        return H1D_OK;
+    int64_t launches = 0;
+    phase_begin(run, 1);
+    CU(sort_items(items, run->sorter, run->stream, launches));
+    phase_end(run, static_cast<int>(launches));
     return H1D_OK;
+}
+int sort_species(h1d_run *run, int s) { return sort_run(run, { SortItem{ run, s } }); }
+
+// the species of the run whose sort interval is up, sorted together
+int sort_due(h1d_run *run)
+{
+    std::vector<SortItem> due;
+    for (int s = 0; s < run->p.n_kinetic; ++s)
+        if (run->sp[s].since_sort >= run->sort_interval)
+            due.push_back({ run, s });
+    return sort_run(run, due);
 }
 
 FieldArgs field_args(h1d_run *run)
@@ -802,9 +943,7 @@ int push_run(h1d_run *run, ArgsOf const &args_of)
 int camcl_step(h1d_run *run)
 {
     h1d_params const &p = run->p;
-    for (int s = 0; s < p.n_kinetic; ++s)
-        if (run->sp[s].since_sort >= run->sort_interval)
-            TRY(sort_species(run, s));
+    TRY(sort_due(run));
     TRY(push_run(run, [run](int s) { return push_args(run, s); }));
     for (int s = 0; s < p.n_kinetic; ++s) {
         if (run->profiling)
@@ -876,9 +1015,8 @@ PushArgs pc_pass_args(h1d_run *run, int s, int pass, int dep_set)
 
 int pc_particles(h1d_run *run, int pass, int dep_set) // pass 0 predictor, 1 corrector, 2 initial deposit
 {
-    for (int s = 0; s < run->p.n_kinetic; ++s)
-        if (pass != 2 && run->sp[s].since_sort >= run->sort_interval)
-            TRY(sort_species(run, s));
+    if (pass != 2)
+        TRY(sort_due(run));
     TRY(push_run(run, [&](int s) { return pc_pass_args(run, s, pass, dep_set); }));
     for (int s = 0; s < run->p.n_kinetic; ++s) {
         if (run->profiling)
@@ -946,12 +1084,15 @@ int finalize_moments(h1d_run *run)
     if (!run->moments_stale)
         return H1D_OK;
     h1d_params const &p = run->p;
+    // particles that drifted since their last sort are sorted first: a warp's particles then
+    // share a few cells and collect_all accumulates in registers (the next steps gain too)
+    std::vector<SortItem> drifted;
+    for (int s = 0; s < p.n_kinetic; ++s)
+        if (run->sp[s].n > 0 && run->sp[s].since_sort > 0)
+            drifted.push_back({ run, s });
+    TRY(sort_run(run, drifted));
     for (int s = 0; s < p.n_kinetic; ++s) {
         SpeciesState &S = run->sp[s];
-        // particles that drifted since their last sort are sorted first: a warp's particles then
-        // share a few cells and collect_all accumulates in registers (the next steps gain too)
-        if (S.n > 0 && S.since_sort > 0)
-            TRY(sort_species(run, s));
         CU(cudaMemsetAsync(S.mom_raw, 0, sizeof(double) * 10 * run->M, run->stream));
         if (S.n > 0 && run->mixed) {
             MomentArgsMixed a{};
@@ -1112,6 +1253,7 @@ struct h1d_batch {
     int                        L = 0, nblocks = 0;
     size_t                     smem = 0;
     bool                       pc = false;        // predictor-corrector members (else CAM-CL)
+    SortScratch                sorter;            // the members' cell sort
     FieldArgs                 *d_table = nullptr; // CAM-CL: [parity][runs]; PC: [phase 1-3][parity][runs]
     FieldBlock                *d_map = nullptr;
     int                        parity = 0;
@@ -1242,15 +1384,16 @@ int build_field_tables(h1d_batch *b)
     return H1D_OK;
 }
 
-// sort every group at the start of a block of b->k steps
+// sort every species of every member at the start of a block of b->k steps, all of them in one
+// launch set per kind (precision, evolving weights) of up to SORT_SEGS species
 int batch_sort_block(h1d_batch *b)
 {
     if (b->since_block >= b->k) {
+        std::vector<SortItem> items;
         for (h1d_run *r : b->runs)
-            for (int s = 0; s < r->p.n_kinetic; ++s) {
-                BTRY(r, sort_species(r, s));
-                b->stats.kernel_launches += r->sp[s].n > 0 ? 5 * sort_plan(static_cast<int>(r->Nx)).passes : 0;
-            }
+            for (int s = 0; s < r->p.n_kinetic; ++s)
+                items.push_back({ r, s });
+        BCU(sort_items(items, b->sorter, b->stream, b->stats.kernel_launches));
         b->since_block = 0;
     }
     return H1D_OK;
@@ -1724,6 +1867,7 @@ int h1d_destroy(h1d_run *run)
     cudaFree(run->d_fallbacks);
     cudaFree(run->EB), cudaFree(run->EBf), cudaFree(run->src_dep), cudaFree(run->charge), cudaFree(run->current), cudaFree(run->d_status), cudaFree(run->d_energy);
     cudaFree(run->stage);
+    run->sorter.release();
     if (run->h_status)
         cudaFreeHost(run->h_status);
     for (auto &S : run->sp) {
@@ -1737,7 +1881,7 @@ int h1d_destroy(h1d_run *run)
             cudaFree(S.psd[k][0]), cudaFree(S.psd[k][1]);
             cudaFree(S.fpsd[k][0]), cudaFree(S.fpsd[k][1]);
         }
-        cudaFree(S.hist), cudaFree(S.part), cudaFree(S.dead), cudaFree(S.dep), cudaFree(S.mom_raw), cudaFree(S.mom);
+        cudaFree(S.dead), cudaFree(S.dep), cudaFree(S.mom_raw), cudaFree(S.mom);
         cudaFree(S.eq);
     }
     for (auto &C : run->cold)
@@ -2178,6 +2322,7 @@ int h1d_batch_destroy(h1d_batch *b)
     }
     drop_graph(b);
     cudaFree(b->d_table), cudaFree(b->d_map);
+    b->sorter.release();
     cudaStreamDestroy(b->stream);
     delete b;
     return H1D_OK;

@@ -21,6 +21,14 @@
 // The first pass reads the keys straight from the particles and counts absorbed particles; the
 // last pass moves the particle records themselves (no separate index array and gather).  Each
 // thread issues all of its loads before it ranks, so a warp keeps 8 loads in flight.
+//
+// One launch of each kernel sorts a whole set of particle segments -- the species of one run, or
+// of every member of an ensemble -- each in its own buffers.  Segment g owns the tiles
+// [tile0[g], tile0[g+1]) and the histogram rows [(radix) * tile0[g], (radix) * tile0[g+1]), so a
+// single exclusive scan over the whole histogram yields each item's place in the concatenation of
+// the sorted segments; subtracting first[g] (the particles of the earlier segments) gives its
+// place in its own segment.  Sorting by (segment, key) this way costs the same launches for 64
+// members as for one.
 #pragma once
 
 #include "device_common.cuh"
@@ -62,6 +70,43 @@ struct SortKeys {
     unsigned           *status;
 };
 enum { KEYS_ARRAY = 0, KEYS_FP64 = 1, KEYS_MIXED = 2 };
+
+// the segments of one launch set (kernel parameter; MAXS == 1 makes them launch constants)
+template <int MAXS>
+struct SortSegs {
+    static constexpr int MAX = MAXS;
+    int                  n;                // segments, none of them empty
+    int                  tile0[MAXS + 1];  // first tile of each segment; tile0[n] = all tiles
+    uint32_t             first[MAXS];      // particles of the earlier segments (sum < 2^32)
+    uint32_t             count[MAXS];      // particles of each segment
+    SortKeys             key[MAXS];
+    uint32_t const      *idx_in[MAXS];     // KEYS_ARRAY passes: the particle index of each key
+};
+
+// the segment that owns tile t: the last g with tile0[g] <= t
+template <int MAXS>
+__device__ __forceinline__ int seg_of(SortSegs<MAXS> const &S, int t)
+{
+    if constexpr (MAXS == 1) {
+        return 0;
+    } else {
+        int lo = 0, hi = S.n - 1;
+        while (lo < hi) {
+            int const mid = (lo + hi + 1) >> 1;
+            if (S.tile0[mid] <= t)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        return lo;
+    }
+}
+
+// where the scatter of each segment writes
+template <class Move, int MAXS>
+struct MoveSegs {
+    Move mv[MAXS];
+};
 
 template <int KIND> struct KeyRaw;
 template <> struct KeyRaw<KEYS_ARRAY> {
@@ -119,19 +164,25 @@ __device__ __forceinline__ uint32_t key_of(SortKeys const &s, KeyRaw<KIND> const
 
 // warp w of a tile owns items [w0, w0 + 256); round r of lane l is item w0 + 32 r + l, so the
 // rounds visit the warp's items in index order
-__device__ __forceinline__ int64_t sort_warp_base()
+__device__ __forceinline__ int64_t sort_warp_base(int tile)
 {
-    return static_cast<int64_t>(blockIdx.x) * SORT_TILE + (threadIdx.x >> 5) * 32 * SORT_ITEMS;
+    return static_cast<int64_t>(tile) * SORT_TILE + (threadIdx.x >> 5) * 32 * SORT_ITEMS;
 }
 
-template <int KIND>
+// hist[(mask + 1) * tile0[g] + digit * ntiles(g) + tile]: each segment's rows digit-major
+template <int KIND, int MAXS>
 __global__ void __launch_bounds__(SORT_THREADS)
-    hist_kernel(SortKeys s, int64_t n, int shift, unsigned mask, int ntiles, uint32_t *hist)
+    hist_kernel(SortSegs<MAXS> const __grid_constant__ S, int shift, unsigned mask, uint32_t *hist)
 {
     __shared__ uint32_t h[256];
-    h[threadIdx.x] = 0;
-    int const     lane = threadIdx.x & 31;
-    int64_t const w0   = sort_warp_base();
+    h[threadIdx.x]          = 0;
+    int const       g       = seg_of(S, static_cast<int>(blockIdx.x));
+    int const       tile    = static_cast<int>(blockIdx.x) - S.tile0[g];
+    int const       ntiles  = S.tile0[g + 1] - S.tile0[g];
+    int64_t const   n       = S.count[g];
+    SortKeys const &s       = S.key[g];
+    int const       lane    = threadIdx.x & 31;
+    int64_t const   w0      = sort_warp_base(tile);
     KeyRaw<KIND>  raw[SORT_ITEMS];
 #pragma unroll
     for (int r = 0; r < SORT_ITEMS; ++r) {
@@ -150,7 +201,8 @@ __global__ void __launch_bounds__(SORT_THREADS)
     }
     __syncthreads();
     if (threadIdx.x <= mask)
-        hist[static_cast<int64_t>(threadIdx.x) * ntiles + blockIdx.x] = h[threadIdx.x];
+        hist[static_cast<int64_t>(mask + 1) * S.tile0[g] + static_cast<int64_t>(threadIdx.x) * ntiles + tile] =
+            h[threadIdx.x];
 }
 
 // block-wide exclusive scan of one value per thread; returns the block total
@@ -330,15 +382,22 @@ struct MoveMixedT {
 };
 using MoveMixed = MoveMixedT<false>;
 
-template <int KIND, class Move>
+template <int KIND, class Move, int MAXS>
 __global__ void __launch_bounds__(SORT_THREADS)
-    scatter_kernel(SortKeys s, uint32_t const *idx_in, int64_t n, int shift, unsigned mask, int ntiles,
-                   uint32_t const *offsets, Move const mv)
+    scatter_kernel(SortSegs<MAXS> const __grid_constant__ S, MoveSegs<Move, MAXS> const __grid_constant__ M,
+                   int shift, unsigned mask, uint32_t const *offsets)
 {
     constexpr int       NW = SORT_THREADS / 32;
     __shared__ uint32_t cnt[NW][256]; // per-warp digit counts, then each warp's start per digit
+    int const           g      = seg_of(S, static_cast<int>(blockIdx.x));
+    int const           tile   = static_cast<int>(blockIdx.x) - S.tile0[g];
+    int const           ntiles = S.tile0[g + 1] - S.tile0[g];
+    int64_t const       n      = S.count[g];
+    SortKeys const     &s      = S.key[g];
+    uint32_t const     *idx_in = S.idx_in[g];
+    Move const         &mv     = M.mv[g];
     int const           lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    int64_t const       w0   = sort_warp_base();
+    int64_t const       w0   = sort_warp_base(tile);
     unsigned const      lt   = (1u << lane) - 1u;
     KeyRaw<KIND>        raw[SORT_ITEMS];
     uint32_t            key[SORT_ITEMS], id[SORT_ITEMS], dig[SORT_ITEMS], rank[SORT_ITEMS];
@@ -378,8 +437,10 @@ __global__ void __launch_bounds__(SORT_THREADS)
         if (w0 + r * 32 + lane < n)
             rec[r] = mv.load(key[r], id[r]);
     __syncthreads();
-    if (threadIdx.x <= mask) { // digit threadIdx.x: the tile's global start plus the earlier warps
-        uint32_t run = offsets[static_cast<int64_t>(threadIdx.x) * ntiles + blockIdx.x];
+    if (threadIdx.x <= mask) { // digit threadIdx.x: the tile's start in its segment plus the earlier warps
+        uint32_t run = offsets[static_cast<int64_t>(mask + 1) * S.tile0[g] + static_cast<int64_t>(threadIdx.x) * ntiles +
+                               tile] -
+                       S.first[g];
 #pragma unroll
         for (int w = 0; w < NW; ++w) {
             uint32_t const c    = cnt[w][threadIdx.x];

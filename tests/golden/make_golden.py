@@ -8,9 +8,9 @@ place, one binary per configuration) and, for every parity configuration, writes
                        and the initial fields
     <name>.step1.bin   after Domain::advance_by(1)
     <name>.step10.bin  after Domain::advance_by(10) from the same initial state
-into tests/golden/.  Needs the reference tree (default /root/reference, or $H1D_REFERENCE).
+into tests/golden/.  Needs the reference tree, given as the argument or as $H1D_REFERENCE.
 
-usage: python tests/golden/make_golden.py
+usage: python tests/golden/make_golden.py [<reference tree>]
 """
 import os
 import shutil
@@ -26,7 +26,9 @@ NAMES = ["p1_cic_periodic", "p2_tsc_mirror_reflecting", "p3_o3_adiabatic_periodi
 
 
 def main():
-    ref = os.environ.get("H1D_REFERENCE", "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("H1D_REFERENCE")
+    if not ref or not os.path.isdir(ref):
+        sys.exit("make_golden.py: give the reference tree as the argument or as $H1D_REFERENCE")
     subprocess.check_call(["make", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={ref}",
                            f"PYTHON={sys.executable}", "-j8"])
     with tempfile.TemporaryDirectory() as tmp:
