@@ -149,12 +149,6 @@ static __device__ SV smooth_n(Cell const &C, int n, double *a, double *v, double
     return { a, v };
 }
 
-// the half-grid geometry and masking factors of one cell, as Ohm's law needs them (a Cell has them
-// too, so the helpers below take either)
-struct HalfGeo {
-    double hcx, hcy, hcz, hnx, hny, hnz, mp1, mp2, ma1, ma2;
-};
-
 __device__ __forceinline__ d3 covar_full(Cell const &C, d3 b) { return { C.fcx * b.x, C.fcy * b.y, C.fcz * b.z }; }
 __device__ __forceinline__ d3 contr_full(Cell const &C, d3 b) { return { C.fnx * b.x, C.fny * b.y, C.fnz * b.z }; }
 template <class G>
@@ -425,31 +419,29 @@ __device__ __forceinline__ double fold_staged(FieldArgs const &a, Cell const &C,
     return v;
 }
 
-// nsm[j] smoothings of item j's arrays (a, v) for every j < n together, ping-ponging with (ta, tv);
-// with_scalar = false smooths the vectors only.  Item j's result is in (a, v) when nsm[j] is even
-// and in (ta, tv) when it is odd.  Ends synchronised.
-__device__ __forceinline__ void smooth_group(Cell const &C, CamclSmem const &S, int n, int const (&nsm)[FB_MAX],
+// nsm_of(j) smoothings of item j's arrays (a, v) for every j < n together (most = the largest
+// count), ping-ponging with (ta, tv); with_scalar = false smooths the vectors only.  Item j's result
+// is in (a, v) when its count is even and in (ta, tv) when it is odd.  The items are visited by a
+// loop, not unrolled: the kernel is latency-bound and its code must stay small.  Ends synchronised.
+template <class NsmOf>
+__device__ __forceinline__ void smooth_group(Cell const &C, CamclSmem const &S, int n, NsmOf const &nsm_of, int most,
                                              bool with_scalar)
 {
     int const tl = max(C.t - 1, 0), tr = min(C.t + 1, C.L - 1), t = C.t;
-    int       most = 0;
-#pragma unroll
-    for (int j = 0; j < FB_MAX; ++j)
-        if (j < n)
-            most = max(most, nsm[j]);
     for (int it = 0; it < most; ++it) {
         __syncthreads();
-#pragma unroll
-        for (int j = 0; j < FB_MAX; ++j) {
-            if (j >= n || it >= nsm[j])
+        bool const odd = it & 1;
+#pragma unroll 1
+        for (int j = 0; j < n; ++j) {
+            if (it >= nsm_of(j))
                 continue;
-            bool const    odd = it & 1;
-            double const *a   = odd ? S.ta(j) : S.a(j);
-            double       *ta  = odd ? S.a(j) : S.ta(j);
-            double const *v   = odd ? S.tv(j) : S.v(j);
-            double       *tv  = odd ? S.v(j) : S.tv(j);
+            double const *a  = odd ? S.ta(j) : S.a(j);
+            double       *ta = odd ? S.a(j) : S.ta(j);
+            double const *v  = odd ? S.tv(j) : S.v(j);
+            double       *tv = odd ? S.v(j) : S.tv(j);
             if (with_scalar)
                 ta[t] = (a[tl] + 2 * a[t] + a[tr]) * .25;
+#pragma unroll
             for (int k = 0; k < 3; ++k)
                 tv[3 * t + k] = (v[3 * tl + k] + 2 * v[3 * t + k] + v[3 * tr + k]) * .25;
         }
@@ -473,6 +465,15 @@ __device__ __forceinline__ SrcItem src_item(FieldArgs const &a, int i)
         return { 1, i, 0 };
     return { 2, i - a.nc, 0 };
 }
+__device__ __forceinline__ int src_nsm(FieldArgs const &a, SrcItem const &it)
+{
+    return it.kind == 0 ? a.k[it.idx].nsm : it.kind == 1 ? a.c[it.idx].nsm : a.e[it.idx].nsm;
+}
+// the smoothing count of item s of the current advance (kinetic species, cold species, external sources)
+__device__ __forceinline__ int adv_nsm(FieldArgs const &a, int s)
+{
+    return s < a.nk ? a.k[s].nsm : s < a.nk + a.nc ? a.c[s - a.nk].nsm : a.e[s - a.nk - a.nc].nsm;
+}
 
 // ------------------------------------------------------------------------------------------------
 // CAM-CL cycle (Domain_CAMCL.cc:57-193)
@@ -485,15 +486,6 @@ __device__ __forceinline__ void camcl_field_body(FieldArgs const &a, int blk)
     CamclSmem const S = carve_camcl(sm, C.L, a.fb);
     int const       t = C.t, Nx = a.Nx, L = C.L;
 
-    // the half-grid geometry of the cell before this one, for its E in the fused subcycle
-    HalfGeo Cm;
-    {
-        long const    N = Nx, i = (C.gm + Nx - 1) % Nx;
-        double const *G = a.geo;
-        Cm = { G[G_HCOV_X * N + i], G[G_HCOV_Y * N + i], G[G_HCOV_Z * N + i], G[G_HCON_X * N + i],
-               G[G_HCON_Y * N + i], G[G_HCON_Z * N + i], G[G_MP1 * N + i],    G[G_MP2 * N + i],
-               G[G_MA1 * N + i],    G[G_MA2 * N + i] };
-    }
     d3 const Bn = ld3(a.B_in, C.gm);
     d3       cold_nV[MAXC];
     for (int ci = 0; ci < a.nc; ++ci)
@@ -504,46 +496,41 @@ __device__ __forceinline__ void camcl_field_body(FieldArgs const &a, int blk)
     d3        J0 = { 0, 0, 0 }, J1 = { 0, 0, 0 };
     int const n_src = 2 * a.nk + a.nc + a.ne;
     for (int i0 = 0; i0 < n_src; i0 += a.fb) {
-        int const n = min(a.fb, n_src - i0);
-        int       nsm[FB_MAX];
-#pragma unroll
-        for (int j = 0; j < FB_MAX; ++j) {
-            nsm[j] = 0;
-            if (j >= n)
-                continue;
+        int const  n      = min(a.fb, n_src - i0);
+        auto const nsm_of = [&](int j) { return src_nsm(a, src_item(a, i0 + j)); };
+        int        most   = 0;
+#pragma unroll 1
+        for (int j = 0; j < n; ++j) {
             SrcItem const it = src_item(a, i0 + j);
+            most             = max(most, src_nsm(a, it));
             if (it.kind == 0)
                 stage_raw(a, C, S, j, a.k[it.idx].raw[it.d]);
             else if (it.kind == 2)
                 stage_raw(a, C, S, j, a.e[it.idx].raw[0]);
         }
         __syncthreads();
-#pragma unroll
-        for (int j = 0; j < FB_MAX; ++j) {
-            if (j >= n)
-                continue;
+#pragma unroll 1
+        for (int j = 0; j < n; ++j) {
             SrcItem const it = src_item(a, i0 + j);
             if (it.kind == 1) {
                 ColdSrc const &K = a.c[it.idx];
                 S.a(j)[t]        = (K.n[C.gm] * K.w) * K.cdcf;
                 sst3(S.v(j), t, (cold_nV[it.idx] * K.w) * K.ccf);
-                nsm[j] = K.nsm;
             } else {
                 KinSrc const &K = it.kind == 0 ? a.k[it.idx] : a.e[it.idx];
                 S.a(j)[t]       = fold_staged(a, C, S, j, 0, K.s1, K.cdcf, K.eq);
+#pragma unroll
                 for (int q = 0; q < 3; ++q)
                     S.v(j)[3 * t + q] = fold_staged(a, C, S, j, 1 + q, K.s1, K.ccf, nullptr);
-                nsm[j] = K.nsm;
             }
         }
-        smooth_group(C, S, n, nsm, true);
-#pragma unroll
-        for (int j = 0; j < FB_MAX; ++j) {
-            if (j >= n)
-                continue;
-            SrcItem const it = src_item(a, i0 + j);
-            double const  r  = smoothed_a(S, j, nsm[j])[t];
-            d3 const      v  = sld3(smoothed_v(S, j, nsm[j]), t);
+        smooth_group(C, S, n, nsm_of, most, true);
+#pragma unroll 1
+        for (int j = 0; j < n; ++j) {
+            SrcItem const it  = src_item(a, i0 + j);
+            int const     nsm = src_nsm(a, it);
+            double const  r   = smoothed_a(S, j, nsm)[t];
+            d3 const      v   = sld3(smoothed_v(S, j, nsm), t);
             if (it.kind == 0 && it.d == 1) {
                 J1 = J1 + v;
                 rho1 += r;
@@ -571,19 +558,16 @@ __device__ __forceinline__ void camcl_field_body(FieldArgs const &a, int blk)
     double const dPe  = dPe_at(a, C, S.Pe);
     double const dPe1 = dPe_at(a, C, S.Pe1);
     d3 const     jc   = contr_half(C, J_avg);
-    // the same for the cell before (dPe_at of cell t - 1 reads Pe at t - 2 and t)
-    double const dPe_m = ((S.Pe[t] - S.Pe[max(t - 2, 0)]) * a.cO2 * Cm.mp1) * Cm.mp2;
-    d3 const     jc_m  = contr_half(Cm, sld3(S.Javg, max(t - 1, 0)));
-    double const rho_m = S.rho_avg[max(t - 1, 0)];
 
-    // 4. subcycle, one barrier per sub-step: each thread computes E at its cell and at the one
-    // before (the value that cell's thread computes, operation for operation), then Faraday's law
+    // 4. subcycle: E at every cell (the covariant E is exchanged through Bavg, free until the
+    // average), then Faraday's law from E at this cell and the one before
     d3 X = Bn, Y = Bn; // X is updated, Y holds the newest B
     for (int i = 0; i <= a.m; ++i) {
         int const    p    = i & 1;
-        d3 const     E    = E_at_g(a, C, t, L, S.Bcov[p], S.Bcon[p], jc, dPe, rho_avg);
-        d3 const     Ec   = covar_half(C, E);
-        d3 const     Em   = t > 0 ? covar_half(Cm, E_at_g(a, Cm, t - 1, L, S.Bcov[p], S.Bcon[p], jc_m, dPe_m, rho_m)) : Ec;
+        d3 const     Ec   = covar_half(C, E_at_g(a, C, t, L, S.Bcov[p], S.Bcon[p], jc, dPe, rho_avg));
+        sst3(S.Bavg, t, Ec);
+        __syncthreads();
+        d3 const     Em   = sld3(S.Bavg, max(t - 1, 0));
         double const dtp  = (i == 0 || i == a.m) ? a.sub_dt : 2.0 * a.sub_dt;
         d3 const     Bnew = B_at_e(a, C, Ec, Em, X, dtp);
         X                 = Bnew;
@@ -610,20 +594,19 @@ __device__ __forceinline__ void camcl_field_body(FieldArgs const &a, int blk)
                         0 * a.O0 + (Bnext.z + Bavg.z) * 0.5 };
     int const n_adv = a.nk + a.nc + a.ne;
     for (int i0 = 0; i0 < n_adv; i0 += a.fb) {
-        int const n = min(a.fb, n_adv - i0);
-        int       nsm[FB_MAX];
-#pragma unroll
-        for (int j = 0; j < FB_MAX; ++j) {
+        int const  n      = min(a.fb, n_adv - i0);
+        auto const nsm_of = [&](int j) { return adv_nsm(a, i0 + j); };
+        int        most   = 0;
+#pragma unroll 1
+        for (int j = 0; j < n; ++j) {
             int const s = i0 + j;
-            if (j < n && (s < a.nk || s >= a.nk + a.nc))
+            most        = max(most, adv_nsm(a, s));
+            if (s < a.nk || s >= a.nk + a.nc)
                 stage_raw(a, C, S, j, (s < a.nk ? a.k[s] : a.e[s - a.nk - a.nc]).raw[1]);
         }
         __syncthreads();
-#pragma unroll
-        for (int j = 0; j < FB_MAX; ++j) {
-            nsm[j] = 0;
-            if (j >= n)
-                continue;
+#pragma unroll 1
+        for (int j = 0; j < n; ++j) {
             int const s = i0 + j;
             double    lam;
             d3        gam;
@@ -633,21 +616,18 @@ __device__ __forceinline__ void camcl_field_body(FieldArgs const &a, int blk)
                 gam             = { fold_staged(a, C, S, j, 1, K.s1, K.gamf, nullptr),
                                     fold_staged(a, C, S, j, 2, K.s1, K.gamf, nullptr),
                                     fold_staged(a, C, S, j, 3, K.s1, K.gamf, nullptr) };
-                nsm[j]          = K.nsm;
             } else {
                 ColdSrc const &K = a.c[s - a.nk];
                 lam              = (K.n[C.gm] * K.w) * K.lamf;
                 gam              = (cold_nV[s - a.nk] * K.w) * K.gamf;
-                nsm[j]           = K.nsm;
             }
             d3 const Jadv = (Es * lam + cross(gam, Bi)) * (0.5 * a.dt);
             sst3(S.v(j), t, { 0 + Jadv.x, 0 + Jadv.y, 0 + Jadv.z });
         }
-        smooth_group(C, S, n, nsm, false);
-#pragma unroll
-        for (int j = 0; j < FB_MAX; ++j)
-            if (j < n)
-                J1 = J1 + sld3(smoothed_v(S, j, nsm[j]), t);
+        smooth_group(C, S, n, nsm_of, most, false);
+#pragma unroll 1
+        for (int j = 0; j < n; ++j)
+            J1 = J1 + sld3(smoothed_v(S, j, adv_nsm(a, i0 + j)), t);
     }
     // 6. E from (B, rho^{N+1}, J^+ advanced)
     d3 const Ef = E_at_g(a, C, t, L, S.Bcov[pb], S.Bcon[pb], contr_half(C, J1), dPe1, rho1);
@@ -771,8 +751,8 @@ __device__ __forceinline__ void pc_field_body(FieldArgs const &a, int blk)
 }
 
 // one run: the arguments are kernel constants, block b covers segment b
-__global__ void __launch_bounds__(512) camcl_field_kernel(FieldArgs a) { camcl_field_body(a, blockIdx.x); }
-__global__ void __launch_bounds__(512) pc_field_kernel(FieldArgs a) { pc_field_body(a, blockIdx.x); }
+__global__ void __launch_bounds__(512) camcl_field_kernel(FieldArgs const __grid_constant__ a) { camcl_field_body(a, blockIdx.x); }
+__global__ void __launch_bounds__(512) pc_field_kernel(FieldArgs const __grid_constant__ a) { pc_field_body(a, blockIdx.x); }
 
 // an ensemble: block b covers segment map[b].seg of run map[b].run, whose arguments it copies
 // from the device table into shared memory
