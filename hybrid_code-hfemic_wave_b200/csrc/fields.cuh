@@ -190,6 +190,23 @@ __device__ __forceinline__ d3 E_at_g(FieldArgs const &a, G const &C, int t, int 
     d3 const  Ec = { (lz.x - dPe) / rho, (lz.y - 0.0) / rho, (lz.z - 0.0) / rho };
     return mask_a(C, contr_half(C, Ec));
 }
+// E_at_g inside the B subcycle: only the y and z components (the ones Faraday's law reads; x is
+// returned as 0), and the division by the density, which the sub-steps share, as a multiplication
+// by its reciprocal (within one rounding of the quotient)
+__device__ __forceinline__ d3 E_sub(FieldArgs const &a, Cell const &C, int t, int L, double const *Bcov, double const *Bcon,
+                                    d3 jc, double inv_rho)
+{
+    int const    tr  = min(t + 1, L - 1);
+    double const B1y = Bcov[3 * tr + 1], B1z = Bcov[3 * tr + 2], B0y = Bcov[3 * t + 1], B0z = Bcov[3 * t + 2];
+    d3           Je  = { 0 - jc.x, (-B1z + B0z) * a.cOsqrtg - jc.y, (+B1y - B0y) * a.cOsqrtg - jc.z };
+    Je               = mask_p(C, Je);
+    d3 const     d1  = sld3(Bcon, tr), d0 = sld3(Bcon, t);
+    d3 const     Bc  = { a.inv_D1 * a.O0 + (d1.x + d0.x) * 0.5, 0 * a.O0 + (d1.y + d0.y) * 0.5, 0 * a.O0 + (d1.z + d0.z) * 0.5 };
+    double const ly  = (Je.z * Bc.x - Je.x * Bc.z) * a.sqrt_g;
+    double const lz  = (Je.x * Bc.y - Je.y * Bc.x) * a.sqrt_g;
+    double const ey  = (ly - 0.0) * inv_rho, ez = (lz - 0.0) * inv_rho;
+    return { 0.0, ((C.hny * ey) * C.ma1) * C.ma2, ((C.hnz * ez) * C.ma1) * C.ma2 }; // mask_a(contr_half(Ec))
+}
 __device__ __forceinline__ d3 E_at(FieldArgs const &a, Cell const &C, double const *Bcov, double const *Bcon, d3 jc,
                                    double dPe, double rho)
 {
@@ -331,7 +348,7 @@ static __device__ d3 cold_push(FieldArgs const &a, Cell const &C, ColdSrc const 
 
 // shared memory of the CAM-CL field body with smoothing groups of fb items (see below)
 constexpr int FB_MAX     = 8;  // items per smoothing group
-constexpr int FS_FIXED_L = 22; // arrays of L doubles outside the groups
+constexpr int FS_FIXED_L = 16; // arrays of L doubles outside the groups
 constexpr int FS_ITEM_L  = 8;  // per item: a, ta (L each), v, tv (3L each)
 constexpr int FS_GHOST   = 24; // per item: 4 quantities x 6 ghost-fold partners
 __host__ __device__ constexpr size_t camcl_smem_bytes(int L, int fb)
@@ -352,7 +369,7 @@ __host__ __device__ constexpr size_t camcl_smem_bytes(int L, int fb)
 // with the same operations, in the same order, as per-species collect_smooth.
 // ------------------------------------------------------------------------------------------------
 struct CamclSmem {
-    double *rho_avg, *Pe, *Pe1, *Javg; // Javg: 3L
+    double *Pe1;                       // L
     double *Bcov[2], *Bcon[2], *Bavg;  // 3L each; Bcov / Bcon ping-pong across the subcycles
     double *items;                     // per item j at items + 8 L j: a (L), ta (L), v (3L), tv (3L)
     double *gh;                        // ghost-fold partners: [item][quantity][6]
@@ -365,11 +382,8 @@ struct CamclSmem {
 __device__ __forceinline__ CamclSmem carve_camcl(double *p, int L, int fb)
 {
     CamclSmem s;
-    s.L       = L;
-    s.rho_avg = p, p += L;
-    s.Pe = p, p += L;
+    s.L   = L;
     s.Pe1 = p, p += L;
-    s.Javg = p, p += 3 * L;
     for (int k = 0; k < 2; ++k) {
         s.Bcov[k] = p, p += 3 * L;
         s.Bcon[k] = p, p += 3 * L;
@@ -486,37 +500,54 @@ __device__ __forceinline__ void camcl_field_body(FieldArgs const &a, int blk)
     CamclSmem const S = carve_camcl(sm, C.L, a.fb);
     int const       t = C.t, Nx = a.Nx, L = C.L;
 
-    d3 const Bn = ld3(a.B_in, C.gm);
-    d3       cold_nV[MAXC];
-    for (int ci = 0; ci < a.nc; ++ci)
-        cold_nV[ci] = cold_push(a, C, a.c[ci], a.E_in);
-
-    // 1-2. sources at x^N and x^{N+1}, every species' collect_smooth in groups
-    double    rho0 = 0, rho1 = 0;
-    d3        J0 = { 0, 0, 0 }, J1 = { 0, 0, 0 };
-    int const n_src = 2 * a.nk + a.nc + a.ne;
-    for (int i0 = 0; i0 < n_src; i0 += a.fb) {
-        int const  n      = min(a.fb, n_src - i0);
-        auto const nsm_of = [&](int j) { return src_nsm(a, src_item(a, i0 + j)); };
-        int        most   = 0;
-#pragma unroll 1
+    // the deposits of a group of source items into shared memory (kinetic and external ones; the
+    // loop is unrolled by four so that their loads are in flight together)
+    int const  n_src     = 2 * a.nk + a.nc + a.ne;
+    auto const stage_src = [&](int i0) {
+        int const n = min(a.fb, n_src - i0);
+#pragma unroll 4
         for (int j = 0; j < n; ++j) {
             SrcItem const it = src_item(a, i0 + j);
-            most             = max(most, src_nsm(a, it));
             if (it.kind == 0)
                 stage_raw(a, C, S, j, a.k[it.idx].raw[it.d]);
             else if (it.kind == 2)
                 stage_raw(a, C, S, j, a.e[it.idx].raw[0]);
         }
+    };
+    stage_src(0); // before the cold push, so that the two rounds of loads overlap
+
+    d3 const Bn = ld3(a.B_in, C.gm);
+    d3       cold_nV[MAXC];
+    double   cold_n[MAXC]; // mom0_full of each cold species at this cell, read once
+    for (int ci = 0; ci < a.nc; ++ci) {
+        cold_n[ci]  = a.c[ci].n[C.gm];
+        cold_nV[ci] = cold_push(a, C, a.c[ci], a.E_in);
+    }
+
+    // 1-2. sources at x^N and x^{N+1}, every species' collect_smooth in groups
+    double rho0 = 0, rho1 = 0;
+    d3     J0 = { 0, 0, 0 }, J1 = { 0, 0, 0 };
+    for (int i0 = 0; i0 < n_src; i0 += a.fb) {
+        int const  n      = min(a.fb, n_src - i0);
+        auto const nsm_of = [&](int j) { return src_nsm(a, src_item(a, i0 + j)); };
+        int        most   = 0;
+        if (i0 > 0) // the first group was staged above
+            stage_src(i0);
+#pragma unroll 1
+        for (int j = 0; j < n; ++j) { // a cold species' sources need no neighbour: formed directly
+            SrcItem const it = src_item(a, i0 + j);
+            most             = max(most, src_nsm(a, it));
+            if (it.kind == 1) {
+                ColdSrc const &K = a.c[it.idx];
+                S.a(j)[t]        = (cold_n[it.idx] * K.w) * K.cdcf;
+                sst3(S.v(j), t, (cold_nV[it.idx] * K.w) * K.ccf);
+            }
+        }
         __syncthreads();
 #pragma unroll 1
         for (int j = 0; j < n; ++j) {
             SrcItem const it = src_item(a, i0 + j);
-            if (it.kind == 1) {
-                ColdSrc const &K = a.c[it.idx];
-                S.a(j)[t]        = (K.n[C.gm] * K.w) * K.cdcf;
-                sst3(S.v(j), t, (cold_nV[it.idx] * K.w) * K.ccf);
-            } else {
+            if (it.kind != 1) {
                 KinSrc const &K = it.kind == 0 ? a.k[it.idx] : a.e[it.idx];
                 S.a(j)[t]       = fold_staged(a, C, S, j, 0, K.s1, K.cdcf, K.eq);
 #pragma unroll
@@ -545,33 +576,51 @@ __device__ __forceinline__ void camcl_field_body(FieldArgs const &a, int blk)
             }
         }
     }
+    // the first group of the current advance (step 5) is staged now, so that its loads complete
+    // during the subcycle (a thread's staging writes only its own cell of the items, which it
+    // has read above, and the ghost partners, which no one reads any more)
+    int const  n_adv     = a.nk + a.nc + a.ne;
+    auto const stage_adv = [&](int i0) {
+        int const n = min(a.fb, n_adv - i0);
+#pragma unroll 4
+        for (int j = 0; j < n; ++j) {
+            int const s = i0 + j;
+            if (s < a.nk || s >= a.nk + a.nc)
+                stage_raw(a, C, S, j, (s < a.nk ? a.k[s] : a.e[s - a.nk - a.nc]).raw[1]);
+        }
+    };
+    stage_adv(0);
+
     // 3. averages
+    // (the pressure gradient at rho_avg enters only the x component of the subcycle's E, which
+    // Faraday's law does not read, so only the one at rho^{N+1} is formed)
     double const rho_avg = (rho0 + rho1) * .5;
     d3 const     J_avg   = (J0 + J1) * .5;
-    S.rho_avg[t]         = rho_avg;
-    sst3(S.Javg, t, J_avg);
-    S.Pe[t]  = Pe_of(a, rho_avg);
-    S.Pe1[t] = Pe_of(a, rho1);
+    S.Pe1[t]             = Pe_of(a, rho1);
     sst3(S.Bcov[0], t, covar_full(C, Bn));
     sst3(S.Bcon[0], t, contr_full(C, Bn));
     __syncthreads();
-    double const dPe  = dPe_at(a, C, S.Pe);
     double const dPe1 = dPe_at(a, C, S.Pe1);
     d3 const     jc   = contr_half(C, J_avg);
 
-    // 4. subcycle: E at every cell (the covariant E is exchanged through Bavg, free until the
-    // average), then Faraday's law from E at this cell and the one before
+    // 4. subcycle: E at every cell (its covariant y and z components are exchanged through Bavg,
+    // free until the average), then Faraday's law from E at this cell and the one before; Ohm's
+    // law reads only the y and z components of the covariant B
+    double const inv_rho = 1.0 / rho_avg;
+    int const    tm      = max(t - 1, 0);
     d3 X = Bn, Y = Bn; // X is updated, Y holds the newest B
     for (int i = 0; i <= a.m; ++i) {
         int const    p    = i & 1;
-        d3 const     Ec   = covar_half(C, E_at_g(a, C, t, L, S.Bcov[p], S.Bcon[p], jc, dPe, rho_avg));
-        sst3(S.Bavg, t, Ec);
+        d3 const     Ec   = covar_half(C, E_sub(a, C, t, L, S.Bcov[p], S.Bcon[p], jc, inv_rho));
+        S.Bavg[2 * t]     = Ec.y;
+        S.Bavg[2 * t + 1] = Ec.z;
         __syncthreads();
-        d3 const     Em   = sld3(S.Bavg, max(t - 1, 0));
+        d3 const     Em   = { 0.0, S.Bavg[2 * tm], S.Bavg[2 * tm + 1] };
         double const dtp  = (i == 0 || i == a.m) ? a.sub_dt : 2.0 * a.sub_dt;
         d3 const     Bnew = B_at_e(a, C, Ec, Em, X, dtp);
         X                 = Bnew;
-        sst3(S.Bcov[1 - p], t, covar_full(C, Bnew));
+        S.Bcov[1 - p][3 * t + 1] = C.fcy * Bnew.y;
+        S.Bcov[1 - p][3 * t + 2] = C.fcz * Bnew.z;
         sst3(S.Bcon[1 - p], t, contr_full(C, Bnew));
         __syncthreads();
         d3 const tmp = X; // the older one is updated next
@@ -592,19 +641,17 @@ __device__ __forceinline__ void camcl_field_body(FieldArgs const &a, int blk)
     d3 const  Bnext = sld3(S.Bavg, min(t + 1, L - 1));
     d3 const  Bi    = { C.hbx + (Bnext.x + Bavg.x) * 0.5, 0 * a.O0 + (Bnext.y + Bavg.y) * 0.5,
                         0 * a.O0 + (Bnext.z + Bavg.z) * 0.5 };
-    int const n_adv = a.nk + a.nc + a.ne;
     for (int i0 = 0; i0 < n_adv; i0 += a.fb) {
         int const  n      = min(a.fb, n_adv - i0);
         auto const nsm_of = [&](int j) { return adv_nsm(a, i0 + j); };
         int        most   = 0;
 #pragma unroll 1
-        for (int j = 0; j < n; ++j) {
-            int const s = i0 + j;
-            most        = max(most, adv_nsm(a, s));
-            if (s < a.nk || s >= a.nk + a.nc)
-                stage_raw(a, C, S, j, (s < a.nk ? a.k[s] : a.e[s - a.nk - a.nc]).raw[1]);
+        for (int j = 0; j < n; ++j)
+            most = max(most, adv_nsm(a, i0 + j));
+        if (i0 > 0) { // the first group was staged before the subcycle
+            stage_adv(i0);
+            __syncthreads();
         }
-        __syncthreads();
 #pragma unroll 1
         for (int j = 0; j < n; ++j) {
             int const s = i0 + j;
@@ -618,7 +665,7 @@ __device__ __forceinline__ void camcl_field_body(FieldArgs const &a, int blk)
                                     fold_staged(a, C, S, j, 3, K.s1, K.gamf, nullptr) };
             } else {
                 ColdSrc const &K = a.c[s - a.nk];
-                lam              = (K.n[C.gm] * K.w) * K.lamf;
+                lam              = (cold_n[s - a.nk] * K.w) * K.lamf;
                 gam              = (cold_nV[s - a.nk] * K.w) * K.gamf;
             }
             d3 const Jadv = (Es * lam + cross(gam, Bi)) * (0.5 * a.dt);
