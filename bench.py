@@ -632,8 +632,23 @@ def ensemble_measure(h, precision, steps=500, members=64):
     finally:
         for r in runs:
             r.close()
-    # the same physics as one run: the first Nx=4096 member's plasma holding as many particles as
-    # the whole ensemble, advanced alone (its own autotuned sort interval and CTAs)
+    # the same members one after another, each alone (their own stream, the library's default
+    # sort interval and CTAs): what the batch replaces
+    alone_ms = 0.0
+    for seed, c in enumerate(cfgs):
+        tr = TimedRun(h, c, None, populate_seed=seed)
+        try:
+            tr.advance(4)
+            m, _, _ = tr.timed(steps)
+            alone_ms += m
+        finally:
+            tr.close()
+    alone = {"workload": f"the {members} members one after another, each alone", "runs_per_s": members / (alone_ms / 1e3),
+             "value": n_particles * steps / (alone_ms / 1e3)}
+
+    # the same plasma as one dense run: the first Nx=4096 member's plasma holding as many particles
+    # as the whole ensemble (about 20 000 per cell, where a sorted warp's particles share a cell),
+    # advanced alone with its own autotuned sort interval and CTAs
     import dataclasses
 
     base = next(c for c in cfgs if c.Nx == max(x.Nx for x in cfgs))
@@ -651,7 +666,8 @@ def ensemble_measure(h, precision, steps=500, members=64):
     return {"workload": f"ensemble of {members} runs (seeds 0..{members - 1}), {steps} steps each, TSC",
             "precision": "mixed" if precision == h.configs.PREC_MIXED else "fp64",
             "runs_per_s": members / (ms / 1e3), "value": value, "unit": METRIC,
-            "single_run_same_physics": single, "over_single_run": value / single["value"],
+            "members_alone": alone, "over_members_alone": value / alone["value"],
+            "dense_single_run": single, "over_dense_single_run": value / single["value"],
             "ms": ms, "particles": n_particles, "Nx": [c.Nx for c in cfgs][:8] + ["..."],
             "autotune": {"steps": tuned_steps, "sort_interval": k, "ctas_per_sm": ctas},
             "gpu_launches": s1["kernel_launches"] - s0["kernel_launches"],
