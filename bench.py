@@ -415,16 +415,18 @@ class TimedRun:
         self.run.close()
 
 
-def roofline_of(prof, precision, steps, traffic_table):
+def roofline_of(prof, precision, steps, traffic_table, workload=None):
     """Roofline of the dominant kernel (the particle pass): algorithmic bytes per launch over its
-    average launch time (CUDA events on the run's stream around every launch)."""
+    average launch time (CUDA events on the run's stream around every launch).  `traffic` is the
+    DRAM bytes per particle of an ncu capture of the same kernel (profiles/push_kernel_traffic.json,
+    keyed by precision, or by precision and workload), scaled to this launch's particles."""
     peak, peak_kind = measured_peak()
     B = BYTES_PER_PARTICLE_STEP[precision]
     push_avg_ms = prof.push_ms / max(prof.push_launches, 1)
     bytes_per_launch = B * prof.particles_pushed / max(prof.push_launches, 1)
     achieved = bytes_per_launch / (push_avg_ms / 1e3) / 1e9
     traffic = None
-    tr = traffic_table.get(precision)
+    tr = traffic_table.get(f"{precision}:{workload}") or traffic_table.get(precision)
     if tr:
         traffic = tr["bytes_per_particle"] * bytes_per_launch / B
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -828,7 +830,7 @@ def main():
                                "absorbing (extension; the reference has no absorbing boundary)",
                                "particles_per_gpu": t2.n_particles, "value": v2, "autotune": tuned2,
                                "unit": METRIC, "ms_per_step": ms2 / k2,
-                               "roofline": roofline_of(prof2, "fp64", k2, traffic)}
+                               "roofline": roofline_of(prof2, "fp64", k2, traffic, c2.name)}
             del st2
 
     e2e = None if args.no_e2e else e2e_measure(h, cfg, st, args.steps, world)

@@ -306,8 +306,7 @@ int h1d_math_check(const double *x, int64_t n, double *out);
  * 20 * (H1D_NOALLOC_MAX_NX + 6) doubles plus a status word, about 0.65 MB, held on every GPU that
  * loads the library until the process exits).  Nx above H1D_NOALLOC_MAX_NX is rejected with
  * H1D_ERR_INVALID_ARG.  The first call on a device looks up that array's device address (once per
- * device, with the device current); make that first call before any stream capture.  All calls
- * share the one array: calls that overlap on the GPU (concurrent streams or threads) race and
+ * device, with the device current).  All calls share the one array: calls that overlap on the GPU (concurrent streams or threads) race and
  * must be serialised by the caller.  The looked-up address is kept for the life of the process:
  * do not call this entry point again on a device after cudaDeviceReset. */
 #define H1D_NOALLOC_MAX_NX 4096
