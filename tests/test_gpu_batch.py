@@ -264,3 +264,38 @@ def test_batch_members_share_one_algorithm(gpu_lib):
             h.abi.Batch([a, c])
     finally:
         a.close(), c.close()
+
+
+def test_batch_sort_is_each_members_stable_cell_sort(gpu_lib):
+    """The batch sorts every species of every member in one launch set (one histogram, scan and
+    scatter launch per radix pass over all segments, with digits sized for the widest grid).  With
+    a sort before every step, each species' device order after one step is exactly the CPU stable
+    sort, by its own full-grid cell, of its uploaded particles: members of 64 to 4096 cells (keys
+    of 7 and 13 bits, sorted together in two passes), with one and two species, FP64."""
+    import os
+
+    from hfemic_b200.loader import initial_state
+    from parity_util import cell_keys
+    from state_io import read_state
+
+    golden = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    p2 = h.configs.parity_p2()
+    cfgs = [p2, h.configs.ensemble_member(0, precision=h.configs.PREC_FP64, ppc_scale=0.2),
+            h.configs.ensemble_member(1, precision=h.configs.PREC_FP64, ppc_scale=0.2)]
+    states = [read_state(os.path.join(golden, f"{p2.name}.init.bin"))]
+    states += [initial_state(c, seed=i) for i, c in enumerate(cfgs[1:], 1)]
+    runs = [h.Run(c, gpu_lib) for c in cfgs]
+    try:
+        for r, st in zip(runs, states):
+            r.upload_state(st)
+        with h.abi.Batch(runs) as b:
+            b.configure(sort_interval=1, use_graphs=False)
+            b.advance(1)
+        for c, r, st in zip(cfgs, runs, states):
+            for s in range(len(c.kinetic)):
+                pid = r.particles(s)["pid"]
+                keys = cell_keys(np.asarray(st["particles"][s]["q1"]), c.Nx)
+                np.testing.assert_array_equal(pid, np.argsort(keys, kind="stable"), err_msg=f"{c.name} species {s}")
+    finally:
+        for r in runs:
+            r.close()
