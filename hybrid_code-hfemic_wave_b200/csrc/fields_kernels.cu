@@ -49,6 +49,11 @@ cudaError_t launch_prep_fields(double *B, double *E, double *EB, float *EBf, int
     prep_fields_kernel<<<(Nx + 2 * PAD + 255) / 256, 256, 0, st>>>(B, E, EB, EBf, Nx);
     return cudaGetLastError();
 }
+cudaError_t launch_ghost_fill(double *dst, double const *src, int nc, int Nx, cudaStream_t st)
+{
+    ghost_fill_kernel<<<1, 32, 0, st>>>(dst, src, nc, Nx);
+    return cudaGetLastError();
+}
 cudaError_t launch_finalize_kinetic(double const *raw, double const *eq, double *out, int Nx, double s1,
                                     int reflecting, cudaStream_t st)
 {

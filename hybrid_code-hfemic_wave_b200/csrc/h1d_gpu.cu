@@ -1030,6 +1030,17 @@ int pc_particles(h1d_run *run, int pass, int dep_set) // pass 0 predictor, 1 cor
 int pc_initial_sources(h1d_run *run) // Domain_PC.cc:36-56
 {
     int const X = run->dset, Y = 1 - X;
+    // the cold fluid's boundary_pass (Domain_PC.cc:46).  The reference updates mom1_full in place
+    // and never writes its ghosts again; here the steps alternate between two nV buffers and write
+    // their interiors, so both buffers get the ghosts
+    int const Nx = static_cast<int>(run->Nx);
+    for (int c = 0; c < run->p.n_cold; ++c) {
+        ColdState &C = run->cold[c];
+        double    *v = C.nV[C.cur] + 3 * PAD;
+        CU(launch_ghost_fill(C.n + PAD, C.n + PAD, 1, Nx, run->stream));
+        CU(launch_ghost_fill(v, v, 3, Nx, run->stream));
+        CU(launch_ghost_fill(C.nV[1 - C.cur] + 3 * PAD, v, 3, Nx, run->stream));
+    }
     TRY(pc_particles(run, 2, Y));
     TRY(launch_run_sources(run, static_cast<double>(run->step) * run->p.dt + 0)); // a predictor copy's update(0)
     TRY(pc_launch_fields(run, 0, Y, X, nullptr, nullptr));

@@ -27,6 +27,7 @@ cudaError_t launch_camcl_fields_batch(FieldArgs const *table, FieldBlock const *
 cudaError_t launch_pc_fields_batch(FieldArgs const *table, FieldBlock const *map, int blocks, int threads,
                                    size_t smem, cudaStream_t st);
 cudaError_t launch_prep_fields(double *B, double *E, double *EB, float *EBf, int Nx, cudaStream_t st);
+cudaError_t launch_ghost_fill(double *dst, double const *src, int nc, int Nx, cudaStream_t st);
 cudaError_t launch_finalize_kinetic(double const *raw, double const *eq, double *out, int Nx, double s1,
                                     int reflecting, cudaStream_t st);
 cudaError_t launch_finalize_cold(double const *n_full, double const *nV_full, double *out, int Nx, double w,

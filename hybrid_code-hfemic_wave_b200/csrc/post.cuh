@@ -30,6 +30,21 @@ __global__ void iota_kernel(int32_t *pid, int64_t n)
 
 __device__ __forceinline__ int wrap(int i, int Nx) { return i < 0 ? i + Nx : i >= Nx ? i - Nx : i; }
 
+// the periodic ghost fill of an interleaved array of `nc` components per cell (a at interior cell
+// 0): the boundary_pass a delegate applies to a grid array (Delegate.cc:76-87), e.g. to the cold
+// fluid's mom0_full / mom1_full at the start of a predictor-corrector run (Domain_PC.cc:46)
+// (the ghosts of `dst` from the interior of `src`, which may be the same array)
+__global__ void ghost_fill_kernel(double *dst, double const *src, int nc, int Nx)
+{
+    int const k = static_cast<int>(threadIdx.x); // PAD ghost cells on each side
+    if (k >= PAD)
+        return;
+    for (int c = 0; c < nc; ++c) {
+        dst[nc * (k - PAD) + c] = src[nc * (Nx - PAD + k) + c];
+        dst[nc * (Nx + k) + c]  = src[nc * k + c];
+    }
+}
+
 // boundary_pass of E and B (periodic ghost fill, Delegate.cc:76-87) and the push record
 // {E, B on the half grid} (PartSpecies.cc:27-34; the last ghost's half-grid B stays NaN)
 __global__ void prep_fields_kernel(double *B, double *E, double *EB, float *EBf, int Nx)

@@ -2,7 +2,11 @@
 
 A run saved after some steps and resumed in a fresh run continues as the original does: FP64
 within 1e-12 (max-norm relative; the resumed run re-sorts its particles, which changes only the
-order of deposit sums), mixed precision within 1e-5.  A save of a resumed run reproduces the
+order of deposit sums), mixed precision within 1e-5.  The grid arrays are compared on the
+interior: a predictor-corrector run refreshes the ghost cells of the cold fluid's full moments
+when it starts, from a checkpoint too, as the reference's Domain_PC::advance_by does after a
+snapshot load (Domain_PC.cc:46), while the uninterrupted run keeps the ghosts it started with;
+nothing reads those ghosts.  A save of a resumed run reproduces the
 image byte for byte, and a checkpoint of other parameters is refused ("signature verification
 failed", Recorder/Snapshot.cc:340-342).
 """
@@ -39,7 +43,7 @@ def test_resume_continues_the_run(gpu_lib, name, precision, tol):
         assert h.abi.step_count(b) == 6
         b.advance(6)
         sb = b.state()
-    errs = state_errors(sb, sa, cfg)
+    errs = state_errors(sb, sa, cfg, interior_only=True)
     print(name, precision, {k: f"{v:.1e}" for k, v in errs.items()})
     assert max(errs.values()) <= tol, errs
 

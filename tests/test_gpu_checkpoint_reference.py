@@ -85,7 +85,9 @@ def test_reference_resumes_a_cuda_checkpoint(gpu_lib, name, precision):
             if precision == h.configs.PREC_MIXED:
                 errs = {k: v for k, v in errs.items() if "particles" not in k}
                 tol = 1e-4
-            print(name, "mixed" if precision else "fp64", steps, f"max {max(errs.values()):.2e}")
+            inner = max(state_errors(st, refs[steps], cfg, interior_only=True).values())
+            print(name, "mixed" if precision else "fp64", steps, f"max {max(errs.values()):.2e}",
+                  f"(interior cells {inner:.2e})")
             bad = {k: v for k, v in errs.items() if not v <= tol}
             assert not bad, (steps, bad)
             if precision == h.configs.PREC_FP64 and steps == 1:
