@@ -126,6 +126,10 @@ struct h1d_run {
     int          sort_interval = 16;
     int          ctas_per_sm   = 0; // CTAs per SM of the particle pass; 0: the kernel's default
     uint64_t     gen           = 0; // bumped by every upload and particle-count change
+    // collect_all formed by the particle pass of the last step (fused_collect): valid while the
+    // step count and the particle generation are unchanged
+    int64_t      collected_step = -1;
+    uint64_t     collected_gen  = 0;
     int          batch_count   = 0; // batches this run is a member of (at most one)
     std::string  msg;
     // profiling: event pairs per phase (0 push, 1 sort, 2 field)
@@ -528,6 +532,8 @@ PushArgsMixed mixed_args(h1d_run *run, int s, PushArgs const &a)
     for (int d = 0; d < 2; ++d)
         for (int q = 0; q < 4; ++q)
             m.dep[d][q] = a.dep[d][q];
+    for (int q = 0; q < 6; ++q)
+        m.nvv[q] = a.nvv[q];
     m.full_min = static_cast<float>(a.full_min), m.xiD1 = static_cast<float>(a.xiD1);
     m.inv_D1 = static_cast<float>(a.inv_D1), m.O0 = static_cast<float>(a.O0), m.dt = static_cast<float>(a.dt);
     m.travel_scale = static_cast<float>(a.travel_scale), m.xiO0_Oc = static_cast<float>(a.xiO0_Oc);
@@ -940,11 +946,54 @@ int push_run(h1d_run *run, ArgsOf const &args_of)
     return H1D_OK;
 }
 
-int camcl_step(h1d_run *run)
+// collect_all (PartSpecies.cc:225-244) deposits with CIC whatever the species' shape, and the
+// particle pass deposits n and nV at the end position with the same weights and velocities.  So
+// when every species is CIC with fixed weights, the pass of an advance_by's last step also
+// deposits the second moments w v_i v_j, and finalize_moments takes n and nV from that step's
+// end-position deposit: no sort and no separate pass over the particles.
+bool fused_collect(h1d_run const *run)
+{
+    h1d_params const &p = run->p;
+    if (p.algorithm != H1D_ALGO_CAMCL || p.n_kinetic < 1)
+        return false;
+    for (int s = 0; s < p.n_kinetic; ++s)
+        if (p.kinetic[s].shape_order != 1 || evolves_psd(p.kinetic[s]))
+            return false;
+    return true;
+}
+
+// the particle pass of one CAM-CL step that also forms collect_all's second moments into mom_raw
+int push_collect(h1d_run *run)
+{
+    h1d_params const &p      = run->p;
+    bool const        mirror = p.xi != 0;
+    for (int s = 0; s < p.n_kinetic; ++s) {
+        SpeciesState &S = run->sp[s];
+        CU(cudaMemsetAsync(S.mom_raw + 4 * run->M, 0, sizeof(double) * 6 * run->M, run->stream));
+        PushArgs a = push_args(run, s);
+        for (int q = 0; q < 6; ++q)
+            a.nvv[q] = S.mom_raw + static_cast<size_t>(4 + q) * run->M + PAD;
+        if (a.n == 0)
+            continue;
+        phase_begin(run, 0);
+        if (run->mixed)
+            CU(launch_push_nvv(mixed_args(run, s, a), mirror, p.particle_bc, run->num_sms * PIPE_CTAS_PER_SM_NVV_MIXED,
+                               run->stream));
+        else
+            CU(launch_push_nvv(a, mirror, p.particle_bc, run->num_sms * PIPE_CTAS_PER_SM_NVV_FP64, run->stream));
+        phase_end(run, 1);
+    }
+    return H1D_OK;
+}
+
+int camcl_step(h1d_run *run, bool collect = false)
 {
     h1d_params const &p = run->p;
     TRY(sort_due(run));
-    TRY(push_run(run, [run](int s) { return push_args(run, s); }));
+    if (collect)
+        TRY(push_collect(run));
+    else
+        TRY(push_run(run, [run](int s) { return push_args(run, s); }));
     for (int s = 0; s < p.n_kinetic; ++s) {
         if (run->profiling)
             run->prof.particles_pushed += run->sp[s].n;
@@ -960,6 +1009,8 @@ int camcl_step(h1d_run *run)
     for (int c = 0; c < p.n_cold; ++c)
         run->cold[c].cur = 1 - run->cold[c].cur;
     run->step++;
+    if (collect)
+        run->collected_step = run->step, run->collected_gen = run->gen;
     return H1D_OK;
 }
 
@@ -1095,6 +1146,27 @@ int finalize_moments(h1d_run *run)
     if (!run->moments_stale)
         return H1D_OK;
     h1d_params const &p = run->p;
+    if (fused_collect(run) && run->collected_step == run->step && run->collected_gen == run->gen) {
+        // the last step's pass formed the sums: n and nV are its end-position deposit, which
+        // the field kernel of that step read and left in place (it clears the other set)
+        int const set = 1 - run->dset;
+        for (int s = 0; s < p.n_kinetic; ++s) {
+            SpeciesState &S = run->sp[s];
+            for (int q = 0; q < 4; ++q)
+                CU(cudaMemcpyAsync(S.mom_raw + static_cast<size_t>(q) * run->M, dep_ptr(run, s, set, 1, q) - PAD,
+                                   sizeof(double) * run->M, cudaMemcpyDeviceToDevice, run->stream));
+            CU(launch_finalize_kinetic(S.mom_raw, S.eq, S.mom, static_cast<int>(run->Nx), 1.0 / p.kinetic[s].moment_norm,
+                                       p.particle_bc == H1D_BC_PERIODIC ? 0 : 1, run->stream));
+        }
+        for (int c = 0; c < p.n_cold; ++c) {
+            ColdState &C = run->cold[c];
+            CU(launch_finalize_cold(C.n, C.nV[C.cur], C.mom, static_cast<int>(run->Nx), p.moment_weighting,
+                                    run->stream));
+        }
+        CU(cudaGetLastError());
+        run->moments_stale = false;
+        return H1D_OK;
+    }
     // particles that drifted since their last sort are sorted first: a warp's particles then
     // share a few cells and collect_all accumulates in registers (the next steps gain too)
     std::vector<SortItem> drifted;
@@ -2094,8 +2166,9 @@ int h1d_advance_async(h1d_run *run, uint32_t n_steps)
     if (first && run->p.algorithm == H1D_ALGO_PC)
         TRY(pc_initial_sources(run));
     run->recurring = true;
+    bool const fuse = fused_collect(run);
     for (uint32_t i = 0; i < n_steps; ++i)
-        TRY(run->p.algorithm == H1D_ALGO_CAMCL ? camcl_step(run) : pc_step(run));
+        TRY(run->p.algorithm == H1D_ALGO_CAMCL ? camcl_step(run, fuse && i + 1 == n_steps) : pc_step(run));
     run->moments_stale = true;
     return H1D_OK;
 }

@@ -31,6 +31,7 @@ struct PushArgs {
     double const  *EB; // per cell {Ex, Ey, Ez, dBx, dBy, dBz}: E and B averaged onto the half grid
                        // (PartSpecies.cc:27-34), pointer at interior cell 0
     double        *dep[2][4]; // [deposit at x^N | x^{N+1}][n, nVx, nVy, nVz], at cell 0
+    double        *nvv[6];    // collect_all's xx, yy, zz, xy, yz, zx sums at cell 0 (NVV launches only)
     double         half_min, full_min, full_max, full_len;
     double         xi, xi2, xiD1, D1, inv_D1, O0, Oc, dt, travel_scale, xiO0_Oc;
     BorisK         boris;
@@ -274,6 +275,11 @@ constexpr size_t PIPE_SMEM       = PipeLayout<false>::COL_OFFSET + PIPE_COL_BYTE
 constexpr size_t PIPE_SMEM_PSD   = PipeLayout<true>::COL_OFFSET + PIPE_COL_BYTES;
 static_assert(2 * PIPE_STAGES * sizeof(uint64_t) <= 128, "barriers fit before the columns");
 static_assert(2 * (PIPE_SMEM_PSD + 1024) <= 233472, "two CTAs with evolving weights fit an SM");
+// a launch that also forms collect_all's second moments (NVV, the last step of an advance_by)
+// holds a second window per warp: three double2 columns per cell; two CTAs fit an SM
+constexpr size_t PIPE_NVV_BYTES = sizeof(double2) * 3 * PIPE_CONSUMER_WARPS * PIPE_W * 32;
+constexpr size_t PIPE_SMEM_NVV  = PipeLayout<false>::COL_OFFSET + PIPE_COL_BYTES + PIPE_NVV_BYTES;
+static_assert(2 * (PIPE_SMEM_NVV + 1024) <= 233472, "two CTAs of a second-moment launch fit an SM");
 
 __device__ __forceinline__ uint32_t round16(uint32_t b) { return (b + 15u) & ~15u; }
 
@@ -363,6 +369,91 @@ struct ColWindow64 {
     }
 };
 
+// collect_all's second moments w v_i v_j of the deposit at the end position (NVV launches): per
+// warp, cell and lane the double2 columns {xx, yy}, {zz, xy}, {yz, zx}, over the cells of the
+// warp's main window (same base, flushed and moved with it)
+struct NvvWindow64 {
+    double2 *col;
+
+    __device__ __forceinline__ double2 &at(int c, int h, int lane) { return col[(c * 3 + h) * 32 + lane]; }
+    __device__ __forceinline__ void     zero(int lane)
+    {
+#pragma unroll
+        for (int c = 0; c < PIPE_W; ++c)
+#pragma unroll
+            for (int h = 0; h < 3; ++h)
+                at(c, h, lane) = make_double2(0, 0);
+    }
+    template <int O>
+    __device__ __forceinline__ void add(int base, Shape<O> const &sh, double const (&v)[6], int lane)
+    {
+        int const r = sh.i0 - base;
+#pragma unroll
+        for (int j = 0; j <= O; ++j)
+#pragma unroll
+            for (int h = 0; h < 3; ++h) {
+                double2 &e = at(r + j, h, lane);
+                double2  t = e;
+                t.x = fma(v[2 * h], sh.w[j], t.x), t.y = fma(v[2 * h + 1], sh.w[j], t.y);
+                e   = t;
+            }
+    }
+    // the columns summed over the warp and added to the moment sums: {xx, yy, zz, xy} of the
+    // PIPE_W cells in one 32-value reduce-scatter (lane l < 4 PIPE_W: value l = 4 c + q), {yz, zx}
+    // in a 16-value one (lanes 2 k, 2 k + 1: value k = 2 c + q)
+    __device__ __forceinline__ void flush(int base, int lane, PushArgs const &a)
+    {
+        if (base == ColWindow64::NONE)
+            return;
+        double x[32], y[16];
+#pragma unroll
+        for (int k = 0; k < 32; ++k)
+            x[k] = 0.0;
+#pragma unroll
+        for (int k = 0; k < 16; ++k)
+            y[k] = 0.0;
+#pragma unroll
+        for (int c = 0; c < PIPE_W; ++c) {
+            double2 const u = at(c, 0, lane), v = at(c, 1, lane), w = at(c, 2, lane);
+            x[4 * c] = u.x, x[4 * c + 1] = u.y, x[4 * c + 2] = v.x, x[4 * c + 3] = v.y;
+            y[2 * c] = w.x, y[2 * c + 1] = w.y;
+#pragma unroll
+            for (int h = 0; h < 3; ++h)
+                at(c, h, lane) = make_double2(0, 0);
+        }
+        double const t0 = reduce_scatter<32>(x, lane);
+        double const t1 = reduce_scatter<16>(y, lane);
+        unsigned     bad = 0;
+        if (lane < 4 * PIPE_W && t0 != 0.0) {
+            int const cell = base + (lane >> 2);
+            if (cell >= -PAD && cell < a.Nx + PAD)
+                atomicAdd(a.nvv[lane & 3] + cell, t0);
+            else
+                bad = ST_OUT_OF_RANGE;
+        }
+        int const k = lane >> 1;
+        if ((lane & 1) == 0 && k < 2 * PIPE_W && t1 != 0.0) {
+            int const cell = base + (k >> 1);
+            if (cell >= -PAD && cell < a.Nx + PAD)
+                atomicAdd(a.nvv[4 + (k & 1)] + cell, t1);
+            else
+                bad = ST_OUT_OF_RANGE;
+        }
+        if (bad)
+            atomicOr(a.status, bad);
+    }
+};
+
+template <int O>
+__device__ __forceinline__ void nvv_direct(PushArgs const &a, Shape<O> const &sh, double const (&v)[6])
+{
+#pragma unroll
+    for (int j = 0; j <= O; ++j)
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+            atomicAdd(a.nvv[q] + sh.i0 + j, v[q] * sh.w[j]);
+}
+
 template <int O>
 __device__ __forceinline__ void deposit_direct(PushArgs const &a, int d, Shape<O> const &sh, double const (&vw)[4])
 {
@@ -400,8 +491,8 @@ __device__ __forceinline__ int group_of(PushGroups<MAXG> const &G, int64_t chunk
     }
 }
 
-template <int O, bool MIRROR, int BC, int MAXG, bool PSD = false>
-__global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(PushGroups<MAXG> const __grid_constant__ G)
+template <int O, bool MIRROR, int BC, int MAXG, bool PSD = false, bool NVV = false>
+__global__ void __launch_bounds__(PIPE_THREADS, NVV ? 2 : PIPE_CTAS_PER_SM) push_kernel(PushGroups<MAXG> const __grid_constant__ G)
 {
     constexpr int      SPAN        = PIPE_W - 1 - O; // largest stencil base offset inside the window
     constexpr int      PIPE_STAGES = PipeLayout<PSD>::STAGES;
@@ -483,6 +574,11 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
     // ---------------- consumers ----------------
     ColWindow64 win;
     win.col  = reinterpret_cast<double2 *>(smraw + PipeLayout<PSD>::COL_OFFSET) + warp * 2 * PIPE_W * 2 * 32;
+    NvvWindow64 nvw{};
+    if constexpr (NVV) {
+        nvw.col = reinterpret_cast<double2 *>(smraw + PipeLayout<PSD>::COL_OFFSET + PIPE_COL_BYTES) + warp * PIPE_W * 3 * 32;
+        nvw.zero(lane);
+    }
     win.base = ColWindow64::NONE;
     win.zero(lane);
     unsigned bad = 0;
@@ -494,6 +590,8 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
             if (gc >= 0) {
                 PushArgs const &ap = G.g[gc];
                 win.flush(lane, ap);
+                if constexpr (NVV)
+                    nvw.flush(win.base, lane, ap);
                 bad = __reduce_or_sync(0xffffffffu, bad);
                 if (bad && lane == 0)
                     atomicOr(ap.status, bad);
@@ -593,6 +691,8 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
             bool const outside = lo <= hi && (lo < win.base || hi > win.base + SPAN);
             if (__any_sync(0xffffffffu, outside)) { // move the window onto this batch
                 win.flush(lane, a);
+                if constexpr (NVV)
+                    nvw.flush(win.base, lane, a);
                 int const mlo = __reduce_min_sync(0xffffffffu, lo);
                 int const mhi = __reduce_max_sync(0xffffffffu, hi);
                 int const gap = SPAN - (mhi - mlo);
@@ -609,10 +709,20 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
                 }
                 if (dd1[k]) {
                     double const vw[4] = { dw1[k], dv1[k].x * dw1[k], dv1[k].y * dw1[k], dv1[k].z * dw1[k] };
-                    if (ds1[k].i0 >= win.base && ds1[k].i0 <= win.base + SPAN)
+                    bool const   inside = ds1[k].i0 >= win.base && ds1[k].i0 <= win.base + SPAN;
+                    if (inside)
                         win.add<O>(1, ds1[k], vw, lane);
                     else
                         deposit_direct<O>(a, 1, ds1[k], vw);
+                    if constexpr (NVV) { // collect_all's w v_i v_j at the end position (PartSpecies.cc:236-239)
+                        d3 const     v = dv1[k];
+                        double const t[6] = { (v.x * v.x) * dw1[k], (v.y * v.y) * dw1[k], (v.z * v.z) * dw1[k],
+                                              (v.x * v.y) * dw1[k], (v.y * v.z) * dw1[k], (v.z * v.x) * dw1[k] };
+                        if (inside)
+                            nvw.add<O>(win.base, ds1[k], t, lane);
+                        else
+                            nvv_direct<O>(a, ds1[k], t);
+                    }
                 }
             }
         }
@@ -624,6 +734,8 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM) push_kernel(Pu
     if (gc >= 0) {
         PushArgs const &a = G.g[gc];
         win.flush(lane, a);
+        if constexpr (NVV)
+            nvw.flush(win.base, lane, a);
         bad = __reduce_or_sync(0xffffffffu, bad);
         if (bad && lane == 0)
             atomicOr(a.status, bad);

@@ -23,6 +23,7 @@ struct PushArgsMixed {
     int          Nx;
     float const *EB; // per cell {Ex, Ey, Ez, dBx, dBy, dBz, 0, 0} in FP32 (EBF_STRIDE), at interior cell 0
     double      *dep[2][4];
+    double      *nvv[6]; // collect_all's xx, yy, zz, xy, yz, zx sums at cell 0 (NVV launches only)
     float        full_min, xiD1, inv_D1, O0, dt, travel_scale, xiO0_Oc, dtOc_2O0, cDtOc_2O0;
     int          fbits;            // F, the fraction bits of a position
     float        scale, inv_scale; // 2^F, 2^-F
@@ -224,15 +225,20 @@ struct PipeStageMixedT {
 using PipeStageMixed = PipeStageMixedT<false>;
 constexpr int    PIPE_STAGES_MIXED      = 3;
 constexpr int    PIPE_CTAS_PER_SM_MIXED = 4;
-template <bool PSD>
+// A launch that also forms collect_all's second moments (NVV, the last step of an advance_by)
+// holds a second window per warp and is one stage shorter, so that three CTAs fit an SM.
+template <bool PSD, bool NVV = false>
 struct MixLayout {
-    static constexpr int    STAGES     = PSD ? PIPE_STAGES_MIXED - 1 : PIPE_STAGES_MIXED;
+    static constexpr int    STAGES     = PSD || NVV ? PIPE_STAGES_MIXED - 1 : PIPE_STAGES_MIXED;
     static constexpr size_t BAR_OFFSET = sizeof(PipeStageMixedT<PSD>) * STAGES;
     static constexpr size_t COL_OFFSET = BAR_OFFSET + 128; // barriers, then 16-byte aligned columns
 };
 constexpr size_t MIX_COL_BYTES        = sizeof(float4) * PIPE_CONSUMER_WARPS * 2 * MIX_W * 32;
+constexpr size_t MIX_NVV_BYTES        = (sizeof(float4) + sizeof(float2)) * PIPE_CONSUMER_WARPS * MIX_W * 32;
 constexpr size_t PIPE_SMEM_MIXED      = MixLayout<false>::COL_OFFSET + MIX_COL_BYTES;
 constexpr size_t PIPE_SMEM_MIXED_PSD  = MixLayout<true>::COL_OFFSET + MIX_COL_BYTES;
+constexpr size_t PIPE_SMEM_MIXED_NVV  = MixLayout<false, true>::COL_OFFSET + MIX_COL_BYTES + MIX_NVV_BYTES;
+static_assert(3 * (PIPE_SMEM_MIXED_NVV + 1024) <= 233472, "three CTAs of a second-moment launch fit an SM");
 static_assert(2 * PIPE_STAGES_MIXED * sizeof(uint64_t) <= 128, "barriers fit before the columns");
 static_assert(PIPE_CTAS_PER_SM_MIXED * (PIPE_SMEM_MIXED_PSD + 1024) <= 233472, "four CTAs with evolving weights fit an SM");
 
@@ -348,6 +354,105 @@ struct ColWindow {
     }
 };
 
+// collect_all's second moments w v_i v_j of the deposit at the end position (NVV launches): per
+// warp and cell, lane-private columns {xx, yy, zz, xy} (float4) and {yz, zx} (float2), over the
+// cells of the warp's main window (same base, flushed and moved with it)
+struct NvvWindow {
+    float4 *c4;
+    float2 *c2;
+
+    __device__ __forceinline__ float4 &a4(int c, int lane) { return c4[c * 32 + lane]; }
+    __device__ __forceinline__ float2 &a2(int c, int lane) { return c2[c * 32 + lane]; }
+    __device__ __forceinline__ void    zero(int lane)
+    {
+#pragma unroll
+        for (int c = 0; c < MIX_W; ++c)
+            a4(c, lane) = make_float4(0.f, 0.f, 0.f, 0.f), a2(c, lane) = make_float2(0.f, 0.f);
+    }
+    template <int O>
+    __device__ __forceinline__ void add(int base, ShapeF<O> const &sh, float const (&v)[6], int lane)
+    {
+        int const r = sh.i0 - base;
+#pragma unroll
+        for (int j = 0; j <= O; ++j) {
+            float4 &e = a4(r + j, lane);
+            float2 &f = a2(r + j, lane);
+            float4  t = e;
+            float2  u = f;
+            t.x = fmaf(v[0], sh.w[j], t.x), t.y = fmaf(v[1], sh.w[j], t.y);
+            t.z = fmaf(v[2], sh.w[j], t.z), t.w = fmaf(v[3], sh.w[j], t.w);
+            u.x = fmaf(v[4], sh.w[j], u.x), u.y = fmaf(v[5], sh.w[j], u.y);
+            e = t, f = u;
+        }
+    }
+    // the columns summed over the warp and added to the moment sums: {xx, yy, zz, xy} of the MIX_W
+    // cells as one 32-value reduce-scatter (lane l: value 4 c + q), {yz, zx} as a 16-value one
+    // (lanes 2 k and 2 k + 1: value k = 2 c + q)
+    __device__ __forceinline__ void flush(int base, int lane, PushArgsMixed const &a)
+    {
+        if (base == ColWindow::NONE)
+            return;
+        float x[32], y[16];
+#pragma unroll
+        for (int c = 0; c < MIX_W; ++c) {
+            float4 const t = a4(c, lane);
+            float2 const u = a2(c, lane);
+            x[4 * c] = t.x, x[4 * c + 1] = t.y, x[4 * c + 2] = t.z, x[4 * c + 3] = t.w;
+            y[2 * c] = u.x, y[2 * c + 1] = u.y;
+            a4(c, lane) = make_float4(0.f, 0.f, 0.f, 0.f), a2(c, lane) = make_float2(0.f, 0.f);
+        }
+#pragma unroll
+        for (int h = 16; h >= 1; h >>= 1) {
+            bool const up = (lane & h) != 0;
+#pragma unroll
+            for (int j = 0; j < h; ++j) {
+                float const send = up ? x[j] : x[j + h];
+                float const keep = up ? x[j + h] : x[j];
+                x[j]             = keep + __shfl_xor_sync(0xffffffffu, send, h);
+            }
+        }
+#pragma unroll
+        for (int h = 8, m = 16; h >= 1; h >>= 1, m >>= 1) {
+            bool const up = (lane & m) != 0;
+#pragma unroll
+            for (int j = 0; j < h; ++j) {
+                float const send = up ? y[j] : y[j + h];
+                float const keep = up ? y[j + h] : y[j];
+                y[j]             = keep + __shfl_xor_sync(0xffffffffu, send, m);
+            }
+        }
+        float const yz = y[0] + __shfl_xor_sync(0xffffffffu, y[0], 1);
+        unsigned    bad = 0;
+        if (x[0] != 0.0f) {
+            int const cell = base + (lane >> 2);
+            if (cell >= -PAD && cell < a.Nx + PAD)
+                atomicAdd(a.nvv[lane & 3] + cell, static_cast<double>(x[0]));
+            else
+                bad = ST_OUT_OF_RANGE;
+        }
+        if ((lane & 1) == 0 && yz != 0.0f) {
+            int const k = lane >> 1, cell = base + (k >> 1);
+            if (cell >= -PAD && cell < a.Nx + PAD)
+                atomicAdd(a.nvv[4 + (k & 1)] + cell, static_cast<double>(yz));
+            else
+                bad = ST_OUT_OF_RANGE;
+        }
+        if (bad)
+            atomicOr(a.status, bad);
+    }
+};
+
+// the second moments of a particle outside the window, by direct atomics
+template <int O>
+__device__ __forceinline__ void nvv_direct(PushArgsMixed const &a, ShapeF<O> const &sh, float const (&v)[6])
+{
+#pragma unroll
+    for (int j = 0; j <= O; ++j)
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+            atomicAdd(a.nvv[q] + sh.i0 + j, static_cast<double>(v[q] * sh.w[j]));
+}
+
 // the groups of one launch, as PushGroups in particles.cuh
 template <int MAXG>
 struct PushGroupsMixed {
@@ -385,16 +490,17 @@ __device__ __forceinline__ void deposit_direct(PushArgsMixed const &a, int d, Sh
     }
 }
 
-template <int O, bool MIRROR, int BC, int MAXG, bool PSD = false>
+template <int O, bool MIRROR, int BC, int MAXG, bool PSD = false, bool NVV = false>
 __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
     push_kernel_mixed(PushGroupsMixed<MAXG> const __grid_constant__ G)
 {
-    constexpr int   STAGES = MixLayout<PSD>::STAGES;
+    using Layout           = MixLayout<PSD, NVV>;
+    constexpr int   STAGES = Layout::STAGES;
     constexpr int   SPAN   = MIX_W - 1 - O; // largest stencil base offset inside the window
     using Stage            = PipeStageMixedT<PSD>;
     extern __shared__ __align__(128) unsigned char smraw[];
     Stage          *stage = reinterpret_cast<Stage *>(smraw);
-    uint64_t       *full  = reinterpret_cast<uint64_t *>(smraw + MixLayout<PSD>::BAR_OFFSET);
+    uint64_t       *full  = reinterpret_cast<uint64_t *>(smraw + Layout::BAR_OFFSET);
     uint64_t       *empty = full + STAGES;
     int const       warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int64_t const   nchunks = G.chunk0[G.n];
@@ -468,7 +574,14 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
 
     // ---------------- consumers ----------------
     ColWindow win;
-    win.col  = reinterpret_cast<float4 *>(smraw + MixLayout<PSD>::COL_OFFSET) + warp * 2 * MIX_W * 32;
+    win.col  = reinterpret_cast<float4 *>(smraw + Layout::COL_OFFSET) + warp * 2 * MIX_W * 32;
+    NvvWindow nvw{};
+    if constexpr (NVV) {
+        unsigned char *const nb = smraw + Layout::COL_OFFSET + MIX_COL_BYTES;
+        nvw.c4 = reinterpret_cast<float4 *>(nb) + warp * MIX_W * 32;
+        nvw.c2 = reinterpret_cast<float2 *>(nb + sizeof(float4) * PIPE_CONSUMER_WARPS * MIX_W * 32) + warp * MIX_W * 32;
+        nvw.zero(lane);
+    }
     win.base = ColWindow::NONE;
     win.zero(lane);
     unsigned bad = 0;
@@ -480,6 +593,8 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
             if (gc >= 0) {
                 PushArgsMixed const &ap = G.g[gc];
                 win.flush(lane, ap);
+                if constexpr (NVV)
+                    nvw.flush(win.base, lane, ap);
                 bad = __reduce_or_sync(0xffffffffu, bad);
                 if (bad && lane == 0)
                     atomicOr(ap.status, bad);
@@ -636,6 +751,8 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
             bool const outside = lo <= hi && (lo < win.base || hi > win.base + SPAN);
             if (__any_sync(0xffffffffu, outside)) { // move the window onto this batch
                 win.flush(lane, a);
+                if constexpr (NVV)
+                    nvw.flush(win.base, lane, a);
                 int const mlo = __reduce_min_sync(0xffffffffu, lo);
                 int const mhi = __reduce_max_sync(0xffffffffu, hi);
                 int const gap = SPAN - (mhi - mlo);
@@ -650,10 +767,20 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                         deposit_direct<O>(a, 0, ds0[k], dv0[k]);
                 }
                 if (dd1[k]) {
-                    if (ds1[k].i0 >= win.base && ds1[k].i0 <= win.base + SPAN)
+                    bool const inside = ds1[k].i0 >= win.base && ds1[k].i0 <= win.base + SPAN;
+                    if (inside)
                         win.add<O>(1, ds1[k], dv1[k], lane);
                     else
                         deposit_direct<O>(a, 1, ds1[k], dv1[k]);
+                    if constexpr (NVV) { // collect_all's w v_i v_j at the end position (PartSpecies.cc:236-239)
+                        float const vx = el(v.x, k), vy = el(v.y, k), vz = el(v.z, k), wk = el(w, k);
+                        float const t[6] = { (vx * vx) * wk, (vy * vy) * wk, (vz * vz) * wk,
+                                             (vx * vy) * wk, (vy * vz) * wk, (vz * vx) * wk };
+                        if (inside)
+                            nvw.add<O>(win.base, ds1[k], t, lane);
+                        else
+                            nvv_direct<O>(a, ds1[k], t);
+                    }
                 }
             }
         }
@@ -665,6 +792,8 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
     if (gc >= 0) {
         PushArgsMixed const &a = G.g[gc];
         win.flush(lane, a);
+        if constexpr (NVV)
+            nvw.flush(win.base, lane, a);
         bad = __reduce_or_sync(0xffffffffu, bad);
         if (bad && lane == 0)
             atomicOr(a.status, bad);

@@ -21,6 +21,18 @@ cudaError_t pk_attr()
                                 static_cast<int>(PSD ? PIPE_SMEM_PSD : PIPE_SMEM));
 }
 
+// the CIC pass that also forms collect_all's second moments (NVV)
+template <bool M, int BC>
+void pk_nvv(PushGroups<1> const &G, dim3 g, cudaStream_t st)
+{
+    push_kernel<1, M, BC, 1, false, true><<<g, PIPE_THREADS, PIPE_SMEM_NVV, st>>>(G);
+}
+template <bool M, int BC>
+cudaError_t pk_nvv_attr()
+{
+    return cudaFuncSetAttribute(push_kernel<1, M, BC, 1, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                static_cast<int>(PIPE_SMEM_NVV));
+}
 
 template <int O, bool M, bool PSD, class GR>
 void pk_bc(GR const &G, int bc, dim3 g, cudaStream_t st)
@@ -75,6 +87,10 @@ cudaError_t set_smem_once()
         e = pk_attrs<BATCH_GROUPS, false>();
     if (e == cudaSuccess)
         e = pk_attrs<1, true>();
+    for (cudaError_t const x : { pk_nvv_attr<false, 0>(), pk_nvv_attr<false, 1>(), pk_nvv_attr<false, 2>(),
+                                 pk_nvv_attr<true, 0>(), pk_nvv_attr<true, 1>(), pk_nvv_attr<true, 2>() })
+        if (e == cudaSuccess)
+            e = x;
     if (e == cudaSuccess && dev >= 0 && dev < 64)
         done[dev] = true;
     return e;
@@ -136,6 +152,23 @@ cudaError_t launch_push_psd(PushArgs const &a, int order, bool mirror, int bc, i
     PushGroups<1> G{};
     G.n = 1, G.chunk0[0] = 0, G.chunk0[1] = total, G.g[0] = a;
     pk_dispatch<true>(G, order, mirror, bc, dim3(static_cast<unsigned>(std::min<int64_t>(total, max_ctas))), st);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_push_nvv(PushArgs const &a, bool mirror, int bc, int max_ctas, cudaStream_t st)
+{
+    int64_t const total = chunks_of(a.n);
+    if (total == 0)
+        return cudaSuccess;
+    PushGroups<1> G{};
+    G.n = 1, G.chunk0[0] = 0, G.chunk0[1] = total, G.g[0] = a;
+    dim3 const g(static_cast<unsigned>(std::min<int64_t>(total, max_ctas)));
+    if (bc == 0)
+        mirror ? pk_nvv<true, BCK_PERIODIC>(G, g, st) : pk_nvv<false, BCK_PERIODIC>(G, g, st);
+    else if (bc == 1)
+        mirror ? pk_nvv<true, BCK_REFLECTING>(G, g, st) : pk_nvv<false, BCK_REFLECTING>(G, g, st);
+    else
+        mirror ? pk_nvv<true, BCK_ABSORBING>(G, g, st) : pk_nvv<false, BCK_ABSORBING>(G, g, st);
     return cudaGetLastError();
 }
 

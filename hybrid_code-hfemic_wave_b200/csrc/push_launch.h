@@ -23,5 +23,11 @@ cudaError_t launch_push_groups(PushArgsMixed const *args, int n, int order, bool
 // one pass over a species whose weights evolve (push_kernel<..., PSD = true>, push_kernel_mixed<..., PSD = true>)
 cudaError_t launch_push_psd(PushArgs const &a, int order, bool mirror, int bc, int max_ctas, cudaStream_t st);
 cudaError_t launch_push_psd(PushArgsMixed const &a, int order, bool mirror, int bc, int max_ctas, cudaStream_t st);
+// a CIC pass (order 1, fixed weights) that also deposits collect_all's second moments into a.nvv
+cudaError_t launch_push_nvv(PushArgs const &a, bool mirror, int bc, int max_ctas, cudaStream_t st);
+cudaError_t launch_push_nvv(PushArgsMixed const &a, bool mirror, int bc, int max_ctas, cudaStream_t st);
+// CTAs per SM of a second-moment launch (its windows take more shared memory)
+constexpr int PIPE_CTAS_PER_SM_NVV_FP64  = 2;
+constexpr int PIPE_CTAS_PER_SM_NVV_MIXED = 3;
 
 } // namespace h1d

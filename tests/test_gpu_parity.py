@@ -291,3 +291,29 @@ def test_device_rounding_and_trig(gpu_lib):
     assert lib.h1d_math_check(t.ctypes.data_as(dp), t.size, out.ctypes.data_as(dp)) == 0
     assert np.max(np.abs(out[:, 3] - np.sin(t))) <= 4e-16
     assert np.max(np.abs(out[:, 4] - np.cos(t))) <= 4e-16
+
+
+@pytest.mark.parametrize("precision, tol", [(h.configs.PREC_FP64, 1e-12), (h.configs.PREC_MIXED, 1e-5)])
+def test_collect_all_formed_by_the_last_pass(gpu_lib, precision, tol):
+    """For CIC species with fixed weights the particle pass of an advance_by's last step also
+    deposits collect_all's second moments, and n, nV come from that step's end-position deposit.
+    The moments equal the ones of the separate collect_all pass (sort, then moments kernel), which
+    a run takes when its particle generation changed since that step (here: an upload of the
+    same fields).  config 1's plasma at Nx 256; mixed precision sums FP32 lane partials in both."""
+    from hfemic_b200.loader import initial_state
+
+    cfg = h.configs.config1().replace(precision=precision)
+    st = initial_state(cfg, seed=4)
+    out = []
+    for fused in (True, False):
+        with h.Run(cfg, gpu_lib, "h1d_") as g:
+            g.upload_state(st)
+            g.advance(7)
+            if not fused:
+                B, E = g.fields()
+                g.upload_fields(B, E)
+            out.append([g.moments(s) for s in range(len(cfg.kinetic))] + [g.energy()])
+    for (n, nV, nvv), (m, mV, mvv) in zip(out[0][:-1], out[1][:-1]):
+        assert rel_err(n, m) <= tol and rel_err(nV, mV) <= tol and rel_err(nvv, mvv) <= tol
+    for key in ("KE_lab", "KE_pla"):
+        assert rel_err(out[0][-1][key], out[1][-1][key]) <= tol, key
