@@ -535,11 +535,12 @@ def error_vs_reference(h, cfg, divisor=64, every=10):
     return res
 
 
-def e2e_measure(h, cfg, st, K, world):
+def e2e_measure(h, cfg, st, K, world, tuned=None):
     """The same metric through the C-ABI with host buffers: upload from pinned memory, K steps as
     advance_by(inner_Nt) chunks with the recorder downloads (fields, sources, moments) after each,
     particles back at the end, all host buffers pinned and owned by the caller; wall clock, max over
-    ranks."""
+    ranks.  The run is configured (h1d_configure) with the sort interval and CTAs the autotuner
+    chose for the device-timed run (`tuned`), as a caller would after tuning once."""
     import numpy as np
     import torch
     import torch.distributed as dist
@@ -561,12 +562,16 @@ def e2e_measure(h, cfg, st, K, world):
     pinned = [pinned_like(p, True) for p in st["particles"]]
     back = [pinned_like(p, False) for p in st["particles"]]
     M = st["B"].shape[0]
-    grids = dict(B=np.empty((M, 3)), E=np.empty((M, 3)), rho=np.empty(M), J=np.empty((M, 3)),
-                 n=np.empty(M), nV=np.empty((M, 3)), nvv=np.empty((M, 6)))
-    for g in grids.values():
-        g.fill(0.0)
+
+    def pinned_grid(*shape):
+        return torch.zeros(*shape, dtype=torch.float64, pin_memory=True).numpy()
+
+    grids = dict(B=pinned_grid(M, 3), E=pinned_grid(M, 3), rho=pinned_grid(M), J=pinned_grid(M, 3),
+                 n=pinned_grid(M), nV=pinned_grid(M, 3), nvv=pinned_grid(M, 6))
     inner = cfg.inner_Nt
     with h.open_run(cfg) as r2:
+        if tuned:
+            h.abi.configure(r2, sort_interval=tuned["sort_interval"], push_ctas_per_sm=tuned["ctas_per_sm"])
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
@@ -598,7 +603,8 @@ def e2e_measure(h, cfg, st, K, world):
     return {"value": n_particles * K * world / e2e_s, "unit": METRIC, "h2d_bytes_per_step": h2d / K,
             "d2h_bytes_per_step": d2h / K,
             "note": f"FP64 host buffers in pinned memory; upload, {K} steps as advance_by({inner}) chunks with "
-                    "field/source/moment downloads after each chunk, particle download at the end"}
+                    "field/source/moment downloads after each chunk, particle download at the end; sort interval "
+                    "and CTAs as the autotuner chose for the device-timed run"}
 
 
 def ensemble_measure(h, precision, steps=500, members=64):
@@ -833,7 +839,7 @@ def main():
                                "roofline": roofline_of(prof2, "fp64", k2, traffic, c2.name)}
             del st2
 
-    e2e = None if args.no_e2e else e2e_measure(h, cfg, st, args.steps, world)
+    e2e = None if args.no_e2e else e2e_measure(h, cfg, st, args.steps, world, tuned)
     del st
 
     if not args.no_ensemble:
