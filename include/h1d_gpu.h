@@ -243,7 +243,10 @@ int h1d_download_fields(h1d_run *run, double *B, double *E);
 /* Domain::charge and Domain::current after the last step ((Nx+2*H1D_PAD) and *3 doubles) */
 int h1d_download_sources(h1d_run *run, double *charge, double *current);
 /* Species::moment<0..2>() of kinetic species `s` after the post-process collect_all
- * (PartSpecies.cc:129-143, 225-244, always CIC) and boundary_gather; any pointer may be NULL */
+ * (PartSpecies.cc:129-143, 225-244, always CIC) and boundary_gather; any pointer may be NULL.
+ * On a CAM-CL run whose species are all CIC with fixed weights, the last step of h1d_advance
+ * forms these sums in its particle pass; otherwise they are computed here, after a sort of the
+ * particles that moved since their last one. */
 int h1d_download_moments(h1d_run *run, int s, double *n, double *nV, double *nvv);
 /* cold species moments after collect_all (ColdSpecies.cc:48-77) and mom0_full/mom1_full */
 int h1d_download_cold(h1d_run *run, int i, double *n, double *nV, double *nvv, double *n_full,
