@@ -22,8 +22,7 @@ CITE = re.compile(r"(?<![\w/.-])((?:[A-Za-z0-9_-]+/)*[A-Za-z0-9_-]+\.(?:cc|hh|h|
 BARE = re.compile(r"(?<=[\s(`]):(\d+(?:-\d+)?(?:,\s*\d+(?:-\d+)?)*)")
 # sources of this repository that may be cited with line numbers too
 OWN = {"h1d_gpu.h", "h1d_oracle.c", "ref_driver.cc", "HDF5Kit.h", "DESIGN.md", "INTEGRATION.md", "README.md",
-       "SURVEY.md", "BASELINE.md", "VERDICT.md", "ADVICE.md", "Inputs.h.in", "domain_gpu.h", "Domain_GPU.h",
-       "Domain_GPU.cc", "h1d_adapter.cc"}
+       "Inputs.h.in", "Domain_GPU.h", "Domain_GPU.cc"}
 SCANNED_DIRS = ("hybrid_code-hfemic_wave_b200", "include", "oracle", "tests", "adapter")
 SCANNED_TOP = ("bench.py", "__graft_entry__.py", "DESIGN.md", "INTEGRATION.md", "README.md")
 SUFFIXES = (".py", ".cu", ".cuh", ".h", ".hh", ".cc", ".c", ".md", "Makefile")
