@@ -481,6 +481,9 @@ double *dep_ptr(h1d_run *run, int s, int set, int d, int q)
     return run->sp[s].dep + ((static_cast<size_t>(set) * 2 + d) * 4 + q) * run->M + PAD;
 }
 
+// the end of the fixed-point grid, Nx 2^F (below 2^31 by the choice of F)
+int32_t pos_len(h1d_run const *run) { return static_cast<int32_t>(run->Nx << run->fbits); }
+
 int ppt_for(h1d_run const *run, int s)
 {
     return mom_ppt(static_cast<double>(run->sp[s].n) / static_cast<double>(run->Nx));
@@ -1999,7 +2002,7 @@ int h1d_upload_particles(h1d_run *run, int s, int64_t n, double const *q1, doubl
                 CU(cudaMemcpyAsync(run->stage, src[k] + o, sizeof(double) * c, cudaMemcpyHostToDevice, run->stream));
                 if (k == 0)
                     q1_to_pos_kernel<<<nb, 256, 0, run->stream>>>(run->stage, c, -0.5 * run->Nx, run->pos_scale,
-                                                                  S.pos[0] + o);
+                                                                  pos_len(run), S.pos[0] + o);
                 else
                     to_f32_kernel<<<nb, 256, 0, run->stream>>>(run->stage, c, S.fbuf[0][k - 1] + o);
                 CU(cudaGetLastError());
@@ -2111,7 +2114,7 @@ int h1d_populate(h1d_run *run, int s, int64_t n, uint64_t seed, double beta1, do
     a.q1min = q1min, a.q1max_in = std::nextafter(q1max, q1min), a.full_min = q1min;
     if (run->mixed)
         a.pos = S.pos[0], a.fvx = S.fbuf[0][0], a.fvy = S.fbuf[0][1], a.fvz = S.fbuf[0][2], a.fw = S.fbuf[0][3],
-        a.scale = run->pos_scale;
+        a.scale = run->pos_scale, a.len = pos_len(run);
     else
         a.q1 = S.buf[0][0], a.vx = S.buf[0][1], a.vy = S.buf[0][2], a.vz = S.buf[0][3], a.w = S.buf[0][4];
     if (n) {

@@ -223,18 +223,25 @@ __global__ void __launch_bounds__(MOM_THREADS, mom_min_blocks<Args>) moments_ker
 
 // FP64 host-layout particles <-> mixed-precision particles (upload and download), one component at
 // a time so that the FP64 staging buffer holds a single array: position q1 <-> the fixed-point
-// X = round((q1 - q1min) 2^F), and velocity / weight components FP64 <-> FP32
-__device__ __forceinline__ int32_t q1_to_pos(double q1, double full_min, double scale)
+// X = round((q1 - q1min) 2^F), and velocity / weight components FP64 <-> FP32.  The grid is
+// [0, len) with len = Nx 2^F; a position inside it (q1 < q1max) that rounds up to len, i.e. lies
+// within half a step of q1max (or one ulp below it, where q1 - q1min itself rounds to Nx),
+// becomes the last position len - 1, so that it stays inside.
+__device__ __forceinline__ int32_t q1_to_pos(double q1, double full_min, double scale, int32_t len)
 {
     double const y  = (q1 - full_min) * scale;
     bool const   ok = y > -1073741824.0 && y < 2147483520.0; // NaN and lost positions map outside the grid
-    return ok ? static_cast<int32_t>(__double2ll_rn(y)) : -0x40000000;
+    if (!ok)
+        return -0x40000000;
+    int32_t const X      = static_cast<int32_t>(__double2ll_rn(y));
+    bool const    inside = q1 < full_min + static_cast<double>(len) / scale; // q1 < q1max, exactly
+    return X >= len && inside ? len - 1 : X;
 }
-__global__ void q1_to_pos_kernel(double const *q1, int64_t n, double full_min, double scale, int32_t *pos)
+__global__ void q1_to_pos_kernel(double const *q1, int64_t n, double full_min, double scale, int32_t len, int32_t *pos)
 {
     int64_t const i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i < n)
-        pos[i] = q1_to_pos(q1[i], full_min, scale);
+        pos[i] = q1_to_pos(q1[i], full_min, scale, len);
 }
 __global__ void to_f32_kernel(double const *src, int64_t n, float *dst)
 {
@@ -278,6 +285,7 @@ struct PopulateArgs {
     int32_t *pos;                                    // mixed-precision storage
     float   *fvx, *fvy, *fvz, *fw;
     double   scale;                                  // 2^F of the fixed-point positions
+    int32_t  len;                                    // Nx 2^F, the end of the fixed-point grid
 };
 
 __device__ __forceinline__ double radical_inverse_dev(uint64_t k, unsigned base)
@@ -335,7 +343,7 @@ __global__ void populate_kernel(PopulateArgs a)
     if (a.q1) {
         a.q1[i] = q1, a.vx[i] = vx, a.vy[i] = vy, a.vz[i] = vz, a.w[i] = 1.0;
     } else {
-        a.pos[i] = q1_to_pos(q1, a.full_min, a.scale);
+        a.pos[i] = q1_to_pos(q1, a.full_min, a.scale, a.len);
         a.fvx[i] = static_cast<float>(vx), a.fvy[i] = static_cast<float>(vy), a.fvz[i] = static_cast<float>(vz);
         a.fw[i] = 1.0f;
     }

@@ -141,10 +141,14 @@ __device__ __forceinline__ uint32_t key_of(SortKeys const &s, KeyRaw<KIND> const
         bool     dead, lost;
         uint32_t k;
         if constexpr (KIND == KEYS_FP64) {
+            // inside the grid is q1min <= q1 < q1max, as the boundary pass tests it
+            // (Delegate.cc:33-50); one ulp below q1max, q1 - q1min may round up to Nx, and such a
+            // particle is in the last cell
             double const f = floor(r.q - s.full_min);
             dead           = s.absorbing && r.w == 0.0;
-            lost           = !(f >= 0.0 && f < static_cast<double>(s.Nx));
-            k              = lost ? (f >= 0.0 ? static_cast<uint32_t>(s.Nx - 1) : 0u) : static_cast<uint32_t>(f);
+            lost           = !(r.q >= s.full_min && r.q < s.full_min + static_cast<double>(s.Nx));
+            k = lost || f >= static_cast<double>(s.Nx) ? (f >= 0.0 ? static_cast<uint32_t>(s.Nx - 1) : 0u)
+                                                       : static_cast<uint32_t>(f);
         } else {
             dead = s.absorbing && r.w == 0.0f;
             lost = r.c < 0 || r.c >= s.Nx;

@@ -50,6 +50,21 @@ def test_one_step(name, gpu_lib, oracle_lib):
         assert rel_err(eg[key], ec[key]) <= TOL1, key
 
 
+@pytest.mark.parametrize("name", ["p1_cic_periodic", "p2_tsc_mirror_reflecting"])
+def test_particle_one_ulp_below_q1max(name, gpu_lib, oracle_lib):
+    """q1 one ulp below q1max is inside the grid (the boundary pass keeps q1 < q1max), although
+    q1 - q1min rounds up to Nx there: the sort (every step here) puts it in the last cell, and the
+    step matches the oracle at the one-step bar."""
+    cfg = h.configs.PARITY[name]().replace(sort_interval=1)
+    init = read_state(os.path.join(GOLDEN, f"{name}.init.bin"))
+    init["particles"][0]["q1"][:2] = [np.nextafter(cfg.q1max, -np.inf), cfg.q1max - 1e-13]
+    assert init["particles"][0]["q1"][0] - cfg.q1min == cfg.Nx  # the subtraction rounds up
+    g, c, eg, ec = run_both(cfg, init, 1, gpu_lib, oracle_lib)
+    errs = state_errors(g, c, cfg)
+    bad = {k: v for k, v in errs.items() if not v <= TOL1}
+    assert not bad, bad
+
+
 @pytest.mark.parametrize("name", ALL)
 def test_ten_steps(name, gpu_lib, oracle_lib):
     cfg = h.configs.PARITY[name]()
