@@ -224,9 +224,9 @@ __global__ void __launch_bounds__(MOM_THREADS, mom_min_blocks<Args>) moments_ker
 // FP64 host-layout particles <-> mixed-precision particles (upload and download), one component at
 // a time so that the FP64 staging buffer holds a single array: position q1 <-> the fixed-point
 // X = round((q1 - q1min) 2^F), and velocity / weight components FP64 <-> FP32.  The grid is
-// [0, len) with len = Nx 2^F; a position inside it (q1 < q1max) that rounds up to len, i.e. lies
-// within half a step of q1max (or one ulp below it, where q1 - q1min itself rounds to Nx),
-// becomes the last position len - 1, so that it stays inside.
+// [0, len) with len = Nx 2^F; a position q1 <= q1max that rounds up to len (within half a step of
+// q1max, one ulp below it where q1 - q1min itself rounds to Nx, or q1max itself, where a wrap or
+// reflection of the boundary pass can round) becomes the last position len - 1, inside the grid.
 __device__ __forceinline__ int32_t q1_to_pos(double q1, double full_min, double scale, int32_t len)
 {
     double const y  = (q1 - full_min) * scale;
@@ -234,7 +234,7 @@ __device__ __forceinline__ int32_t q1_to_pos(double q1, double full_min, double 
     if (!ok)
         return -0x40000000;
     int32_t const X      = static_cast<int32_t>(__double2ll_rn(y));
-    bool const    inside = q1 < full_min + static_cast<double>(len) / scale; // q1 < q1max, exactly
+    bool const    inside = q1 <= full_min + static_cast<double>(len) / scale; // q1 <= q1max, exactly
     return X >= len && inside ? len - 1 : X;
 }
 __global__ void q1_to_pos_kernel(double const *q1, int64_t n, double full_min, double scale, int32_t len, int32_t *pos)

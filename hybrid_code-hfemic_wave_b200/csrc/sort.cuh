@@ -141,12 +141,14 @@ __device__ __forceinline__ uint32_t key_of(SortKeys const &s, KeyRaw<KIND> const
         bool     dead, lost;
         uint32_t k;
         if constexpr (KIND == KEYS_FP64) {
-            // inside the grid is q1min <= q1 < q1max, as the boundary pass tests it
-            // (Delegate.cc:33-50); one ulp below q1max, q1 - q1min may round up to Nx, and such a
-            // particle is in the last cell
+            // a kept particle lies in q1min <= q1 <= q1max: the boundary pass (Delegate.cc:33-50,
+            // 101-145) leaves q1 < q1max, except that its wrap or reflection can round to q1max
+            // itself, which the reference deposits into the ghost cell and wraps on the next pass.
+            // Such a particle, and one an ulp below q1max where q1 - q1min rounds up to Nx, sorts
+            // into the last cell.
             double const f = floor(r.q - s.full_min);
             dead           = s.absorbing && r.w == 0.0;
-            lost           = !(r.q >= s.full_min && r.q < s.full_min + static_cast<double>(s.Nx));
+            lost           = !(r.q >= s.full_min && r.q <= s.full_min + static_cast<double>(s.Nx));
             k = lost || f >= static_cast<double>(s.Nx) ? (f >= 0.0 ? static_cast<uint32_t>(s.Nx - 1) : 0u)
                                                        : static_cast<uint32_t>(f);
         } else {

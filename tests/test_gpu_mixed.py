@@ -117,21 +117,21 @@ def test_mixed_upload_download_round_trip(gpu_lib):
 
 @pytest.mark.parametrize("name", ["p1_cic_periodic", "p2_tsc_mirror_reflecting"])
 def test_mixed_right_edge_stays_inside(gpu_lib, name):
-    """A position inside the grid within half a fixed-point step of q1max rounds up to Nx 2^F, one
-    past the grid; upload (like the device loader, through the same conversion) keeps it on the last
-    position Nx 2^F - 1, in cell Nx - 1, and the run sorts and steps it as an ordinary particle."""
+    """A position within half a fixed-point step of q1max, or q1max itself (where the boundary
+    pass's wrap can round to), rounds to Nx 2^F, one past the grid; upload (like the device loader,
+    through the same conversion) keeps it on the last position Nx 2^F - 1, in cell Nx - 1, and the
+    run sorts and steps it as an ordinary particle."""
     cfg = h.configs.PARITY[name]().replace(precision=MIXED, sort_interval=1)
     init = read_state(os.path.join(GOLDEN, f"{name}.init.bin"))
     step = 2.0 ** -h.configs.position_fraction_bits(cfg.Nx)
-    edge = [np.nextafter(cfg.q1max, -np.inf), cfg.q1max - 0.25 * step, cfg.q1max - 0.49 * step]
+    edge = [np.nextafter(cfg.q1max, -np.inf), cfg.q1max - 0.25 * step, cfg.q1max - 0.49 * step, cfg.q1max]
     q1 = init["particles"][0]["q1"]
-    q1[:3] = edge
-    assert np.all(q1[:3] < cfg.q1max)
+    q1[:4] = edge
     with h.Run(cfg, gpu_lib, "h1d_") as m:
         m.upload_state(init)
         p = m.particles(0)  # upload order until the first sort
-        np.testing.assert_array_equal(p["pid"][:3], [0, 1, 2])
-        got = p["q1"][:3]
+        np.testing.assert_array_equal(p["pid"][:4], [0, 1, 2, 3])
+        got = p["q1"][:4]
         assert np.all(got < cfg.q1max) and np.all(got >= cfg.q1max - step)
         assert np.all(np.floor(got - cfg.q1min) == cfg.Nx - 1)
         m.advance(2)  # sorts (interval 1) and pushes them: no particle is reported outside the grid

@@ -51,13 +51,14 @@ def test_one_step(name, gpu_lib, oracle_lib):
 
 
 @pytest.mark.parametrize("name", ["p1_cic_periodic", "p2_tsc_mirror_reflecting"])
-def test_particle_one_ulp_below_q1max(name, gpu_lib, oracle_lib):
-    """q1 one ulp below q1max is inside the grid (the boundary pass keeps q1 < q1max), although
-    q1 - q1min rounds up to Nx there: the sort (every step here) puts it in the last cell, and the
-    step matches the oracle at the one-step bar."""
+def test_particles_at_the_right_end(name, gpu_lib, oracle_lib):
+    """q1 one ulp below q1max is inside the grid although q1 - q1min rounds up to Nx there, and q1
+    = q1max itself is where the boundary pass's wrap or reflection can round to (the reference
+    deposits such a particle into the ghost cell and wraps it on its next pass): the sort (every
+    step here) puts both in the last cell, and the step matches the oracle at the one-step bar."""
     cfg = h.configs.PARITY[name]().replace(sort_interval=1)
     init = read_state(os.path.join(GOLDEN, f"{name}.init.bin"))
-    init["particles"][0]["q1"][:2] = [np.nextafter(cfg.q1max, -np.inf), cfg.q1max - 1e-13]
+    init["particles"][0]["q1"][:3] = [np.nextafter(cfg.q1max, -np.inf), cfg.q1max - 1e-13, cfg.q1max]
     assert init["particles"][0]["q1"][0] - cfg.q1min == cfg.Nx  # the subtraction rounds up
     g, c, eg, ec = run_both(cfg, init, 1, gpu_lib, oracle_lib)
     errs = state_errors(g, c, cfg)
