@@ -6,7 +6,8 @@ C library).  Tolerances: positions within 1e-12 (absolute, in cells), velocities
 (max-norm relative); in mixed precision the position is the host position rounded to the nearest
 2^-F cell (F = configs.position_fraction_bits(Nx)), so the cell index of every particle equals
 floor(q1 - q1min) of the host position except within half a step 2^-F of a cell boundary, where
-rounding may carry it across, and the velocities equal the host's FP32 rounding.
+rounding may carry it across (within half a step of q1max the position stays on the grid's last
+position, up to one step away), and the velocities equal the host's FP32 rounding.
 """
 import numpy as np
 import pytest
@@ -39,7 +40,11 @@ def test_populate_matches_host_loader(gpu_lib, xi, precision):
         near = np.abs(x - np.round(x)) <= tol
         cell_d = np.floor(dev["q1"] - cfg.q1min)
         assert np.array_equal(cell_d[~near], np.floor(x)[~near])
-        assert np.max(np.abs(dev["q1"] - host["q1"])) <= tol
+        # within half a step of q1max the position is kept on the grid's last position instead
+        edge = x > cfg.Nx - tol
+        assert np.max(np.abs(dev["q1"] - host["q1"])[~edge], initial=0.0) <= tol
+        assert np.max(np.abs(dev["q1"] - host["q1"])[edge], initial=0.0) <= step + 1e-11
+        assert np.all(dev["q1"] < cfg.q1max)
         for key in ("vx", "vy", "vz"):
             assert rel_err(dev[key], host[key].astype(np.float32)) <= 1e-6, key
     assert np.all(dev["w"] == 1.0)
