@@ -29,6 +29,144 @@ using namespace h1d;
 
 namespace {
 
+// ------------------------------------------------------------------------------------------------
+// Device memory of the library.  Runs, batches and served requests come and go, and each holds
+// tens of buffers; with cudaMalloc / cudaFree every one of them maps or unmaps device memory
+// through the driver, which on a busy host took from milliseconds up to a second per run.  So
+// the library allocates from a memory pool of its own per device that keeps freed blocks
+// (release threshold: never), with the semantics of cudaMalloc / cudaFree kept:
+//   dmalloc  a block from the pool, allocated on an internal stream that is then synchronised,
+//            so the block is usable from any stream on return;
+//   dfree    waits for the device to be idle (as cudaFree does) and returns the block to the pool.
+// Blocks the pool holds but no run uses count as free device memory for admission
+// (pool_idle_bytes).  A pinned slab holds the runs' status words (one cudaMallocHost per slab
+// of 4096 words instead of one per run).
+// ------------------------------------------------------------------------------------------------
+constexpr int MAX_DEVICES = 64;
+struct DevicePool {
+    cudaMemPool_t pool   = nullptr;
+    cudaStream_t  stream = nullptr;
+};
+std::mutex pool_mu;
+DevicePool pools[MAX_DEVICES];
+
+cudaError_t device_pool(int dev, DevicePool *&out)
+{
+    if (dev < 0 || dev >= MAX_DEVICES)
+        return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(pool_mu);
+    DevicePool &P = pools[dev];
+    if (!P.pool) {
+        cudaMemPoolProps props{};
+        props.allocType     = cudaMemAllocationTypePinned;
+        props.handleTypes   = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id   = dev;
+        cudaMemPool_t pool  = nullptr;
+        if (cudaError_t const e = cudaMemPoolCreate(&pool, &props))
+            return e;
+        uint64_t keep = UINT64_MAX;
+        cudaStream_t st = nullptr;
+        cudaError_t e   = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e == cudaSuccess)
+            e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            cudaMemPoolDestroy(pool);
+            return e;
+        }
+        P.pool = pool, P.stream = st;
+    }
+    out = &P;
+    return cudaSuccess;
+}
+
+cudaError_t dmalloc_raw(void **p, size_t bytes)
+{
+    *p      = nullptr;
+    int dev = 0;
+    if (cudaError_t const e = cudaGetDevice(&dev))
+        return e;
+    DevicePool *P = nullptr;
+    if (cudaError_t const e = device_pool(dev, P))
+        return e;
+    if (cudaError_t const e = cudaMallocFromPoolAsync(p, bytes ? bytes : 1, P->pool, P->stream)) {
+        *p = nullptr;
+        return e;
+    }
+    cudaError_t const e = cudaStreamSynchronize(P->stream);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(*p, P->stream);
+        *p = nullptr;
+    }
+    return e;
+}
+template <class T>
+cudaError_t dmalloc(T **p, size_t bytes)
+{
+    return dmalloc_raw(reinterpret_cast<void **>(p), bytes);
+}
+
+// the block goes back to the pool of the device it lives on, once the device is idle
+void dfree(void *p)
+{
+    if (!p)
+        return;
+    cudaPointerAttributes at{};
+    DevicePool           *P = nullptr;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess || device_pool(at.device, P) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(p);
+        return;
+    }
+    cudaDeviceSynchronize();
+    cudaFreeAsync(p, P->stream);
+}
+
+// device memory the library's pool on `dev` holds without a run using it
+size_t pool_idle_bytes(int dev)
+{
+    DevicePool *P = nullptr;
+    if (device_pool(dev, P) != cudaSuccess)
+        return 0;
+    uint64_t reserved = 0, used = 0;
+    if (cudaMemPoolGetAttribute(P->pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess
+        || cudaMemPoolGetAttribute(P->pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess)
+        return 0;
+    return reserved > used ? static_cast<size_t>(reserved - used) : 0;
+}
+
+// pinned status words from slabs of 4096
+struct StatusSlabs {
+    std::mutex              mu;
+    std::vector<unsigned *> slabs, free;
+};
+StatusSlabs status_slabs;
+constexpr int STATUS_SLAB = 4096;
+
+unsigned *status_word()
+{
+    std::lock_guard<std::mutex> lock(status_slabs.mu);
+    if (status_slabs.free.empty()) {
+        unsigned *slab = nullptr;
+        if (cudaMallocHost(&slab, sizeof(unsigned) * STATUS_SLAB) != cudaSuccess)
+            return nullptr;
+        status_slabs.slabs.push_back(slab);
+        for (int i = STATUS_SLAB - 1; i >= 0; --i)
+            status_slabs.free.push_back(slab + i);
+    }
+    unsigned *w = status_slabs.free.back();
+    status_slabs.free.pop_back();
+    *w = 0;
+    return w;
+}
+void release_status_word(unsigned *w)
+{
+    if (!w)
+        return;
+    std::lock_guard<std::mutex> lock(status_slabs.mu);
+    status_slabs.free.push_back(w);
+}
+
 constexpr int FIELD_BLOCK_MIN = 256;
 
 // shared memory of a field launch of L threads: the predictor-corrector layout or the CAM-CL
@@ -81,7 +219,7 @@ struct SortScratch {
     int64_t   hist_cap = 0, part_cap = 0;
     void      release()
     {
-        cudaFree(hist), cudaFree(part);
+        dfree(hist), dfree(part);
         hist = part = nullptr, hist_cap = part_cap = 0;
     }
 };
@@ -464,7 +602,7 @@ double ccf(h1d_params const &p, double Oc, double op) { return cdcf(p, Oc, op) /
 template <class T>
 int dalloc(h1d_run *run, T **ptr, size_t count)
 {
-    CU(cudaMalloc(reinterpret_cast<void **>(ptr), sizeof(T) * (count ? count : 1)));
+    CU(dmalloc(reinterpret_cast<void **>(ptr), sizeof(T) * (count ? count : 1)));
     CU(cudaMemsetAsync(*ptr, 0, sizeof(T) * (count ? count : 1), run->stream));
     return H1D_OK;
 }
@@ -597,9 +735,9 @@ cudaError_t grow(uint32_t *&buf, int64_t &cap, int64_t need)
 {
     if (need <= cap)
         return cudaSuccess;
-    cudaFree(buf);
+    dfree(buf);
     buf = nullptr, cap = 0;
-    cudaError_t const e = cudaMalloc(&buf, sizeof(uint32_t) * need);
+    cudaError_t const e = dmalloc(&buf, sizeof(uint32_t) * need);
     if (e == cudaSuccess)
         cap = need;
     return e;
@@ -1269,37 +1407,37 @@ int ensure_capacity(h1d_run *run, int s, int64_t n)
     for (int k = 0; k < 2; ++k) {
         if (run->mixed) {
             for (auto *&b : S.fbuf[k]) {
-                cudaFree(b);
+                dfree(b);
                 b = nullptr;
-                CU(cudaMalloc(&b, sizeof(float) * cap));
+                CU(dmalloc(&b, sizeof(float) * cap));
             }
-            cudaFree(S.pos[k]);
+            dfree(S.pos[k]);
             S.pos[k] = nullptr;
-            CU(cudaMalloc(&S.pos[k], sizeof(int32_t) * cap));
+            CU(dmalloc(&S.pos[k], sizeof(int32_t) * cap));
             if (evolves_psd(run->p.kinetic[s]))
                 for (auto *&b : S.fpsd[k]) {
-                    cudaFree(b);
+                    dfree(b);
                     b = nullptr;
-                    CU(cudaMalloc(&b, sizeof(float) * cap));
+                    CU(dmalloc(&b, sizeof(float) * cap));
                 }
         } else {
             for (auto *&b : S.buf[k]) {
-                cudaFree(b);
+                dfree(b);
                 b = nullptr;
-                CU(cudaMalloc(&b, sizeof(double) * cap));
+                CU(dmalloc(&b, sizeof(double) * cap));
             }
             if (evolves_psd(run->p.kinetic[s]))
                 for (auto *&b : S.psd[k]) {
-                    cudaFree(b);
+                    dfree(b);
                     b = nullptr;
-                    CU(cudaMalloc(&b, sizeof(double) * cap));
+                    CU(dmalloc(&b, sizeof(double) * cap));
                 }
         }
-        cudaFree(S.pid[k]), cudaFree(S.keys[k]), cudaFree(S.idx[k]);
+        dfree(S.pid[k]), dfree(S.keys[k]), dfree(S.idx[k]);
         S.pid[k] = nullptr, S.keys[k] = nullptr, S.idx[k] = nullptr;
-        CU(cudaMalloc(&S.pid[k], sizeof(int32_t) * cap));
-        CU(cudaMalloc(&S.keys[k], sizeof(uint32_t) * cap));
-        CU(cudaMalloc(&S.idx[k], sizeof(uint32_t) * cap));
+        CU(dmalloc(&S.pid[k], sizeof(int32_t) * cap));
+        CU(dmalloc(&S.keys[k], sizeof(uint32_t) * cap));
+        CU(dmalloc(&S.idx[k], sizeof(uint32_t) * cap));
     }
     S.cap = cap;
     return H1D_OK;
@@ -1456,10 +1594,10 @@ int build_field_tables(h1d_batch *b)
         a.fb = fb;
     size_t const smem = field_smem_bytes(L, fb);
     if (L != b->L || static_cast<int>(map.size()) != b->nblocks || !b->d_table) {
-        cudaFree(b->d_table), cudaFree(b->d_map);
+        dfree(b->d_table), dfree(b->d_map);
         b->d_table = nullptr, b->d_map = nullptr;
-        BCU(cudaMalloc(&b->d_table, sizeof(FieldArgs) * tab.size()));
-        BCU(cudaMalloc(&b->d_map, sizeof(FieldBlock) * map.size()));
+        BCU(dmalloc(&b->d_table, sizeof(FieldArgs) * tab.size()));
+        BCU(dmalloc(&b->d_map, sizeof(FieldBlock) * map.size()));
         BCU(set_field_batch_smem(smem));
         drop_graph(b);
     }
@@ -1758,8 +1896,8 @@ int h1d_math_check(double const *x, int64_t n, double *out)
     if (n == 0)
         return H1D_OK;
     double *dx = nullptr, *dout = nullptr;
-    if (cudaMalloc(&dx, sizeof(double) * n) != cudaSuccess || cudaMalloc(&dout, sizeof(double) * 5 * n) != cudaSuccess) {
-        cudaFree(dx);
+    if (dmalloc(&dx, sizeof(double) * n) != cudaSuccess || dmalloc(&dout, sizeof(double) * 5 * n) != cudaSuccess) {
+        dfree(dx);
         return H1D_ERR_OOM;
     }
     int st = H1D_OK;
@@ -1771,8 +1909,8 @@ int h1d_math_check(double const *x, int64_t n, double *out)
             || cudaMemcpy(out, dout, sizeof(double) * 5 * n, cudaMemcpyDeviceToHost) != cudaSuccess)
             st = H1D_ERR_CUDA;
     }
-    cudaFree(dx);
-    cudaFree(dout);
+    dfree(dx);
+    dfree(dout);
     return st;
 }
 
@@ -1909,7 +2047,7 @@ int h1d_create(h1d_params const *params, h1d_run **out)
         || (run->mixed && dalloc(run, &run->stage, run->stage_n))
         || (p.n_sources > 0 && dalloc(run, &run->src_dep, 4 * M * p.n_sources)))
         return fail(H1D_ERR_OOM);
-    if (cudaMallocHost(&run->h_status, sizeof(unsigned)) != cudaSuccess)
+    if (!(run->h_status = status_word()))
         return fail(H1D_ERR_OOM);
     for (int s = 0; s < p.n_kinetic; ++s) {
         SpeciesState &S = run->sp[s];
@@ -1947,31 +2085,30 @@ int h1d_destroy(h1d_run *run)
         return H1D_OK;
     if (run->stream)
         cudaStreamSynchronize(run->stream);
-    cudaFree(run->geo);
+    dfree(run->geo);
     for (int k = 0; k < 2; ++k)
-        cudaFree(run->B[k]), cudaFree(run->E[k]), cudaFree(run->E1[k]);
-    cudaFree(run->d_fallbacks);
-    cudaFree(run->EB), cudaFree(run->EBf), cudaFree(run->src_dep), cudaFree(run->charge), cudaFree(run->current), cudaFree(run->d_status), cudaFree(run->d_energy);
-    cudaFree(run->stage);
+        dfree(run->B[k]), dfree(run->E[k]), dfree(run->E1[k]);
+    dfree(run->d_fallbacks);
+    dfree(run->EB), dfree(run->EBf), dfree(run->src_dep), dfree(run->charge), dfree(run->current), dfree(run->d_status), dfree(run->d_energy);
+    dfree(run->stage);
     run->sorter.release();
-    if (run->h_status)
-        cudaFreeHost(run->h_status);
+    release_status_word(run->h_status);
     for (auto &S : run->sp) {
         for (int k = 0; k < 2; ++k) {
             for (auto *b : S.buf[k])
-                cudaFree(b);
+                dfree(b);
             for (auto *b : S.fbuf[k])
-                cudaFree(b);
-            cudaFree(S.pos[k]);
-            cudaFree(S.pid[k]), cudaFree(S.keys[k]), cudaFree(S.idx[k]);
-            cudaFree(S.psd[k][0]), cudaFree(S.psd[k][1]);
-            cudaFree(S.fpsd[k][0]), cudaFree(S.fpsd[k][1]);
+                dfree(b);
+            dfree(S.pos[k]);
+            dfree(S.pid[k]), dfree(S.keys[k]), dfree(S.idx[k]);
+            dfree(S.psd[k][0]), dfree(S.psd[k][1]);
+            dfree(S.fpsd[k][0]), dfree(S.fpsd[k][1]);
         }
-        cudaFree(S.dead), cudaFree(S.dep), cudaFree(S.mom_raw), cudaFree(S.mom);
-        cudaFree(S.eq);
+        dfree(S.dead), dfree(S.dep), dfree(S.mom_raw), dfree(S.mom);
+        dfree(S.eq);
     }
     for (auto &C : run->cold)
-        cudaFree(C.n), cudaFree(C.nV[0]), cudaFree(C.nV[1]), cudaFree(C.mom);
+        dfree(C.n), dfree(C.nV[0]), dfree(C.nV[1]), dfree(C.mom);
     for (auto &[k, b, e] : run->ev_done)
         cudaEventDestroy(b), cudaEventDestroy(e);
     for (auto e : run->ev_pool)
@@ -2408,7 +2545,7 @@ int h1d_batch_destroy(h1d_batch *b)
             b->runs[i]->sp[s].since_sort = std::min(b->runs[i]->sp[s].since_sort, b->since_block);
     }
     drop_graph(b);
-    cudaFree(b->d_table), cudaFree(b->d_map);
+    dfree(b->d_table), dfree(b->d_map);
     b->sorter.release();
     cudaStreamDestroy(b->stream);
     delete b;
@@ -2557,7 +2694,7 @@ int h1d_vhistogram(h1d_run *run, int s, double ext_loc, double ext_len, double v
     SpeciesState const &S    = run->sp[s];
     size_t const        bins = static_cast<size_t>(v1dim * v2dim);
     double             *d    = nullptr;
-    CU(cudaMalloc(&d, sizeof(double) * (3 * bins + 1)));
+    CU(dmalloc(&d, sizeof(double) * (3 * bins + 1)));
     auto *count = reinterpret_cast<unsigned long long *>(d + 3 * bins);
     int   st    = H1D_OK;
     if (cudaMemsetAsync(d, 0, sizeof(double) * (3 * bins + 1), run->stream) != cudaSuccess)
@@ -2583,7 +2720,7 @@ int h1d_vhistogram(h1d_run *run, int s, double ext_loc, double ext_len, double v
     if (st == H1D_OK && (cudaMemcpyAsync(h.data(), d, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, run->stream) != cudaSuccess
                          || cudaStreamSynchronize(run->stream) != cudaSuccess))
         st = set_err(run, H1D_ERR_CUDA, "h1d_vhistogram: copy failed");
-    cudaFree(d);
+    dfree(d);
     TRY(st);
     unsigned long long c = 0;
     std::memcpy(&c, &h[3 * bins], sizeof c);
@@ -2907,8 +3044,12 @@ int h1d_server_tick(h1d_server *sv, int *n_active, int *n_queued)
                 ++it;
                 continue;
             }
-            if (!asked)
+            if (!asked) { // free device memory, and the blocks the library's pool keeps for reuse
+                int dev = 0;
+                cudaGetDevice(&dev);
                 cudaMemGetInfo(&free_b, &total_b), asked = true;
+                free_b += pool_idle_bytes(dev);
+            }
             if (r->bytes + (size_t{ 256 } << 20) > free_b) {
                 ++it;
                 continue;
