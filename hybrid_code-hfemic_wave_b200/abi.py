@@ -631,6 +631,19 @@ def step_count(run: Run) -> int:
     return n.value
 
 
+def trim_device_memory(path: str, keep_bytes: int = 0) -> int:
+    """Return the library's unused pooled device memory on the current device to the driver,
+    keeping at most `keep_bytes` (h1d_trim_device_memory); returns the bytes the pool still holds."""
+    lib = C.CDLL(path)
+    fn = lib.h1d_trim_device_memory
+    fn.argtypes, fn.restype = [C.c_size_t, C.POINTER(C.c_size_t)], C.c_int
+    held = C.c_size_t()
+    rc = fn(keep_bytes, C.byref(held))
+    if rc != 0:
+        raise H1DError(rc, "h1d_trim_device_memory failed")
+    return held.value
+
+
 def vhistogram(run: Run, s: int, extent, v1, v2, prefix: str = "h1d_"):
     """VHistogramRecorder of kinetic species s: extent = (loc, len) in q1, v1 = (min, len, bins)
     for the parallel and v2 = (min, len, bins) for the perpendicular speed.  Returns (hist, total)

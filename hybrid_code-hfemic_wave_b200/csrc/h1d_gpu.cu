@@ -2079,6 +2079,28 @@ int h1d_create(h1d_params const *params, h1d_run **out)
     return H1D_OK;
 }
 
+int h1d_trim_device_memory(size_t keep_bytes, size_t *pool_bytes)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return H1D_ERR_NO_DEVICE;
+    }
+    DevicePool *P = nullptr;
+    if (device_pool(dev, P) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess
+        || cudaMemPoolTrimTo(P->pool, keep_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return H1D_ERR_CUDA;
+    }
+    if (pool_bytes) {
+        uint64_t reserved = 0;
+        if (cudaMemPoolGetAttribute(P->pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess)
+            return H1D_ERR_CUDA;
+        *pool_bytes = static_cast<size_t>(reserved);
+    }
+    return H1D_OK;
+}
+
 int h1d_destroy(h1d_run *run)
 {
     if (!run)

@@ -199,6 +199,15 @@ size_t h1d_params_size(void);
 int h1d_create(const h1d_params *params, h1d_run **out);
 int h1d_destroy(h1d_run *run);
 
+/* Device memory.  The library allocates its device buffers (runs, batches, served requests) from
+ * a memory pool of its own per device, which keeps the blocks a destroyed run releases for the
+ * next run instead of returning them to the driver (the reference holds its grids and particles
+ * in host containers and has no counterpart).  h1d_trim_device_memory returns the pool's unused
+ * blocks on the current device to the driver, keeping at most `keep_bytes` of them;
+ * *pool_bytes, when not null, receives the device memory the pool still holds afterwards (blocks
+ * in use included). */
+int h1d_trim_device_memory(size_t keep_bytes, size_t *pool_bytes);
+
 /* Particles of kinetic species `s` as SoA, positions q1 in [-Nx/2, Nx/2) (ParamSet.cc:22).
  * Replaces any previous particles of that species. */
 int h1d_upload_particles(h1d_run *run, int s, int64_t n, const double *q1, const double *vx,
