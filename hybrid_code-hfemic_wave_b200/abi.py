@@ -352,6 +352,7 @@ def _declare_batch(lib):
         "h1d_batch_destroy": ([v], C.c_int),
         "h1d_batch_advance": ([v, C.c_uint32], C.c_int),
         "h1d_batch_advance_async": ([v, C.c_uint32], C.c_int),
+        "h1d_batch_advance_members_async": ([v, C.POINTER(C.c_uint32)], C.c_int),
         "h1d_batch_synchronize": ([v], C.c_int),
         "h1d_batch_get_stream": ([v, C.POINTER(C.c_void_p)], C.c_int),
         "h1d_batch_configure": ([v, C.c_int, C.c_int, C.c_int], C.c_int),
@@ -414,6 +415,15 @@ class Batch:
 
     def synchronize(self):
         self._check(self.lib.h1d_batch_synchronize(self.h))
+
+    def advance_members(self, n_steps):
+        """Member i advances by n_steps[i] (h1d_batch_advance_members_async), then the batch
+        synchronises."""
+        if len(n_steps) != len(self.runs):
+            raise ValueError("advance_members: one step count per member")
+        arr = (C.c_uint32 * len(n_steps))(*[int(x) for x in n_steps])
+        self._check(self.lib.h1d_batch_advance_members_async(self.h, arr))
+        self.synchronize()
 
     def stream(self):
         s = C.c_void_p()

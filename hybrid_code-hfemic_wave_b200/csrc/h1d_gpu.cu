@@ -1480,6 +1480,8 @@ struct h1d_batch {
     SortScratch                sorter;            // the members' cell sort
     FieldArgs                 *d_table = nullptr; // CAM-CL: [parity][runs]; PC: [phase 1-3][parity][runs]
     FieldBlock                *d_map = nullptr;
+    std::vector<FieldBlock>    map_all, map_live;  // every member's field blocks / those launched now
+    std::vector<char>          active;             // members the next steps advance (all when empty)
     int                        parity = 0;
     cudaGraph_t                graph = nullptr;
     cudaGraphExec_t            exec = nullptr;
@@ -1511,6 +1513,9 @@ int bset_err(h1d_batch *b, int code, std::string const &m)
         if (st_ != H1D_OK)                                                                                   \
             return bset_err(b, st_, (r)->msg);                                                               \
     } while (0)
+
+// whether member i takes the next step (every member, unless an advance by member counts runs)
+bool member_on(h1d_batch const *b, size_t i) { return b->active.empty() || b->active[i]; }
 
 bool graph_eligible(h1d_batch const *b)
 {
@@ -1602,6 +1607,7 @@ int build_field_tables(h1d_batch *b)
         drop_graph(b);
     }
     b->L = L, b->nblocks = static_cast<int>(map.size()), b->smem = smem, b->parity = 0;
+    b->map_all = map, b->active.clear();
     BCU(cudaMemcpyAsync(b->d_table, tab.data(), sizeof(FieldArgs) * tab.size(), cudaMemcpyHostToDevice, b->stream));
     BCU(cudaMemcpyAsync(b->d_map, map.data(), sizeof(FieldBlock) * map.size(), cudaMemcpyHostToDevice, b->stream));
     BCU(cudaStreamSynchronize(b->stream));
@@ -1614,10 +1620,12 @@ int batch_sort_block(h1d_batch *b)
 {
     if (b->since_block >= b->k) {
         std::vector<SortItem> items;
-        for (h1d_run *r : b->runs)
-            for (int s = 0; s < r->p.n_kinetic; ++s)
-                items.push_back({ r, s });
-        BCU(sort_items(items, b->sorter, b->stream, b->stats.kernel_launches));
+        for (size_t i = 0; i < b->runs.size(); ++i)
+            if (member_on(b, i))
+                for (int s = 0; s < b->runs[i]->p.n_kinetic; ++s)
+                    items.push_back({ b->runs[i], s });
+        if (!items.empty())
+            BCU(sort_items(items, b->sorter, b->stream, b->stats.kernel_launches));
         b->since_block = 0;
     }
     return H1D_OK;
@@ -1638,7 +1646,10 @@ int batch_push(h1d_batch *b, int pass)
     std::vector<Kind>                       kinds;
     std::vector<std::vector<PushArgs>>      fp;
     std::vector<std::vector<PushArgsMixed>> mx;
-    for (h1d_run *r : b->runs)
+    for (size_t i = 0; i < b->runs.size(); ++i) {
+        if (!member_on(b, i))
+            continue;
+        h1d_run *r = b->runs[i];
         for (int s = 0; s < r->p.n_kinetic; ++s) {
             if (r->sp[s].n == 0)
                 continue;
@@ -1660,6 +1671,7 @@ int batch_push(h1d_batch *b, int pass)
             else
                 fp[ki].push_back(a);
         }
+    }
     for (size_t ki = 0; ki < kinds.size(); ++ki) {
         Kind const &kd = kinds[ki];
         if (kd.mixed)
@@ -1678,7 +1690,10 @@ int batch_push(h1d_batch *b, int pass)
 // the host side of one step of every member
 void batch_step_done(h1d_batch *b)
 {
-    for (h1d_run *r : b->runs) {
+    for (size_t i = 0; i < b->runs.size(); ++i) {
+        if (!member_on(b, i))
+            continue;
+        h1d_run *r = b->runs[i];
         r->fcur ^= 1;
         if (!b->pc)
             r->dset ^= 1;
@@ -1703,8 +1718,8 @@ int batch_step_pc(h1d_batch *b)
     auto const   table = [&](int phase) { return b->d_table + ((phase - 1) * 2 + b->parity) * R; };
     BCU(launch_pc_fields_batch(table(1), b->d_map, b->nblocks, b->L, b->smem, b->stream));
     TRY(batch_push(b, 0));
-    for (h1d_run *r : b->runs)
-        if (r->p.n_sources > 0) {
+    for (size_t i = 0; i < b->runs.size(); ++i)
+        if (h1d_run *r = b->runs[i]; member_on(b, i) && r->p.n_sources > 0) {
             BTRY(r, launch_run_sources(r, static_cast<double>(r->step) * r->p.dt + r->p.dt));
             b->stats.kernel_launches += 1;
         }
@@ -1724,8 +1739,8 @@ int batch_step(h1d_batch *b)
     TRY(batch_sort_block(b));
     TRY(batch_push(b, -1));
     // external sources of the members that have them, then the field cycle of every member
-    for (h1d_run *r : b->runs)
-        if (r->p.n_sources > 0) {
+    for (size_t i = 0; i < b->runs.size(); ++i)
+        if (h1d_run *r = b->runs[i]; member_on(b, i) && r->p.n_sources > 0) {
             BTRY(r, launch_run_sources(r, static_cast<double>(r->step) * r->p.dt + 0.5 * r->p.dt));
             b->stats.kernel_launches += 1;
         }
@@ -1830,6 +1845,75 @@ int batch_advance(h1d_batch *b, uint32_t n_steps)
         if (int const st = batch_step(b))
             return st;
     return H1D_OK;
+}
+
+// the members the next steps advance (on[i] != 0), and the field launch's blocks to match: the
+// block map keeps only their blocks (each block still names its member's table entry)
+int batch_set_active(h1d_batch *b, std::vector<char> const &on)
+{
+    b->active = on;
+    b->map_live.clear();
+    for (FieldBlock const &f : b->map_all)
+        if (on[static_cast<size_t>(f.run)])
+            b->map_live.push_back(f);
+    b->nblocks = static_cast<int>(b->map_live.size());
+    if (b->nblocks > 0)
+        BCU(cudaMemcpyAsync(b->d_map, b->map_live.data(), sizeof(FieldBlock) * b->map_live.size(),
+                            cudaMemcpyHostToDevice, b->stream));
+    return H1D_OK;
+}
+int batch_set_all(h1d_batch *b)
+{
+    b->active.clear();
+    b->nblocks = static_cast<int>(b->map_all.size());
+    if (b->nblocks > 0)
+        BCU(cudaMemcpyAsync(b->d_map, b->map_all.data(), sizeof(FieldBlock) * b->map_all.size(),
+                            cudaMemcpyHostToDevice, b->stream));
+    return H1D_OK;
+}
+
+// advance member i by steps[i] (eager steps): every member steps until the smallest count is
+// reached, that member drops out of the particle passes, the sorts and the field launch, and the
+// others go on; each member's state is then that of its own advance_by(steps[i])
+int batch_advance_members(h1d_batch *b, uint32_t const *steps)
+{
+    size_t const R = b->runs.size();
+    uint32_t     n = 0;
+    for (size_t i = 0; i < R; ++i)
+        n = std::max(n, steps[i]);
+    bool uniform = true;
+    for (size_t i = 0; i < R; ++i)
+        uniform = uniform && steps[i] == n;
+    if (uniform)
+        return batch_advance(b, n);
+    for (h1d_run *r : b->runs)
+        r->profiling = false;
+    std::vector<h1d_run *> moving;
+    for (size_t i = 0; i < R; ++i)
+        if (steps[i] > 0)
+            moving.push_back(b->runs[i]);
+    std::vector<h1d_run *> const all = b->runs;
+    b->runs                          = moving; // members that do not step are not prepared either
+    int st                           = batch_prepare(b);
+    b->runs                          = all;
+    if (st != H1D_OK)
+        return st;
+    TRY(build_field_tables(b));
+    std::vector<char> on(R, 0);
+    uint32_t          done = 0;
+    while (st == H1D_OK && done < n) {
+        uint32_t next = n; // the next count at which a member stops
+        for (size_t i = 0; i < R; ++i) {
+            on[i] = steps[i] > done;
+            if (on[i])
+                next = std::min(next, steps[i]);
+        }
+        st = batch_set_active(b, on);
+        for (; st == H1D_OK && done < next; ++done)
+            st = batch_step(b);
+    }
+    int const back = batch_set_all(b);
+    return st != H1D_OK ? st : back;
 }
 
 int batch_check(h1d_batch *b)
@@ -2581,6 +2665,13 @@ int h1d_batch_advance_async(h1d_batch *b, uint32_t n_steps)
     return batch_advance(b, n_steps);
 }
 
+int h1d_batch_advance_members_async(h1d_batch *b, uint32_t const *n_steps)
+{
+    if (!b || !n_steps)
+        return H1D_ERR_INVALID_ARG;
+    return batch_advance_members(b, n_steps);
+}
+
 int h1d_batch_synchronize(h1d_batch *b)
 {
     if (!b)
@@ -2813,7 +2904,7 @@ struct ServerReq {
     h1d_request         rq{};
     size_t              bytes = 0;
     int                 state = H1D_REQ_QUEUED, status = H1D_OK;
-    uint32_t            done_steps = 0;
+    uint32_t            done_steps = 0, tick_steps = 0; // steps taken / steps of the current tick
     h1d_run            *run = nullptr;
     double              t_submit = 0, t_admit = 0, t_done = 0;
     std::vector<double> B, E, energy, n, nV, nvv;
@@ -3044,14 +3135,20 @@ int h1d_server_tick(h1d_server *sv, int *n_active, int *n_queued)
         sv->stats.batches_built++;
     }
 
-    // 2. the quantum of every batch (up to the nearest completion), enqueued without waiting
-    uint32_t q = static_cast<uint32_t>(sv->quantum);
-    for (ServerReq *r : sv->active)
-        q = std::min(q, r->rq.n_steps - r->done_steps);
+    // 2. the quantum of every batch, enqueued without waiting: each member advances by the quantum
+    // or by the steps it has left, whichever is fewer (members in the order their batch was built)
     int launched[2] = { H1D_OK, H1D_OK };
-    for (int alg = 0; alg < 2; ++alg)
-        if (sv->batch[alg])
-            launched[alg] = h1d_batch_advance_async(sv->batch[alg], q);
+    for (int alg = 0; alg < 2; ++alg) {
+        if (!sv->batch[alg])
+            continue;
+        std::vector<uint32_t> steps;
+        for (ServerReq *r : sv->active)
+            if (r->rq.params.algorithm == alg) {
+                r->tick_steps = std::min(static_cast<uint32_t>(sv->quantum), r->rq.n_steps - r->done_steps);
+                steps.push_back(r->tick_steps);
+            }
+        launched[alg] = h1d_batch_advance_members_async(sv->batch[alg], steps.data());
+    }
 
     // 3. admission while the batches run: every queued request that fits the budget (in arrival
     // order) and the device, its memory reserved under the lock, its run built outside it
@@ -3105,7 +3202,7 @@ int h1d_server_tick(h1d_server *sv, int *n_active, int *n_queued)
             if (r->rq.params.algorithm != alg)
                 continue;
             if (st == H1D_OK) {
-                r->done_steps += q;
+                r->done_steps += r->tick_steps;
                 continue;
             }
             // a failed launch fails every member; otherwise only the members whose run reports an error
@@ -3113,7 +3210,7 @@ int h1d_server_tick(h1d_server *sv, int *n_active, int *n_queued)
             if (own != H1D_OK)
                 ended.push_back({ r, own }), r->msg = h1d_status_string(r->run);
             else
-                r->done_steps += q;
+                r->done_steps += r->tick_steps;
         }
     }
 

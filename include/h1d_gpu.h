@@ -370,6 +370,12 @@ int h1d_batch_create(h1d_run *const *runs, int n_runs, h1d_batch **out);
 int h1d_batch_destroy(h1d_batch *batch);
 int h1d_batch_advance(h1d_batch *batch, uint32_t n_steps);
 int h1d_batch_advance_async(h1d_batch *batch, uint32_t n_steps);
+/* Member i (in the order given to h1d_batch_create) advances by n_steps[i]: all members step
+ * together until the smallest count is reached, then that member leaves the particle passes, the
+ * sorts and the field launch, and the rest go on, so each member ends as its own
+ * advance_by(n_steps[i]) would leave it (a count of 0 leaves a member as it was).  Steps are eager
+ * when the counts differ; equal counts are h1d_batch_advance_async. */
+int h1d_batch_advance_members_async(h1d_batch *batch, const uint32_t *n_steps);
 int h1d_batch_synchronize(h1d_batch *batch);
 int h1d_batch_get_stream(h1d_batch *batch, void **stream);
 /* sort_interval > 0 sets the block length (0 keeps it); push_ctas_per_sm as in h1d_configure;

@@ -299,3 +299,63 @@ def test_batch_sort_is_each_members_stable_cell_sort(gpu_lib):
     finally:
         for r in runs:
             r.close()
+
+
+def _alone(gpu_lib, cfgs, states, totals):
+    out = []
+    for c, st, n in zip(cfgs, states, totals):
+        with h.Run(c, gpu_lib) as r:
+            h.abi.configure(r, sort_interval=4)
+            r.upload_state(st)
+            if n:
+                r.advance(n)
+            out.append(r.state())
+    return out
+
+
+def _members_by_counts(gpu_lib, cfgs, states, counts, then):
+    runs = [h.Run(c, gpu_lib) for c in cfgs]
+    try:
+        for r, st in zip(runs, states):
+            h.abi.configure(r, sort_interval=4)
+            r.upload_state(st)
+        with h.abi.Batch(runs) as b:
+            b.configure(sort_interval=4)
+            b.advance_members(counts)  # each member by its own count, eager
+            b.advance(then)            # then all together again, graph pairs included
+            steps = [h.abi.step_count(r) for r in runs]
+            together = [r.state() for r in runs]
+    finally:
+        for r in runs:
+            r.close()
+    return steps, together
+
+
+@pytest.mark.parametrize("precision,tol", [(h.configs.PREC_FP64, 1e-10), (h.configs.PREC_MIXED, 1e-4)])
+def test_batch_members_advance_by_their_own_counts(gpu_lib, precision, tol):
+    """h1d_batch_advance_members_async: members advanced by 13, 40, 0 and 27 steps (the one with 0
+    stays as it was), then all by 17 more, equal each run advanced alone by its total."""
+    cfgs, states = _members(precision)
+    counts, then = [13, 40, 0, 27], 17
+    totals = [c + then for c in counts]
+    steps, together = _members_by_counts(gpu_lib, cfgs, states, counts, then)
+    assert steps == totals
+    for c, a, t in zip(cfgs, _alone(gpu_lib, cfgs, states, totals), together):
+        errs = _field_errs(t, a, c)
+        assert max(errs.values()) <= tol, (c.name, errs)
+        pa, pt = by_pid(a["particles"][0]), by_pid(t["particles"][0])
+        assert rel_err(pt["vx"], pa["vx"]) <= tol
+
+
+def test_pc_batch_members_advance_by_their_own_counts(gpu_lib):
+    """The same for predictor-corrector members (TSC mirror reflecting; delta-f periodic)."""
+    names = ["p4_pc_tsc_mirror_reflecting", "p8_pc_psd_periodic"]
+    cfgs, states = _fixture_members(names, h.configs.PREC_FP64)
+    counts, then = [7, 12], 5
+    totals = [c + then for c in counts]
+    steps, together = _members_by_counts(gpu_lib, cfgs, states, counts, then)
+    assert steps == totals
+    for c, a, t in zip(cfgs, _alone(gpu_lib, cfgs, states, totals), together):
+        errs = state_errors(t, a, c)
+        bad = {k: v for k, v in errs.items() if not v <= 1e-10}
+        assert not bad, (c.name, bad)
