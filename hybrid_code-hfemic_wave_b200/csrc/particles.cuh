@@ -519,13 +519,14 @@ __global__ void __launch_bounds__(PIPE_THREADS, NVV ? 2 : PIPE_CTAS_PER_SM) push
     if (warp == PIPE_CONSUMER_WARPS) { // ---------------- producer ----------------
         if (lane == 0) {
             int gl = -1, gr = -1; // groups of the chunk being loaded / retired
-            for (int64_t i = 0; i < mine + PIPE_STAGES; ++i) {
-                int const s = static_cast<int>(i % PIPE_STAGES);
+            int      s  = 0; // i % PIPE_STAGES
+            uint32_t ph = 0; // (i / PIPE_STAGES) & 1; both kept incrementally, without a 64-bit division per chunk
+            for (int64_t i = 0; i < mine + PIPE_STAGES; ++i, s = s + 1 == PIPE_STAGES ? 0 : s + 1, ph ^= s == 0 ? 1u : 0u) {
                 if (i >= PIPE_STAGES && i - PIPE_STAGES < mine) { // retire the chunk held by stage s
                     int64_t const   j = i - PIPE_STAGES;
                     gr                = group_of(G, c0 + j, gr);
                     PushArgs const &a = G.g[gr];
-                    if (!mbar_wait(&empty[s], static_cast<uint32_t>((j / PIPE_STAGES) & 1))) {
+                    if (!mbar_wait(&empty[s], ph ^ 1u)) { // the phase of chunk j = i - PIPE_STAGES
                         atomicOr(a.status, ST_TIMEOUT);
                         break;
                     }
@@ -583,8 +584,9 @@ __global__ void __launch_bounds__(PIPE_THREADS, NVV ? 2 : PIPE_CTAS_PER_SM) push
     win.zero(lane);
     unsigned bad = 0;
     int      gc  = -1; // current group
-    for (int64_t i = 0; i < mine; ++i) {
-        int const s  = static_cast<int>(i % PIPE_STAGES);
+    int      s  = 0; // i % PIPE_STAGES
+    uint32_t ph = 0; // (i / PIPE_STAGES) & 1
+    for (int64_t i = 0; i < mine; ++i, s = s + 1 == PIPE_STAGES ? 0 : s + 1, ph ^= s == 0 ? 1u : 0u) {
         int const gi = group_of(G, c0 + i, gc);
         if (gi != gc) { // entering the next group: settle the previous group's window and status
             if (gc >= 0) {
@@ -602,7 +604,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, NVV ? 2 : PIPE_CTAS_PER_SM) push
         }
         PushArgs const &a        = G.g[gc];
         bool const      load_pid = a.randomize != 0;
-        if (!mbar_wait(&full[s], static_cast<uint32_t>((i / PIPE_STAGES) & 1))) {
+        if (!mbar_wait(&full[s], ph)) {
             bad |= ST_TIMEOUT;
             break;
         }

@@ -520,13 +520,14 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
     if (warp == PIPE_CONSUMER_WARPS) { // ---------------- producer ----------------
         if (lane == 0) {
             int gl = -1, gr = -1;
-            for (int64_t i = 0; i < mine + STAGES; ++i) {
-                int const s = static_cast<int>(i % STAGES);
+            int      s  = 0; // i % STAGES
+            uint32_t ph = 0; // (i / STAGES) & 1; both kept incrementally, without a 64-bit division per chunk
+            for (int64_t i = 0; i < mine + STAGES; ++i, s = s + 1 == STAGES ? 0 : s + 1, ph ^= s == 0 ? 1u : 0u) {
                 if (i >= STAGES && i - STAGES < mine) {
                     int64_t const        j = i - STAGES;
                     gr                     = group_of(G, c0 + j, gr);
                     PushArgsMixed const &a = G.g[gr];
-                    if (!mbar_wait(&empty[s], static_cast<uint32_t>((j / STAGES) & 1))) {
+                    if (!mbar_wait(&empty[s], ph ^ 1u)) { // the phase of chunk j = i - STAGES
                         atomicOr(a.status, ST_TIMEOUT);
                         break;
                     }
@@ -586,8 +587,9 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
     win.zero(lane);
     unsigned bad = 0;
     int      gc  = -1;
-    for (int64_t i = 0; i < mine; ++i) {
-        int const s  = static_cast<int>(i % STAGES);
+    int      s  = 0; // i % STAGES
+    uint32_t ph = 0; // (i / STAGES) & 1
+    for (int64_t i = 0; i < mine; ++i, s = s + 1 == STAGES ? 0 : s + 1, ph ^= s == 0 ? 1u : 0u) {
         int const gi = group_of(G, c0 + i, gc);
         if (gi != gc) { // entering the next group: settle the previous group's window and status
             if (gc >= 0) {
@@ -605,7 +607,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
         }
         PushArgsMixed const &a        = G.g[gc];
         bool const           load_pid = a.randomize != 0;
-        if (!mbar_wait(&full[s], static_cast<uint32_t>((i / STAGES) & 1))) {
+        if (!mbar_wait(&full[s], ph)) {
             bad |= ST_TIMEOUT;
             break;
         }
