@@ -691,6 +691,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, NVV ? 2 : PIPE_CTAS_PER_SM) push
                     lo = min(lo, ds1[k].i0), hi = max(hi, ds1[k].i0);
             }
             bool const outside = lo <= hi && (lo < win.base || hi > win.base + SPAN);
+            bool       all_in  = true; // every deposit of the lane inside the window
             if (__any_sync(0xffffffffu, outside)) { // move the window onto this batch
                 win.flush(lane, a);
                 if constexpr (NVV)
@@ -699,31 +700,56 @@ __global__ void __launch_bounds__(PIPE_THREADS, NVV ? 2 : PIPE_CTAS_PER_SM) push
                 int const mhi = __reduce_max_sync(0xffffffffu, hi);
                 int const gap = SPAN - (mhi - mlo);
                 win.base      = gap > 0 ? mlo - gap / 2 : mlo;
+                all_in        = lo > hi || (lo >= win.base && hi <= win.base + SPAN);
             }
+            // collect_all's w v_i v_j at the end position (PartSpecies.cc:236-239)
+            auto nvv_terms = [&](int k, double (&t)[6]) {
+                d3 const v = dv1[k];
+                t[0] = (v.x * v.x) * dw1[k], t[1] = (v.y * v.y) * dw1[k], t[2] = (v.z * v.z) * dw1[k];
+                t[3] = (v.x * v.y) * dw1[k], t[4] = (v.y * v.z) * dw1[k], t[5] = (v.z * v.x) * dw1[k];
+            };
+            if (all_in) { // the usual case: no check per deposit
 #pragma unroll
-            for (int k = 0; k < PIPE_PPT; ++k) {
-                if (dd0[k]) {
-                    double const vw[4] = { dw0[k], dv0[k].x * dw0[k], dv0[k].y * dw0[k], dv0[k].z * dw0[k] };
-                    if (ds0[k].i0 >= win.base && ds0[k].i0 <= win.base + SPAN)
+                for (int k = 0; k < PIPE_PPT; ++k) {
+                    if (dd0[k]) {
+                        double const vw[4] = { dw0[k], dv0[k].x * dw0[k], dv0[k].y * dw0[k], dv0[k].z * dw0[k] };
                         win.add<O>(0, ds0[k], vw, lane);
-                    else
-                        deposit_direct<O>(a, 0, ds0[k], vw);
-                }
-                if (dd1[k]) {
-                    double const vw[4] = { dw1[k], dv1[k].x * dw1[k], dv1[k].y * dw1[k], dv1[k].z * dw1[k] };
-                    bool const   inside = ds1[k].i0 >= win.base && ds1[k].i0 <= win.base + SPAN;
-                    if (inside)
+                    }
+                    if (dd1[k]) {
+                        double const vw[4] = { dw1[k], dv1[k].x * dw1[k], dv1[k].y * dw1[k], dv1[k].z * dw1[k] };
                         win.add<O>(1, ds1[k], vw, lane);
-                    else
-                        deposit_direct<O>(a, 1, ds1[k], vw);
-                    if constexpr (NVV) { // collect_all's w v_i v_j at the end position (PartSpecies.cc:236-239)
-                        d3 const     v = dv1[k];
-                        double const t[6] = { (v.x * v.x) * dw1[k], (v.y * v.y) * dw1[k], (v.z * v.z) * dw1[k],
-                                              (v.x * v.y) * dw1[k], (v.y * v.z) * dw1[k], (v.z * v.x) * dw1[k] };
-                        if (inside)
+                        if constexpr (NVV) {
+                            double t[6];
+                            nvv_terms(k, t);
                             nvw.add<O>(win.base, ds1[k], t, lane);
+                        }
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < PIPE_PPT; ++k) {
+                    if (dd0[k]) {
+                        double const vw[4] = { dw0[k], dv0[k].x * dw0[k], dv0[k].y * dw0[k], dv0[k].z * dw0[k] };
+                        if (ds0[k].i0 >= win.base && ds0[k].i0 <= win.base + SPAN)
+                            win.add<O>(0, ds0[k], vw, lane);
                         else
-                            nvv_direct<O>(a, ds1[k], t);
+                            deposit_direct<O>(a, 0, ds0[k], vw);
+                    }
+                    if (dd1[k]) {
+                        double const vw[4] = { dw1[k], dv1[k].x * dw1[k], dv1[k].y * dw1[k], dv1[k].z * dw1[k] };
+                        bool const   inside = ds1[k].i0 >= win.base && ds1[k].i0 <= win.base + SPAN;
+                        if (inside)
+                            win.add<O>(1, ds1[k], vw, lane);
+                        else
+                            deposit_direct<O>(a, 1, ds1[k], vw);
+                        if constexpr (NVV) {
+                            double t[6];
+                            nvv_terms(k, t);
+                            if (inside)
+                                nvw.add<O>(win.base, ds1[k], t, lane);
+                            else
+                                nvv_direct<O>(a, ds1[k], t);
+                        }
                     }
                 }
             }

@@ -101,6 +101,23 @@ __device__ __forceinline__ ShapeF<O> make_shape_f(int cell, float off)
     }
     return s;
 }
+// the shape of a fixed-point position X (make_shape_f of its cell and offset).  For CIC the
+// position relative to the half grid, X - 2^(F-1), gives the base cell (arithmetic shift) and the
+// weight of the upper cell (its low F bits) in one integer step; the weights are the same floats.
+template <int O>
+__device__ __forceinline__ ShapeF<O> make_shape_fx(int32_t X, int F, float inv_scale)
+{
+    if constexpr (O == 1) {
+        int32_t const H = static_cast<int32_t>(static_cast<uint32_t>(X) - (1u << (F - 1)));
+        ShapeF<1>     s;
+        s.i0   = H >> F;
+        s.w[1] = static_cast<float>(H & ((1 << F) - 1)) * inv_scale;
+        s.w[0] = 1.0f - s.w[1];
+        return s;
+    } else {
+        return make_shape_f<O>(X >> F, static_cast<float>(X & ((1 << F) - 1)) * inv_scale);
+    }
+}
 template <int O>
 __device__ __forceinline__ bool stencil_ok_f(ShapeF<O> const &sh, int Nx)
 {
@@ -658,8 +675,9 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
         float2    off;
 #pragma unroll
         for (int k = 0; k < 2; ++k) { // E and dB at the particles, each into its half of the pairs
-            cell[k] = pos_cell(X[k], a.fbits), el(off, k) = pos_off(X[k], a.fbits, a.inv_scale);
-            ds0[k]  = make_shape_f<O>(cell[k], el(off, k));
+            if constexpr (MIRROR) // the position itself, for the background field
+                cell[k] = pos_cell(X[k], a.fbits), el(off, k) = pos_off(X[k], a.fbits, a.inv_scale);
+            ds0[k] = make_shape_fx<O>(X[k], a.fbits, a.inv_scale);
             in0[k]  = stencil_ok_f(ds0[k], a.Nx);
             push[k] = in0[k] && alive[k] && a.move_steps != 0;
             if (!in0[k] && live[k])
@@ -722,7 +740,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                     el(w, k) = 0.0f, X[k] = half, vk = { 0, 0, 0 };
                 el(v.x, k) = vk.x, el(v.y, k) = vk.y, el(v.z, k) = vk.z;
             }
-            ds1[k] = make_shape_f<O>(pos_cell(X[k], a.fbits), pos_off(X[k], a.fbits, a.inv_scale));
+            ds1[k] = make_shape_fx<O>(X[k], a.fbits, a.inv_scale);
             dd0[k] = live[k] && in0[k] && (a.deposit_mask & 1);
             dd1[k] = live[k] && (a.deposit_mask & 2) && el(w, k) != 0.0f && stencil_ok_f(ds1[k], a.Nx);
         }
@@ -751,6 +769,7 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                     lo = min(lo, ds1[k].i0), hi = max(hi, ds1[k].i0);
             }
             bool const outside = lo <= hi && (lo < win.base || hi > win.base + SPAN);
+            bool       all_in  = true; // every deposit of the lane inside the window
             if (__any_sync(0xffffffffu, outside)) { // move the window onto this batch
                 win.flush(lane, a);
                 if constexpr (NVV)
@@ -759,29 +778,51 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
                 int const mhi = __reduce_max_sync(0xffffffffu, hi);
                 int const gap = SPAN - (mhi - mlo);
                 win.base      = gap > 0 ? mlo - gap / 2 : mlo;
+                all_in        = lo > hi || (lo >= win.base && hi <= win.base + SPAN);
             }
+            // collect_all's w v_i v_j at the end position (PartSpecies.cc:236-239)
+            auto nvv_terms = [&](int k, float (&t)[6]) {
+                float const vx = el(v.x, k), vy = el(v.y, k), vz = el(v.z, k), wk = el(w, k);
+                t[0] = (vx * vx) * wk, t[1] = (vy * vy) * wk, t[2] = (vz * vz) * wk;
+                t[3] = (vx * vy) * wk, t[4] = (vy * vz) * wk, t[5] = (vz * vx) * wk;
+            };
+            if (all_in) { // the usual case: no check per deposit
 #pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                if (dd0[k]) {
-                    if (ds0[k].i0 >= win.base && ds0[k].i0 <= win.base + SPAN)
+                for (int k = 0; k < 2; ++k) {
+                    if (dd0[k])
                         win.add<O>(0, ds0[k], dv0[k], lane);
-                    else
-                        deposit_direct<O>(a, 0, ds0[k], dv0[k]);
-                }
-                if (dd1[k]) {
-                    bool const inside = ds1[k].i0 >= win.base && ds1[k].i0 <= win.base + SPAN;
-                    if (inside)
+                    if (dd1[k]) {
                         win.add<O>(1, ds1[k], dv1[k], lane);
-                    else
-                        deposit_direct<O>(a, 1, ds1[k], dv1[k]);
-                    if constexpr (NVV) { // collect_all's w v_i v_j at the end position (PartSpecies.cc:236-239)
-                        float const vx = el(v.x, k), vy = el(v.y, k), vz = el(v.z, k), wk = el(w, k);
-                        float const t[6] = { (vx * vx) * wk, (vy * vy) * wk, (vz * vz) * wk,
-                                             (vx * vy) * wk, (vy * vz) * wk, (vz * vx) * wk };
-                        if (inside)
+                        if constexpr (NVV) {
+                            float t[6];
+                            nvv_terms(k, t);
                             nvw.add<O>(win.base, ds1[k], t, lane);
+                        }
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    if (dd0[k]) {
+                        if (ds0[k].i0 >= win.base && ds0[k].i0 <= win.base + SPAN)
+                            win.add<O>(0, ds0[k], dv0[k], lane);
                         else
-                            nvv_direct<O>(a, ds1[k], t);
+                            deposit_direct<O>(a, 0, ds0[k], dv0[k]);
+                    }
+                    if (dd1[k]) {
+                        bool const inside = ds1[k].i0 >= win.base && ds1[k].i0 <= win.base + SPAN;
+                        if (inside)
+                            win.add<O>(1, ds1[k], dv1[k], lane);
+                        else
+                            deposit_direct<O>(a, 1, ds1[k], dv1[k]);
+                        if constexpr (NVV) {
+                            float t[6];
+                            nvv_terms(k, t);
+                            if (inside)
+                                nvw.add<O>(win.base, ds1[k], t, lane);
+                            else
+                                nvv_direct<O>(a, ds1[k], t);
+                        }
                     }
                 }
             }

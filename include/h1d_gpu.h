@@ -339,7 +339,7 @@ int h1d_checkpoint_load(h1d_run *run, const void *buffer, size_t size);
 int h1d_step_count(h1d_run *run, int64_t *step);
 
 /* Tuning of a run: steps between cell sorts (0 keeps the current value) and CTAs per SM of the
- * particle pass (0 = the kernel's default, at most 2 for FP64 and 4 for mixed precision).  No
+ * particle pass (0 = the kernel's default, at most 3 for FP64 and 4 for mixed precision).  No
  * counterpart in the reference, which never sorts. */
 int h1d_configure(h1d_run *run, int sort_interval, int push_ctas_per_sm);
 /* Autotuner (no counterpart in the reference): advances the run by real CAM-CL steps while timing
