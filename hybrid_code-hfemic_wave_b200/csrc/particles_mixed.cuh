@@ -682,16 +682,17 @@ __global__ void __launch_bounds__(PIPE_THREADS, PIPE_CTAS_PER_SM_MIXED)
             push[k] = in0[k] && alive[k] && a.move_steps != 0;
             if (!in0[k] && live[k])
                 bad |= ST_OUT_OF_RANGE;
-            if (push[k]) {
+            // a particle that is not pushed reads the records of cells 0..O instead of its own (its
+            // velocity is not updated below), so the loads need no branch
+            int const ib = push[k] ? ds0[k].i0 : 0;
 #pragma unroll
-                for (int j = 0; j <= O; ++j) {
-                    float const *q  = a.EB + EBF_STRIDE * (ds0[k].i0 + j);
-                    float4 const x0 = __ldg(reinterpret_cast<float4 const *>(q));
-                    float4 const x1 = __ldg(reinterpret_cast<float4 const *>(q + 4));
-                    float const  wj = ds0[k].w[j];
-                    el(E.x, k) += x0.x * wj, el(E.y, k) += x0.y * wj, el(E.z, k) += x0.z * wj;
-                    el(dB.x, k) += x0.w * wj, el(dB.y, k) += x1.x * wj, el(dB.z, k) += x1.y * wj;
-                }
+            for (int j = 0; j <= O; ++j) {
+                float const *q  = a.EB + EBF_STRIDE * (ib + j);
+                float4 const x0 = __ldg(reinterpret_cast<float4 const *>(q));
+                float4 const x1 = __ldg(reinterpret_cast<float4 const *>(q + 4));
+                float const  wj = ds0[k].w[j];
+                el(E.x, k) += x0.x * wj, el(E.y, k) += x0.y * wj, el(E.z, k) += x0.z * wj;
+                el(dB.x, k) += x0.w * wj, el(dB.y, k) += x1.x * wj, el(dB.z, k) += x1.y * wj;
             }
         }
         // the Boris push of both particles (as in boris_push, device_common.cuh)
